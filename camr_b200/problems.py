@@ -1,0 +1,130 @@
+"""Initial data of the benchmark configurations (host side, numpy).
+
+Each generator returns the conserved state on the valid cells of the domain
+as a float64 array of shape (NVAR, nz, ny, nx) (component planes outermost,
+i fastest: the Array4 layout), before CAMR::initData's epilogue
+(enforce_consistent_e + computeTemp), which the level driver applies.
+
+State layout (Source/Utils/IndexDefines.H:17-83): URHO 0, UMX 1, UMY 2, UMZ 3,
+UEDEN 4, UEINT 5, UTEMP 6, UFS 7..9.
+"""
+import numpy as np
+
+NVAR = 10
+URHO, UMX, UMY, UMZ, UEDEN, UEINT, UTEMP, UFS = 0, 1, 2, 3, 4, 5, 6, 7
+
+
+def cell_centres(n, prob_lo=(0.0, 0.0, 0.0), dx=None, lo=(0, 0, 0)):
+    """x, y, z of cell centres as prob_lo + (i + 0.5)*dx (Exec/Sod/prob.H:24)."""
+    out = []
+    for d in range(3):
+        i = np.arange(lo[d], lo[d] + n[d], dtype=np.float64)
+        out.append(prob_lo[d] + (i + 0.5) * dx[d])
+    return out
+
+
+def sod(n, dx, prob_lo=(0.0, 0.0, 0.0), direction=0, gamma=1.4, p_l=1.0, p_r=0.1,
+        rho_l=1.0, rho_r=0.125, u_l=0.0, u_r=0.0, x0=0.5):
+    """Sod shock tube, CAMR_initdata of Exec/Sod/prob.H:15-107 (prob.type = direction)."""
+    s = np.zeros((NVAR, n[2], n[1], n[0]))
+    xs = cell_centres(n, prob_lo, dx)
+    x = xs[direction]
+    left = x < x0
+    shape = [1, 1, 1]
+    shape[2 - direction] = n[direction]
+    left = left.reshape(shape)
+    Pt = np.where(left, p_l, p_r)
+    rhot = np.where(left, rho_l, rho_r)
+    ut = np.where(left, u_l, u_r)
+    full = (n[2], n[1], n[0])
+    Pt, rhot, ut = (np.broadcast_to(a, full) for a in (Pt, rhot, ut))
+    s[URHO] = rhot
+    mom = [UMX, UMY, UMY][direction]  # prob.type 2 writes UMY, as the reference does
+    s[mom] = rhot * ut
+    et = Pt / (gamma - 1.0)
+    s[UEINT] = et
+    s[UEDEN] = et + 0.5 * rhot * ut * ut
+    s[UTEMP] = 0.0
+    s[UFS] = 1.0 * s[URHO]
+    s[UFS + 1] = 0.0 * s[URHO]
+    s[UFS + 2] = 0.0 * s[URHO]
+    return s
+
+
+def blobs(n, dx, prob_lo=(0.0, 0.0, 0.0), gamma=1.4, nblobs=16, seed=1, p_blob=10.0,
+          r_min=0.03, r_max=0.08, amp=0.1, p0=1.0):
+    """Smooth periodic density with seeded spherical overpressure blobs.
+
+    rho = 1 + amp*sin(2 pi x) sin(2 pi y) sin(2 pi z), p = p0, zero velocity,
+    p = p_blob inside each blob (periodic distance to the centre < radius).
+    Blob draws from numpy's PCG64 generator seeded with `seed`: per blob the
+    centre (x, y, z) then the radius.
+    """
+    x, y, z = cell_centres(n, prob_lo, dx)
+    X = x[None, None, :]
+    Y = y[None, :, None]
+    Z = z[:, None, None]
+    rho = 1.0 + amp * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y) * np.sin(2 * np.pi * Z)
+    p = np.full((n[2], n[1], n[0]), p0)
+    rng = np.random.default_rng(seed)
+    L = [n[d] * dx[d] for d in range(3)]
+    for _ in range(nblobs):
+        c = rng.uniform(0.0, 1.0, size=3) * np.array(L) + np.array(prob_lo)
+        r = rng.uniform(r_min, r_max)
+        dxs = []
+        for d, arr in enumerate((X, Y, Z)):
+            dd = np.abs(arr - c[d])
+            dd = np.minimum(dd, L[d] - dd)
+            dxs.append(dd)
+        inside = dxs[0] ** 2 + dxs[1] ** 2 + dxs[2] ** 2 < r * r
+        p = np.where(inside, p_blob, p)
+    s = np.zeros((NVAR, n[2], n[1], n[0]))
+    s[URHO] = rho
+    et = p / (gamma - 1.0)
+    s[UEINT] = et
+    s[UEDEN] = et
+    s[UFS] = 1.0 * rho
+    s[UFS + 1] = 0.0 * rho
+    s[UFS + 2] = 0.0 * rho
+    return s
+
+
+def random_smooth(n, seed=0, amp=0.2, vel=0.3, gamma=1.4):
+    """Seeded smooth random state with non-zero velocities and species mix.
+
+    Used by parity tests: every field is a sum of a few random Fourier modes,
+    so slopes, limiters and Riemann branches take many different paths.
+    """
+    rng = np.random.default_rng(seed)
+    grids = np.meshgrid(*(np.arange(n[d]) / n[d] for d in (2, 1, 0)), indexing="ij")
+    Z, Y, X = grids
+
+    def field(a):
+        f = np.zeros((n[2], n[1], n[0]))
+        for _ in range(3):
+            k = rng.integers(1, 4, size=3)
+            ph = rng.uniform(0, 2 * np.pi, size=3)
+            f += a * np.sin(2 * np.pi * k[0] * X + ph[0]) * np.sin(2 * np.pi * k[1] * Y + ph[1]) \
+                * np.sin(2 * np.pi * k[2] * Z + ph[2])
+        return f
+
+    rho = 1.0 + field(amp) + 0.5 * amp * rng.uniform(-1, 1, size=(n[2], n[1], n[0]))
+    p = 1.0 + field(2 * amp) + amp * rng.uniform(-1, 1, size=(n[2], n[1], n[0]))
+    # a few sharp jumps so that flattening and the shock branches fire
+    jump = rng.uniform(0, 1, size=(n[2], n[1], n[0])) < 0.05
+    p = np.where(jump, p * 8.0, p)
+    u = [field(vel) for _ in range(3)]
+    y0 = 0.6 + field(0.1)
+    y1 = 0.3 - 0.5 * field(0.1)
+    y2 = 1.0 - y0 - y1
+    s = np.zeros((NVAR, n[2], n[1], n[0]))
+    s[URHO] = rho
+    for d in range(3):
+        s[UMX + d] = rho * u[d]
+    ke = 0.5 * rho * (u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    s[UEINT] = p / (gamma - 1.0)
+    s[UEDEN] = s[UEINT] + ke
+    s[UFS] = rho * y0
+    s[UFS + 1] = rho * y1
+    s[UFS + 2] = rho * y2
+    return s

@@ -1,0 +1,16 @@
+"""CPU oracle for the hydro advance (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+package, and only as the checker.  It wraps two shared libraries with one C
+interface (oracle_abi.h):
+
+* ``restate``: the repo's CPU restatement (hydro_restate.cpp + level_driver.cpp)
+* ``ref``: the reference's own per-box hydro sources compiled against the
+  AMReX stand-in in amrex_shim/ (ref_glue.cpp + level_driver.cpp), built into
+  oracle/_ref/ by ``make ref`` where the reference sources are available.
+"""
+from .binding import (  # noqa: F401
+    NVAR, QVAR, NGDNV, Params, Level, load, default_params, make_level,
+    hydro_box, advance, advance_fixed_dt, est_dt, init_finalize,
+    expand_state, clean_state, build, lib_path,
+)

@@ -1,0 +1,3 @@
+// Forwarding header of the oracle's AMReX stand-in.
+#pragma once
+#include "AMReX_shim_core.H"

@@ -1,0 +1,164 @@
+"""ctypes binding of the oracle libraries (see oracle_abi.h)."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NVAR, QVAR, NGDNV = 10, 11, 6
+_LIBS = {}
+
+
+def lib_path(kind):
+    if kind == "restate":
+        return os.path.join(HERE, "_lib", "libcamr_oracle.so")
+    if kind == "ref":
+        return os.path.join(HERE, "_ref", "libcamr_ref.so")
+    raise ValueError(kind)
+
+
+def build(ref=None):
+    """Build the restatement, and the reference library when its sources exist."""
+    subprocess.run(["make", "-C", HERE, "all"], check=True)
+    src = os.environ.get("CAMR_REF_SRC", "/root/reference/Source")
+    if ref is None:
+        ref = os.path.isdir(src)
+    if ref:
+        subprocess.run(["make", "-C", HERE, "ref", f"REF_SRC={src}"], check=True)
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "do_mol", "ppm_type", "plm_iorder", "use_pslope", "use_flattening",
+        "transverse_reset_density", "dual_energy_update_E_from_e",
+        "allow_negative_energy", "allow_small_energy", "add_grav_src",
+        "pad0", "pad1")] + [(n, C.c_double) for n in (
+        "difmag", "small", "small_dens", "small_temp", "small_pres",
+        "dual_energy_eta1", "dual_energy_eta2", "const_grav", "cfl",
+        "init_shrink", "change_max", "fixed_dt", "initial_dt", "max_dt",
+        "eos_gamma", "smallu", "small_num")]
+
+
+class Level(C.Structure):
+    _fields_ = [("dom_lo", C.c_int * 3), ("dom_hi", C.c_int * 3),
+                ("is_periodic", C.c_int * 3), ("bc_lo", C.c_int * 3),
+                ("bc_hi", C.c_int * 3), ("max_grid_size", C.c_int * 3),
+                ("tile_size", C.c_int * 3), ("nthreads", C.c_int),
+                ("dx", C.c_double * 3)]
+
+
+_I3 = C.c_int * 3
+_D3 = C.c_double * 3
+_DP = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def load(kind="restate"):
+    if kind in _LIBS:
+        return _LIBS[kind]
+    path = lib_path(kind)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle`)")
+    lib = C.CDLL(path)
+    lib.orc_hydro_box.restype = C.c_long
+    lib.orc_hydro_box.argtypes = [
+        C.POINTER(Params), _I3, _I3, _I3, _I3, _I3, _I3, _DP, _I3, _I3,
+        C.c_void_p, _DP, _I3, _I3, _DP, _DP, _DP, _D3, C.c_double]
+    lib.orc_default_params.argtypes = [C.POINTER(Params)]
+    lib.orc_init_finalize.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP]
+    lib.orc_est_dt.restype = C.c_double
+    lib.orc_est_dt.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP]
+    lib.orc_advance.restype = C.c_long
+    lib.orc_advance.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP, C.c_int,
+                                C.c_int, C.POINTER(C.c_double), C.c_void_p]
+    lib.orc_advance_fixed_dt.restype = C.c_long
+    lib.orc_advance_fixed_dt.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP,
+                                         C.c_int, _DP]
+    lib.orc_expand_state.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP, C.c_int, _DP]
+    lib.orc_clean_state.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP]
+    _LIBS[kind] = lib
+    return lib
+
+
+def default_params(**kw):
+    p = Params()
+    load("restate").orc_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def make_level(n, lo=(0, 0, 0), periodic=(1, 1, 1), bc_lo=(0, 0, 0), bc_hi=(0, 0, 0),
+               dx=None, max_grid_size=(0, 0, 0), tile_size=(0, 0, 0), nthreads=None,
+               prob_len=(1.0, 1.0, 1.0)):
+    lev = Level()
+    for d in range(3):
+        lev.dom_lo[d] = lo[d]
+        lev.dom_hi[d] = lo[d] + n[d] - 1
+        lev.is_periodic[d] = periodic[d]
+        lev.bc_lo[d] = bc_lo[d]
+        lev.bc_hi[d] = bc_hi[d]
+        lev.max_grid_size[d] = max_grid_size[d]
+        lev.tile_size[d] = tile_size[d]
+        lev.dx[d] = dx[d] if dx is not None else prob_len[d] / n[d]
+    lev.nthreads = nthreads or os.cpu_count() or 1
+    return lev
+
+
+def hydro_box(kind, p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, uin, uin_lo, dx, dt,
+              src=None):
+    """Per-box hydro; returns (dsdt on bx, [flx_x, flx_y, flx_z], nassert)."""
+    lib = load(kind)
+    bx_lo, bx_hi = list(bx_lo), list(bx_hi)
+    nb = [bx_hi[d] - bx_lo[d] + 1 for d in range(3)]
+    uin = np.ascontiguousarray(uin, dtype=np.float64)
+    uin_hi = [uin_lo[d] + uin.shape[3 - d] - 1 for d in range(3)]
+    dsdt = np.zeros((NVAR, nb[2], nb[1], nb[0]))
+    flx = []
+    for d in range(3):
+        s = list(nb)
+        s[d] += 1
+        flx.append(np.zeros((NVAR, s[2], s[1], s[0])))
+    srcp = None
+    if src is not None:
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        srcp = src.ctypes.data
+    nass = lib.orc_hydro_box(C.byref(p), _I3(*bx_lo), _I3(*bx_hi), _I3(*dom_lo),
+                             _I3(*dom_hi), _I3(*bclo), _I3(*bchi), uin, _I3(*uin_lo),
+                             _I3(*uin_hi), srcp, dsdt, _I3(*bx_lo), _I3(*bx_hi),
+                             flx[0], flx[1], flx[2], _D3(*dx), float(dt))
+    return dsdt, flx, nass
+
+
+def init_finalize(kind, p, lev, state):
+    load(kind).orc_init_finalize(C.byref(p), C.byref(lev), state)
+
+
+def est_dt(kind, p, lev, state):
+    return load(kind).orc_est_dt(C.byref(p), C.byref(lev), np.ascontiguousarray(state))
+
+
+def advance(kind, p, lev, state, nsteps, first_step=True, dt_prev=0.0):
+    """Advance in place; returns (dt_last, dt_history, nassert)."""
+    hist = np.zeros(nsteps)
+    dtp = C.c_double(dt_prev)
+    n = load(kind).orc_advance(C.byref(p), C.byref(lev), state, nsteps, int(first_step),
+                               C.byref(dtp), hist.ctypes.data)
+    return dtp.value, hist, n
+
+
+def advance_fixed_dt(kind, p, lev, state, dts):
+    dts = np.ascontiguousarray(dts, dtype=np.float64)
+    return load(kind).orc_advance_fixed_dt(C.byref(p), C.byref(lev), state, len(dts), dts)
+
+
+def expand_state(kind, p, lev, state, ng=4):
+    n = [lev.dom_hi[d] - lev.dom_lo[d] + 1 for d in range(3)]
+    border = np.zeros((NVAR, n[2] + 2 * ng, n[1] + 2 * ng, n[0] + 2 * ng))
+    load(kind).orc_expand_state(C.byref(p), C.byref(lev), np.ascontiguousarray(state), ng,
+                                border)
+    return border
+
+
+def clean_state(kind, p, lev, state):
+    load(kind).orc_clean_state(C.byref(p), C.byref(lev), state)
