@@ -1,0 +1,941 @@
+#include "hydro_kernels.cuh"
+
+namespace camr {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+inline unsigned grid_for(int64_t n) { return unsigned((n + kBlock - 1) / kBlock); }
+
+__device__ __forceinline__ int64_t gtid() {
+  return int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+}
+
+__device__ __forceinline__ void load_es(const double* a, const Space& s, int64_t at, double* r) {
+#pragma unroll
+  for (int n = 0; n < ES_N; ++n) r[n] = a[at + n * s.sn];
+}
+__device__ __forceinline__ void store_es(double* a, const Space& s, int64_t at, const double* r) {
+#pragma unroll
+  for (int n = 0; n < ES_N; ++n) a[at + n * s.sn] = r[n];
+}
+__device__ __forceinline__ void load_fr(const double* a, const Space& s, int64_t at, double* r) {
+#pragma unroll
+  for (int n = 0; n < FR_N; ++n) r[n] = a[at + n * s.sn];
+}
+__device__ __forceinline__ CellAux load_aux(const double* q, const Space& s, int64_t at,
+                                            double gamma) {
+  CellAux a;
+  a.c = q[at + SQ_C * s.sn];
+  a.csml = q[at + SQ_CSML * s.sn];
+  a.gamc = gamma;  // qaux QGAMC = EOS::REY2Gam = gamma (Hydro_ctoprim.H:83,96)
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// K1: conservative -> primitive (Source/Hydro/Hydro_ctoprim.H:11-101) and,
+// with sources, primitive sources (:106-157).
+__global__ void __launch_bounds__(kBlock) k_ctoprim(Region r, Space s, DFab u, DFab src,
+                                                     bool has_src, KParams P, double* q,
+                                                     double* srcq, DevError* err) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int64_t at = s.idx(i, j, k);
+  const double rho = u(i, j, k, URHO);
+  if (!(rho > 0.)) {
+    // The reference leaves q untouched here; downstream use is undefined.
+    report_error(err, 1, i, j, k);
+    return;
+  }
+  const double rhoinv = 1.0 / rho;
+  const double vx = u(i, j, k, UMX) * rhoinv;
+  const double vy = u(i, j, k, UMY) * rhoinv;
+  const double vz = u(i, j, k, UMZ) * rhoinv;
+  const double kineng = 0.5 * rho * (vx * vx + vy * vy + vz * vz);
+  const double ueden = u(i, j, k, UEDEN);
+  const double ueint = u(i, j, k, UEINT);
+  if (!P.allow_negative_energy && (!(ueden > 0.) || !(ueint > 0.))) report_error(err, 1, i, j, k);
+  double e;
+  if ((ueden - kineng) / ueden > P.dual_energy_eta1) {
+    e = (ueden - kineng) * rhoinv;
+  } else {
+    e = ueint * rhoinv;
+  }
+  double y[NSPEC];
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) y[sp] = u(i, j, k, UFS + sp) * rhoinv;
+  const double p = (P.gamma - 1.0) * rho * e;
+  const double rhoe = e * rho;
+  const double cs = sqrt(P.gamma * p / rho);
+  q[at + SQ_RHO * s.sn] = rho;
+  q[at + SQ_U * s.sn] = vx;
+  q[at + SQ_V * s.sn] = vy;
+  q[at + SQ_W * s.sn] = vz;
+  q[at + SQ_P * s.sn] = p;
+  q[at + SQ_REINT * s.sn] = rhoe;
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) q[at + (SQ_FS + sp) * s.sn] = y[sp];
+  q[at + SQ_C * s.sn] = cs;
+  q[at + SQ_CSML * s.sn] = dmax(P.small_num, P.small_num * cs);
+  if (has_src) {
+    // hydro_srctoprim with the EOS derivatives of ctoprim
+    // (QDPDE = (gamma-1)*rho, QDPDR = (gamma-1)*e).
+    const double dpde = (P.gamma - 1.0) * rho;
+    const double dpdr = (P.gamma - 1.0) * e;
+    const double srcrho = src(i, j, k, URHO);
+    const double sq_reint = src(i, j, k, UEINT);
+    srcq[at + ES_RHO * s.sn] = srcrho;
+    srcq[at + ES_U * s.sn] = (src(i, j, k, UMX) - vx * srcrho) * rhoinv;
+    srcq[at + ES_V * s.sn] = (src(i, j, k, UMY) - vy * srcrho) * rhoinv;
+    srcq[at + ES_W * s.sn] = (src(i, j, k, UMZ) - vz * srcrho) * rhoinv;
+    srcq[at + ES_REINT * s.sn] = sq_reint;
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) {
+      srcq[at + (ES_FS + sp) * s.sn] = (src(i, j, k, UFS + sp) - y[sp] * srcrho) * rhoinv;
+    }
+    srcq[at + ES_P * s.sn] = dpde * (sq_reint - rhoe * srcrho * rhoinv) * rhoinv + dpdr * srcrho;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: shock flattening of a cell (min over the three directions, as the
+// reference's trace loops do: PLM Godunov_3D.cpp:109-115, PPM PPM.cpp:120-126)
+// and the nodal divergence at the cell's low corner when it is a node of bx
+// (Source/Hydro/Hydro_utils_K.H:12-169).
+__global__ void __launch_bounds__(kBlock) k_flatten_divu(Region r, Space s, KGeom g,
+                                                          KParams P, bool do_flat,
+                                                          const double* q, double* flat,
+                                                          double* divu) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int64_t at = s.idx(i, j, k);
+  if (do_flat) {
+    double fl = 1.0;
+    if (P.use_flattening == 1) {
+      const int64_t st[3] = {1, s.sy, s.sz};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double pp[7], un[7];
+#pragma unroll
+        for (int o = -3; o <= 3; ++o) {
+          pp[o + 3] = q[at + o * st[d] + SQ_P * s.sn];
+          un[o + 3] = q[at + o * st[d] + (SQ_U + d) * s.sn];
+        }
+        fl = dmin(fl, flatten_dir(pp, un));
+      }
+    }
+    flat[at] = fl;
+  }
+  if (i < g.lo[0] || j < g.lo[1] || k < g.lo[2] || i > g.hi[0] + 1 || j > g.hi[1] + 1 ||
+      k > g.hi[2] + 1) {
+    return;
+  }
+  const int NS = CAMR_BC_NOSLIPWALL;
+  const double dxx = g.dx[0], dy = g.dx[1], dz = g.dx[2];
+  auto Q = [&](int ii, int jj, int kk, int n) { return q[s.idx(ii, jj, kk) + n * s.sn]; };
+  const int QUx = SQ_U, QVx = SQ_V, QWx = SQ_W;
+  double ux = 0.25 * (Q(i, j, k, QUx) - Q(i - 1, j, k, QUx) + Q(i, j, k - 1, QUx) -
+                      Q(i - 1, j, k - 1, QUx) + Q(i, j - 1, k, QUx) - Q(i - 1, j - 1, k, QUx) +
+                      Q(i, j - 1, k - 1, QUx) - Q(i - 1, j - 1, k - 1, QUx)) / dxx;
+  double vy = 0.25 * (Q(i, j, k, QVx) - Q(i, j - 1, k, QVx) + Q(i, j, k - 1, QVx) -
+                      Q(i, j - 1, k - 1, QVx) + Q(i - 1, j, k, QVx) - Q(i - 1, j - 1, k, QVx) +
+                      Q(i - 1, j, k - 1, QVx) - Q(i - 1, j - 1, k - 1, QVx)) / dy;
+  double wz = 0.25 * (Q(i, j, k, QWx) - Q(i, j, k - 1, QWx) + Q(i - 1, j, k, QWx) -
+                      Q(i - 1, j, k - 1, QWx) + Q(i, j - 1, k, QWx) - Q(i, j - 1, k - 1, QWx) +
+                      Q(i - 1, j - 1, k, QWx) - Q(i - 1, j - 1, k - 1, QWx)) / dz;
+  const int* dlo = g.dlo;
+  const int* dhi = g.dhi;
+  const int* bclo = g.bclo;
+  const int* bchi = g.bchi;
+  if (i == dlo[0] && bclo[0] == NS) {
+    vy = 0.5 * (Q(i, j, k, QVx) - Q(i, j - 1, k, QVx) + Q(i, j, k - 1, QVx) - Q(i, j - 1, k - 1, QVx)) / dy;
+    wz = 0.5 * (Q(i, j, k, QWx) - Q(i, j, k - 1, QWx) + Q(i, j - 1, k, QWx) - Q(i, j - 1, k - 1, QWx)) / dz;
+  } else if (i == dhi[0] + 1 && bchi[0] == NS) {
+    vy = 0.5 * (Q(i - 1, j, k, QVx) - Q(i - 1, j - 1, k, QVx) + Q(i - 1, j, k - 1, QVx) - Q(i - 1, j - 1, k - 1, QVx)) / dy;
+    wz = 0.5 * (Q(i - 1, j, k, QWx) - Q(i - 1, j, k - 1, QWx) + Q(i - 1, j - 1, k, QWx) - Q(i - 1, j - 1, k - 1, QWx)) / dz;
+  }
+  if (j == dlo[1] && bclo[1] == NS) {
+    ux = 0.5 * (Q(i, j, k, QUx) - Q(i - 1, j, k, QUx) + Q(i, j, k - 1, QUx) - Q(i - 1, j, k - 1, QUx)) / dxx;
+    wz = 0.5 * (Q(i, j, k, QWx) - Q(i, j, k - 1, QWx) + Q(i - 1, j, k, QWx) - Q(i - 1, j, k - 1, QWx)) / dz;
+  } else if (j == dhi[1] + 1 && bchi[1] == NS) {
+    ux = 0.5 * (Q(i, j - 1, k, QUx) - Q(i - 1, j - 1, k, QUx) + Q(i, j - 1, k - 1, QUx) - Q(i - 1, j - 1, k - 1, QUx)) / dxx;
+    wz = 0.5 * (Q(i, j - 1, k, QWx) - Q(i, j - 1, k - 1, QWx) + Q(i - 1, j - 1, k, QWx) - Q(i - 1, j - 1, k - 1, QWx)) / dz;
+  }
+  if (k == dlo[2] && bclo[2] == NS) {
+    ux = 0.5 * (Q(i, j, k, QUx) - Q(i - 1, j, k, QUx) + Q(i, j - 1, k, QUx) - Q(i - 1, j - 1, k, QUx)) / dxx;
+    vy = 0.5 * (Q(i, j, k, QVx) - Q(i, j - 1, k, QVx) + Q(i - 1, j, k, QVx) - Q(i - 1, j - 1, k, QVx)) / dy;
+  } else if (k == dhi[2] + 1 && bchi[2] == NS) {
+    ux = 0.5 * (Q(i, j, k - 1, QUx) - Q(i - 1, j, k - 1, QUx) + Q(i, j - 1, k - 1, QUx) - Q(i - 1, j - 1, k - 1, QUx)) / dxx;
+    vy = 0.5 * (Q(i, j, k - 1, QVx) - Q(i, j - 1, k - 1, QVx) + Q(i - 1, j, k - 1, QVx) - Q(i - 1, j - 1, k - 1, QVx)) / dy;
+  }
+  if (j == dlo[1] && bclo[1] == NS && k == dlo[2] && bclo[2] == NS) {
+    ux = (Q(i, j, k, QUx) - Q(i - 1, j, k, QUx)) / dxx;
+  } else if ((j == dhi[1] + 1 && bchi[1] == NS) && (k == dlo[2] && bclo[2] == NS)) {
+    ux = (Q(i, j - 1, k, QUx) - Q(i - 1, j - 1, k, QUx)) / dxx;
+  } else if ((j == dlo[1] && bclo[1] == NS) && (k == dhi[2] + 1 && bchi[2] == NS)) {
+    ux = (Q(i, j, k - 1, QUx) - Q(i - 1, j, k - 1, QUx)) / dxx;
+  } else if ((j == dhi[1] + 1 && bchi[1] == NS) && (k == dhi[2] + 1 && bchi[2] == NS)) {
+    ux = (Q(i, j - 1, k - 1, QUx) - Q(i - 1, j - 1, k - 1, QUx)) / dxx;
+  }
+  if (i == dlo[0] && bclo[0] == NS && k == dlo[2] && bclo[2] == NS) {
+    vy = (Q(i, j, k, QVx) - Q(i, j - 1, k, QVx)) / dy;
+  } else if ((i == dhi[0] + 1 && bchi[0] == NS) && (k == dlo[2] && bclo[2] == NS)) {
+    vy = (Q(i - 1, j, k, QVx) - Q(i - 1, j - 1, k, QVx)) / dy;
+  } else if ((i == dlo[0] && bclo[0] == NS) && (k == dhi[2] + 1 && bchi[2] == NS)) {
+    vy = (Q(i, j, k - 1, QVx) - Q(i, j - 1, k - 1, QVx)) / dy;
+  } else if ((i == dhi[0] + 1 && bchi[0] == NS) && (k == dhi[2] + 1 && bchi[2] == NS)) {
+    vy = (Q(i - 1, j, k - 1, QVx) - Q(i - 1, j - 1, k - 1, QVx)) / dy;
+  }
+  if (i == dlo[0] && bclo[0] == NS && j == dlo[1] && bclo[1] == NS) {
+    wz = (Q(i, j, k, QWx) - Q(i, j, k - 1, QWx)) / dz;
+  } else if ((i == dhi[0] + 1 && bchi[0] == NS) && (j == dlo[1] && bclo[1] == NS)) {
+    wz = (Q(i - 1, j, k, QWx) - Q(i - 1, j, k - 1, QWx)) / dz;
+  } else if ((i == dlo[0] && bclo[0] == NS) && (j == dhi[1] + 1 && bchi[1] == NS)) {
+    wz = (Q(i, j - 1, k, QWx) - Q(i, j - 1, k - 1, QWx)) / dz;
+  } else if ((i == dhi[0] + 1 && bchi[0] == NS) && (j == dhi[1] + 1 && bchi[1] == NS)) {
+    wz = (Q(i - 1, j - 1, k, QWx) - Q(i - 1, j - 1, k - 1, QWx)) / dz;
+  }
+  divu[at] = ux + vy + wz;
+}
+
+// ---------------------------------------------------------------------------
+// K3: normal predictor of one cell in direction blockIdx.y: PPM with
+// characteristic tracing (PPM.cpp:101-410) or PLM (Godunov_3D.cpp:104-152 +
+// PLM.H:170-323).  Writes the plus state on the cell's low face (SP) and the
+// minus state on its high face (SM).
+__global__ void __launch_bounds__(kBlock) k_trace(Region r, Space s, KGeom g, KParams P,
+                                                   DtRef dtr, const double* q,
+                                                   const double* flat, double* sm0,
+                                                   double* sm1, double* sm2, double* sp0,
+                                                   double* sp1, double* sp2) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int d = blockIdx.y;
+  const int64_t at = s.idx(i, j, k);
+  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
+  const double dt = dtr.get();
+  const double dtdx = dt / g.dx[d];
+  const double fl = flat[at];
+  double* smd = (d == 0) ? sm0 : (d == 1) ? sm1 : sm2;
+  double* spd = (d == 0) ? sp0 : (d == 1) ? sp1 : sp2;
+  const int un_slot = SQ_U + d;
+  const int t1 = (d == 0) ? SQ_V : (d == 1) ? SQ_W : SQ_U;  // QUT of PPM.cpp:84-97
+  const int t2 = (d == 0) ? SQ_W : (d == 1) ? SQ_U : SQ_V;  // QUTT
+  double qp_o[ES_N], qm_o[ES_N];
+
+  auto stencil = [&](int slot, double* v) {
+#pragma unroll
+    for (int o = -2; o <= 2; ++o) v[o + 2] = q[at + o * st + slot * s.sn];
+  };
+
+  if (P.ppm_type == 1) {
+    const double rho_c = q[at + SQ_RHO * s.sn];
+    const double p_c = q[at + SQ_P * s.sn];
+    const double cc = sqrt(P.gamma * p_c / rho_c);  // q_aux(QGAMC)*p/rho, PPM.cpp:113
+    const double un = q[at + un_slot * s.sn];
+    const double speeds[3] = {un - cc, un, un + cc};
+    // rho, un, p, rhoe: all three waves of both integrals.
+    Traced4 Ip, Im;
+    const int slots4[4] = {SQ_RHO, un_slot, SQ_P, SQ_REINT};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      double sv[5];
+      stencil(slots4[v], sv);
+      double smv, spv;
+      ppm_reconstruct(sv[0], sv[1], sv[2], sv[3], sv[4], fl, smv, spv);
+      const double s6 = 6.0 * sv[2] - 3.0 * (smv + spv);
+      double* ipv = (v == 0) ? Ip.rho : (v == 1) ? Ip.un : (v == 2) ? Ip.p : Ip.re;
+      double* imv = (v == 0) ? Im.rho : (v == 1) ? Im.un : (v == 2) ? Im.p : Im.re;
+#pragma unroll
+      for (int w = 0; w < 3; ++w) ppm_wave(smv, spv, s6, speeds[w], dtdx, ipv[w], imv[w]);
+    }
+    // Transverse velocities and species: only the u-wave integrals are read
+    // (PPM.cpp:193-199, :303-305, :401-403).
+    const int slots_mid[2 + NSPEC] = {t1, t2, SQ_FS, SQ_FS + 1, SQ_FS + 2};
+    const int es_mid[2 + NSPEC] = {ES_U + (t1 - SQ_U), ES_U + (t2 - SQ_U), ES_FS, ES_FS + 1,
+                                   ES_FS + 2};
+#pragma unroll
+    for (int v = 0; v < 2 + NSPEC; ++v) {
+      double sv[5];
+      stencil(slots_mid[v], sv);
+      double smv, spv;
+      ppm_reconstruct(sv[0], sv[1], sv[2], sv[3], sv[4], fl, smv, spv);
+      const double s6 = 6.0 * sv[2] - 3.0 * (smv + spv);
+      double ipm, imm;
+      ppm_wave(smv, spv, s6, speeds[1], dtdx, ipm, imm);
+      qp_o[es_mid[v]] = imm;
+      qm_o[es_mid[v]] = ipm;
+    }
+    // The traced gamma (PPM.cpp:146-157) of a gamma-law gas: the stencil is
+    // constant, so both edge values equal gamma exactly, the Colella-Sekora
+    // limiter returns gamma and s6 = 0, hence every wave integral is gamma.
+    const double gam_ref = P.gamma;
+    double o_rho, o_un, o_p, o_re;
+    ppm_project(Im, 0, gam_ref, un, cc, true, P, o_rho, o_un, o_p, o_re);
+    qp_o[ES_RHO] = o_rho;
+    qp_o[ES_U + d] = o_un;
+    qp_o[ES_P] = o_p;
+    qp_o[ES_REINT] = o_re;
+    ppm_project(Ip, 2, gam_ref, un, cc, false, P, o_rho, o_un, o_p, o_re);
+    qm_o[ES_RHO] = o_rho;
+    qm_o[ES_U + d] = o_un;
+    qm_o[ES_P] = o_p;
+    qm_o[ES_REINT] = o_re;
+  } else {
+    // PLM: slopes of every traced component (PLM.H:19-79), then hydro_plm_d.
+    double slope[ES_N];
+    const int slot_of[ES_N] = {SQ_RHO, SQ_U, SQ_V, SQ_W, SQ_P, SQ_REINT, SQ_FS, SQ_FS + 1,
+                               SQ_FS + 2};
+#pragma unroll
+    for (int n = 0; n < ES_N; ++n) {
+      double sv[5];
+      stencil(slot_of[n], sv);
+      slope[n] = plm_slope(sv[0], sv[1], sv[2], sv[3], sv[4], fl, P.plm_iorder);
+    }
+    const int l0 = d;
+    const int l1 = (d == 0) ? 1 : 0;
+    const int l2 = (d == 2) ? 1 : 2;
+    const double cc = q[at + SQ_C * s.sn];
+    const double dtdx_p = dt / g.dx[d];
+    const double cs = cc * cc;
+    const double rho = q[at + SQ_RHO * s.sn];
+    const double vel[3] = {q[at + SQ_U * s.sn], q[at + SQ_V * s.sn], q[at + SQ_W * s.sn]};
+    const double pr = q[at + SQ_P * s.sn];
+    const double rhoe = q[at + SQ_REINT * s.sn];
+    const double enth = ((rhoe + pr) / rho) / cs;
+    const double drho = slope[ES_RHO];
+    const double dvel[3] = {slope[ES_U], slope[ES_V], slope[ES_W]};
+    const double dp = slope[ES_P];
+    const double drhoe = slope[ES_REINT];
+    const double alpham = 0.5 * (dp / (rho * cc) - dvel[d]) * rho / cc;
+    const double alphap = 0.5 * (dp / (rho * cc) + dvel[d]) * rho / cc;
+    const double alpha0r = drho - dp / cs;
+    const double alpha0e = drhoe - dp * enth;
+    const double alpha0v = dvel[l1];
+    const double alpha0w = dvel[l2];
+    const double wv[3] = {vel[d] - cc, vel[d], vel[d] + cc};
+    {
+      const double rho_ref = rho - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * drho;
+      double vel_ref[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        vel_ref[a] = vel[a] - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * dvel[a];
+      const double p_ref = pr - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * dp;
+      const double rhoe_ref = rhoe - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * drhoe;
+      const double apright = 0.25 * dtdx_p * (wv[0] - wv[2]) * (1.0 - copysign(1.0, wv[2])) * alphap;
+      const double amright = 0.0;
+      const double azrright = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0r;
+      const double azeright = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0e;
+      const double azv1rght = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0v;
+      const double azw1rght = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0w;
+      double r0 = rho_ref + apright + amright + azrright;
+      qp_o[ES_RHO] = dmax(r0, P.small_dens);
+      qp_o[ES_U + l0] = vel_ref[l0] + (apright - amright) * cc / rho;
+      qp_o[ES_U + l1] = vel_ref[l1] + azv1rght;
+      qp_o[ES_U + l2] = vel_ref[l2] + azw1rght;
+      double p0 = p_ref + (apright + amright) * cs;
+      qp_o[ES_P] = dmax(p0, P.small_pres);
+      qp_o[ES_REINT] = rhoe_ref + (apright + amright) * enth * cs + azeright;
+    }
+    {
+      const double rho_ref = rho + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * drho;
+      double vel_ref[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        vel_ref[a] = vel[a] + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * dvel[a];
+      const double p_ref = pr + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * dp;
+      const double rhoe_ref = rhoe + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * drhoe;
+      const double apleft = 0.0;
+      const double amleft = 0.25 * dtdx_p * (wv[2] - wv[0]) * (1.0 + copysign(1.0, wv[0])) * alpham;
+      const double azrleft = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0r;
+      const double azeleft = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0e;
+      const double azv1left = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0v;
+      const double azw1left = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0w;
+      double r0 = rho_ref + apleft + amleft + azrleft;
+      qm_o[ES_RHO] = dmax(r0, P.small_dens);
+      qm_o[ES_U + l0] = vel_ref[l0] + (apleft - amleft) * cc / rho;
+      qm_o[ES_U + l1] = vel_ref[l1] + azv1left;
+      qm_o[ES_U + l2] = vel_ref[l2] + azw1left;
+      double p0 = p_ref + (apleft + amleft) * cs;
+      qm_o[ES_P] = dmax(p0, P.small_pres);
+      qm_o[ES_REINT] = rhoe_ref + (apleft + amleft) * enth * cs + azeleft;
+    }
+    const double vel_ad = vel[l0];
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) {
+      const double qn = q[at + (SQ_FS + sp) * s.sn];
+      {
+        const double spzero = (vel_ad > 0) ? -1.0 : vel_ad * dtdx_p;
+        const double acmprght = 0.5 * (-1.0 - spzero) * slope[ES_FS + sp];
+        qp_o[ES_FS + sp] = qn + acmprght;
+      }
+      {
+        const double spzero = vel_ad >= 0 ? vel_ad * dtdx_p : 1.0;
+        const double acmpleft = 0.5 * (1.0 - spzero) * slope[ES_FS + sp];
+        qm_o[ES_FS + sp] = qn + acmpleft;
+      }
+    }
+  }
+  store_es(spd, s, at, qp_o);
+  store_es(smd, s, at + st, qm_o);
+}
+
+// ---------------------------------------------------------------------------
+// K4: first-pass Riemann fluxes (Godunov_3D.cpp:180-216).  blockIdx.y = E.
+__global__ void __launch_bounds__(kBlock) k_flux1(Region r0, Region r1, Region r2, Space s,
+                                                   KGeom g, KParams P, const double* q,
+                                                   double* sm0, double* sm1, double* sm2,
+                                                   double* sp0, double* sp1, double* sp2,
+                                                   double* f0, double* f1, double* f2) {
+  const int E = blockIdx.y;
+  const Region& r = (E == 0) ? r0 : (E == 1) ? r1 : r2;
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  double* smE = (E == 0) ? sm0 : (E == 1) ? sm1 : sm2;
+  double* spE = (E == 0) ? sp0 : (E == 1) ? sp1 : sp2;
+  double* fE = (E == 0) ? f0 : (E == 1) ? f1 : f2;
+  const int64_t st = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
+  const int64_t at = s.idx(i, j, k);
+  double ql[ES_N], qr[ES_N], f[NVAR], qpres, qun;
+  load_es(smE, s, at, ql);
+  load_es(spE, s, at, qr);
+  const CellAux aL = load_aux(q, s, at - st, P.gamma);
+  const CellAux aR = load_aux(q, s, at, P.gamma);
+  const int idx = (E == 0) ? i : (E == 1) ? j : k;
+  cmpflx(ql, qr, aL, aR, E, idx, g.bclo[E], g.bchi[E], g.dlo[E], g.dhi[E], P, f, qpres, qun);
+  // The reference's first-pass cmpflx edits the predictor states in place at
+  // a physical-boundary face; the transverse passes read the edited values.
+  if (idx == g.dlo[E] || idx == g.dhi[E] + 1) {
+    smE[at + ES_RHO * s.sn] = ql[ES_RHO];
+    smE[at + ES_P * s.sn] = ql[ES_P];
+    smE[at + ES_REINT * s.sn] = ql[ES_REINT];
+    spE[at + ES_RHO * s.sn] = qr[ES_RHO];
+    spE[at + ES_P * s.sn] = qr[ES_P];
+    spE[at + ES_REINT * s.sn] = qr[ES_REINT];
+  }
+  fE[at + FR_RHO * s.sn] = f[URHO];
+  fE[at + FR_MX * s.sn] = f[UMX];
+  fE[at + FR_MY * s.sn] = f[UMY];
+  fE[at + FR_MZ * s.sn] = f[UMZ];
+  fE[at + FR_E * s.sn] = f[UEDEN];
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) fE[at + (FR_FS + sp) * s.sn] = f[UFS + sp];
+  fE[at + FR_PRES * s.sn] = qpres;
+  fE[at + FR_UN * s.sn] = qun;
+}
+
+struct Ptr6 {
+  double* p[6];
+};
+struct Ptr3 {
+  double* p[3];
+};
+struct Reg6 {
+  Region r[6];
+};
+
+// ---------------------------------------------------------------------------
+// K5: second pass "D|E": D-face states corrected by E fluxes (hydro_transdo,
+// Godunov_3D.cpp:218-380), then the Riemann flux.  blockIdx.y = combo(D,E).
+__global__ void __launch_bounds__(kBlock) k_flux2(Reg6 regs, Space s, KGeom g, KParams P,
+                                                   DtRef dtr, const double* q, Ptr3 sm,
+                                                   Ptr3 sp, Ptr3 f1, Ptr6 f2) {
+  const int c = blockIdx.y;
+  const int D = c / 2;
+  const int e_ = c % 2;
+  const int E = (e_ < D) ? e_ : e_ + 1;
+  int i, j, k;
+  if (!region_cell(regs.r[c], gtid(), i, j, k)) return;
+  const int64_t stD = (D == 0) ? 1 : (D == 1) ? s.sy : s.sz;
+  const int64_t stE = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
+  const int64_t at = s.idx(i, j, k);
+  const double dt = dtr.get();
+  const double cdtdx = 1.0 / 3.0 * dt / g.dx[E];
+  const double* fE = f1.p[E];
+  double qm[ES_N], qp[ES_N], qn[ES_N];
+  {
+    // minus half of cell f - e_D
+    const int64_t cell = at - stD;
+    double lo[FR_N], hi[FR_N];
+    load_fr(fE, s, cell, lo);
+    load_fr(fE, s, cell + stE, hi);
+    const TTerms t = transdo_terms(lo, hi, cdtdx);
+    load_es(sm.p[D], s, at, qn);
+    transdo_side(t, P.gamma, qn, cdtdx, P, qm);
+  }
+  {
+    // plus half of cell f
+    double lo[FR_N], hi[FR_N];
+    load_fr(fE, s, at, lo);
+    load_fr(fE, s, at + stE, hi);
+    const TTerms t = transdo_terms(lo, hi, cdtdx);
+    load_es(sp.p[D], s, at, qn);
+    transdo_side(t, P.gamma, qn, cdtdx, P, qp);
+  }
+  const CellAux aL = load_aux(q, s, at - stD, P.gamma);
+  const CellAux aR = load_aux(q, s, at, P.gamma);
+  const int idx = (D == 0) ? i : (D == 1) ? j : k;
+  double f[NVAR], qpres, qun;
+  cmpflx(qm, qp, aL, aR, D, idx, g.bclo[D], g.bchi[D], g.dlo[D], g.dhi[D], P, f, qpres, qun);
+  double* o = f2.p[c];
+  o[at + FR_RHO * s.sn] = f[URHO];
+  o[at + FR_MX * s.sn] = f[UMX];
+  o[at + FR_MY * s.sn] = f[UMY];
+  o[at + FR_MZ * s.sn] = f[UMZ];
+  o[at + FR_E * s.sn] = f[UEDEN];
+#pragma unroll
+  for (int spc = 0; spc < NSPEC; ++spc) o[at + (FR_FS + spc) * s.sn] = f[UFS + spc];
+  o[at + FR_PRES * s.sn] = qpres;
+  o[at + FR_UN * s.sn] = qun;
+}
+
+// Artificial viscosity, species normalisation and area weighting of one
+// face flux (Hydro_adjust_fluxes.cpp:13-44; hydro_artif_visc.H:7-64;
+// Hydro_utils_K.H:207-234).  uL/uR: the conserved state of the cells left
+// and right of the face; dv: divu at the face's 4 nodes (corner, +t1, +t2,
+// +t1+t2).
+__device__ __forceinline__ void adjust_flux(double* f, const double* uL, const double* uR,
+                                            const double* dv, int dir, int idx, double dx,
+                                            const KGeom& g, const KParams& P, double area) {
+  const double div = P.difmag * dmin(0.0, 0.25 * (dv[0] + dv[1] + dv[2] + dv[3]));
+  const bool at_bndry = (idx == g.dlo[dir] && g.bclo[dir] == CAMR_BC_NOSLIPWALL) ||
+                        (idx == g.dhi[dir] + 1 && g.bchi[dir] == CAMR_BC_NOSLIPWALL);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) {
+    if (n == UTEMP) continue;
+    const bool is_tang_vel = (dir == 0 && (n == UMY || n == UMZ)) ||
+                             (dir == 1 && (n == UMX || n == UMZ)) ||
+                             (dir == 2 && (n == UMX || n == UMY));
+    if (!(at_bndry && is_tang_vel)) f[n] += dx * div * (uR[n] - uL[n]);
+  }
+  f[UTEMP] = 0.0;
+  double summ = 0.0;
+#pragma unroll
+  for (int n = UFS; n < UFS + NSPEC; ++n) summ += f[n];
+  const double fac = (summ != 0.0) ? f[URHO] / summ : 1.0;
+#pragma unroll
+  for (int n = UFS; n < UFS + NSPEC; ++n) f[n] *= fac;
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) f[n] *= area;
+}
+
+__device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, double qun,
+                                                      int F, int i, int j, int k,
+                                                      const Space& s, const KGeom& g,
+                                                      const KParams& P, const DFab& uin,
+                                                      const double* divu, DFab flx,
+                                                      double* qf) {
+  const int eF[3] = {F == 0, F == 1, F == 2};
+  const int t1 = (F == 0) ? 1 : 0;
+  const int t2 = (F == 2) ? 1 : 2;
+  const int64_t st1 = (t1 == 0) ? 1 : (t1 == 1) ? s.sy : s.sz;
+  const int64_t st2 = (t2 == 0) ? 1 : (t2 == 1) ? s.sy : s.sz;
+  const int64_t at = s.idx(i, j, k);
+  double dv[4];
+  dv[0] = divu[at];
+  dv[1] = divu[at + st1];
+  dv[2] = divu[at + st2];
+  dv[3] = divu[at + st1 + st2];
+  double uL[NVAR], uR[NVAR];
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) {
+    uL[n] = uin(i - eF[0], j - eF[1], k - eF[2], n);
+    uR[n] = uin(i, j, k, n);
+  }
+  const double area = (F == 0) ? g.dx[1] * g.dx[2] : (F == 1) ? g.dx[0] * g.dx[2]
+                                                              : g.dx[0] * g.dx[1];
+  const int idx = (F == 0) ? i : (F == 1) ? j : k;
+  adjust_flux(f, uL, uR, dv, F, idx, g.dx[F], g, P, area);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) flx(i, j, k, n) = f[n];
+  qf[at] = qpres;
+  qf[at + s.sn] = qun;
+}
+
+// ---------------------------------------------------------------------------
+// K6: final fluxes on the F-faces of bx (Godunov_3D.cpp:388-452):
+// hydro_transdd halves of the two cells, Riemann, then adjust_fluxes.
+__global__ void __launch_bounds__(kBlock) k_flux3(Region r0, Region r1, Region r2, Space s,
+                                                   KGeom g, KParams P, DtRef dtr,
+                                                   const double* q, const double* srcq,
+                                                   bool has_src, Ptr3 sm, Ptr3 sp, Ptr6 f2,
+                                                   const double* divu, DFab uin, DFab fx,
+                                                   DFab fy, DFab fz, Ptr3 qf) {
+  const int F = blockIdx.y;
+  const Region& r = (F == 0) ? r0 : (F == 1) ? r1 : r2;
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int t0 = (F == 0) ? 1 : 0;
+  const int t1 = (F == 2) ? 1 : 2;
+  const int64_t stF = (F == 0) ? 1 : (F == 1) ? s.sy : s.sz;
+  const int64_t st0 = (t0 == 0) ? 1 : (t0 == 1) ? s.sy : s.sz;
+  const int64_t st1 = (t1 == 0) ? 1 : (t1 == 1) ? s.sy : s.sz;
+  const double* fa = f2.p[combo(t0, t1)];
+  const double* fb = f2.p[combo(t1, t0)];
+  const int64_t at = s.idx(i, j, k);
+  const double dt = dtr.get();
+  const double hdt = 0.5 * dt;
+  const double cdtdx0 = 0.5 * dt / g.dx[t0];
+  const double cdtdx1 = 0.5 * dt / g.dx[t1];
+  double qm[ES_N], qp[ES_N], qn[ES_N], sq[ES_N];
+#pragma unroll
+  for (int n = 0; n < ES_N; ++n) sq[n] = 0.0;
+  {
+    const int64_t cell = at - stF;
+    double a0[FR_N], a1[FR_N], b0[FR_N], b1[FR_N];
+    load_fr(fa, s, cell, a0);
+    load_fr(fa, s, cell + st0, a1);
+    load_fr(fb, s, cell, b0);
+    load_fr(fb, s, cell + st1, b1);
+    const TDTerms t = transdd_terms(a0, a1, b0, b1, P.gamma, cdtdx0, cdtdx1);
+    if (has_src) load_es(srcq, s, cell, sq);
+    load_es(sm.p[F], s, at, qn);
+    transdd_side(t, qn, sq, hdt, P, qm);
+  }
+  {
+    double a0[FR_N], a1[FR_N], b0[FR_N], b1[FR_N];
+    load_fr(fa, s, at, a0);
+    load_fr(fa, s, at + st0, a1);
+    load_fr(fb, s, at, b0);
+    load_fr(fb, s, at + st1, b1);
+    const TDTerms t = transdd_terms(a0, a1, b0, b1, P.gamma, cdtdx0, cdtdx1);
+    if (has_src) load_es(srcq, s, at, sq);
+    load_es(sp.p[F], s, at, qn);
+    transdd_side(t, qn, sq, hdt, P, qp);
+  }
+  const CellAux aL = load_aux(q, s, at - stF, P.gamma);
+  const CellAux aR = load_aux(q, s, at, P.gamma);
+  const int idx = (F == 0) ? i : (F == 1) ? j : k;
+  double f[NVAR], qpres, qun;
+  cmpflx(qm, qp, aL, aR, F, idx, g.bclo[F], g.bchi[F], g.dlo[F], g.dhi[F], P, f, qpres, qun);
+  const DFab flx = (F == 0) ? fx : (F == 1) ? fy : fz;
+  face_adjust_and_store(f, qpres, qun, F, i, j, k, s, g, P, uin, divu, flx, qf.p[F]);
+}
+
+// ---------------------------------------------------------------------------
+// MOL slopes (Source/Hydro/MOL/MOL_hydro_K.H:24-255) of a cell in direction
+// blockIdx.y.  Slot 1 (entropy) is never read by mol_riemann_{x,y,z} and is
+// not produced.  Stored slots: 0, 2, 3, 4, QREINT, species.
+enum { SL_0 = 0, SL_2 = 1, SL_3 = 2, SL_4 = 3, SL_RE = 4, SL_FS = 5, SL_N = 8 };
+
+__global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Region r2, Space s,
+                                                       KParams P, const double* q,
+                                                       Ptr3 slope) {
+  const int d = blockIdx.y;
+  const Region& r = (d == 0) ? r0 : (d == 1) ? r1 : r2;
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int64_t at = s.idx(i, j, k);
+  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
+  double* o = slope.p[d];
+  if (P.plm_iorder == 1) {
+#pragma unroll
+    for (int n = 0; n < SL_N; ++n) o[at + n * s.sn] = 0.;
+    return;
+  }
+  const double plm_theta = 2.0;
+  auto Q = [&](int off, int slot) { return q[at + off * st + slot * s.sn]; };
+  const int un = SQ_U + d;
+  const int t1 = (d == 0) ? SQ_V : SQ_U;
+  const int t2 = (d == 2) ? SQ_V : SQ_W;
+  const double c = Q(0, SQ_C);
+  double dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
+  double drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
+  o[at + SL_0 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  const double cs2 = c * c;
+  dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
+  drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
+  o[at + SL_2 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  dlft = Q(0, t1) - Q(-1, t1);
+  drgt = Q(1, t1) - Q(0, t1);
+  o[at + SL_3 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  dlft = Q(0, t2) - Q(-1, t2);
+  drgt = Q(1, t2) - Q(0, t2);
+  o[at + SL_4 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  const double enth = (Q(0, SQ_REINT) + Q(0, SQ_P)) / dmax(Q(0, SQ_RHO), P.small_dens);
+  dlft = (Q(0, SQ_REINT) - Q(-1, SQ_REINT)) - enth * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
+  drgt = (Q(1, SQ_REINT) - Q(0, SQ_REINT)) - enth * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
+  o[at + SL_RE * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) {
+    const int n = SQ_FS + sp;
+    dlft = Q(0, SQ_RHO) * Q(0, n) - Q(-1, SQ_RHO) * Q(-1, n) - Q(0, n) * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
+    drgt = Q(1, SQ_RHO) * Q(1, n) - Q(0, SQ_RHO) * Q(0, n) - Q(0, n) * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
+    o[at + (SL_FS + sp) * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  }
+}
+
+// MOL face pass: edge states of mol_riemann_{x,y,z} (MOL_riemann_K.H:12-488),
+// Riemann flux, then adjust_fluxes.
+__global__ void __launch_bounds__(kBlock) k_mol_flux(Region r0, Region r1, Region r2, Space s,
+                                                      KGeom g, KParams P, const double* q,
+                                                      Ptr3 slope, const double* divu,
+                                                      DFab uin, DFab fx, DFab fy, DFab fz,
+                                                      Ptr3 qf) {
+  const int d = blockIdx.y;
+  const Region& r = (d == 0) ? r0 : (d == 1) ? r1 : r2;
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int64_t at = s.idx(i, j, k);
+  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
+  const int64_t atL = at - st;
+  const double* sl = slope.p[d];
+  auto Q = [&](int64_t c, int slot) { return q[c + slot * s.sn]; };
+  auto S = [&](int64_t c, int slot) { return sl[c + slot * s.sn]; };
+  const int un = SQ_U + d;
+  const int t1 = (d == 0) ? SQ_V : SQ_U;
+  const int t2 = (d == 2) ? SQ_V : SQ_W;
+  double ql[ES_N], qr[ES_N];
+  {
+    const double cspeed = Q(atL, SQ_C);
+    const double enth = (Q(atL, SQ_REINT) + Q(atL, SQ_P)) / dmax(Q(atL, SQ_RHO), P.small_dens);
+    const double d0 = S(atL, SL_0), d2 = S(atL, SL_2);
+    double pl = Q(atL, SQ_P) + 0.5 * (d0 + d2) * cspeed;
+    ql[ES_P] = dmax(pl, P.small_pres);
+    ql[ES_U + d] = Q(atL, un) + 0.5 * ((d2 - d0) / Q(atL, SQ_RHO));
+    ql[ES_U + (t1 - SQ_U)] = Q(atL, t1) + 0.5 * S(atL, SL_3);
+    ql[ES_U + (t2 - SQ_U)] = Q(atL, t2) + 0.5 * S(atL, SL_4);
+    double sum = 0.;
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) {
+      const double specden = Q(atL, SQ_RHO) * Q(atL, SQ_FS + sp) +
+                             0.5 * (S(atL, SL_FS + sp) + Q(atL, SQ_FS + sp) * (d0 + d2) / cspeed);
+      sum += specden;
+      ql[ES_FS + sp] = specden;
+    }
+    if (sum < P.small_dens) {
+      // The reference falls back to the RIGHT cell's species here
+      // (MOL_riemann_K.H:82-86).
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = Q(at, SQ_FS + sp);
+    } else {
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = ql[ES_FS + sp] / sum;
+    }
+    ql[ES_RHO] = dmax(sum, P.small_dens);
+    ql[ES_REINT] = Q(atL, SQ_REINT) + 0.5 * (S(atL, SL_RE) + enth * (d0 + d2) / cspeed);
+  }
+  {
+    const double cspeed = Q(at, SQ_C);
+    const double enth = (Q(at, SQ_REINT) + Q(at, SQ_P)) / dmax(Q(at, SQ_RHO), P.small_dens);
+    const double d0 = S(at, SL_0), d2 = S(at, SL_2);
+    double pr = Q(at, SQ_P) - 0.5 * (d0 + d2) * cspeed;
+    qr[ES_P] = dmax(pr, P.small_pres);
+    qr[ES_U + d] = Q(at, un) - 0.5 * ((d2 - d0) / Q(at, SQ_RHO));
+    qr[ES_U + (t1 - SQ_U)] = Q(at, t1) - 0.5 * S(at, SL_3);
+    qr[ES_U + (t2 - SQ_U)] = Q(at, t2) - 0.5 * S(at, SL_4);
+    double sum = 0.;
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) {
+      const double specden = Q(at, SQ_RHO) * Q(at, SQ_FS + sp) -
+                             0.5 * (S(at, SL_FS + sp) + Q(at, SQ_FS + sp) * (d0 + d2) / cspeed);
+      sum += specden;
+      qr[ES_FS + sp] = specden;
+    }
+    if (sum < P.small_dens) {
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = Q(at, SQ_FS + sp);
+    } else {
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = qr[ES_FS + sp] / sum;
+    }
+    qr[ES_RHO] = dmax(sum, P.small_dens);
+    qr[ES_REINT] = Q(at, SQ_REINT) - 0.5 * (S(at, SL_RE) + enth * (d0 + d2) / cspeed);
+  }
+  const CellAux aL = load_aux(q, s, atL, P.gamma);
+  const CellAux aR = load_aux(q, s, at, P.gamma);
+  const int idx = (d == 0) ? i : (d == 1) ? j : k;
+  double f[NVAR], qpres, qun;
+  cmpflx(ql, qr, aL, aR, d, idx, g.bclo[d], g.bchi[d], g.dlo[d], g.dhi[d], P, f, qpres, qun);
+  const DFab flx = (d == 0) ? fx : (d == 1) ? fy : fz;
+  face_adjust_and_store(f, qpres, qun, d, i, j, k, s, g, P, uin, divu, flx, qf.p[d]);
+}
+
+// ---------------------------------------------------------------------------
+// K7: hydro_consup (Hydro_utils_K.H:239-257) with pdivu (:175-202).
+__global__ void __launch_bounds__(kBlock) k_consup(Region r, Space s, KGeom g, DFab fx,
+                                                    DFab fy, DFab fz, Ptr3 qf, DFab dsdt) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int64_t at = s.idx(i, j, k);
+  const double a0 = g.dx[1] * g.dx[2], a1 = g.dx[0] * g.dx[2], a2 = g.dx[0] * g.dx[1];
+  const double vol = g.dx[0] * g.dx[1] * g.dx[2];
+  const double* q1 = qf.p[0];
+  const double* q2 = qf.p[1];
+  const double* q3 = qf.p[2];
+  const int64_t sn = s.sn;
+  const double pdivu =
+      0.5 *
+      ((q1[at + 1] + q1[at]) * (q1[at + 1 + sn] * a0 - q1[at + sn] * a0) +
+       (q2[at + s.sy] + q2[at]) * (q2[at + s.sy + sn] * a1 - q2[at + sn] * a1) +
+       (q3[at + s.sz] + q3[at]) * (q3[at + s.sz + sn] * a2 - q3[at + sn] * a2)) /
+      vol;
+  const double volinv = 1.0 / vol;
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) {
+    dsdt(i, j, k, n) += (fx(i, j, k, n) - fx(i + 1, j, k, n) + fy(i, j, k, n) -
+                         fy(i, j + 1, k, n) + fz(i, j, k, n) - fz(i, j, k + 1, n)) *
+                        volinv;
+  }
+  dsdt(i, j, k, UEINT) -= pdivu;
+}
+
+}  // namespace
+
+size_t work_doubles(const Space& s, bool mol, bool has_src) {
+  size_t c = SQ_N + 1 /*divu*/;
+  if (has_src) c += ES_N;
+  if (!mol) {
+    c += 1 /*flat*/ + 6 * ES_N + 3 * FR_N + 6 * FR_N;
+  } else {
+    c += 3 * SL_N;
+  }
+  c += 3 * 2 /*qf*/;
+  return c * size_t(s.sn);
+}
+
+void work_carve(Work& w, double* base, bool mol, bool has_src) {
+  double* p = base;
+  const int64_t sn = w.s.sn;
+  auto take = [&](int ncomp) {
+    double* r = p;
+    p += int64_t(ncomp) * sn;
+    return r;
+  };
+  w.q = take(SQ_N);
+  w.divu = take(1);
+  w.srcq = has_src ? take(ES_N) : nullptr;
+  w.flat = nullptr;
+  for (int d = 0; d < 3; ++d) w.sm[d] = w.sp[d] = w.f1[d] = w.slope[d] = nullptr;
+  for (int c = 0; c < 6; ++c) w.f2[c] = nullptr;
+  if (!mol) {
+    w.flat = take(1);
+    for (int d = 0; d < 3; ++d) {
+      w.sm[d] = take(ES_N);
+      w.sp[d] = take(ES_N);
+      w.f1[d] = take(FR_N);
+    }
+    for (int c = 0; c < 6; ++c) w.f2[c] = take(FR_N);
+  } else {
+    for (int d = 0; d < 3; ++d) w.slope[d] = take(SL_N);
+  }
+  for (int d = 0; d < 3; ++d) w.qf[d] = take(2);
+}
+
+cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_t st) {
+  const KGeom& g = L.g;
+  const Space& s = w.s;
+  int lo4[3], hi4[3], lo1[3], hi1[3];
+  for (int d = 0; d < 3; ++d) {
+    lo4[d] = g.lo[d] - NGROW;
+    hi4[d] = g.hi[d] + NGROW;
+    lo1[d] = g.lo[d] - 1;
+    hi1[d] = g.hi[d] + 1;
+  }
+  const Region r4 = make_region(lo4, hi4);
+  const Region r1 = make_region(lo1, hi1);
+  k_ctoprim<<<grid_for(r4.count()), kBlock, 0, st>>>(r4, s, L.uin, L.src, L.has_src, L.P, w.q,
+                                                     w.srcq, L.err);
+  k_flatten_divu<<<grid_for(r1.count()), kBlock, 0, st>>>(r1, s, g, L.P, !L.mol, w.q, w.flat,
+                                                          w.divu);
+  count_launch(2);
+  Ptr3 qf{{w.qf[0], w.qf[1], w.qf[2]}};
+  if (!L.mol) {
+    k_trace<<<dim3(grid_for(r1.count()), 3), kBlock, 0, st>>>(
+        r1, s, g, L.P, L.dt, w.q, w.flat, w.sm[0], w.sm[1], w.sm[2], w.sp[0], w.sp[1], w.sp[2]);
+    // first pass: E-faces [lo,hi+1] x grow(bx,1) in the other directions
+    Region rf[3];
+    for (int E = 0; E < 3; ++E) {
+      int lo[3], hi[3];
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = (d == E) ? g.lo[d] : g.lo[d] - 1;
+        hi[d] = (d == E) ? g.hi[d] + 1 : g.hi[d] + 1;
+      }
+      rf[E] = make_region(lo, hi);
+    }
+    int64_t m = 0;
+    for (int E = 0; E < 3; ++E) m = (rf[E].count() > m) ? rf[E].count() : m;
+    k_flux1<<<dim3(grid_for(m), 3), kBlock, 0, st>>>(rf[0], rf[1], rf[2], s, g, L.P, w.q,
+                                                    w.sm[0], w.sm[1], w.sm[2], w.sp[0],
+                                                    w.sp[1], w.sp[2], w.f1[0], w.f1[1],
+                                                    w.f1[2]);
+    // second pass "D|E": D-faces [lo,hi+1], F in grow 1, E in bx
+    Reg6 r6;
+    m = 0;
+    for (int D = 0; D < 3; ++D)
+      for (int E = 0; E < 3; ++E) {
+        if (E == D) continue;
+        const int F = 3 - D - E;
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = g.lo[d];
+          hi[d] = g.hi[d];
+        }
+        hi[D] += 1;
+        lo[F] -= 1;
+        hi[F] += 1;
+        r6.r[combo(D, E)] = make_region(lo, hi);
+        m = (r6.r[combo(D, E)].count() > m) ? r6.r[combo(D, E)].count() : m;
+      }
+    Ptr3 sm{{w.sm[0], w.sm[1], w.sm[2]}}, sp{{w.sp[0], w.sp[1], w.sp[2]}},
+        f1{{w.f1[0], w.f1[1], w.f1[2]}};
+    Ptr6 f2;
+    for (int c = 0; c < 6; ++c) f2.p[c] = w.f2[c];
+    k_flux2<<<dim3(grid_for(m), 6), kBlock, 0, st>>>(r6, s, g, L.P, L.dt, w.q, sm, sp, f1, f2);
+    // final pass on the faces of bx
+    Region rb[3];
+    m = 0;
+    for (int F = 0; F < 3; ++F) {
+      int lo[3], hi[3];
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = g.lo[d];
+        hi[d] = g.hi[d];
+      }
+      hi[F] += 1;
+      rb[F] = make_region(lo, hi);
+      m = (rb[F].count() > m) ? rb[F].count() : m;
+    }
+    k_flux3<<<dim3(grid_for(m), 3), kBlock, 0, st>>>(rb[0], rb[1], rb[2], s, g, L.P, L.dt, w.q,
+                                                    w.srcq, L.has_src, sm, sp, f2, w.divu,
+                                                    L.uin, L.flx[0], L.flx[1], L.flx[2], qf);
+    count_launch(4);
+  } else {
+    Region rs[3], rb[3];
+    int64_t ms = 0, mb = 0;
+    for (int d = 0; d < 3; ++d) {
+      int lo[3], hi[3], flo[3], fhi[3];
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = flo[a] = g.lo[a];
+        hi[a] = fhi[a] = g.hi[a];
+      }
+      lo[d] -= 1;
+      hi[d] += 1;
+      fhi[d] += 1;
+      rs[d] = make_region(lo, hi);
+      rb[d] = make_region(flo, fhi);
+      ms = (rs[d].count() > ms) ? rs[d].count() : ms;
+      mb = (rb[d].count() > mb) ? rb[d].count() : mb;
+    }
+    Ptr3 sl{{w.slope[0], w.slope[1], w.slope[2]}};
+    k_mol_slope<<<dim3(grid_for(ms), 3), kBlock, 0, st>>>(rs[0], rs[1], rs[2], s, L.P, w.q, sl);
+    k_mol_flux<<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(rb[0], rb[1], rb[2], s, g, L.P, w.q,
+                                                        sl, w.divu, L.uin, L.flx[0], L.flx[1],
+                                                        L.flx[2], qf);
+    count_launch(2);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t st) {
+  cudaError_t e = launch_hydro_fluxes(L, w, st);
+  if (e != cudaSuccess) return e;
+  const Region rb = make_region(L.g.lo, L.g.hi);
+  Ptr3 qf{{w.qf[0], w.qf[1], w.qf[2]}};
+  k_consup<<<grid_for(rb.count()), kBlock, 0, st>>>(rb, w.s, L.g, L.flx[0], L.flx[1], L.flx[2],
+                                                    qf, L.dsdt);
+  count_launch(1);
+  return cudaGetLastError();
+}
+
+}  // namespace camr

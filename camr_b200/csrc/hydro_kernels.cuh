@@ -1,0 +1,71 @@
+// Kernels of the per-box hydro right-hand side and their launcher.
+//
+// Work decomposition (CTU, the reference's Godunov_umeth):
+//   K1 ctoprim        cells of grow(bx,4)            -> Q (+ SRCQ)
+//   K2 flatten/divu   cells of grow(bx,1)            -> FLAT, DIVU on nodes of bx
+//   K3 trace          (cell of grow(bx,1), dir)      -> SM[d], SP[d] face states
+//   K4 flux1          (E-face, E)                    -> F1[E], BC edits of SM/SP
+//   K5 flux2          (D-face, D|E combination)      -> F2[D|E]
+//   K6 flux3          (F-face of bx, F)              -> flx[F] (caller), QF[F]
+//   K7 consup         cells of bx                    -> dsdt += ...
+// MOL (MOL_umeth): K1, K2 (divu only), slopes per (cell, dir), one face
+// pass (edge states + Riemann + adjust), K7.
+// Every face flux is computed once, on exactly the faces whose value reaches
+// the box's fluxes and dsdt.
+#pragma once
+
+#include "hydro_point.cuh"
+
+namespace camr {
+
+// dt either as a value or read from device memory (the level driver keeps
+// the dt sequence on the device so a whole step can be graph-captured).
+struct DtRef {
+  double v;
+  const double* p;
+  __device__ __forceinline__ double get() const { return p ? *p : v; }
+};
+
+// Intermediate arrays of one box, all indexed in the box's Space.
+struct Work {
+  Space s;
+  double* q;        // SQ_N comps
+  double* srcq;     // ES_N comps (only with sources)
+  double* flat;     // 1 comp
+  double* divu;     // 1 comp (nodes)
+  double* sm[3];    // ES_N comps each (minus state on d-faces)
+  double* sp[3];    // ES_N comps each (plus state on d-faces)
+  double* f1[3];    // FR_N comps each
+  double* f2[6];    // FR_N comps each, index combo(D,E)
+  double* qf[3];    // 2 comps each: interface pressure, normal velocity
+  double* slope[3]; // MOL: 8 comps each
+};
+
+// Combination index of the second-pass "D|E" fluxes.
+__host__ __device__ __forceinline__ int combo(int D, int E) {
+  return D * 2 + ((E > D) ? E - 1 : E);
+}
+
+size_t work_doubles(const Space& s, bool mol, bool has_src);
+void work_carve(Work& w, double* base, bool mol, bool has_src);
+
+struct HydroLaunch {
+  KGeom g;
+  KParams P;
+  DFab uin;
+  DFab src;        // valid when has_src
+  bool has_src;
+  bool mol;
+  DFab flx[3];     // caller flux fabs (faces of bx)
+  DFab dsdt;       // caller dsdt (bx), accumulated
+  DtRef dt;
+  DevError* err;
+};
+
+// Issue the whole per-box hydro on `stream` (7 or 5 kernel launches).
+cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t stream);
+
+// Pieces reused by the level driver.
+cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_t stream);
+
+}  // namespace camr

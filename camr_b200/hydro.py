@@ -1,0 +1,173 @@
+"""Host-side mirror of CAMR's hydro call surface over the C ABI.
+
+* :func:`hydro_umdrv` mirrors the per-box ``hydro_umdrv``
+  (Source/Hydro/Hydro.H:11-35): Sborder fab in, area-weighted face fluxes and
+  an accumulated dSdt out.
+* :class:`Level` mirrors one AMR level's ``CAMR::advance`` loop
+  (Source/CAMR_advance.cpp:38-164) with Amr's dt logic.
+
+Device memory comes from torch tensors (plumbing only); all arithmetic runs
+in libcamr_b200.so.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import native
+from .native import BC, NVAR, Fab, Geom, LevelDesc, check, default_params, lib
+
+NGROW = 4
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def fab_of(t, lo):
+    """Array4 view of a contiguous (ncomp, nz, ny, nx) float64 CUDA tensor."""
+    torch = _torch()
+    if t.dtype != torch.float64 or not t.is_contiguous() or not t.is_cuda:
+        raise ValueError("fab tensors must be contiguous float64 CUDA tensors")
+    nc, nz, ny, nx = t.shape
+    f = Fab()
+    f.ptr = t.data_ptr()
+    for d, n in enumerate((nx, ny, nz)):
+        f.lo[d] = lo[d]
+        f.hi[d] = lo[d] + n - 1
+    f.jstride = nx
+    f.kstride = nx * ny
+    f.nstride = nx * ny * nz
+    f.ncomp = nc
+    return f
+
+
+def make_geom(n, dom_lo=(0, 0, 0), is_periodic=(1, 1, 1), bc_lo=(0, 0, 0), bc_hi=(0, 0, 0),
+              dx=None, prob_lo=(0.0, 0.0, 0.0), prob_hi=(1.0, 1.0, 1.0)):
+    g = Geom()
+    for d in range(3):
+        g.dom_lo[d] = dom_lo[d]
+        g.dom_hi[d] = dom_lo[d] + n[d] - 1
+        g.is_periodic[d] = int(is_periodic[d])
+        g.bc_lo[d] = BC[bc_lo[d]] if isinstance(bc_lo[d], str) else int(bc_lo[d])
+        g.bc_hi[d] = BC[bc_hi[d]] if isinstance(bc_hi[d], str) else int(bc_hi[d])
+        g.dx[d] = dx[d] if dx is not None else (prob_hi[d] - prob_lo[d]) / n[d]
+        g.prob_lo[d] = prob_lo[d]
+    return g
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        torch = _torch()
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def hydro_umdrv(bx_lo, bx_hi, geom, uin, uin_lo, dsdt, flx, params, dt, src=None, stream=None):
+    """Per-box hydro (the drop-in for the reference's hydro_umdrv).
+
+    uin: (NVAR, nz, ny, nx) CUDA float64 tensor covering grow(bx,4) starting
+    at uin_lo; dsdt: (NVAR, ...) on bx, accumulated; flx: three tensors on
+    the faces of bx (overwritten).  Raises CamrError on a non-OK status.
+    """
+    lo = (C.c_int * 3)(*bx_lo)
+    hi = (C.c_int * 3)(*bx_hi)
+    fu = fab_of(uin, uin_lo)
+    fd = fab_of(dsdt, bx_lo)
+    ff = [fab_of(f, bx_lo) for f in flx]
+    fs = fab_of(src, uin_lo) if src is not None else None
+    st = lib().camr_hydro_umdrv(C.byref(lo), C.byref(hi), C.byref(geom), C.byref(fu),
+                                C.byref(fs) if fs is not None else None, C.byref(fd),
+                                C.byref(ff[0]), C.byref(ff[1]), C.byref(ff[2]),
+                                C.byref(params), float(dt), C.c_void_p(_stream_ptr(stream)))
+    check(st, "camr_hydro_umdrv")
+
+
+class Level:
+    """One uniform level advanced on the GPU through the C ABI."""
+
+    def __init__(self, geom, params, max_grid_size=(0, 0, 0), use_graph=True, stream=None):
+        """stream=None: the library gives the level a non-blocking stream of its own."""
+        desc = LevelDesc()
+        desc.geom = geom
+        for d in range(3):
+            desc.max_grid_size[d] = max_grid_size[d]
+        desc.use_graph = int(use_graph)
+        self.params = params
+        self.geom = geom
+        self.n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+        self.ncell = self.n[0] * self.n[1] * self.n[2]
+        sp = None if stream is None else getattr(stream, "cuda_stream", stream)
+        h = C.c_void_p()
+        check(lib().camr_level_create(C.byref(desc), C.byref(params), C.c_void_p(sp),
+                                      C.byref(h)), "camr_level_create")
+        self._h = h
+        s = C.c_void_p()
+        check(lib().camr_level_stream(self._h, C.byref(s)), "camr_level_stream")
+        self.stream_ptr = s.value or 0
+
+    def torch_stream(self):
+        """The level's stream as a torch stream (for CUDA events)."""
+        torch = _torch()
+        return torch.cuda.ExternalStream(self.stream_ptr)
+
+    def close(self):
+        if self._h:
+            lib().camr_level_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, state):
+        """state: numpy (host) or CUDA tensor of shape (NVAR, nz, ny, nx)."""
+        if isinstance(state, np.ndarray):
+            a = np.ascontiguousarray(state, dtype=np.float64)
+            assert a.shape == (NVAR, self.n[2], self.n[1], self.n[0])
+            check(lib().camr_level_set_state(self._h, a.ctypes.data, 1), "set_state")
+            self.sync()
+        else:
+            assert state.is_cuda and state.is_contiguous()
+            check(lib().camr_level_set_state(self._h, state.data_ptr(), 0), "set_state")
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.empty((NVAR, self.n[2], self.n[1], self.n[0]))
+        if isinstance(out, np.ndarray):
+            check(lib().camr_level_get_state(self._h, out.ctypes.data, 1), "get_state")
+        else:
+            check(lib().camr_level_get_state(self._h, out.data_ptr(), 0), "get_state")
+        return out
+
+    def init_finalize(self):
+        check(lib().camr_level_init_finalize(self._h), "init_finalize")
+
+    def advance(self, nsteps, fixed_dts=None):
+        ptr = None
+        if fixed_dts is not None:
+            arr = np.ascontiguousarray(fixed_dts, dtype=np.float64)
+            assert len(arr) == nsteps
+            ptr = arr.ctypes.data
+            self._keep = arr
+        check(lib().camr_level_advance(self._h, int(nsteps), ptr), "advance")
+
+    def last_dt(self):
+        v = C.c_double()
+        check(lib().camr_level_last_dt(self._h, C.byref(v)), "last_dt")
+        return v.value
+
+    def est_dt(self):
+        v = C.c_double()
+        check(lib().camr_level_est_dt(self._h, C.byref(v)), "est_dt")
+        return v.value
+
+    def error(self):
+        info = native.ErrorInfo()
+        lib().camr_level_get_error(self._h, C.byref(info))
+        return (info.code, info.i, info.j, info.k)
+
+    def sync(self):
+        _torch().cuda.synchronize()

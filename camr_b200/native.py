@@ -1,0 +1,115 @@
+"""ctypes binding of libcamr_b200.so (the C ABI of include/camr_b200.h).
+
+The shared library is built in-tree (camr_b200/_lib/) by camr_b200.build.
+Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libcamr_b200.so")
+
+NVAR = 10
+STATUS = {0: "CAMR_OK", 1: "CAMR_ERR_INVALID", 2: "CAMR_ERR_UNSUPPORTED", 3: "CAMR_ERR_CUDA",
+          4: "CAMR_ERR_NUMERIC", 5: "CAMR_ERR_NOMEM", 6: "CAMR_ERR_TIMEOUT"}
+
+# Boundary-condition words (Source/Utils/IndexDefines.H:7-12).
+BC = {"Interior": 0, "Inflow": 1, "Outflow": 2, "Symmetry": 3, "SlipWall": 4, "NoSlipWall": 5}
+
+
+class CamrError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)}")
+
+
+class HydroParams(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "do_mol", "ppm_type", "plm_iorder", "use_pslope", "use_flattening",
+        "transverse_reset_density", "dual_energy_update_E_from_e", "allow_negative_energy",
+        "allow_small_energy", "add_grav_src", "riemann_solver", "pad0")] + [
+        (n, C.c_double) for n in (
+            "difmag", "small", "small_dens", "small_temp", "small_pres", "dual_energy_eta1",
+            "dual_energy_eta2", "const_grav", "cfl", "init_shrink", "change_max", "fixed_dt",
+            "initial_dt", "max_dt", "eos_gamma", "smallu", "small_num")]
+
+
+class Fab(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("lo", C.c_int * 3), ("hi", C.c_int * 3),
+                ("jstride", C.c_int64), ("kstride", C.c_int64), ("nstride", C.c_int64),
+                ("ncomp", C.c_int), ("pad0", C.c_int)]
+
+
+class Geom(C.Structure):
+    _fields_ = [("dom_lo", C.c_int * 3), ("dom_hi", C.c_int * 3), ("is_periodic", C.c_int * 3),
+                ("bc_lo", C.c_int * 3), ("bc_hi", C.c_int * 3), ("pad0", C.c_int),
+                ("dx", C.c_double * 3), ("prob_lo", C.c_double * 3)]
+
+
+class LevelDesc(C.Structure):
+    _fields_ = [("geom", Geom), ("max_grid_size", C.c_int * 3), ("use_graph", C.c_int)]
+
+
+class ErrorInfo(C.Structure):
+    _fields_ = [("code", C.c_int), ("i", C.c_int), ("j", C.c_int), ("k", C.c_int)]
+
+
+_lib = None
+
+# Every entry point of include/camr_b200.h with its ctypes signature.
+SIGNATURES = {
+    "camr_default_params": (None, [C.POINTER(HydroParams)]),
+    "camr_version": (C.c_char_p, []),
+    "camr_hydro_umdrv": (C.c_int, [C.POINTER(C.c_int * 3), C.POINTER(C.c_int * 3),
+                                   C.POINTER(Geom), C.POINTER(Fab), C.POINTER(Fab),
+                                   C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
+                                   C.POINTER(Fab), C.POINTER(HydroParams), C.c_double,
+                                   C.c_void_p]),
+    "camr_level_create": (C.c_int, [C.POINTER(LevelDesc), C.POINTER(HydroParams), C.c_void_p,
+                                    C.POINTER(C.c_void_p)]),
+    "camr_level_destroy": (C.c_int, [C.c_void_p]),
+    "camr_level_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_level_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_level_init_finalize": (C.c_int, [C.c_void_p]),
+    "camr_level_advance": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "camr_level_last_dt": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "camr_level_est_dt": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "camr_level_state_fab": (C.c_int, [C.c_void_p, C.POINTER(Fab)]),
+    "camr_level_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
+    "camr_launch_count": (C.c_int64, []),
+    "camr_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_last_error_string": (C.c_char_p, []),
+}
+
+
+def lib():
+    """Load libcamr_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"camr_b200 native library not built: {LIB_PATH} "
+                          "(run `python -c 'import camr_b200.build as b; b.build()'`)")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return _lib
+
+
+def check(status, what):
+    if status != 0:
+        detail = lib().camr_last_error_string().decode() if status == 3 else ""
+        raise CamrError(status, f"{what} {detail}".strip())
+
+
+def default_params(**overrides):
+    p = HydroParams()
+    lib().camr_default_params(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p

@@ -1,0 +1,205 @@
+/* camr_b200: B200-native (sm_100a) hydro advance for CAMR, C ABI.
+ *
+ * Every entry point takes plain pointers and sizes, returns a camr_status and
+ * never aborts.  Device arrays use the Array4 layout of the reference:
+ * component planes outermost, i fastest,
+ *     idx = (i-lo0) + (j-lo1)*jstride + (k-lo2)*kstride + n*nstride.
+ * State index layout (3-D, 3 species, Source/Utils/IndexDefines.H:17-83):
+ *     URHO 0, UMX 1, UMY 2, UMZ 3, UEDEN 4, UEINT 5, UTEMP 6, UFS 7..9.
+ * All arithmetic is FP64 and reproduces the reference bit for bit (the
+ * library is built with -fmad=false; the reference CPU build uses
+ * -ffp-contract=off).
+ *
+ * Streams are passed as `void*` holding a cudaStream_t (NULL = the legacy
+ * default stream).  Work is stream-ordered; nothing synchronises the device
+ * unless the entry point says so.
+ */
+#ifndef CAMR_B200_H
+#define CAMR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CAMR_OK = 0,
+  CAMR_ERR_INVALID = 1,       /* bad argument (null pointer, empty box, ...) */
+  CAMR_ERR_UNSUPPORTED = 2,   /* parameter combination not implemented */
+  CAMR_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+  CAMR_ERR_NUMERIC = 4,       /* device error word set (see camr_get_error) */
+  CAMR_ERR_NOMEM = 5,         /* device allocation failed */
+  CAMR_ERR_TIMEOUT = 6        /* a bounded device wait gave up */
+} camr_status;
+
+/* Boundary-condition words of CAMR.lo_bc / CAMR.hi_bc
+ * (Source/Utils/IndexDefines.H:7-12). */
+enum {
+  CAMR_BC_INTERIOR = 0, CAMR_BC_INFLOW = 1, CAMR_BC_OUTFLOW = 2,
+  CAMR_BC_SYMMETRY = 3, CAMR_BC_SLIPWALL = 4, CAMR_BC_NOSLIPWALL = 5
+};
+
+enum { CAMR_NVAR = 10, CAMR_QVAR = 11, CAMR_NGDNV = 6 };
+
+/* The CAMR.* ParmParse parameters the hydro advance reads, by their
+ * reference names (Source/Params/_cpp_parameters), plus eos_gamma (the
+ * reference's compile-time EOS::gamma, Source/EOS/GammaLaw/EOS.H:16) and the
+ * two constants of Source/Utils/CAMR_Constants.H:9-10.  camr_default_params
+ * fills the reference defaults. */
+typedef struct {
+  int do_mol;
+  int ppm_type;
+  int plm_iorder;
+  int use_pslope;
+  int use_flattening;
+  int transverse_reset_density;
+  int dual_energy_update_E_from_e;
+  int allow_negative_energy;
+  int allow_small_energy;
+  int add_grav_src;
+  int riemann_solver;   /* 0 = the reference's two-shock solver (riemannus) */
+  int pad0;
+  double difmag;
+  double small;
+  double small_dens;
+  double small_temp;
+  double small_pres;
+  double dual_energy_eta1;
+  double dual_energy_eta2;
+  double const_grav;
+  double cfl;
+  double init_shrink;
+  double change_max;
+  double fixed_dt;
+  double initial_dt;
+  double max_dt;
+  double eos_gamma;
+  double smallu;
+  double small_num;
+} camr_hydro_params;
+
+/* Non-owning view of one Array4 on the device (AMReX FArrayBox::array()). */
+typedef struct {
+  double* ptr;
+  int lo[3];
+  int hi[3];
+  int64_t jstride;
+  int64_t kstride;
+  int64_t nstride;
+  int ncomp;
+  int pad0;
+} camr_fab;
+
+/* Geometry of the level a box belongs to. */
+typedef struct {
+  int dom_lo[3];
+  int dom_hi[3];
+  int is_periodic[3];
+  int bc_lo[3];
+  int bc_hi[3];
+  int pad0;
+  double dx[3];
+  double prob_lo[3];
+} camr_geom;
+
+/* Device error record (first failure wins). */
+typedef struct {
+  int code;      /* 0 none, 1 non-positive density/energy seen by ctoprim, 2 NaN,
+                    3 density exactly zero in enforce_min_density, 4 index
+                    out of range */
+  int i, j, k;   /* cell of the first failure */
+} camr_error_info;
+
+/* Fill every default of Source/Params/_cpp_parameters. */
+void camr_default_params(camr_hydro_params* p);
+
+/* Library version string. */
+const char* camr_version(void);
+
+/* ---------------------------------------------------------------------
+ * Per-box hydro: the drop-in for
+ *   hydro_umdrv (Source/Hydro/Hydro.H:11-35, Source/Hydro/Hydro_umdrv.cpp:11-93)
+ * together with the caller-side ctoprim/srctoprim launches of
+ *   CAMR::construct_hydro_source (Source/Hydro/CAMR_construct_hydro_source.cpp:95-143).
+ * uin: NVAR comps covering at least grow(bx,4), ghost cells filled and
+ * cleaned (the reference's Sborder).  dsdt: NVAR on bx, ACCUMULATED (+=)
+ * as the reference does.  flx[d]: NVAR on surroundingNodes(bx,d),
+ * overwritten with the area-weighted fluxes (artificial viscosity included)
+ * that feed the flux registers.  area[d]/vol may be NULL for Cartesian
+ * metrics from geom->dx.  Temporaries come from a stream-ordered pool
+ * (cudaMallocAsync), as the reference takes them from The_Async_Arena.
+ * Sources: src may be NULL (zero sources); otherwise NVAR comps on the same
+ * region as uin (the reference's sources_for_hydro).
+ */
+camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3],
+                             const camr_geom* geom, const camr_fab* uin,
+                             const camr_fab* src, camr_fab* dsdt,
+                             camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                             const camr_hydro_params* p, double dt,
+                             void* stream);
+
+/* ---------------------------------------------------------------------
+ * Level-level API: one uniform level owned by the library on one GPU.
+ * Replaces CAMR::CAMR_advance (Source/CAMR_advance.cpp:38-164) with its
+ * construct_hydro_source box loop, expand_state/clean_state
+ * (Source/CAMR.cpp:1243-1262), the gravity source Saxpys, post_timestep's
+ * clean_state, and Amr's dt logic (estTimeStep/computeNewDt,
+ * Source/CAMR.cpp:490-635).  The level's boxes are advanced as one padded
+ * domain: results are identical for any box decomposition.
+ */
+typedef struct camr_level camr_level;
+
+typedef struct {
+  camr_geom geom;
+  int max_grid_size[3];   /* box size of the level (enforce_min_density's
+                             neighbour window); 0 = whole domain */
+  int use_graph;          /* capture each step in a CUDA graph */
+} camr_level_desc;
+
+/* stream: the cudaStream_t the level issues its work on; NULL makes the
+ * library create a non-blocking stream of its own (the legacy default
+ * stream cannot be captured into a CUDA graph). */
+camr_status camr_level_create(const camr_level_desc* desc,
+                              const camr_hydro_params* p, void* stream,
+                              camr_level** out);
+camr_status camr_level_destroy(camr_level* lev);
+
+/* Copy the valid-cell state in/out.  `state` holds NVAR comps on the
+ * domain's valid cells, shape (NVAR, nz, ny, nx), i fastest.  host != 0:
+ * the pointer is host memory (pinned for async); otherwise device memory. */
+camr_status camr_level_set_state(camr_level* lev, const double* state, int host);
+camr_status camr_level_get_state(camr_level* lev, double* state, int host);
+
+/* CAMR::initData's epilogue: enforce_consistent_e then computeTemp. */
+camr_status camr_level_init_finalize(camr_level* lev);
+
+/* Advance nsteps coarse steps.  The dt of each step is computed on the
+ * device (first step: computeInitialDt; later: computeNewDt) unless
+ * fixed_dts is non-NULL (host array of nsteps dts).  Stream-ordered; no
+ * host synchronisation. */
+camr_status camr_level_advance(camr_level* lev, int nsteps, const double* fixed_dts);
+
+/* dt history / last dt (synchronises the level's stream). */
+camr_status camr_level_last_dt(camr_level* lev, double* dt);
+camr_status camr_level_est_dt(camr_level* lev, double* dt);
+
+/* The stream the level's work is issued on (for events / synchronisation). */
+camr_status camr_level_stream(camr_level* lev, void** stream);
+
+/* Device pointer to the padded state (domain grown by 4), and its layout. */
+camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab);
+
+/* Read and clear the device error word (synchronises the level's stream). */
+camr_status camr_level_get_error(camr_level* lev, camr_error_info* info);
+
+/* Text of the last CUDA error this thread saw in the library ("" if none). */
+const char* camr_last_error_string(void);
+
+/* Kernel launches issued by the library so far (for accounting). */
+int64_t camr_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

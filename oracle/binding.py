@@ -106,7 +106,7 @@ def make_level(n, lo=(0, 0, 0), periodic=(1, 1, 1), bc_lo=(0, 0, 0), bc_hi=(0, 0
 
 
 def hydro_box(kind, p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, uin, uin_lo, dx, dt,
-              src=None):
+              src=None, dsdt_init=None):
     """Per-box hydro; returns (dsdt on bx, [flx_x, flx_y, flx_z], nassert)."""
     lib = load(kind)
     bx_lo, bx_hi = list(bx_lo), list(bx_hi)
@@ -114,6 +114,8 @@ def hydro_box(kind, p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, uin, uin_lo, dx
     uin = np.ascontiguousarray(uin, dtype=np.float64)
     uin_hi = [uin_lo[d] + uin.shape[3 - d] - 1 for d in range(3)]
     dsdt = np.zeros((NVAR, nb[2], nb[1], nb[0]))
+    if dsdt_init is not None:
+        dsdt[...] = dsdt_init
     flx = []
     for d in range(3):
         s = list(nb)
