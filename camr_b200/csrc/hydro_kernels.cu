@@ -835,13 +835,19 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
   }
   const Region r4 = make_region(lo4, hi4);
   const Region r1 = make_region(lo1, hi1);
+  auto mark = [&](const char* what) {
+    if (L.timer) L.timer->mark(st, what);
+  };
+  mark("ctoprim");
   k_ctoprim<<<grid_for(r4.count()), kBlock, 0, st>>>(r4, s, L.uin, L.src, L.has_src, L.P, w.q,
                                                      w.srcq, L.err);
+  mark("flatten_divu");
   k_flatten_divu<<<grid_for(r1.count()), kBlock, 0, st>>>(r1, s, g, L.P, !L.mol, w.q, w.flat,
                                                           w.divu);
   count_launch(2);
   Ptr3 qf{{w.qf[0], w.qf[1], w.qf[2]}};
   if (!L.mol) {
+    mark("trace");
     k_trace<<<dim3(grid_for(r1.count()), 3), kBlock, 0, st>>>(
         r1, s, g, L.P, L.dt, w.q, w.flat, w.sm[0], w.sm[1], w.sm[2], w.sp[0], w.sp[1], w.sp[2]);
     // first pass: E-faces [lo,hi+1] x grow(bx,1) in the other directions
@@ -856,6 +862,7 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
     }
     int64_t m = 0;
     for (int E = 0; E < 3; ++E) m = (rf[E].count() > m) ? rf[E].count() : m;
+    mark("flux1");
     k_flux1<<<dim3(grid_for(m), 3), kBlock, 0, st>>>(rf[0], rf[1], rf[2], s, g, L.P, w.q,
                                                     w.sm[0], w.sm[1], w.sm[2], w.sp[0],
                                                     w.sp[1], w.sp[2], w.f1[0], w.f1[1],
@@ -882,6 +889,7 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
         f1{{w.f1[0], w.f1[1], w.f1[2]}};
     Ptr6 f2;
     for (int c = 0; c < 6; ++c) f2.p[c] = w.f2[c];
+    mark("flux2");
     k_flux2<<<dim3(grid_for(m), 6), kBlock, 0, st>>>(r6, s, g, L.P, L.dt, w.q, sm, sp, f1, f2);
     // final pass on the faces of bx
     Region rb[3];
@@ -896,6 +904,7 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       rb[F] = make_region(lo, hi);
       m = (rb[F].count() > m) ? rb[F].count() : m;
     }
+    mark("flux3");
     k_flux3<<<dim3(grid_for(m), 3), kBlock, 0, st>>>(rb[0], rb[1], rb[2], s, g, L.P, L.dt, w.q,
                                                     w.srcq, L.has_src, sm, sp, f2, w.divu,
                                                     L.uin, L.flx[0], L.flx[1], L.flx[2], qf);
@@ -918,7 +927,9 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       mb = (rb[d].count() > mb) ? rb[d].count() : mb;
     }
     Ptr3 sl{{w.slope[0], w.slope[1], w.slope[2]}};
+    mark("mol_slope");
     k_mol_slope<<<dim3(grid_for(ms), 3), kBlock, 0, st>>>(rs[0], rs[1], rs[2], s, L.P, w.q, sl);
+    mark("mol_flux");
     k_mol_flux<<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(rb[0], rb[1], rb[2], s, g, L.P, w.q,
                                                         sl, w.divu, L.uin, L.flx[0], L.flx[1],
                                                         L.flx[2], qf);

@@ -49,6 +49,21 @@ __host__ __device__ __forceinline__ int combo(int D, int E) {
 size_t work_doubles(const Space& s, bool mol, bool has_src);
 void work_carve(Work& w, double* base, bool mol, bool has_src);
 
+// Optional per-stage event marks (profiling): mark() records the next event
+// on the launch stream before a stage is issued.
+struct StageTimer {
+  static constexpr int kMax = 40;
+  cudaEvent_t ev[kMax];
+  const char* name[kMax];
+  int n = 0;
+  void mark(cudaStream_t st, const char* what) {
+    if (n < kMax) {
+      name[n] = what;
+      cudaEventRecord(ev[n++], st);
+    }
+  }
+};
+
 struct HydroLaunch {
   KGeom g;
   KParams P;
@@ -60,6 +75,7 @@ struct HydroLaunch {
   DFab dsdt;       // caller dsdt (bx), accumulated
   DtRef dt;
   DevError* err;
+  StageTimer* timer = nullptr;
 };
 
 // Issue the whole per-box hydro on `stream` (7 or 5 kernel launches).

@@ -606,6 +606,7 @@ struct camr_level {
   double* staging;     // packed (NVAR x ncell) device buffer for state I/O
   double* fixed_dev;   // device copy of one fixed dt
   bool own_stream;     // the library created `stream` (caller passed NULL)
+  int64_t kernels_per_step;  // launches inside one captured step
 };
 
 namespace {
@@ -861,7 +862,8 @@ camr_status camr_level_init_finalize(camr_level* lev) {
   return cuda_status(cudaGetLastError());
 }
 
-static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_dev) {
+static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_dev,
+                              StageTimer* tm = nullptr) {
   LevelState& S = lev->st;
   const LGeom& L = lev->L;
   cudaStream_t st = lev->stream;
@@ -869,16 +871,23 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   const int64_t npad = int64_t(L.pn[0]) * L.pn[1] * L.pn[2];
   DtCtl c{lev->hp.cfl, lev->hp.max_dt, lev->hp.fixed_dt, lev->hp.initial_dt,
           lev->hp.init_shrink, lev->hp.change_max};
+  auto mark = [&](const char* what) {
+    if (tm) tm->mark(st, what);
+  };
   if (first) {
+    mark("est_dt");
     k_reset_bits<<<1, 1, 0, st>>>(S.dtmin_bits);
     k_est_dt<<<gv, kBlk, 0, st>>>(L, lev->P, S.S, S.dtmin_bits);
     count_launch(2);
   }
   // dt of this step (computeInitialDt / computeNewDt) from the CFL min of
   // the current state.
+  mark("dt_next");
   k_dt_next<<<1, 1, 0, st>>>(c, first ? 1 : 0, fixed_dev, S.dtmin_bits, S.dt_cur, S.dt_hist,
                              S.nstep, lev->hist_cap);
+  mark("clean_copy");
   k_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, S.S, S.S_old, S.err);
+  mark("expand");
   k_expand<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S_old, S.B, S.err);
   count_launch(3);
   HydroLaunch H;
@@ -896,6 +905,7 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   H.mol = lev->hp.do_mol != 0;
   H.dt = DtRef{0.0, S.dt_cur};
   H.err = reinterpret_cast<DevError*>(S.err);
+  H.timer = tm;
   auto sdfab = [&](double* p) {
     DFab f;
     f.p = p;
@@ -918,21 +928,26 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   cudaError_t e = launch_hydro_fluxes(H, S.w, st);
   if (e != cudaSuccess) return e;
   if (!H.mol) {
+    mark("update");
     k_update_ctu<<<gv, kBlk, 0, st>>>(L, sp, lev->P, S.dt_cur, S.B, S.S_old, fp, S.S,
                                       S.dtmin_bits, S.err);
     count_launch();
   } else {
+    mark("update_mol1");
     k_update_mol1<<<gv, kBlk, 0, st>>>(L, sp, lev->P, S.dt_cur, S.B, S.S_old, fp, S.S);
+    mark("expand2");
     k_expand<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S, S.B2, S.err);
     count_launch(2);
     H.uin = sdfab(S.B2);
     H.src = H.uin;
     e = launch_hydro_fluxes(H, S.w, st);
     if (e != cudaSuccess) return e;
+    mark("update_mol2");
     k_update_mol2<<<gv, kBlk, 0, st>>>(L, sp, lev->P, S.dt_cur, S.B2, S.S_old, fp, S.S,
                                        S.dtmin_bits, S.err);
     count_launch();
   }
+  mark("end");
   return cudaGetLastError();
 }
 
@@ -956,7 +971,11 @@ camr_status camr_level_advance(camr_level* lev, int nsteps, const double* fixed_
         cudaGraph_t g;
         e = cudaStreamBeginCapture(lev->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_status(e);
+        const int64_t before = g_launches.load();
         cudaError_t e1 = issue_step(lev, false, nullptr);
+        // issuing during capture counted the kernels once; replays add them
+        lev->kernels_per_step = g_launches.load() - before;
+        g_launches -= lev->kernels_per_step;
         e = cudaStreamEndCapture(lev->stream, &g);
         if (e1 != cudaSuccess) return cuda_status(e1);
         if (e != cudaSuccess) return cuda_status(e);
@@ -966,6 +985,7 @@ camr_status camr_level_advance(camr_level* lev, int nsteps, const double* fixed_
         lev->graph_ready = true;
       }
       e = cudaGraphLaunch(lev->graph, lev->stream);
+      count_launch(int(lev->kernels_per_step));
     } else {
       e = issue_step(lev, first, fixed_dev);
     }
@@ -1011,6 +1031,32 @@ camr_status camr_level_est_dt(camr_level* lev, double* dt) {
   if (estdt_hydro < estdt) estdt = estdt_hydro;
   *dt = estdt;
   return CAMR_OK;
+}
+
+camr_status camr_level_profile_step(camr_level* lev, float* stage_ms, const char** names,
+                                    int max_stages, int* nstages) {
+  if (!lev || !stage_ms || !nstages || lev->steps_taken == 0) return CAMR_ERR_INVALID;
+  StageTimer tm;
+  for (int i = 0; i < StageTimer::kMax; ++i) {
+    if (cudaEventCreate(&tm.ev[i]) != cudaSuccess) return CAMR_ERR_CUDA;
+  }
+  cudaError_t e = issue_step(lev, false, nullptr, &tm);
+  if (e == cudaSuccess) e = cudaEventSynchronize(tm.ev[tm.n - 1]);
+  int ns = 0;
+  for (int i = 0; i + 1 < tm.n && ns < max_stages; ++i, ++ns) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, tm.ev[i], tm.ev[i + 1]);
+    stage_ms[ns] = ms;
+    if (names) names[ns] = tm.name[i];
+  }
+  *nstages = ns;
+  for (int i = 0; i < StageTimer::kMax; ++i) cudaEventDestroy(tm.ev[i]);
+  lev->steps_taken++;
+  return cuda_status(e);
+}
+
+int64_t camr_level_kernels_per_step(camr_level* lev) {
+  return lev ? lev->kernels_per_step : 0;
 }
 
 camr_status camr_level_stream(camr_level* lev, void** stream) {

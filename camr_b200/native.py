@@ -79,6 +79,11 @@ SIGNATURES = {
     "camr_launch_count": (C.c_int64, []),
     "camr_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_last_error_string": (C.c_char_p, []),
+    "camr_level_profile_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_float),
+                                          C.POINTER(C.c_char_p), C.c_int,
+                                          C.POINTER(C.c_int)]),
+    "camr_level_kernels_per_step": (C.c_int64, [C.c_void_p]),
+    "camr_measure_fp64_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
 }
 
 

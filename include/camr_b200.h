@@ -184,6 +184,17 @@ camr_status camr_level_advance(camr_level* lev, int nsteps, const double* fixed_
 camr_status camr_level_last_dt(camr_level* lev, double* dt);
 camr_status camr_level_est_dt(camr_level* lev, double* dt);
 
+/* Take one (uncaptured) step with a CUDA event before every stage and
+ * return each stage's device time in ms and its name (static strings).
+ * Requires a previous step (the dt comes from computeNewDt). */
+camr_status camr_level_profile_step(camr_level* lev, float* stage_ms,
+                                    const char** names, int max_stages,
+                                    int* nstages);
+
+/* Kernel launches inside one graph-captured step (0 before the first
+ * capture). */
+int64_t camr_level_kernels_per_step(camr_level* lev);
+
 /* The stream the level's work is issued on (for events / synchronisation). */
 camr_status camr_level_stream(camr_level* lev, void** stream);
 
@@ -196,7 +207,12 @@ camr_status camr_level_get_error(camr_level* lev, camr_error_info* info);
 /* Text of the last CUDA error this thread saw in the library ("" if none). */
 const char* camr_last_error_string(void);
 
-/* Kernel launches issued by the library so far (for accounting). */
+/* Measure the FP64 FMA throughput of the device with independent DFMA
+ * chains (a roofline denominator); synchronises.  Result in TFLOP/s. */
+camr_status camr_measure_fp64_peak(double* tflops, void* stream);
+
+/* Kernel launches issued by the library so far (for accounting; graph
+ * replays count the kernels they contain). */
 int64_t camr_launch_count(void);
 
 #ifdef __cplusplus
