@@ -204,6 +204,34 @@ camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab);
 /* Read and clear the device error word (synchronises the level's stream). */
 camr_status camr_level_get_error(camr_level* lev, camr_error_info* info);
 
+/* ---------------------------------------------------------------------
+ * Allocation-free per-box hydro.  No counterpart in the reference: it is
+ * camr_hydro_umdrv for callers that may not allocate device memory while
+ * they run (code inside an arena or pool that owns all device memory,
+ * real-time loops that forbid allocator calls after start-up, hosts where
+ * cudaMalloc/cudaMallocAsync would fight another allocator).  Same
+ * arguments and results as camr_hydro_umdrv; the scratch is a fixed
+ * CAMR_NOALLOC_SCRATCH_BYTES array in device memory, which every GPU that
+ * loads the library keeps until the process exits.  Boxes whose scratch
+ * does not fit are rejected with CAMR_ERR_INVALID (camr_noalloc_last_error
+ * says why).  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * race on it and must be serialised by the caller.  Calls no cudaMalloc,
+ * cudaFree or allocating library routine.
+ */
+#define CAMR_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx_hi[3],
+                                     const camr_geom* geom, const camr_fab* uin,
+                                     const camr_fab* src, camr_fab* dsdt,
+                                     camr_fab* flx0, camr_fab* flx1,
+                                     camr_fab* flx2, const camr_hydro_params* p,
+                                     double dt, void* stream);
+
+/* Why the last camr_hydro_umdrv_noalloc call on this thread was rejected
+ * ("" if it was not). */
+const char* camr_noalloc_last_error(void);
+
 /* Text of the last CUDA error this thread saw in the library ("" if none). */
 const char* camr_last_error_string(void);
 
