@@ -6,6 +6,21 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// Minimum resident blocks per SM of the heavy kernels (register budget);
+// chosen by measurement (see the tuning notes in the design document).
+#ifndef CAMR_MINB_TRACE
+#define CAMR_MINB_TRACE 4
+#endif
+#ifndef CAMR_MINB_FLUX1
+#define CAMR_MINB_FLUX1 1
+#endif
+#ifndef CAMR_MINB_FLUX2
+#define CAMR_MINB_FLUX2 1
+#endif
+#ifndef CAMR_MINB_FLUX3
+#define CAMR_MINB_FLUX3 4
+#endif
+
 inline unsigned grid_for(int64_t n) { return unsigned((n + kBlock - 1) / kBlock); }
 
 __device__ __forceinline__ int64_t gtid() {
@@ -204,24 +219,19 @@ __global__ void __launch_bounds__(kBlock) k_flatten_divu(Region r, Space s, KGeo
 // characteristic tracing (PPM.cpp:101-410) or PLM (Godunov_3D.cpp:104-152 +
 // PLM.H:170-323).  Writes the plus state on the cell's low face (SP) and the
 // minus state on its high face (SM).
-__global__ void __launch_bounds__(kBlock) k_trace(Region r, Space s, KGeom g, KParams P,
-                                                   DtRef dtr, const double* q,
-                                                   const double* flat, double* sm0,
-                                                   double* sm1, double* sm2, double* sp0,
-                                                   double* sp1, double* sp2) {
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
-  const int d = blockIdx.y;
+template <int d>
+__device__ __forceinline__ void trace_body(int i, int j, int k, const Space& s,
+                                           const KGeom& g, const KParams& P,
+                                           const DtRef& dtr, const double* q,
+                                           const double* flat, double* smd, double* spd) {
   const int64_t at = s.idx(i, j, k);
   const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
   const double dt = dtr.get();
   const double dtdx = dt / g.dx[d];
   const double fl = flat[at];
-  double* smd = (d == 0) ? sm0 : (d == 1) ? sm1 : sm2;
-  double* spd = (d == 0) ? sp0 : (d == 1) ? sp1 : sp2;
-  const int un_slot = SQ_U + d;
-  const int t1 = (d == 0) ? SQ_V : (d == 1) ? SQ_W : SQ_U;  // QUT of PPM.cpp:84-97
-  const int t2 = (d == 0) ? SQ_W : (d == 1) ? SQ_U : SQ_V;  // QUTT
+  constexpr int un_slot = SQ_U + d;
+  constexpr int t1 = (d == 0) ? SQ_V : (d == 1) ? SQ_W : SQ_U;  // QUT of PPM.cpp:84-97
+  constexpr int t2 = (d == 0) ? SQ_W : (d == 1) ? SQ_U : SQ_V;  // QUTT
   double qp_o[ES_N], qm_o[ES_N];
 
   auto stencil = [&](int slot, double* v) {
@@ -293,9 +303,9 @@ __global__ void __launch_bounds__(kBlock) k_trace(Region r, Space s, KGeom g, KP
       stencil(slot_of[n], sv);
       slope[n] = plm_slope(sv[0], sv[1], sv[2], sv[3], sv[4], fl, P.plm_iorder);
     }
-    const int l0 = d;
-    const int l1 = (d == 0) ? 1 : 0;
-    const int l2 = (d == 2) ? 1 : 2;
+    constexpr int l0 = d;
+    constexpr int l1 = (d == 0) ? 1 : 0;
+    constexpr int l2 = (d == 2) ? 1 : 2;
     const double cc = q[at + SQ_C * s.sn];
     const double dtdx_p = dt / g.dx[d];
     const double cs = cc * cc;
@@ -381,20 +391,26 @@ __global__ void __launch_bounds__(kBlock) k_trace(Region r, Space s, KGeom g, KP
   store_es(smd, s, at + st, qm_o);
 }
 
-// ---------------------------------------------------------------------------
-// K4: first-pass Riemann fluxes (Godunov_3D.cpp:180-216).  blockIdx.y = E.
-__global__ void __launch_bounds__(kBlock) k_flux1(Region r0, Region r1, Region r2, Space s,
-                                                   KGeom g, KParams P, const double* q,
-                                                   double* sm0, double* sm1, double* sm2,
-                                                   double* sp0, double* sp1, double* sp2,
-                                                   double* f0, double* f1, double* f2) {
-  const int E = blockIdx.y;
-  const Region& r = (E == 0) ? r0 : (E == 1) ? r1 : r2;
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_TRACE) k_trace(Region r, Space s, KGeom g, KParams P,
+                                                   DtRef dtr, const double* q,
+                                                   const double* flat, double* sm0,
+                                                   double* sm1, double* sm2, double* sp0,
+                                                   double* sp1, double* sp2) {
   int i, j, k;
   if (!region_cell(r, gtid(), i, j, k)) return;
-  double* smE = (E == 0) ? sm0 : (E == 1) ? sm1 : sm2;
-  double* spE = (E == 0) ? sp0 : (E == 1) ? sp1 : sp2;
-  double* fE = (E == 0) ? f0 : (E == 1) ? f1 : f2;
+  switch (blockIdx.y) {
+    case 0: trace_body<0>(i, j, k, s, g, P, dtr, q, flat, sm0, sp0); break;
+    case 1: trace_body<1>(i, j, k, s, g, P, dtr, q, flat, sm1, sp1); break;
+    default: trace_body<2>(i, j, k, s, g, P, dtr, q, flat, sm2, sp2); break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K4: first-pass Riemann fluxes (Godunov_3D.cpp:180-216).  blockIdx.y = E.
+template <int E>
+__device__ __forceinline__ void flux1_body(int i, int j, int k, const Space& s, const KGeom& g,
+                                           const KParams& P, const double* q, double* smE,
+                                           double* spE, double* fE) {
   const int64_t st = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
   const int64_t at = s.idx(i, j, k);
   double ql[ES_N], qr[ES_N], f[NVAR], qpres, qun;
@@ -403,7 +419,7 @@ __global__ void __launch_bounds__(kBlock) k_flux1(Region r0, Region r1, Region r
   const CellAux aL = load_aux(q, s, at - st, P.gamma);
   const CellAux aR = load_aux(q, s, at, P.gamma);
   const int idx = (E == 0) ? i : (E == 1) ? j : k;
-  cmpflx(ql, qr, aL, aR, E, idx, g.bclo[E], g.bchi[E], g.dlo[E], g.dhi[E], P, f, qpres, qun);
+  cmpflx<E>(ql, qr, aL, aR, idx, g.bclo[E], g.bchi[E], g.dlo[E], g.dhi[E], P, f, qpres, qun);
   // The reference's first-pass cmpflx edits the predictor states in place at
   // a physical-boundary face; the transverse passes read the edited values.
   if (idx == g.dlo[E] || idx == g.dhi[E] + 1) {
@@ -425,6 +441,25 @@ __global__ void __launch_bounds__(kBlock) k_flux1(Region r0, Region r1, Region r
   fE[at + FR_UN * s.sn] = qun;
 }
 
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX1) k_flux1(Region r0, Region r1, Region r2, Space s,
+                                                   KGeom g, KParams P, const double* q,
+                                                   double* sm0, double* sm1, double* sm2,
+                                                   double* sp0, double* sp1, double* sp2,
+                                                   double* f0, double* f1, double* f2) {
+  int i, j, k;
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(r0, gtid(), i, j, k)) flux1_body<0>(i, j, k, s, g, P, q, sm0, sp0, f0);
+      break;
+    case 1:
+      if (region_cell(r1, gtid(), i, j, k)) flux1_body<1>(i, j, k, s, g, P, q, sm1, sp1, f1);
+      break;
+    default:
+      if (region_cell(r2, gtid(), i, j, k)) flux1_body<2>(i, j, k, s, g, P, q, sm2, sp2, f2);
+      break;
+  }
+}
+
 struct Ptr6 {
   double* p[6];
 };
@@ -438,21 +473,16 @@ struct Reg6 {
 // ---------------------------------------------------------------------------
 // K5: second pass "D|E": D-face states corrected by E fluxes (hydro_transdo,
 // Godunov_3D.cpp:218-380), then the Riemann flux.  blockIdx.y = combo(D,E).
-__global__ void __launch_bounds__(kBlock) k_flux2(Reg6 regs, Space s, KGeom g, KParams P,
-                                                   DtRef dtr, const double* q, Ptr3 sm,
-                                                   Ptr3 sp, Ptr3 f1, Ptr6 f2) {
-  const int c = blockIdx.y;
-  const int D = c / 2;
-  const int e_ = c % 2;
-  const int E = (e_ < D) ? e_ : e_ + 1;
-  int i, j, k;
-  if (!region_cell(regs.r[c], gtid(), i, j, k)) return;
+template <int D, int E>
+__device__ __forceinline__ void flux2_body(int i, int j, int k, const Space& s, const KGeom& g,
+                                           const KParams& P, const DtRef& dtr, const double* q,
+                                           const double* smD, const double* spD,
+                                           const double* fE, double* o) {
   const int64_t stD = (D == 0) ? 1 : (D == 1) ? s.sy : s.sz;
   const int64_t stE = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
   const int64_t at = s.idx(i, j, k);
   const double dt = dtr.get();
   const double cdtdx = 1.0 / 3.0 * dt / g.dx[E];
-  const double* fE = f1.p[E];
   double qm[ES_N], qp[ES_N], qn[ES_N];
   {
     // minus half of cell f - e_D
@@ -461,7 +491,7 @@ __global__ void __launch_bounds__(kBlock) k_flux2(Reg6 regs, Space s, KGeom g, K
     load_fr(fE, s, cell, lo);
     load_fr(fE, s, cell + stE, hi);
     const TTerms t = transdo_terms(lo, hi, cdtdx);
-    load_es(sm.p[D], s, at, qn);
+    load_es(smD, s, at, qn);
     transdo_side(t, P.gamma, qn, cdtdx, P, qm);
   }
   {
@@ -470,15 +500,14 @@ __global__ void __launch_bounds__(kBlock) k_flux2(Reg6 regs, Space s, KGeom g, K
     load_fr(fE, s, at, lo);
     load_fr(fE, s, at + stE, hi);
     const TTerms t = transdo_terms(lo, hi, cdtdx);
-    load_es(sp.p[D], s, at, qn);
+    load_es(spD, s, at, qn);
     transdo_side(t, P.gamma, qn, cdtdx, P, qp);
   }
   const CellAux aL = load_aux(q, s, at - stD, P.gamma);
   const CellAux aR = load_aux(q, s, at, P.gamma);
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
   double f[NVAR], qpres, qun;
-  cmpflx(qm, qp, aL, aR, D, idx, g.bclo[D], g.bchi[D], g.dlo[D], g.dhi[D], P, f, qpres, qun);
-  double* o = f2.p[c];
+  cmpflx<D>(qm, qp, aL, aR, idx, g.bclo[D], g.bchi[D], g.dlo[D], g.dhi[D], P, f, qpres, qun);
   o[at + FR_RHO * s.sn] = f[URHO];
   o[at + FR_MX * s.sn] = f[UMX];
   o[at + FR_MY * s.sn] = f[UMY];
@@ -490,13 +519,37 @@ __global__ void __launch_bounds__(kBlock) k_flux2(Reg6 regs, Space s, KGeom g, K
   o[at + FR_UN * s.sn] = qun;
 }
 
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX2) k_flux2(Reg6 regs, Space s, KGeom g, KParams P,
+                                                   DtRef dtr, const double* q, Ptr3 sm,
+                                                   Ptr3 sp, Ptr3 f1, Ptr6 f2) {
+  int i, j, k;
+  const int64_t t = gtid();
+#define CAMR_F2(D, E)                                                                   \
+  case combo(D, E):                                                                     \
+    if (region_cell(regs.r[combo(D, E)], t, i, j, k))                                   \
+      flux2_body<D, E>(i, j, k, s, g, P, dtr, q, sm.p[D], sp.p[D], f1.p[E],             \
+                       f2.p[combo(D, E)]);                                              \
+    break;
+  switch (blockIdx.y) {
+    CAMR_F2(0, 1)
+    CAMR_F2(0, 2)
+    CAMR_F2(1, 0)
+    CAMR_F2(1, 2)
+    CAMR_F2(2, 0)
+    CAMR_F2(2, 1)
+    default: break;
+  }
+#undef CAMR_F2
+}
+
 // Artificial viscosity, species normalisation and area weighting of one
 // face flux (Hydro_adjust_fluxes.cpp:13-44; hydro_artif_visc.H:7-64;
 // Hydro_utils_K.H:207-234).  uL/uR: the conserved state of the cells left
 // and right of the face; dv: divu at the face's 4 nodes (corner, +t1, +t2,
 // +t1+t2).
+template <int dir>
 __device__ __forceinline__ void adjust_flux(double* f, const double* uL, const double* uR,
-                                            const double* dv, int dir, int idx, double dx,
+                                            const double* dv, int idx, double dx,
                                             const KGeom& g, const KParams& P, double area) {
   const double div = P.difmag * dmin(0.0, 0.25 * (dv[0] + dv[1] + dv[2] + dv[3]));
   const bool at_bndry = (idx == g.dlo[dir] && g.bclo[dir] == CAMR_BC_NOSLIPWALL) ||
@@ -520,15 +573,16 @@ __device__ __forceinline__ void adjust_flux(double* f, const double* uL, const d
   for (int n = 0; n < NVAR; ++n) f[n] *= area;
 }
 
+template <int F>
 __device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, double qun,
-                                                      int F, int i, int j, int k,
+                                                      int i, int j, int k,
                                                       const Space& s, const KGeom& g,
                                                       const KParams& P, const DFab& uin,
                                                       const double* divu, DFab flx,
                                                       double* qf) {
-  const int eF[3] = {F == 0, F == 1, F == 2};
-  const int t1 = (F == 0) ? 1 : 0;
-  const int t2 = (F == 2) ? 1 : 2;
+  constexpr int e0 = (F == 0), e1 = (F == 1), e2 = (F == 2);
+  constexpr int t1 = (F == 0) ? 1 : 0;
+  constexpr int t2 = (F == 2) ? 1 : 2;
   const int64_t st1 = (t1 == 0) ? 1 : (t1 == 1) ? s.sy : s.sz;
   const int64_t st2 = (t2 == 0) ? 1 : (t2 == 1) ? s.sy : s.sz;
   const int64_t at = s.idx(i, j, k);
@@ -540,13 +594,13 @@ __device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, d
   double uL[NVAR], uR[NVAR];
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) {
-    uL[n] = uin(i - eF[0], j - eF[1], k - eF[2], n);
+    uL[n] = uin(i - e0, j - e1, k - e2, n);
     uR[n] = uin(i, j, k, n);
   }
   const double area = (F == 0) ? g.dx[1] * g.dx[2] : (F == 1) ? g.dx[0] * g.dx[2]
                                                               : g.dx[0] * g.dx[1];
   const int idx = (F == 0) ? i : (F == 1) ? j : k;
-  adjust_flux(f, uL, uR, dv, F, idx, g.dx[F], g, P, area);
+  adjust_flux<F>(f, uL, uR, dv, idx, g.dx[F], g, P, area);
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) flx(i, j, k, n) = f[n];
   qf[at] = qpres;
@@ -556,23 +610,19 @@ __device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, d
 // ---------------------------------------------------------------------------
 // K6: final fluxes on the F-faces of bx (Godunov_3D.cpp:388-452):
 // hydro_transdd halves of the two cells, Riemann, then adjust_fluxes.
-__global__ void __launch_bounds__(kBlock) k_flux3(Region r0, Region r1, Region r2, Space s,
-                                                   KGeom g, KParams P, DtRef dtr,
-                                                   const double* q, const double* srcq,
-                                                   bool has_src, Ptr3 sm, Ptr3 sp, Ptr6 f2,
-                                                   const double* divu, DFab uin, DFab fx,
-                                                   DFab fy, DFab fz, Ptr3 qf) {
-  const int F = blockIdx.y;
-  const Region& r = (F == 0) ? r0 : (F == 1) ? r1 : r2;
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
-  const int t0 = (F == 0) ? 1 : 0;
-  const int t1 = (F == 2) ? 1 : 2;
+template <int F>
+__device__ __forceinline__ void flux3_body(int i, int j, int k, const Space& s, const KGeom& g,
+                                           const KParams& P, const DtRef& dtr,
+                                           const double* q, const double* srcq, bool has_src,
+                                           const double* smF, const double* spF,
+                                           const double* fa, const double* fb,
+                                           const double* divu, const DFab& uin, DFab flx,
+                                           double* qfF) {
+  constexpr int t0 = (F == 0) ? 1 : 0;
+  constexpr int t1 = (F == 2) ? 1 : 2;
   const int64_t stF = (F == 0) ? 1 : (F == 1) ? s.sy : s.sz;
   const int64_t st0 = (t0 == 0) ? 1 : (t0 == 1) ? s.sy : s.sz;
   const int64_t st1 = (t1 == 0) ? 1 : (t1 == 1) ? s.sy : s.sz;
-  const double* fa = f2.p[combo(t0, t1)];
-  const double* fb = f2.p[combo(t1, t0)];
   const int64_t at = s.idx(i, j, k);
   const double dt = dtr.get();
   const double hdt = 0.5 * dt;
@@ -590,7 +640,7 @@ __global__ void __launch_bounds__(kBlock) k_flux3(Region r0, Region r1, Region r
     load_fr(fb, s, cell + st1, b1);
     const TDTerms t = transdd_terms(a0, a1, b0, b1, P.gamma, cdtdx0, cdtdx1);
     if (has_src) load_es(srcq, s, cell, sq);
-    load_es(sm.p[F], s, at, qn);
+    load_es(smF, s, at, qn);
     transdd_side(t, qn, sq, hdt, P, qm);
   }
   {
@@ -601,16 +651,42 @@ __global__ void __launch_bounds__(kBlock) k_flux3(Region r0, Region r1, Region r
     load_fr(fb, s, at + st1, b1);
     const TDTerms t = transdd_terms(a0, a1, b0, b1, P.gamma, cdtdx0, cdtdx1);
     if (has_src) load_es(srcq, s, at, sq);
-    load_es(sp.p[F], s, at, qn);
+    load_es(spF, s, at, qn);
     transdd_side(t, qn, sq, hdt, P, qp);
   }
   const CellAux aL = load_aux(q, s, at - stF, P.gamma);
   const CellAux aR = load_aux(q, s, at, P.gamma);
   const int idx = (F == 0) ? i : (F == 1) ? j : k;
   double f[NVAR], qpres, qun;
-  cmpflx(qm, qp, aL, aR, F, idx, g.bclo[F], g.bchi[F], g.dlo[F], g.dhi[F], P, f, qpres, qun);
-  const DFab flx = (F == 0) ? fx : (F == 1) ? fy : fz;
-  face_adjust_and_store(f, qpres, qun, F, i, j, k, s, g, P, uin, divu, flx, qf.p[F]);
+  cmpflx<F>(qm, qp, aL, aR, idx, g.bclo[F], g.bchi[F], g.dlo[F], g.dhi[F], P, f, qpres, qun);
+  face_adjust_and_store<F>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfF);
+}
+
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX3) k_flux3(Region r0, Region r1, Region r2, Space s,
+                                                   KGeom g, KParams P, DtRef dtr,
+                                                   const double* q, const double* srcq,
+                                                   bool has_src, Ptr3 sm, Ptr3 sp, Ptr6 f2,
+                                                   const double* divu, DFab uin, DFab fx,
+                                                   DFab fy, DFab fz, Ptr3 qf) {
+  int i, j, k;
+  const int64_t t = gtid();
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(r0, t, i, j, k))
+        flux3_body<0>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[0], sp.p[0],
+                      f2.p[combo(1, 2)], f2.p[combo(2, 1)], divu, uin, fx, qf.p[0]);
+      break;
+    case 1:
+      if (region_cell(r1, t, i, j, k))
+        flux3_body<1>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[1], sp.p[1],
+                      f2.p[combo(0, 2)], f2.p[combo(2, 0)], divu, uin, fy, qf.p[1]);
+      break;
+    default:
+      if (region_cell(r2, t, i, j, k))
+        flux3_body<2>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[2], sp.p[2],
+                      f2.p[combo(0, 1)], f2.p[combo(1, 0)], divu, uin, fz, qf.p[2]);
+      break;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -619,16 +695,11 @@ __global__ void __launch_bounds__(kBlock) k_flux3(Region r0, Region r1, Region r
 // not produced.  Stored slots: 0, 2, 3, 4, QREINT, species.
 enum { SL_0 = 0, SL_2 = 1, SL_3 = 2, SL_4 = 3, SL_RE = 4, SL_FS = 5, SL_N = 8 };
 
-__global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Region r2, Space s,
-                                                       KParams P, const double* q,
-                                                       Ptr3 slope) {
-  const int d = blockIdx.y;
-  const Region& r = (d == 0) ? r0 : (d == 1) ? r1 : r2;
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
+template <int d>
+__device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space& s,
+                                               const KParams& P, const double* q, double* o) {
   const int64_t at = s.idx(i, j, k);
   const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
-  double* o = slope.p[d];
   if (P.plm_iorder == 1) {
 #pragma unroll
     for (int n = 0; n < SL_N; ++n) o[at + n * s.sn] = 0.;
@@ -636,9 +707,9 @@ __global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Regi
   }
   const double plm_theta = 2.0;
   auto Q = [&](int off, int slot) { return q[at + off * st + slot * s.sn]; };
-  const int un = SQ_U + d;
-  const int t1 = (d == 0) ? SQ_V : SQ_U;
-  const int t2 = (d == 2) ? SQ_V : SQ_W;
+  constexpr int un = SQ_U + d;
+  constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
+  constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
   const double c = Q(0, SQ_C);
   double dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
   double drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
@@ -666,26 +737,40 @@ __global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Regi
   }
 }
 
+__global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Region r2, Space s,
+                                                       KParams P, const double* q,
+                                                       Ptr3 slope) {
+  int i, j, k;
+  const int64_t t = gtid();
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(r0, t, i, j, k)) mol_slope_body<0>(i, j, k, s, P, q, slope.p[0]);
+      break;
+    case 1:
+      if (region_cell(r1, t, i, j, k)) mol_slope_body<1>(i, j, k, s, P, q, slope.p[1]);
+      break;
+    default:
+      if (region_cell(r2, t, i, j, k)) mol_slope_body<2>(i, j, k, s, P, q, slope.p[2]);
+      break;
+  }
+}
+
 // MOL face pass: edge states of mol_riemann_{x,y,z} (MOL_riemann_K.H:12-488),
 // Riemann flux, then adjust_fluxes.
-__global__ void __launch_bounds__(kBlock) k_mol_flux(Region r0, Region r1, Region r2, Space s,
-                                                      KGeom g, KParams P, const double* q,
-                                                      Ptr3 slope, const double* divu,
-                                                      DFab uin, DFab fx, DFab fy, DFab fz,
-                                                      Ptr3 qf) {
-  const int d = blockIdx.y;
-  const Region& r = (d == 0) ? r0 : (d == 1) ? r1 : r2;
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
+template <int d>
+__device__ __forceinline__ void mol_flux_body(int i, int j, int k, const Space& s,
+                                              const KGeom& g, const KParams& P,
+                                              const double* q, const double* sl,
+                                              const double* divu, const DFab& uin, DFab flx,
+                                              double* qfd) {
   const int64_t at = s.idx(i, j, k);
   const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
   const int64_t atL = at - st;
-  const double* sl = slope.p[d];
   auto Q = [&](int64_t c, int slot) { return q[c + slot * s.sn]; };
   auto S = [&](int64_t c, int slot) { return sl[c + slot * s.sn]; };
-  const int un = SQ_U + d;
-  const int t1 = (d == 0) ? SQ_V : SQ_U;
-  const int t2 = (d == 2) ? SQ_V : SQ_W;
+  constexpr int un = SQ_U + d;
+  constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
+  constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
   double ql[ES_N], qr[ES_N];
   {
     const double cspeed = Q(atL, SQ_C);
@@ -747,9 +832,31 @@ __global__ void __launch_bounds__(kBlock) k_mol_flux(Region r0, Region r1, Regio
   const CellAux aR = load_aux(q, s, at, P.gamma);
   const int idx = (d == 0) ? i : (d == 1) ? j : k;
   double f[NVAR], qpres, qun;
-  cmpflx(ql, qr, aL, aR, d, idx, g.bclo[d], g.bchi[d], g.dlo[d], g.dhi[d], P, f, qpres, qun);
-  const DFab flx = (d == 0) ? fx : (d == 1) ? fy : fz;
-  face_adjust_and_store(f, qpres, qun, d, i, j, k, s, g, P, uin, divu, flx, qf.p[d]);
+  cmpflx<d>(ql, qr, aL, aR, idx, g.bclo[d], g.bchi[d], g.dlo[d], g.dhi[d], P, f, qpres, qun);
+  face_adjust_and_store<d>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfd);
+}
+
+__global__ void __launch_bounds__(kBlock) k_mol_flux(Region r0, Region r1, Region r2, Space s,
+                                                      KGeom g, KParams P, const double* q,
+                                                      Ptr3 slope, const double* divu,
+                                                      DFab uin, DFab fx, DFab fy, DFab fz,
+                                                      Ptr3 qf) {
+  int i, j, k;
+  const int64_t t = gtid();
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(r0, t, i, j, k))
+        mol_flux_body<0>(i, j, k, s, g, P, q, slope.p[0], divu, uin, fx, qf.p[0]);
+      break;
+    case 1:
+      if (region_cell(r1, t, i, j, k))
+        mol_flux_body<1>(i, j, k, s, g, P, q, slope.p[1], divu, uin, fy, qf.p[1]);
+      break;
+    default:
+      if (region_cell(r2, t, i, j, k))
+        mol_flux_body<2>(i, j, k, s, g, P, q, slope.p[2], divu, uin, fz, qf.p[2]);
+      break;
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -42,7 +42,7 @@ struct Work {
 };
 
 // Combination index of the second-pass "D|E" fluxes.
-__host__ __device__ __forceinline__ int combo(int D, int E) {
+__host__ __device__ constexpr int combo(int D, int E) {
   return D * 2 + ((E > D) ? E - 1 : E);
 }
 

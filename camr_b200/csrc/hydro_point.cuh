@@ -120,13 +120,14 @@ __device__ __forceinline__ ROut riemannus(double rl_in, double ul, double vl, do
 // place at a physical-boundary face exactly as the reference modifies its
 // state arrays (:239-282).  f[UTEMP] is left at 0 (flux arrays start from
 // setVal(0), CAMR_construct_hydro_source.cpp:88).
+template <int dir>
 __device__ __forceinline__ void cmpflx(double* ql, double* qr, const CellAux& aL,
-                                       const CellAux& aR, int dir, int idx, int bclo,
-                                       int bchi, int domlo, int domhi, const KParams& P,
-                                       double* f, double& q_pres, double& q_un) {
-  const int iu = ES_U + dir;
-  const int iv = (dir == 0) ? ES_V : ES_U;
-  const int iv2 = (dir == 2) ? ES_V : ES_W;
+                                       const CellAux& aR, int idx, int bclo, int bchi,
+                                       int domlo, int domhi, const KParams& P, double* f,
+                                       double& q_pres, double& q_un) {
+  constexpr int iu = ES_U + dir;
+  constexpr int iv = (dir == 0) ? ES_V : ES_U;
+  constexpr int iv2 = (dir == 2) ? ES_V : ES_W;
   const double cav = 0.5 * (aR.c + aL.c);
   const double smallc = dmax(aR.csml, aL.csml);
   double gamcl = aL.gamc;
@@ -174,9 +175,9 @@ __device__ __forceinline__ void cmpflx(double* ql, double* qr, const CellAux& aL
   const ROut o = riemannus(ql[ES_RHO], ul, vl, v2l, ql[ES_P], ql[ES_REINT], qr[ES_RHO], ur,
                            vr, v2r, qr[ES_P], qr[ES_REINT], cav, gamcl, gamcr, P.small, smallc,
                            P.small_dens, P.small_pres, P.smallu);
-  const int fu = UMX + dir;
-  const int fv = (dir == 0) ? UMY : UMX;
-  const int fv2 = (dir == 2) ? UMY : UMZ;
+  constexpr int fu = UMX + dir;
+  constexpr int fv = (dir == 0) ? UMY : UMX;
+  constexpr int fv2 = (dir == 2) ? UMY : UMZ;
   f[URHO] = o.f_rho;
   f[fu] = o.f_un;
   f[fv] = o.f_ut1;
@@ -281,13 +282,15 @@ __device__ __forceinline__ double flatten_dir(const double* p, const double* un)
   double tst = (qmun - qpun >= 0.0) ? 1.0 : 0.0;
   double tmp = dmin(qp, qm);
   const double chi = (fabs(dp) / tmp) > shktst ? tst : 0.0;
-  // offsets: qpshft at 1-ishft, qmshft at -(1+ishft), ... (flatten.H:78-83)
-  const double qpshft = p[3 + 1 - ishft];
-  const double qmshft = p[3 - (1 + ishft)];
-  const double qpunshft = un[3 + 1 - ishft];
-  const double qmunshft = un[3 - (1 + ishft)];
-  const double qppshft = p[3 + 2 - ishft];
-  const double qmmshft = p[3 - (2 + ishft)];
+  // offsets 1-ishft, -(1+ishft), 2-ishft, -(2+ishft) (flatten.H:78-83),
+  // with ishft = +-1 spelled out so the stencil stays in registers
+  const bool up = ishft == 1;
+  const double qpshft = up ? p[3] : p[5];
+  const double qmshft = up ? p[1] : p[3];
+  const double qpunshft = up ? un[3] : un[5];
+  const double qmunshft = up ? un[1] : un[3];
+  const double qppshft = up ? p[4] : p[6];
+  const double qmmshft = up ? p[0] : p[2];
   dp = qpshft - qmshft;
   denom = dmax(small_pres, fabs(qppshft - qmmshft));
   zeta = fabs(dp) / denom;

@@ -7,7 +7,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libcamr_b200.so")
+# CAMR_B200_LIB selects another build of the library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("CAMR_B200_LIB") or os.path.join(HERE, "_lib", "libcamr_b200.so")
 
 NVAR = 10
 STATUS = {0: "CAMR_OK", 1: "CAMR_ERR_INVALID", 2: "CAMR_ERR_UNSUPPORTED", 3: "CAMR_ERR_CUDA",
