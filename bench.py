@@ -294,6 +294,11 @@ def run_camr(args, world, rank, local, pg):
                "sample": f"one full {n[0]}^3 step of the workload ({secs:.1f} s), "
                          "reference hydro kernels, tiles 1024x16x16, all host threads"}
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        L.close()
+        batched = batched_comparison(args)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -308,9 +313,152 @@ def run_camr(args, world, rank, local, pg):
             "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "stages_ms": acc, "device_error": list(err),
+            "batched_amr_patches": batched,
         }
         print(json.dumps(line))
     L.close()
+
+
+def amr_box_inputs(boxes, fine_n, dev):
+    """Per-box Sborder fabs (box grown by 4) of a smooth flow with overpressure
+    blobs, evaluated at the fine cells' centres on the device (test data)."""
+    import torch
+    gamma = 1.4
+    brng = np.random.default_rng(1)
+    blobs = []
+    for _ in range(16):
+        c = brng.uniform(0.0, 1.0, size=3)
+        r = brng.uniform(0.03, 0.08)
+        blobs.append((c, r))
+    out = []
+    two_pi = 2 * np.pi
+    for lo, hi in boxes:
+        ax = [torch.arange(lo[d] - 4, hi[d] + 5, device=dev, dtype=torch.float64) for d in range(3)]
+        x = ((ax[0] + 0.5) / fine_n)[None, None, :]
+        y = ((ax[1] + 0.5) / fine_n)[None, :, None]
+        z = ((ax[2] + 0.5) / fine_n)[:, None, None]
+        rho = 1.0 + 0.1 * torch.sin(two_pi * x) * torch.sin(two_pi * y) * torch.sin(two_pi * z)
+        p = torch.ones_like(rho)
+        for c, r in blobs:
+            d2 = 0.0
+            for arr, cc in zip((x, y, z), c):
+                dd = torch.abs(arr - cc)
+                dd = torch.minimum(dd, 1.0 - dd)
+                d2 = d2 + dd * dd
+            p = torch.where(d2 < r * r, torch.full_like(p, 10.0), p)
+        u = 0.2 * torch.sin(two_pi * y) * torch.ones_like(rho)
+        v = 0.2 * torch.sin(two_pi * z) * torch.ones_like(rho)
+        w = 0.2 * torch.sin(two_pi * x) * torch.ones_like(rho)
+        U = torch.empty((10,) + rho.shape, dtype=torch.float64, device=dev)
+        U[0] = rho
+        U[1], U[2], U[3] = rho * u, rho * v, rho * w
+        U[5] = p / (gamma - 1.0)
+        U[4] = U[5] + 0.5 * rho * (u * u + v * v + w * w)
+        U[6] = (gamma - 1.0) * (U[5] / rho) * 26.93 / 8.31446261815324e7
+        U[7], U[8], U[9] = rho, 0.0 * rho, 0.0 * rho
+        nb = [hi[d] - lo[d] + 1 for d in range(3)]
+        dsdt = torch.zeros((10, nb[2], nb[1], nb[0]), dtype=torch.float64, device=dev)
+        flx = []
+        for d in range(3):
+            sh = list(nb)
+            sh[d] += 1
+            flx.append(torch.zeros((10, sh[2], sh[1], sh[0]), dtype=torch.float64, device=dev))
+        out.append((list(lo), list(hi), U.contiguous(), [lo[d] - 4 for d in range(3)], dsdt, flx))
+    return out
+
+
+def batched_comparison(args, steps=5, warmup=2):
+    """Hydro of one level step over the uneven fine-level boxes: batched
+    work-list launches vs per-box launches (same plan, same boxes)."""
+    import torch
+
+    from camr_b200 import hydro, native, problems
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    fine_n = 512
+    boxes = problems.amr_box_list(nbox=args.nbox, fine_n=fine_n)
+    cells = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in boxes)
+    items = amr_box_inputs(boxes, fine_n, dev)
+    geom = hydro.make_geom((fine_n,) * 3)
+    prm = native.default_params(do_mol=0, ppm_type=1, cfl=CFL)
+    dt = 0.25 / fine_n / 4.0
+    b = hydro.Batch(items, geom, prm)
+    torch.cuda.synchronize()
+    b.autotune(dt)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    res = {}
+    for name, mode in (("per_box", hydro.Batch.PER_BOX), ("batched", hydro.Batch.PERSISTENT)):
+        for _ in range(warmup):
+            b.run(dt, mode)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            b.run(dt, mode)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[name] = {"ms": ms, "zone_updates_per_s": cells / (ms * 1e-3)}
+    out = {"boxes": len(boxes), "cells": cells, "per_box": res["per_box"],
+           "batched": res["batched"],
+           "speedup_batched_vs_per_box": res["per_box"]["ms"] / res["batched"]["ms"],
+           "tuning_cells_per_block_and_grid": b.tuning()}
+    b.close()
+    del items
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_batched(args, rank):
+    """Batched vs per-box launches over the uneven fine-level boxes of the
+    two-level configuration (hydro of one level step, CTU-PPM)."""
+    import torch
+
+    from camr_b200 import build, hydro, native, problems
+    if not os.path.exists(native.LIB_PATH):
+        build.build()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    fine_n = 512
+    boxes = problems.amr_box_list(nbox=args.nbox, fine_n=fine_n)
+    cells = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in boxes)
+    items = amr_box_inputs(boxes, fine_n, dev)
+    geom = hydro.make_geom((fine_n,) * 3)
+    prm = native.default_params(do_mol=0, ppm_type=1, cfl=CFL)
+    dt = 0.25 / fine_n / 4.0
+    b = hydro.Batch(items, geom, prm)
+    torch.cuda.synchronize()
+    b.autotune(dt)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    res = {}
+    for name, mode in (("per_box", hydro.Batch.PER_BOX), ("batched", hydro.Batch.PERSISTENT)):
+        for _ in range(args.warmup):
+            b.run(dt, mode)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            b.run(dt, mode)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[name] = {"ms": ms, "zone_updates_per_s": cells / (ms * 1e-3)}
+    tuning = b.tuning()
+    b.close()
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s (FP64, 1xB200), batched uneven AMR patches",
+            "value": res["batched"]["zone_updates_per_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["batched"]["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (uneven fine boxes around seeded blobs, box seed 7)",
+            "config": {"workload": "c2 fine level: hydro of one level step over uneven boxes",
+                       "boxes": len(boxes), "cells": cells, "box_sizes": [16, 24, 32, 48, 64],
+                       "method": "CTU-PPM"},
+            "per_box": res["per_box"], "batched": res["batched"],
+            "speedup_batched_vs_per_box": res["per_box"]["ms"] / res["batched"]["ms"],
+            "tuning": tuning,
+        }
+        print(json.dumps(line))
 
 
 def main():
@@ -321,7 +469,14 @@ def main():
     ap.add_argument("--impl", choices=["camr", "reference"], default="camr")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", choices=["c1", "c2-batched"], default="c1")
+    ap.add_argument("--nbox", type=int, default=350)
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-vs-per-box comparison in the default line")
     args = ap.parse_args()
+    if args.workload == "c2-batched":
+        run_batched(args, int(os.environ.get("RANK", "0")))
+        return
     if args.impl == "reference":
         # CPU-only arm: rank 0 alone runs it; other ranks exit without work.
         world = int(os.environ.get("WORLD_SIZE", "1"))

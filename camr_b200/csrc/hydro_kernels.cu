@@ -51,11 +51,9 @@ __device__ __forceinline__ CellAux load_aux(const double* q, const Space& s, int
 // ---------------------------------------------------------------------------
 // K1: conservative -> primitive (Source/Hydro/Hydro_ctoprim.H:11-101) and,
 // with sources, primitive sources (:106-157).
-__global__ void __launch_bounds__(kBlock) k_ctoprim(Region r, Space s, DFab u, DFab src,
-                                                     bool has_src, KParams P, double* q,
-                                                     double* srcq, DevError* err) {
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
+__device__ __forceinline__ void ctoprim_body(int i, int j, int k, const Space& s, const DFab& u,
+                                             const DFab& src, bool has_src, const KParams& P,
+                                             double* q, double* srcq, DevError* err) {
   const int64_t at = s.idx(i, j, k);
   const double rho = u(i, j, k, URHO);
   if (!(rho > 0.)) {
@@ -113,17 +111,23 @@ __global__ void __launch_bounds__(kBlock) k_ctoprim(Region r, Space s, DFab u, D
   }
 }
 
+__global__ void __launch_bounds__(kBlock) k_ctoprim(Region r, Space s, DFab u, DFab src,
+                                                     bool has_src, KParams P, double* q,
+                                                     double* srcq, DevError* err) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  ctoprim_body(i, j, k, s, u, src, has_src, P, q, srcq, err);
+}
+
 // ---------------------------------------------------------------------------
 // K2: shock flattening of a cell (min over the three directions, as the
 // reference's trace loops do: PLM Godunov_3D.cpp:109-115, PPM PPM.cpp:120-126)
 // and the nodal divergence at the cell's low corner when it is a node of bx
 // (Source/Hydro/Hydro_utils_K.H:12-169).
-__global__ void __launch_bounds__(kBlock) k_flatten_divu(Region r, Space s, KGeom g,
-                                                          KParams P, bool do_flat,
-                                                          const double* q, double* flat,
-                                                          double* divu) {
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
+__device__ __forceinline__ void flatten_divu_body(int i, int j, int k, const Space& s,
+                                                  const KGeom& g, const KParams& P,
+                                                  bool do_flat, const double* q, double* flat,
+                                                  double* divu) {
   const int64_t at = s.idx(i, j, k);
   if (do_flat) {
     double fl = 1.0;
@@ -212,6 +216,15 @@ __global__ void __launch_bounds__(kBlock) k_flatten_divu(Region r, Space s, KGeo
     wz = (Q(i - 1, j - 1, k, QWx) - Q(i - 1, j - 1, k - 1, QWx)) / dz;
   }
   divu[at] = ux + vy + wz;
+}
+
+__global__ void __launch_bounds__(kBlock) k_flatten_divu(Region r, Space s, KGeom g,
+                                                          KParams P, bool do_flat,
+                                                          const double* q, double* flat,
+                                                          double* divu) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  flatten_divu_body(i, j, k, s, g, P, do_flat, q, flat, divu);
 }
 
 // ---------------------------------------------------------------------------
@@ -861,10 +874,9 @@ __global__ void __launch_bounds__(kBlock) k_mol_flux(Region r0, Region r1, Regio
 
 // ---------------------------------------------------------------------------
 // K7: hydro_consup (Hydro_utils_K.H:239-257) with pdivu (:175-202).
-__global__ void __launch_bounds__(kBlock) k_consup(Region r, Space s, KGeom g, DFab fx,
-                                                    DFab fy, DFab fz, Ptr3 qf, DFab dsdt) {
-  int i, j, k;
-  if (!region_cell(r, gtid(), i, j, k)) return;
+__device__ __forceinline__ void consup_body(int i, int j, int k, const Space& s, const KGeom& g,
+                                            const DFab& fx, const DFab& fy, const DFab& fz,
+                                            const Ptr3& qf, const DFab& dsdt) {
   const int64_t at = s.idx(i, j, k);
   const double a0 = g.dx[1] * g.dx[2], a1 = g.dx[0] * g.dx[2], a2 = g.dx[0] * g.dx[1];
   const double vol = g.dx[0] * g.dx[1] * g.dx[2];
@@ -888,6 +900,117 @@ __global__ void __launch_bounds__(kBlock) k_consup(Region r, Space s, KGeom g, D
   dsdt(i, j, k, UEINT) -= pdivu;
 }
 
+__global__ void __launch_bounds__(kBlock) k_consup(Region r, Space s, KGeom g, DFab fx,
+                                                    DFab fy, DFab fz, Ptr3 qf, DFab dsdt) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  consup_body(i, j, k, s, g, fx, fy, fz, qf, dsdt);
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched (work-list) versions of the stages: one launch covers every box of
+// a level.  Each work item is (box, sub-direction, region, first block); a
+// block finds its item by binary search over the items' first-block prefix
+// and runs the same per-cell body as the per-box kernels.  The grid may be
+// smaller than the block count (persistent, grid-stride over blocks).
+
+__device__ __forceinline__ int find_item(const BatchItem* items, int n, int64_t b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].block0 <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int STAGE>
+__device__ __forceinline__ void batched_cell(const BoxCtx& c, int sub, int i, int j, int k,
+                                             const KParams& P, const DtRef& dt, DevError* err) {
+  const Work& w = c.w;
+  if constexpr (STAGE == BS_CTOPRIM) {
+    ctoprim_body(i, j, k, w.s, c.uin, c.src, c.has_src, P, w.q, w.srcq, err);
+  } else if constexpr (STAGE == BS_FLATDIVU) {
+    flatten_divu_body(i, j, k, w.s, c.g, P, !c.mol, w.q, w.flat, w.divu);
+  } else if constexpr (STAGE == BS_TRACE) {
+    switch (sub) {
+      case 0: trace_body<0>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[0], w.sp[0]); break;
+      case 1: trace_body<1>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[1], w.sp[1]); break;
+      default: trace_body<2>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[2], w.sp[2]); break;
+    }
+  } else if constexpr (STAGE == BS_FLUX1) {
+    switch (sub) {
+      case 0: flux1_body<0>(i, j, k, w.s, c.g, P, w.q, w.sm[0], w.sp[0], w.f1[0]); break;
+      case 1: flux1_body<1>(i, j, k, w.s, c.g, P, w.q, w.sm[1], w.sp[1], w.f1[1]); break;
+      default: flux1_body<2>(i, j, k, w.s, c.g, P, w.q, w.sm[2], w.sp[2], w.f1[2]); break;
+    }
+  } else if constexpr (STAGE == BS_FLUX2) {
+#define CAMR_BF2(D, E)                                                                  \
+  case combo(D, E):                                                                     \
+    flux2_body<D, E>(i, j, k, w.s, c.g, P, dt, w.q, w.sm[D], w.sp[D], w.f1[E],          \
+                     w.f2[combo(D, E)]);                                                \
+    break;
+    switch (sub) {
+      CAMR_BF2(0, 1)
+      CAMR_BF2(0, 2)
+      CAMR_BF2(1, 0)
+      CAMR_BF2(1, 2)
+      CAMR_BF2(2, 0)
+      CAMR_BF2(2, 1)
+      default: break;
+    }
+#undef CAMR_BF2
+  } else if constexpr (STAGE == BS_FLUX3) {
+    switch (sub) {
+      case 0:
+        flux3_body<0>(i, j, k, w.s, c.g, P, dt, w.q, w.srcq, c.has_src, w.sm[0], w.sp[0],
+                      w.f2[combo(1, 2)], w.f2[combo(2, 1)], w.divu, c.uin, c.flx[0], w.qf[0]);
+        break;
+      case 1:
+        flux3_body<1>(i, j, k, w.s, c.g, P, dt, w.q, w.srcq, c.has_src, w.sm[1], w.sp[1],
+                      w.f2[combo(0, 2)], w.f2[combo(2, 0)], w.divu, c.uin, c.flx[1], w.qf[1]);
+        break;
+      default:
+        flux3_body<2>(i, j, k, w.s, c.g, P, dt, w.q, w.srcq, c.has_src, w.sm[2], w.sp[2],
+                      w.f2[combo(0, 1)], w.f2[combo(1, 0)], w.divu, c.uin, c.flx[2], w.qf[2]);
+        break;
+    }
+  } else if constexpr (STAGE == BS_MOLSLOPE) {
+    switch (sub) {
+      case 0: mol_slope_body<0>(i, j, k, w.s, P, w.q, w.slope[0]); break;
+      case 1: mol_slope_body<1>(i, j, k, w.s, P, w.q, w.slope[1]); break;
+      default: mol_slope_body<2>(i, j, k, w.s, P, w.q, w.slope[2]); break;
+    }
+  } else if constexpr (STAGE == BS_MOLFLUX) {
+    switch (sub) {
+      case 0: mol_flux_body<0>(i, j, k, w.s, c.g, P, w.q, w.slope[0], w.divu, c.uin, c.flx[0], w.qf[0]); break;
+      case 1: mol_flux_body<1>(i, j, k, w.s, c.g, P, w.q, w.slope[1], w.divu, c.uin, c.flx[1], w.qf[1]); break;
+      default: mol_flux_body<2>(i, j, k, w.s, c.g, P, w.q, w.slope[2], w.divu, c.uin, c.flx[2], w.qf[2]); break;
+    }
+  } else {
+    Ptr3 qf{{w.qf[0], w.qf[1], w.qf[2]}};
+    consup_body(i, j, k, w.s, c.g, c.flx[0], c.flx[1], c.flx[2], qf, c.dsdt);
+  }
+}
+
+template <int STAGE, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
+    kb_stage(const BoxCtx* __restrict__ boxes, const BatchItem* __restrict__ items, int nitems,
+             int64_t nblocks, int chunk, KParams P, DtRef dt, DevError* err) {
+  for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const int it = find_item(items, nitems, b);
+    const BatchItem item = items[it];
+    const BoxCtx& c = boxes[item.box];
+    const int64_t base = (b - item.block0) * int64_t(kBlock) * chunk;
+    for (int q = 0; q < chunk; ++q) {
+      int i, j, k;
+      if (region_cell(item.r, base + int64_t(q) * kBlock + threadIdx.x, i, j, k)) {
+        batched_cell<STAGE>(c, item.sub, i, j, k, P, dt, err);
+      }
+    }
+  }
+}
 }  // namespace
 
 size_t work_doubles(const Space& s, bool mol, bool has_src) {
@@ -1043,6 +1166,132 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
     count_launch(2);
   }
   return cudaGetLastError();
+}
+
+
+int batched_min_blocks(int stage) {
+  switch (stage) {
+    case BS_TRACE: return CAMR_MINB_TRACE;
+    case BS_FLUX1: return CAMR_MINB_FLUX1;
+    case BS_FLUX2: return CAMR_MINB_FLUX2;
+    case BS_FLUX3: return CAMR_MINB_FLUX3;
+    default: return 1;
+  }
+}
+
+const void* batched_kernel(int stage) {
+  switch (stage) {
+    case BS_CTOPRIM: return reinterpret_cast<const void*>(&kb_stage<BS_CTOPRIM, 1>);
+    case BS_FLATDIVU: return reinterpret_cast<const void*>(&kb_stage<BS_FLATDIVU, 1>);
+    case BS_TRACE: return reinterpret_cast<const void*>(&kb_stage<BS_TRACE, CAMR_MINB_TRACE>);
+    case BS_FLUX1: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX1, CAMR_MINB_FLUX1>);
+    case BS_FLUX2: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX2, CAMR_MINB_FLUX2>);
+    case BS_FLUX3: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX3, CAMR_MINB_FLUX3>);
+    case BS_MOLSLOPE: return reinterpret_cast<const void*>(&kb_stage<BS_MOLSLOPE, 1>);
+    case BS_MOLFLUX: return reinterpret_cast<const void*>(&kb_stage<BS_MOLFLUX, 1>);
+    default: return reinterpret_cast<const void*>(&kb_stage<BS_CONSUP, 1>);
+  }
+}
+
+cudaError_t launch_batched_stage(int stage, const BoxCtx* boxes, const BatchItem* items,
+                                 int nitems, int64_t nblocks, int chunk, unsigned grid,
+                                 const KParams& P, DtRef dt, DevError* err, cudaStream_t st) {
+  if (nblocks <= 0) return cudaSuccess;
+  if (grid == 0 || grid > nblocks) grid = unsigned(nblocks);
+  switch (stage) {
+#define CAMR_LB(S, M)                                                                     \
+  case S:                                                                                 \
+    kb_stage<S, M><<<grid, kBlock, 0, st>>>(boxes, items, nitems, nblocks, chunk, P, dt, err); \
+    break;
+    CAMR_LB(BS_CTOPRIM, 1)
+    CAMR_LB(BS_FLATDIVU, 1)
+    CAMR_LB(BS_TRACE, CAMR_MINB_TRACE)
+    CAMR_LB(BS_FLUX1, CAMR_MINB_FLUX1)
+    CAMR_LB(BS_FLUX2, CAMR_MINB_FLUX2)
+    CAMR_LB(BS_FLUX3, CAMR_MINB_FLUX3)
+    CAMR_LB(BS_MOLSLOPE, 1)
+    CAMR_LB(BS_MOLFLUX, 1)
+    CAMR_LB(BS_CONSUP, 1)
+#undef CAMR_LB
+    default: return cudaErrorInvalidValue;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+// Regions of one box for each batched stage (the same ones the per-box
+// launcher uses).  Returns the number of sub-regions written to out.
+int stage_regions(int stage, const KGeom& g, Region* out) {
+  int lo[3], hi[3];
+  auto set = [&](int a_lo0, int a_lo1, int a_lo2, int a_hi0, int a_hi1, int a_hi2) {
+    lo[0] = a_lo0; lo[1] = a_lo1; lo[2] = a_lo2;
+    hi[0] = a_hi0; hi[1] = a_hi1; hi[2] = a_hi2;
+  };
+  switch (stage) {
+    case BS_CTOPRIM:
+      set(g.lo[0] - NGROW, g.lo[1] - NGROW, g.lo[2] - NGROW, g.hi[0] + NGROW, g.hi[1] + NGROW,
+          g.hi[2] + NGROW);
+      out[0] = make_region(lo, hi);
+      return 1;
+    case BS_FLATDIVU:
+      set(g.lo[0] - 1, g.lo[1] - 1, g.lo[2] - 1, g.hi[0] + 1, g.hi[1] + 1, g.hi[2] + 1);
+      out[0] = make_region(lo, hi);
+      return 1;
+    case BS_TRACE:
+      set(g.lo[0] - 1, g.lo[1] - 1, g.lo[2] - 1, g.hi[0] + 1, g.hi[1] + 1, g.hi[2] + 1);
+      for (int d = 0; d < 3; ++d) out[d] = make_region(lo, hi);
+      return 3;
+    case BS_FLUX1:
+      for (int E = 0; E < 3; ++E) {
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = (d == E) ? g.lo[d] : g.lo[d] - 1;
+          hi[d] = g.hi[d] + 1;
+        }
+        out[E] = make_region(lo, hi);
+      }
+      return 3;
+    case BS_FLUX2:
+      for (int D = 0; D < 3; ++D)
+        for (int E = 0; E < 3; ++E) {
+          if (E == D) continue;
+          const int F = 3 - D - E;
+          for (int d = 0; d < 3; ++d) {
+            lo[d] = g.lo[d];
+            hi[d] = g.hi[d];
+          }
+          hi[D] += 1;
+          lo[F] -= 1;
+          hi[F] += 1;
+          out[combo(D, E)] = make_region(lo, hi);
+        }
+      return 6;
+    case BS_FLUX3:
+    case BS_MOLFLUX:
+      for (int F = 0; F < 3; ++F) {
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = g.lo[d];
+          hi[d] = g.hi[d];
+        }
+        hi[F] += 1;
+        out[F] = make_region(lo, hi);
+      }
+      return 3;
+    case BS_MOLSLOPE:
+      for (int dd = 0; dd < 3; ++dd) {
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = g.lo[d];
+          hi[d] = g.hi[d];
+        }
+        lo[dd] -= 1;
+        hi[dd] += 1;
+        out[dd] = make_region(lo, hi);
+      }
+      return 3;
+    default:
+      set(g.lo[0], g.lo[1], g.lo[2], g.hi[0], g.hi[1], g.hi[2]);
+      out[0] = make_region(lo, hi);
+      return 1;
+  }
 }
 
 cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t st) {

@@ -78,6 +78,38 @@ struct HydroLaunch {
   StageTimer* timer = nullptr;
 };
 
+// ---- batched (work-list) launches over many boxes of one level ----
+enum { BS_CTOPRIM = 0, BS_FLATDIVU, BS_TRACE, BS_FLUX1, BS_FLUX2, BS_FLUX3, BS_MOLSLOPE,
+       BS_MOLFLUX, BS_CONSUP, BS_COUNT };
+
+// Everything one box of a batch needs on the device.
+struct BoxCtx {
+  KGeom g;
+  Work w;
+  DFab uin, src;
+  DFab flx[3];
+  DFab dsdt;
+  bool has_src;
+  bool mol;
+};
+
+// One work item of a batched stage: `region` of box `box` in sub-direction
+// `sub`, starting at global block `block0`.
+struct BatchItem {
+  int64_t block0;
+  Region r;
+  int box;
+  int sub;
+};
+
+int stage_regions(int stage, const KGeom& g, Region* out);
+cudaError_t launch_batched_stage(int stage, const BoxCtx* boxes, const BatchItem* items,
+                                 int nitems, int64_t nblocks, int chunk, unsigned grid,
+                                 const KParams& P, DtRef dt, DevError* err, cudaStream_t st);
+const void* batched_kernel(int stage);
+int batched_min_blocks(int stage);
+constexpr int kBatchBlock = 128;
+
 // Issue the whole per-box hydro on `stream` (7 or 5 kernel launches).
 cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t stream);
 

@@ -171,3 +171,59 @@ class Level:
 
     def sync(self):
         _torch().cuda.synchronize()
+
+
+class Batch:
+    """A batched hydro plan over the boxes of one level (camr_batch_*).
+
+    boxes: list of (lo, hi, uin, uin_lo, dsdt, flx) with CUDA float64
+    tensors as for hydro_umdrv; the tensors must stay alive with the plan.
+    """
+
+    PERSISTENT = 0
+    PER_BOX = 1
+
+    def __init__(self, boxes, geom, params, stream=None):
+        self._keep = boxes
+        n = len(boxes)
+        tasks = (native.BoxTask * n)()
+        for t, (lo, hi, uin, uin_lo, dsdt, flx) in zip(tasks, boxes):
+            for d in range(3):
+                t.lo[d] = lo[d]
+                t.hi[d] = hi[d]
+            t.uin = fab_of(uin, uin_lo)
+            t.dsdt = fab_of(dsdt, lo)
+            for d in range(3):
+                t.flx[d] = fab_of(flx[d], lo)
+        self._stream = _stream_ptr(stream)
+        h = C.c_void_p()
+        check(lib().camr_batch_create(n, tasks, C.byref(geom), C.byref(params),
+                                      C.c_void_p(self._stream), C.byref(h)), "camr_batch_create")
+        self._h = h
+
+    def run(self, dt, mode=PERSISTENT):
+        check(lib().camr_batch_run(self._h, float(dt), None, int(mode), C.c_void_p(self._stream)),
+              "camr_batch_run")
+
+    def autotune(self, dt):
+        check(lib().camr_batch_autotune(self._h, float(dt), C.c_void_p(self._stream)),
+              "camr_batch_autotune")
+
+    def tuning(self):
+        ch = (C.c_int * 9)()
+        gr = (C.c_uint * 9)()
+        check(lib().camr_batch_tuning(self._h, ch, gr, 9), "camr_batch_tuning")
+        names = ["ctoprim", "flatten_divu", "trace", "flux1", "flux2", "flux3", "mol_slope",
+                 "mol_flux", "consup"]
+        return {n: (int(c) * 128, int(g)) for n, c, g in zip(names, ch, gr)}
+
+    def close(self):
+        if self._h:
+            lib().camr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

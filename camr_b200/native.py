@@ -47,6 +47,11 @@ class Geom(C.Structure):
                 ("dx", C.c_double * 3), ("prob_lo", C.c_double * 3)]
 
 
+class BoxTask(C.Structure):
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("uin", Fab), ("src", Fab),
+                ("dsdt", Fab), ("flx", Fab * 3)]
+
+
 class LevelDesc(C.Structure):
     _fields_ = [("geom", Geom), ("max_grid_size", C.c_int * 3), ("use_graph", C.c_int)]
 
@@ -91,6 +96,15 @@ SIGNATURES = {
                                            C.POINTER(Fab), C.POINTER(HydroParams), C.c_double,
                                            C.c_void_p]),
     "camr_noalloc_last_error": (C.c_char_p, []),
+    "camr_batch_create": (C.c_int, [C.c_int, C.POINTER(BoxTask), C.POINTER(Geom),
+                                    C.POINTER(HydroParams), C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_batch_destroy": (C.c_int, [C.c_void_p]),
+    "camr_batch_run": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
+    "camr_batch_autotune": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
+    "camr_batch_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint),
+                                    C.c_int]),
+    "camr_hydro_umdrv_batched": (C.c_int, [C.c_int, C.POINTER(BoxTask), C.POINTER(Geom),
+                                           C.POINTER(HydroParams), C.c_double, C.c_void_p]),
 }
 
 

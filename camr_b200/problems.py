@@ -128,3 +128,41 @@ def random_smooth(n, seed=0, amp=0.2, vel=0.3, gamma=1.4):
     s[UFS + 1] = rho * y1
     s[UFS + 2] = rho * y2
     return s
+
+
+def amr_box_list(nbox=350, fine_n=512, sizes=(16, 24, 32, 48, 64), seed=7, nblobs=16,
+                 blob_seed=1, align=8, max_tries=200000):
+    """Synthetic fine-level box list of the two-level configuration.
+
+    Boxes with per-dimension sizes drawn uniformly from `sizes` are placed
+    without overlap on the fine index space (fine_n^3, refinement ratio 2 of
+    the base level), each centred near one of the overpressure blobs of the
+    base data (where the flow has its gradients), at `align`-aligned
+    corners.  Returns a list of (lo, hi) integer triples.  The reference
+    builds its boxes with AMReX's clusterer, which is not available here;
+    this list stands in for it with the same box-size statistics.
+    """
+    rng = np.random.default_rng(seed)
+    brng = np.random.default_rng(blob_seed)
+    centres = []
+    for _ in range(nblobs):
+        c = brng.uniform(0.0, 1.0, size=3)
+        brng.uniform(0.03, 0.08)
+        centres.append(c * fine_n)
+    occ = np.zeros((fine_n // align,) * 3, dtype=bool)
+    boxes = []
+    tries = 0
+    while len(boxes) < nbox and tries < max_tries:
+        tries += 1
+        sz = rng.choice(sizes, size=3)
+        c = centres[rng.integers(len(centres))] + rng.normal(0.0, fine_n * 0.08, size=3)
+        lo = np.floor((c - sz / 2) / align).astype(int) * align
+        lo = np.clip(lo, 0, fine_n - sz)
+        lo = (lo // align) * align
+        a = lo // align
+        b = (lo + sz + align - 1) // align
+        if occ[a[0]:b[0], a[1]:b[1], a[2]:b[2]].any():
+            continue
+        occ[a[0]:b[0], a[1]:b[1], a[2]:b[2]] = True
+        boxes.append((tuple(int(v) for v in lo), tuple(int(v) for v in lo + sz - 1)))
+    return boxes

@@ -140,6 +140,53 @@ camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3],
                              void* stream);
 
 /* ---------------------------------------------------------------------
+ * Batched per-box hydro over the boxes of one level (uneven sizes allowed):
+ * the work-list form of the reference's MFIter box loop
+ * (Source/Hydro/CAMR_construct_hydro_source.cpp:71-254).  Each task is one
+ * box with its own fabs, exactly as for camr_hydro_umdrv; results are
+ * identical to calling camr_hydro_umdrv box by box.
+ */
+typedef struct {
+  int lo[3];
+  int hi[3];
+  camr_fab uin;     /* covers grow(box,4), ghost cells filled and cleaned */
+  camr_fab src;     /* ptr NULL = zero sources */
+  camr_fab dsdt;    /* on the box, accumulated */
+  camr_fab flx[3];  /* on the box's faces, overwritten */
+} camr_box_task;
+
+typedef struct camr_batch camr_batch;
+
+enum {
+  CAMR_BATCH_PERSISTENT = 0,  /* one launch per stage for all boxes (work list) */
+  CAMR_BATCH_PER_BOX = 1      /* the plain per-box launch sequence, box by box */
+};
+
+/* Build a plan: per-box workspaces (one device allocation) and the work-item
+ * tables of every stage.  The fab pointers of the tasks are kept: run the
+ * plan again after refilling the same fabs. */
+camr_status camr_batch_create(int nbox, const camr_box_task* tasks,
+                              const camr_geom* geom, const camr_hydro_params* p,
+                              void* stream, camr_batch** out);
+camr_status camr_batch_destroy(camr_batch* b);
+/* Run the plan.  dt_dev (may be NULL) points to a device double read by the
+ * kernels instead of dt, so a captured CUDA graph can follow a changing dt. */
+camr_status camr_batch_run(camr_batch* b, double dt, const double* dt_dev,
+                           int mode, void* stream);
+/* Time each stage's candidates (cells per block 128/256/512; grid = one
+ * block per work unit, or 1x / 2x the resident blocks of the device as a
+ * persistent grid-stride launch) on the plan's own boxes and keep the
+ * fastest.  Leaves dsdt untouched; synchronises. */
+camr_status camr_batch_autotune(camr_batch* b, double dt, void* stream);
+/* The chosen cells-per-block factor and grid of each stage (n >= 9). */
+camr_status camr_batch_tuning(camr_batch* b, int* chunk, unsigned* grid, int n);
+/* One-shot convenience: create, run persistent, destroy (synchronises). */
+camr_status camr_hydro_umdrv_batched(int nbox, const camr_box_task* tasks,
+                                     const camr_geom* geom,
+                                     const camr_hydro_params* p, double dt,
+                                     void* stream);
+
+/* ---------------------------------------------------------------------
  * Level-level API: one uniform level owned by the library on one GPU.
  * Replaces CAMR::CAMR_advance (Source/CAMR_advance.cpp:38-164) with its
  * construct_hydro_source box loop, expand_state/clean_state
