@@ -52,22 +52,25 @@ def sod(n, dx, prob_lo=(0.0, 0.0, 0.0), direction=0, gamma=1.4, p_l=1.0, p_r=0.1
 
 
 def blobs(n, dx, prob_lo=(0.0, 0.0, 0.0), gamma=1.4, nblobs=16, seed=1, p_blob=10.0,
-          r_min=0.03, r_max=0.08, amp=0.1, p0=1.0):
+          r_min=0.03, r_max=0.08, amp=0.1, p0=1.0, lo=(0, 0, 0), vel=None,
+          domain_len=None):
     """Smooth periodic density with seeded spherical overpressure blobs.
 
     rho = 1 + amp*sin(2 pi x) sin(2 pi y) sin(2 pi z), p = p0, zero velocity,
     p = p_blob inside each blob (periodic distance to the centre < radius).
     Blob draws from numpy's PCG64 generator seeded with `seed`: per blob the
-    centre (x, y, z) then the radius.
+    centre (x, y, z) then the radius.  `lo` offsets the cell indices (a box
+    of a finer level, with `domain_len` the periodic domain's length); `vel`
+    adds a uniform velocity (u, v, w).
     """
-    x, y, z = cell_centres(n, prob_lo, dx)
+    x, y, z = cell_centres(n, prob_lo, dx, lo)
     X = x[None, None, :]
     Y = y[None, :, None]
     Z = z[:, None, None]
     rho = 1.0 + amp * np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y) * np.sin(2 * np.pi * Z)
     p = np.full((n[2], n[1], n[0]), p0)
     rng = np.random.default_rng(seed)
-    L = [n[d] * dx[d] for d in range(3)]
+    L = list(domain_len) if domain_len is not None else [n[d] * dx[d] for d in range(3)]
     for _ in range(nblobs):
         c = rng.uniform(0.0, 1.0, size=3) * np.array(L) + np.array(prob_lo)
         r = rng.uniform(r_min, r_max)
@@ -83,6 +86,10 @@ def blobs(n, dx, prob_lo=(0.0, 0.0, 0.0), gamma=1.4, nblobs=16, seed=1, p_blob=1
     et = p / (gamma - 1.0)
     s[UEINT] = et
     s[UEDEN] = et
+    if vel is not None:
+        for d in range(3):
+            s[UMX + d] = rho * vel[d]
+        s[UEDEN] = et + 0.5 * rho * (vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)
     s[UFS] = 1.0 * rho
     s[UFS + 1] = 0.0 * rho
     s[UFS + 2] = 0.0 * rho
@@ -166,3 +173,21 @@ def amr_box_list(nbox=350, fine_n=512, sizes=(16, 24, 32, 48, 64), seed=7, nblob
         occ[a[0]:b[0], a[1]:b[1], a[2]:b[2]] = True
         boxes.append((tuple(int(v) for v in lo), tuple(int(v) for v in lo + sz - 1)))
     return boxes
+
+
+def amr_initial(n0, boxes, vel=(0.4, -0.3, 0.2), **kw):
+    """Two-level initial data of a periodic unit cube: the base level (n0
+    cells per side) and the fine boxes (refinement ratio 2) sampled from the
+    same `blobs` field at their own cell centres.  boxes: (lo, hi) fine
+    index triples.  Returns (S0, S1) with S1 the boxes' states back to back,
+    flattened."""
+    dx0 = tuple(1.0 / v for v in n0)
+    S0 = blobs(n0, dx0, vel=vel, **kw)
+    dx1 = tuple(0.5 / v for v in n0)
+    parts = []
+    for lo, hi in boxes:
+        nb = tuple(hi[d] - lo[d] + 1 for d in range(3))
+        parts.append(blobs(nb, dx1, lo=tuple(lo), vel=vel, domain_len=(1.0, 1.0, 1.0),
+                           **kw).ravel())
+    S1 = np.concatenate(parts) if parts else np.zeros(0)
+    return S0, S1

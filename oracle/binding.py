@@ -76,6 +76,9 @@ def load(kind="restate"):
                                          C.c_int, _DP]
     lib.orc_expand_state.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP, C.c_int, _DP]
     lib.orc_clean_state.argtypes = [C.POINTER(Params), C.POINTER(Level), _DP]
+    lib.orc_amr_run.restype = C.c_long
+    lib.orc_amr_run.argtypes = [C.POINTER(Params), C.POINTER(Level), C.c_int, C.c_void_p,
+                                _DP, _DP, C.c_int, C.c_int, C.c_int, _DP, C.c_void_p]
     _LIBS[kind] = lib
     return lib
 
@@ -164,3 +167,19 @@ def expand_state(kind, p, lev, state, ng=4):
 
 def clean_state(kind, p, lev, state):
     load(kind).orc_clean_state(C.byref(p), C.byref(lev), state)
+
+
+def amr_run(kind, p, lev0, boxes, S0, S1, nsteps, do_init=False, first_step=True,
+            clock=None):
+    """Two-level run in place.  boxes: (nbox, 6) int array of fine lo/hi;
+    S0: coarse valid state; S1: 1-D array, the fine boxes' states back to
+    back; clock: float64[4] (times of both levels, last dt of both levels),
+    updated in place.  Returns (dt history (nsteps, 2), nassert)."""
+    boxes = np.ascontiguousarray(boxes, dtype=np.int32).reshape(-1, 6)
+    hist = np.zeros((max(nsteps, 1), 2))
+    if clock is None:
+        clock = np.zeros(4)
+    n = load(kind).orc_amr_run(C.byref(p), C.byref(lev0), len(boxes), boxes.ctypes.data,
+                               S0, S1, nsteps, int(do_init), int(first_step), clock,
+                               hist.ctypes.data)
+    return hist[:nsteps], n

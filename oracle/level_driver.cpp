@@ -311,8 +311,57 @@ long expand_state(const Eos& eos, const orc_params& p, const orc_level& L, const
 }
 
 // construct_hydro_source over all tiles: dsdt = 0, then each tile's hydro.
+// Coarse side of a two-level flux register (restating AMReX YAFluxRegister
+// for refinement ratio 2): per coarse cell, its fine-box id (-1 if not
+// covered), the coarse cells outside the fine region that share a face
+// with it ("boundary cells"), and the accumulated correction d.
+struct FluxReg {
+  Fab d;                    // NVAR comps on the coarse domain (CrseAdd sums)
+  Fab cfp;                  // NVAR comps on the coarse domain (FineAdd sums)
+  std::vector<int> cmap;    // coarse cell -> fine box id or -1
+  std::vector<char> bnd;    // coarse cell is a coarse-fine boundary cell
+  int lo[3], n[3];
+  int periodic[3];
+  int cell(int i, int j, int k) const {
+    int c[3] = {i, j, k};
+    for (int d = 0; d < 3; ++d) {
+      int v = c[d] - lo[d];
+      if (periodic[d]) v = ((v % n[d]) + n[d]) % n[d];
+      else if (v < 0 || v >= n[d]) return -1;
+      c[d] = v;
+    }
+    return c[0] + n[0] * (c[1] + n[1] * c[2]);
+  }
+  int box_at(int i, int j, int k) const {
+    const int c = cell(i, j, k);
+    return c < 0 ? -1 : cmap[c];
+  }
+};
+
+// YAFluxRegister::CrseAdd on one tile: for every coarse-fine boundary cell
+// of the tile, remove the coarse flux through each face it shares with a
+// fine-covered cell (faces in the order x-, x+, y-, y+, z-, z+), scaled by
+// dt/vol (the fluxes are area-weighted).
+void crse_add(FluxReg& fr, const Box3& bx, const Fab* f, double dtdx) {
+  for_box(bx, [&](int i, int j, int k) {
+    const int c = fr.cell(i, j, k);
+    if (c < 0 || !fr.bnd[c]) return;
+    const int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int d = 0; d < 3; ++d) {
+      if (fr.box_at(i - e[d][0], j - e[d][1], k - e[d][2]) >= 0) {
+        for (int n = 0; n < NVAR; ++n) fr.d(i, j, k, n) -= dtdx * f[d](i, j, k, n);
+      }
+      if (fr.box_at(i + e[d][0], j + e[d][1], k + e[d][2]) >= 0) {
+        for (int n = 0; n < NVAR; ++n)
+          fr.d(i, j, k, n) += dtdx * f[d](i + e[d][0], j + e[d][1], k + e[d][2], n);
+      }
+    }
+  });
+}
+
 long hydro_level(const orc_params& p, const orc_level& L, const Grid& g, const Fab& B,
-                 const Fab* src, const Fab& dsdt, double dt) {
+                 const Fab* src, const Fab& dsdt, double dt, FluxReg* fr = nullptr,
+                 double fr_dtdx = 0.0) {
   const int nth = nthreads_of(L);
   par_cells(g, nth, [&](int i, int j, int k) {
     for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = 0.0;
@@ -331,6 +380,14 @@ long hydro_level(const orc_params& p, const orc_level& L, const Grid& g, const F
     nerr += orc_hydro_box(&p, bx.lo, bx.hi, L.dom_lo, L.dom_hi, L.bc_lo, L.bc_hi, B.p, B.lo,
                           B.hi, src ? src->p : nullptr, dsdt.p, dsdt.lo, dsdt.hi,
                           f[0].data(), f[1].data(), f[2].data(), L.dx, dt);
+    if (fr) {
+      Fab ff[3];
+      for (int d = 0; d < 3; ++d) {
+        const Box3 fb = faces(bx, d);
+        ff[d].view(f[d].data(), fb.lo, fb.hi, NVAR);
+      }
+      crse_add(*fr, bx, ff, fr_dtdx);
+    }
   }
   return nerr;
 }
@@ -397,7 +454,11 @@ struct Work {
 
 // One CAMR::advance + post_timestep on the state S (valid cells), in place.
 long advance_one(const Eos& eos, const orc_params& p, const orc_level& L, const Grid& g,
-                 const Fab& S, Work& w, double dt) {
+                 const Fab& S, Work& w, double dt, FluxReg* fr = nullptr, bool post = true) {
+  // CrseAdd scale of one construct_hydro_source call: fac_for_reflux*dt/vol
+  // (CAMR_construct_hydro_source.cpp:24, :245-247).
+  const double vol = L.dx[0] * L.dx[1] * L.dx[2];
+  const double fr_dtdx = ((p.do_mol ? 0.5 : 1.0) * dt) / vol;
   const int nth = nthreads_of(L);
   long nerr = 0;
   // swapTimeLevels: S_old <- S; clean_state(S_old).
@@ -417,12 +478,12 @@ long advance_one(const Eos& eos, const orc_params& p, const orc_level& L, const 
     });
   }
   if (p.do_mol) {
-    nerr += hydro_level(p, L, g, w.B, nullptr, w.dsdt, dt);
+    nerr += hydro_level(p, L, g, w.B, nullptr, w.dsdt, dt, fr, fr_dtdx);
     par_cells(g, nth, [&](int i, int j, int k) {
       for (int n = 0; n < NVAR; ++n) S(i, j, k, n) += dt * w.dsdt(i, j, k, n);
     });
     nerr += expand_state(eos, p, L, g, S, w.B2);
-    nerr += hydro_level(p, L, g, w.B2, nullptr, w.dsdt2, dt);
+    nerr += hydro_level(p, L, g, w.B2, nullptr, w.dsdt2, dt, fr, fr_dtdx);
     par_cells(g, nth, [&](int i, int j, int k) {
       for (int n = 0; n < NVAR; ++n) {
         S(i, j, k, n) = 0.5 * w.B2(i, j, k, n) + 0.5 * w.S_old(i, j, k, n);
@@ -460,7 +521,7 @@ long advance_one(const Eos& eos, const orc_params& p, const orc_level& L, const 
                 for (int n = 0; n < NVAR; ++n) sf(i, j, k, n) = sf(img[0], img[1], img[2], n);
               });
     }
-    nerr += hydro_level(p, L, g, w.B, &w.sfh, w.dsdt, dt);
+    nerr += hydro_level(p, L, g, w.B, &w.sfh, w.dsdt, dt, fr, fr_dtdx);
     par_cells(g, nth, [&](int i, int j, int k) {
       for (int n = 0; n < NVAR; ++n) S(i, j, k, n) += dt * w.dsdt(i, j, k, n);
     });
@@ -474,7 +535,7 @@ long advance_one(const Eos& eos, const orc_params& p, const orc_level& L, const 
     nerr += clean_state_valid(eos, p, L, g, S);
   }
   // CAMR::post_timestep: clean_state(S_new).
-  nerr += clean_state_valid(eos, p, L, g, S);
+  if (post) nerr += clean_state_valid(eos, p, L, g, S);
   return nerr;
 }
 
@@ -490,6 +551,553 @@ void alloc_work(const Grid& g, Work& w) {
   w.sfh.alloc(b4.lo, b4.hi, NVAR);
 }
 
+
+// ===========================================================================
+// Two-level AMR with subcycling (refinement ratio 2), restating AMReX's
+// Amr::timeStep / FillPatchTwoLevels / YAFluxRegister / average_down as
+// CAMR drives them (Source/CAMR_advance.cpp:38-164, Source/CAMR.cpp:566-635,
+// :679-718, :803-851, :1048-1066; Source/Hydro/CAMR_construct_hydro_source.cpp:243-254).
+// AMReX itself is absent, so these steps follow its documented algorithms;
+// the order of a few floating-point sums (flux-register contributions to one
+// coarse cell) is this file's choice.  Periodic domains only.
+
+constexpr int RR = 2;  // refinement ratio
+
+struct Fine {
+  std::vector<Box3> boxes;
+  orc_level L;
+  std::vector<Fab> S, S_old, B, B2, dsdt, dsdt2, sfh;
+  std::vector<std::vector<double>> fbuf[3];
+  std::vector<Fab> F[3];  // face fluxes of the last hydro call
+};
+
+inline int wrap(int v, int lo, int n) { return lo + (((v - lo) % n) + n) % n; }
+
+FluxReg make_fluxreg(const Grid& gc, const orc_level& Lc, const std::vector<Box3>& fboxes) {
+  FluxReg fr;
+  for (int d = 0; d < 3; ++d) {
+    fr.lo[d] = gc.dom.lo[d];
+    fr.n[d] = gc.n[d];
+    fr.periodic[d] = Lc.is_periodic[d];
+  }
+  const size_t nc = size_t(gc.ncell);
+  fr.cmap.assign(nc, -1);
+  fr.bnd.assign(nc, 0);
+  for (int b = 0; b < int(fboxes.size()); ++b) {
+    Box3 cb;
+    for (int d = 0; d < 3; ++d) {
+      cb.lo[d] = fboxes[b].lo[d] / RR;
+      cb.hi[d] = fboxes[b].hi[d] / RR;
+    }
+    for_box(cb, [&](int i, int j, int k) { fr.cmap[fr.cell(i, j, k)] = b; });
+  }
+  for_box(gc.dom, [&](int i, int j, int k) {
+    const int c = fr.cell(i, j, k);
+    if (fr.cmap[c] >= 0) return;
+    const int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int d = 0; d < 3; ++d)
+      if (fr.box_at(i - e[d][0], j - e[d][1], k - e[d][2]) >= 0 ||
+          fr.box_at(i + e[d][0], j + e[d][1], k + e[d][2]) >= 0)
+        fr.bnd[c] = 1;
+  });
+  fr.d.alloc(gc.dom.lo, gc.dom.hi, NVAR);
+  fr.cfp.alloc(gc.dom.lo, gc.dom.hi, NVAR);
+  return fr;
+}
+
+// Coarse data at time t from the old/new coarse states (StateData::getData
+// then FillPatchSingleLevel's time interpolation).
+struct CoarseAt {
+  const Fab* old_s;
+  const Fab* new_s;
+  double t0, t1, t;
+  int mode;  // 0 new, 1 old, 2 interpolate
+  double alpha, beta;
+  // StateData::getData: the new (old) data when t is within
+  // 1e-3 (t1 - t0) of t1 (t0), else both, combined by LinComb with
+  // alpha = (t1 - t)/(t1 - t0), beta = (t - t0)/(t1 - t0).
+  void init() {
+    const double teps = (t1 - t0) * 1.e-3;
+    if (t > t1 - teps && t < t1 + teps) mode = 0;
+    else if (t > t0 - teps && t < t0 + teps) mode = 1;
+    else {
+      mode = 2;
+      alpha = (t1 - t) / (t1 - t0);
+      beta = (t - t0) / (t1 - t0);
+    }
+  }
+  double operator()(int i, int j, int k, int n) const {
+    if (mode == 0) return (*new_s)(i, j, k, n);
+    if (mode == 1) return (*old_s)(i, j, k, n);
+    return alpha * (*old_s)(i, j, k, n) + beta * (*new_s)(i, j, k, n);
+  }
+};
+
+// Conservative linear interpolation of component n to fine cell (fi,fj,fk)
+// (AMReX CellConservativeLinear with limiting, ratio 2).  Per direction an
+// MC-limited slope: dc = (u+ - u-)/2, s = min(|2(u+ - u)|, |2(u - u-)|) when
+// those agree in sign (else 0), s = sign(dc) min(s, |dc|); then one factor
+// alpha <= 1 for all three slopes keeps every fine child inside the min/max
+// of the 27 coarse neighbours (the children lie at most (r-1)/(2r) = 1/4 of
+// a slope from the centre).  fine = u + ox*sx + oy*sy + oz*sz, o = -+1/4.
+double cons_interp(const CoarseAt& C, const Grid& gc, int fi, int fj, int fk, int n) {
+  const int f[3] = {fi, fj, fk};
+  int c[3];
+  for (int d = 0; d < 3; ++d) c[d] = (f[d] >= 0) ? f[d] / RR : -((-f[d] + RR - 1) / RR);
+  auto at = [&](int di, int dj, int dk) {
+    return C(wrap(c[0] + di, gc.dom.lo[0], gc.n[0]), wrap(c[1] + dj, gc.dom.lo[1], gc.n[1]),
+             wrap(c[2] + dk, gc.dom.lo[2], gc.n[2]), n);
+  };
+  const double uc = at(0, 0, 0);
+  double sl[3];
+  const int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int d = 0; d < 3; ++d) {
+    const double up = at(e[d][0], e[d][1], e[d][2]);
+    const double um = at(-e[d][0], -e[d][1], -e[d][2]);
+    const double dc = 0.5 * (up - um);
+    const double df = 2.0 * (up - uc);
+    const double db = 2.0 * (uc - um);
+    double sv = (df * db >= 0.0) ? std::min(std::fabs(df), std::fabs(db)) : 0.0;
+    sv = std::copysign(1.0, dc) * std::min(sv, std::fabs(dc));
+    sl[d] = sv;
+  }
+  double alpha = 1.0;
+  if (sl[0] != 0.0 || sl[1] != 0.0 || sl[2] != 0.0) {
+    const double dumax = std::fabs(sl[0]) * 0.25 + std::fabs(sl[1]) * 0.25 + std::fabs(sl[2]) * 0.25;
+    double umax = uc, umin = uc;
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) {
+          const double v = at(di, dj, dk);
+          umax = std::max(umax, v);
+          umin = std::min(umin, v);
+        }
+    if (dumax * alpha > (umax - uc)) alpha = (umax - uc) / dumax;
+    if (dumax * alpha > (uc - umin)) alpha = (uc - umin) / dumax;
+  }
+  double off[3];
+  for (int d = 0; d < 3; ++d) off[d] = (f[d] - RR * c[d] == 0) ? -0.25 : 0.25;
+  return uc + off[0] * (sl[0] * alpha) + off[1] * (sl[1] * alpha) + off[2] * (sl[2] * alpha);
+}
+
+// FillBoundary of the fine level: every ghost cell of grow(box, 4) that a
+// fine box covers (through the periodic domain) gets that box's valid value.
+void fine_fill_boundary(const Fine& fn, const FluxReg& fr, std::vector<Fab>& Bv) {
+  int fdlo[3], fn_n[3];
+  for (int d = 0; d < 3; ++d) {
+    fdlo[d] = fn.L.dom_lo[d];
+    fn_n[d] = fn.L.dom_hi[d] - fn.L.dom_lo[d] + 1;
+  }
+  const int nb = int(fn.boxes.size());
+  for (int b = 0; b < nb; ++b) {
+    const Box3& bx = fn.boxes[b];
+    for_box(grow(bx, 4), [&](int i, int j, int k) {
+      const bool valid = i >= bx.lo[0] && i <= bx.hi[0] && j >= bx.lo[1] && j <= bx.hi[1] &&
+                         k >= bx.lo[2] && k <= bx.hi[2];
+      if (valid) return;
+      const int wi = wrap(i, fdlo[0], fn_n[0]), wj = wrap(j, fdlo[1], fn_n[1]),
+                wk = wrap(k, fdlo[2], fn_n[2]);
+      const int ob = fr.box_at(wi / RR, wj / RR, wk / RR);
+      if (ob >= 0)
+        for (int n = 0; n < NVAR; ++n) Bv[b](i, j, k, n) = Bv[ob](wi, wj, wk, n);
+    });
+  }
+}
+
+// FillPatchTwoLevels + clean_state of every fine box's Sborder from the fine
+// valid data src and the coarse data at time t.
+void fine_expand(const Eos& eos, const orc_params& p, Fine& fn, const Grid& gc,
+                 const FluxReg& fr, const std::vector<Fab>& src, const CoarseAt& C,
+                 std::vector<Fab>& Bv) {
+  const int nb = int(fn.boxes.size());
+  const int nth = nthreads_of(fn.L);
+  int fdlo[3], fn_n[3];
+  for (int d = 0; d < 3; ++d) {
+    fdlo[d] = fn.L.dom_lo[d];
+    fn_n[d] = fn.L.dom_hi[d] - fn.L.dom_lo[d] + 1;
+  }
+  // valid cells, then enforce_min_density and normalize_species on them
+#pragma omp parallel for num_threads(nth) schedule(dynamic)
+  for (int b = 0; b < nb; ++b) {
+    const Box3& bx = fn.boxes[b];
+    for_box(bx, [&](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) Bv[b](i, j, k, n) = src[b](i, j, k, n);
+    });
+    enforce_min_density_tile(eos, p, Bv[b], bx);
+    for_box(bx, [&](int i, int j, int k) { normalize_species_cell(Bv[b], i, j, k); });
+  }
+  // ghost cells: fine-fine from the other boxes' cleaned valid data
+  // (FillBoundary at the end of normalize_species), coarse-fine from the
+  // interpolated coarse data; then computeTemp on every cell
+  fine_fill_boundary(fn, fr, Bv);
+#pragma omp parallel for num_threads(nth) schedule(dynamic)
+  for (int b = 0; b < nb; ++b) {
+    const Box3& bx = fn.boxes[b];
+    for_box(grow(bx, 4), [&](int i, int j, int k) {
+      const bool valid = i >= bx.lo[0] && i <= bx.hi[0] && j >= bx.lo[1] && j <= bx.hi[1] &&
+                         k >= bx.lo[2] && k <= bx.hi[2];
+      if (valid) return;
+      const int wi = wrap(i, fdlo[0], fn_n[0]), wj = wrap(j, fdlo[1], fn_n[1]),
+                wk = wrap(k, fdlo[2], fn_n[2]);
+      if (fr.box_at(wi / RR, wj / RR, wk / RR) < 0)
+        for (int n = 0; n < NVAR; ++n) Bv[b](i, j, k, n) = cons_interp(C, gc, i, j, k, n);
+    });
+  }
+#pragma omp parallel for num_threads(nth) schedule(dynamic)
+  for (int b = 0; b < nb; ++b) {
+    for_box(grow(fn.boxes[b], 4), [&](int i, int j, int k) { compute_temp_cell(eos, p, Bv[b], i, j, k); });
+  }
+}
+
+// YAFluxRegister::FineAdd for one fine hydro call, box after box: for
+// each side of each fine box, every coarse cell just outside it that no
+// fine box covers gets the fine fluxes of its 4 fine faces (slower
+// transverse index outer), scaled by dt_f/(vol_f * ratio^3); subtracted on
+// the box's low side, added on its high side.  The sums go to cfp, which
+// the reflux adds to the CrseAdd sums.
+void fine_add(FluxReg& fr, const Grid& gc, const Fine& fn, double dtdx) {
+  for (size_t b = 0; b < fn.boxes.size(); ++b) {
+    Box3 cb;
+    for (int d = 0; d < 3; ++d) {
+      cb.lo[d] = fn.boxes[b].lo[d] / RR;
+      cb.hi[d] = fn.boxes[b].hi[d] / RR;
+    }
+    for (int d = 0; d < 3; ++d) {
+      const int t1 = (d == 0) ? 1 : 0;  // faster transverse index
+      const int t2 = (d == 2) ? 1 : 2;  // slower transverse index
+      for (int side = 0; side < 2; ++side) {
+        Box3 adj = cb;
+        adj.lo[d] = adj.hi[d] = side ? cb.hi[d] + 1 : cb.lo[d] - 1;
+        const int fface = side ? RR * (cb.hi[d] + 1) : RR * cb.lo[d];
+        for (int n = 0; n < NVAR; ++n)
+          for_box(adj, [&](int i, int j, int k) {
+            if (fr.box_at(i, j, k) >= 0) return;
+            const int cc[3] = {i, j, k};
+            int w[3];
+            for (int e = 0; e < 3; ++e) w[e] = wrap(cc[e], gc.dom.lo[e], gc.n[e]);
+            double& acc = fr.cfp(w[0], w[1], w[2], n);
+            for (int a2 = 0; a2 < RR; ++a2)
+              for (int a1 = 0; a1 < RR; ++a1) {
+                int fi[3];
+                fi[d] = fface;
+                fi[t1] = RR * cc[t1] + a1;
+                fi[t2] = RR * cc[t2] + a2;
+                const double v = dtdx * fn.F[d][b](fi[0], fi[1], fi[2], n);
+                if (side) acc += v;
+                else acc -= v;
+              }
+          });
+      }
+    }
+  }
+}
+
+double est_dt_boxes(const Eos& eos, const orc_params& p, const orc_level& L,
+                    const std::vector<Box3>& boxes, const std::vector<Fab>& S) {
+  if (p.fixed_dt > 0.0) return p.fixed_dt;
+  double estdt = p.max_dt;
+  double estdt_hydro = p.max_dt / p.cfl;
+  double dt = std::numeric_limits<double>::max();
+  for (size_t b = 0; b < boxes.size(); ++b) {
+    for_box(boxes[b], [&](int i, int j, int k) {
+      const Fab& U = S[b];
+      const double rho = U(i, j, k, URHO);
+      const double rhoInv = 1.0 / rho;
+      const double eint = U(i, j, k, UEINT) / rho;
+      const double pres = eos.rey2p(rho, eint);
+      const double c = std::sqrt(eos.gamma * pres / rho);
+      dt = std::min(dt, L.dx[0] / (c + std::fabs(U(i, j, k, UMX) * rhoInv)));
+      dt = std::min(dt, L.dx[1] / (c + std::fabs(U(i, j, k, UMY) * rhoInv)));
+      dt = std::min(dt, L.dx[2] / (c + std::fabs(U(i, j, k, UMZ) * rhoInv)));
+    });
+  }
+  estdt_hydro = std::min(estdt_hydro, dt);
+  estdt_hydro *= p.cfl;
+  if (estdt_hydro < estdt) estdt = estdt_hydro;
+  return estdt;
+}
+
+long clean_boxes(const Eos& eos, const orc_params& p, Fine& fn, std::vector<Fab>& S) {
+  long nerr = 0;
+  const int nb = int(fn.boxes.size());
+  const int nth = nthreads_of(fn.L);
+#pragma omp parallel for num_threads(nth) reduction(+ : nerr) schedule(dynamic)
+  for (int b = 0; b < nb; ++b) {
+    nerr += enforce_min_density_tile(eos, p, S[b], fn.boxes[b]);
+    for_box(fn.boxes[b], [&](int i, int j, int k) { normalize_species_cell(S[b], i, j, k); });
+    for_box(fn.boxes[b], [&](int i, int j, int k) { compute_temp_cell(eos, p, S[b], i, j, k); });
+  }
+  return nerr;
+}
+
+// hydro of every fine box (construct_hydro_source on level 1), then FineAdd.
+long fine_hydro(const orc_params& p, Fine& fn, std::vector<Fab>& Bv, std::vector<Fab>& dsdt,
+                const std::vector<Fab>* src, double dt, FluxReg& fr, const Grid& gc,
+                double dtdx_fine) {
+  long nerr = 0;
+  const int nb = int(fn.boxes.size());
+  const int nth = nthreads_of(fn.L);
+#pragma omp parallel for num_threads(nth) reduction(+ : nerr) schedule(dynamic)
+  for (int b = 0; b < nb; ++b) {
+    const Box3& bx = fn.boxes[b];
+    for_box(bx, [&](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) dsdt[b](i, j, k, n) = 0.0;
+    });
+    nerr += orc_hydro_box(&p, bx.lo, bx.hi, fn.L.dom_lo, fn.L.dom_hi, fn.L.bc_lo, fn.L.bc_hi,
+                          Bv[b].p, Bv[b].lo, Bv[b].hi, src ? (*src)[b].p : nullptr, dsdt[b].p, dsdt[b].lo,
+                          dsdt[b].hi, fn.F[0][b].p, fn.F[1][b].p, fn.F[2][b].p, fn.L.dx, dt);
+  }
+  fine_add(fr, gc, fn, dtdx_fine);
+  return nerr;
+}
+
+// One fine-level CAMR::advance + post_timestep (finest level).
+long fine_advance(const Eos& eos, const orc_params& p, Fine& fn, const Grid& gc, FluxReg& fr,
+                  const Fab& c_old, const Fab& c_new, double tc0, double tc1, double tf_old,
+                  double tf_new, double dt) {
+  long nerr = 0;
+  const int nb = int(fn.boxes.size());
+  const double volf = fn.L.dx[0] * fn.L.dx[1] * fn.L.dx[2];
+  const double dtdx_f = ((p.do_mol ? 0.5 : 1.0) * dt) / (volf * double(RR * RR * RR));
+  for (int b = 0; b < nb; ++b) {
+    for_box(fn.boxes[b], [&](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) fn.S_old[b](i, j, k, n) = fn.S[b](i, j, k, n);
+    });
+  }
+  nerr += clean_boxes(eos, p, fn, fn.S_old);
+  CoarseAt C0{&c_old, &c_new, tc0, tc1, tf_old, 0, 0.0, 0.0};
+  C0.init();
+  fine_expand(eos, p, fn, gc, fr, fn.S_old, C0, fn.B);
+  for (int b = 0; b < nb; ++b) {
+    for_box(fn.boxes[b], [&](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) fn.S[b](i, j, k, n) = fn.B[b](i, j, k, n);
+      if (p.add_grav_src) {
+        double src[NVAR];
+        for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+        src[UMZ] = p.const_grav * fn.S_old[b](i, j, k, URHO);
+        src[UEDEN] = p.const_grav * fn.S_old[b](i, j, k, UMZ);
+        for (int n = 0; n < NVAR; ++n) fn.S[b](i, j, k, n) += dt * src[n];
+      }
+    });
+  }
+  if (p.do_mol) {
+    nerr += fine_hydro(p, fn, fn.B, fn.dsdt, nullptr, dt, fr, gc, dtdx_f);
+    for (int b = 0; b < nb; ++b)
+      for_box(fn.boxes[b], [&](int i, int j, int k) {
+        for (int n = 0; n < NVAR; ++n) fn.S[b](i, j, k, n) += dt * fn.dsdt[b](i, j, k, n);
+      });
+    CoarseAt C1{&c_old, &c_new, tc0, tc1, tf_new, 0, 0.0, 0.0};
+    C1.init();
+    fine_expand(eos, p, fn, gc, fr, fn.S, C1, fn.B2);
+    nerr += fine_hydro(p, fn, fn.B2, fn.dsdt2, nullptr, dt, fr, gc, dtdx_f);
+    for (int b = 0; b < nb; ++b)
+      for_box(fn.boxes[b], [&](int i, int j, int k) {
+        for (int n = 0; n < NVAR; ++n)
+          fn.S[b](i, j, k, n) = 0.5 * fn.B2[b](i, j, k, n) + 0.5 * fn.S_old[b](i, j, k, n);
+        for (int n = 0; n < NVAR; ++n) fn.S[b](i, j, k, n) += 0.5 * dt * fn.dsdt2[b](i, j, k, n);
+      });
+  } else {
+    // sources_for_hydro: 0 + 1.0 * old source on valid cells, FillBoundary
+    // from the other fine boxes, zero on the coarse-fine ghost cells.
+    for (int b = 0; b < nb; ++b) {
+      for (auto& v : fn.sfh[b].own) v = 0.0;
+      if (p.add_grav_src)
+        for_box(fn.boxes[b], [&](int i, int j, int k) {
+          double src[NVAR];
+          for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+          src[UMZ] = p.const_grav * fn.S_old[b](i, j, k, URHO);
+          src[UEDEN] = p.const_grav * fn.S_old[b](i, j, k, UMZ);
+          for (int n = 0; n < NVAR; ++n) fn.sfh[b](i, j, k, n) += 1.0 * src[n];
+        });
+    }
+    if (p.add_grav_src) fine_fill_boundary(fn, fr, fn.sfh);
+    nerr += fine_hydro(p, fn, fn.B, fn.dsdt, &fn.sfh, dt, fr, gc, dtdx_f);
+    for (int b = 0; b < nb; ++b)
+      for_box(fn.boxes[b], [&](int i, int j, int k) {
+        for (int n = 0; n < NVAR; ++n) fn.S[b](i, j, k, n) += dt * fn.dsdt[b](i, j, k, n);
+      });
+  }
+  nerr += clean_boxes(eos, p, fn, fn.S);
+  if (p.add_grav_src) {
+    for (int b = 0; b < nb; ++b)
+      for_box(fn.boxes[b], [&](int i, int j, int k) {
+        double src[NVAR];
+        for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+        src[UMZ] = 0.5 * p.const_grav * (fn.S[b](i, j, k, URHO) - fn.S_old[b](i, j, k, URHO));
+        src[UEDEN] = 0.5 * p.const_grav * (fn.S[b](i, j, k, UMZ) - fn.S_old[b](i, j, k, UMZ));
+        for (int n = 0; n < NVAR; ++n) fn.S[b](i, j, k, n) += dt * src[n];
+      });
+    nerr += clean_boxes(eos, p, fn, fn.S);
+  }
+  nerr += clean_boxes(eos, p, fn, fn.S);  // post_timestep of the finest level
+  return nerr;
+}
+
+void avg_down(const Grid& gc, const Fine& fn, const Fab& Sc) {
+  for (size_t b = 0; b < fn.boxes.size(); ++b) {
+    Box3 cb;
+    for (int d = 0; d < 3; ++d) {
+      cb.lo[d] = fn.boxes[b].lo[d] / RR;
+      cb.hi[d] = fn.boxes[b].hi[d] / RR;
+    }
+    const double volfrac = 1.0 / static_cast<double>(RR * RR * RR);
+    for_box(cb, [&](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) {
+        double c = 0.0;
+        for (int kr = 0; kr < RR; ++kr)
+          for (int jr = 0; jr < RR; ++jr)
+            for (int ir = 0; ir < RR; ++ir)
+              c += fn.S[b](RR * i + ir, RR * j + jr, RR * k + kr, n);
+        Sc(i, j, k, n) = volfrac * c;
+      }
+    });
+  }
+  (void)gc;
+}
+
+}  // namespace
+}  // namespace orc
+
+extern "C" long orc_amr_run(const orc_params* p, const orc_level* lev0, int nbox,
+                            const int* boxes, double* S0, double* S1, int nsteps, int do_init,
+                            int first_step, double* clock, double* dt_hist) {
+  using namespace orc;
+  const Eos eos{p->eos_gamma};
+  const orc_level& Lc = *lev0;
+  const Grid gc = make_grid(Lc);
+  Fab Sc;
+  Sc.view(S0, gc.dom.lo, gc.dom.hi, NVAR);
+  Fine fn;
+  fn.L = Lc;
+  for (int d = 0; d < 3; ++d) {
+    fn.L.dom_lo[d] = Lc.dom_lo[d] * RR;
+    fn.L.dom_hi[d] = (Lc.dom_hi[d] + 1) * RR - 1;
+    fn.L.dx[d] = Lc.dx[d] / RR;
+    fn.L.max_grid_size[d] = 0;
+    fn.L.tile_size[d] = 0;
+  }
+  size_t off = 0;
+  for (int b = 0; b < nbox; ++b) {
+    Box3 bx;
+    for (int d = 0; d < 3; ++d) {
+      bx.lo[d] = boxes[6 * b + d];
+      bx.hi[d] = boxes[6 * b + 3 + d];
+    }
+    fn.boxes.push_back(bx);
+  }
+  const int nb = nbox;
+  fn.S.resize(nb);
+  fn.S_old.resize(nb);
+  fn.B.resize(nb);
+  fn.B2.resize(nb);
+  fn.dsdt.resize(nb);
+  fn.dsdt2.resize(nb);
+  fn.sfh.resize(nb);
+  for (int d = 0; d < 3; ++d) {
+    fn.fbuf[d].resize(nb);
+    fn.F[d].resize(nb);
+  }
+  for (int b = 0; b < nb; ++b) {
+    const Box3& bx = fn.boxes[b];
+    fn.S[b].view(S1 + off, bx.lo, bx.hi, NVAR);
+    off += size_t(fn.S[b].sn) * NVAR;
+    fn.S_old[b].alloc(bx.lo, bx.hi, NVAR);
+    const Box3 g4 = grow(bx, 4);
+    fn.B[b].alloc(g4.lo, g4.hi, NVAR);
+    fn.B2[b].alloc(g4.lo, g4.hi, NVAR);
+    fn.sfh[b].alloc(g4.lo, g4.hi, NVAR);
+    fn.dsdt[b].alloc(bx.lo, bx.hi, NVAR);
+    fn.dsdt2[b].alloc(bx.lo, bx.hi, NVAR);
+    for (int d = 0; d < 3; ++d) {
+      const Box3 fb = faces(bx, d);
+      fn.fbuf[d][b].resize(size_t(fb.hi[0] - fb.lo[0] + 1) * (fb.hi[1] - fb.lo[1] + 1) *
+                           (fb.hi[2] - fb.lo[2] + 1) * NVAR);
+      fn.F[d][b].view(fn.fbuf[d][b].data(), fb.lo, fb.hi, NVAR);
+    }
+  }
+  FluxReg fr = make_fluxreg(gc, Lc, fn.boxes);
+  Work w;
+  alloc_work(gc, w);
+  long nerr = 0;
+  if (do_init) {
+    // CAMR::initData epilogue on both levels, then post_init's avgDown.
+    orc_init_finalize(p, &Lc, S0);
+    for (int b = 0; b < nb; ++b) {
+      for_box(fn.boxes[b], [&](int i, int j, int k) {
+        Fab& U = fn.S[b];
+        const double rhoInv = 1.0 / U(i, j, k, URHO);
+        const double u = U(i, j, k, UMX) * rhoInv;
+        const double v = U(i, j, k, UMY) * rhoInv;
+        const double ww = U(i, j, k, UMZ) * rhoInv;
+        U(i, j, k, UEDEN) = U(i, j, k, UEINT) + 0.5 * U(i, j, k, URHO) * (u * u + v * v + ww * ww);
+        compute_temp_cell(eos, *p, U, i, j, k);
+      });
+    }
+    avg_down(gc, fn, Sc);
+  }
+  double dtl[2] = {clock[2], clock[3]};
+  double tc_new = clock[0], tf_new = clock[1];
+  const int ncyc[2] = {1, RR};
+  for (int step = 0; step < nsteps; ++step) {
+    // Amr::computeInitialDt / CAMR::computeNewDt over both levels
+    double dtm[2];
+    dtm[0] = est_dt(eos, *p, Lc, gc, Sc);
+    dtm[1] = est_dt_boxes(eos, *p, fn.L, fn.boxes, fn.S);
+    if (step == 0 && first_step) {
+      for (int l = 0; l < 2; ++l)
+        dtm[l] = (p->initial_dt > 0.0) ? p->initial_dt : p->init_shrink * dtm[l];
+    } else if (p->fixed_dt <= 0.0) {
+      for (int l = 0; l < 2; ++l) dtm[l] = std::min(dtm[l], p->change_max * dtl[l]);
+    }
+    double dt_0 = std::numeric_limits<double>::max();
+    int nf = 1;
+    for (int l = 0; l < 2; ++l) {
+      nf *= ncyc[l];
+      dt_0 = std::min(dt_0, nf * dtm[l]);
+    }
+    nf = 1;
+    for (int l = 0; l < 2; ++l) {
+      nf *= ncyc[l];
+      dtl[l] = dt_0 / nf;
+    }
+    if (dt_hist) {
+      dt_hist[2 * step] = dtl[0];
+      dt_hist[2 * step + 1] = dtl[1];
+    }
+    // level 0: flux register reset, advance (CrseAdd), keep old/new
+    for (auto& v : fr.d.own) v = 0.0;
+    for (auto& v : fr.cfp.own) v = 0.0;
+    const double tc_old = tc_new;
+    tc_new = tc_new + dtl[0];
+    nerr += advance_one(eos, *p, Lc, gc, Sc, w, dtl[0], &fr, false);
+    // level 1: two subcycled steps
+    Fab c_new_copy(gc.dom.lo, gc.dom.hi, NVAR);
+    std::memcpy(c_new_copy.p, Sc.p, sizeof(double) * size_t(gc.ncell) * NVAR);
+    for (int sc = 0; sc < RR; ++sc) {
+      const double tf_old = tf_new;
+      tf_new = tf_new + dtl[1];
+      nerr += fine_advance(eos, *p, fn, gc, fr, w.S_old, c_new_copy, tc_old, tc_new, tf_old,
+                           tf_new, dtl[1]);
+    }
+    // post_timestep(0): reflux, avgDown, clean_state
+    for_box(gc.dom, [&](int i, int j, int k) {
+      for (int n = 0; n < NVAR; ++n) {
+        const double dcorr = fr.d(i, j, k, n) + fr.cfp(i, j, k, n);
+        Sc(i, j, k, n) = Sc(i, j, k, n) + dcorr;
+      }
+    });
+    avg_down(gc, fn, Sc);
+    nerr += clean_state_valid(eos, *p, Lc, gc, Sc);
+  }
+  clock[0] = tc_new;
+  clock[1] = tf_new;
+  clock[2] = dtl[0];
+  clock[3] = dtl[1];
+  return nerr;
+}
+
+namespace orc {
+namespace {
 }  // namespace
 }  // namespace orc
 

@@ -117,6 +117,19 @@ long orc_advance_fixed_dt(const orc_params* p, const orc_level* lev,
 void orc_expand_state(const orc_params* p, const orc_level* lev,
                       const double* state, int ng, double* border);
 
+/* Two-level AMR run (refinement ratio 2, subcycling, reflux, average
+ * down; periodic domains).  lev0: the base level.  boxes: nbox fine boxes
+ * as lo0,lo1,lo2,hi0,hi1,hi2 in the fine index space (coarse-aligned).
+ * S0: base state (valid cells); S1: the fine boxes' states, box after box,
+ * each (NVAR, nz, ny, nx).  do_init: apply initData's epilogue to both
+ * levels and post_init's average-down first.  first_step: take the
+ * first dt from computeInitialDt.  clock (in/out): time of level 0, time
+ * of level 1, last dt of level 0, last dt of level 1.  dt_hist (may be
+ * NULL): 2*nsteps doubles, the dt of each level per coarse step. */
+long orc_amr_run(const orc_params* p, const orc_level* lev0, int nbox, const int* boxes,
+                 double* S0, double* S1, int nsteps, int do_init, int first_step,
+                 double* clock, double* dt_hist);
+
 /* clean_state on the valid cells (Source/CAMR.cpp:1253-1262). */
 void orc_clean_state(const orc_params* p, const orc_level* lev, double* state);
 
