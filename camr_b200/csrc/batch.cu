@@ -49,6 +49,7 @@ bool stage_used(int stage, bool mol) {
 struct camr_batch {
   int nbox = 0;
   bool mol = false;
+  bool fluxes_only = false;  // no dsdt: the caller forms the update from the fluxes
   bool has_src = false;
   KParams P;
   std::vector<BoxCtx> host_boxes;
@@ -63,12 +64,14 @@ struct camr_batch {
 
 namespace {
 
-camr_status fill_box(const camr_box_task& t, const camr_geom& geom, bool mol, BoxCtx& c) {
+camr_status fill_box(const camr_box_task& t, const camr_geom& geom, bool mol, bool need_dsdt,
+                     BoxCtx& c) {
   for (int d = 0; d < 3; ++d) {
     if (t.hi[d] < t.lo[d]) return CAMR_ERR_INVALID;
     if (!t.uin.ptr || t.uin.lo[d] > t.lo[d] - NGROW || t.uin.hi[d] < t.hi[d] + NGROW)
       return CAMR_ERR_INVALID;
-    if (!t.dsdt.ptr || t.dsdt.lo[d] > t.lo[d] || t.dsdt.hi[d] < t.hi[d]) return CAMR_ERR_INVALID;
+    if (need_dsdt && (!t.dsdt.ptr || t.dsdt.lo[d] > t.lo[d] || t.dsdt.hi[d] < t.hi[d]))
+      return CAMR_ERR_INVALID;
     if (!t.flx[d].ptr) return CAMR_ERR_INVALID;
     c.g.lo[d] = t.lo[d];
     c.g.hi[d] = t.hi[d];
@@ -84,6 +87,7 @@ camr_status fill_box(const camr_box_task& t, const camr_geom& geom, bool mol, Bo
   for (int d = 0; d < 3; ++d) c.flx[d] = make_dfab(t.flx[d]);
   c.dsdt = make_dfab(t.dsdt);
   c.mol = mol;
+  (void)need_dsdt;
   c.w.s = make_space(t.lo, t.hi);
   return CAMR_OK;
 }
@@ -139,10 +143,11 @@ const int kOrderMol[] = {BS_CTOPRIM, BS_FLATDIVU, BS_MOLSLOPE, BS_MOLFLUX, BS_CO
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-camr_status camr_batch_create(int nbox, const camr_box_task* tasks, const camr_geom* geom,
-                              const camr_hydro_params* p, void* stream, camr_batch** out) {
+camr_status batch_create_impl(int nbox, const camr_box_task* tasks, const camr_geom* geom,
+                              const camr_hydro_params* p, void* stream, bool fluxes_only,
+                              camr_batch** out) {
   if (nbox <= 0 || !tasks || !geom || !p || !out) return CAMR_ERR_INVALID;
   if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
@@ -151,12 +156,13 @@ camr_status camr_batch_create(int nbox, const camr_box_task* tasks, const camr_g
   if (!b) return CAMR_ERR_NOMEM;
   b->nbox = nbox;
   b->mol = p->do_mol != 0;
+  b->fluxes_only = fluxes_only;
   b->P = make_kparams(*p);
   b->host_boxes.resize(nbox);
   size_t total = 0;
   std::vector<size_t> offs(nbox);
   for (int i = 0; i < nbox; ++i) {
-    camr_status cs = fill_box(tasks[i], *geom, b->mol, b->host_boxes[i]);
+    camr_status cs = fill_box(tasks[i], *geom, b->mol, !fluxes_only, b->host_boxes[i]);
     if (cs != CAMR_OK) {
       delete b;
       return cs;
@@ -195,6 +201,26 @@ camr_status camr_batch_create(int nbox, const camr_box_task* tasks, const camr_g
   return CAMR_OK;
 }
 
+}  // namespace
+
+namespace camr {
+
+camr_status batch_create_fluxes(int nbox, const camr_box_task* tasks, const camr_geom* geom,
+                                const camr_hydro_params* p, cudaStream_t st, camr_batch** out) {
+  return batch_create_impl(nbox, tasks, geom, p, st, true, out);
+}
+
+const Work& batch_work(const camr_batch* b, int box) { return b->host_boxes[box].w; }
+
+}  // namespace camr
+
+extern "C" {
+
+camr_status camr_batch_create(int nbox, const camr_box_task* tasks, const camr_geom* geom,
+                              const camr_hydro_params* p, void* stream, camr_batch** out) {
+  return batch_create_impl(nbox, tasks, geom, p, stream, false, out);
+}
+
 camr_status camr_batch_destroy(camr_batch* b) {
   if (!b) return CAMR_ERR_INVALID;
   for (int s = 0; s < BS_COUNT; ++s)
@@ -227,11 +253,11 @@ camr_status camr_batch_run(camr_batch* b, double dt, const double* dt_dev, int m
       L.dsdt = c.dsdt;
       L.dt = dtr;
       L.err = nullptr;
-      e = launch_hydro(L, c.w, st);
+      e = b->fluxes_only ? launch_hydro_fluxes(L, c.w, st) : launch_hydro(L, c.w, st);
     }
   } else {
     const int* order = b->mol ? kOrderMol : kOrderCtu;
-    const int n = b->mol ? 5 : 7;
+    const int n = (b->mol ? 5 : 7) - (b->fluxes_only ? 1 : 0);
     for (int s = 0; s < n && e == cudaSuccess; ++s) {
       const int stage = order[s];
       e = run_stage(b, stage, b->chunk_ix[stage], b->grid[stage], dtr, st);

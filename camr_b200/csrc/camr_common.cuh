@@ -172,5 +172,11 @@ __device__ __forceinline__ void report_error(DevError* e, int code, int i, int j
 }
 
 void count_launch(int n = 1);
+int64_t launches_now();        // kernels issued so far (camr_launch_count)
+void launches_sub(int64_t n);  // take back launches counted during a capture
+// CAMR_OK, or CAMR_ERR_CUDA with the CUDA error text kept for
+// camr_last_error_string.
+camr_status cuda_status_of(cudaError_t e);
+const char* last_error_text();
 
 }  // namespace camr

@@ -110,6 +110,13 @@ const void* batched_kernel(int stage);
 int batched_min_blocks(int stage);
 constexpr int kBatchBlock = 128;
 
+// A batch plan whose stages stop at the face fluxes (flx and the interface
+// p, u_n of each box's Work): the caller forms the update itself.  The
+// tasks' dsdt fabs are not used.  Run with camr_batch_run.
+camr_status batch_create_fluxes(int nbox, const camr_box_task* tasks, const camr_geom* geom,
+                                const camr_hydro_params* p, cudaStream_t st, camr_batch** out);
+const Work& batch_work(const camr_batch* b, int box);
+
 // Issue the whole per-box hydro on `stream` (7 or 5 kernel launches).
 cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t stream);
 

@@ -20,573 +20,25 @@
 #include <new>
 #include <vector>
 
-#include "hydro_kernels.cuh"
+#include "level_point.cuh"
 
 namespace camr {
 
-static std::atomic<int64_t> g_launches{0};
+std::atomic<int64_t> g_launches{0};
 void count_launch(int n) { g_launches += n; }
+int64_t launches_now() { return g_launches.load(); }
 
-namespace {
+static thread_local char g_last_error[256] = "";
 
-constexpr int kBlk = 256;
-inline unsigned grid_of(int64_t n) { return unsigned((n + kBlk - 1) / kBlk); }
-__device__ __forceinline__ int64_t tid() { return int64_t(blockIdx.x) * blockDim.x + threadIdx.x; }
-
-// Per-level constants of the state arrays (padded domain, NVAR comps).
-struct LGeom {
-  int dlo[3], dhi[3];       // domain
-  int plo[3];               // padded lo = dlo - NGROW
-  int pn[3];                // padded extent
-  int64_t sy, sz, sn;
-  int periodic[3];
-  int bclo[3], bchi[3];
-  int boxsz[3];             // enforce_min_density window (box size)
-  double dx[3];
-  __host__ __device__ int64_t idx(int i, int j, int k) const {
-    return (i - plo[0]) + (j - plo[1]) * sy + (k - plo[2]) * sz;
-  }
-};
-
-struct LevelState {
-  double* S;       // state (valid cells meaningful)
-  double* S_old;
-  double* B;       // Sborder
-  double* B2;      // MOL stage-2 Sborder
-  double* flx[3];  // face fluxes of the domain box (NVAR comps, Space-indexed)
-  double* work;
-  Work w;
-  double* dt_cur;          // device: dt of the step being taken
-  double* dt_hist;         // device: dt of every step
-  unsigned long long* dtmin_bits;  // device: running CFL min
-  int* nstep;              // device: steps taken
-  DevError* err;
-};
-
-// BC kind of component n in direction dir for physical BC word phys
-// (Source/Utils/CAMR_setup.cpp:19-21): 1 ext_dir, 2 foextrap,
-// 3 reflect_even, 4 reflect_odd.
-__device__ __forceinline__ int bc_kind(int n, int dir, int phys) {
-  const int scalar_bc[6] = {0, 1, 2, 3, 3, 3};
-  const int norm_vel_bc[6] = {0, 1, 2, 4, 4, 4};
-  const int tang_vel_bc[6] = {0, 1, 2, 3, 3, 4};
-  if (n >= UMX && n <= UMZ) return (n - UMX == dir) ? norm_vel_bc[phys] : tang_vel_bc[phys];
-  return scalar_bc[phys];
+camr_status cuda_status_of(cudaError_t e) {
+  if (e == cudaSuccess) return CAMR_OK;
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s", cudaGetErrorName(e),
+                cudaGetErrorString(e));
+  return CAMR_ERR_CUDA;
 }
+const char* last_error_text() { return g_last_error; }
+void launches_sub(int64_t n) { g_launches -= n; }
 
-// computeTemp body: reset_internal_energy (Source/Utils/CAMR_reset_internal_e.H:13-129)
-// then T (Source/CAMR.cpp:1166-1183).
-__device__ __forceinline__ void compute_temp(double* s, const KParams& P) {
-  const double rho = s[URHO];
-  const double rhoInv = 1.0 / rho;
-  const double Up = s[UMX] * rhoInv;
-  const double Vp = s[UMY] * rhoInv;
-  const double Wp = s[UMZ] * rhoInv;
-  const double ke = 0.5 * (Up * Up + Vp * Vp + Wp * Wp);
-  const double eden = s[UEDEN] * rhoInv;
-  double massfrac[NSPEC];
-#pragma unroll
-  for (int sp = 0; sp < NSPEC; ++sp) massfrac[sp] = s[sp + UFS] * rhoInv;
-  double e_out = 0.;
-  double small_e = 0.;
-  const double small_T = P.small_temp;
-  if (P.allow_small_energy == 0) {
-    small_e = eos_rty2e(P.gamma, small_T, massfrac);
-    if (eden < small_e) {
-      if (s[UEINT] * rhoInv < small_e) {
-        const double T = dmax(s[UTEMP], small_T);
-        e_out = eos_rty2e(P.gamma, T, massfrac);
-        s[UEINT] = rho * e_out;
-      }
-      s[UEDEN] = s[UEINT] + rho * ke;
-    } else {
-      const double rho_eint = s[UEDEN] - s[URHO] * ke;
-      if (rho_eint > 0. && rho_eint / s[UEDEN] > P.dual_energy_eta2) s[UEINT] = rho_eint;
-      if (s[UEINT] * rhoInv < small_e) {
-        const double T = dmax(s[UTEMP], small_T);
-        e_out = eos_rty2e(P.gamma, T, massfrac);
-        if (P.dual_energy_update_E_from_e == 1) s[UEDEN] += (rho * e_out - s[UEINT]);
-        s[UEINT] = s[URHO] * e_out;
-      }
-    }
-  } else if (P.allow_negative_energy == 0) {
-    if (s[UEDEN] < 0.) {
-      if (s[UEINT] < 0.) {
-        e_out = eos_rty2e(P.gamma, small_T, massfrac);
-        s[UEINT] = rho * e_out;
-      }
-      s[UEDEN] = s[UEINT] + rho * ke;
-    } else {
-      const double rho_eint = s[UEDEN] - rho * ke;
-      if (rho_eint > 0. && rho_eint / s[UEDEN] > P.dual_energy_eta2) {
-        s[UEINT] = rho_eint;
-      } else if (s[UEINT] > 0 && P.dual_energy_update_E_from_e == 1) {
-        s[UEDEN] = s[UEINT] + rho * ke;
-      } else if (s[UEINT] <= 0.) {
-        e_out = eos_rty2e(P.gamma, small_T, massfrac);
-        s[UEINT] = rho * e_out;
-        if (P.dual_energy_update_E_from_e == 1) s[UEDEN] += (rho * e_out - s[UEINT]);
-      }
-    }
-  } else {
-    s[UEINT] = s[UEDEN] - rho * ke;
-  }
-  const double rhoInv2 = 1.0 / s[URHO];
-  const double e = s[UEINT] * rhoInv2;
-  s[UTEMP] = eos_ey2t(P.gamma, e);
-}
-
-// normalize_species (Source/CAMR.cpp:884-905).
-__device__ __forceinline__ void normalize_species(double* s) {
-  double sum = 0.;
-#pragma unroll
-  for (int sp = 0; sp < NSPEC; ++sp) {
-    s[UFS + sp] = dmax(dmin(s[URHO], s[UFS + sp]), 0.0);
-    sum += s[UFS + sp];
-  }
-  if (s[URHO] > 0.) {
-    sum /= s[URHO];
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) s[UFS + sp] /= sum;
-  }
-}
-
-__device__ __forceinline__ void load_cell(const double* a, const LGeom& L, int64_t at, double* s) {
-#pragma unroll
-  for (int n = 0; n < NVAR; ++n) s[n] = a[at + n * L.sn];
-}
-__device__ __forceinline__ void store_cell(double* a, const LGeom& L, int64_t at, const double* s) {
-#pragma unroll
-  for (int n = 0; n < NVAR; ++n) a[at + n * L.sn] = s[n];
-}
-
-// enforce_min_density (Source/CAMR.cpp:941-1045) of the valid cell (i,j,k)
-// reading neighbours from `src` (the array being cleaned, before cleaning),
-// within the level box that contains the cell.
-__device__ void enforce_min_density(double* s, const double* src, const LGeom& L,
-                                    const KParams& P, int i, int j, int k, DevError* err) {
-  if (s[URHO] == 0.) {
-    report_error(err, 3, i, j, k);
-    return;
-  }
-  if (!(s[URHO] < P.small_dens)) return;
-  int blo[3], bhi[3];
-  const int c[3] = {i, j, k};
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int b = (c[d] - L.dlo[d]) / L.boxsz[d];
-    blo[d] = L.dlo[d] + b * L.boxsz[d];
-    bhi[d] = min(blo[d] + L.boxsz[d] - 1, L.dhi[d]);
-  }
-  double max_dens = s[URHO];
-  int is = i, js = j, ks = k;
-  for (int kk = -1; kk <= 1; kk++)
-    for (int jj = -1; jj <= 1; jj++)
-      for (int ii = -1; ii <= 1; ii++) {
-        if (i + ii >= blo[0] && j + jj >= blo[1] && k + kk >= blo[2] && i + ii <= bhi[0] &&
-            j + jj <= bhi[1] && k + kk <= bhi[2]) {
-          const double r = src[L.idx(i + ii, j + jj, k + kk)];
-          if (r > max_dens) {
-            is = i + ii; js = j + jj; ks = k + kk;
-            max_dens = r;
-          }
-        }
-      }
-  if (max_dens < P.small_dens) {
-    double massfrac[NSPEC];
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) massfrac[sp] = s[UFS + sp] / s[URHO];
-    const double small_e = eos_rty2e(P.gamma, P.small_temp, massfrac);
-    s[URHO] = P.small_dens;
-    s[UTEMP] = P.small_temp;
-    s[UMX] = 0.;
-    s[UMY] = 0.;
-    s[UMZ] = 0.;
-    s[UEINT] = P.small_dens * small_e;
-    s[UEDEN] = s[UEINT];
-  } else {
-    load_cell(src, L, L.idx(is, js, ks), s);
-  }
-}
-
-__device__ __forceinline__ bool padded_cell(const LGeom& L, int64_t t, int& i, int& j, int& k) {
-  const int64_t n = int64_t(L.pn[0]) * L.pn[1] * L.pn[2];
-  if (t >= n) return false;
-  const int64_t nxy = int64_t(L.pn[0]) * L.pn[1];
-  k = int(t / nxy);
-  const int64_t r = t - int64_t(k) * nxy;
-  j = int(r / L.pn[0]);
-  i = int(r - int64_t(j) * L.pn[0]);
-  i += L.plo[0];
-  j += L.plo[1];
-  k += L.plo[2];
-  return true;
-}
-
-__device__ __forceinline__ bool valid_cell(const LGeom& L, int64_t t, int& i, int& j, int& k) {
-  const int n0 = L.dhi[0] - L.dlo[0] + 1, n1 = L.dhi[1] - L.dlo[1] + 1,
-            n2 = L.dhi[2] - L.dlo[2] + 1;
-  if (t >= int64_t(n0) * n1 * n2) return false;
-  const int64_t nxy = int64_t(n0) * n1;
-  k = int(t / nxy);
-  const int64_t r = t - int64_t(k) * nxy;
-  j = int(r / n0);
-  i = int(r - int64_t(j) * n0);
-  i += L.dlo[0];
-  j += L.dlo[1];
-  k += L.dlo[2];
-  return true;
-}
-
-// clean_state on valid cells: S_old = clean(S)  (CAMR_advance.cpp:83).
-__global__ void __launch_bounds__(kBlk) k_clean_copy(LGeom L, KParams P, const double* S,
-                                                      double* out, DevError* err) {
-  int i, j, k;
-  if (!valid_cell(L, tid(), i, j, k)) return;
-  const int64_t at = L.idx(i, j, k);
-  double s[NVAR];
-  load_cell(S, L, at, s);
-  enforce_min_density(s, S, L, P, i, j, k, err);
-  normalize_species(s);
-  compute_temp(s, P);
-  store_cell(out, L, at, s);
-}
-
-// expand_state: FillPatch(src) into B, then clean_state(B)
-// (Source/CAMR.cpp:1243-1262).  Cells inside the periodic extension of the
-// domain take the cleaned value of their periodic image (FillBoundary after
-// normalize_species); physical-boundary ghosts take the BC-mapped values of
-// src (foextrap / reflect_even / reflect_odd; ext_dir copies the boundary
-// cell as Exec/Sod's bcnormal does) and only computeTemp.
-__global__ void __launch_bounds__(kBlk) k_expand(LGeom L, KParams P, const double* src,
-                                                  double* B, DevError* err) {
-  int i, j, k;
-  if (!padded_cell(L, tid(), i, j, k)) return;
-  const int c[3] = {i, j, k};
-  int img[3];
-  bool physical = false;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    img[d] = c[d];
-    if (c[d] < L.dlo[d] || c[d] > L.dhi[d]) {
-      if (L.periodic[d]) {
-        const int len = L.dhi[d] - L.dlo[d] + 1;
-        img[d] = L.dlo[d] + (((c[d] - L.dlo[d]) % len) + len) % len;
-      } else {
-        physical = true;
-      }
-    }
-  }
-  double s[NVAR];
-  if (!physical) {
-    load_cell(src, L, L.idx(img[0], img[1], img[2]), s);
-    enforce_min_density(s, src, L, P, img[0], img[1], img[2], err);
-    normalize_species(s);
-  } else {
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) {
-      int id[3] = {img[0], img[1], img[2]};
-      bool neg = false;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        if (L.periodic[d]) continue;
-        if (id[d] < L.dlo[d]) {
-          const int t = bc_kind(n, d, L.bclo[d]);
-          if (t == 1 || t == 2) id[d] = L.dlo[d];
-          else { id[d] = 2 * L.dlo[d] - id[d] - 1; if (t == 4) neg = !neg; }
-        } else if (id[d] > L.dhi[d]) {
-          const int t = bc_kind(n, d, L.bchi[d]);
-          if (t == 1 || t == 2) id[d] = L.dhi[d];
-          else { id[d] = 2 * L.dhi[d] - id[d] + 1; if (t == 4) neg = !neg; }
-        }
-      }
-      const double v = src[L.idx(id[0], id[1], id[2]) + n * L.sn];
-      s[n] = neg ? -v : v;
-    }
-  }
-  compute_temp(s, P);
-  store_cell(B, L, L.idx(i, j, k), s);
-}
-
-// Block-wide min of positive doubles into *bits (order-preserving as u64).
-__device__ __forceinline__ void block_min_dt(double v, unsigned long long* bits) {
-  unsigned long long b = __double_as_longlong(v);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long other = __shfl_down_sync(0xffffffffu, b, o);
-    b = (other < b) ? other : b;
-  }
-  __shared__ unsigned long long warp_min[kBlk / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) warp_min[wid] = b;
-  __syncthreads();
-  if (wid == 0) {
-    b = (lane < kBlk / 32) ? warp_min[lane] : ~0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long other = __shfl_down_sync(0xffffffffu, b, o);
-      b = (other < b) ? other : b;
-    }
-    if (lane == 0) atomicMin(bits, b);
-  }
-}
-
-// CAMR_estdt_hydro body (Source/Utils/Timestep.H:34-56) of one cell.
-__device__ __forceinline__ double cell_dt(const double* s, const LGeom& L, const KParams& P) {
-  const double rho = s[URHO];
-  const double rhoInv = 1.0 / rho;
-  const double eint = s[UEINT] / rho;
-  const double pres = (P.gamma - 1.0) * rho * eint;
-  const double c = sqrt(P.gamma * pres / rho);
-  double dt = DBL_MAX;
-  const double ux = s[UMX] * rhoInv;
-  dt = dmin(dt, L.dx[0] / (c + fabs(ux)));
-  const double uy = s[UMY] * rhoInv;
-  dt = dmin(dt, L.dx[1] / (c + fabs(uy)));
-  const double uz = s[UMZ] * rhoInv;
-  dt = dmin(dt, L.dx[2] / (c + fabs(uz)));
-  return dt;
-}
-
-__global__ void __launch_bounds__(kBlk) k_est_dt(LGeom L, KParams P, const double* S,
-                                                  unsigned long long* bits) {
-  int i, j, k;
-  double v = DBL_MAX;
-  if (valid_cell(L, tid(), i, j, k)) {
-    double s[NVAR];
-    load_cell(S, L, L.idx(i, j, k), s);
-    v = cell_dt(s, L, P);
-  }
-  block_min_dt(v, bits);
-}
-
-// The end of a coarse step on one valid cell, from the state right after
-// the hydro Saxpy: clean_state, the new-source correction (+ its
-// clean_state) and post_timestep's clean_state; then the cell's CFL dt.
-__device__ __forceinline__ double finish_step(double* s, const double* sold, const KParams& P,
-                                              const LGeom& L, double dt, int i, int j, int k,
-                                              DevError* err) {
-  // clean_state(S_new): enforce_min_density cannot see the other cells'
-  // post-Saxpy values inside this fused pass; a density below the floor is
-  // reported instead of reset.
-  if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
-  normalize_species(s);
-  compute_temp(s, P);
-  if (P.add_grav_src) {
-    double src[NVAR];
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
-    src[UMZ] = 0.5 * P.const_grav * (s[URHO] - sold[URHO]);
-    src[UEDEN] = 0.5 * P.const_grav * (s[UMZ] - sold[UMZ]);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-    if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
-    normalize_species(s);
-    compute_temp(s, P);
-  }
-  if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
-  normalize_species(s);
-  compute_temp(s, P);
-  return cell_dt(s, L, P);
-}
-
-// hydro_update of one cell (Hydro_utils_K.H:239-257): returns dSdt.
-__device__ __forceinline__ void cell_dsdt(const LGeom& L, const Space& sp, int i, int j, int k,
-                                          double* const* flx, double* const* qf, double* hs) {
-  const double a0 = L.dx[1] * L.dx[2], a1 = L.dx[0] * L.dx[2], a2 = L.dx[0] * L.dx[1];
-  const double vol = L.dx[0] * L.dx[1] * L.dx[2];
-  const int64_t at = sp.idx(i, j, k);
-  const int64_t sn = sp.sn;
-  const double* q1 = qf[0];
-  const double* q2 = qf[1];
-  const double* q3 = qf[2];
-  const double pdivu =
-      0.5 *
-      ((q1[at + 1] + q1[at]) * (q1[at + 1 + sn] * a0 - q1[at + sn] * a0) +
-       (q2[at + sp.sy] + q2[at]) * (q2[at + sp.sy + sn] * a1 - q2[at + sn] * a1) +
-       (q3[at + sp.sz] + q3[at]) * (q3[at + sp.sz + sn] * a2 - q3[at + sn] * a2)) /
-      vol;
-  const double volinv = 1.0 / vol;
-  const double* fx = flx[0];
-  const double* fy = flx[1];
-  const double* fz = flx[2];
-#pragma unroll
-  for (int n = 0; n < NVAR; ++n) {
-    const int64_t o = at + n * sn;
-    // construct_hydro_source zeroes src_to_fill first (:14): 0 + update.
-    hs[n] = 0.0 + (fx[o] - fx[o + 1] + fy[o] - fy[o + sp.sy] + fz[o] - fz[o + sp.sz]) * volinv;
-  }
-  hs[UEINT] -= pdivu;
-}
-
-struct FluxPtrs {
-  double* f[3];
-  double* q[3];
-};
-
-// CTU: S_new = Sborder (+ dt*src_old) + dt*dSdt, then finish_step.
-__global__ void __launch_bounds__(kBlk) k_update_ctu(LGeom L, Space sp, KParams P,
-                                                      const double* dtp, const double* B,
-                                                      const double* S_old, FluxPtrs fp,
-                                                      double* S, unsigned long long* bits,
-                                                      DevError* err) {
-  int i, j, k;
-  double v = DBL_MAX;
-  if (valid_cell(L, tid(), i, j, k)) {
-    const double dt = *dtp;
-    const int64_t at = L.idx(i, j, k);
-    double s[NVAR], sold[NVAR], hs[NVAR];
-    load_cell(B, L, at, s);
-    load_cell(S_old, L, at, sold);
-    if (P.add_grav_src) {
-      double src[NVAR];
-#pragma unroll
-      for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
-      src[UMZ] = P.const_grav * sold[URHO];
-      src[UEDEN] = P.const_grav * sold[UMZ];
-#pragma unroll
-      for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-    }
-    cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += dt * hs[n];
-    v = finish_step(s, sold, P, L, dt, i, j, k, err);
-    store_cell(S, L, at, s);
-  }
-  block_min_dt(v, bits);
-}
-
-// MOL stage 1: S_new = Sborder (+ dt*src_old) + dt*k1 (not cleaned).
-__global__ void __launch_bounds__(kBlk) k_update_mol1(LGeom L, Space sp, KParams P,
-                                                       const double* dtp, const double* B,
-                                                       const double* S_old, FluxPtrs fp,
-                                                       double* S) {
-  int i, j, k;
-  if (!valid_cell(L, tid(), i, j, k)) return;
-  const double dt = *dtp;
-  const int64_t at = L.idx(i, j, k);
-  double s[NVAR], hs[NVAR];
-  load_cell(B, L, at, s);
-  if (P.add_grav_src) {
-    double src[NVAR];
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
-    src[UMZ] = P.const_grav * S_old[at + URHO * L.sn];
-    src[UEDEN] = P.const_grav * S_old[at + UMZ * L.sn];
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-  }
-  cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-  for (int n = 0; n < NVAR; ++n) s[n] += dt * hs[n];
-  store_cell(S, L, at, s);
-}
-
-// MOL stage 2: S_new = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2 (LinComb then
-// Saxpy, CAMR_advance.cpp:134-135), then finish_step.
-__global__ void __launch_bounds__(kBlk) k_update_mol2(LGeom L, Space sp, KParams P,
-                                                       const double* dtp, const double* B2,
-                                                       const double* S_old, FluxPtrs fp,
-                                                       double* S, unsigned long long* bits,
-                                                       DevError* err) {
-  int i, j, k;
-  double v = DBL_MAX;
-  if (valid_cell(L, tid(), i, j, k)) {
-    const double dt = *dtp;
-    const int64_t at = L.idx(i, j, k);
-    double s[NVAR], sold[NVAR], b[NVAR], hs[NVAR];
-    load_cell(B2, L, at, b);
-    load_cell(S_old, L, at, sold);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
-    cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * hs[n];
-    v = finish_step(s, sold, P, L, dt, i, j, k, err);
-    store_cell(S, L, at, s);
-  }
-  block_min_dt(v, bits);
-}
-
-struct DtCtl {
-  double cfl, max_dt, fixed_dt, initial_dt, init_shrink, change_max;
-};
-
-// estTimeStep's tail + computeInitialDt / computeNewDt for one level
-// (Source/CAMR.cpp:490-635), on one thread; resets the CFL accumulator.
-__global__ void k_dt_next(DtCtl c, int first, const double* fixed, unsigned long long* bits,
-                          double* dt_cur, double* hist, int* nstep, int hist_cap) {
-  double est;
-  if (c.fixed_dt > 0.0) {
-    est = c.fixed_dt;
-  } else {
-    double estdt = c.max_dt;
-    const double max_dt_over_cfl = c.max_dt / c.cfl;
-    double estdt_hydro = max_dt_over_cfl;
-    const double dtc = __longlong_as_double((long long)*bits);
-    estdt_hydro = dmin(estdt_hydro, dtc);
-    estdt_hydro *= c.cfl;
-    if (estdt_hydro < estdt) estdt = estdt_hydro;
-    est = estdt;
-  }
-  double dt;
-  if (fixed) {
-    dt = *fixed;
-  } else if (first) {
-    double init_dt = (c.initial_dt > 0.0) ? c.initial_dt : c.init_shrink * est;
-    double dt_0 = DBL_MAX;
-    dt_0 = dmin(dt_0, 1 * init_dt);
-    dt = dt_0 / 1;
-  } else {
-    double dt_min = est;
-    if (c.fixed_dt <= 0.0) dt_min = dmin(dt_min, c.change_max * *dt_cur);
-    double dt_0 = DBL_MAX;
-    dt_0 = dmin(dt_0, 1 * dt_min);
-    dt = dt_0 / 1;
-  }
-  *dt_cur = dt;
-  const int n = *nstep;
-  if (n < hist_cap) hist[n] = dt;
-  *nstep = n + 1;
-  *bits = (unsigned long long)__double_as_longlong(DBL_MAX);
-}
-
-__global__ void k_reset_bits(unsigned long long* bits) {
-  *bits = (unsigned long long)__double_as_longlong(DBL_MAX);
-}
-
-// enforce_consistent_e (Source/CAMR.cpp:910-939) then computeTemp.
-__global__ void __launch_bounds__(kBlk) k_init_finalize(LGeom L, KParams P, double* S) {
-  int i, j, k;
-  if (!valid_cell(L, tid(), i, j, k)) return;
-  const int64_t at = L.idx(i, j, k);
-  double s[NVAR];
-  load_cell(S, L, at, s);
-  const double rhoInv = 1.0 / s[URHO];
-  const double u = s[UMX] * rhoInv;
-  const double v = s[UMY] * rhoInv;
-  const double w = s[UMZ] * rhoInv;
-  s[UEDEN] = s[UEINT] + 0.5 * s[URHO] * (u * u + v * v + w * w);
-  compute_temp(s, P);
-  store_cell(S, L, at, s);
-}
-
-// Copy between a packed (NVAR, nz, ny, nx) array and the padded state.
-__global__ void __launch_bounds__(kBlk) k_pack(LGeom L, const double* padded, double* packed,
-                                                int to_packed) {
-  int i, j, k;
-  const int64_t t = tid();
-  if (!valid_cell(L, t, i, j, k)) return;
-  const int64_t nc = int64_t(L.dhi[0] - L.dlo[0] + 1) * (L.dhi[1] - L.dlo[1] + 1) *
-                     (L.dhi[2] - L.dlo[2] + 1);
-  const int64_t at = L.idx(i, j, k);
-  for (int n = 0; n < NVAR; ++n) {
-    if (to_packed) packed[t + n * nc] = padded[at + n * L.sn];
-    else const_cast<double*>(padded)[at + n * L.sn] = packed[t + n * nc];
-  }
-}
-
-}  // namespace
 }  // namespace camr
 
 using namespace camr;
@@ -611,14 +63,7 @@ struct camr_level {
 
 namespace {
 
-thread_local char g_last_error[256] = "";
-
-camr_status cuda_status(cudaError_t e) {
-  if (e == cudaSuccess) return CAMR_OK;
-  std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s", cudaGetErrorName(e),
-                cudaGetErrorString(e));
-  return CAMR_ERR_CUDA;
-}
+camr_status cuda_status(cudaError_t e) { return camr::cuda_status_of(e); }
 
 camr_status check_params(const camr_hydro_params* p) {
   if (!p) return CAMR_ERR_INVALID;
@@ -1065,7 +510,7 @@ camr_status camr_level_stream(camr_level* lev, void** stream) {
   return CAMR_OK;
 }
 
-const char* camr_last_error_string(void) { return g_last_error; }
+const char* camr_last_error_string(void) { return last_error_text(); }
 
 camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab) {
   if (!lev || !fab) return CAMR_ERR_INVALID;

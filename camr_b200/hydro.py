@@ -227,3 +227,99 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class AmrHierarchy:
+    """Two-level AMR hierarchy (ratio 2, subcycled) advanced on the GPU
+    (camr_amr_*): the base level `geom` (periodic) and fine boxes given as
+    (lo, hi) fine index triples, coarse-aligned."""
+
+    def __init__(self, geom, params, boxes, max_grid_size=(0, 0, 0), use_graph=True,
+                 stream=None):
+        desc = LevelDesc()
+        desc.geom = geom
+        for d in range(3):
+            desc.max_grid_size[d] = max_grid_size[d]
+        desc.use_graph = int(use_graph)
+        self.params = params
+        self.geom = geom
+        self.boxes = [(tuple(lo), tuple(hi)) for lo, hi in boxes]
+        self.n0 = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+        arr = np.array([list(lo) + list(hi) for lo, hi in self.boxes], dtype=np.int32)
+        self._boxes = np.ascontiguousarray(arr)
+        sp = None if stream is None else getattr(stream, "cuda_stream", stream)
+        h = C.c_void_p()
+        check(lib().camr_amr_create(C.byref(desc), len(self.boxes), self._boxes.ctypes.data,
+                                    C.byref(params), C.c_void_p(sp), C.byref(h)),
+              "camr_amr_create")
+        self._h = h
+        s = C.c_void_p()
+        check(lib().camr_amr_stream(self._h, C.byref(s)), "camr_amr_stream")
+        self.stream_ptr = s.value or 0
+        self.fine_cells = int(lib().camr_amr_fine_cells(self._h))
+
+    def torch_stream(self):
+        return _torch().cuda.ExternalStream(self.stream_ptr)
+
+    def close(self):
+        if self._h:
+            lib().camr_amr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, S0, S1):
+        """S0: (NVAR, nz, ny, nx) base state; S1: the fine boxes' states back
+        to back (flat), numpy (host) or CUDA tensors."""
+        if isinstance(S0, np.ndarray):
+            a = np.ascontiguousarray(S0, dtype=np.float64)
+            b = np.ascontiguousarray(S1, dtype=np.float64)
+            assert a.size == NVAR * self.n0[0] * self.n0[1] * self.n0[2]
+            assert b.size == NVAR * self.fine_cells
+            check(lib().camr_amr_set_state(self._h, a.ctypes.data, b.ctypes.data, 1),
+                  "camr_amr_set_state")
+            self.sync()
+        else:
+            check(lib().camr_amr_set_state(self._h, S0.data_ptr(), S1.data_ptr(), 0),
+                  "camr_amr_set_state")
+
+    def get_state(self, S0=None, S1=None):
+        if S0 is None:
+            S0 = np.empty((NVAR, self.n0[2], self.n0[1], self.n0[0]))
+            S1 = np.empty(NVAR * self.fine_cells)
+        if isinstance(S0, np.ndarray):
+            check(lib().camr_amr_get_state(self._h, S0.ctypes.data, S1.ctypes.data, 1),
+                  "camr_amr_get_state")
+        else:
+            check(lib().camr_amr_get_state(self._h, S0.data_ptr(), S1.data_ptr(), 0),
+                  "camr_amr_get_state")
+        return S0, S1
+
+    def init_finalize(self):
+        check(lib().camr_amr_init_finalize(self._h), "camr_amr_init_finalize")
+
+    def advance(self, nsteps):
+        check(lib().camr_amr_advance(self._h, int(nsteps)), "camr_amr_advance")
+
+    def clock(self):
+        c = (C.c_double * 4)()
+        check(lib().camr_amr_clock(self._h, c), "camr_amr_clock")
+        return list(c)
+
+    def autotune(self):
+        check(lib().camr_amr_autotune(self._h), "camr_amr_autotune")
+
+    def kernels_per_step(self):
+        return int(lib().camr_amr_kernels_per_step(self._h))
+
+    def error(self):
+        info = native.ErrorInfo()
+        lib().camr_amr_get_error(self._h, C.byref(info))
+        return (info.code, info.i, info.j, info.k)
+
+    def sync(self):
+        _torch().cuda.synchronize()

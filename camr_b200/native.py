@@ -105,6 +105,19 @@ SIGNATURES = {
                                     C.c_int]),
     "camr_hydro_umdrv_batched": (C.c_int, [C.c_int, C.POINTER(BoxTask), C.POINTER(Geom),
                                            C.POINTER(HydroParams), C.c_double, C.c_void_p]),
+    "camr_amr_create": (C.c_int, [C.POINTER(LevelDesc), C.c_int, C.c_void_p,
+                                  C.POINTER(HydroParams), C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_amr_destroy": (C.c_int, [C.c_void_p]),
+    "camr_amr_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_amr_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_amr_init_finalize": (C.c_int, [C.c_void_p]),
+    "camr_amr_advance": (C.c_int, [C.c_void_p, C.c_int]),
+    "camr_amr_clock": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "camr_amr_autotune": (C.c_int, [C.c_void_p]),
+    "camr_amr_fine_cells": (C.c_int64, [C.c_void_p]),
+    "camr_amr_kernels_per_step": (C.c_int64, [C.c_void_p]),
+    "camr_amr_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_amr_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
 }
 
 

@@ -252,6 +252,62 @@ camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab);
 camr_status camr_level_get_error(camr_level* lev, camr_error_info* info);
 
 /* ---------------------------------------------------------------------
+ * Two-level AMR hierarchy (refinement ratio 2, subcycled): a base level
+ * covering the domain and a fixed set of fine boxes.  Replaces, for two
+ * levels, Amr::timeStep's recursion (level 0 advance, two level-1 substeps,
+ * level 0 post_timestep) around CAMR::CAMR_advance
+ * (Source/CAMR_advance.cpp:38-164): the fine level's FillPatch from its own
+ * boxes and from the base level interpolated in time and space
+ * (conservative linear), the flux register (CrseAdd / FineAdd,
+ * Source/Hydro/CAMR_construct_hydro_source.cpp:243-254) and its reflux,
+ * avgDown and the coarse clean_state of post_timestep
+ * (Source/CAMR.cpp:679-718, :803-851, :1048-1066), and computeNewDt /
+ * computeInitialDt over both levels (:566-676).  Periodic domains; the box
+ * layout stays fixed (no regridding).
+ */
+typedef struct camr_amr camr_amr;
+
+/* base: the level-0 description (domain, max_grid_size, use_graph).
+ * boxes: nbox fine boxes, each lo0,lo1,lo2,hi0,hi1,hi2 in the fine index
+ * space; every lo even and every hi odd (whole coarse cells), inside the
+ * fine domain, not overlapping.  stream as for camr_level_create. */
+camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* boxes,
+                            const camr_hydro_params* p, void* stream, camr_amr** out);
+camr_status camr_amr_destroy(camr_amr* a);
+
+/* Copy the states in/out: S0 the base level's valid cells (NVAR, nz, ny,
+ * nx); S1 the fine boxes' valid cells, box after box, each (NVAR, nz, ny,
+ * nx).  host != 0: host pointers.  set_state resets the clock: the next
+ * step starts at time 0 with computeInitialDt. */
+camr_status camr_amr_set_state(camr_amr* a, const double* S0, const double* S1, int host);
+camr_status camr_amr_get_state(camr_amr* a, double* S0, double* S1, int host);
+
+/* CAMR::initData's epilogue on both levels, then post_init's avgDown. */
+camr_status camr_amr_init_finalize(camr_amr* a);
+
+/* Advance nsteps coarse steps (each: one base step, two fine substeps,
+ * reflux, average down).  Stream-ordered; after the first step every step
+ * replays one CUDA graph when use_graph is set. */
+camr_status camr_amr_advance(camr_amr* a, int nsteps);
+
+/* clock[0..3]: time of level 0, time of level 1, last dt of level 0, last
+ * dt of level 1 (synchronises). */
+camr_status camr_amr_clock(camr_amr* a, double clock[4]);
+
+/* Autotune the fine level's batched hydro on its current state (after at
+ * least one step); synchronises. */
+camr_status camr_amr_autotune(camr_amr* a);
+
+/* Number of fine cells (valid) and kernel launches inside one captured
+ * coarse step (0 before the first capture). */
+int64_t camr_amr_fine_cells(camr_amr* a);
+int64_t camr_amr_kernels_per_step(camr_amr* a);
+camr_status camr_amr_stream(camr_amr* a, void** stream);
+
+/* Read and clear the device error word of both levels (synchronises). */
+camr_status camr_amr_get_error(camr_amr* a, camr_error_info* info);
+
+/* ---------------------------------------------------------------------
  * Allocation-free per-box hydro.  No counterpart in the reference: it is
  * camr_hydro_umdrv for callers that may not allocate device memory while
  * they run (code inside an arena or pool that owns all device memory,
