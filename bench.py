@@ -295,9 +295,11 @@ def run_camr(args, world, rank, local, pg):
                          "reference hydro kernels, tiles 1024x16x16, all host threads"}
 
     batched = None
+    amr = None
     if rank == 0 and world == 1 and not args.no_batched:
         L.close()
         batched = batched_comparison(args)
+        amr = amr_comparison(args)
 
     if rank == 0:
         line = {
@@ -314,6 +316,7 @@ def run_camr(args, world, rank, local, pg):
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "stages_ms": acc, "device_error": list(err),
             "batched_amr_patches": batched,
+            "amr_two_level": amr,
         }
         print(json.dumps(line))
     L.close()
@@ -405,6 +408,62 @@ def batched_comparison(args, steps=5, warmup=2):
     b.close()
     del items
     torch.cuda.empty_cache()
+    return out
+
+
+def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
+    """The two-level configuration end to end on the device: base 256^3 +
+    the uneven fine boxes (ratio 2, two subcycled fine steps per coarse
+    step, flux-register reflux, average down).  Zone-updates per coarse
+    step = base cells + 2 x fine cells.  The fine hydro runs as the batched
+    work-list launches inside one graph-captured step, and, for comparison,
+    as plain per-box launch sequences (no graph)."""
+    import torch
+
+    from camr_b200 import hydro, native, problems
+    n0 = (256, 256, 256)
+    fine_n = 512
+    boxes = problems.amr_box_list(nbox=args.nbox, fine_n=fine_n)
+    S0, S1 = problems.amr_initial(n0, boxes, vel=None)
+    geom = hydro.make_geom(n0)
+    out = {"base": list(n0), "boxes": len(boxes)}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    methods = (("mol_plm", dict(do_mol=1, ppm_type=0, cfl=0.3), True),
+               ("ctu_ppm", dict(do_mol=0, ppm_type=1, cfl=CFL), False))
+    for name, kw, compare in methods:
+        h = hydro.AmrHierarchy(geom, native.default_params(**kw), boxes,
+                               max_grid_size=(64, 64, 64))
+        st = h.torch_stream()
+        zones = n0[0] * n0[1] * n0[2] + 2 * h.fine_cells
+        h.set_state(S0, S1)
+        h.init_finalize()
+        h.advance(1)
+        h.autotune()
+        h.advance(warmup)
+        torch.cuda.synchronize()
+        res = {"fine_cells": h.fine_cells, "zone_updates_per_step": zones}
+        modes = [("batched_graph", h.PERSISTENT, steps)]
+        if compare:
+            modes.append(("per_box", h.PER_BOX, per_box_steps))
+        for mname, mode, k in modes:
+            h.set_fine_mode(mode)
+            h.advance(1)
+            torch.cuda.synchronize()
+            e0.record(st)
+            h.advance(k)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / k
+            res[mname] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3)}
+        res["kernels_per_step_graph"] = h.kernels_per_step()
+        res["device_error"] = list(h.error())
+        if compare:
+            res["speedup_batched_graph_vs_per_box"] = (res["per_box"]["ms_per_step"] /
+                                                       res["batched_graph"]["ms_per_step"])
+        out[name] = res
+        h.close()
+        torch.cuda.empty_cache()
     return out
 
 

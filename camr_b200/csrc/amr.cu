@@ -628,6 +628,7 @@ struct camr_amr {
   unsigned long long *bits0 = nullptr, *bits1 = nullptr;
   DevError* err = nullptr;
   double *staging0 = nullptr, *staging1 = nullptr;
+  int fine_mode = CAMR_BATCH_PERSISTENT;
   int steps_taken = 0;
   bool graph_ready = false;
   cudaGraphExec_t graph;
@@ -782,7 +783,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first) {
     kf_expand<<<gf_grown, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[0],
                                          a->S1_old, a->B1, fdlo, fdn, a->err);
     count_launch(3);
-    camr_status cs = camr_batch_run(a->plan, 0.0, dt1, CAMR_BATCH_PERSISTENT, st);
+    camr_status cs = camr_batch_run(a->plan, 0.0, dt1, a->fine_mode, st);
     if (cs != CAMR_OK) return cudaErrorLaunchFailure;
     k_fine_add<<<gb, kBlk, 0, st>>>(R, F, FP, dt1, fac, volf8);
     count_launch();
@@ -796,7 +797,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first) {
       kf_expand<<<gf_grown, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[1],
                                            a->S1, a->B1, fdlo, fdn, a->err);
       count_launch(2);
-      cs = camr_batch_run(a->plan, 0.0, dt1, CAMR_BATCH_PERSISTENT, st);
+      cs = camr_batch_run(a->plan, 0.0, dt1, a->fine_mode, st);
       if (cs != CAMR_OK) return cudaErrorLaunchFailure;
       k_fine_add<<<gb, kBlk, 0, st>>>(R, F, FP, dt1, fac, volf8);
       kf_update_mol2<<<gf_valid, kBlk, 0, st>>>(F, FP, P, dt1, a->B1, a->S1_old, a->S1, fbits,
@@ -1157,7 +1158,7 @@ camr_status camr_amr_advance(camr_amr* a, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     const bool first = a->steps_taken == 0;
     cudaError_t e;
-    if (!first && a->desc.use_graph) {
+    if (!first && a->desc.use_graph && a->fine_mode == CAMR_BATCH_PERSISTENT) {
       if (!a->graph_ready) {
         cudaGraph_t gr;
         e = cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal);
@@ -1210,6 +1211,12 @@ camr_status camr_amr_autotune(camr_amr* a) {
     a->graph_ready = false;
   }
   return camr_batch_autotune(a->plan, h.dt1, a->stream);
+}
+
+camr_status camr_amr_set_fine_mode(camr_amr* a, int mode) {
+  if (!a || (mode != CAMR_BATCH_PERSISTENT && mode != CAMR_BATCH_PER_BOX)) return CAMR_ERR_INVALID;
+  a->fine_mode = mode;
+  return CAMR_OK;
 }
 
 int64_t camr_amr_fine_cells(camr_amr* a) { return a ? a->ncell1 : 0; }

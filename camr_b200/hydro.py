@@ -313,6 +313,12 @@ class AmrHierarchy:
     def autotune(self):
         check(lib().camr_amr_autotune(self._h), "camr_amr_autotune")
 
+    PERSISTENT = 0
+    PER_BOX = 1
+
+    def set_fine_mode(self, mode):
+        check(lib().camr_amr_set_fine_mode(self._h, int(mode)), "camr_amr_set_fine_mode")
+
     def kernels_per_step(self):
         return int(lib().camr_amr_kernels_per_step(self._h))
 

@@ -114,6 +114,7 @@ SIGNATURES = {
     "camr_amr_advance": (C.c_int, [C.c_void_p, C.c_int]),
     "camr_amr_clock": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "camr_amr_autotune": (C.c_int, [C.c_void_p]),
+    "camr_amr_set_fine_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "camr_amr_fine_cells": (C.c_int64, [C.c_void_p]),
     "camr_amr_kernels_per_step": (C.c_int64, [C.c_void_p]),
     "camr_amr_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),

@@ -298,6 +298,12 @@ camr_status camr_amr_clock(camr_amr* a, double clock[4]);
  * least one step); synchronises. */
 camr_status camr_amr_autotune(camr_amr* a);
 
+/* How the fine level's hydro is issued: CAMR_BATCH_PERSISTENT (default:
+ * one work-list launch per stage for all boxes, the step graph-captured) or
+ * CAMR_BATCH_PER_BOX (the plain per-box launch sequences, box by box, as
+ * the reference's MFIter loop issues them; no graph).  Same results. */
+camr_status camr_amr_set_fine_mode(camr_amr* a, int mode);
+
 /* Number of fine cells (valid) and kernel launches inside one captured
  * coarse step (0 before the first capture). */
 int64_t camr_amr_fine_cells(camr_amr* a);

@@ -80,13 +80,23 @@ def test_amr_gpu_matches_oracle(method, oracle_kind):
     assert_bitwise(g1, o1, "level 1")
 
 
-def test_amr_gpu_graph_equals_eager():
+def test_amr_gpu_graph_equals_eager_and_per_box():
     _torch()
     S0, S1 = P.amr_initial(N0, BOXES, nblobs=4, r_min=0.1, r_max=0.2)
     a = gpu_run("ctu_ppm", N0, BOXES, 3, S0, S1, use_graph=True)
     b = gpu_run("ctu_ppm", N0, BOXES, 3, S0, S1, use_graph=False)
     for x, y, w in zip(a, b, ("level 0", "level 1", "clock")):
         assert_bitwise(x, y, w)
+    geom = hydro.make_geom(N0)
+    h = hydro.AmrHierarchy(geom, native.default_params(**METHODS["ctu_ppm"]), BOXES)
+    h.set_fine_mode(h.PER_BOX)
+    h.set_state(S0, S1)
+    h.init_finalize()
+    h.advance(3)
+    c0, c1 = h.get_state()
+    h.close()
+    assert_bitwise(c0, a[0], "level 0 (per-box fine hydro)")
+    assert_bitwise(c1, a[1], "level 1 (per-box fine hydro)")
 
 
 def test_amr_gpu_larger_matches_oracle_and_conserves(oracle_kind):
