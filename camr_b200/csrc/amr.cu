@@ -116,50 +116,6 @@ __device__ __forceinline__ double coarse_at(const LGeom& Lc, const double* c_old
   return ct.alpha * c_old[at] + ct.beta * c_new[at];
 }
 
-// AMReX CellConservativeLinear (ratio 2, with limiting) of component n at
-// fine cell (fi,fj,fk): per-direction MC-limited slopes, one factor alpha
-// keeping the fine children inside the min/max of the 27 coarse
-// neighbours, fine = u + ox*sx + oy*sy + oz*sz with o = -+1/4.
-__device__ double cons_interp(const LGeom& Lc, const double* c_old, const double* c_new,
-                              const CoarseT& ct, int fi, int fj, int fk, int n) {
-  const int f[3] = {fi, fj, fk};
-  int c[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) c[d] = floordiv2(f[d]);
-  const double uc = coarse_at(Lc, c_old, c_new, ct, c[0], c[1], c[2], n);
-  double sl[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int ex = d == 0, ey = d == 1, ez = d == 2;
-    const double up = coarse_at(Lc, c_old, c_new, ct, c[0] + ex, c[1] + ey, c[2] + ez, n);
-    const double um = coarse_at(Lc, c_old, c_new, ct, c[0] - ex, c[1] - ey, c[2] - ez, n);
-    const double dc = 0.5 * (up - um);
-    const double df = 2.0 * (up - uc);
-    const double db = 2.0 * (uc - um);
-    double sv = (df * db >= 0.0) ? dmin(fabs(df), fabs(db)) : 0.0;
-    sv = copysign(1.0, dc) * dmin(sv, fabs(dc));
-    sl[d] = sv;
-  }
-  double alpha = 1.0;
-  if (sl[0] != 0.0 || sl[1] != 0.0 || sl[2] != 0.0) {
-    const double dumax = fabs(sl[0]) * 0.25 + fabs(sl[1]) * 0.25 + fabs(sl[2]) * 0.25;
-    double umax = uc, umin = uc;
-    for (int dk = -1; dk <= 1; ++dk)
-      for (int dj = -1; dj <= 1; ++dj)
-        for (int di = -1; di <= 1; ++di) {
-          const double v = coarse_at(Lc, c_old, c_new, ct, c[0] + di, c[1] + dj, c[2] + dk, n);
-          umax = dmax(umax, v);
-          umin = dmin(umin, v);
-        }
-    if (dumax * alpha > (umax - uc)) alpha = (umax - uc) / dumax;
-    if (dumax * alpha > (uc - umin)) alpha = (uc - umin) / dumax;
-  }
-  double off[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) off[d] = (f[d] - RR * c[d] == 0) ? -0.25 : 0.25;
-  return uc + off[0] * (sl[0] * alpha) + off[1] * (sl[1] * alpha) + off[2] * (sl[2] * alpha);
-}
-
 #define FINE_VALID_PROLOGUE                                          \
   const int b = box_of_block(F.vb0, F.nbox, blockIdx.x);             \
   const LGeom& L = F.L[b];                                           \
@@ -213,17 +169,14 @@ __global__ void __launch_bounds__(kBlk) kf_est_dt(FineDev F, KParams P, const do
   block_min_dt(v, bits);
 }
 
-// expand_state on the fine level: FillPatchTwoLevels(src, t) then
-// clean_state, one pass over every box's grown cells.  Valid cells and
-// ghost cells that a fine box covers (through the periodic domain) take the
-// cleaned value of that box's cell (enforce_min_density + normalize_species,
-// then FillBoundary); the other ghost cells take the coarse data at time t
-// interpolated conservatively; computeTemp on all.
-__global__ void __launch_bounds__(kBlk) kf_expand(FineDev F, KParams P, CoarseMap CM, LGeom Lc,
-                                                   const double* c_old, const double* c_new,
-                                                   const CoarseT* ctp, const double* src,
-                                                   double* B, int3 fdlo, int3 fdn,
-                                                   DevError* err) {
+// expand_state on the fine level, part 1: valid cells and the ghost cells
+// that a fine box covers (through the periodic domain) take the cleaned
+// value of that box's cell (enforce_min_density + normalize_species, then
+// FillBoundary), then computeTemp.  The coarse-fine ghost cells are left to
+// kf_interp.
+__global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap CM,
+                                                 const double* src, double* B, int3 fdlo,
+                                                 int3 fdn, DevError* err) {
   const int b = box_of_block(F.gb0, F.nbox, blockIdx.x);
   const LGeom& L = F.L[b];
   const int64_t t = (int64_t(blockIdx.x) - F.gb0[b]) * kBlk + threadIdx.x;
@@ -236,25 +189,111 @@ __global__ void __launch_bounds__(kBlk) kf_expand(FineDev F, KParams P, CoarseMa
     const double* sb = src + F.off[b];
     load_cell(sb, L, L.idx(i, j, k), s);
     enforce_min_density(s, sb, L, P, i, j, k, err);
-    normalize_species(s);
   } else {
     const int wi = wrapi(i, fdlo.x, fdn.x), wj = wrapi(j, fdlo.y, fdn.y),
               wk = wrapi(k, fdlo.z, fdn.z);
     const int ob = CM.cmap[CM.cell(floordiv2(wi), floordiv2(wj), floordiv2(wk))];
-    if (ob >= 0) {
-      const LGeom& Lo = F.L[ob];
-      const double* so = src + F.off[ob];
-      load_cell(so, Lo, Lo.idx(wi, wj, wk), s);
-      enforce_min_density(s, so, Lo, P, wi, wj, wk, err);
-      normalize_species(s);
-    } else {
-      const CoarseT ct = *ctp;
-#pragma unroll 1
-      for (int n = 0; n < NVAR; ++n) s[n] = cons_interp(Lc, c_old, c_new, ct, i, j, k, n);
-    }
+    if (ob < 0) return;
+    const LGeom& Lo = F.L[ob];
+    const double* so = src + F.off[ob];
+    load_cell(so, Lo, Lo.idx(wi, wj, wk), s);
+    enforce_min_density(s, so, Lo, P, wi, wj, wk, err);
   }
+  normalize_species(s);
   compute_temp(s, P);
   store_cell(B + F.off[b], L, L.idx(i, j, k), s);
+}
+
+// expand_state on the fine level, part 2: the ghost cells no fine box
+// covers, one thread per coarse cell of grow(coarsened box, 2) outside the
+// coarsened box and outside every fine box.  Per component the 27 coarse
+// neighbours at the fine time are gathered once; the AMReX
+// CellConservativeLinear slopes (ratio 2, with limiting) give the 8 fine
+// children: per-direction MC-limited slopes, one factor alpha keeping the
+// children inside the neighbours' min/max, child = u + ox*sx + oy*sy + oz*sz
+// with o = -+1/4.  Then computeTemp on each child.
+__global__ void __launch_bounds__(kBlk) kf_interp(FineDev F, KParams P, CoarseMap CM,
+                                                   LGeom Lc, const double* c_old,
+                                                   const double* c_new, const CoarseT* ctp,
+                                                   const int64_t* ib0, double* B) {
+  const int b = box_of_block(ib0, F.nbox, blockIdx.x);
+  const LGeom& L = F.L[b];
+  const int64_t t = (int64_t(blockIdx.x) - ib0[b]) * kBlk + threadIdx.x;
+  int clo[3], cn[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    clo[d] = floordiv2(L.dlo[d]) - 2;
+    cn[d] = floordiv2(L.dhi[d]) - floordiv2(L.dlo[d]) + 1 + 4;
+  }
+  if (t >= int64_t(cn[0]) * cn[1] * cn[2]) return;
+  const int64_t nxy = int64_t(cn[0]) * cn[1];
+  const int kk = int(t / nxy);
+  const int64_t r = t - int64_t(kk) * nxy;
+  const int jj = int(r / cn[0]);
+  const int ii = int(r - int64_t(jj) * cn[0]);
+  if (ii >= 2 && ii < cn[0] - 2 && jj >= 2 && jj < cn[1] - 2 && kk >= 2 && kk < cn[2] - 2) return;
+  const int ci = clo[0] + ii, cj = clo[1] + jj, ck = clo[2] + kk;
+  if (CM.cmap[CM.cell(ci, cj, ck)] >= 0) return;
+  const CoarseT ct = *ctp;
+  double* Bb = B + F.off[b];
+  const int64_t at0 = L.idx(RR * ci, RR * cj, RR * ck);
+  const int64_t cstep[3] = {1, L.sy, L.sz};
+  for (int n = 0; n < NVAR; ++n) {
+    double v[27];
+#pragma unroll
+    for (int dk = -1; dk <= 1; ++dk)
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+        for (int di = -1; di <= 1; ++di)
+          v[(dk + 1) * 9 + (dj + 1) * 3 + (di + 1)] =
+              coarse_at(Lc, c_old, c_new, ct, ci + di, cj + dj, ck + dk, n);
+    const double uc = v[13];
+    const double up[3] = {v[14], v[16], v[22]};
+    const double um[3] = {v[12], v[10], v[4]};
+    double sl[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double dc = 0.5 * (up[d] - um[d]);
+      const double df = 2.0 * (up[d] - uc);
+      const double db = 2.0 * (uc - um[d]);
+      double sv = (df * db >= 0.0) ? dmin(fabs(df), fabs(db)) : 0.0;
+      sv = copysign(1.0, dc) * dmin(sv, fabs(dc));
+      sl[d] = sv;
+    }
+    double alpha = 1.0;
+    if (sl[0] != 0.0 || sl[1] != 0.0 || sl[2] != 0.0) {
+      const double dumax = fabs(sl[0]) * 0.25 + fabs(sl[1]) * 0.25 + fabs(sl[2]) * 0.25;
+      double umax = uc, umin = uc;
+#pragma unroll
+      for (int q = 0; q < 27; ++q) {
+        umax = dmax(umax, v[q]);
+        umin = dmin(umin, v[q]);
+      }
+      if (dumax * alpha > (umax - uc)) alpha = (umax - uc) / dumax;
+      if (dumax * alpha > (uc - umin)) alpha = (uc - umin) / dumax;
+    }
+    const double sa[3] = {sl[0] * alpha, sl[1] * alpha, sl[2] * alpha};
+    double* Bn = Bb + at0 + int64_t(n) * L.sn;
+#pragma unroll
+    for (int kc = 0; kc < RR; ++kc)
+#pragma unroll
+      for (int jc = 0; jc < RR; ++jc)
+#pragma unroll
+        for (int ic = 0; ic < RR; ++ic) {
+          const double ox = ic ? 0.25 : -0.25, oy = jc ? 0.25 : -0.25, oz = kc ? 0.25 : -0.25;
+          Bn[ic * cstep[0] + jc * cstep[1] + kc * cstep[2]] =
+              uc + ox * sa[0] + oy * sa[1] + oz * sa[2];
+        }
+  }
+#pragma unroll 1
+  for (int q = 0; q < 8; ++q) {
+    const int64_t at = at0 + (q & 1) * cstep[0] + ((q >> 1) & 1) * cstep[1] + (q >> 2) * cstep[2];
+    double s[NVAR];
+    load_cell(Bb, L, at, s);
+    compute_temp(s, P);
+    store_cell(Bb, L, at, s);
+  }
 }
 
 struct FinePools {
@@ -609,9 +648,10 @@ struct camr_amr {
   int64_t pool = 0;  // doubles per state pool
   double *S1 = nullptr, *S1_old = nullptr, *B1 = nullptr;
   double* flx1[3] = {nullptr, nullptr, nullptr};
-  std::vector<int64_t> h_vb0, h_gb0;
+  std::vector<int64_t> h_vb0, h_gb0, h_ib0;
   LGeom* d_L = nullptr;
-  int64_t *d_off = nullptr, *d_vb0 = nullptr, *d_gb0 = nullptr, *d_poff = nullptr;
+  int64_t *d_off = nullptr, *d_vb0 = nullptr, *d_gb0 = nullptr, *d_poff = nullptr,
+          *d_ib0 = nullptr;
   double** d_qf = nullptr;
   camr_batch* plan = nullptr;
   int fdlo[3], fdn[3];
@@ -691,6 +731,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first) {
   const int64_t npad0 = int64_t(Lc.pn[0]) * Lc.pn[1] * Lc.pn[2];
   const unsigned gf_valid = unsigned(a->h_vb0[a->nbox]);
   const unsigned gf_grown = unsigned(a->h_gb0[a->nbox]);
+  const unsigned gf_interp = unsigned(a->h_ib0[a->nbox]);
   const double* dt0 = &a->clock->dt0;
   const double* dt1 = &a->clock->dt1;
   DtCtl c{a->hp.cfl, a->hp.max_dt, a->hp.fixed_dt, a->hp.initial_dt, a->hp.init_shrink,
@@ -780,9 +821,10 @@ cudaError_t amr_issue_step(camr_amr* a, bool first) {
     unsigned long long* fbits = (sc == RR - 1) ? a->bits1 : nullptr;
     k_fine_clock<<<1, 1, 0, st>>>(a->clock);
     kf_clean_copy<<<gf_valid, kBlk, 0, st>>>(F, P, a->S1, a->S1_old, a->err);
-    kf_expand<<<gf_grown, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[0],
-                                         a->S1_old, a->B1, fdlo, fdn, a->err);
-    count_launch(3);
+    kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1_old, a->B1, fdlo, fdn, a->err);
+    kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[0],
+                                          a->d_ib0, a->B1);
+    count_launch(4);
     camr_status cs = camr_batch_run(a->plan, 0.0, dt1, a->fine_mode, st);
     if (cs != CAMR_OK) return cudaErrorLaunchFailure;
     k_fine_add<<<gb, kBlk, 0, st>>>(R, F, FP, dt1, fac, volf8);
@@ -794,9 +836,10 @@ cudaError_t amr_issue_step(camr_amr* a, bool first) {
     } else {
       kf_update_mol1<<<gf_valid, kBlk, 0, st>>>(F, FP, P, dt1, a->B1, a->S1_old, a->S1);
       // Sborder of the second stage reuses B1 (the first one is consumed)
-      kf_expand<<<gf_grown, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[1],
-                                           a->S1, a->B1, fdlo, fdn, a->err);
-      count_launch(2);
+      kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1, a->B1, fdlo, fdn, a->err);
+      kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[1],
+                                            a->d_ib0, a->B1);
+      count_launch(3);
       cs = camr_batch_run(a->plan, 0.0, dt1, a->fine_mode, st);
       if (cs != CAMR_OK) return cudaErrorLaunchFailure;
       k_fine_add<<<gb, kBlk, 0, st>>>(R, F, FP, dt1, fac, volf8);
@@ -817,7 +860,7 @@ void amr_free(camr_amr* a) {
   if (a->plan) camr_batch_destroy(a->plan);
   void* ptrs[] = {a->S0, a->S0_old, a->B0, a->B0_2, a->flx0[0], a->flx0[1], a->flx0[2],
                   a->work0, a->S1, a->S1_old, a->B1, a->flx1[0], a->flx1[1], a->flx1[2],
-                  a->d_L, a->d_off, a->d_vb0, a->d_gb0, a->d_poff, a->d_qf, a->d_cmap,
+                  a->d_L, a->d_off, a->d_vb0, a->d_gb0, a->d_ib0, a->d_poff, a->d_qf, a->d_cmap,
                   a->d_bmap, a->d_bcell, a->d_mask, a->d_cstart, a->d_contrib, a->d_reg,
                   a->d_cfp, a->clock, a->hist, a->bits0, a->bits1, a->err, a->staging0,
                   a->staging1};
@@ -927,6 +970,7 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
   std::vector<int64_t> off(nbox), poff(nbox);
   a->h_vb0.assign(nbox + 1, 0);
   a->h_gb0.assign(nbox + 1, 0);
+  a->h_ib0.assign(nbox + 1, 0);
   int64_t total = 0, ptotal = 0;
   for (int b = 0; b < nbox; ++b) {
     const int* bx = boxes + 6 * b;
@@ -959,6 +1003,9 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
     a->ncell1 += nv;
     a->h_vb0[b + 1] = a->h_vb0[b] + (nv + kBlk - 1) / kBlk;
     a->h_gb0[b + 1] = a->h_gb0[b] + (ng + kBlk - 1) / kBlk;
+    int64_t nci = 1;  // coarse cells of grow(coarsened box, 2)
+    for (int d = 0; d < 3; ++d) nci *= (hi[d] - lo[d] + 1) / RR + 4;
+    a->h_ib0[b + 1] = a->h_ib0[b] + (nci + kBlk - 1) / kBlk;
   }
   a->pool = total;
   const size_t pbytes = size_t(total) * sizeof(double);
@@ -981,6 +1028,7 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
   if (e == cudaSuccess) e = upload(&a->d_poff, poff, st);
   if (e == cudaSuccess) e = upload(&a->d_vb0, a->h_vb0, st);
   if (e == cudaSuccess) e = upload(&a->d_gb0, a->h_gb0, st);
+  if (e == cudaSuccess) e = upload(&a->d_ib0, a->h_ib0, st);
   // the fine hydro plan (fluxes only) over the B1 pool
   std::vector<camr_box_task> tasks(nbox);
   for (int b = 0; b < nbox; ++b) {
