@@ -119,6 +119,15 @@ SIGNATURES = {
     "camr_amr_kernels_per_step": (C.c_int64, [C.c_void_p]),
     "camr_amr_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_amr_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
+    "camr_adjoint_create": (C.c_int, [C.POINTER(Geom), C.POINTER(HydroParams), C.c_int,
+                                      C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_adjoint_destroy": (C.c_int, [C.c_void_p]),
+    "camr_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_void_p]),
+    "camr_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "camr_adjoint_dts": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
+    "camr_adjoint_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_adjoint_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
 }
 
 

@@ -314,6 +314,34 @@ camr_status camr_amr_stream(camr_amr* a, void** stream);
 camr_status camr_amr_get_error(camr_amr* a, camr_error_info* info);
 
 /* ---------------------------------------------------------------------
+ * Discrete adjoint of the MOL level step (SSP-RK2, PLM slopes, two-shock
+ * Riemann; periodic uniform level, do_mol = 1, default energy flags).  No
+ * counterpart in the reference: it differentiates the CAMR_advance MOL
+ * path (Source/CAMR_advance.cpp:124-136 and what it calls) by hand, step by
+ * step in reverse, with the dt sequence of the forward pass frozen and
+ * checkpoint-and-recompute over time steps.
+ */
+typedef struct camr_adjoint camr_adjoint;
+
+camr_status camr_adjoint_create(const camr_geom* geom, const camr_hydro_params* p,
+                                int checkpoint_every, void* stream, camr_adjoint** out);
+camr_status camr_adjoint_destroy(camr_adjoint* a);
+/* Forward nsteps steps from S0 to S_final (device pointers, valid cells
+ * (NVAR, nz, ny, nx)).  dt per step: computeInitialDt / computeNewDt on the
+ * device, or the host array fixed_dts.  Keeps a checkpoint every
+ * checkpoint_every steps and the dt sequence for the backward pass. */
+camr_status camr_adjoint_forward(camr_adjoint* a, const double* S0, double* S_final,
+                                 int nsteps, const double* fixed_dts);
+/* Adjoint of the last forward run: lam0 = (dS_final/dS0)^T lam_final
+ * (device pointers, same layout).  UTEMP carries no adjoint (no other
+ * state variable depends on it). */
+camr_status camr_adjoint_backward(camr_adjoint* a, const double* lam_final, double* lam0);
+/* The dt sequence of the last forward run (synchronises). */
+camr_status camr_adjoint_dts(camr_adjoint* a, double* dts, int n);
+camr_status camr_adjoint_stream(camr_adjoint* a, void** stream);
+camr_status camr_adjoint_get_error(camr_adjoint* a, camr_error_info* info);
+
+/* ---------------------------------------------------------------------
  * Allocation-free per-box hydro.  No counterpart in the reference: it is
  * camr_hydro_umdrv for callers that may not allocate device memory while
  * they run (code inside an arena or pool that owns all device memory,
