@@ -37,6 +37,20 @@ class AdjointLevel:
                                         C.c_void_p(sp), C.byref(h)), "camr_adjoint_create")
         self._h = h
         self.nsteps = 0
+        st = C.c_void_p()
+        check(lib().camr_adjoint_stream(self._h, C.byref(st)), "camr_adjoint_stream")
+        self._stream = torch.cuda.ExternalStream(st.value) if st.value else None
+
+    def _enter(self):
+        """Inputs written by torch's current stream must be complete."""
+        _torch().cuda.current_stream().synchronize()
+
+    def _leave(self):
+        """Outputs must be complete before torch's stream reads them."""
+        if self._stream is not None:
+            self._stream.synchronize()
+        else:
+            _torch().cuda.synchronize()
 
     def close(self):
         if self._h:
@@ -63,9 +77,11 @@ class AdjointLevel:
             self._dts = np.ascontiguousarray(fixed_dts, dtype=np.float64)
             assert len(self._dts) == nsteps
             ptr = self._dts.ctypes.data
+        self._enter()
         check(lib().camr_adjoint_forward(self._h, C.c_void_p(S0.data_ptr()),
                                          C.c_void_p(out.data_ptr()), int(nsteps), ptr),
               "camr_adjoint_forward")
+        self._leave()
         self.nsteps = nsteps
         return out
 
@@ -74,8 +90,10 @@ class AdjointLevel:
         lam_final = lam_final.contiguous()
         self._check_state(lam_final)
         out = torch.empty_like(lam_final)
+        self._enter()
         check(lib().camr_adjoint_backward(self._h, C.c_void_p(lam_final.data_ptr()),
                                           C.c_void_p(out.data_ptr())), "camr_adjoint_backward")
+        self._leave()
         return out
 
     def dts(self):

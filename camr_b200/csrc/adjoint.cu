@@ -70,11 +70,6 @@ __device__ __forceinline__ void atomic_add_cell(double* a, int64_t at, int64_t s
     if (v[c] != 0.0) atomicAdd(a + at + c * sn, v[c]);
 }
 
-__device__ __forceinline__ bool in_box(const LGeom& L, int i, int j, int k) {
-  return i >= L.dlo[0] && i <= L.dhi[0] && j >= L.dlo[1] && j <= L.dhi[1] && k >= L.dlo[2] &&
-         k <= L.dhi[2];
-}
-
 // Face VJP of direction d on the faces of the domain box: the face's share
 // of the update (its flux in dSdt of the two cells and its interface p, u_n
 // in their p div u), then face_vjp, scattered to the cells' primitive

@@ -47,6 +47,9 @@ struct Par {
 CAMR_HD double hmax(double a, double b) { return (a < b) ? b : a; }  // std::max
 CAMR_HD double hmin(double a, double b) { return (b < a) ? b : a; }  // std::min
 CAMR_HD double sgn(double x) { return (x < 0.0) ? -1.0 : 1.0; }
+// Derivative of |x|, taken as 0 at x = 0 (where the limiters' |dl|, |dr|
+// sit when a field is exactly flat or exactly zero).
+CAMR_HD double dabs(double x) { return (x > 0.0) ? 1.0 : ((x < 0.0) ? -1.0 : 0.0); }
 
 // ---------------------------------------------------------------------------
 // Two-shock Riemann solver with its intermediates.
@@ -646,9 +649,9 @@ CAMR_HD void limiter_vjp(const LimTape& t, double b, double& bdl, double& bdr) {
     bdl += 0.5 * b;
     bdr += 0.5 * b;
   } else if (t.which == 1) {
-    bdl += b * dsgn * theta * sgn(t.dl);
+    bdl += b * dsgn * theta * dabs(t.dl);
   } else if (t.which == 2) {
-    bdr += b * dsgn * theta * sgn(t.dr);
+    bdr += b * dsgn * theta * dabs(t.dr);
   }
 }
 

@@ -110,43 +110,89 @@ def test_adjoint_matches_taped_reference():
         assert err < 1e-9, (c, err)
 
 
+def smooth_state(n, seed):
+    """A smooth periodic flow with non-zero velocities (no kinks of the
+    limiters or Riemann branches at the finite-difference scale)."""
+    rng = np.random.default_rng(seed)
+    x, y, z = P.cell_centres(n, dx=tuple(1.0 / v for v in n))
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    X, Y, Z = X.transpose(2, 1, 0), Y.transpose(2, 1, 0), Z.transpose(2, 1, 0)
+
+    def f(a):
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        k = rng.integers(1, 3, 3)
+        return a * np.sin(2 * np.pi * k[0] * X + ph[0]) * np.sin(2 * np.pi * k[1] * Y + ph[1]) \
+            * np.sin(2 * np.pi * k[2] * Z + ph[2])
+
+    rho = 1.0 + f(0.2)
+    u = [0.3 + f(0.2), -0.2 + f(0.2), 0.1 + f(0.2)]
+    p = 1.0 + f(0.3)
+    s = np.zeros((P.NVAR,) + rho.shape)
+    s[P.URHO] = rho
+    for d in range(3):
+        s[P.UMX + d] = rho * u[d]
+    s[P.UEINT] = p / 0.4
+    s[P.UEDEN] = s[P.UEINT] + 0.5 * rho * (u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    s[P.UTEMP] = 0.4 * (s[P.UEINT] / rho) * 26.93 / 8.31446261815324e7
+    s[P.UFS] = rho
+    return s
+
+
 def test_adjoint_finite_differences():
+    """d/d rho0 of the mass inside a sphere after 8 steps, perturbing the
+    initial density at fixed pressure and velocity (URHO, the first species
+    and the momenta / energies that carry u and p)."""
     torch = _torch()
     adjoint = _adj()
     n = (24, 24, 24)
-    s, rr = blast(n)
+    s = smooth_state(n, 5)
+    x, y, z = P.cell_centres(n, dx=tuple(1.0 / v for v in n))
+    rr = np.sqrt((x[None, None, :] - 0.5) ** 2 + (y[None, :, None] - 0.5) ** 2 +
+                 (z[:, None, None] - 0.5) ** 2)
     geom = hydro.make_geom(n)
     prm = native.default_params(do_mol=1, cfl=0.3)
     A = adjoint.AdjointLevel(geom, prm, checkpoint_every=3)
     nsteps = 8
     dV = 1.0 / (n[0] * n[1] * n[2])
-    mask = (rr < 0.2).astype(np.float64) * np.ones((n[2], n[1], n[0]))
-    out = A.forward(torch.from_numpy(s).cuda(), nsteps)
+    mask = (rr < 0.2).astype(np.float64)
+    A.forward(torch.from_numpy(s).cuda(), nsteps)
     dts = A.dts()
     lam = np.zeros_like(s)
     lam[P.URHO] = mask * dV
     g = A.backward(torch.from_numpy(lam).cuda()).cpu().numpy()
-    # perturb the initial density at fixed p, u: URHO and the first species
-    grad_rho = g[P.URHO] + g[P.UFS]
+    rho = s[P.URHO]
+    u = s[P.UMX:P.UMZ + 1] / rho
+    ke = 0.5 * (u ** 2).sum(axis=0)
+    # d(state)/d(rho) at fixed p, u
+    grad_rho = g[P.URHO] + g[P.UFS] + (g[P.UMX:P.UMZ + 1] * u).sum(axis=0) + g[P.UEDEN] * ke
 
     def J(state):
         o = A.forward(torch.from_numpy(state).cuda(), nsteps, fixed_dts=dts).cpu().numpy()
         return (o[P.URHO] * mask).sum() * dV
 
+    # cells inside the sphere, where dJ/drho is of order dV (far outside it
+    # the gradient is below the finite differences' round-off floor)
     rng = np.random.default_rng(64)
-    cells = [(12, 12, 12), (12, 13, 14), (10, 12, 12)]
-    cells += [tuple(int(v) for v in rng.integers(6, 18, size=3)) for _ in range(5)]
+    inside = np.argwhere(mask > 0)
+    cells = [tuple(int(v) for v in inside[t]) for t in rng.choice(len(inside), 8, replace=False)]
+    errs = []
     for (k, j, i) in cells:
-        eps = 1e-6 * s[P.URHO, k, j, i]
-        sp, sm = s.copy(), s.copy()
-        for st, sg in ((sp, 1.0), (sm, -1.0)):
-            st[P.URHO, k, j, i] += sg * eps
-            st[P.UFS, k, j, i] += sg * eps
-        fd = (J(sp) - J(sm)) / (2 * eps)
+        eps = 1e-6 * rho[k, j, i]
+        res = []
+        for sg in (1.0, -1.0):
+            st = s.copy()
+            r1 = rho[k, j, i] + sg * eps
+            st[P.URHO, k, j, i] = r1
+            st[P.UFS, k, j, i] = r1
+            st[P.UMX:P.UMZ + 1, k, j, i] = r1 * u[:, k, j, i]
+            st[P.UEDEN, k, j, i] = s[P.UEINT, k, j, i] + r1 * ke[k, j, i]
+            res.append(J(st))
+        fd = (res[0] - res[1]) / (2 * eps)
         ad = grad_rho[k, j, i]
-        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)) + 1e-14, ((k, j, i), fd, ad)
+        errs.append(abs(fd - ad) / max(abs(fd), abs(ad)))
     A.close()
-    del out
+    assert np.median(errs) <= 1e-6, errs
+    assert max(errs) <= 1e-5, errs
 
 
 def test_autograd_function_gives_library_gradient():
@@ -165,5 +211,6 @@ def test_autograd_function_gives_library_gradient():
     lam = torch.zeros_like(S)
     lam[P.URHO] = w.reshape(S[0].shape)
     ref = A.backward(lam)
-    assert torch.equal(S0.grad, ref)
+    # the scatter sums use FP64 atomics: two runs agree to round-off
+    assert torch.allclose(S0.grad, ref, rtol=1e-12, atol=1e-14 * float(ref.abs().max()))
     A.close()
