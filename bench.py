@@ -296,10 +296,12 @@ def run_camr(args, world, rank, local, pg):
 
     batched = None
     amr = None
+    adj = None
     if rank == 0 and world == 1 and not args.no_batched:
         L.close()
         batched = batched_comparison(args)
         amr = amr_comparison(args)
+        adj = adjoint_comparison(args)
 
     if rank == 0:
         line = {
@@ -317,6 +319,7 @@ def run_camr(args, world, rank, local, pg):
             "stages_ms": acc, "device_error": list(err),
             "batched_amr_patches": batched,
             "amr_two_level": amr,
+            "adjoint_c3": adj,
         }
         print(json.dumps(line))
     L.close()
@@ -467,6 +470,75 @@ def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
     return out
 
 
+def adjoint_comparison(args, n=128, nsteps=200, every=20, fd_cells=0):
+    """The adjoint configuration: 128^3 periodic, MOL-PLM RK2 (CFL 0.3),
+    200 steps with a checkpoint every 20, J = mass inside the sphere r < 0.2
+    at the final time, dJ/d(initial rho) from the hand-written adjoint.
+    Reports forward and backward device times and their ratio per step;
+    with fd_cells > 0 also central differences (eps = 1e-6 rho) at that many
+    seeded cells inside the sphere."""
+    import torch
+
+    from camr_b200 import adjoint, hydro, native, problems
+    nn = (n, n, n)
+    s, r = problems.grf_blast(nn)
+    geom = hydro.make_geom(nn)
+    prm = native.default_params(do_mol=1, ppm_type=0, cfl=0.3)
+    A = adjoint.AdjointLevel(geom, prm, checkpoint_every=every)
+    S0 = torch.from_numpy(s).cuda()
+    dV = 1.0 / (n ** 3)
+    mask = torch.from_numpy((r < 0.2).astype(np.float64)).cuda()
+    lam = torch.zeros_like(S0)
+    lam[0] = mask * dV
+    A.forward(S0, 2)          # warm-up (module load, allocation)
+    A.backward(lam)
+    torch.cuda.synchronize()
+    st = A._stream if A._stream is not None else torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(st)
+    A.forward(S0, nsteps)
+    ev[1].record(st)
+    g = A.backward(lam)
+    ev[2].record(st)
+    torch.cuda.synchronize()
+    fwd_ms = ev[0].elapsed_time(ev[1])
+    bwd_ms = ev[1].elapsed_time(ev[2])
+    dts = A.dts()
+    grad = (g[0] + g[7]).cpu().numpy()  # d/d rho at fixed p, u = 0
+    out = {"domain": list(nn), "steps": nsteps, "checkpoint_every": every,
+           "forward_ms_per_step": fwd_ms / nsteps,
+           "backward_ms_per_step": bwd_ms / nsteps,
+           "adjoint_over_forward": bwd_ms / fwd_ms,
+           "timing": "CUDA events on the adjoint's stream",
+           "device_error": list(A.error())}
+    if fd_cells:
+        rng = np.random.default_rng(64)
+        inside = np.argwhere(r < 0.2)
+        cells = [tuple(int(v) for v in inside[t])
+                 for t in rng.choice(len(inside), fd_cells, replace=False)]
+        errs = []
+        for (k, j, i) in cells:
+            eps = 1e-6 * s[0, k, j, i]
+            res = []
+            for sg in (1.0, -1.0):
+                st = s.copy()
+                st[0, k, j, i] += sg * eps
+                st[7, k, j, i] += sg * eps
+                o = A.forward(torch.from_numpy(st).cuda(), nsteps, fixed_dts=dts)
+                res.append(float((o[0] * mask).sum()) * dV)
+            fd = (res[0] - res[1]) / (2 * eps)
+            ad = float(grad[k, j, i])
+            errs.append(abs(fd - ad) / max(abs(fd), abs(ad)))
+        errs = np.array(errs)
+        out["fd_check"] = {"cells": fd_cells, "eps_rel": 1e-6,
+                           "median_rel_err": float(np.median(errs)),
+                           "max_rel_err": float(errs.max()),
+                           "frac_within_1e-6": float(np.mean(errs <= 1e-6))}
+    A.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_batched(args, rank):
     """Batched vs per-box launches over the uneven fine-level boxes of the
     two-level configuration (hydro of one level step, CTU-PPM)."""
@@ -528,11 +600,23 @@ def main():
     ap.add_argument("--impl", choices=["camr", "reference"], default="camr")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["c1", "c2-batched"], default="c1")
+    ap.add_argument("--workload", choices=["c1", "c2-batched", "c3-adjoint"], default="c1")
+    ap.add_argument("--fd-cells", type=int, default=64,
+                    help="finite-difference cells of the c3-adjoint workload")
     ap.add_argument("--nbox", type=int, default=350)
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-per-box comparison in the default line")
     args = ap.parse_args()
+    if args.workload == "c3-adjoint":
+        import torch
+        from camr_b200 import build, native
+        if not os.path.exists(native.LIB_PATH):
+            build.build()
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"workload": "c3-adjoint",
+                              **adjoint_comparison(args, fd_cells=args.fd_cells)}))
+        return
     if args.workload == "c2-batched":
         run_batched(args, int(os.environ.get("RANK", "0")))
         return

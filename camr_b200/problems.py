@@ -191,3 +191,32 @@ def amr_initial(n0, boxes, vel=(0.4, -0.3, 0.2), **kw):
                            **kw).ravel())
     S1 = np.concatenate(parts) if parts else np.zeros(0)
     return S0, S1
+
+
+def grf_blast(n, seed=3, corr=0.1, amp=0.05, p_blast=20.0, r_blast=0.05, gamma=1.4):
+    """Adjoint configuration initial data on the periodic unit cube:
+    rho = 1 + amp * g with g a Gaussian random field (white noise from
+    numpy's PCG64 seeded with `seed`, filtered in Fourier space by a Gaussian
+    kernel exp(-|x|^2 / (2 corr^2)), normalised to zero mean and unit
+    variance), p = 1, zero velocity, and a centred blast p = p_blast for
+    r < r_blast.  Species (1, 0, 0).  Returns (state, r) with r the distance
+    of each cell centre from the centre."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((n[2], n[1], n[0]))
+    kz = np.fft.fftfreq(n[2]) * n[2]
+    ky = np.fft.fftfreq(n[1]) * n[1]
+    kx = np.fft.fftfreq(n[0]) * n[0]
+    K2 = kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
+    g = np.real(np.fft.ifftn(np.fft.fftn(w) * np.exp(-2.0 * np.pi ** 2 * corr ** 2 * K2)))
+    g = (g - g.mean()) / g.std()
+    x, y, z = cell_centres(n, dx=tuple(1.0 / v for v in n))
+    r = np.sqrt((x[None, None, :] - 0.5) ** 2 + (y[None, :, None] - 0.5) ** 2 +
+                (z[:, None, None] - 0.5) ** 2)
+    rho = 1.0 + amp * g
+    p = np.where(r < r_blast, p_blast, 1.0)
+    s = np.zeros((NVAR, n[2], n[1], n[0]))
+    s[URHO] = rho
+    s[UEINT] = p / (gamma - 1.0)
+    s[UEDEN] = s[UEINT]
+    s[UFS] = rho
+    return s, r
