@@ -600,7 +600,10 @@ def main():
     ap.add_argument("--impl", choices=["camr", "reference"], default="camr")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["c1", "c2-batched", "c3-adjoint"], default="c1")
+    ap.add_argument("--workload", choices=["c1", "c2-batched", "c2-amr", "c3-adjoint"],
+                    default="c1")
+    ap.add_argument("--adj-n", type=int, default=128, help="c3-adjoint domain size")
+    ap.add_argument("--adj-steps", type=int, default=200, help="c3-adjoint steps")
     ap.add_argument("--fd-cells", type=int, default=64,
                     help="finite-difference cells of the c3-adjoint workload")
     ap.add_argument("--nbox", type=int, default=350)
@@ -615,7 +618,17 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({"workload": "c3-adjoint",
-                              **adjoint_comparison(args, fd_cells=args.fd_cells)}))
+                              **adjoint_comparison(args, n=args.adj_n, nsteps=args.adj_steps,
+                                                   fd_cells=args.fd_cells)}))
+        return
+    if args.workload == "c2-amr":
+        import torch
+        from camr_b200 import build, native
+        if not os.path.exists(native.LIB_PATH):
+            build.build()
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"workload": "c2-amr", **amr_comparison(args)}))
         return
     if args.workload == "c2-batched":
         run_batched(args, int(os.environ.get("RANK", "0")))

@@ -316,27 +316,19 @@ __global__ void __launch_bounds__(kBlk) k_adj_expand(LGeom L, KParams P, const d
 // second clean after the zero gravity source when add_grav_src), with
 // S_pre = B2/2 + S_old/2 + dt/2 k2.  Writes the adjoints of B2 (valid
 // cells; ghost cells zeroed by the caller), of S_old (first half) and of k2.
-__global__ void __launch_bounds__(kBlk) k_adj_final(LGeom L, Space sp, KParams P,
-                                                     const double* dtp, const double* B2,
-                                                     const double* S_old, FluxPtrs fp,
-                                                     const double* Lout, double* LB2,
-                                                     double* LSold, double* Ldsdt) {
+__global__ void __launch_bounds__(kBlk) k_adj_final(LGeom L, KParams P, const double* dtp,
+                                                     const double* Spre, const double* Lout,
+                                                     double* LB2, double* LSold,
+                                                     double* Ldsdt) {
   int i, j, k;
   if (!valid_cell(L, tid(), i, j, k)) return;
   const double dt = *dtp;
   const int64_t at = L.idx(i, j, k);
-  double s0[NV], sold[NV], b[NV], hs[NV];
-  load_cell(B2, L, at, b);
-  load_cell(S_old, L, at, sold);
-  for (int n = 0; n < NV; ++n) s0[n] = 0.5 * b[n] + 0.5 * sold[n];
-  cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
-  for (int n = 0; n < NV; ++n) s0[n] += 0.5 * dt * hs[n];
   const Par Pr = par_of(P);
-  // forward states of the cleans
   const int ncl = P.add_grav_src ? 3 : 2;
   double st[3][NV];
   CleanTape tp;
-  for (int n = 0; n < NV; ++n) st[0][n] = s0[n];
+  load_cell(Spre, L, at, st[0]);
   for (int c = 1; c < ncl; ++c) clean_fwd(st[c - 1], Pr, tp, st[c]);
   double lam[NV], lnext[NV];
   load_cell(Lout, L, at, lam);
@@ -382,6 +374,31 @@ __global__ void __launch_bounds__(kBlk) k_adj_first_clean(LGeom L, KParams P, co
   store_cell(lam, L, at, out);
 }
 
+// The state before the end-of-step cleans: S_pre = B2/2 + S_old/2 + dt/2 k2.
+__global__ void __launch_bounds__(kBlk) k_store_pre(LGeom L, Space sp, const double* dtp,
+                                                     const double* B2, const double* S_old,
+                                                     FluxPtrs fp, double* out) {
+  int i, j, k;
+  if (!valid_cell(L, tid(), i, j, k)) return;
+  const double dt = *dtp;
+  const int64_t at = L.idx(i, j, k);
+  double b[NV], so[NV], hs[NV];
+  load_cell(B2, L, at, b);
+  load_cell(S_old, L, at, so);
+  cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
+  for (int n = 0; n < NV; ++n) {
+    double v = 0.5 * b[n] + 0.5 * so[n];
+    v += 0.5 * dt * hs[n];
+    out[at + n * L.sn] = v;
+  }
+}
+
+// Forward intermediates of one step that its adjoint reads.
+struct StepTape {
+  double *Sn, *S_old, *B, *Sstar, *B2, *Spre;
+  Work w1, w2;
+};
+
 }  // namespace
 }  // namespace camr
 
@@ -413,6 +430,11 @@ struct camr_adjoint {
   // step-start states of one segment
   std::vector<double*> ckpt;
   std::vector<double*> seg;
+  // per-step tapes of one segment (kept when they fit in device memory)
+  std::vector<double*> tape_mem;
+  std::vector<StepTape> tapes;
+  bool tapes_ok = false;
+  double* Spre = nullptr;  // the S_pre of the recompute path
   int nsteps = 0;
   double* staging = nullptr;
   size_t sbytes = 0;
@@ -422,14 +444,22 @@ namespace {
 
 unsigned nblk(int64_t n) { return unsigned((n + kBlk - 1) / kBlk); }
 
-// One forward MOL step on a->S with dt read from *dtp: the kernels of the
-// level driver, in its order.  bits (may be NULL) receives the CFL minimum.
-cudaError_t fwd_step(camr_adjoint* a, const double* dtp, unsigned long long* bits) {
+// One forward MOL step from a->S with dt read from *dtp, writing the step's
+// intermediates into `t` (S_old, B, S*, B2, the two Works; S_pre when
+// t.Spre is set; a copy of S_n when t.Sn is another array) and, when
+// `advance`, the new state into a->S: the kernels of the level driver, in
+// its order.  bits (may be NULL) receives the CFL minimum of the new state.
+cudaError_t fwd_step_tape(camr_adjoint* a, const double* dtp, unsigned long long* bits,
+                          const StepTape& t, bool advance) {
   cudaStream_t st = a->stream;
   const LGeom& L = a->G.L;
   const int64_t npad = int64_t(L.pn[0]) * L.pn[1] * L.pn[2];
-  k_clean_copy<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, a->S, a->S_old, a->err);
-  k_expand<<<nblk(npad), kBlk, 0, st>>>(L, a->P, a->S_old, a->B, a->err);
+  if (t.Sn && t.Sn != a->S) {
+    cudaError_t e = cudaMemcpyAsync(t.Sn, a->S, a->sbytes, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  k_clean_copy<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, a->S, t.S_old, a->err);
+  k_expand<<<nblk(npad), kBlk, 0, st>>>(L, a->P, t.S_old, t.B, a->err);
   count_launch(2);
   HydroLaunch H;
   for (int d = 0; d < 3; ++d) {
@@ -457,81 +487,53 @@ cudaError_t fwd_step(camr_adjoint* a, const double* dtp, unsigned long long* bit
   };
   for (int d = 0; d < 3; ++d) H.flx[d] = sdfab(a->flx[d]);
   H.dsdt = sdfab(nullptr);
-  H.uin = sdfab(a->B);
+  H.uin = sdfab(t.B);
   H.src = H.uin;
-  cudaError_t e = launch_hydro_fluxes(H, a->w1, st);
+  cudaError_t e = launch_hydro_fluxes(H, t.w1, st);
   if (e != cudaSuccess) return e;
   FluxPtrs fp1, fp2;
   for (int d = 0; d < 3; ++d) {
     fp1.f[d] = fp2.f[d] = a->flx[d];
-    fp1.q[d] = a->w1.qf[d];
-    fp2.q[d] = a->w2.qf[d];
+    fp1.q[d] = t.w1.qf[d];
+    fp2.q[d] = t.w2.qf[d];
   }
-  k_update_mol1<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, a->P, dtp, a->B, a->S_old, fp1,
-                                                 a->Sstar);
-  k_expand<<<nblk(npad), kBlk, 0, st>>>(L, a->P, a->Sstar, a->B2, a->err);
+  k_update_mol1<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, a->P, dtp, t.B, t.S_old, fp1,
+                                                 t.Sstar);
+  k_expand<<<nblk(npad), kBlk, 0, st>>>(L, a->P, t.Sstar, t.B2, a->err);
   count_launch(2);
-  H.uin = sdfab(a->B2);
+  H.uin = sdfab(t.B2);
   H.src = H.uin;
-  e = launch_hydro_fluxes(H, a->w2, st);
+  e = launch_hydro_fluxes(H, t.w2, st);
   if (e != cudaSuccess) return e;
-  k_update_mol2<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, a->P, dtp, a->B2, a->S_old, fp2,
-                                                 a->S, bits, a->err, 1);
-  count_launch();
+  if (t.Spre) {
+    k_store_pre<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, dtp, t.B2, t.S_old, fp2, t.Spre);
+    count_launch();
+  }
+  if (advance) {
+    k_update_mol2<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, a->P, dtp, t.B2, t.S_old, fp2,
+                                                   a->S, bits, a->err, 1);
+    count_launch();
+  }
   return cudaGetLastError();
 }
 
-// Recompute the forward intermediates of one step from S_n (copied into
-// a->S first), without writing the step's result.
-cudaError_t fwd_intermediates(camr_adjoint* a, const double* dtp) {
-  cudaStream_t st = a->stream;
-  const LGeom& L = a->G.L;
-  const int64_t npad = int64_t(L.pn[0]) * L.pn[1] * L.pn[2];
-  k_clean_copy<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, a->S, a->S_old, a->err);
-  k_expand<<<nblk(npad), kBlk, 0, st>>>(L, a->P, a->S_old, a->B, a->err);
-  count_launch(2);
-  HydroLaunch H;
-  for (int d = 0; d < 3; ++d) {
-    H.g.lo[d] = L.dlo[d];
-    H.g.hi[d] = L.dhi[d];
-    H.g.dlo[d] = L.dlo[d];
-    H.g.dhi[d] = L.dhi[d];
-    H.g.bclo[d] = L.bclo[d];
-    H.g.bchi[d] = L.bchi[d];
-    H.g.dx[d] = L.dx[d];
-  }
-  H.P = a->P;
-  H.has_src = false;
-  H.mol = true;
-  H.dt = DtRef{0.0, dtp};
-  H.err = a->err;
-  auto sdfab = [&](double* p) {
-    DFab f;
-    f.p = p;
-    for (int d = 0; d < 3; ++d) f.lo[d] = L.plo[d];
-    f.sy = L.sy;
-    f.sz = L.sz;
-    f.sn = L.sn;
-    return f;
-  };
-  for (int d = 0; d < 3; ++d) H.flx[d] = sdfab(a->flx[d]);
-  H.dsdt = sdfab(nullptr);
-  H.uin = sdfab(a->B);
-  H.src = H.uin;
-  cudaError_t e = launch_hydro_fluxes(H, a->w1, st);
-  if (e != cudaSuccess) return e;
-  FluxPtrs fp1;
-  for (int d = 0; d < 3; ++d) {
-    fp1.f[d] = a->flx[d];
-    fp1.q[d] = a->w1.qf[d];
-  }
-  k_update_mol1<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, a->P, dtp, a->B, a->S_old, fp1,
-                                                 a->Sstar);
-  k_expand<<<nblk(npad), kBlk, 0, st>>>(L, a->P, a->Sstar, a->B2, a->err);
-  count_launch(2);
-  H.uin = sdfab(a->B2);
-  H.src = H.uin;
-  return launch_hydro_fluxes(H, a->w2, st);
+StepTape scratch_tape(camr_adjoint* a) {
+  StepTape t;
+  t.Sn = a->S;
+  t.S_old = a->S_old;
+  t.B = a->B;
+  t.Sstar = a->Sstar;
+  t.B2 = a->B2;
+  t.Spre = a->Spre;
+  t.w1 = a->w1;
+  t.w2 = a->w2;
+  return t;
+}
+
+cudaError_t fwd_step(camr_adjoint* a, const double* dtp, unsigned long long* bits) {
+  StepTape t = scratch_tape(a);
+  t.Spre = nullptr;
+  return fwd_step_tape(a, dtp, bits, t, true);
 }
 
 // Adjoint of one L(B) evaluation: Ldsdt (valid cells) -> LB (+=, padded).
@@ -585,47 +587,77 @@ cudaError_t hydro_adj(camr_adjoint* a, const double* Bp, const Work& w, double* 
   return cudaGetLastError();
 }
 
-// Reverse one step n: a->Lam holds the adjoint of S_{n+1} (valid cells);
-// a->S holds S_n.  On return a->Lam holds the adjoint of S_n.
-cudaError_t adj_step(camr_adjoint* a, const double* dtp) {
+// Reverse one step: a->Lam holds the adjoint of S_{n+1} (valid cells); `t`
+// holds the step's forward intermediates.  On return a->Lam holds the
+// adjoint of S_n.
+cudaError_t adj_step(camr_adjoint* a, const double* dtp, const StepTape& t) {
   cudaStream_t st = a->stream;
   const LGeom& L = a->G.L;
-  cudaError_t e = fwd_intermediates(a, dtp);
-  if (e != cudaSuccess) return e;
   // padded adjoint arrays start from zero (ghost cells receive the scatter)
   const size_t b = a->sbytes;
-  e = cudaMemsetAsync(a->LB2, 0, b, st);
+  cudaError_t e = cudaMemsetAsync(a->LB2, 0, b, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(a->LB, 0, b, st);
   if (e != cudaSuccess) return e;
-  FluxPtrs fp2;
-  for (int d = 0; d < 3; ++d) {
-    fp2.f[d] = a->flx[d];
-    fp2.q[d] = a->w2.qf[d];
-  }
-  k_adj_final<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->G.sp, a->P, dtp, a->B2, a->S_old, fp2,
-                                               a->Lam, a->LB2, a->LSold, a->Ldsdt);
+  k_adj_final<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, dtp, t.Spre, a->Lam, a->LB2, a->LSold,
+                                               a->Ldsdt);
   count_launch();
-  e = hydro_adj(a, a->B2, a->w2, a->LB2);
+  e = hydro_adj(a, t.B2, t.w2, a->LB2);
   if (e != cudaSuccess) return e;
-  k_adj_expand<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, a->Sstar, a->LB2, a->LStar, 0);
+  k_adj_expand<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, t.Sstar, a->LB2, a->LStar, 0);
   k_adj_stage1<<<nblk(a->ncell), kBlk, 0, st>>>(L, dtp, a->LStar, a->LB, a->Ldsdt);
   count_launch(2);
-  e = hydro_adj(a, a->B, a->w1, a->LB);
+  e = hydro_adj(a, t.B, t.w1, a->LB);
   if (e != cudaSuccess) return e;
-  k_adj_expand<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, a->S_old, a->LB, a->LSold, 1);
-  k_adj_first_clean<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, a->S, a->LSold, a->Lam);
+  k_adj_expand<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, t.S_old, a->LB, a->LSold, 1);
+  k_adj_first_clean<<<nblk(a->ncell), kBlk, 0, st>>>(L, a->P, t.Sn, a->LSold, a->Lam);
   count_launch(2);
   return cudaGetLastError();
 }
 
+// Per-step tapes for a segment of `every` steps, if they fit in half of the
+// free device memory.
+bool alloc_tapes(camr_adjoint* a) {
+  if (a->tapes_ok) return true;
+  const size_t wb = work_doubles(a->G.sp, true, false) * sizeof(double);
+  const size_t per = 6 * a->sbytes + 2 * wb;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
+  if (per * size_t(a->every) > free_b / 2) return false;
+  for (int n = 0; n < a->every; ++n) {
+    double* m = nullptr;
+    if (cudaMalloc(reinterpret_cast<void**>(&m), per) != cudaSuccess) return false;
+    a->tape_mem.push_back(m);
+    StepTape t;
+    double* p = m;
+    auto take = [&](size_t bytes) {
+      double* r = p;
+      p += bytes / sizeof(double);
+      return r;
+    };
+    t.Sn = take(a->sbytes);
+    t.S_old = take(a->sbytes);
+    t.B = take(a->sbytes);
+    t.Sstar = take(a->sbytes);
+    t.B2 = take(a->sbytes);
+    t.Spre = take(a->sbytes);
+    t.w1.s = t.w2.s = a->G.sp;
+    work_carve(t.w1, take(wb), true, false);
+    work_carve(t.w2, take(wb), true, false);
+    a->tapes.push_back(t);
+  }
+  a->tapes_ok = true;
+  return true;
+}
+
 void adj_free(camr_adjoint* a) {
-  void* ptrs[] = {a->S, a->S_old, a->B, a->B2, a->Sstar, a->flx[0], a->flx[1], a->flx[2],
+  void* ptrs[] = {a->S, a->S_old, a->B, a->B2, a->Sstar, a->Spre, a->flx[0], a->flx[1], a->flx[2],
                   a->work1, a->work2, a->dt_cur, a->dt_hist, a->bits, a->nstep, a->err,
                   a->Lam, a->LB, a->LB2, a->LSold, a->LStar, a->Ldsdt, a->Lq, a->staging};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (double* p : a->ckpt) cudaFree(p);
   for (double* p : a->seg) cudaFree(p);
+  for (double* p : a->tape_mem) cudaFree(p);
   if (a->own_stream) cudaStreamDestroy(a->stream);
   delete a;
 }
@@ -680,7 +712,8 @@ camr_status camr_adjoint_create(const camr_geom* geom, const camr_hydro_params* 
     if (e == cudaSuccess) e = cudaMemsetAsync(*ptr, 0, bytes, a->stream);
   };
   for (double** pp : {&a->S, &a->S_old, &a->B, &a->B2, &a->Sstar, &a->flx[0], &a->flx[1],
-                      &a->flx[2], &a->Lam, &a->LB, &a->LB2, &a->LSold, &a->LStar, &a->Ldsdt})
+                      &a->flx[2], &a->Lam, &a->LB, &a->LB2, &a->LSold, &a->LStar, &a->Ldsdt,
+                      &a->Spre})
     alloc(pp, a->sbytes);
   const size_t wb = work_doubles(a->G.sp, true, false) * sizeof(double);
   alloc(&a->work1, wb);
@@ -782,18 +815,29 @@ camr_status camr_adjoint_backward(camr_adjoint* a, const double* lam_final, doub
     a->seg.push_back(p);
   }
   const int nseg = (a->nsteps + a->every - 1) / a->every;
+  const bool taped = alloc_tapes(a);
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int n0 = sg * a->every;
     const int n1 = std::min(a->nsteps, n0 + a->every);
-    // recompute the segment's step-start states from its checkpoint
     e = cudaMemcpyAsync(a->S, a->ckpt[sg], a->sbytes, cudaMemcpyDeviceToDevice, st);
-    for (int n = n0; n < n1 && e == cudaSuccess; ++n) {
-      e = cudaMemcpyAsync(a->seg[n - n0], a->S, a->sbytes, cudaMemcpyDeviceToDevice, st);
-      if (e == cudaSuccess && n + 1 < n1) e = fwd_step(a, a->dt_hist + n, nullptr);
-    }
-    for (int n = n1 - 1; n >= n0 && e == cudaSuccess; --n) {
-      e = cudaMemcpyAsync(a->S, a->seg[n - n0], a->sbytes, cudaMemcpyDeviceToDevice, st);
-      if (e == cudaSuccess) e = adj_step(a, a->dt_hist + n);
+    if (taped) {
+      // replay the segment keeping every step's intermediates
+      for (int n = n0; n < n1 && e == cudaSuccess; ++n)
+        e = fwd_step_tape(a, a->dt_hist + n, nullptr, a->tapes[n - n0], n + 1 < n1);
+      for (int n = n1 - 1; n >= n0 && e == cudaSuccess; --n)
+        e = adj_step(a, a->dt_hist + n, a->tapes[n - n0]);
+    } else {
+      // keep only the step-start states; recompute each step's intermediates
+      for (int n = n0; n < n1 && e == cudaSuccess; ++n) {
+        e = cudaMemcpyAsync(a->seg[n - n0], a->S, a->sbytes, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && n + 1 < n1) e = fwd_step(a, a->dt_hist + n, nullptr);
+      }
+      const StepTape t = scratch_tape(a);
+      for (int n = n1 - 1; n >= n0 && e == cudaSuccess; --n) {
+        e = cudaMemcpyAsync(a->S, a->seg[n - n0], a->sbytes, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = fwd_step_tape(a, a->dt_hist + n, nullptr, t, false);
+        if (e == cudaSuccess) e = adj_step(a, a->dt_hist + n, t);
+      }
     }
     if (e != cudaSuccess) return cuda_status_of(e);
   }
