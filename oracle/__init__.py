@@ -12,5 +12,5 @@ interface (oracle_abi.h):
 from .binding import (  # noqa: F401
     NVAR, QVAR, NGDNV, Params, Level, load, default_params, make_level,
     hydro_box, advance, advance_fixed_dt, est_dt, init_finalize,
-    expand_state, clean_state, amr_run, build, lib_path,
+    expand_state, clean_state, amr_run, build, lib_path, lib_path_eb, hydro_box_eb,
 )

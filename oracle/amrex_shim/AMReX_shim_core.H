@@ -92,6 +92,7 @@ struct IntVect {
   int v[3] = {0, 0, 0};
   IntVect() = default;
   IntVect(int a, int b, int c) { v[0] = a; v[1] = b; v[2] = c; }
+  explicit IntVect(int a) { v[0] = v[1] = v[2] = a; }
   int& operator[](int i) { return v[i]; }
   int operator[](int i) const { return v[i]; }
   static IntVect TheDimensionVector(int d) {
@@ -108,11 +109,41 @@ inline IntVect operator*(int s, const IntVect& a) {
   return IntVect(s * a[0], s * a[1], s * a[2]);
 }
 
+template <class T>
+struct Array4;
+
 struct Box {
   IntVect lo, hi;
   int nodal[3] = {0, 0, 0};
   Box() = default;
   Box(const IntVect& l, const IntVect& h) : lo(l), hi(h) {}
+  // The index range of an array (cell-centred).
+  template <class T>
+  explicit Box(const Array4<T>& a);
+  Box& grow(int n) {
+    for (int d = 0; d < 3; ++d) { lo[d] -= n; hi[d] += n; }
+    return *this;
+  }
+  Box& grow(const IntVect& n) {
+    for (int d = 0; d < 3; ++d) { lo[d] -= n[d]; hi[d] += n[d]; }
+    return *this;
+  }
+  Box& surroundingNodes() {
+    for (int d = 0; d < 3; ++d)
+      if (!nodal[d]) { hi[d] += 1; nodal[d] = 1; }
+    return *this;
+  }
+  Box& operator&=(const Box& o) {
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::max(lo[d], o.lo[d]);
+      hi[d] = std::min(hi[d], o.hi[d]);
+    }
+    return *this;
+  }
+  bool contains(const IntVect& p) const {
+    return p[0] >= lo[0] && p[0] <= hi[0] && p[1] >= lo[1] && p[1] <= hi[1] &&
+           p[2] >= lo[2] && p[2] <= hi[2];
+  }
   const int* loVect() const { return lo.v; }
   const int* hiVect() const { return hi.v; }
   GpuArray<int, 3> loVect3d() const { return {{lo[0], lo[1], lo[2]}}; }
@@ -181,6 +212,22 @@ struct Array4 {
   }
 };
 
+template <class T>
+Box::Box(const Array4<T>& a)
+    : lo(a.begin), hi(IntVect(a.end[0] - 1, a.end[1] - 1, a.end[2] - 1)) {}
+
+// Node-centred version of a cell box (every direction of `t` that is 1).
+inline Box convert(const Box& b, const IntVect& t) {
+  Box r = b;
+  for (int d = 0; d < 3; ++d)
+    if (t[d] && !r.nodal[d]) { r.hi[d] += 1; r.nodal[d] = 1; }
+  return r;
+}
+
+// Types named only in declarations of the reference's EB entry points.
+class MFIter;
+class EBFArrayBoxFactory;
+
 struct Arena {};
 inline Arena* The_Async_Arena() { return nullptr; }
 inline Arena* The_Arena() { return nullptr; }
@@ -215,10 +262,21 @@ class FArrayBox {
 class Geometry {
  public:
   Geometry() = default;
-  explicit Geometry(const Box& dom) : dom_(dom) {}
+  explicit Geometry(const Box& dom, const int* periodic = nullptr) : dom_(dom) {
+    for (int d = 0; d < 3; ++d) per_[d] = periodic ? periodic[d] : 0;
+  }
   const Box& Domain() const { return dom_; }
+  bool isPeriodic(int d) const { return per_[d] != 0; }
+  // The domain grown by n in its periodic directions.
+  Box growPeriodicDomain(int n) const {
+    Box r = dom_;
+    for (int d = 0; d < 3; ++d)
+      if (per_[d]) { r.lo[d] -= n; r.hi[d] += n; }
+    return r;
+  }
  private:
   Box dom_;
+  int per_[3] = {0, 0, 0};
 };
 
 struct BCRec {
@@ -236,6 +294,13 @@ inline void ParallelFor(const Box& b, F&& f) {
 }
 template <class F>
 inline void Loop(const Box& b, F&& f) { ParallelFor(b, f); }
+template <class F>
+inline void ParallelFor(const Box& b, int ncomp, F&& f) {
+  for (int n = 0; n < ncomp; ++n)
+    for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+      for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+        for (int i = b.lo[0]; i <= b.hi[0]; ++i) f(i, j, k, n);
+}
 
 namespace Gpu {
 inline void streamSynchronize() {}

@@ -10,6 +10,55 @@ NVAR, QVAR, NGDNV = 10, 11, 6
 _LIBS = {}
 
 
+def lib_path_eb():
+    return os.path.join(HERE, "_ref", "libcamr_ref_eb.so")
+
+
+_EB = None
+
+
+def load_eb():
+    """The reference's EB hydro (oracle/_ref/libcamr_ref_eb.so)."""
+    global _EB
+    if _EB is None:
+        path = lib_path_eb()
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"EB oracle library missing: {path} (run `make -C oracle ref`)")
+        lib = C.CDLL(path)
+        lib.orc_hydro_box_eb.restype = C.c_long
+        _EB = lib
+    return _EB
+
+
+def hydro_box_eb(p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, periodic, uin, g_lo, geo, dx, dt,
+                 redist=1, weights_type=2):
+    """Per-box EB hydro (MOL).  uin: (NVAR, ...) over G = [g_lo, g_lo + shape - 1];
+    geo: eb_geometry.sphere_geometry output over the same G.  Returns
+    (dsdt on bx, [flx_x, flx_y, flx_z] on bx faces, nassert)."""
+    lib = load_eb()
+    nb = [bx_hi[d] - bx_lo[d] + 1 for d in range(3)]
+    uin = np.ascontiguousarray(uin, dtype=np.float64)
+    g_hi = [g_lo[d] + uin.shape[3 - d] - 1 for d in range(3)]
+    dsdt = np.zeros((NVAR, nb[2], nb[1], nb[0]))
+    flx = []
+    for d in range(3):
+        s = list(nb)
+        s[d] += 1
+        flx.append(np.zeros((NVAR, s[2], s[1], s[0])))
+    I3 = _I3
+    arr = [np.ascontiguousarray(a, dtype=np.float64) for a in geo["ap"]]
+    fcs = [np.ascontiguousarray(a, dtype=np.float64) for a in geo["fc"]]
+    flag = np.ascontiguousarray(geo["flag"], dtype=np.uint32)
+    vf = np.ascontiguousarray(geo["vfrac"], dtype=np.float64)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    n = lib.orc_hydro_box_eb(C.byref(p), I3(*bx_lo), I3(*bx_hi), I3(*dom_lo), I3(*dom_hi),
+                             I3(*bclo), I3(*bchi), I3(*periodic), P(uin), I3(*g_lo), I3(*g_hi),
+                             P(flag), P(vf), P(arr[0]), P(arr[1]), P(arr[2]), P(fcs[0]),
+                             P(fcs[1]), P(fcs[2]), int(redist), int(weights_type), P(dsdt),
+                             P(flx[0]), P(flx[1]), P(flx[2]), _D3(*dx), C.c_double(dt))
+    return dsdt, flx, n
+
+
 def lib_path(kind):
     if kind == "restate":
         return os.path.join(HERE, "_lib", "libcamr_oracle.so")

@@ -130,6 +130,23 @@ long orc_amr_run(const orc_params* p, const orc_level* lev0, int nbox, const int
                  double* S0, double* S1, int nsteps, int do_init, int first_step,
                  double* clock, double* dt_hist);
 
+/* Per-box EB hydro, MOL (oracle/_ref/libcamr_ref_eb.so only): the
+ * reference's EB kernels (hydro_ctoprim, MOL_umeth_eb, adjust_fluxes_eb,
+ * hydro_consup_eb) in hydro_umdrv_eb's order, then flux redistribution
+ * (redist = 1, restated) or none (redist = 0).  uin, flag, vfrac cover G =
+ * [g_lo, g_hi] (at least grow(bx, 5)); ap[d] and fc[d] (2 comps) cover
+ * surroundingNodes(G, d).  flag: bits 0-1 type (0 regular, 1 cut, 3
+ * covered), bit 2 + (di+1) + 3(dj+1) + 9(dk+1) connectivity.  dsdt (bx) is
+ * overwritten; flx[d] receive the face-centroid fluxes of bx's faces. */
+long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const int bx_hi[3],
+                      const int dom_lo[3], const int dom_hi[3], const int bclo[3],
+                      const int bchi[3], const int periodic[3], const double* uin,
+                      const int g_lo[3], const int g_hi[3], const unsigned* flag,
+                      const double* vfrac, const double* ap0, const double* ap1,
+                      const double* ap2, const double* fc0, const double* fc1, const double* fc2,
+                      int redist, int weights_type, double* dsdt, double* flx0, double* flx1,
+                      double* flx2, const double dx[3], double dt);
+
 /* clean_state on the valid cells (Source/CAMR.cpp:1253-1262). */
 void orc_clean_state(const orc_params* p, const orc_level* lev, double* state);
 
