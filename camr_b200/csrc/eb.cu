@@ -1,0 +1,627 @@
+// Embedded-boundary hydro of one box, MOL (SSP-RK2 right-hand side):
+// hydro_umdrv_eb with do_mol = 1 (Source/Hydro/Hydro_umdrv_eb.cpp:14-191)
+// and flux redistribution, as one stream of kernels:
+//
+//   K1 ctoprim            cells of grow(bx,5); covered cells get q = 0
+//                         (CAMR_construct_hydro_source.cpp:101-111)
+//   K2 EB slopes          cells of grow(bx,3), per direction; zero unless
+//                         both neighbours are connected (MOL_hydro_eb_K.H)
+//   K3 faces              faces of grow(bx,2), transverse +1: edge states +
+//                         Riemann on connected faces, else zero
+//                         (MOL/MOL_umeth_eb.cpp:21-191)
+//   K4 EB div u           nodes of grow(bx,4) inside the (periodically grown)
+//                         domain (Hydro_utils_eb_K.H:31-78)
+//   K5 adjust             artificial viscosity on every face of the flux
+//                         box; species normalisation and area on open faces
+//                         (Hydro_adjust_fluxes.cpp:48-171)
+//   K6 divergence         cells of grow(bx,2): face-centroid interpolated
+//                         fluxes, the wall flux of cut cells, -div, p div u,
+//                         the redistribution weight (Hydro_consup.cpp:29-98,
+//                         Hydro_utils_eb_K.H:82-575, Hydro_hypflux_eb_K.H)
+//   K7/K8 redistribution  flux redistribution (restated AMReX FluxRedist):
+//                         per cut cell of grow(bx,1) the neighbourhood
+//                         average and the mass to move, then each cell of bx
+//                         gathers what its cut neighbours send, in raster
+//                         order of the senders.
+//
+// Geometry (flags, volume and area fractions, face centroids) comes from
+// the caller over a region G covering grow(bx,5).
+#include <cuda_runtime.h>
+
+#include <new>
+
+#include "cell_point.cuh"
+#include "hydro_kernels.cuh"
+
+namespace camr {
+namespace {
+
+constexpr int kEB = 128;
+
+__device__ __forceinline__ int64_t etid() { return int64_t(blockIdx.x) * blockDim.x + threadIdx.x; }
+inline unsigned eblk(int64_t n) { return unsigned((n + kEB - 1) / kEB); }
+
+__device__ __forceinline__ bool f_covered(unsigned w) { return (w & 3u) == 3u; }
+__device__ __forceinline__ bool f_regular(unsigned w) { return (w & 3u) == 0u; }
+__device__ __forceinline__ bool f_single(unsigned w) { return (w & 3u) == 1u; }
+__device__ __forceinline__ bool f_conn(unsigned w, int di, int dj, int dk) {
+  return (w >> (2 + (di + 1) + 3 * (dj + 1) + 9 * (dk + 1))) & 1u;
+}
+
+// Geometry views over G (cells) and surroundingNodes(G, d) (faces).
+struct EBG {
+  const unsigned* flag;
+  const double* vfrac;
+  const double* ap[3];
+  const double* fc[3];
+  int lo[3], n[3];
+  __device__ __forceinline__ int64_t c(int i, int j, int k) const {
+    return (i - lo[0]) + int64_t(n[0]) * ((j - lo[1]) + int64_t(n[1]) * (k - lo[2]));
+  }
+  __device__ __forceinline__ int64_t f(int d, int i, int j, int k) const {
+    const int nx = n[0] + (d == 0), ny = n[1] + (d == 1);
+    return (i - lo[0]) + int64_t(nx) * ((j - lo[1]) + int64_t(ny) * (k - lo[2]));
+  }
+  __device__ __forceinline__ int64_t fn(int d) const {
+    return int64_t(n[0] + (d == 0)) * (n[1] + (d == 1)) * (n[2] + (d == 2));
+  }
+  __device__ __forceinline__ unsigned fl(int i, int j, int k) const { return flag[c(i, j, k)]; }
+  __device__ __forceinline__ double vf(int i, int j, int k) const { return vfrac[c(i, j, k)]; }
+  __device__ __forceinline__ double a(int d, int i, int j, int k) const { return ap[d][f(d, i, j, k)]; }
+  __device__ __forceinline__ double fcv(int d, int comp, int i, int j, int k) const {
+    return fc[d][f(d, i, j, k) + comp * fn(d)];
+  }
+};
+
+struct EBWork {
+  Space s;  // bx grown by 5 (+1 face layer)
+  double *q, *sl[3], *ft[3], *qf[3], *divu, *divc, *wt, *optmp, *delm, *wtinv;
+};
+
+__global__ void __launch_bounds__(kEB) k_eb_ctoprim(Region r, EBWork W, EBG G, DFab u, KParams P,
+                                                     DevError* err) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const Space& s = W.s;
+  if (f_covered(G.fl(i, j, k))) {
+    const int64_t at = s.idx(i, j, k);
+    for (int n = 0; n < SQ_N; ++n) W.q[at + n * s.sn] = 0.;
+    return;
+  }
+  ctoprim_body(i, j, k, s, u, u, false, P, W.q, nullptr, err);
+}
+
+template <int d>
+__device__ __forceinline__ void eb_slope_cell(int i, int j, int k, const EBWork& W, const EBG& G,
+                                              const KParams& P) {
+  const unsigned w = G.fl(i, j, k);
+  if (f_covered(w)) return;
+  constexpr int e0 = (d == 0), e1 = (d == 1), e2 = (d == 2);
+  const bool left_ok = f_conn(w, -e0, -e1, -e2) && !f_covered(G.fl(i - e0, j - e1, k - e2));
+  const bool rght_ok = f_conn(w, e0, e1, e2) && !f_covered(G.fl(i + e0, j + e1, k + e2));
+  if (left_ok && rght_ok) {
+    mol_slope_body<d>(i, j, k, W.s, P, W.q, W.sl[d]);
+  } else {
+    const int64_t at = W.s.idx(i, j, k);
+    for (int n = 0; n < SL_N; ++n) W.sl[d][at + n * W.s.sn] = 0.;
+  }
+}
+
+__global__ void __launch_bounds__(kEB) k_eb_slope(Region r, EBWork W, EBG G, KParams P) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  switch (blockIdx.y) {
+    case 0: eb_slope_cell<0>(i, j, k, W, G, P); break;
+    case 1: eb_slope_cell<1>(i, j, k, W, G, P); break;
+    default: eb_slope_cell<2>(i, j, k, W, G, P); break;
+  }
+}
+
+template <int d>
+__device__ __forceinline__ void eb_face(int i, int j, int k, const EBWork& W, const EBG& G,
+                                        const KGeom& g, const KParams& P) {
+  constexpr int e0 = (d == 0), e1 = (d == 1), e2 = (d == 2);
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  if (f_conn(G.fl(i, j, k), -e0, -e1, -e2) && !f_covered(G.fl(i - e0, j - e1, k - e2))) {
+    double f[NVAR], qpres, qun;
+    mol_edges_cmpflx<d>(i, j, k, s, g, P, W.q, W.sl[d], f, qpres, qun);
+    for (int n = 0; n < NVAR; ++n) W.ft[d][at + n * s.sn] = f[n];
+    W.qf[d][at] = qpres;
+    W.qf[d][at + s.sn] = qun;
+  } else {
+    W.qf[d][at] = 0.;
+    W.qf[d][at + s.sn] = 0.;
+  }
+  W.ft[d][at + UTEMP * s.sn] = 0.0;
+}
+
+__global__ void __launch_bounds__(kEB) k_eb_face(Region r0, Region r1, Region r2, EBWork W, EBG G,
+                                                  KGeom g, KParams P) {
+  int i, j, k;
+  const int64_t t = etid();
+  switch (blockIdx.y) {
+    case 0: if (region_cell(r0, t, i, j, k)) eb_face<0>(i, j, k, W, G, g, P); break;
+    case 1: if (region_cell(r1, t, i, j, k)) eb_face<1>(i, j, k, W, G, g, P); break;
+    default: if (region_cell(r2, t, i, j, k)) eb_face<2>(i, j, k, W, G, g, P); break;
+  }
+}
+
+// eb_divu (Hydro_utils_eb_K.H:31-78) at node (i,j,k).
+__global__ void __launch_bounds__(kEB) k_eb_divu(Region r, EBWork W, EBG G, KGeom g) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const Space& s = W.s;
+  const double surrounding_vol = G.vf(i, j, k) + G.vf(i - 1, j, k) + G.vf(i, j - 1, k) +
+                                 G.vf(i - 1, j - 1, k) + G.vf(i, j, k - 1) +
+                                 G.vf(i - 1, j, k - 1) + G.vf(i, j - 1, k - 1) +
+                                 G.vf(i - 1, j - 1, k - 1);
+  const double cutoff = 8.0 * (1.0 - 1.e-12);
+  double dv = 0.0;
+  if (surrounding_vol >= cutoff) {
+    auto Q = [&](int ii, int jj, int kk, int n) { return W.q[s.idx(ii, jj, kk) + n * s.sn]; };
+    const double dxinv0 = 1. / g.dx[0], dxinv1 = 1. / g.dx[1], dxinv2 = 1. / g.dx[2];
+    const double ux = 0.25 *
+        (Q(i, j, k, SQ_U) - Q(i - 1, j, k, SQ_U) + Q(i, j, k - 1, SQ_U) -
+         Q(i - 1, j, k - 1, SQ_U) + Q(i, j - 1, k, SQ_U) - Q(i - 1, j - 1, k, SQ_U) +
+         Q(i, j - 1, k - 1, SQ_U) - Q(i - 1, j - 1, k - 1, SQ_U)) * dxinv0;
+    const double vy = 0.25 *
+        (Q(i, j, k, SQ_V) - Q(i, j - 1, k, SQ_V) + Q(i, j, k - 1, SQ_V) -
+         Q(i, j - 1, k - 1, SQ_V) + Q(i - 1, j, k, SQ_V) - Q(i - 1, j - 1, k, SQ_V) +
+         Q(i - 1, j, k - 1, SQ_V) - Q(i - 1, j - 1, k - 1, SQ_V)) * dxinv1;
+    const double wz = 0.25 *
+        (Q(i, j, k, SQ_W) - Q(i, j, k - 1, SQ_W) + Q(i - 1, j, k, SQ_W) -
+         Q(i - 1, j, k - 1, SQ_W) + Q(i, j - 1, k, SQ_W) - Q(i, j - 1, k - 1, SQ_W) +
+         Q(i - 1, j - 1, k, SQ_W) - Q(i - 1, j - 1, k - 1, SQ_W)) * dxinv2;
+    dv = ux + vy + wz;
+  }
+  W.divu[s.idx(i, j, k)] = dv;
+}
+
+// adjust_fluxes_eb on one face: hydro_artif_visc, then (open faces)
+// hydro_norm_spec_flx and hydro_ext_flx_eb.
+template <int d>
+__device__ __forceinline__ void eb_adjust(int i, int j, int k, const EBWork& W, const EBG& G,
+                                          const KGeom& g, const KParams& P, const DFab& u) {
+  const Space& s = W.s;
+  constexpr int e0 = (d == 0), e1 = (d == 1), e2 = (d == 2);
+  constexpr int t1 = (d == 0) ? 1 : 0;
+  constexpr int t2 = (d == 2) ? 1 : 2;
+  const int64_t st1 = (t1 == 0) ? 1 : (t1 == 1) ? s.sy : s.sz;
+  const int64_t st2 = (t2 == 0) ? 1 : (t2 == 1) ? s.sy : s.sz;
+  const int64_t at = s.idx(i, j, k);
+  double* fx = W.ft[d];
+  const double div = P.difmag * dmin(0.0, 0.25 * (W.divu[at] + W.divu[at + st1] +
+                                                   W.divu[at + st2] + W.divu[at + st1 + st2]));
+  const int idx = (d == 0) ? i : (d == 1) ? j : k;
+  const bool at_bndry = (idx == g.dlo[d] && g.bclo[d] == CAMR_BC_NOSLIPWALL) ||
+                        (idx == g.dhi[d] + 1 && g.bchi[d] == CAMR_BC_NOSLIPWALL);
+  for (int n = 0; n < NVAR; ++n) {
+    if (n == UTEMP) continue;
+    const bool is_tang_vel = (d == 0 && (n == UMY || n == UMZ)) ||
+                             (d == 1 && (n == UMX || n == UMZ)) ||
+                             (d == 2 && (n == UMX || n == UMY));
+    if (!(at_bndry && is_tang_vel))
+      fx[at + n * s.sn] += g.dx[d] * div * (u(i, j, k, n) - u(i - e0, j - e1, k - e2, n));
+  }
+  fx[at + UTEMP * s.sn] = 0.0;
+  if (G.a(d, i, j, k) > 0.) {
+    double summ = 0.0;
+    for (int n = UFS; n < UFS + NSPEC; ++n) summ += fx[at + n * s.sn];
+    const double fac = (summ != 0.0) ? fx[at + URHO * s.sn] / summ : 1.0;
+    for (int n = UFS; n < UFS + NSPEC; ++n) fx[at + n * s.sn] *= fac;
+    const double areafac = (d == 0) ? g.dx[1] * g.dx[2] : (d == 1) ? g.dx[0] * g.dx[2]
+                                                                   : g.dx[1] * g.dx[0];
+    for (int n = 0; n < NVAR; ++n) fx[at + n * s.sn] *= areafac;
+  }
+}
+
+__global__ void __launch_bounds__(kEB) k_eb_adjust(Region r0, Region r1, Region r2, EBWork W,
+                                                    EBG G, KGeom g, KParams P, DFab u) {
+  int i, j, k;
+  const int64_t t = etid();
+  switch (blockIdx.y) {
+    case 0: if (region_cell(r0, t, i, j, k)) eb_adjust<0>(i, j, k, W, G, g, P, u); break;
+    case 1: if (region_cell(r1, t, i, j, k)) eb_adjust<1>(i, j, k, W, G, g, P, u); break;
+    default: if (region_cell(r2, t, i, j, k)) eb_adjust<2>(i, j, k, W, G, g, P, u); break;
+  }
+}
+
+// Value of face array `a` (component comp of stride sn) at the centroid of
+// face (i,j,k) of direction d: bilinear blend with the neighbouring faces in
+// the transverse directions the centroid leans to, when connected.
+template <int d>
+__device__ __forceinline__ double face_centroid_value(const double* a, const Space& s,
+                                                      const EBG& G, int i, int j, int k,
+                                                      double aval) {
+  const double apv = G.a(d, i, j, k);
+  if (apv != 0.0 && apv != 1.0) {
+    constexpr int ta = (d == 0) ? 1 : 0;  // first transverse direction
+    constexpr int tb = (d == 2) ? 1 : 2;  // second
+    const double c0 = G.fcv(d, 0, i, j, k), c1 = G.fcv(d, 1, i, j, k);
+    const int oa = static_cast<int>(copysign(1.0, c0));
+    const int ob = static_cast<int>(copysign(1.0, c1));
+    int da[3] = {0, 0, 0}, db[3] = {0, 0, 0};
+    da[ta] = oa;
+    db[tb] = ob;
+    const unsigned w = G.fl(i, j, k);
+    const double fa = f_conn(w, da[0], da[1], da[2]) ? fabs(c0) : 0.0;
+    const double fb = f_conn(w, db[0], db[1], db[2]) ? fabs(c1) : 0.0;
+    const double va = a[s.idx(i + da[0], j + da[1], k + da[2])];
+    const double vb = a[s.idx(i + db[0], j + db[1], k + db[2])];
+    const double vab = a[s.idx(i + da[0] + db[0], j + da[1] + db[1], k + da[2] + db[2])];
+    aval = (1.0 - fa) * (1.0 - fb) * aval + fa * (1.0 - fb) * va + fb * (1.0 - fa) * vb +
+           fa * fb * vab;
+  }
+  return aval;
+}
+
+// Normal velocity at the centroid of face (ii,jj,kk) of direction dd from
+// the interface records (p, u_n) of the faces, or 0 on a closed face
+// (eb_pdivu, Hydro_utils_eb_K.H:171-270).
+template <int dd>
+__device__ __forceinline__ double pdivu_face(const double* qq, const Space& s, const EBG& G,
+                                             int ii, int jj, int kk) {
+  if (G.a(dd, ii, jj, kk) > 0.0)
+    return face_centroid_value<dd>(qq + s.sn, s, G, ii, jj, kk, qq[s.idx(ii, jj, kk) + s.sn]);
+  return 0.0;
+}
+
+// compute_hyp_wallflux (Hydro_hypflux_eb_K.H): the flux through the EB wall
+// of a cut cell from the Riemann problem (u_n, -u_n) with the wall normal
+// given by the area-fraction differences.
+__device__ __forceinline__ void wall_flux(const double* q, const Space& s, int64_t at,
+                                          double axm, double axp, double aym, double ayp,
+                                          double azm, double azp, const KParams& P,
+                                          double* fw) {
+  const double u = q[at + SQ_U * s.sn];
+  const double v = q[at + SQ_V * s.sn];
+  const double w = q[at + SQ_W * s.sn];
+  const double apnorm = sqrt((axm - axp) * (axm - axp) + (aym - ayp) * (aym - ayp) +
+                             (azm - azp) * (azm - azp));
+  const double apnorminv = 1. / apnorm;
+  const double un = u * (axm - axp) * apnorminv + v * (aym - ayp) * apnorminv +
+                    w * (azm - azp) * apnorminv;
+  const double rho = q[at + SQ_RHO * s.sn];
+  const double p = q[at + SQ_P * s.sn];
+  const double qrei = q[at + SQ_REINT * s.sn];
+  const double gamc = P.gamma;
+  const double cav = q[at + SQ_C * s.sn];
+  const double smallc = q[at + SQ_CSML * s.sn];
+  const ROut o = riemannus(rho, un, 0., 0., p, qrei, rho, -un, 0., 0., p, qrei, cav, gamc, gamc,
+                           P.small, smallc, P.small_dens, P.small_pres, P.smallu);
+  for (int n = 0; n < NVAR; ++n) fw[n] = 0.;
+  fw[URHO] = o.f_rho;
+  fw[UEDEN] = o.f_eden;
+  fw[UEINT] = o.f_eint;
+  fw[UMX] = (axm - axp) * o.f_un;
+  fw[UMY] = (aym - ayp) * o.f_un;
+  fw[UMZ] = (azm - azp) * o.f_un;
+}
+
+// eb_compute_div for all components + eb_pdivu + the redistribution weight
+// of one cell of grow(bx,2); writes the face-centroid fluxes of bx's faces.
+__global__ void __launch_bounds__(kEB) k_eb_div(Region r, EBWork W, EBG G, KGeom g, KParams P,
+                                                 DFab fo0, DFab fo1, DFab fo2, int wtype) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const unsigned w = G.fl(i, j, k);
+  if (f_covered(w)) return;
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  const bool valid_cell = g.lo[0] <= i && i <= g.hi[0] && g.lo[1] <= j && j <= g.hi[1] &&
+                          g.lo[2] <= k && k <= g.hi[2];
+  const bool x_high = (i == g.hi[0]), y_high = (j == g.hi[1]), z_high = (k == g.hi[2]);
+  const double dxinv0 = 1. / g.dx[0], dxinv1 = 1. / g.dx[1], dxinv2 = 1. / g.dx[2];
+  const double cell_vol_inv = dxinv0 * dxinv1 * dxinv2;
+  const double* fx = W.ft[0];
+  const double* fy = W.ft[1];
+  const double* fz = W.ft[2];
+  const int64_t sx = 1, sy = s.sy, sz = s.sz;
+  if (f_regular(w)) {
+    for (int n = 0; n < NVAR; ++n) {
+      const int64_t o = at + n * s.sn;
+      double dv = cell_vol_inv * (fx[o + sx] - fx[o]) + cell_vol_inv * (fy[o + sy] - fy[o]) +
+                  cell_vol_inv * (fz[o + sz] - fz[o]);
+      W.divc[o] = dv * -1.0;
+      if (valid_cell) {
+        fo0(i, j, k, n) = fx[o];
+        fo1(i, j, k, n) = fy[o];
+        fo2(i, j, k, n) = fz[o];
+        if (x_high) fo0(i + 1, j, k, n) = fx[o + sx];
+        if (y_high) fo1(i, j + 1, k, n) = fy[o + sy];
+        if (z_high) fo2(i, j, k + 1, n) = fz[o + sz];
+      }
+    }
+  } else {
+    double fw[NVAR];
+    wall_flux(W.q, s, at, G.a(0, i, j, k), G.a(0, i + 1, j, k), G.a(1, i, j, k),
+              G.a(1, i, j + 1, k), G.a(2, i, j, k), G.a(2, i, j, k + 1), P, fw);
+    const double vfc = G.vf(i, j, k);
+    for (int n = 0; n < NVAR; ++n) {
+      const int64_t o = at + n * s.sn;
+      const double* ax = fx + n * s.sn;
+      const double* ay = fy + n * s.sn;
+      const double* az = fz + n * s.sn;
+      const double fxm = face_centroid_value<0>(ax, s, G, i, j, k, fx[o]);
+      const double fxp = face_centroid_value<0>(ax, s, G, i + 1, j, k, fx[o + sx]);
+      const double fym = face_centroid_value<1>(ay, s, G, i, j, k, fy[o]);
+      const double fyp = face_centroid_value<1>(ay, s, G, i, j + 1, k, fy[o + sy]);
+      const double fzm = face_centroid_value<2>(az, s, G, i, j, k, fz[o]);
+      const double fzp = face_centroid_value<2>(az, s, G, i, j, k + 1, fz[o + sz]);
+      if (valid_cell) {
+        fo0(i, j, k, n) = fxm;
+        fo1(i, j, k, n) = fym;
+        fo2(i, j, k, n) = fzm;
+        if (x_high) fo0(i + 1, j, k, n) = fxp;
+        if (y_high) fo1(i, j + 1, k, n) = fyp;
+        if (z_high) fo2(i, j, k + 1, n) = fzp;
+      }
+      double dv = cell_vol_inv / vfc *
+                  (G.a(0, i + 1, j, k) * fxp - G.a(0, i, j, k) * fxm + G.a(1, i, j + 1, k) * fyp -
+                   G.a(1, i, j, k) * fym + G.a(2, i, j, k + 1) * fzp - G.a(2, i, j, k) * fzm);
+      dv += fw[n] * dxinv0 / vfc;
+      W.divc[o] = dv * -1.0;
+    }
+  }
+  // p div u (eb_pdivu)
+  const double* q1 = W.qf[0];
+  const double* q2 = W.qf[1];
+  const double* q3 = W.qf[2];
+  const int64_t sn = s.sn;
+  if (f_regular(w)) {
+    const double pdivu =
+        0.5 * ((q1[at + sx] + q1[at]) * (q1[at + sx + sn] - q1[at + sn]) * dxinv0 +
+               (q2[at + sy] + q2[at]) * (q2[at + sy + sn] - q2[at + sn]) * dxinv1 +
+               (q3[at + sz] + q3[at]) * (q3[at + sz + sn] - q3[at + sn]) * dxinv2);
+    W.divc[at + UEINT * sn] -= pdivu;
+  } else {
+    const double fxm = pdivu_face<0>(q1, s, G, i, j, k), fxp = pdivu_face<0>(q1, s, G, i + 1, j, k);
+    const double fym = pdivu_face<1>(q2, s, G, i, j, k), fyp = pdivu_face<1>(q2, s, G, i, j + 1, k);
+    const double fzm = pdivu_face<2>(q3, s, G, i, j, k), fzp = pdivu_face<2>(q3, s, G, i, j, k + 1);
+    W.divc[at + UEINT * sn] -=
+        (1.0 / G.vf(i, j, k)) * W.q[at + SQ_P * sn] *
+        (dxinv0 * (G.a(0, i + 1, j, k) * fxp - G.a(0, i, j, k) * fxm) +
+         dxinv1 * (G.a(1, i, j + 1, k) * fyp - G.a(1, i, j, k) * fym) +
+         dxinv2 * (G.a(2, i, j, k + 1) * fzp - G.a(2, i, j, k) * fzm));
+  }
+  double wv;
+  if (wtype == 0) {
+    wv = 1.0;
+  } else if (wtype == 1) {
+    const double uu = W.q[at + SQ_U * sn], vv = W.q[at + SQ_V * sn], ww = W.q[at + SQ_W * sn];
+    wv = W.q[at + SQ_RHO * sn] * (W.q[at + SQ_REINT * sn] + 0.5 * (uu * uu + vv * vv + ww * ww));
+  } else if (wtype == 2) {
+    wv = W.q[at + SQ_RHO * sn];
+  } else {
+    wv = G.vf(i, j, k);
+  }
+  W.wt[at] = wv;
+}
+
+// Domain grown by 2 in its periodic directions (the redistribution's dbox).
+struct DBox {
+  int lo[3], hi[3];
+  __device__ __forceinline__ bool has(int i, int j, int k) const {
+    return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+  }
+};
+
+// Flux redistribution, part 1 (cut cells of grow(bx,1)): divnc, the
+// cell's own correction optmp and the mass delm it sends, and the inverse
+// of its neighbourhood weight.
+__global__ void __launch_bounds__(kEB) k_eb_redist1(Region r, EBWork W, EBG G, DBox db) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const unsigned w = G.fl(i, j, k);
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  if (!f_single(w)) {
+    for (int n = 0; n < NVAR; ++n) W.delm[at + n * s.sn] = 0.0;
+    return;
+  }
+  double wtot = 0.0;
+  for (int kk = -1; kk <= 1; ++kk)
+    for (int jj = -1; jj <= 1; ++jj)
+      for (int ii = -1; ii <= 1; ++ii)
+        if (f_conn(w, ii, jj, kk) && db.has(i + ii, j + jj, k + kk))
+          wtot += G.vf(i + ii, j + jj, k + kk) * W.wt[s.idx(i + ii, j + jj, k + kk)];
+  W.wtinv[at] = 1.0 / wtot;
+  for (int n = 0; n < NVAR; ++n) {
+    double divnc = 0.0, vtot = 0.0;
+    for (int kk = -1; kk <= 1; ++kk)
+      for (int jj = -1; jj <= 1; ++jj)
+        for (int ii = -1; ii <= 1; ++ii)
+          if (f_conn(w, ii, jj, kk) && db.has(i + ii, j + jj, k + kk)) {
+            const double wf = G.vf(i + ii, j + jj, k + kk);
+            vtot += wf;
+            divnc += wf * W.divc[s.idx(i + ii, j + jj, k + kk) + n * s.sn];
+          }
+    divnc /= vtot;
+    const double vfc = G.vf(i, j, k);
+    const double op = (1.0 - vfc) * (divnc - W.divc[at + n * s.sn]);
+    W.optmp[at + n * s.sn] = op;
+    W.delm[at + n * s.sn] = -vfc * op;
+  }
+}
+
+// Part 2 (cells of bx): gather the mass the cut cells of the neighbourhood
+// send (senders in raster order), and the final dSdt.
+__global__ void __launch_bounds__(kEB) k_eb_redist2(Region r, EBWork W, EBG G, DBox db,
+                                                     KGeom g, DFab dsdt, int redist) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  const unsigned wc = G.fl(i, j, k);
+  if (f_covered(wc)) {
+    for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = 0.0;
+    return;
+  }
+  if (!redist) {
+    for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = W.divc[at + n * s.sn];
+    return;
+  }
+  const bool recv = db.has(i, j, k);
+  const double wtc = W.wt[at];
+  for (int n = 0; n < NVAR; ++n) {
+    double acc = f_single(wc) ? W.optmp[at + n * s.sn] : 0.0;
+    if (recv) {
+      for (int kk = -1; kk <= 1; ++kk)
+        for (int jj = -1; jj <= 1; ++jj)
+          for (int ii = -1; ii <= 1; ++ii) {
+            const int si = i + ii, sj = j + jj, sk = k + kk;
+            if (si < g.lo[0] - 1 || si > g.hi[0] + 1 || sj < g.lo[1] - 1 || sj > g.hi[1] + 1 ||
+                sk < g.lo[2] - 1 || sk > g.hi[2] + 1)
+              continue;
+            const unsigned ws = G.fl(si, sj, sk);
+            if (!f_single(ws) || !f_conn(ws, -ii, -jj, -kk)) continue;
+            const int64_t as = s.idx(si, sj, sk);
+            acc += W.delm[as + n * s.sn] * W.wtinv[as] * wtc;
+          }
+    }
+    dsdt(i, j, k, n) = W.divc[at + n * s.sn] + acc;
+  }
+}
+
+__global__ void __launch_bounds__(kEB) k_eb_zero_faces(Region r, DFab f) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  for (int n = 0; n < NVAR; ++n) f(i, j, k, n) = 0.0;
+}
+
+}  // namespace
+}  // namespace camr
+
+using namespace camr;
+
+extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3],
+                                           const camr_geom* geom, const camr_fab* uin,
+                                           const camr_eb_geom* eb, camr_fab* dsdt,
+                                           camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                                           const camr_hydro_params* p, int redist, double dt,
+                                           void* stream) {
+  (void)dt;
+  if (!bx_lo || !bx_hi || !geom || !uin || !eb || !dsdt || !flx0 || !flx1 || !flx2 || !p)
+    return CAMR_ERR_INVALID;
+  if (!p->do_mol || p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  for (int d = 0; d < 3; ++d) {
+    if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
+    if (uin->lo[d] > bx_lo[d] - 5 || uin->hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
+    if (eb->g_lo[d] > bx_lo[d] - 5 || eb->g_hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
+  }
+  if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
+      !eb->fc[1] || !eb->fc[2])
+    return CAMR_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  EBWork W;
+  for (int d = 0; d < 3; ++d) {
+    W.s.lo[d] = bx_lo[d] - 5;
+    W.s.n[d] = bx_hi[d] - bx_lo[d] + 1 + 11;
+  }
+  W.s.sy = W.s.n[0];
+  W.s.sz = W.s.sy * W.s.n[1];
+  W.s.sn = W.s.sz * W.s.n[2];
+  const int ncomp = SQ_N + 3 * SL_N + 3 * NVAR + 3 * 2 + 1 + NVAR + 1 + 2 * NVAR + 1;
+  const size_t bytes = size_t(ncomp) * W.s.sn * sizeof(double);
+  double* base = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess)
+    return CAMR_ERR_NOMEM;
+  cudaError_t e = cudaMemsetAsync(base, 0, bytes, st);
+  double* ptr = base;
+  auto take = [&](int nc) {
+    double* r = ptr;
+    ptr += size_t(nc) * W.s.sn;
+    return r;
+  };
+  W.q = take(SQ_N);
+  for (int d = 0; d < 3; ++d) W.sl[d] = take(SL_N);
+  for (int d = 0; d < 3; ++d) W.ft[d] = take(NVAR);
+  for (int d = 0; d < 3; ++d) W.qf[d] = take(2);
+  W.divu = take(1);
+  W.divc = take(NVAR);
+  W.wt = take(1);
+  W.optmp = take(NVAR);
+  W.delm = take(NVAR);
+  W.wtinv = take(1);
+  EBG G;
+  G.flag = eb->flag;
+  G.vfrac = eb->vfrac;
+  for (int d = 0; d < 3; ++d) {
+    G.ap[d] = eb->ap[d];
+    G.fc[d] = eb->fc[d];
+    G.lo[d] = eb->g_lo[d];
+    G.n[d] = eb->g_hi[d] - eb->g_lo[d] + 1;
+  }
+  KGeom g;
+  for (int d = 0; d < 3; ++d) {
+    g.lo[d] = bx_lo[d];
+    g.hi[d] = bx_hi[d];
+    g.dlo[d] = geom->dom_lo[d];
+    g.dhi[d] = geom->dom_hi[d];
+    g.bclo[d] = geom->bc_lo[d];
+    g.bchi[d] = geom->bc_hi[d];
+    g.dx[d] = geom->dx[d];
+  }
+  const KParams P = make_kparams(*p);
+  const DFab U = make_dfab(*uin);
+  auto reg = [&](int grow_lo, int grow_hi, int fdir, int tgrow) {
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+      const int gr = (d == fdir) ? 0 : tgrow;
+      lo[d] = bx_lo[d] - grow_lo - gr;
+      hi[d] = bx_hi[d] + grow_hi + gr + (d == fdir ? 1 : 0);
+    }
+    return make_region(lo, hi);
+  };
+  // zero the output faces (covered cells leave theirs untouched)
+  DFab fo[3] = {make_dfab(*flx0), make_dfab(*flx1), make_dfab(*flx2)};
+  for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
+    const Region rf = reg(0, 0, d, 0);
+    k_eb_zero_faces<<<eblk(rf.count()), kEB, 0, st>>>(rf, fo[d]);
+  }
+  const Region r5 = reg(5, 5, -1, 0);
+  k_eb_ctoprim<<<eblk(r5.count()), kEB, 0, st>>>(r5, W, G, U, P, nullptr);
+  const Region r3 = reg(3, 3, -1, 0);
+  k_eb_slope<<<dim3(eblk(r3.count()), 3), kEB, 0, st>>>(r3, W, G, P);
+  Region rf[3], ra[3];
+  int64_t mf = 0, ma = 0;
+  for (int d = 0; d < 3; ++d) {
+    rf[d] = reg(2, 2, d, 1);  // faces of grow(bx,2), transverse +1
+    ra[d] = reg(3, 3, d, 0);  // faces of grow(bx,3)
+    mf = rf[d].count() > mf ? rf[d].count() : mf;
+    ma = ra[d].count() > ma ? ra[d].count() : ma;
+  }
+  k_eb_face<<<dim3(eblk(mf), 3), kEB, 0, st>>>(rf[0], rf[1], rf[2], W, G, g, P);
+  // nodes of grow(bx,4) inside the domain grown by 16 in periodic directions
+  int nlo[3], nhi[3];
+  for (int d = 0; d < 3; ++d) {
+    nlo[d] = bx_lo[d] - 4;
+    nhi[d] = bx_hi[d] + 5;
+    const int glo = geom->is_periodic[d] ? geom->dom_lo[d] - 16 : geom->dom_lo[d];
+    const int ghi = geom->is_periodic[d] ? geom->dom_hi[d] + 1 + 16 : geom->dom_hi[d] + 1;
+    nlo[d] = nlo[d] > glo ? nlo[d] : glo;
+    nhi[d] = nhi[d] < ghi ? nhi[d] : ghi;
+  }
+  const Region rn = make_region(nlo, nhi);
+  if (rn.count() > 0) k_eb_divu<<<eblk(rn.count()), kEB, 0, st>>>(rn, W, G, g);
+  k_eb_adjust<<<dim3(eblk(ma), 3), kEB, 0, st>>>(ra[0], ra[1], ra[2], W, G, g, P, U);
+  const Region r2 = reg(2, 2, -1, 0);
+  k_eb_div<<<eblk(r2.count()), kEB, 0, st>>>(r2, W, G, g, P, fo[0], fo[1], fo[2], 2);
+  DBox db;
+  for (int d = 0; d < 3; ++d) {
+    db.lo[d] = geom->is_periodic[d] ? geom->dom_lo[d] - 2 : geom->dom_lo[d];
+    db.hi[d] = geom->is_periodic[d] ? geom->dom_hi[d] + 2 : geom->dom_hi[d];
+  }
+  if (redist) {
+    const Region r1 = reg(1, 1, -1, 0);
+    k_eb_redist1<<<eblk(r1.count()), kEB, 0, st>>>(r1, W, G, db);
+  }
+  const Region r0 = reg(0, 0, -1, 0);
+  k_eb_redist2<<<eblk(r0.count()), kEB, 0, st>>>(r0, W, G, db, g, make_dfab(*dsdt), redist);
+  count_launch(redist ? 12 : 11);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaError_t e2 = cudaFreeAsync(base, st);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  return cuda_status_of(e2);
+}

@@ -1,4 +1,5 @@
 #include "hydro_kernels.cuh"
+#include "cell_point.cuh"
 
 namespace camr {
 
@@ -6,8 +7,10 @@ namespace {
 
 constexpr int kBlock = 128;
 
-// Minimum resident blocks per SM of the heavy kernels (register budget);
-// chosen by measurement (see the tuning notes in the design document).
+// Minimum resident blocks per SM of the heavy kernels (register budget):
+// 4 for trace and flux3 (128 registers per thread) gave the shortest 256^3
+// CTU-PPM step on B200 among 1/2/4; flux1 and flux2 keep their natural
+// register count.
 #ifndef CAMR_MINB_TRACE
 #define CAMR_MINB_TRACE 4
 #endif
@@ -25,90 +28,6 @@ inline unsigned grid_for(int64_t n) { return unsigned((n + kBlock - 1) / kBlock)
 
 __device__ __forceinline__ int64_t gtid() {
   return int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-}
-
-__device__ __forceinline__ void load_es(const double* a, const Space& s, int64_t at, double* r) {
-#pragma unroll
-  for (int n = 0; n < ES_N; ++n) r[n] = a[at + n * s.sn];
-}
-__device__ __forceinline__ void store_es(double* a, const Space& s, int64_t at, const double* r) {
-#pragma unroll
-  for (int n = 0; n < ES_N; ++n) a[at + n * s.sn] = r[n];
-}
-__device__ __forceinline__ void load_fr(const double* a, const Space& s, int64_t at, double* r) {
-#pragma unroll
-  for (int n = 0; n < FR_N; ++n) r[n] = a[at + n * s.sn];
-}
-__device__ __forceinline__ CellAux load_aux(const double* q, const Space& s, int64_t at,
-                                            double gamma) {
-  CellAux a;
-  a.c = q[at + SQ_C * s.sn];
-  a.csml = q[at + SQ_CSML * s.sn];
-  a.gamc = gamma;  // qaux QGAMC = EOS::REY2Gam = gamma (Hydro_ctoprim.H:83,96)
-  return a;
-}
-
-// ---------------------------------------------------------------------------
-// K1: conservative -> primitive (Source/Hydro/Hydro_ctoprim.H:11-101) and,
-// with sources, primitive sources (:106-157).
-__device__ __forceinline__ void ctoprim_body(int i, int j, int k, const Space& s, const DFab& u,
-                                             const DFab& src, bool has_src, const KParams& P,
-                                             double* q, double* srcq, DevError* err) {
-  const int64_t at = s.idx(i, j, k);
-  const double rho = u(i, j, k, URHO);
-  if (!(rho > 0.)) {
-    // The reference leaves q untouched here; downstream use is undefined.
-    report_error(err, 1, i, j, k);
-    return;
-  }
-  const double rhoinv = 1.0 / rho;
-  const double vx = u(i, j, k, UMX) * rhoinv;
-  const double vy = u(i, j, k, UMY) * rhoinv;
-  const double vz = u(i, j, k, UMZ) * rhoinv;
-  const double kineng = 0.5 * rho * (vx * vx + vy * vy + vz * vz);
-  const double ueden = u(i, j, k, UEDEN);
-  const double ueint = u(i, j, k, UEINT);
-  if (!P.allow_negative_energy && (!(ueden > 0.) || !(ueint > 0.))) report_error(err, 1, i, j, k);
-  double e;
-  if ((ueden - kineng) / ueden > P.dual_energy_eta1) {
-    e = (ueden - kineng) * rhoinv;
-  } else {
-    e = ueint * rhoinv;
-  }
-  double y[NSPEC];
-#pragma unroll
-  for (int sp = 0; sp < NSPEC; ++sp) y[sp] = u(i, j, k, UFS + sp) * rhoinv;
-  const double p = (P.gamma - 1.0) * rho * e;
-  const double rhoe = e * rho;
-  const double cs = sqrt(P.gamma * p / rho);
-  q[at + SQ_RHO * s.sn] = rho;
-  q[at + SQ_U * s.sn] = vx;
-  q[at + SQ_V * s.sn] = vy;
-  q[at + SQ_W * s.sn] = vz;
-  q[at + SQ_P * s.sn] = p;
-  q[at + SQ_REINT * s.sn] = rhoe;
-#pragma unroll
-  for (int sp = 0; sp < NSPEC; ++sp) q[at + (SQ_FS + sp) * s.sn] = y[sp];
-  q[at + SQ_C * s.sn] = cs;
-  q[at + SQ_CSML * s.sn] = dmax(P.small_num, P.small_num * cs);
-  if (has_src) {
-    // hydro_srctoprim with the EOS derivatives of ctoprim
-    // (QDPDE = (gamma-1)*rho, QDPDR = (gamma-1)*e).
-    const double dpde = (P.gamma - 1.0) * rho;
-    const double dpdr = (P.gamma - 1.0) * e;
-    const double srcrho = src(i, j, k, URHO);
-    const double sq_reint = src(i, j, k, UEINT);
-    srcq[at + ES_RHO * s.sn] = srcrho;
-    srcq[at + ES_U * s.sn] = (src(i, j, k, UMX) - vx * srcrho) * rhoinv;
-    srcq[at + ES_V * s.sn] = (src(i, j, k, UMY) - vy * srcrho) * rhoinv;
-    srcq[at + ES_W * s.sn] = (src(i, j, k, UMZ) - vz * srcrho) * rhoinv;
-    srcq[at + ES_REINT * s.sn] = sq_reint;
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) {
-      srcq[at + (ES_FS + sp) * s.sn] = (src(i, j, k, UFS + sp) - y[sp] * srcrho) * rhoinv;
-    }
-    srcq[at + ES_P * s.sn] = dpde * (sq_reint - rhoe * srcrho * rhoinv) * rhoinv + dpdr * srcrho;
-  }
 }
 
 __global__ void __launch_bounds__(kBlock) k_ctoprim(Region r, Space s, DFab u, DFab src,
@@ -703,53 +622,6 @@ __global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX3) k_flux3(Region r0, Re
 }
 
 // ---------------------------------------------------------------------------
-// MOL slopes (Source/Hydro/MOL/MOL_hydro_K.H:24-255) of a cell in direction
-// blockIdx.y.  Slot 1 (entropy) is never read by mol_riemann_{x,y,z} and is
-// not produced.  Stored slots: 0, 2, 3, 4, QREINT, species.
-enum { SL_0 = 0, SL_2 = 1, SL_3 = 2, SL_4 = 3, SL_RE = 4, SL_FS = 5, SL_N = 8 };
-
-template <int d>
-__device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space& s,
-                                               const KParams& P, const double* q, double* o) {
-  const int64_t at = s.idx(i, j, k);
-  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
-  if (P.plm_iorder == 1) {
-#pragma unroll
-    for (int n = 0; n < SL_N; ++n) o[at + n * s.sn] = 0.;
-    return;
-  }
-  const double plm_theta = 2.0;
-  auto Q = [&](int off, int slot) { return q[at + off * st + slot * s.sn]; };
-  constexpr int un = SQ_U + d;
-  constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
-  constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
-  const double c = Q(0, SQ_C);
-  double dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
-  double drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
-  o[at + SL_0 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
-  const double cs2 = c * c;
-  dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
-  drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
-  o[at + SL_2 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
-  dlft = Q(0, t1) - Q(-1, t1);
-  drgt = Q(1, t1) - Q(0, t1);
-  o[at + SL_3 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
-  dlft = Q(0, t2) - Q(-1, t2);
-  drgt = Q(1, t2) - Q(0, t2);
-  o[at + SL_4 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
-  const double enth = (Q(0, SQ_REINT) + Q(0, SQ_P)) / dmax(Q(0, SQ_RHO), P.small_dens);
-  dlft = (Q(0, SQ_REINT) - Q(-1, SQ_REINT)) - enth * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
-  drgt = (Q(1, SQ_REINT) - Q(0, SQ_REINT)) - enth * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
-  o[at + SL_RE * s.sn] = mol_limiter(dlft, drgt, plm_theta);
-#pragma unroll
-  for (int sp = 0; sp < NSPEC; ++sp) {
-    const int n = SQ_FS + sp;
-    dlft = Q(0, SQ_RHO) * Q(0, n) - Q(-1, SQ_RHO) * Q(-1, n) - Q(0, n) * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
-    drgt = Q(1, SQ_RHO) * Q(1, n) - Q(0, SQ_RHO) * Q(0, n) - Q(0, n) * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
-    o[at + (SL_FS + sp) * s.sn] = mol_limiter(dlft, drgt, plm_theta);
-  }
-}
-
 __global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Region r2, Space s,
                                                        KParams P, const double* q,
                                                        Ptr3 slope) {
@@ -768,84 +640,15 @@ __global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Regi
   }
 }
 
-// MOL face pass: edge states of mol_riemann_{x,y,z} (MOL_riemann_K.H:12-488),
-// Riemann flux, then adjust_fluxes.
+// MOL face pass: edge states + Riemann (mol_edges_cmpflx), then adjust_fluxes.
 template <int d>
 __device__ __forceinline__ void mol_flux_body(int i, int j, int k, const Space& s,
                                               const KGeom& g, const KParams& P,
                                               const double* q, const double* sl,
                                               const double* divu, const DFab& uin, DFab flx,
                                               double* qfd) {
-  const int64_t at = s.idx(i, j, k);
-  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
-  const int64_t atL = at - st;
-  auto Q = [&](int64_t c, int slot) { return q[c + slot * s.sn]; };
-  auto S = [&](int64_t c, int slot) { return sl[c + slot * s.sn]; };
-  constexpr int un = SQ_U + d;
-  constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
-  constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
-  double ql[ES_N], qr[ES_N];
-  {
-    const double cspeed = Q(atL, SQ_C);
-    const double enth = (Q(atL, SQ_REINT) + Q(atL, SQ_P)) / dmax(Q(atL, SQ_RHO), P.small_dens);
-    const double d0 = S(atL, SL_0), d2 = S(atL, SL_2);
-    double pl = Q(atL, SQ_P) + 0.5 * (d0 + d2) * cspeed;
-    ql[ES_P] = dmax(pl, P.small_pres);
-    ql[ES_U + d] = Q(atL, un) + 0.5 * ((d2 - d0) / Q(atL, SQ_RHO));
-    ql[ES_U + (t1 - SQ_U)] = Q(atL, t1) + 0.5 * S(atL, SL_3);
-    ql[ES_U + (t2 - SQ_U)] = Q(atL, t2) + 0.5 * S(atL, SL_4);
-    double sum = 0.;
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) {
-      const double specden = Q(atL, SQ_RHO) * Q(atL, SQ_FS + sp) +
-                             0.5 * (S(atL, SL_FS + sp) + Q(atL, SQ_FS + sp) * (d0 + d2) / cspeed);
-      sum += specden;
-      ql[ES_FS + sp] = specden;
-    }
-    if (sum < P.small_dens) {
-      // The reference falls back to the RIGHT cell's species here
-      // (MOL_riemann_K.H:82-86).
-#pragma unroll
-      for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = Q(at, SQ_FS + sp);
-    } else {
-#pragma unroll
-      for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = ql[ES_FS + sp] / sum;
-    }
-    ql[ES_RHO] = dmax(sum, P.small_dens);
-    ql[ES_REINT] = Q(atL, SQ_REINT) + 0.5 * (S(atL, SL_RE) + enth * (d0 + d2) / cspeed);
-  }
-  {
-    const double cspeed = Q(at, SQ_C);
-    const double enth = (Q(at, SQ_REINT) + Q(at, SQ_P)) / dmax(Q(at, SQ_RHO), P.small_dens);
-    const double d0 = S(at, SL_0), d2 = S(at, SL_2);
-    double pr = Q(at, SQ_P) - 0.5 * (d0 + d2) * cspeed;
-    qr[ES_P] = dmax(pr, P.small_pres);
-    qr[ES_U + d] = Q(at, un) - 0.5 * ((d2 - d0) / Q(at, SQ_RHO));
-    qr[ES_U + (t1 - SQ_U)] = Q(at, t1) - 0.5 * S(at, SL_3);
-    qr[ES_U + (t2 - SQ_U)] = Q(at, t2) - 0.5 * S(at, SL_4);
-    double sum = 0.;
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) {
-      const double specden = Q(at, SQ_RHO) * Q(at, SQ_FS + sp) -
-                             0.5 * (S(at, SL_FS + sp) + Q(at, SQ_FS + sp) * (d0 + d2) / cspeed);
-      sum += specden;
-      qr[ES_FS + sp] = specden;
-    }
-    if (sum < P.small_dens) {
-#pragma unroll
-      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = Q(at, SQ_FS + sp);
-    } else {
-#pragma unroll
-      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = qr[ES_FS + sp] / sum;
-    }
-    qr[ES_RHO] = dmax(sum, P.small_dens);
-    qr[ES_REINT] = Q(at, SQ_REINT) - 0.5 * (S(at, SL_RE) + enth * (d0 + d2) / cspeed);
-  }
-  const CellAux aL = load_aux(q, s, atL, P.gamma);
-  const CellAux aR = load_aux(q, s, at, P.gamma);
-  const int idx = (d == 0) ? i : (d == 1) ? j : k;
   double f[NVAR], qpres, qun;
-  cmpflx<d>(ql, qr, aL, aR, idx, g.bclo[d], g.bchi[d], g.dlo[d], g.dhi[d], P, f, qpres, qun);
+  mol_edges_cmpflx<d>(i, j, k, s, g, P, q, sl, f, qpres, qun);
   face_adjust_and_store<d>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfd);
 }
 

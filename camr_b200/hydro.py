@@ -83,6 +83,52 @@ def hydro_umdrv(bx_lo, bx_hi, geom, uin, uin_lo, dsdt, flx, params, dt, src=None
     check(st, "camr_hydro_umdrv")
 
 
+def eb_geometry_to_device(geo, device="cuda"):
+    """eb_geometry.sphere_geometry output -> dict of CUDA tensors (kept
+    alive by the caller) and the camr_eb_geom struct pointing at them."""
+    torch = _torch()
+    t = {"flag": torch.from_numpy(geo["flag"].astype(np.int32)).to(device),
+         "vfrac": torch.from_numpy(geo["vfrac"]).to(device),
+         "ap": [torch.from_numpy(a).to(device) for a in geo["ap"]],
+         "fc": [torch.from_numpy(a).contiguous().to(device) for a in geo["fc"]]}
+    g = native.EBGeom()
+    g.flag = t["flag"].data_ptr()
+    g.vfrac = t["vfrac"].data_ptr()
+    for d in range(3):
+        g.ap[d] = t["ap"][d].data_ptr()
+        g.fc[d] = t["fc"][d].data_ptr()
+        g.g_lo[d] = geo["lo"][d]
+        g.g_hi[d] = geo["hi"][d]
+    t["struct"] = g
+    return t
+
+
+def hydro_umdrv_eb(bx_lo, bx_hi, geom, uin, uin_lo, ebdev, params, redist=True, dt=0.0,
+                   stream=None):
+    """EB per-box hydro (MOL) on CUDA tensors: uin (NVAR, ...) over a region
+    starting at uin_lo covering grow(bx, 5); ebdev from eb_geometry_to_device.
+    Returns (dsdt, [flx_x, flx_y, flx_z]) as new CUDA tensors."""
+    torch = _torch()
+    nb = [bx_hi[d] - bx_lo[d] + 1 for d in range(3)]
+    dsdt = torch.zeros((NVAR, nb[2], nb[1], nb[0]), dtype=torch.float64, device=uin.device)
+    flx = []
+    for d in range(3):
+        sh = list(nb)
+        sh[d] += 1
+        flx.append(torch.zeros((NVAR, sh[2], sh[1], sh[0]), dtype=torch.float64,
+                               device=uin.device))
+    lo3, hi3 = (C.c_int * 3)(*bx_lo), (C.c_int * 3)(*bx_hi)
+    fu = fab_of(uin, uin_lo)
+    fd = fab_of(dsdt, bx_lo)
+    ff = [fab_of(f, bx_lo) for f in flx]
+    check(lib().camr_hydro_umdrv_eb(C.byref(lo3), C.byref(hi3), C.byref(geom), C.byref(fu),
+                                    C.byref(ebdev["struct"]), C.byref(fd), C.byref(ff[0]),
+                                    C.byref(ff[1]), C.byref(ff[2]), C.byref(params),
+                                    int(bool(redist)), float(dt), C.c_void_p(_stream_ptr(stream))),
+          "camr_hydro_umdrv_eb")
+    return dsdt, flx
+
+
 class Level:
     """One uniform level advanced on the GPU through the C ABI."""
 

@@ -52,6 +52,11 @@ class BoxTask(C.Structure):
                 ("dsdt", Fab), ("flx", Fab * 3)]
 
 
+class EBGeom(C.Structure):
+    _fields_ = [("flag", C.c_void_p), ("vfrac", C.c_void_p), ("ap", C.c_void_p * 3),
+                ("fc", C.c_void_p * 3), ("g_lo", C.c_int * 3), ("g_hi", C.c_int * 3)]
+
+
 class LevelDesc(C.Structure):
     _fields_ = [("geom", Geom), ("max_grid_size", C.c_int * 3), ("use_graph", C.c_int)]
 
@@ -119,6 +124,11 @@ SIGNATURES = {
     "camr_amr_kernels_per_step": (C.c_int64, [C.c_void_p]),
     "camr_amr_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_amr_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
+    "camr_hydro_umdrv_eb": (C.c_int, [C.POINTER(C.c_int * 3), C.POINTER(C.c_int * 3),
+                                      C.POINTER(Geom), C.POINTER(Fab), C.POINTER(EBGeom),
+                                      C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
+                                      C.POINTER(Fab), C.POINTER(HydroParams), C.c_int,
+                                      C.c_double, C.c_void_p]),
     "camr_adjoint_create": (C.c_int, [C.POINTER(Geom), C.POINTER(HydroParams), C.c_int,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_adjoint_destroy": (C.c_int, [C.c_void_p]),

@@ -342,6 +342,36 @@ camr_status camr_adjoint_stream(camr_adjoint* a, void** stream);
 camr_status camr_adjoint_get_error(camr_adjoint* a, camr_error_info* info);
 
 /* ---------------------------------------------------------------------
+ * Embedded-boundary per-box hydro, MOL: hydro_umdrv_eb with do_mol = 1
+ * (Source/Hydro/Hydro_umdrv_eb.cpp:14-191) with flux redistribution
+ * (AMReX's FluxRedist, restated).  Geometry on a cell region G covering
+ * grow(bx, 5), device pointers, i fastest:
+ *   flag   G cells: bits 0-1 type (0 regular, 1 cut, 3 covered), bit
+ *          2 + (di+1) + 3 (dj+1) + 9 (dk+1) connectivity to neighbour
+ *          (di,dj,dk) (the cell itself included)
+ *   vfrac  G cells; ap[d] faces of G in direction d (surroundingNodes(G, d));
+ *   fc[d]  2 components (transverse directions in x, y, z order) on the
+ *          same faces, component planes outermost.
+ * uin covers grow(bx, 5).  dsdt (bx) is overwritten (the reference's
+ * redistribution writes it); flx[d] receive the face-centroid fluxes of
+ * bx's faces.  redist: 1 = flux redistribution, 0 = none.
+ */
+typedef struct {
+  const unsigned* flag;
+  const double* vfrac;
+  const double* ap[3];
+  const double* fc[3];
+  int g_lo[3];
+  int g_hi[3];
+} camr_eb_geom;
+
+camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3], const camr_geom* geom,
+                                const camr_fab* uin, const camr_eb_geom* eb, camr_fab* dsdt,
+                                camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                                const camr_hydro_params* p, int redist, double dt,
+                                void* stream);
+
+/* ---------------------------------------------------------------------
  * Allocation-free per-box hydro.  No counterpart in the reference: it is
  * camr_hydro_umdrv for callers that may not allocate device memory while
  * they run (code inside an arena or pool that owns all device memory,
