@@ -161,7 +161,14 @@ __device__ void adj_face_body(int i, int j, int k, const AdjGeom& G, const KPara
   atomic_add_cell(LB, uR, L.sn, bin.uR, NV);
 }
 
-__global__ void __launch_bounds__(kBlk) k_adj_face(Region r0, Region r1, Region r2, AdjGeom G,
+// Face VJP launch shape: 128 threads; the minimum resident blocks per SM
+// bounds the registers of this (register-heavy) kernel.
+#ifndef CAMR_ADJ_FACE_MINB
+#define CAMR_ADJ_FACE_MINB 2
+#endif
+constexpr int kFaceBlk = 128;
+
+__global__ void __launch_bounds__(kFaceBlk, CAMR_ADJ_FACE_MINB) k_adj_face(Region r0, Region r1, Region r2, AdjGeom G,
                                                     KParams P, const double* B, const double* q,
                                                     APtr3 sl, const double* divu, APtr3 qf,
                                                     const double* Ldsdt, double* Lq, APtr3 Lsl,
@@ -566,7 +573,8 @@ cudaError_t hydro_adj(camr_adjoint* a, const double* Bp, const Work& w, double* 
     mf = std::max(mf, rf[F].count());
     ms = std::max(ms, rs[F].count());
   }
-  k_adj_face<<<dim3(nblk(mf), 3), kBlk, 0, st>>>(rf[0], rf[1], rf[2], a->G, a->P, Bp, w.q, sl,
+  k_adj_face<<<dim3(unsigned((mf + kFaceBlk - 1) / kFaceBlk), 3), kFaceBlk, 0, st>>>(
+      rf[0], rf[1], rf[2], a->G, a->P, Bp, w.q, sl,
                                                  w.divu, qf, a->Ldsdt, a->Lq, Lsl, a->Ldivu,
                                                  LBp);
   k_adj_slope<<<dim3(nblk(ms), 3), kBlk, 0, st>>>(rs[0], rs[1], rs[2], s, a->P, w.q, Lsl, a->Lq);

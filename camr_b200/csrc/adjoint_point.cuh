@@ -222,8 +222,9 @@ CAMR_HD void riemann_vjp(const RIn& in, double gam, const Par& P, const RTape& t
   // frac = max(0, min(1, frac0))
   const double b_frac0 = (t.frac0 < 1.0 && 0.0 < t.frac0) ? b_frac : 0.0;
   const double b_ratio = 0.5 * b_frac0;
-  double b_spout = b_ratio / t.scr, b_spin = b_ratio / t.scr;
-  const double b_scr = -b_ratio * t.ratio / t.scr;
+  const double iscr = 1.0 / t.scr;
+  double b_spout = b_ratio * iscr, b_spin = b_ratio * iscr;
+  const double b_scr = -b_ratio * t.ratio * iscr;
   if (t.scr_zero) {
     bi.cav += b_scr * P.small;
   } else {
@@ -249,10 +250,11 @@ CAMR_HD void riemann_vjp(const RIn& in, double gam, const Par& P, const RTape& t
   else b_cstar0 = b_cstar;
   const double gamco = gam;
   if (t.cstar0 > 0.0) {
-    const double B = gamco * t.pstar / t.rstar;
+    const double irs = 1.0 / t.rstar;
+    const double B = gamco * t.pstar * irs;
     const double b_B = b_cstar0 * 0.5 / t.cstar0 * sgn(B);
-    b_pstar += b_B * gamco / t.rstar;
-    b_rstar += -b_B * B / t.rstar;
+    b_pstar += b_B * gamco * irs;
+    b_rstar += -b_B * B * irs;
   }
   // estar = reo + (pstar - po)*entho
   b_reo += b_estar;
@@ -299,8 +301,9 @@ CAMR_HD void riemann_vjp(const RIn& in, double gam, const Par& P, const RTape& t
   }
   // ustar = mask0 ? 0 : ustar0
   const double b_ustar0 = t.mask0 ? 0.0 : b_ustar;
-  const double b_numu = b_ustar0 / t.den;
-  double b_den = -b_ustar0 * t.ustar0 / t.den;
+  const double iden = 1.0 / t.den;
+  const double b_numu = b_ustar0 * iden;
+  double b_den = -b_ustar0 * t.ustar0 * iden;
   double b_wl = b_numu * in.ul, b_wr = b_numu * in.ur;
   bi.ul += b_numu * t.wl;
   bi.ur += b_numu * t.wr;
@@ -308,8 +311,8 @@ CAMR_HD void riemann_vjp(const RIn& in, double gam, const Par& P, const RTape& t
   b_pr -= b_numu;
   // pstar = max(pstar0, small_pres)
   const double b_pstar0 = (t.pstar0 < P.small_pres) ? 0.0 : b_pstar;
-  const double b_nump = b_pstar0 / t.den;
-  b_den += -b_pstar0 * t.pstar0 / t.den;
+  const double b_nump = b_pstar0 * iden;
+  b_den += -b_pstar0 * t.pstar0 * iden;
   b_wr += b_nump * t.pl;
   b_pl += b_nump * t.wr;
   b_wl += b_nump * t.pr;
@@ -419,16 +422,19 @@ CAMR_HD void edge_vjp(const double* q, const double* s, double sign, const Par& 
   constexpr int un = QU + d;
   constexpr int t1 = (d == 0) ? QV : QU;
   constexpr int t2 = (d == 2) ? QV : QW;
-  const double c = q[QC];
+  const double ic = 1.0 / q[QC];
+  const double ic2 = ic * ic;
+  const double ir = 1.0 / q[QR];
+  const double irden = 1.0 / t.rden;
   double b_a = 0.0, b_c = 0.0, b_enth = 0.0, b_sum = 0.0;
   // re
   bq[QRE] += be.re;
   {
     const double tt = sign * 0.5 * be.re;
     bs[SRE] += tt;
-    b_enth += tt * t.a / c;
-    b_a += tt * t.enth / c;
-    b_c += -tt * (t.enth * t.a) / (c * c);
+    b_enth += tt * t.a * ic;
+    b_a += tt * t.enth * ic;
+    b_c += -tt * (t.enth * t.a) * ic2;
   }
   // rho = max(sum, small_dens)
   if (!(t.sum < P.small_dens)) b_sum += be.rho;
@@ -437,9 +443,10 @@ CAMR_HD void edge_vjp(const double* q, const double* s, double sign, const Par& 
   if (t.fallback) {
     for (int sp = 0; sp < NSP; ++sp) byq[sp] += be.y[sp];
   } else {
+    const double isum = 1.0 / t.sum;
     for (int sp = 0; sp < NSP; ++sp) {
-      b_sd[sp] += be.y[sp] / t.sum;
-      b_sum += -be.y[sp] * e.y[sp] / t.sum;
+      b_sd[sp] += be.y[sp] * isum;
+      b_sum += -be.y[sp] * e.y[sp] * isum;
     }
   }
   for (int sp = 0; sp < NSP; ++sp) {
@@ -448,9 +455,9 @@ CAMR_HD void edge_vjp(const double* q, const double* s, double sign, const Par& 
     bq[QY + sp] += b * q[QR];
     const double tt = sign * 0.5 * b;
     bs[SY + sp] += tt;
-    bq[QY + sp] += tt * t.a / c;
-    b_a += tt * q[QY + sp] / c;
-    b_c += -tt * (q[QY + sp] * t.a) / (c * c);
+    bq[QY + sp] += tt * t.a * ic;
+    b_a += tt * q[QY + sp] * ic;
+    b_c += -tt * (q[QY + sp] * t.a) * ic2;
   }
   // transverse velocities
   bq[t1] += be.t1;
@@ -461,21 +468,21 @@ CAMR_HD void edge_vjp(const double* q, const double* s, double sign, const Par& 
   bq[un] += be.un;
   {
     const double tt = sign * 0.5 * be.un;
-    bs[S2] += tt / q[QR];
-    bs[S0] -= tt / q[QR];
-    bq[QR] += -tt * (s[S2] - s[S0]) / (q[QR] * q[QR]);
+    bs[S2] += tt * ir;
+    bs[S0] -= tt * ir;
+    bq[QR] += -tt * (s[S2] - s[S0]) * ir * ir;
   }
   // p = max(p0, small_pres)
   if (!(t.p0 < P.small_pres)) {
     const double b = be.p;
     bq[QP] += b;
-    b_a += sign * 0.5 * b * c;
+    b_a += sign * 0.5 * b * q[QC];
     b_c += sign * 0.5 * b * t.a;
   }
   // enth = (re + p)/max(rho, small_dens)
-  bq[QRE] += b_enth / t.rden;
-  bq[QP] += b_enth / t.rden;
-  if (!(q[QR] < P.small_dens)) bq[QR] += -b_enth * t.enth / t.rden;
+  bq[QRE] += b_enth * irden;
+  bq[QP] += b_enth * irden;
+  if (!(q[QR] < P.small_dens)) bq[QR] += -b_enth * t.enth * irden;
   bs[S0] += b_a;
   bs[S2] += b_a;
   bq[QC] += b_c;
@@ -557,8 +564,9 @@ CAMR_HD void face_vjp(const FaceIn& in, double dx, double area, const Par& P,
     }
   }
   if (t.summ != 0.0) {
-    b_f1[RHO] += b_fac / t.summ;
-    const double b_summ = -b_fac * t.fac / t.summ;
+    const double isumm = 1.0 / t.summ;
+    b_f1[RHO] += b_fac * isumm;
+    const double b_summ = -b_fac * t.fac * isumm;
     for (int n = FS; n < FS + NSP; ++n) b_f1[n] += b_summ;
   }
   b_f1[TEMP] = 0.0;
@@ -697,6 +705,10 @@ CAMR_HD void slope_vjp(const double* qm, const double* q0, const double* qp, con
   constexpr int t1 = (d == 0) ? QV : QU;
   constexpr int t2 = (d == 2) ? QV : QW;
   const double c = q0[QC];
+  const double ic = 1.0 / c;
+  const double ics2 = 1.0 / t.cs2;
+  const double ics4 = ics2 * ics2;
+  const double irden = 1.0 / t.rden;
   double b_c = 0.0, b_cs2 = 0.0, b_enth = 0.0;
   // species
   for (int sp = 0; sp < NSP; ++sp) {
@@ -708,38 +720,38 @@ CAMR_HD void slope_vjp(const double* qm, const double* q0, const double* qp, con
     bq0[n] += bdl * q0[QR];
     bqm[QR] -= bdl * qm[n];
     bqm[n] -= bdl * qm[QR];
-    bq0[n] -= bdl * (q0[QP] - qm[QP]) / t.cs2;
-    bq0[QP] -= bdl * q0[n] / t.cs2;
-    bqm[QP] += bdl * q0[n] / t.cs2;
-    b_cs2 += bdl * q0[n] * (q0[QP] - qm[QP]) / (t.cs2 * t.cs2);
+    bq0[n] -= bdl * (q0[QP] - qm[QP]) * ics2;
+    bq0[QP] -= bdl * q0[n] * ics2;
+    bqm[QP] += bdl * q0[n] * ics2;
+    b_cs2 += bdl * q0[n] * (q0[QP] - qm[QP]) * ics4;
     // dr = rp*yp - r0*y0 - y0*(pp-p0)/cs2
     bqp[QR] += bdr * qp[n];
     bqp[n] += bdr * qp[QR];
     bq0[QR] -= bdr * q0[n];
     bq0[n] -= bdr * q0[QR];
-    bq0[n] -= bdr * (qp[QP] - q0[QP]) / t.cs2;
-    bqp[QP] -= bdr * q0[n] / t.cs2;
-    bq0[QP] += bdr * q0[n] / t.cs2;
-    b_cs2 += bdr * q0[n] * (qp[QP] - q0[QP]) / (t.cs2 * t.cs2);
+    bq0[n] -= bdr * (qp[QP] - q0[QP]) * ics2;
+    bqp[QP] -= bdr * q0[n] * ics2;
+    bq0[QP] += bdr * q0[n] * ics2;
+    b_cs2 += bdr * q0[n] * (qp[QP] - q0[QP]) * ics4;
   }
   {
     double bdl = 0.0, bdr = 0.0;
     limiter_vjp(t.lt[SRE], bo[SRE], bdl, bdr);
     bq0[QRE] += bdl;
     bqm[QRE] -= bdl;
-    b_enth -= bdl * (q0[QP] - qm[QP]) / t.cs2;
-    bq0[QP] -= bdl * t.enth / t.cs2;
-    bqm[QP] += bdl * t.enth / t.cs2;
-    b_cs2 += bdl * t.enth * (q0[QP] - qm[QP]) / (t.cs2 * t.cs2);
+    b_enth -= bdl * (q0[QP] - qm[QP]) * ics2;
+    bq0[QP] -= bdl * t.enth * ics2;
+    bqm[QP] += bdl * t.enth * ics2;
+    b_cs2 += bdl * t.enth * (q0[QP] - qm[QP]) * ics4;
     bqp[QRE] += bdr;
     bq0[QRE] -= bdr;
-    b_enth -= bdr * (qp[QP] - q0[QP]) / t.cs2;
-    bqp[QP] -= bdr * t.enth / t.cs2;
-    bq0[QP] += bdr * t.enth / t.cs2;
-    b_cs2 += bdr * t.enth * (qp[QP] - q0[QP]) / (t.cs2 * t.cs2);
-    bq0[QRE] += b_enth / t.rden;
-    bq0[QP] += b_enth / t.rden;
-    if (!(q0[QR] < P.small_dens)) bq0[QR] += -b_enth * t.enth / t.rden;
+    b_enth -= bdr * (qp[QP] - q0[QP]) * ics2;
+    bqp[QP] -= bdr * t.enth * ics2;
+    bq0[QP] += bdr * t.enth * ics2;
+    b_cs2 += bdr * t.enth * (qp[QP] - q0[QP]) * ics4;
+    bq0[QRE] += b_enth * irden;
+    bq0[QP] += b_enth * irden;
+    if (!(q0[QR] < P.small_dens)) bq0[QR] += -b_enth * t.enth * irden;
   }
   {
     double bdl = 0.0, bdr = 0.0;
@@ -760,15 +772,15 @@ CAMR_HD void slope_vjp(const double* qm, const double* q0, const double* qp, con
     double bdl = 0.0, bdr = 0.0;
     limiter_vjp(t.lt[w == 0 ? S0 : S2], bo[w == 0 ? S0 : S2], bdl, bdr);
     // dl = 0.5*(p0-pm)/c + sg*0.5*r0*(u0-um)
-    bq0[QP] += bdl * 0.5 / c;
-    bqm[QP] -= bdl * 0.5 / c;
-    b_c += -bdl * 0.5 * (q0[QP] - qm[QP]) / (c * c);
+    bq0[QP] += bdl * 0.5 * ic;
+    bqm[QP] -= bdl * 0.5 * ic;
+    b_c += -bdl * 0.5 * (q0[QP] - qm[QP]) * ic * ic;
     bq0[QR] += bdl * sg * 0.5 * (q0[un] - qm[un]);
     bq0[un] += bdl * sg * 0.5 * q0[QR];
     bqm[un] -= bdl * sg * 0.5 * q0[QR];
-    bqp[QP] += bdr * 0.5 / c;
-    bq0[QP] -= bdr * 0.5 / c;
-    b_c += -bdr * 0.5 * (qp[QP] - q0[QP]) / (c * c);
+    bqp[QP] += bdr * 0.5 * ic;
+    bq0[QP] -= bdr * 0.5 * ic;
+    b_c += -bdr * 0.5 * (qp[QP] - q0[QP]) * ic * ic;
     bq0[QR] += bdr * sg * 0.5 * (qp[un] - q0[un]);
     bqp[un] += bdr * sg * 0.5 * q0[QR];
     bq0[un] -= bdr * sg * 0.5 * q0[QR];
