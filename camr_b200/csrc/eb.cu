@@ -26,12 +26,17 @@
 //
 // Geometry (flags, volume and area fractions, face centroids) comes from
 // the caller over a region G covering grow(bx,5).
+//
+// The EB level (camr_eb_level_*) runs the single-level MOL step around
+// these kernels with the EB build's covered-cell guards, on the domain as
+// one box with a persistent workspace.
 #include <cuda_runtime.h>
 
 #include <new>
 
 #include "cell_point.cuh"
 #include "hydro_kernels.cuh"
+#include "level_point.cuh"
 
 namespace camr {
 namespace {
@@ -130,20 +135,47 @@ __device__ __forceinline__ void eb_face(int i, int j, int k, const EBWork& W, co
     W.qf[d][at] = qpres;
     W.qf[d][at + s.sn] = qun;
   } else {
+    // a closed face carries no Riemann flux (artificial viscosity is added
+    // to it later); zeroing it here keeps a reused workspace free of the
+    // previous evaluation's values
+    for (int n = 0; n < NVAR; ++n) W.ft[d][at + n * s.sn] = 0.;
     W.qf[d][at] = 0.;
     W.qf[d][at + s.sn] = 0.;
   }
   W.ft[d][at + UTEMP * s.sn] = 0.0;
 }
 
-__global__ void __launch_bounds__(kEB) k_eb_face(Region r0, Region r1, Region r2, EBWork W, EBG G,
+__device__ __forceinline__ bool in_region(const Region& r, int i, int j, int k) {
+  return i >= r.lo[0] && i < r.lo[0] + r.n[0] && j >= r.lo[1] && j < r.lo[1] + r.n[1] &&
+         k >= r.lo[2] && k < r.lo[2] + r.n[2];
+}
+
+// Faces of the flux box ra[d] (faces of grow(bx,3)): the Riemann flux on
+// the faces of rf[d] (faces of grow(bx,2), transverse +1), zero on the
+// outer layer, which only the artificial viscosity touches.
+template <int d>
+__device__ __forceinline__ void eb_face_or_zero(const Region& rf, int i, int j, int k,
+                                                const EBWork& W, const EBG& G, const KGeom& g,
+                                                const KParams& P) {
+  if (in_region(rf, i, j, k)) {
+    eb_face<d>(i, j, k, W, G, g, P);
+    return;
+  }
+  const int64_t at = W.s.idx(i, j, k);
+  for (int n = 0; n < NVAR; ++n) W.ft[d][at + n * W.s.sn] = 0.;
+  W.qf[d][at] = 0.;
+  W.qf[d][at + W.s.sn] = 0.;
+}
+
+__global__ void __launch_bounds__(kEB) k_eb_face(Region r0, Region r1, Region r2, Region a0,
+                                                  Region a1, Region a2, EBWork W, EBG G,
                                                   KGeom g, KParams P) {
   int i, j, k;
   const int64_t t = etid();
   switch (blockIdx.y) {
-    case 0: if (region_cell(r0, t, i, j, k)) eb_face<0>(i, j, k, W, G, g, P); break;
-    case 1: if (region_cell(r1, t, i, j, k)) eb_face<1>(i, j, k, W, G, g, P); break;
-    default: if (region_cell(r2, t, i, j, k)) eb_face<2>(i, j, k, W, G, g, P); break;
+    case 0: if (region_cell(a0, t, i, j, k)) eb_face_or_zero<0>(r0, i, j, k, W, G, g, P); break;
+    case 1: if (region_cell(a1, t, i, j, k)) eb_face_or_zero<1>(r1, i, j, k, W, G, g, P); break;
+    default: if (region_cell(a2, t, i, j, k)) eb_face_or_zero<2>(r2, i, j, k, W, G, g, P); break;
   }
 }
 
@@ -309,8 +341,8 @@ __global__ void __launch_bounds__(kEB) k_eb_div(Region r, EBWork W, EBG G, KGeom
   if (f_covered(w)) return;
   const Space& s = W.s;
   const int64_t at = s.idx(i, j, k);
-  const bool valid_cell = g.lo[0] <= i && i <= g.hi[0] && g.lo[1] <= j && j <= g.hi[1] &&
-                          g.lo[2] <= k && k <= g.hi[2];
+  const bool valid_cell = fo0.p && g.lo[0] <= i && i <= g.hi[0] && g.lo[1] <= j &&
+                          j <= g.hi[1] && g.lo[2] <= k && k <= g.hi[2];
   const bool x_high = (i == g.hi[0]), y_high = (j == g.hi[1]), z_high = (k == g.hi[2]);
   const double dxinv0 = 1. / g.dx[0], dxinv1 = 1. / g.dx[1], dxinv2 = 1. / g.dx[2];
   const double cell_vol_inv = dxinv0 * dxinv1 * dxinv2;
@@ -490,44 +522,39 @@ __global__ void __launch_bounds__(kEB) k_eb_zero_faces(Region r, DFab f) {
   for (int n = 0; n < NVAR; ++n) f(i, j, k, n) = 0.0;
 }
 
-}  // namespace
-}  // namespace camr
 
-using namespace camr;
-
-extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3],
-                                           const camr_geom* geom, const camr_fab* uin,
-                                           const camr_eb_geom* eb, camr_fab* dsdt,
-                                           camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
-                                           const camr_hydro_params* p, int redist, double dt,
-                                           void* stream) {
-  (void)dt;
-  if (!bx_lo || !bx_hi || !geom || !uin || !eb || !dsdt || !flx0 || !flx1 || !flx2 || !p)
-    return CAMR_ERR_INVALID;
-  if (!p->do_mol || p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
-  for (int d = 0; d < 3; ++d) {
-    if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
-    if (uin->lo[d] > bx_lo[d] - 5 || uin->hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
-    if (eb->g_lo[d] > bx_lo[d] - 5 || eb->g_hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
-  }
-  if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
-      !eb->fc[1] || !eb->fc[2])
-    return CAMR_ERR_INVALID;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
+// One EB hydro evaluation of box bx: the launch geometry of K1-K8 and the
+// workspace they share.  The workspace may be reused across evaluations of
+// the same box: every intermediate a kernel reads is rewritten by an
+// earlier kernel of the same evaluation or never written at all (covered
+// cells' slopes, divergences and weights keep their first zero fill).
+struct EBPlan {
   EBWork W;
+  EBG G;
+  KGeom g;
+  KParams P;
+  DBox db;
+  int redist, wtype;
+  Region r5, r3, r2, r1, r0, rn, rf[3], ra[3];
+  int64_t ma;
+};
+
+// The Space of bx: grown by 5, one more high layer for faces.
+inline Space eb_space(const int bx_lo[3], const int bx_hi[3]) {
+  Space s;
   for (int d = 0; d < 3; ++d) {
-    W.s.lo[d] = bx_lo[d] - 5;
-    W.s.n[d] = bx_hi[d] - bx_lo[d] + 1 + 11;
+    s.lo[d] = bx_lo[d] - 5;
+    s.n[d] = bx_hi[d] - bx_lo[d] + 1 + 11;
   }
-  W.s.sy = W.s.n[0];
-  W.s.sz = W.s.sy * W.s.n[1];
-  W.s.sn = W.s.sz * W.s.n[2];
-  const int ncomp = SQ_N + 3 * SL_N + 3 * NVAR + 3 * 2 + 1 + NVAR + 1 + 2 * NVAR + 1;
-  const size_t bytes = size_t(ncomp) * W.s.sn * sizeof(double);
-  double* base = nullptr;
-  if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess)
-    return CAMR_ERR_NOMEM;
-  cudaError_t e = cudaMemsetAsync(base, 0, bytes, st);
+  s.sy = s.n[0];
+  s.sz = s.sy * s.n[1];
+  s.sn = s.sz * s.n[2];
+  return s;
+}
+
+constexpr int kEBWorkComps = SQ_N + 3 * SL_N + 3 * NVAR + 3 * 2 + 1 + NVAR + 1 + 2 * NVAR + 1;
+
+inline void eb_carve(EBWork& W, double* base) {
   double* ptr = base;
   auto take = [&](int nc) {
     double* r = ptr;
@@ -544,84 +571,662 @@ extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3
   W.optmp = take(NVAR);
   W.delm = take(NVAR);
   W.wtinv = take(1);
-  EBG G;
-  G.flag = eb->flag;
-  G.vfrac = eb->vfrac;
+}
+
+inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], const camr_geom& geom,
+                         const camr_eb_geom& eb, const camr_hydro_params& p, int redist) {
+  E.W.s = eb_space(bx_lo, bx_hi);
+  E.G.flag = eb.flag;
+  E.G.vfrac = eb.vfrac;
   for (int d = 0; d < 3; ++d) {
-    G.ap[d] = eb->ap[d];
-    G.fc[d] = eb->fc[d];
-    G.lo[d] = eb->g_lo[d];
-    G.n[d] = eb->g_hi[d] - eb->g_lo[d] + 1;
+    E.G.ap[d] = eb.ap[d];
+    E.G.fc[d] = eb.fc[d];
+    E.G.lo[d] = eb.g_lo[d];
+    E.G.n[d] = eb.g_hi[d] - eb.g_lo[d] + 1;
+    E.g.lo[d] = bx_lo[d];
+    E.g.hi[d] = bx_hi[d];
+    E.g.dlo[d] = geom.dom_lo[d];
+    E.g.dhi[d] = geom.dom_hi[d];
+    E.g.bclo[d] = geom.bc_lo[d];
+    E.g.bchi[d] = geom.bc_hi[d];
+    E.g.dx[d] = geom.dx[d];
+    E.db.lo[d] = geom.is_periodic[d] ? geom.dom_lo[d] - 2 : geom.dom_lo[d];
+    E.db.hi[d] = geom.is_periodic[d] ? geom.dom_hi[d] + 2 : geom.dom_hi[d];
   }
-  KGeom g;
-  for (int d = 0; d < 3; ++d) {
-    g.lo[d] = bx_lo[d];
-    g.hi[d] = bx_hi[d];
-    g.dlo[d] = geom->dom_lo[d];
-    g.dhi[d] = geom->dom_hi[d];
-    g.bclo[d] = geom->bc_lo[d];
-    g.bchi[d] = geom->bc_hi[d];
-    g.dx[d] = geom->dx[d];
-  }
-  const KParams P = make_kparams(*p);
-  const DFab U = make_dfab(*uin);
-  auto reg = [&](int grow_lo, int grow_hi, int fdir, int tgrow) {
+  E.P = make_kparams(p);
+  E.redist = redist;
+  E.wtype = p.eb_weights_type;
+  auto reg = [&](int grow, int fdir, int tgrow) {
     int lo[3], hi[3];
     for (int d = 0; d < 3; ++d) {
       const int gr = (d == fdir) ? 0 : tgrow;
-      lo[d] = bx_lo[d] - grow_lo - gr;
-      hi[d] = bx_hi[d] + grow_hi + gr + (d == fdir ? 1 : 0);
+      lo[d] = bx_lo[d] - grow - gr;
+      hi[d] = bx_hi[d] + grow + gr + (d == fdir ? 1 : 0);
     }
     return make_region(lo, hi);
   };
-  // zero the output faces (covered cells leave theirs untouched)
-  DFab fo[3] = {make_dfab(*flx0), make_dfab(*flx1), make_dfab(*flx2)};
-  for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
-    const Region rf = reg(0, 0, d, 0);
-    k_eb_zero_faces<<<eblk(rf.count()), kEB, 0, st>>>(rf, fo[d]);
-  }
-  const Region r5 = reg(5, 5, -1, 0);
-  k_eb_ctoprim<<<eblk(r5.count()), kEB, 0, st>>>(r5, W, G, U, P, nullptr);
-  const Region r3 = reg(3, 3, -1, 0);
-  k_eb_slope<<<dim3(eblk(r3.count()), 3), kEB, 0, st>>>(r3, W, G, P);
-  Region rf[3], ra[3];
-  int64_t mf = 0, ma = 0;
+  E.r5 = reg(5, -1, 0);
+  E.r3 = reg(3, -1, 0);
+  E.r2 = reg(2, -1, 0);
+  E.r1 = reg(1, -1, 0);
+  E.r0 = reg(0, -1, 0);
+  E.ma = 0;
   for (int d = 0; d < 3; ++d) {
-    rf[d] = reg(2, 2, d, 1);  // faces of grow(bx,2), transverse +1
-    ra[d] = reg(3, 3, d, 0);  // faces of grow(bx,3)
-    mf = rf[d].count() > mf ? rf[d].count() : mf;
-    ma = ra[d].count() > ma ? ra[d].count() : ma;
+    E.rf[d] = reg(2, d, 1);  // faces of grow(bx,2), transverse +1
+    E.ra[d] = reg(3, d, 0);  // faces of grow(bx,3)
+    E.ma = E.ra[d].count() > E.ma ? E.ra[d].count() : E.ma;
   }
-  k_eb_face<<<dim3(eblk(mf), 3), kEB, 0, st>>>(rf[0], rf[1], rf[2], W, G, g, P);
   // nodes of grow(bx,4) inside the domain grown by 16 in periodic directions
   int nlo[3], nhi[3];
   for (int d = 0; d < 3; ++d) {
     nlo[d] = bx_lo[d] - 4;
     nhi[d] = bx_hi[d] + 5;
-    const int glo = geom->is_periodic[d] ? geom->dom_lo[d] - 16 : geom->dom_lo[d];
-    const int ghi = geom->is_periodic[d] ? geom->dom_hi[d] + 1 + 16 : geom->dom_hi[d] + 1;
+    const int glo = geom.is_periodic[d] ? geom.dom_lo[d] - 16 : geom.dom_lo[d];
+    const int ghi = geom.is_periodic[d] ? geom.dom_hi[d] + 1 + 16 : geom.dom_hi[d] + 1;
     nlo[d] = nlo[d] > glo ? nlo[d] : glo;
     nhi[d] = nhi[d] < ghi ? nhi[d] : ghi;
   }
-  const Region rn = make_region(nlo, nhi);
-  if (rn.count() > 0) k_eb_divu<<<eblk(rn.count()), kEB, 0, st>>>(rn, W, G, g);
-  k_eb_adjust<<<dim3(eblk(ma), 3), kEB, 0, st>>>(ra[0], ra[1], ra[2], W, G, g, P, U);
-  const Region r2 = reg(2, 2, -1, 0);
-  k_eb_div<<<eblk(r2.count()), kEB, 0, st>>>(r2, W, G, g, P, fo[0], fo[1], fo[2], 2);
-  DBox db;
+  E.rn = make_region(nlo, nhi);
+}
+
+// K1-K8 on the stream; fo[d].p may be null (no face-flux output).
+// Returns the number of kernels issued.
+inline int eb_issue(const EBPlan& E, const DFab& U, const DFab& dsdt, const DFab* fo,
+                    cudaStream_t st) {
+  int nk = 0;
+  const EBWork& W = E.W;
+  k_eb_ctoprim<<<eblk(E.r5.count()), kEB, 0, st>>>(E.r5, W, E.G, U, E.P, nullptr);
+  k_eb_slope<<<dim3(eblk(E.r3.count()), 3), kEB, 0, st>>>(E.r3, W, E.G, E.P);
+  k_eb_face<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.rf[0], E.rf[1], E.rf[2], E.ra[0], E.ra[1],
+                                                  E.ra[2], W, E.G, E.g, E.P);
+  nk += 3;
+  if (E.rn.count() > 0) {
+    k_eb_divu<<<eblk(E.rn.count()), kEB, 0, st>>>(E.rn, W, E.G, E.g);
+    ++nk;
+  }
+  k_eb_adjust<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.ra[0], E.ra[1], E.ra[2], W, E.G, E.g, E.P,
+                                                    U);
+  k_eb_div<<<eblk(E.r2.count()), kEB, 0, st>>>(E.r2, W, E.G, E.g, E.P, fo[0], fo[1], fo[2],
+                                               E.wtype);
+  nk += 2;
+  if (E.redist) {
+    k_eb_redist1<<<eblk(E.r1.count()), kEB, 0, st>>>(E.r1, W, E.G, E.db);
+    ++nk;
+  }
+  k_eb_redist2<<<eblk(E.r0.count()), kEB, 0, st>>>(E.r0, W, E.G, E.db, E.g, dsdt, E.redist);
+  ++nk;
+  return nk;
+}
+
+// ---------------------------------------------------------------------------
+// EB level: the level step of the single-level driver with the EB build's
+// guards (Source/CAMR.cpp:877-891 normalize_species and :960-968
+// enforce_min_density skip covered cells; reset_internal_energy runs where
+// rho > 0, Utils/CAMR_reset_internal_e.H:36-38; computeTemp sets T = 0 first,
+// Source/CAMR.cpp:1164-1168; the CFL minimum skips covered cells,
+// Utils/Timestep.H:32-56).  The domain is one box with 5 ghost cells
+// (CAMR::numGrow() with flux redistribution, Source/CAMR.H:455-479).
+
+__device__ __forceinline__ void temp_eb(double* s, const KParams& P) {
+  if (s[URHO] > 0.) {
+    compute_temp(s, P);
+  } else {
+    s[UTEMP] = 0.0;
+  }
+}
+
+__device__ __forceinline__ bool cov_at(const EBG& G, int i, int j, int k) {
+  return f_covered(G.fl(i, j, k));
+}
+
+__global__ void __launch_bounds__(kBlk) k_ebl_est_dt(LGeom L, KParams P, EBG G, const double* S,
+                                                      unsigned long long* bits) {
+  int i, j, k;
+  double v = DBL_MAX;
+  if (valid_cell(L, tid(), i, j, k) && !cov_at(G, i, j, k)) {
+    double s[NVAR];
+    load_cell(S, L, L.idx(i, j, k), s);
+    v = cell_dt(s, L, P);
+  }
+  block_min_dt(v, bits);
+}
+
+__global__ void __launch_bounds__(kBlk) k_ebl_clean_copy(LGeom L, KParams P, EBG G,
+                                                          const double* S, double* out,
+                                                          DevError* err) {
+  int i, j, k;
+  if (!valid_cell(L, tid(), i, j, k)) return;
+  const int64_t at = L.idx(i, j, k);
+  double s[NVAR];
+  load_cell(S, L, at, s);
+  if (!cov_at(G, i, j, k)) {
+    enforce_min_density(s, S, L, P, i, j, k, err);
+    normalize_species(s);
+  }
+  temp_eb(s, P);
+  store_cell(out, L, at, s);
+}
+
+// expand_state with the EB guards (fill rules as k_expand's).
+__global__ void __launch_bounds__(kBlk) k_ebl_expand(LGeom L, KParams P, EBG G,
+                                                      const double* src, double* B,
+                                                      DevError* err) {
+  int i, j, k;
+  if (!padded_cell(L, tid(), i, j, k)) return;
+  const int c[3] = {i, j, k};
+  int img[3];
+  bool physical = false;
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
-    db.lo[d] = geom->is_periodic[d] ? geom->dom_lo[d] - 2 : geom->dom_lo[d];
-    db.hi[d] = geom->is_periodic[d] ? geom->dom_hi[d] + 2 : geom->dom_hi[d];
+    img[d] = c[d];
+    if (c[d] < L.dlo[d] || c[d] > L.dhi[d]) {
+      if (L.periodic[d]) {
+        const int len = L.dhi[d] - L.dlo[d] + 1;
+        img[d] = L.dlo[d] + (((c[d] - L.dlo[d]) % len) + len) % len;
+      } else {
+        physical = true;
+      }
+    }
   }
-  if (redist) {
-    const Region r1 = reg(1, 1, -1, 0);
-    k_eb_redist1<<<eblk(r1.count()), kEB, 0, st>>>(r1, W, G, db);
+  double s[NVAR];
+  if (!physical) {
+    load_cell(src, L, L.idx(img[0], img[1], img[2]), s);
+    if (!cov_at(G, img[0], img[1], img[2])) {
+      enforce_min_density(s, src, L, P, img[0], img[1], img[2], err);
+      normalize_species(s);
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) {
+      int id[3] = {img[0], img[1], img[2]};
+      bool neg = false;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (L.periodic[d]) continue;
+        if (id[d] < L.dlo[d]) {
+          const int t = bc_kind(n, d, L.bclo[d]);
+          if (t == 1 || t == 2) id[d] = L.dlo[d];
+          else { id[d] = 2 * L.dlo[d] - id[d] - 1; if (t == 4) neg = !neg; }
+        } else if (id[d] > L.dhi[d]) {
+          const int t = bc_kind(n, d, L.bchi[d]);
+          if (t == 1 || t == 2) id[d] = L.dhi[d];
+          else { id[d] = 2 * L.dhi[d] - id[d] + 1; if (t == 4) neg = !neg; }
+        }
+      }
+      const double v = src[L.idx(id[0], id[1], id[2]) + n * L.sn];
+      s[n] = neg ? -v : v;
+    }
   }
-  const Region r0 = reg(0, 0, -1, 0);
-  k_eb_redist2<<<eblk(r0.count()), kEB, 0, st>>>(r0, W, G, db, g, make_dfab(*dsdt), redist);
-  count_launch(redist ? 12 : 11);
+  temp_eb(s, P);
+  store_cell(B, L, L.idx(i, j, k), s);
+}
+
+// MOL stage 1: S = Sborder (+ dt*src_old) + dt*k1.
+__global__ void __launch_bounds__(kBlk) k_ebl_update1(LGeom L, KParams P, const double* dtp,
+                                                       const double* B, const double* S_old,
+                                                       const double* dsdt, double* S) {
+  int i, j, k;
+  if (!valid_cell(L, tid(), i, j, k)) return;
+  const double dt = *dtp;
+  const int64_t at = L.idx(i, j, k);
+  double s[NVAR];
+  load_cell(B, L, at, s);
+  if (P.add_grav_src) {
+    double src[NVAR];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+    src[UMZ] = P.const_grav * S_old[at + URHO * L.sn];
+    src[UEDEN] = P.const_grav * S_old[at + UMZ * L.sn];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
+  }
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] += dt * dsdt[at + n * L.sn];
+  store_cell(S, L, at, s);
+}
+
+// clean_state of one cell inside the fused end of step: a density under
+// the floor is reported (enforce_min_density cannot see its neighbours'
+// new values here).
+__device__ __forceinline__ void clean_eb_cell(double* s, const KParams& P, bool cov, int i, int j,
+                                              int k, DevError* err) {
+  if (!cov) {
+    if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
+    normalize_species(s);
+  }
+  temp_eb(s, P);
+}
+
+// MOL stage 2: S = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2, then clean_state,
+// the new-source correction (+ clean_state), post_timestep's clean_state,
+// and the cell's CFL dt.
+__global__ void __launch_bounds__(kBlk) k_ebl_update2(LGeom L, KParams P, EBG G,
+                                                       const double* dtp, const double* B2,
+                                                       const double* S_old, const double* dsdt,
+                                                       double* S, unsigned long long* bits,
+                                                       DevError* err) {
+  int i, j, k;
+  double v = DBL_MAX;
+  if (valid_cell(L, tid(), i, j, k)) {
+    const double dt = *dtp;
+    const int64_t at = L.idx(i, j, k);
+    const bool cov = cov_at(G, i, j, k);
+    double s[NVAR], sold[NVAR], b[NVAR];
+    load_cell(B2, L, at, b);
+    load_cell(S_old, L, at, sold);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * dsdt[at + n * L.sn];
+    clean_eb_cell(s, P, cov, i, j, k, err);
+    if (P.add_grav_src) {
+      double src[NVAR];
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+      src[UMZ] = 0.5 * P.const_grav * (s[URHO] - sold[URHO]);
+      src[UEDEN] = 0.5 * P.const_grav * (s[UMZ] - sold[UMZ]);
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
+      clean_eb_cell(s, P, cov, i, j, k, err);
+    }
+    clean_eb_cell(s, P, cov, i, j, k, err);
+    if (!cov) v = cell_dt(s, L, P);
+    store_cell(S, L, at, s);
+  }
+  block_min_dt(v, bits);
+}
+
+// initData's epilogue with the EB guards: enforce_consistent_e where
+// rho > 0 (Source/CAMR.cpp:910-939), then computeTemp.
+__global__ void __launch_bounds__(kBlk) k_ebl_init_finalize(LGeom L, KParams P, double* S) {
+  int i, j, k;
+  if (!valid_cell(L, tid(), i, j, k)) return;
+  const int64_t at = L.idx(i, j, k);
+  double s[NVAR];
+  load_cell(S, L, at, s);
+  if (s[URHO] > 0.) {
+    const double rhoInv = 1.0 / s[URHO];
+    const double u = s[UMX] * rhoInv;
+    const double v = s[UMY] * rhoInv;
+    const double w = s[UMZ] * rhoInv;
+    s[UEDEN] = s[UEINT] + 0.5 * s[URHO] * (u * u + v * v + w * w);
+  }
+  temp_eb(s, P);
+  store_cell(S, L, at, s);
+}
+
+}  // namespace
+}  // namespace camr
+
+using namespace camr;
+
+extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3],
+                                           const camr_geom* geom, const camr_fab* uin,
+                                           const camr_eb_geom* eb, camr_fab* dsdt,
+                                           camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                                           const camr_hydro_params* p, int redist, double dt,
+                                           void* stream) {
+  (void)dt;
+  if (!bx_lo || !bx_hi || !geom || !uin || !eb || !dsdt || !flx0 || !flx1 || !flx2 || !p)
+    return CAMR_ERR_INVALID;
+  if (!p->do_mol || p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
+    return CAMR_ERR_INVALID;
+  for (int d = 0; d < 3; ++d) {
+    if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
+    if (uin->lo[d] > bx_lo[d] - 5 || uin->hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
+    if (eb->g_lo[d] > bx_lo[d] - 5 || eb->g_hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
+  }
+  if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
+      !eb->fc[1] || !eb->fc[2])
+    return CAMR_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  EBPlan E;
+  eb_plan_init(E, bx_lo, bx_hi, *geom, *eb, *p, redist);
+  const size_t bytes = size_t(kEBWorkComps) * E.W.s.sn * sizeof(double);
+  double* base = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess)
+    return CAMR_ERR_NOMEM;
+  cudaError_t e = cudaMemsetAsync(base, 0, bytes, st);
+  eb_carve(E.W, base);
+  // zero the output faces (covered cells leave theirs untouched)
+  const DFab fo[3] = {make_dfab(*flx0), make_dfab(*flx1), make_dfab(*flx2)};
+  int nk = 0;
+  for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = bx_lo[a];
+      hi[a] = bx_hi[a] + (a == d ? 1 : 0);
+    }
+    const Region rf = make_region(lo, hi);
+    k_eb_zero_faces<<<eblk(rf.count()), kEB, 0, st>>>(rf, fo[d]);
+    ++nk;
+  }
+  if (e == cudaSuccess) nk += eb_issue(E, make_dfab(*uin), make_dfab(*dsdt), fo, st);
+  count_launch(nk);
   if (e == cudaSuccess) e = cudaGetLastError();
   cudaError_t e2 = cudaFreeAsync(base, st);
   if (e != cudaSuccess) return cuda_status_of(e);
   return cuda_status_of(e2);
 }
+
+// ---------------------------------------------------------------------------
+// EB level API.
+
+struct camr_eb_level {
+  camr_hydro_params hp;
+  KParams P;
+  camr_level_desc desc;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  LGeom L;
+  int64_t ncell = 0, npad = 0;
+  double *S = nullptr, *S_old = nullptr, *B = nullptr, *B2 = nullptr, *dsdt = nullptr;
+  double *work = nullptr, *staging = nullptr, *fixed_dev = nullptr;
+  double *dt_cur = nullptr, *dt_hist = nullptr;
+  unsigned long long* bits = nullptr;
+  int* nstep = nullptr;
+  DevError* err = nullptr;
+  unsigned* flag = nullptr;
+  double *vfrac = nullptr, *ap[3] = {nullptr, nullptr, nullptr}, *fc[3] = {nullptr, nullptr, nullptr};
+  EBPlan plan;
+  int hist_cap = 1 << 16;
+  int64_t steps_taken = 0;
+  cudaGraphExec_t graph = nullptr;
+  bool graph_ready = false;
+  int64_t kernels_per_step = 0;
+};
+
+namespace {
+
+DFab level_dfab(const LGeom& L, double* p) {
+  DFab f;
+  f.p = p;
+  for (int d = 0; d < 3; ++d) f.lo[d] = L.plo[d];
+  f.sy = L.sy;
+  f.sz = L.sz;
+  f.sn = L.sn;
+  return f;
+}
+
+cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_dev) {
+  const LGeom& L = lev->L;
+  cudaStream_t st = lev->stream;
+  const unsigned gv = grid_of(lev->ncell);
+  const unsigned gp = grid_of(lev->npad);
+  const EBG& G = lev->plan.G;
+  DtCtl c{lev->hp.cfl, lev->hp.max_dt, lev->hp.fixed_dt, lev->hp.initial_dt,
+          lev->hp.init_shrink, lev->hp.change_max};
+  int nk = 0;
+  if (first) {
+    k_reset_bits<<<1, 1, 0, st>>>(lev->bits);
+    k_ebl_est_dt<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->bits);
+    nk += 2;
+  }
+  k_dt_next<<<1, 1, 0, st>>>(c, first ? 1 : 0, fixed_dev, lev->bits, lev->dt_cur, lev->dt_hist,
+                             lev->nstep, lev->hist_cap);
+  k_ebl_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->S_old, lev->err);
+  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err);
+  nk += 3;
+  const DFab none[3] = {level_dfab(L, nullptr), level_dfab(L, nullptr), level_dfab(L, nullptr)};
+  const DFab ds = level_dfab(L, lev->dsdt);
+  nk += eb_issue(lev->plan, level_dfab(L, lev->B), ds, none, st);
+  k_ebl_update1<<<gv, kBlk, 0, st>>>(L, lev->P, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
+                                     lev->S);
+  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B2, lev->err);
+  nk += 2;
+  nk += eb_issue(lev->plan, level_dfab(L, lev->B2), ds, none, st);
+  k_ebl_update2<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B2, lev->S_old, lev->dsdt,
+                                     lev->S, lev->bits, lev->err);
+  nk += 1;
+  count_launch(nk);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom* eb,
+                                 const camr_hydro_params* p, int redist, void* stream,
+                                 camr_eb_level** out) {
+  if (!desc || !eb || !p || !out) return CAMR_ERR_INVALID;
+  *out = nullptr;
+  if (!p->do_mol || p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
+    return CAMR_ERR_INVALID;
+  const camr_geom& g = desc->geom;
+  for (int d = 0; d < 3; ++d) {
+    if (g.dom_hi[d] < g.dom_lo[d]) return CAMR_ERR_INVALID;
+    if (!g.is_periodic[d] && (g.bc_lo[d] == CAMR_BC_INTERIOR || g.bc_hi[d] == CAMR_BC_INTERIOR))
+      return CAMR_ERR_INVALID;
+    if (eb->g_lo[d] != g.dom_lo[d] - 5 || eb->g_hi[d] != g.dom_hi[d] + 5) return CAMR_ERR_INVALID;
+  }
+  if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
+      !eb->fc[1] || !eb->fc[2])
+    return CAMR_ERR_INVALID;
+  camr_eb_level* lev = new (std::nothrow) camr_eb_level();
+  if (!lev) return CAMR_ERR_NOMEM;
+  lev->hp = *p;
+  lev->P = make_kparams(*p);
+  lev->desc = *desc;
+  lev->stream = static_cast<cudaStream_t>(stream);
+  if (!lev->stream) {
+    if (cudaStreamCreateWithFlags(&lev->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete lev;
+      return CAMR_ERR_CUDA;
+    }
+    lev->own_stream = true;
+  }
+  LGeom& L = lev->L;
+  for (int d = 0; d < 3; ++d) {
+    L.dlo[d] = g.dom_lo[d];
+    L.dhi[d] = g.dom_hi[d];
+    L.plo[d] = g.dom_lo[d] - 5;
+    L.pn[d] = g.dom_hi[d] - g.dom_lo[d] + 1 + 10;
+    L.periodic[d] = g.is_periodic[d];
+    L.bclo[d] = g.bc_lo[d];
+    L.bchi[d] = g.bc_hi[d];
+    L.dx[d] = g.dx[d];
+    const int n = g.dom_hi[d] - g.dom_lo[d] + 1;
+    L.boxsz[d] = desc->max_grid_size[d] > 0 ? desc->max_grid_size[d] : n;
+  }
+  L.sy = L.pn[0];
+  L.sz = L.sy * L.pn[1];
+  L.sn = L.sz * L.pn[2];
+  lev->ncell = int64_t(g.dom_hi[0] - g.dom_lo[0] + 1) * (g.dom_hi[1] - g.dom_lo[1] + 1) *
+               (g.dom_hi[2] - g.dom_lo[2] + 1);
+  lev->npad = L.sn;
+  const size_t state_bytes = size_t(L.sn) * NVAR * sizeof(double);
+  const Space ws = eb_space(g.dom_lo, g.dom_hi);
+  const size_t work_bytes = size_t(kEBWorkComps) * ws.sn * sizeof(double);
+  const int64_t gc = int64_t(eb->g_hi[0] - eb->g_lo[0] + 1) * (eb->g_hi[1] - eb->g_lo[1] + 1) *
+                     (eb->g_hi[2] - eb->g_lo[2] + 1);
+  int64_t gf[3];
+  for (int d = 0; d < 3; ++d) {
+    gf[d] = 1;
+    for (int a = 0; a < 3; ++a) gf[d] *= int64_t(eb->g_hi[a] - eb->g_lo[a] + 1 + (a == d));
+  }
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** ptr, size_t b) {
+    if (e == cudaSuccess) e = cudaMalloc(ptr, b);
+    if (e == cudaSuccess) e = cudaMemsetAsync(*ptr, 0, b, lev->stream);
+  };
+  alloc(reinterpret_cast<void**>(&lev->S), state_bytes);
+  alloc(reinterpret_cast<void**>(&lev->S_old), state_bytes);
+  alloc(reinterpret_cast<void**>(&lev->B), state_bytes);
+  alloc(reinterpret_cast<void**>(&lev->B2), state_bytes);
+  alloc(reinterpret_cast<void**>(&lev->dsdt), state_bytes);
+  alloc(reinterpret_cast<void**>(&lev->work), work_bytes);
+  alloc(reinterpret_cast<void**>(&lev->staging), size_t(lev->ncell) * NVAR * sizeof(double));
+  alloc(reinterpret_cast<void**>(&lev->fixed_dev), sizeof(double));
+  alloc(reinterpret_cast<void**>(&lev->dt_cur), sizeof(double));
+  alloc(reinterpret_cast<void**>(&lev->dt_hist), sizeof(double) * lev->hist_cap);
+  alloc(reinterpret_cast<void**>(&lev->bits), sizeof(unsigned long long));
+  alloc(reinterpret_cast<void**>(&lev->nstep), sizeof(int));
+  alloc(reinterpret_cast<void**>(&lev->err), sizeof(DevError));
+  alloc(reinterpret_cast<void**>(&lev->flag), size_t(gc) * sizeof(unsigned));
+  alloc(reinterpret_cast<void**>(&lev->vfrac), size_t(gc) * sizeof(double));
+  for (int d = 0; d < 3; ++d) {
+    alloc(reinterpret_cast<void**>(&lev->ap[d]), size_t(gf[d]) * sizeof(double));
+    alloc(reinterpret_cast<void**>(&lev->fc[d]), size_t(2 * gf[d]) * sizeof(double));
+  }
+  // the geometry is copied into the level (device or host source)
+  auto copy = [&](void* dst, const void* src, size_t b) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyDefault, lev->stream);
+  };
+  copy(lev->flag, eb->flag, size_t(gc) * sizeof(unsigned));
+  copy(lev->vfrac, eb->vfrac, size_t(gc) * sizeof(double));
+  for (int d = 0; d < 3; ++d) {
+    copy(lev->ap[d], eb->ap[d], size_t(gf[d]) * sizeof(double));
+    copy(lev->fc[d], eb->fc[d], size_t(2 * gf[d]) * sizeof(double));
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) {
+    camr_eb_level_destroy(lev);
+    return e == cudaErrorMemoryAllocation ? CAMR_ERR_NOMEM : cuda_status_of(e);
+  }
+  camr_eb_geom own = *eb;
+  own.flag = lev->flag;
+  own.vfrac = lev->vfrac;
+  for (int d = 0; d < 3; ++d) {
+    own.ap[d] = lev->ap[d];
+    own.fc[d] = lev->fc[d];
+  }
+  eb_plan_init(lev->plan, g.dom_lo, g.dom_hi, g, own, *p, redist);
+  lev->plan.W.s = ws;
+  eb_carve(lev->plan.W, lev->work);
+  *out = lev;
+  return CAMR_OK;
+}
+
+camr_status camr_eb_level_destroy(camr_eb_level* lev) {
+  if (!lev) return CAMR_ERR_INVALID;
+  if (lev->graph_ready) cudaGraphExecDestroy(lev->graph);
+  void* ptrs[] = {lev->S,       lev->S_old,  lev->B,     lev->B2,    lev->dsdt,  lev->work,
+                  lev->staging, lev->fixed_dev, lev->dt_cur, lev->dt_hist, lev->bits, lev->nstep,
+                  lev->err,     lev->flag,   lev->vfrac, lev->ap[0], lev->ap[1], lev->ap[2],
+                  lev->fc[0],   lev->fc[1],  lev->fc[2]};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (lev->own_stream) cudaStreamDestroy(lev->stream);
+  delete lev;
+  return CAMR_OK;
+}
+
+camr_status camr_eb_level_set_state(camr_eb_level* lev, const double* state, int host) {
+  if (!lev || !state) return CAMR_ERR_INVALID;
+  const size_t bytes = size_t(lev->ncell) * NVAR * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(lev->staging, state, bytes,
+                                  host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                  lev->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  k_pack<<<grid_of(lev->ncell), kBlk, 0, lev->stream>>>(lev->L, lev->S, lev->staging, 0);
+  count_launch();
+  lev->steps_taken = 0;
+  return cuda_status_of(cudaGetLastError());
+}
+
+camr_status camr_eb_level_get_state(camr_eb_level* lev, double* state, int host) {
+  if (!lev || !state) return CAMR_ERR_INVALID;
+  k_pack<<<grid_of(lev->ncell), kBlk, 0, lev->stream>>>(lev->L, lev->S, lev->staging, 1);
+  count_launch();
+  const size_t bytes = size_t(lev->ncell) * NVAR * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(state, lev->staging, bytes,
+                                  host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                  lev->stream);
+  if (e == cudaSuccess && host) e = cudaStreamSynchronize(lev->stream);
+  return cuda_status_of(e);
+}
+
+camr_status camr_eb_level_init_finalize(camr_eb_level* lev) {
+  if (!lev) return CAMR_ERR_INVALID;
+  k_ebl_init_finalize<<<grid_of(lev->ncell), kBlk, 0, lev->stream>>>(lev->L, lev->P, lev->S);
+  count_launch();
+  return cuda_status_of(cudaGetLastError());
+}
+
+camr_status camr_eb_level_advance(camr_eb_level* lev, int nsteps, const double* fixed_dts) {
+  if (!lev || nsteps < 0) return CAMR_ERR_INVALID;
+  for (int s = 0; s < nsteps; ++s) {
+    const bool first = lev->steps_taken == 0;
+    const double* fixed_dev = nullptr;
+    cudaError_t e;
+    if (fixed_dts) {
+      e = cudaMemcpyAsync(lev->fixed_dev, &fixed_dts[s], sizeof(double), cudaMemcpyHostToDevice,
+                          lev->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+      if (e != cudaSuccess) return cuda_status_of(e);
+      fixed_dev = lev->fixed_dev;
+    }
+    if (!first && !fixed_dts && lev->desc.use_graph) {
+      if (!lev->graph_ready) {
+        cudaGraph_t gr;
+        e = cudaStreamBeginCapture(lev->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_status_of(e);
+        const int64_t before = launches_now();
+        const cudaError_t e1 = eb_issue_step(lev, false, nullptr);
+        lev->kernels_per_step = launches_now() - before;
+        launches_sub(lev->kernels_per_step);
+        e = cudaStreamEndCapture(lev->stream, &gr);
+        if (e1 != cudaSuccess) return cuda_status_of(e1);
+        if (e != cudaSuccess) return cuda_status_of(e);
+        e = cudaGraphInstantiate(&lev->graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return cuda_status_of(e);
+        lev->graph_ready = true;
+      }
+      e = cudaGraphLaunch(lev->graph, lev->stream);
+      count_launch(int(lev->kernels_per_step));
+    } else {
+      e = eb_issue_step(lev, first, fixed_dev);
+    }
+    if (e != cudaSuccess) return cuda_status_of(e);
+    lev->steps_taken++;
+  }
+  return CAMR_OK;
+}
+
+camr_status camr_eb_level_dts(camr_eb_level* lev, double* dts, int n, int* nsteps) {
+  if (!lev || (n > 0 && !dts)) return CAMR_ERR_INVALID;
+  int taken = 0;
+  cudaError_t e = cudaMemcpyAsync(&taken, lev->nstep, sizeof(int), cudaMemcpyDeviceToHost,
+                                  lev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  if (nsteps) *nsteps = taken;
+  const int m = taken < n ? taken : n;
+  const int cap = m < lev->hist_cap ? m : lev->hist_cap;
+  if (cap > 0) {
+    e = cudaMemcpyAsync(dts, lev->dt_hist, sizeof(double) * cap, cudaMemcpyDeviceToHost,
+                        lev->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  }
+  return cuda_status_of(e);
+}
+
+int64_t camr_eb_level_kernels_per_step(camr_eb_level* lev) {
+  return lev ? lev->kernels_per_step : 0;
+}
+
+camr_status camr_eb_level_stream(camr_eb_level* lev, void** stream) {
+  if (!lev || !stream) return CAMR_ERR_INVALID;
+  *stream = lev->stream;
+  return CAMR_OK;
+}
+
+camr_status camr_eb_level_get_error(camr_eb_level* lev, camr_error_info* info) {
+  if (!lev || !info) return CAMR_ERR_INVALID;
+  DevError h{};
+  cudaError_t e = cudaMemcpyAsync(&h, lev->err, sizeof(h), cudaMemcpyDeviceToHost, lev->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(lev->err, 0, sizeof(DevError), lev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  info->code = h.code;
+  info->i = h.i;
+  info->j = h.j;
+  info->k = h.k;
+  return h.code ? CAMR_ERR_NUMERIC : CAMR_OK;
+}
+
+}  // extern "C"

@@ -93,6 +93,7 @@ void camr_default_params(camr_hydro_params* p) {
   p->allow_small_energy = 1;
   p->add_grav_src = 1;
   p->riemann_solver = 0;
+  p->eb_weights_type = 2;
   p->difmag = 0.1;
   p->small = 1.e-8;
   p->small_dens = 1.e-7;

@@ -209,3 +209,14 @@ def sphere_geometry(lo, hi, dx, prob_lo=(0.0, 0.0, 0.0), center=(0.5, 0.5, 0.5),
         out["ap"].append(np.ascontiguousarray(ap[d][tuple(s)]))
         out["fc"].append(np.ascontiguousarray(fc[d][(slice(None),) + tuple(s)]))
     return out
+
+
+def set_covered(state, geo, lo=(0, 0, 0)):
+    """EB_set_covered(S, 0) (Source/CAMR.cpp:418-420): zero every component
+    of the covered cells of state (NVAR, nz, ny, nx) whose first cell is
+    `lo`; geo covers a region containing it."""
+    n = state.shape[1:]
+    off = [lo[d] - geo["lo"][d] for d in range(3)]
+    flag = geo["flag"][off[2]:off[2] + n[0], off[1]:off[1] + n[1], off[0]:off[0] + n[2]]
+    state[:, (flag & 3) == COVERED] = 0.0
+    return state

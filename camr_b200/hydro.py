@@ -219,6 +219,109 @@ class Level:
         _torch().cuda.synchronize()
 
 
+class EBLevel:
+    """One uniform level with an embedded boundary (MOL), advanced on the GPU
+    through camr_eb_level_*.  geo: eb_geometry.sphere_geometry output over
+    grow(domain, 5) (copied into the level).  redist: 1 FluxRedist, 0
+    NoRedist."""
+
+    def __init__(self, geom, params, geo, redist=1, max_grid_size=(0, 0, 0), use_graph=True,
+                 stream=None):
+        desc = LevelDesc()
+        desc.geom = geom
+        for d in range(3):
+            desc.max_grid_size[d] = max_grid_size[d]
+        desc.use_graph = int(use_graph)
+        self.params = params
+        self.geom = geom
+        self.n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+        self.ncell = self.n[0] * self.n[1] * self.n[2]
+        host = {"flag": np.ascontiguousarray(geo["flag"], dtype=np.uint32),
+                "vfrac": np.ascontiguousarray(geo["vfrac"], dtype=np.float64),
+                "ap": [np.ascontiguousarray(a, dtype=np.float64) for a in geo["ap"]],
+                "fc": [np.ascontiguousarray(a, dtype=np.float64) for a in geo["fc"]]}
+        g = native.EBGeom()
+        g.flag = host["flag"].ctypes.data
+        g.vfrac = host["vfrac"].ctypes.data
+        for d in range(3):
+            g.ap[d] = host["ap"][d].ctypes.data
+            g.fc[d] = host["fc"][d].ctypes.data
+            g.g_lo[d] = geo["lo"][d]
+            g.g_hi[d] = geo["hi"][d]
+        sp = None if stream is None else getattr(stream, "cuda_stream", stream)
+        h = C.c_void_p()
+        check(lib().camr_eb_level_create(C.byref(desc), C.byref(g), C.byref(params),
+                                         int(redist), C.c_void_p(sp), C.byref(h)),
+              "camr_eb_level_create")
+        self._h = h
+        s = C.c_void_p()
+        check(lib().camr_eb_level_stream(self._h, C.byref(s)), "camr_eb_level_stream")
+        self.stream_ptr = s.value or 0
+
+    def torch_stream(self):
+        return _torch().cuda.ExternalStream(self.stream_ptr)
+
+    def close(self):
+        if self._h:
+            lib().camr_eb_level_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, state):
+        """state: numpy (host) or CUDA tensor of shape (NVAR, nz, ny, nx)."""
+        if isinstance(state, np.ndarray):
+            a = np.ascontiguousarray(state, dtype=np.float64)
+            assert a.shape == (NVAR, self.n[2], self.n[1], self.n[0])
+            check(lib().camr_eb_level_set_state(self._h, a.ctypes.data, 1), "set_state")
+            self.sync()
+        else:
+            assert state.is_cuda and state.is_contiguous()
+            check(lib().camr_eb_level_set_state(self._h, state.data_ptr(), 0), "set_state")
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.empty((NVAR, self.n[2], self.n[1], self.n[0]))
+        if isinstance(out, np.ndarray):
+            check(lib().camr_eb_level_get_state(self._h, out.ctypes.data, 1), "get_state")
+        else:
+            check(lib().camr_eb_level_get_state(self._h, out.data_ptr(), 0), "get_state")
+        return out
+
+    def init_finalize(self):
+        check(lib().camr_eb_level_init_finalize(self._h), "init_finalize")
+
+    def advance(self, nsteps, fixed_dts=None):
+        ptr = None
+        if fixed_dts is not None:
+            arr = np.ascontiguousarray(fixed_dts, dtype=np.float64)
+            assert len(arr) == nsteps
+            ptr = arr.ctypes.data
+            self._keep = arr
+        check(lib().camr_eb_level_advance(self._h, int(nsteps), ptr), "advance")
+
+    def dts(self, n=1 << 16):
+        buf = (C.c_double * n)()
+        taken = C.c_int()
+        check(lib().camr_eb_level_dts(self._h, buf, n, C.byref(taken)), "dts")
+        return np.array(buf[:min(taken.value, n)])
+
+    def kernels_per_step(self):
+        return int(lib().camr_eb_level_kernels_per_step(self._h))
+
+    def error(self):
+        info = native.ErrorInfo()
+        lib().camr_eb_level_get_error(self._h, C.byref(info))
+        return (info.code, info.i, info.j, info.k)
+
+    def sync(self):
+        _torch().cuda.synchronize()
+
+
 class Batch:
     """A batched hydro plan over the boxes of one level (camr_batch_*).
 

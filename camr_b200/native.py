@@ -28,7 +28,7 @@ class HydroParams(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "do_mol", "ppm_type", "plm_iorder", "use_pslope", "use_flattening",
         "transverse_reset_density", "dual_energy_update_E_from_e", "allow_negative_energy",
-        "allow_small_energy", "add_grav_src", "riemann_solver", "pad0")] + [
+        "allow_small_energy", "add_grav_src", "riemann_solver", "eb_weights_type")] + [
         (n, C.c_double) for n in (
             "difmag", "small", "small_dens", "small_temp", "small_pres", "dual_energy_eta1",
             "dual_energy_eta2", "const_grav", "cfl", "init_shrink", "change_max", "fixed_dt",
@@ -129,6 +129,19 @@ SIGNATURES = {
                                       C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
                                       C.POINTER(Fab), C.POINTER(HydroParams), C.c_int,
                                       C.c_double, C.c_void_p]),
+    "camr_eb_level_create": (C.c_int, [C.POINTER(LevelDesc), C.POINTER(EBGeom),
+                                       C.POINTER(HydroParams), C.c_int, C.c_void_p,
+                                       C.POINTER(C.c_void_p)]),
+    "camr_eb_level_destroy": (C.c_int, [C.c_void_p]),
+    "camr_eb_level_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_eb_level_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_eb_level_init_finalize": (C.c_int, [C.c_void_p]),
+    "camr_eb_level_advance": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "camr_eb_level_dts": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int,
+                                    C.POINTER(C.c_int)]),
+    "camr_eb_level_kernels_per_step": (C.c_int64, [C.c_void_p]),
+    "camr_eb_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "camr_eb_level_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
     "camr_adjoint_create": (C.c_int, [C.POINTER(Geom), C.POINTER(HydroParams), C.c_int,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_adjoint_destroy": (C.c_int, [C.c_void_p]),

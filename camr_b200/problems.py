@@ -220,3 +220,13 @@ def grf_blast(n, seed=3, corr=0.1, amp=0.05, p_blast=20.0, r_blast=0.05, gamma=1
     s[UEDEN] = s[UEINT]
     s[UFS] = rho
     return s, r
+
+
+def sod_sphere(n, dx, geo, p_l=1.0, p_r=0.1, rho_l=1.0, rho_r=0.125, x0=0.5):
+    """Sod states (x < x0 left) with a rigid sphere: CAMR_initdata of
+    Exec/SodPlusSphere/prob.H:12-47 on every cell, then EB_set_covered
+    (covered cells zero).  geo: the sphere geometry over a region containing
+    the domain [0, n-1]."""
+    from .eb_geometry import set_covered
+    s = sod(n, dx, p_l=p_l, p_r=p_r, rho_l=rho_l, rho_r=rho_r, x0=x0)
+    return set_covered(s, geo)

@@ -59,7 +59,8 @@ typedef struct {
   int allow_small_energy;
   int add_grav_src;
   int riemann_solver;   /* 0 = the reference's two-shock solver (riemannus) */
-  int pad0;
+  int eb_weights_type;  /* EB flux-redistribution weights (Hydro_utils_eb_K.H:
+                           560-575): 0 one, 1 rho*(e + ke), 2 rho, 3 vfrac */
   double difmag;
   double small;
   double small_dens;
@@ -370,6 +371,35 @@ camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3], const ca
                                 camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
                                 const camr_hydro_params* p, int redist, double dt,
                                 void* stream);
+
+/* ---------------------------------------------------------------------
+ * EB level: one uniform level with an embedded boundary, MOL only
+ * (CAMR_advance's do_mol branch, Source/CAMR_advance.cpp:38-164, with
+ * hydro_umdrv_eb per stage and the EB build's clean_state / computeTemp /
+ * estTimeStep guards for covered cells).  The domain is advanced as one box
+ * with 5 ghost cells.  eb: geometry over exactly grow(domain, 5), host or
+ * device memory, copied into the level.  redist: 0 NoRedist, 1 FluxRedist
+ * (StateRedist is not provided: CAMR_ERR_INVALID).  Covered cells hold zero
+ * state (initData's EB_set_covered); set_state/get_state/advance/dts as
+ * for camr_level_*.
+ */
+typedef struct camr_eb_level camr_eb_level;
+
+camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom* eb,
+                                 const camr_hydro_params* p, int redist, void* stream,
+                                 camr_eb_level** out);
+camr_status camr_eb_level_destroy(camr_eb_level* lev);
+camr_status camr_eb_level_set_state(camr_eb_level* lev, const double* state, int host);
+camr_status camr_eb_level_get_state(camr_eb_level* lev, double* state, int host);
+/* initData's epilogue with the EB guards: enforce_consistent_e where rho > 0,
+ * computeTemp (T = 0 where rho <= 0). */
+camr_status camr_eb_level_init_finalize(camr_eb_level* lev);
+camr_status camr_eb_level_advance(camr_eb_level* lev, int nsteps, const double* fixed_dts);
+/* The dt of every step taken since creation (at most n), and their count. */
+camr_status camr_eb_level_dts(camr_eb_level* lev, double* dts, int n, int* nsteps);
+int64_t camr_eb_level_kernels_per_step(camr_eb_level* lev);
+camr_status camr_eb_level_stream(camr_eb_level* lev, void** stream);
+camr_status camr_eb_level_get_error(camr_eb_level* lev, camr_error_info* info);
 
 /* ---------------------------------------------------------------------
  * Allocation-free per-box hydro.  No counterpart in the reference: it is

@@ -7,10 +7,13 @@ interface (oracle_abi.h):
 * ``restate``: the repo's CPU restatement (hydro_restate.cpp + level_driver.cpp)
 * ``ref``: the reference's own per-box hydro sources compiled against the
   AMReX stand-in in amrex_shim/ (ref_glue.cpp + level_driver.cpp), built into
-  oracle/_ref/ by ``make ref`` where the reference sources are available.
+  oracle/_ref/ by ``make ref`` where the reference sources are available;
+  ``make ref`` also builds the reference's EB hydro (with AMREX_USE_EB) with
+  the EB per-box entry point and the EB level driver (ref_glue_eb.cpp).
 """
 from .binding import (  # noqa: F401
     NVAR, QVAR, NGDNV, Params, Level, load, default_params, make_level,
     hydro_box, advance, advance_fixed_dt, est_dt, init_finalize,
     expand_state, clean_state, amr_run, build, lib_path, lib_path_eb, hydro_box_eb,
+    eb_advance, eb_init_finalize,
 )

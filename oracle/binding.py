@@ -59,6 +59,35 @@ def hydro_box_eb(p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, periodic, uin, g_l
     return dsdt, flx, n
 
 
+def eb_advance(p, lev, geo, state, nsteps, first_step=True, dt_prev=0.0, redist=1):
+    """EB level steps (MOL) on the whole domain as one box.  geo: geometry
+    over grow(domain, 5); state (NVAR, nz, ny, nx) updated in place.
+    Returns (dt_last, dt_hist, nassert)."""
+    lib = load_eb()
+    if not hasattr(lib, "_eb_adv_ready"):
+        lib.orc_eb_advance.restype = C.c_long
+        lib._eb_adv_ready = True
+    assert state.dtype == np.float64 and state.flags["C_CONTIGUOUS"]
+    arr = [np.ascontiguousarray(a, dtype=np.float64) for a in geo["ap"]]
+    fcs = [np.ascontiguousarray(a, dtype=np.float64) for a in geo["fc"]]
+    flag = np.ascontiguousarray(geo["flag"], dtype=np.uint32)
+    vf = np.ascontiguousarray(geo["vfrac"], dtype=np.float64)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    dtp = C.c_double(dt_prev)
+    hist = np.zeros(max(nsteps, 1))
+    n = lib.orc_eb_advance(C.byref(p), C.byref(lev), P(flag), P(vf), P(arr[0]), P(arr[1]),
+                           P(arr[2]), P(fcs[0]), P(fcs[1]), P(fcs[2]), P(state), int(nsteps),
+                           int(bool(first_step)), C.byref(dtp), P(hist), int(redist))
+    return dtp.value, hist[:nsteps], n
+
+
+def eb_init_finalize(p, lev, state):
+    """initData's epilogue with the EB guards on state (NVAR, nz, ny, nx)."""
+    lib = load_eb()
+    assert state.dtype == np.float64 and state.flags["C_CONTIGUOUS"]
+    lib.orc_eb_init_finalize(C.byref(p), C.byref(lev), state.ctypes.data_as(C.c_void_p))
+
+
 def lib_path(kind):
     if kind == "restate":
         return os.path.join(HERE, "_lib", "libcamr_oracle.so")

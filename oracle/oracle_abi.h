@@ -147,6 +147,18 @@ long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const int bx_hi[3
                       int redist, int weights_type, double* dsdt, double* flx0, double* flx1,
                       double* flx2, const double dx[3], double dt);
 
+/* EB level steps, MOL (oracle/_ref/libcamr_ref_eb.so only): the level
+ * driver's step with the EB build's guards, the whole domain as one EB box.
+ * Geometry over grow(domain, 5) as for orc_hydro_box_eb; state: valid
+ * cells, updated in place (covered cells zero). */
+long orc_eb_advance(const orc_params* p, const orc_level* lev, const unsigned* flag,
+                    const double* vfrac, const double* ap0, const double* ap1, const double* ap2,
+                    const double* fc0, const double* fc1, const double* fc2, double* state,
+                    int nsteps, int first_step, double* dt_prev, double* dt_hist, int redist);
+
+/* initData's epilogue with the EB guards (rho > 0 only), valid cells. */
+void orc_eb_init_finalize(const orc_params* p, const orc_level* lev, double* state);
+
 /* clean_state on the valid cells (Source/CAMR.cpp:1253-1262). */
 void orc_clean_state(const orc_params* p, const orc_level* lev, double* state);
 

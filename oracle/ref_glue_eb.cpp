@@ -185,3 +185,366 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
   });
   return shim_assert_count();
 }
+
+// ---------------------------------------------------------------------------
+// EB level step (MOL), the restated level driver's CAMR_advance + post_timestep
+// (Source/CAMR_advance.cpp:38-164, Source/CAMR.cpp:679-718) with the EB
+// build's guards: covered cells skip enforce_min_density and
+// normalize_species (Source/CAMR.cpp:877-891, :960-968), reset_internal_energy
+// runs only where rho > 0 (Utils/CAMR_reset_internal_e.H:36-38), computeTemp
+// sets T = 0 first (Source/CAMR.cpp:1164-1168), and the CFL minimum skips
+// covered cells (:522-540).  The domain is advanced as one box; its ghost
+// cells (5, numGrow for MOL + flux redistribution, CAMR.H:455-479) are
+// filled as the single-level driver fills them.  Covered cells hold the
+// state EB_set_covered gives them at initialisation (zero).
+#include "EOS.H"
+
+namespace {
+
+struct LevelEB {
+  Box dom, G;
+  int periodic[3];
+  int bclo[3], bchi[3];
+  double dx[3];
+  Array4<EBCellFlag const> flag;
+};
+
+inline bool covered(const LevelEB& L, int i, int j, int k) { return L.flag(i, j, k).isCovered(); }
+
+// reset_internal_energy on one cell (Utils/CAMR_reset_internal_e.H:13-129),
+// skipped where rho <= 0 as the EB build does.
+void reset_e_eb(const orc_params* p, Array4<Real> const& S, int i, int j, int k) {
+  const Real rho = S(i, j, k, URHO);
+  if (!(rho > 0.)) return;
+  const Real rhoInv = 1.0 / rho;
+  const Real Up = S(i, j, k, UMX) * rhoInv;
+  const Real Vp = S(i, j, k, UMY) * rhoInv;
+  const Real Wp = S(i, j, k, UMZ) * rhoInv;
+  const Real ke = 0.5 * (Up * Up + Vp * Vp + Wp * Wp);
+  const Real eden = S(i, j, k, UEDEN) * rhoInv;
+  Real massfrac[NUM_SPECIES];
+  for (int n = 0; n < NUM_SPECIES; ++n) massfrac[n] = S(i, j, k, n + UFS) * rhoInv;
+  Real e_out = 0., small_e = 0.;
+  const Real small_T = p->small_temp;
+  if (p->allow_small_energy == 0) {
+    EOS::RTY2E(rho, small_T, massfrac, small_e);
+    if (eden < small_e) {
+      if (S(i, j, k, UEINT) * rhoInv < small_e) {
+        const Real T = std::max(S(i, j, k, UTEMP), small_T);
+        EOS::RTY2E(rho, T, massfrac, e_out);
+        S(i, j, k, UEINT) = rho * e_out;
+      }
+      S(i, j, k, UEDEN) = S(i, j, k, UEINT) + rho * ke;
+    } else {
+      const Real rho_eint = S(i, j, k, UEDEN) - S(i, j, k, URHO) * ke;
+      if (rho_eint > 0. && rho_eint / S(i, j, k, UEDEN) > p->dual_energy_eta2)
+        S(i, j, k, UEINT) = rho_eint;
+      if (S(i, j, k, UEINT) * rhoInv < small_e) {
+        const Real T = std::max(S(i, j, k, UTEMP), small_T);
+        EOS::RTY2E(rho, T, massfrac, e_out);
+        if (p->dual_energy_update_E_from_e == 1)
+          S(i, j, k, UEDEN) += (rho * e_out - S(i, j, k, UEINT));
+        S(i, j, k, UEINT) = S(i, j, k, URHO) * e_out;
+      }
+    }
+  } else if (p->allow_negative_energy == 0) {
+    if (S(i, j, k, UEDEN) < 0.) {
+      if (S(i, j, k, UEINT) < 0.) {
+        EOS::RTY2E(rho, small_T, massfrac, e_out);
+        S(i, j, k, UEINT) = rho * e_out;
+      }
+      S(i, j, k, UEDEN) = S(i, j, k, UEINT) + rho * ke;
+    } else {
+      const Real rho_eint = S(i, j, k, UEDEN) - rho * ke;
+      if (rho_eint > 0. && rho_eint / S(i, j, k, UEDEN) > p->dual_energy_eta2) {
+        S(i, j, k, UEINT) = rho_eint;
+      } else if (S(i, j, k, UEINT) > 0 && p->dual_energy_update_E_from_e == 1) {
+        S(i, j, k, UEDEN) = S(i, j, k, UEINT) + rho * ke;
+      } else if (S(i, j, k, UEINT) <= 0.) {
+        EOS::RTY2E(rho, small_T, massfrac, e_out);
+        S(i, j, k, UEINT) = rho * e_out;
+        if (p->dual_energy_update_E_from_e == 1)
+          S(i, j, k, UEDEN) += (rho * e_out - S(i, j, k, UEINT));
+      }
+    }
+  } else {
+    S(i, j, k, UEINT) = S(i, j, k, UEDEN) - rho * ke;
+  }
+}
+
+void temp_eb(const orc_params* p, Array4<Real> const& S, int i, int j, int k) {
+  reset_e_eb(p, S, i, j, k);
+  S(i, j, k, UTEMP) = 0.0;
+  if (S(i, j, k, URHO) > 0.) {
+    const Real rhoInv = 1.0 / S(i, j, k, URHO);
+    Real T = S(i, j, k, UTEMP);
+    const Real e = S(i, j, k, UEINT) * rhoInv;
+    Real massfrac[NUM_SPECIES];
+    for (int n = 0; n < NUM_SPECIES; ++n) massfrac[n] = S(i, j, k, UFS + n) * rhoInv;
+    const Real rho = S(i, j, k, URHO);
+    EOS::REY2T(rho, e, massfrac, T);
+    S(i, j, k, UTEMP) = T;
+  }
+}
+
+void normalize_eb(Array4<Real> const& S, int i, int j, int k) {
+  Real sum = 0.;
+  for (int n = 0; n < NUM_SPECIES; n++) {
+    S(i, j, k, UFS + n) = std::max(std::min(S(i, j, k, URHO), S(i, j, k, UFS + n)), 0.0);
+    sum += S(i, j, k, UFS + n);
+  }
+  if (S(i, j, k, URHO) > 0.) {
+    sum /= S(i, j, k, URHO);
+    for (int n = 0; n < NUM_SPECIES; n++) S(i, j, k, UFS + n) /= sum;
+  }
+}
+
+// enforce_min_density over the box `t` (the domain: one tile), skipping
+// covered cells; returns the number of cells with zero density.
+long enforce_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S, const Box& t) {
+  long nerr = 0;
+  ParallelFor(t, [&](int i, int j, int k) {
+    if (covered(L, i, j, k)) return;
+    if (S(i, j, k, URHO) == 0.) {
+      ++nerr;
+    } else if (S(i, j, k, URHO) < p->small_dens) {
+      Real max_dens = S(i, j, k, URHO);
+      int is = i, js = j, ks = k;
+      for (int kk = -1; kk <= 1; kk++)
+        for (int jj = -1; jj <= 1; jj++)
+          for (int ii = -1; ii <= 1; ii++)
+            if (t.contains(IntVect(i + ii, j + jj, k + kk)) &&
+                S(i + ii, j + jj, k + kk, URHO) > max_dens) {
+              is = i + ii; js = j + jj; ks = k + kk;
+              max_dens = S(is, js, ks, URHO);
+            }
+      if (max_dens < p->small_dens) {
+        Real massfrac[NUM_SPECIES];
+        for (int n = 0; n < NUM_SPECIES; ++n) massfrac[n] = S(i, j, k, UFS + n) / S(i, j, k, URHO);
+        Real small_e;
+        EOS::RTY2E(p->small_dens, p->small_temp, massfrac, small_e);
+        S(i, j, k, URHO) = p->small_dens;
+        S(i, j, k, UTEMP) = p->small_temp;
+        S(i, j, k, UMX) = 0.;
+        S(i, j, k, UMY) = 0.;
+        S(i, j, k, UMZ) = 0.;
+        S(i, j, k, UEINT) = p->small_dens * small_e;
+        S(i, j, k, UEDEN) = S(i, j, k, UEINT);
+      } else {
+        for (int n = 0; n < NVAR; ++n) S(i, j, k, n) = S(is, js, ks, n);
+      }
+    }
+  });
+  return nerr;
+}
+
+long clean_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S) {
+  long nerr = enforce_eb(p, L, S, L.dom);
+  ParallelFor(L.dom, [&](int i, int j, int k) {
+    if (!covered(L, i, j, k)) normalize_eb(S, i, j, k);
+  });
+  ParallelFor(L.dom, [&](int i, int j, int k) { temp_eb(p, S, i, j, k); });
+  return nerr;
+}
+
+// BC kind of component n in direction d for the physical BC word phys
+// (Source/Utils/CAMR_setup.cpp:19-21): 1 ext_dir, 2 foextrap, 3 even, 4 odd.
+int bc_kind_of(int n, int d, int phys) {
+  static const int scalar_bc[] = {0, 1, 2, 3, 3, 3};
+  static const int norm_vel_bc[] = {0, 1, 2, 4, 4, 4};
+  static const int tang_vel_bc[] = {0, 1, 2, 3, 3, 4};
+  if (n == UMX || n == UMY || n == UMZ) return (n - UMX == d) ? norm_vel_bc[phys] : tang_vel_bc[phys];
+  return scalar_bc[phys];
+}
+
+// expand_state: FillPatch(src) into B over G + clean_state(B).
+long expand_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& src,
+               Array4<Real> const& B) {
+  ParallelFor(L.dom, [&](int i, int j, int k) {
+    for (int n = 0; n < NVAR; ++n) B(i, j, k, n) = src(i, j, k, n);
+  });
+  long nerr = enforce_eb(p, L, B, L.dom);
+  ParallelFor(L.dom, [&](int i, int j, int k) {
+    if (!covered(L, i, j, k)) normalize_eb(B, i, j, k);
+  });
+  ParallelFor(L.G, [&](int i, int j, int k) {
+    const int c[3] = {i, j, k};
+    bool inside = true, physical = false;
+    int img[3];
+    for (int d = 0; d < 3; ++d) {
+      img[d] = c[d];
+      if (c[d] < L.dom.lo[d] || c[d] > L.dom.hi[d]) {
+        inside = false;
+        if (L.periodic[d]) {
+          const int len = L.dom.hi[d] - L.dom.lo[d] + 1;
+          img[d] = L.dom.lo[d] + (((c[d] - L.dom.lo[d]) % len) + len) % len;
+        } else {
+          physical = true;
+        }
+      }
+    }
+    if (inside) return;
+    for (int n = 0; n < NVAR; ++n) {
+      if (!physical) {
+        B(i, j, k, n) = B(img[0], img[1], img[2], n);
+        continue;
+      }
+      int id[3] = {img[0], img[1], img[2]};
+      bool neg = false;
+      for (int d = 0; d < 3; ++d) {
+        if (L.periodic[d]) continue;
+        if (id[d] < L.dom.lo[d]) {
+          const int t = bc_kind_of(n, d, L.bclo[d]);
+          if (t == 1 || t == 2) id[d] = L.dom.lo[d];
+          else { id[d] = 2 * L.dom.lo[d] - id[d] - 1; if (t == 4) neg = !neg; }
+        } else if (id[d] > L.dom.hi[d]) {
+          const int t = bc_kind_of(n, d, L.bchi[d]);
+          if (t == 1 || t == 2) id[d] = L.dom.hi[d];
+          else { id[d] = 2 * L.dom.hi[d] - id[d] + 1; if (t == 4) neg = !neg; }
+        }
+      }
+      const Real v = src(id[0], id[1], id[2], n);
+      B(i, j, k, n) = neg ? -v : v;
+    }
+  });
+  ParallelFor(L.G, [&](int i, int j, int k) { temp_eb(p, B, i, j, k); });
+  return nerr;
+}
+
+double est_dt_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S) {
+  if (p->fixed_dt > 0.0) return p->fixed_dt;
+  double estdt = p->max_dt;
+  double estdt_hydro = p->max_dt / p->cfl;
+  double dt = std::numeric_limits<double>::max();
+  ParallelFor(L.dom, [&](int i, int j, int k) {
+    if (covered(L, i, j, k)) return;
+    const double rho = S(i, j, k, URHO);
+    const double rhoInv = 1.0 / rho;
+    const double eint = S(i, j, k, UEINT) / rho;
+    const double pres = (p->eos_gamma - 1.0) * rho * eint;
+    const double c = std::sqrt(p->eos_gamma * pres / rho);
+    dt = std::min(dt, L.dx[0] / (c + std::fabs(S(i, j, k, UMX) * rhoInv)));
+    dt = std::min(dt, L.dx[1] / (c + std::fabs(S(i, j, k, UMY) * rhoInv)));
+    dt = std::min(dt, L.dx[2] / (c + std::fabs(S(i, j, k, UMZ) * rhoInv)));
+  });
+  estdt_hydro = std::min(estdt_hydro, dt);
+  estdt_hydro *= p->cfl;
+  if (estdt_hydro < estdt) estdt = estdt_hydro;
+  return estdt;
+}
+
+}  // namespace
+
+extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const unsigned* flag_in,
+                               const double* vfrac, const double* ap0, const double* ap1,
+                               const double* ap2, const double* fc0, const double* fc1,
+                               const double* fc2, double* state, int nsteps, int first_step,
+                               double* dt_prev, double* dt_hist, int redist) {
+  LevelEB L;
+  for (int d = 0; d < 3; ++d) {
+    L.dom.lo[d] = lev->dom_lo[d];
+    L.dom.hi[d] = lev->dom_hi[d];
+    L.periodic[d] = lev->is_periodic[d];
+    L.bclo[d] = lev->bc_lo[d];
+    L.bchi[d] = lev->bc_hi[d];
+    L.dx[d] = lev->dx[d];
+  }
+  L.G = amrex::grow(L.dom, 5);
+  std::vector<EBCellFlag> fl(size_t(L.G.numPts()));
+  for (size_t c = 0; c < fl.size(); ++c) fl[c] = EBCellFlag(flag_in[c]);
+  L.flag = Array4<EBCellFlag const>(fl.data(), L.G.lo,
+                                    IntVect(L.G.hi[0] + 1, L.G.hi[1] + 1, L.G.hi[2] + 1), 1);
+  auto S = view(state, L.dom.lo.v, L.dom.hi.v, NVAR);
+  FArrayBox Sold_f(L.dom, NVAR), B_f(L.G, NVAR), B2_f(L.G, NVAR), d1_f(L.dom, NVAR),
+      d2_f(L.dom, NVAR);
+  auto S_old = Sold_f.array();
+  auto B = B_f.array();
+  auto B2 = B2_f.array();
+  auto k1 = d1_f.array();
+  auto k2 = d2_f.array();
+  std::vector<double> fbuf[3];
+  for (int d = 0; d < 3; ++d) {
+    Box fb = amrex::surroundingNodes(L.dom, d);
+    fbuf[d].assign(size_t(fb.numPts()) * NVAR, 0.0);
+  }
+  const int g_lo[3] = {L.G.lo[0], L.G.lo[1], L.G.lo[2]};
+  const int g_hi[3] = {L.G.hi[0], L.G.hi[1], L.G.hi[2]};
+  const int* dlo = L.dom.lo.v;
+  const int* dhi = L.dom.hi.v;
+  long nerr = 0;
+  double dt_level = *dt_prev;
+  for (int step = 0; step < nsteps; ++step) {
+    double dt;
+    const double est = est_dt_eb(p, L, S);
+    if (first_step && step == 0) {
+      const double init_dt = (p->initial_dt > 0.0) ? p->initial_dt : p->init_shrink * est;
+      dt = std::min(std::numeric_limits<double>::max(), 1 * init_dt) / 1;
+    } else {
+      double dt_min = est;
+      if (p->fixed_dt <= 0.0) dt_min = std::min(dt_min, p->change_max * dt_level);
+      dt = std::min(std::numeric_limits<double>::max(), 1 * dt_min) / 1;
+    }
+    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S_old(i, j, k, n) = S(i, j, k, n); });
+    nerr += clean_eb(p, L, S_old);
+    nerr += expand_eb(p, L, S_old, B);
+    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S(i, j, k, n) = B(i, j, k, n); });
+    if (p->add_grav_src) {
+      ParallelFor(L.dom, [&](int i, int j, int k) {
+        Real src[NVAR];
+        for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+        src[UMZ] = p->const_grav * S_old(i, j, k, URHO);
+        src[UEDEN] = p->const_grav * S_old(i, j, k, UMZ);
+        for (int n = 0; n < NVAR; ++n) S(i, j, k, n) += dt * src[n];
+      });
+    }
+    nerr += orc_hydro_box_eb(p, dlo, dhi, dlo, dhi, L.bclo, L.bchi, L.periodic, B.p, g_lo, g_hi,
+                             flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, redist, 2, k1.p,
+                             fbuf[0].data(), fbuf[1].data(), fbuf[2].data(), L.dx, dt);
+    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S(i, j, k, n) += dt * k1(i, j, k, n); });
+    nerr += expand_eb(p, L, S, B2);
+    nerr += orc_hydro_box_eb(p, dlo, dhi, dlo, dhi, L.bclo, L.bchi, L.periodic, B2.p, g_lo, g_hi,
+                             flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, redist, 2, k2.p,
+                             fbuf[0].data(), fbuf[1].data(), fbuf[2].data(), L.dx, dt);
+    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
+      S(i, j, k, n) = 0.5 * B2(i, j, k, n) + 0.5 * S_old(i, j, k, n);
+    });
+    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
+      S(i, j, k, n) += 0.5 * dt * k2(i, j, k, n);
+    });
+    nerr += clean_eb(p, L, S);
+    if (p->add_grav_src) {
+      ParallelFor(L.dom, [&](int i, int j, int k) {
+        Real src[NVAR];
+        for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+        src[UMZ] = 0.5 * p->const_grav * (S(i, j, k, URHO) - S_old(i, j, k, URHO));
+        src[UEDEN] = 0.5 * p->const_grav * (S(i, j, k, UMZ) - S_old(i, j, k, UMZ));
+        for (int n = 0; n < NVAR; ++n) S(i, j, k, n) += dt * src[n];
+      });
+      nerr += clean_eb(p, L, S);
+    }
+    nerr += clean_eb(p, L, S);
+    dt_level = dt;
+    if (dt_hist) dt_hist[step] = dt;
+  }
+  *dt_prev = dt_level;
+  return nerr;
+}
+
+// initData's epilogue in the EB build (Source/CAMR.cpp:414-420):
+// enforce_consistent_e where rho > 0 (:910-939), then computeTemp.
+extern "C" void orc_eb_init_finalize(const orc_params* p, const orc_level* lev, double* state) {
+  const int* lo = lev->dom_lo;
+  const int* hi = lev->dom_hi;
+  auto S = view(state, lo, hi, NVAR);
+  const Box dom(IntVect(lo[0], lo[1], lo[2]), IntVect(hi[0], hi[1], hi[2]));
+  ParallelFor(dom, [&](int i, int j, int k) {
+    if (S(i, j, k, URHO) > 0.) {
+      const Real rhoInv = 1.0 / S(i, j, k, URHO);
+      const Real u = S(i, j, k, UMX) * rhoInv;
+      const Real v = S(i, j, k, UMY) * rhoInv;
+      const Real w = S(i, j, k, UMZ) * rhoInv;
+      S(i, j, k, UEDEN) = S(i, j, k, UEINT) + 0.5 * S(i, j, k, URHO) * (u * u + v * v + w * w);
+    }
+  });
+  ParallelFor(dom, [&](int i, int j, int k) { temp_eb(p, S, i, j, k); });
+}

@@ -106,3 +106,56 @@ def test_eb_box_conserves_mass_and_energy():
         tot = (vf * d[c]).sum()
         ref = (vf * np.abs(d[c])).sum()
         assert abs(tot) <= 1e-13 * ref, (c, tot, ref)
+
+
+@pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
+@pytest.mark.parametrize("kind,redist", [("periodic", 1), ("periodic", 0), ("sod", 1)])
+def test_eb_level_steps_match_oracle(kind, redist):
+    """camr_eb_level_* steps (dt on the device, graph-captured after the
+    first step) against the EB oracle's level driver: states and dts."""
+    _torch()
+    from test_oracle_eb import eb_level_case
+    n = (16, 16, 16) if kind == "periodic" else (32, 16, 16)
+    p, lev, geo, s = eb_level_case(kind, n=n)
+    if not redist:
+        p.fixed_dt = 1e-4
+    ref = s.copy()
+    nsteps = 6
+    _, ref_dts, nass = oracle.eb_advance(p, lev, geo, ref, nsteps, redist=redist)
+    assert nass == 0
+    if kind == "periodic":
+        geom = hydro.make_geom(n, dx=(1.0 / n[0],) * 3)
+    else:
+        geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
+                               dx=(2.0 / n[0],) * 3)
+    prm = native.default_params(do_mol=1, cfl=0.3, fixed_dt=p.fixed_dt)
+    L = hydro.EBLevel(geom, prm, geo, redist=redist)
+    L.set_state(s)
+    L.advance(nsteps)
+    got = L.get_state()
+    dts = L.dts()
+    assert L.error()[0] == 0
+    assert L.kernels_per_step() > 0
+    assert_bitwise(dts, ref_dts, "dt")
+    assert_bitwise(got, ref, "state")
+    L.close()
+
+
+def test_eb_level_init_finalize_matches_oracle():
+    _torch()
+    if not HAVE_EB:
+        pytest.skip("EB oracle library not built")
+    from test_oracle_eb import eb_level_case
+    n = (32, 16, 16)
+    p, lev, geo, _ = eb_level_case("sod", n=n)
+    dx = 2.0 / n[0]
+    raw = np.ascontiguousarray(E.set_covered(P.sod_sphere(n, (dx,) * 3, geo), geo))
+    ref = raw.copy()
+    oracle.eb_init_finalize(p, lev, ref)
+    geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
+                           dx=(dx,) * 3)
+    L = hydro.EBLevel(geom, native.default_params(do_mol=1, cfl=0.3), geo)
+    L.set_state(raw)
+    L.init_finalize()
+    assert_bitwise(L.get_state(), ref, "state")
+    L.close()
