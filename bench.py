@@ -297,11 +297,13 @@ def run_camr(args, world, rank, local, pg):
     batched = None
     amr = None
     adj = None
+    ebc = None
     if rank == 0 and world == 1 and not args.no_batched:
         L.close()
         batched = batched_comparison(args)
         amr = amr_comparison(args)
         adj = adjoint_comparison(args)
+        ebc = eb_comparison(args)
 
     if rank == 0:
         line = {
@@ -320,6 +322,7 @@ def run_camr(args, world, rank, local, pg):
             "batched_amr_patches": batched,
             "amr_two_level": amr,
             "adjoint_c3": adj,
+            "eb_c4": ebc,
         }
         print(json.dumps(line))
     L.close()
@@ -470,6 +473,103 @@ def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
     return out
 
 
+def eb_comparison(args, n=(256, 128, 128), nsteps=150, warmup=3, cpu_n=(64, 32, 32)):
+    """The embedded-boundary configuration: Sod (x < 0.5 left) with a rigid
+    sphere r = 0.15 at (1, 0.5, 0.5) on [0,2]x[0,1]^2 (256x128x128), x
+    outflow, y/z slip walls, MOL-PLM RK2 at CFL 0.3 with flux
+    redistribution, 150 steps (dt on the device, graph-captured).  The
+    domain is one EB box: regular, cut and covered cells share every launch.
+    Also the same level without the sphere (the regular MOL level driver)
+    for the EB overhead, and the reference's EB kernels on the host on a
+    small sample of the same problem."""
+    import torch
+
+    from camr_b200 import eb_geometry, hydro, native, problems
+    dx = 2.0 / n[0]
+    t0 = time.time()
+    geo = eb_geometry.sphere_geometry((-5, -5, -5), (n[0] + 4, n[1] + 4, n[2] + 4), dx,
+                                      center=(1.0, 0.5, 0.5), radius=0.15)
+    geo_s = time.time() - t0
+    s0 = problems.sod_sphere(n, (dx,) * 3, geo)
+    geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
+                           dx=(dx,) * 3)
+    prm = native.default_params(do_mol=1, ppm_type=0, cfl=0.3)
+    typ = geo["flag"][5:-5, 5:-5, 5:-5] & 3
+    nb = [v // 32 for v in n]
+    t = typ.reshape(nb[2], 32, nb[1], 32, nb[0], 32)
+    has_cov = (t == 3).any(axis=(1, 3, 5))
+    has_cut = (t == 1).any(axis=(1, 3, 5))
+    all_cov = (t == 3).all(axis=(1, 3, 5))
+    boxes = {"regular": int((~has_cov & ~has_cut).sum()), "cut": int((has_cut & ~all_cov).sum()),
+             "covered": int(all_cov.sum())}
+    zones = n[0] * n[1] * n[2]
+    out = {"domain": list(n), "cells": zones, "cut_cells": int((typ == 1).sum()),
+           "covered_cells": int((typ == 3).sum()), "boxes_32": boxes,
+           "geometry_build_s": geo_s, "method": "MOL-PLM RK2, two-shock Riemann, FluxRedist",
+           "cfl": 0.3, "steps": nsteps}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    L = hydro.EBLevel(geom, prm, geo, redist=1)
+    st = L.torch_stream()
+    L.set_state(s0)
+    L.init_finalize()
+    L.advance(warmup)
+    torch.cuda.synchronize()
+    e0.record(st)
+    L.advance(nsteps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / nsteps
+    fin = L.get_state()
+    out["eb_level"] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3),
+                       "kernels_per_step_graph": L.kernels_per_step(),
+                       "device_error": list(L.error()),
+                       "t_final": float(L.dts().sum()),
+                       "finite": bool(np.isfinite(fin).all())}
+    L.close()
+    del L
+    torch.cuda.empty_cache()
+    # the same domain and flow without the sphere, regular MOL level driver
+    R = hydro.Level(geom, prm, use_graph=True)
+    st = R.torch_stream()
+    R.set_state(problems.sod(n, (dx,) * 3))
+    R.init_finalize()
+    R.advance(warmup)
+    torch.cuda.synchronize()
+    e0.record(st)
+    R.advance(nsteps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    msr = e0.elapsed_time(e1) / nsteps
+    out["regular_level_same_domain"] = {"ms_per_step": msr,
+                                        "zone_updates_per_s": zones / (msr * 1e-3)}
+    out["eb_over_regular_time"] = ms / msr
+    R.close()
+    del R
+    torch.cuda.empty_cache()
+    if not args.no_cpu:
+        import oracle
+        if os.path.exists(oracle.lib_path_eb()):
+            cdx = 2.0 / cpu_n[0]
+            cgeo = eb_geometry.sphere_geometry((-5, -5, -5), tuple(v + 4 for v in cpu_n), cdx,
+                                               center=(1.0, 0.5, 0.5), radius=0.15)
+            cs = np.ascontiguousarray(problems.sod_sphere(cpu_n, (cdx,) * 3, cgeo))
+            cp = oracle.default_params(do_mol=1, cfl=0.3)
+            clev = oracle.make_level(cpu_n, periodic=(0, 0, 0), bc_lo=(2, 4, 4),
+                                     bc_hi=(2, 4, 4), dx=(cdx,) * 3)
+            oracle.eb_init_finalize(cp, clev, cs)
+            csteps = 2
+            t0 = time.time()
+            oracle.eb_advance(cp, clev, cgeo, cs, csteps)
+            secs = time.time() - t0
+            out["cpu_baseline"] = {
+                "value": cpu_n[0] * cpu_n[1] * cpu_n[2] * csteps / secs,
+                "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+                "sample": f"{cpu_n[0]}x{cpu_n[1]}x{cpu_n[2]} Sod+sphere, {csteps} level steps, "
+                          "the reference's EB hydro kernels (one thread)"}
+    return out
+
+
 def adjoint_comparison(args, n=128, nsteps=200, every=20, fd_cells=0):
     """The adjoint configuration: 128^3 periodic, MOL-PLM RK2 (CFL 0.3),
     200 steps with a checkpoint every 20, J = mass inside the sphere r < 0.2
@@ -600,7 +700,7 @@ def main():
     ap.add_argument("--impl", choices=["camr", "reference"], default="camr")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["c1", "c2-batched", "c2-amr", "c3-adjoint"],
+    ap.add_argument("--workload", choices=["c1", "c2-batched", "c2-amr", "c3-adjoint", "c4-eb"],
                     default="c1")
     ap.add_argument("--adj-n", type=int, default=128, help="c3-adjoint domain size")
     ap.add_argument("--adj-steps", type=int, default=200, help="c3-adjoint steps")
@@ -620,6 +720,15 @@ def main():
             print(json.dumps({"workload": "c3-adjoint",
                               **adjoint_comparison(args, n=args.adj_n, nsteps=args.adj_steps,
                                                    fd_cells=args.fd_cells)}))
+        return
+    if args.workload == "c4-eb":
+        import torch
+        from camr_b200 import build, native
+        if not os.path.exists(native.LIB_PATH):
+            build.build()
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"workload": "c4-eb", **eb_comparison(args)}))
         return
     if args.workload == "c2-amr":
         import torch
