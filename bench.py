@@ -117,6 +117,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def profile_range(args, on):
+    """With --profile-range, bracket a timed region with cudaProfilerStart /
+    cudaProfilerStop so that `ncu --profile-from-start off` lists exactly the
+    launches of that region."""
+    if not getattr(args, "profile_range", False):
+        return
+    import torch
+    torch.cuda.synchronize()
+    if on:
+        torch.cuda.profiler.start()
+    else:
+        torch.cuda.profiler.stop()
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -221,10 +235,12 @@ def run_camr(args, world, rank, local, pg):
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
+    profile_range(args, True)
     e0.record(st)
     L.advance(args.steps)
     e1.record(st)
     torch.cuda.synchronize()
+    profile_range(args, False)
     clocks = sampler.stop()
     barrier()
     ms = e0.elapsed_time(e1)
@@ -417,7 +433,7 @@ def batched_comparison(args, steps=5, warmup=2):
     return out
 
 
-def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
+def amr_comparison(args, steps=None, per_box_steps=2, warmup=3):
     """The two-level configuration end to end on the device: base 256^3 +
     the uneven fine boxes (ratio 2, two subcycled fine steps per coarse
     step, flux-register reflux, average down).  Zone-updates per coarse
@@ -427,6 +443,8 @@ def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
     import torch
 
     from camr_b200 import hydro, native, problems
+    if steps is None:
+        steps = args.amr_steps
     n0 = (256, 256, 256)
     fine_n = 512
     boxes = problems.amr_box_list(nbox=args.nbox, fine_n=fine_n)
@@ -456,10 +474,15 @@ def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
             h.set_fine_mode(mode)
             h.advance(1)
             torch.cuda.synchronize()
+            prof = name == "mol_plm" and mname == "batched_graph"
+            if prof:
+                profile_range(args, True)
             e0.record(st)
             h.advance(k)
             e1.record(st)
             torch.cuda.synchronize()
+            if prof:
+                profile_range(args, False)
             ms = e0.elapsed_time(e1) / k
             res[mname] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3)}
         res["kernels_per_step_graph"] = h.kernels_per_step()
@@ -473,7 +496,7 @@ def amr_comparison(args, steps=4, per_box_steps=2, warmup=3):
     return out
 
 
-def eb_comparison(args, n=(256, 128, 128), nsteps=150, warmup=3, cpu_n=(64, 32, 32)):
+def eb_comparison(args, n=(256, 128, 128), nsteps=None, warmup=3, cpu_n=(64, 32, 32)):
     """The embedded-boundary configuration: Sod (x < 0.5 left) with a rigid
     sphere r = 0.15 at (1, 0.5, 0.5) on [0,2]x[0,1]^2 (256x128x128), x
     outflow, y/z slip walls, MOL-PLM RK2 at CFL 0.3 with flux
@@ -485,6 +508,8 @@ def eb_comparison(args, n=(256, 128, 128), nsteps=150, warmup=3, cpu_n=(64, 32, 
     import torch
 
     from camr_b200 import eb_geometry, hydro, native, problems
+    if nsteps is None:
+        nsteps = args.eb_steps
     dx = 2.0 / n[0]
     t0 = time.time()
     geo = eb_geometry.sphere_geometry((-5, -5, -5), (n[0] + 4, n[1] + 4, n[2] + 4), dx,
@@ -515,10 +540,12 @@ def eb_comparison(args, n=(256, 128, 128), nsteps=150, warmup=3, cpu_n=(64, 32, 
     L.init_finalize()
     L.advance(warmup)
     torch.cuda.synchronize()
+    profile_range(args, True)
     e0.record(st)
     L.advance(nsteps)
     e1.record(st)
     torch.cuda.synchronize()
+    profile_range(args, False)
     ms = e0.elapsed_time(e1) / nsteps
     fin = L.get_state()
     out["eb_level"] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3),
@@ -707,6 +734,11 @@ def main():
     ap.add_argument("--fd-cells", type=int, default=64,
                     help="finite-difference cells of the c3-adjoint workload")
     ap.add_argument("--nbox", type=int, default=350)
+    ap.add_argument("--amr-steps", type=int, default=4, help="timed coarse steps of c2-amr")
+    ap.add_argument("--eb-steps", type=int, default=150, help="timed steps of c4-eb")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the timed region (C1 steps; c2-amr MOL batched steps; "
+                         "c4-eb EB level steps) with cudaProfilerStart/Stop")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-per-box comparison in the default line")
     args = ap.parse_args()
