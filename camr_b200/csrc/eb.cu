@@ -10,10 +10,11 @@
 //                         Riemann on connected faces, else zero
 //                         (MOL/MOL_umeth_eb.cpp:21-191)
 //   K4 EB div u           nodes of grow(bx,4) inside the (periodically grown)
-//                         domain (Hydro_utils_eb_K.H:31-78)
+//                         domain (Hydro_utils_eb_K.H:31-78); issued before K3
 //   K5 adjust             artificial viscosity on every face of the flux
 //                         box; species normalisation and area on open faces
-//                         (Hydro_adjust_fluxes.cpp:48-171)
+//                         (Hydro_adjust_fluxes.cpp:48-171); inside K3's
+//                         kernel, after each face's flux
 //   K6 divergence         cells of grow(bx,2): face-centroid interpolated
 //                         fluxes, the wall flux of cut cells, -div, p div u,
 //                         the redistribution weight (Hydro_consup.cpp:29-98,
@@ -145,6 +146,10 @@ __device__ __forceinline__ void eb_face(int i, int j, int k, const EBWork& W, co
   W.ft[d][at + UTEMP * s.sn] = 0.0;
 }
 
+template <int d>
+__device__ __forceinline__ void eb_adjust(int i, int j, int k, const EBWork& W, const EBG& G,
+                                          const KGeom& g, const KParams& P, const DFab& u);
+
 __device__ __forceinline__ bool in_region(const Region& r, int i, int j, int k) {
   return i >= r.lo[0] && i < r.lo[0] + r.n[0] && j >= r.lo[1] && j < r.lo[1] + r.n[1] &&
          k >= r.lo[2] && k < r.lo[2] + r.n[2];
@@ -152,30 +157,36 @@ __device__ __forceinline__ bool in_region(const Region& r, int i, int j, int k) 
 
 // Faces of the flux box ra[d] (faces of grow(bx,3)): the Riemann flux on
 // the faces of rf[d] (faces of grow(bx,2), transverse +1), zero on the
-// outer layer, which only the artificial viscosity touches.
+// outer layer; then adjust_fluxes_eb on every face of ra[d] (its
+// artificial viscosity is added to the face's own value, so doing it here
+// rather than in a separate pass changes no bits; nodal div u is computed
+// before this kernel).
 template <int d>
 __device__ __forceinline__ void eb_face_or_zero(const Region& rf, int i, int j, int k,
                                                 const EBWork& W, const EBG& G, const KGeom& g,
-                                                const KParams& P) {
+                                                const KParams& P, const DFab& u) {
   if (in_region(rf, i, j, k)) {
     eb_face<d>(i, j, k, W, G, g, P);
-    return;
+  } else {
+    const int64_t at = W.s.idx(i, j, k);
+    for (int n = 0; n < NVAR; ++n) W.ft[d][at + n * W.s.sn] = 0.;
+    W.qf[d][at] = 0.;
+    W.qf[d][at + W.s.sn] = 0.;
   }
-  const int64_t at = W.s.idx(i, j, k);
-  for (int n = 0; n < NVAR; ++n) W.ft[d][at + n * W.s.sn] = 0.;
-  W.qf[d][at] = 0.;
-  W.qf[d][at + W.s.sn] = 0.;
+  eb_adjust<d>(i, j, k, W, G, g, P, u);
 }
 
 __global__ void __launch_bounds__(kEB) k_eb_face(Region r0, Region r1, Region r2, Region a0,
                                                   Region a1, Region a2, EBWork W, EBG G,
-                                                  KGeom g, KParams P) {
+                                                  KGeom g, KParams P, DFab u) {
   int i, j, k;
   const int64_t t = etid();
   switch (blockIdx.y) {
-    case 0: if (region_cell(a0, t, i, j, k)) eb_face_or_zero<0>(r0, i, j, k, W, G, g, P); break;
-    case 1: if (region_cell(a1, t, i, j, k)) eb_face_or_zero<1>(r1, i, j, k, W, G, g, P); break;
-    default: if (region_cell(a2, t, i, j, k)) eb_face_or_zero<2>(r2, i, j, k, W, G, g, P); break;
+    case 0: if (region_cell(a0, t, i, j, k)) eb_face_or_zero<0>(r0, i, j, k, W, G, g, P, u); break;
+    case 1: if (region_cell(a1, t, i, j, k)) eb_face_or_zero<1>(r1, i, j, k, W, G, g, P, u); break;
+    default:
+      if (region_cell(a2, t, i, j, k)) eb_face_or_zero<2>(r2, i, j, k, W, G, g, P, u);
+      break;
   }
 }
 
@@ -245,17 +256,6 @@ __device__ __forceinline__ void eb_adjust(int i, int j, int k, const EBWork& W, 
     const double areafac = (d == 0) ? g.dx[1] * g.dx[2] : (d == 1) ? g.dx[0] * g.dx[2]
                                                                    : g.dx[1] * g.dx[0];
     for (int n = 0; n < NVAR; ++n) fx[at + n * s.sn] *= areafac;
-  }
-}
-
-__global__ void __launch_bounds__(kEB) k_eb_adjust(Region r0, Region r1, Region r2, EBWork W,
-                                                    EBG G, KGeom g, KParams P, DFab u) {
-  int i, j, k;
-  const int64_t t = etid();
-  switch (blockIdx.y) {
-    case 0: if (region_cell(r0, t, i, j, k)) eb_adjust<0>(i, j, k, W, G, g, P, u); break;
-    case 1: if (region_cell(r1, t, i, j, k)) eb_adjust<1>(i, j, k, W, G, g, P, u); break;
-    default: if (region_cell(r2, t, i, j, k)) eb_adjust<2>(i, j, k, W, G, g, P, u); break;
   }
 }
 
@@ -494,23 +494,34 @@ __global__ void __launch_bounds__(kEB) k_eb_redist2(Region r, EBWork W, EBG G, D
     for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = W.divc[at + n * s.sn];
     return;
   }
-  const bool recv = db.has(i, j, k);
+  // the cut cells that send to this cell, in raster order (most cells
+  // have none: they take divc, plus their own correction if cut)
+  int64_t from[27];
+  int nfrom = 0;
+  if (db.has(i, j, k)) {
+    for (int kk = -1; kk <= 1; ++kk)
+      for (int jj = -1; jj <= 1; ++jj)
+        for (int ii = -1; ii <= 1; ++ii) {
+          const int si = i + ii, sj = j + jj, sk = k + kk;
+          if (si < g.lo[0] - 1 || si > g.hi[0] + 1 || sj < g.lo[1] - 1 || sj > g.hi[1] + 1 ||
+              sk < g.lo[2] - 1 || sk > g.hi[2] + 1)
+            continue;
+          const unsigned ws = G.fl(si, sj, sk);
+          if (!f_single(ws) || !f_conn(ws, -ii, -jj, -kk)) continue;
+          from[nfrom++] = s.idx(si, sj, sk);
+        }
+  }
+  const bool own = f_single(wc);
+  if (!own && nfrom == 0) {
+    for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = W.divc[at + n * s.sn] + 0.0;
+    return;
+  }
   const double wtc = W.wt[at];
   for (int n = 0; n < NVAR; ++n) {
-    double acc = f_single(wc) ? W.optmp[at + n * s.sn] : 0.0;
-    if (recv) {
-      for (int kk = -1; kk <= 1; ++kk)
-        for (int jj = -1; jj <= 1; ++jj)
-          for (int ii = -1; ii <= 1; ++ii) {
-            const int si = i + ii, sj = j + jj, sk = k + kk;
-            if (si < g.lo[0] - 1 || si > g.hi[0] + 1 || sj < g.lo[1] - 1 || sj > g.hi[1] + 1 ||
-                sk < g.lo[2] - 1 || sk > g.hi[2] + 1)
-              continue;
-            const unsigned ws = G.fl(si, sj, sk);
-            if (!f_single(ws) || !f_conn(ws, -ii, -jj, -kk)) continue;
-            const int64_t as = s.idx(si, sj, sk);
-            acc += W.delm[as + n * s.sn] * W.wtinv[as] * wtc;
-          }
+    double acc = own ? W.optmp[at + n * s.sn] : 0.0;
+    for (int q = 0; q < nfrom; ++q) {
+      const int64_t as = from[q];
+      acc += W.delm[as + n * s.sn] * W.wtinv[as] * wtc;
     }
     dsdt(i, j, k, n) = W.divc[at + n * s.sn] + acc;
   }
@@ -637,15 +648,13 @@ inline int eb_issue(const EBPlan& E, const DFab& U, const DFab& dsdt, const DFab
   const EBWork& W = E.W;
   k_eb_ctoprim<<<eblk(E.r5.count()), kEB, 0, st>>>(E.r5, W, E.G, U, E.P, nullptr);
   k_eb_slope<<<dim3(eblk(E.r3.count()), 3), kEB, 0, st>>>(E.r3, W, E.G, E.P);
-  k_eb_face<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.rf[0], E.rf[1], E.rf[2], E.ra[0], E.ra[1],
-                                                  E.ra[2], W, E.G, E.g, E.P);
-  nk += 3;
+  nk += 2;
   if (E.rn.count() > 0) {
     k_eb_divu<<<eblk(E.rn.count()), kEB, 0, st>>>(E.rn, W, E.G, E.g);
     ++nk;
   }
-  k_eb_adjust<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.ra[0], E.ra[1], E.ra[2], W, E.G, E.g, E.P,
-                                                    U);
+  k_eb_face<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.rf[0], E.rf[1], E.rf[2], E.ra[0], E.ra[1],
+                                                  E.ra[2], W, E.G, E.g, E.P, U);
   k_eb_div<<<eblk(E.r2.count()), kEB, 0, st>>>(E.r2, W, E.G, E.g, E.P, fo[0], fo[1], fo[2],
                                                E.wtype);
   nk += 2;
