@@ -520,13 +520,15 @@ def eb_comparison(args, n=(256, 128, 128), nsteps=None, warmup=3, cpu_n=(64, 32,
                            dx=(dx,) * 3)
     prm = native.default_params(do_mol=1, ppm_type=0, cfl=0.3)
     typ = geo["flag"][5:-5, 5:-5, 5:-5] & 3
-    nb = [v // 32 for v in n]
-    t = typ.reshape(nb[2], 32, nb[1], 32, nb[0], 32)
-    has_cov = (t == 3).any(axis=(1, 3, 5))
-    has_cut = (t == 1).any(axis=(1, 3, 5))
-    all_cov = (t == 3).all(axis=(1, 3, 5))
-    boxes = {"regular": int((~has_cov & ~has_cut).sum()), "cut": int((has_cut & ~all_cov).sum()),
-             "covered": int(all_cov.sum())}
+    gtyp = geo["flag"] & 3
+    boxes = {"regular": 0, "cut": 0, "covered": 0}
+    for k in range(0, n[2], 32):
+        for j in range(0, n[1], 32):
+            for i in range(0, n[0], 32):
+                b = typ[k:k + 32, j:j + 32, i:i + 32]
+                g2 = gtyp[3 + k:7 + k + 32, 3 + j:7 + j + 32, 3 + i:7 + i + 32]
+                boxes["covered" if np.all(b == 3) else
+                      "regular" if np.all(g2 == 0) else "cut"] += 1
     zones = n[0] * n[1] * n[2]
     out = {"domain": list(n), "cells": zones, "cut_cells": int((typ == 1).sum()),
            "covered_cells": int((typ == 3).sum()), "boxes_32": boxes,
@@ -534,28 +536,43 @@ def eb_comparison(args, n=(256, 128, 128), nsteps=None, warmup=3, cpu_n=(64, 32,
            "cfl": 0.3, "steps": nsteps}
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    L = hydro.EBLevel(geom, prm, geo, redist=1)
-    st = L.torch_stream()
-    L.set_state(s0)
-    L.init_finalize()
-    L.advance(warmup)
-    torch.cuda.synchronize()
-    profile_range(args, True)
-    e0.record(st)
-    L.advance(nsteps)
-    e1.record(st)
-    torch.cuda.synchronize()
-    profile_range(args, False)
-    ms = e0.elapsed_time(e1) / nsteps
-    fin = L.get_state()
-    out["eb_level"] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3),
-                       "kernels_per_step_graph": L.kernels_per_step(),
-                       "device_error": list(L.error()),
-                       "t_final": float(L.dts().sum()),
-                       "finite": bool(np.isfinite(fin).all())}
-    L.close()
-    del L
-    torch.cuda.empty_cache()
+    # 32^3 boxes (the configuration): regular boxes through the batched
+    # regular hydro, cut boxes through the EB hydro, covered boxes skipped;
+    # then the whole domain as one EB box for comparison
+    for key, mgs, k in (("eb_level", (32, 32, 32), nsteps),
+                        ("eb_level_one_box", (0, 0, 0), max(1, nsteps // 5))):
+        L = hydro.EBLevel(geom, prm, geo, redist=1, max_grid_size=mgs)
+        st = L.torch_stream()
+        L.set_state(s0)
+        L.init_finalize()
+        L.advance(1)
+        L.autotune()
+        L.advance(warmup)
+        torch.cuda.synchronize()
+        prof = key == "eb_level"
+        if prof:
+            profile_range(args, True)
+        e0.record(st)
+        L.advance(k)
+        e1.record(st)
+        torch.cuda.synchronize()
+        if prof:
+            profile_range(args, False)
+        ms = e0.elapsed_time(e1) / k
+        fin = L.get_state()
+        out[key] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3),
+                    "steps": k, "max_grid_size": list(mgs),
+                    "kernels_per_step_graph": L.kernels_per_step(),
+                    "boxes": L.boxes(),
+                    "device_error": list(L.error()),
+                    "t_final": float(L.dts().sum()),
+                    "finite": bool(np.isfinite(fin).all())}
+        if prof:
+            ms_main = ms
+        L.close()
+        del L
+        torch.cuda.empty_cache()
+    ms = ms_main
     # the same domain and flow without the sphere, regular MOL level driver
     R = hydro.Level(geom, prm, use_graph=True)
     st = R.torch_stream()

@@ -87,6 +87,8 @@ camr_status fill_box(const camr_box_task& t, const camr_geom& geom, bool mol, bo
   for (int d = 0; d < 3; ++d) c.flx[d] = make_dfab(t.flx[d]);
   c.dsdt = make_dfab(t.dsdt);
   c.mol = mol;
+  c.ebflag = nullptr;
+  for (int d = 0; d < 3; ++d) c.eblo[d] = c.ebn[d] = 0;
   (void)need_dsdt;
   c.w.s = make_space(t.lo, t.hi);
   return CAMR_OK;
@@ -147,7 +149,8 @@ namespace {
 
 camr_status batch_create_impl(int nbox, const camr_box_task* tasks, const camr_geom* geom,
                               const camr_hydro_params* p, void* stream, bool fluxes_only,
-                              camr_batch** out) {
+                              camr_batch** out, const unsigned* ebflag = nullptr,
+                              const int* eblo = nullptr, const int* ebn = nullptr) {
   if (nbox <= 0 || !tasks || !geom || !p || !out) return CAMR_ERR_INVALID;
   if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
@@ -166,6 +169,19 @@ camr_status batch_create_impl(int nbox, const camr_box_task* tasks, const camr_g
     if (cs != CAMR_OK) {
       delete b;
       return cs;
+    }
+    if (ebflag) {
+      BoxCtx& c = b->host_boxes[i];
+      c.ebflag = ebflag;
+      for (int d = 0; d < 3; ++d) {
+        c.eblo[d] = eblo[d];
+        c.ebn[d] = ebn[d];
+        // the flags must cover the ctoprim region grow(box, 4)
+        if (c.g.lo[d] - NGROW < eblo[d] || c.g.hi[d] + NGROW >= eblo[d] + ebn[d]) {
+          delete b;
+          return CAMR_ERR_INVALID;
+        }
+      }
     }
     b->has_src = b->has_src || b->host_boxes[i].has_src;
     offs[i] = total;
@@ -211,6 +227,13 @@ camr_status batch_create_fluxes(int nbox, const camr_box_task* tasks, const camr
 }
 
 const Work& batch_work(const camr_batch* b, int box) { return b->host_boxes[box].w; }
+
+camr_status batch_create_eb(int nbox, const camr_box_task* tasks, const camr_geom* geom,
+                            const camr_hydro_params* p, cudaStream_t st, const unsigned* flag,
+                            const int glo[3], const int gn[3], camr_batch** out) {
+  if (!flag || !glo || !gn) return CAMR_ERR_INVALID;
+  return batch_create_impl(nbox, tasks, geom, p, st, false, out, flag, glo, gn);
+}
 
 }  // namespace camr
 

@@ -33,7 +33,11 @@
 // one box with a persistent workspace.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <array>
+#include <cstring>
 #include <new>
+#include <vector>
 
 #include "cell_point.cuh"
 #include "hydro_kernels.cuh"
@@ -930,15 +934,26 @@ struct camr_eb_level {
   bool own_stream = false;
   LGeom L;
   int64_t ncell = 0, npad = 0;
-  double *S = nullptr, *S_old = nullptr, *B = nullptr, *B2 = nullptr, *dsdt = nullptr;
-  double *work = nullptr, *staging = nullptr, *fixed_dev = nullptr;
+  double *S = nullptr, *S_old = nullptr, *B = nullptr, *dsdt = nullptr;
+  double *staging = nullptr, *fixed_dev = nullptr;
   double *dt_cur = nullptr, *dt_hist = nullptr;
   unsigned long long* bits = nullptr;
   int* nstep = nullptr;
   DevError* err = nullptr;
   unsigned* flag = nullptr;
   double *vfrac = nullptr, *ap[3] = {nullptr, nullptr, nullptr}, *fc[3] = {nullptr, nullptr, nullptr};
-  EBPlan plan;
+  EBG G;                          // the level's geometry view (flags for the guards)
+  std::vector<EBPlan> plans;      // cut boxes: EB hydro, one workspace each
+  std::vector<double*> plan_work;
+  camr_batch* regular = nullptr;  // regular boxes: the batched regular hydro
+  double* regular_flx = nullptr;  // their face fluxes (scratch)
+  int nbox_regular = 0, nbox_cut = 0, nbox_covered = 0;
+  // side streams for the cut boxes: their launch sequences run concurrently
+  // with each other and with the regular boxes' batch (fork/join by events,
+  // captured into the step's graph as parallel branches)
+  std::vector<cudaStream_t> side;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
   int hist_cap = 1 << 16;
   int64_t steps_taken = 0;
   cudaGraphExec_t graph = nullptr;
@@ -958,12 +973,53 @@ DFab level_dfab(const LGeom& L, double* p) {
   return f;
 }
 
+camr_fab level_fab(const LGeom& L, double* p) {
+  camr_fab f;
+  std::memset(&f, 0, sizeof(f));
+  f.ptr = p;
+  for (int d = 0; d < 3; ++d) {
+    f.lo[d] = L.plo[d];
+    f.hi[d] = L.plo[d] + L.pn[d] - 1;
+  }
+  f.jstride = L.sy;
+  f.kstride = L.sz;
+  f.nstride = L.sn;
+  f.ncomp = NVAR;
+  return f;
+}
+
+// construct_hydro_source of one stage (CAMR_construct_hydro_source.cpp:71-254
+// in an EB build): src_to_fill = 0; per box: covered boxes nothing, boxes
+// whose grow(bx,2) is all regular the regular hydro (batched), the others
+// hydro_umdrv_eb.  Sborder is lev->B.
+int eb_hydro_stage(camr_eb_level* lev, cudaStream_t st) {
+  int nk = 0;
+  cudaMemsetAsync(lev->dsdt, 0, size_t(lev->L.sn) * NVAR * sizeof(double), st);
+  const int nside = int(lev->side.size());
+  if (nside) {
+    cudaEventRecord(lev->ev_fork, st);
+    for (cudaStream_t s2 : lev->side) cudaStreamWaitEvent(s2, lev->ev_fork, 0);
+  }
+  const DFab none[3] = {level_dfab(lev->L, nullptr), level_dfab(lev->L, nullptr),
+                        level_dfab(lev->L, nullptr)};
+  const DFab U = level_dfab(lev->L, lev->B);
+  const DFab ds = level_dfab(lev->L, lev->dsdt);
+  for (size_t b = 0; b < lev->plans.size(); ++b)
+    nk += eb_issue(lev->plans[b], U, ds, none, nside ? lev->side[b % nside] : st);
+  if (lev->regular) camr_batch_run(lev->regular, 0.0, lev->dt_cur, CAMR_BATCH_PERSISTENT, st);
+  for (int i = 0; i < nside; ++i) {
+    cudaEventRecord(lev->ev_join[i], lev->side[i]);
+    cudaStreamWaitEvent(st, lev->ev_join[i], 0);
+  }
+  return nk;
+}
+
 cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_dev) {
   const LGeom& L = lev->L;
   cudaStream_t st = lev->stream;
   const unsigned gv = grid_of(lev->ncell);
   const unsigned gp = grid_of(lev->npad);
-  const EBG& G = lev->plan.G;
+  const EBG& G = lev->G;
   DtCtl c{lev->hp.cfl, lev->hp.max_dt, lev->hp.fixed_dt, lev->hp.initial_dt,
           lev->hp.init_shrink, lev->hp.change_max};
   int nk = 0;
@@ -977,19 +1033,36 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   k_ebl_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->S_old, lev->err);
   k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err);
   nk += 3;
-  const DFab none[3] = {level_dfab(L, nullptr), level_dfab(L, nullptr), level_dfab(L, nullptr)};
-  const DFab ds = level_dfab(L, lev->dsdt);
-  nk += eb_issue(lev->plan, level_dfab(L, lev->B), ds, none, st);
+  nk += eb_hydro_stage(lev, st);
   k_ebl_update1<<<gv, kBlk, 0, st>>>(L, lev->P, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
                                      lev->S);
-  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B2, lev->err);
+  // stage 2's Sborder reuses B (stage 1's is dead after the update)
+  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B, lev->err);
   nk += 2;
-  nk += eb_issue(lev->plan, level_dfab(L, lev->B2), ds, none, st);
-  k_ebl_update2<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B2, lev->S_old, lev->dsdt,
+  nk += eb_hydro_stage(lev, st);
+  k_ebl_update2<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
                                      lev->S, lev->bits, lev->err);
   nk += 1;
   count_launch(nk);
   return cudaGetLastError();
+}
+
+// The level's boxes: the domain chopped by max_grid_size from the low end
+// (the last box in a direction takes the remainder).
+std::vector<std::array<int, 6>> level_boxes(const camr_geom& g, const int mgs[3]) {
+  std::vector<std::array<int, 6>> out;
+  int step[3];
+  for (int d = 0; d < 3; ++d) {
+    const int n = g.dom_hi[d] - g.dom_lo[d] + 1;
+    step[d] = mgs[d] > 0 ? mgs[d] : n;
+  }
+  for (int k = g.dom_lo[2]; k <= g.dom_hi[2]; k += step[2])
+    for (int j = g.dom_lo[1]; j <= g.dom_hi[1]; j += step[1])
+      for (int i = g.dom_lo[0]; i <= g.dom_hi[0]; i += step[0])
+        out.push_back({i, j, k, std::min(i + step[0] - 1, g.dom_hi[0]),
+                       std::min(j + step[1] - 1, g.dom_hi[1]),
+                       std::min(k + step[2] - 1, g.dom_hi[2])});
+  return out;
 }
 
 }  // namespace
@@ -1001,7 +1074,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
                                  camr_eb_level** out) {
   if (!desc || !eb || !p || !out) return CAMR_ERR_INVALID;
   *out = nullptr;
-  if (!p->do_mol || p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  if (!p->do_mol || p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
     return CAMR_ERR_INVALID;
   const camr_geom& g = desc->geom;
@@ -1010,6 +1083,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
     if (!g.is_periodic[d] && (g.bc_lo[d] == CAMR_BC_INTERIOR || g.bc_hi[d] == CAMR_BC_INTERIOR))
       return CAMR_ERR_INVALID;
     if (eb->g_lo[d] != g.dom_lo[d] - 5 || eb->g_hi[d] != g.dom_hi[d] + 5) return CAMR_ERR_INVALID;
+    if (desc->max_grid_size[d] < 0) return CAMR_ERR_INVALID;
   }
   if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
       !eb->fc[1] || !eb->fc[2])
@@ -1047,14 +1121,13 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
                (g.dom_hi[2] - g.dom_lo[2] + 1);
   lev->npad = L.sn;
   const size_t state_bytes = size_t(L.sn) * NVAR * sizeof(double);
-  const Space ws = eb_space(g.dom_lo, g.dom_hi);
-  const size_t work_bytes = size_t(kEBWorkComps) * ws.sn * sizeof(double);
-  const int64_t gc = int64_t(eb->g_hi[0] - eb->g_lo[0] + 1) * (eb->g_hi[1] - eb->g_lo[1] + 1) *
-                     (eb->g_hi[2] - eb->g_lo[2] + 1);
+  int gn[3];
+  for (int d = 0; d < 3; ++d) gn[d] = eb->g_hi[d] - eb->g_lo[d] + 1;
+  const int64_t gc = int64_t(gn[0]) * gn[1] * gn[2];
   int64_t gf[3];
   for (int d = 0; d < 3; ++d) {
     gf[d] = 1;
-    for (int a = 0; a < 3; ++a) gf[d] *= int64_t(eb->g_hi[a] - eb->g_lo[a] + 1 + (a == d));
+    for (int a = 0; a < 3; ++a) gf[d] *= int64_t(gn[a] + (a == d));
   }
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** ptr, size_t b) {
@@ -1064,9 +1137,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   alloc(reinterpret_cast<void**>(&lev->S), state_bytes);
   alloc(reinterpret_cast<void**>(&lev->S_old), state_bytes);
   alloc(reinterpret_cast<void**>(&lev->B), state_bytes);
-  alloc(reinterpret_cast<void**>(&lev->B2), state_bytes);
   alloc(reinterpret_cast<void**>(&lev->dsdt), state_bytes);
-  alloc(reinterpret_cast<void**>(&lev->work), work_bytes);
   alloc(reinterpret_cast<void**>(&lev->staging), size_t(lev->ncell) * NVAR * sizeof(double));
   alloc(reinterpret_cast<void**>(&lev->fixed_dev), sizeof(double));
   alloc(reinterpret_cast<void**>(&lev->dt_cur), sizeof(double));
@@ -1090,7 +1161,10 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
     copy(lev->ap[d], eb->ap[d], size_t(gf[d]) * sizeof(double));
     copy(lev->fc[d], eb->fc[d], size_t(2 * gf[d]) * sizeof(double));
   }
+  std::vector<unsigned> hflag(static_cast<size_t>(gc));
   if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(hflag.data(), lev->flag, size_t(gc) * sizeof(unsigned), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) {
     camr_eb_level_destroy(lev);
     return e == cudaErrorMemoryAllocation ? CAMR_ERR_NOMEM : cuda_status_of(e);
@@ -1101,10 +1175,129 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   for (int d = 0; d < 3; ++d) {
     own.ap[d] = lev->ap[d];
     own.fc[d] = lev->fc[d];
+    lev->G.lo[d] = eb->g_lo[d];
+    lev->G.n[d] = gn[d];
+    lev->G.ap[d] = lev->ap[d];
+    lev->G.fc[d] = lev->fc[d];
   }
-  eb_plan_init(lev->plan, g.dom_lo, g.dom_hi, g, own, *p, redist);
-  lev->plan.W.s = ws;
-  eb_carve(lev->plan.W, lev->work);
+  lev->G.flag = lev->flag;
+  lev->G.vfrac = lev->vfrac;
+  // classify the boxes (CAMR_construct_hydro_source.cpp:76-78, :150-153)
+  auto typ = [&](int i, int j, int k) {
+    return hflag[size_t((i - eb->g_lo[0]) +
+                        int64_t(gn[0]) * ((j - eb->g_lo[1]) + int64_t(gn[1]) * (k - eb->g_lo[2])))] &
+           3u;
+  };
+  std::vector<camr_box_task> reg_tasks;
+  std::vector<std::array<int, 6>> cut_boxes;
+  for (const auto& b : level_boxes(g, desc->max_grid_size)) {
+    bool all_cov = true;
+    for (int k = b[2]; k <= b[5] && all_cov; ++k)
+      for (int j = b[1]; j <= b[4] && all_cov; ++j)
+        for (int i = b[0]; i <= b[3]; ++i)
+          if (typ(i, j, k) != 3u) {
+            all_cov = false;
+            break;
+          }
+    if (all_cov) {
+      lev->nbox_covered++;
+      continue;
+    }
+    bool all_reg = true;
+    for (int k = b[2] - 2; k <= b[5] + 2 && all_reg; ++k)
+      for (int j = b[1] - 2; j <= b[4] + 2 && all_reg; ++j)
+        for (int i = b[0] - 2; i <= b[3] + 2; ++i)
+          if (typ(i, j, k) != 0u) {
+            all_reg = false;
+            break;
+          }
+    if (all_reg) {
+      camr_box_task t;
+      std::memset(&t, 0, sizeof(t));
+      for (int d = 0; d < 3; ++d) {
+        t.lo[d] = b[d];
+        t.hi[d] = b[3 + d];
+      }
+      t.uin = level_fab(L, lev->B);
+      t.dsdt = level_fab(L, lev->dsdt);
+      reg_tasks.push_back(t);
+    } else {
+      cut_boxes.push_back(b);
+    }
+  }
+  lev->nbox_regular = int(reg_tasks.size());
+  lev->nbox_cut = int(cut_boxes.size());
+  // regular boxes: face-flux scratch, then the batch plan
+  if (!reg_tasks.empty()) {
+    size_t per = 0;
+    std::vector<size_t> off(reg_tasks.size());
+    for (size_t b = 0; b < reg_tasks.size(); ++b) {
+      off[b] = per;
+      for (int d = 0; d < 3; ++d) {
+        int64_t n = NVAR;
+        for (int a = 0; a < 3; ++a) n *= (reg_tasks[b].hi[a] - reg_tasks[b].lo[a] + 1 + (a == d));
+        per += size_t(n);
+      }
+    }
+    alloc(reinterpret_cast<void**>(&lev->regular_flx), per * sizeof(double));
+    for (size_t b = 0; b < reg_tasks.size() && e == cudaSuccess; ++b) {
+      double* ptr = lev->regular_flx + off[b];
+      camr_box_task& t = reg_tasks[b];
+      for (int d = 0; d < 3; ++d) {
+        camr_fab& f = t.flx[d];
+        f.ptr = ptr;
+        int ext[3];
+        for (int a = 0; a < 3; ++a) {
+          f.lo[a] = t.lo[a];
+          f.hi[a] = t.hi[a] + (a == d);
+          ext[a] = f.hi[a] - f.lo[a] + 1;
+        }
+        f.jstride = ext[0];
+        f.kstride = int64_t(ext[0]) * ext[1];
+        f.nstride = f.kstride * ext[2];
+        f.ncomp = NVAR;
+        ptr += f.nstride * NVAR;
+      }
+    }
+    if (e == cudaSuccess) {
+      const camr_status cs = batch_create_eb(int(reg_tasks.size()), reg_tasks.data(), &g, p,
+                                             lev->stream, lev->flag, eb->g_lo, gn,
+                                             &lev->regular);
+      if (cs != CAMR_OK) {
+        camr_eb_level_destroy(lev);
+        return cs;
+      }
+    }
+  }
+  // cut boxes: one EB plan and workspace each, spread over side streams
+  const int nside = int(std::min<size_t>(cut_boxes.size(), 8));
+  if (e == cudaSuccess && nside > 0) e = cudaEventCreateWithFlags(&lev->ev_fork, cudaEventDisableTiming);
+  for (int i = 0; i < nside && e == cudaSuccess; ++i) {
+    cudaStream_t s2;
+    cudaEvent_t ej;
+    e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+    if (e != cudaSuccess) break;
+    lev->side.push_back(s2);
+    e = cudaEventCreateWithFlags(&ej, cudaEventDisableTiming);
+    if (e != cudaSuccess) break;
+    lev->ev_join.push_back(ej);
+  }
+  for (const auto& b : cut_boxes) {
+    const int lo[3] = {b[0], b[1], b[2]}, hi[3] = {b[3], b[4], b[5]};
+    EBPlan E;
+    eb_plan_init(E, lo, hi, g, own, *p, redist);
+    double* w = nullptr;
+    alloc(reinterpret_cast<void**>(&w), size_t(kEBWorkComps) * E.W.s.sn * sizeof(double));
+    if (e != cudaSuccess) break;
+    lev->plan_work.push_back(w);
+    eb_carve(E.W, w);
+    lev->plans.push_back(E);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) {
+    camr_eb_level_destroy(lev);
+    return e == cudaErrorMemoryAllocation ? CAMR_ERR_NOMEM : cuda_status_of(e);
+  }
   *out = lev;
   return CAMR_OK;
 }
@@ -1112,12 +1305,18 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
 camr_status camr_eb_level_destroy(camr_eb_level* lev) {
   if (!lev) return CAMR_ERR_INVALID;
   if (lev->graph_ready) cudaGraphExecDestroy(lev->graph);
-  void* ptrs[] = {lev->S,       lev->S_old,  lev->B,     lev->B2,    lev->dsdt,  lev->work,
-                  lev->staging, lev->fixed_dev, lev->dt_cur, lev->dt_hist, lev->bits, lev->nstep,
-                  lev->err,     lev->flag,   lev->vfrac, lev->ap[0], lev->ap[1], lev->ap[2],
-                  lev->fc[0],   lev->fc[1],  lev->fc[2]};
+  if (lev->regular) camr_batch_destroy(lev->regular);
+  void* ptrs[] = {lev->S,       lev->S_old,   lev->B,      lev->dsdt,       lev->staging,
+                  lev->fixed_dev, lev->dt_cur, lev->dt_hist, lev->bits,     lev->nstep,
+                  lev->err,     lev->flag,    lev->vfrac,  lev->ap[0],      lev->ap[1],
+                  lev->ap[2],   lev->fc[0],   lev->fc[1],  lev->fc[2],      lev->regular_flx};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (double* w : lev->plan_work)
+    if (w) cudaFree(w);
+  for (cudaEvent_t ev : lev->ev_join) cudaEventDestroy(ev);
+  if (lev->ev_fork) cudaEventDestroy(lev->ev_fork);
+  for (cudaStream_t s2 : lev->side) cudaStreamDestroy(s2);
   if (lev->own_stream) cudaStreamDestroy(lev->stream);
   delete lev;
   return CAMR_OK;
@@ -1212,6 +1411,31 @@ camr_status camr_eb_level_dts(camr_eb_level* lev, double* dts, int n, int* nstep
     if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
   }
   return cuda_status_of(e);
+}
+
+camr_status camr_eb_level_autotune(camr_eb_level* lev) {
+  if (!lev) return CAMR_ERR_INVALID;
+  if (!lev->regular) return CAMR_OK;
+  double dt = 0.0;
+  cudaError_t e = cudaMemcpyAsync(&dt, lev->dt_cur, sizeof(double), cudaMemcpyDeviceToHost,
+                                  lev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  const camr_status cs = camr_batch_autotune(lev->regular, dt, lev->stream);
+  // a captured step holds the old launch shapes
+  if (cs == CAMR_OK && lev->graph_ready) {
+    cudaGraphExecDestroy(lev->graph);
+    lev->graph_ready = false;
+  }
+  return cs;
+}
+
+camr_status camr_eb_level_boxes(camr_eb_level* lev, int* regular, int* cut, int* covered) {
+  if (!lev) return CAMR_ERR_INVALID;
+  if (regular) *regular = lev->nbox_regular;
+  if (cut) *cut = lev->nbox_cut;
+  if (covered) *covered = lev->nbox_covered;
+  return CAMR_OK;
 }
 
 int64_t camr_eb_level_kernels_per_step(camr_eb_level* lev) {

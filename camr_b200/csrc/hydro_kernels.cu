@@ -733,6 +733,17 @@ __device__ __forceinline__ void batched_cell(const BoxCtx& c, int sub, int i, in
                                              const KParams& P, const DtRef& dt, DevError* err) {
   const Work& w = c.w;
   if constexpr (STAGE == BS_CTOPRIM) {
+    if (c.ebflag) {
+      const int64_t f = (i - c.eblo[0]) +
+                        int64_t(c.ebn[0]) * ((j - c.eblo[1]) + int64_t(c.ebn[1]) * (k - c.eblo[2]));
+      if ((c.ebflag[f] & 3u) == 3u) {
+        const int64_t at = w.s.idx(i, j, k);
+        for (int n = 0; n < SQ_N; ++n) w.q[at + n * w.s.sn] = 0.;
+        if (c.has_src)
+          for (int n = 0; n < ES_N; ++n) w.srcq[at + n * w.s.sn] = 0.;
+        return;
+      }
+    }
     ctoprim_body(i, j, k, w.s, c.uin, c.src, c.has_src, P, w.q, w.srcq, err);
   } else if constexpr (STAGE == BS_FLATDIVU) {
     flatten_divu_body(i, j, k, w.s, c.g, P, !c.mol, w.q, w.flat, w.divu);

@@ -91,6 +91,11 @@ struct BoxCtx {
   DFab dsdt;
   bool has_src;
   bool mol;
+  // EB cell flags over [eblo, eblo + ebn) (null outside an EB level):
+  // ctoprim leaves q = 0 in covered cells, as construct_hydro_source does
+  // in an EB build (CAMR_construct_hydro_source.cpp:108-120).
+  const unsigned* ebflag;
+  int eblo[3], ebn[3];
 };
 
 // One work item of a batched stage: `region` of box `box` in sub-direction
@@ -116,6 +121,12 @@ constexpr int kBatchBlock = 128;
 camr_status batch_create_fluxes(int nbox, const camr_box_task* tasks, const camr_geom* geom,
                                 const camr_hydro_params* p, cudaStream_t st, camr_batch** out);
 const Work& batch_work(const camr_batch* b, int box);
+
+// A full batch plan (dsdt accumulated) for the regular boxes of an EB level:
+// ctoprim skips the covered cells of the flag array over [glo, glo + gn).
+camr_status batch_create_eb(int nbox, const camr_box_task* tasks, const camr_geom* geom,
+                            const camr_hydro_params* p, cudaStream_t st, const unsigned* flag,
+                            const int glo[3], const int gn[3], camr_batch** out);
 
 // Issue the whole per-box hydro on `stream` (7 or 5 kernel launches).
 cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t stream);

@@ -313,6 +313,15 @@ class EBLevel:
     def kernels_per_step(self):
         return int(lib().camr_eb_level_kernels_per_step(self._h))
 
+    def autotune(self):
+        check(lib().camr_eb_level_autotune(self._h), "camr_eb_level_autotune")
+
+    def boxes(self):
+        r, c, v = C.c_int(), C.c_int(), C.c_int()
+        check(lib().camr_eb_level_boxes(self._h, C.byref(r), C.byref(c), C.byref(v)),
+              "camr_eb_level_boxes")
+        return {"regular": r.value, "cut": c.value, "covered": v.value}
+
     def error(self):
         info = native.ErrorInfo()
         lib().camr_eb_level_get_error(self._h, C.byref(info))

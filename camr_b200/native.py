@@ -139,6 +139,9 @@ SIGNATURES = {
     "camr_eb_level_advance": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "camr_eb_level_dts": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int,
                                     C.POINTER(C.c_int)]),
+    "camr_eb_level_autotune": (C.c_int, [C.c_void_p]),
+    "camr_eb_level_boxes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]),
     "camr_eb_level_kernels_per_step": (C.c_int64, [C.c_void_p]),
     "camr_eb_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_eb_level_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),

@@ -376,8 +376,11 @@ camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3], const ca
  * EB level: one uniform level with an embedded boundary, MOL only
  * (CAMR_advance's do_mol branch, Source/CAMR_advance.cpp:38-164, with
  * hydro_umdrv_eb per stage and the EB build's clean_state / computeTemp /
- * estTimeStep guards for covered cells).  The domain is advanced as one box
- * with 5 ghost cells.  eb: geometry over exactly grow(domain, 5), host or
+ * estTimeStep guards for covered cells), 5 ghost cells.  desc->max_grid_size
+ * chops the domain into boxes (0 = one box): as in an EB build's
+ * construct_hydro_source, covered boxes are skipped, boxes whose grow(box,2)
+ * is all regular run the regular hydro (one batched launch per stage for
+ * all of them) and the others the EB hydro.  eb: geometry over exactly grow(domain, 5), host or
  * device memory, copied into the level.  redist: 0 NoRedist, 1 FluxRedist
  * (StateRedist is not provided: CAMR_ERR_INVALID).  Covered cells hold zero
  * state (initData's EB_set_covered); set_state/get_state/advance/dts as
@@ -397,6 +400,13 @@ camr_status camr_eb_level_init_finalize(camr_eb_level* lev);
 camr_status camr_eb_level_advance(camr_eb_level* lev, int nsteps, const double* fixed_dts);
 /* The dt of every step taken since creation (at most n), and their count. */
 camr_status camr_eb_level_dts(camr_eb_level* lev, double* dts, int n, int* nsteps);
+/* Time the regular boxes' batched stages on the level's current Sborder and
+ * keep the fastest launch shapes (camr_batch_autotune); call after a step.
+ * Synchronises. */
+camr_status camr_eb_level_autotune(camr_eb_level* lev);
+/* How the level's boxes were classified: all-regular grow(box,2) (regular
+ * hydro), cut (EB hydro), covered (skipped). */
+camr_status camr_eb_level_boxes(camr_eb_level* lev, int* regular, int* cut, int* covered);
 int64_t camr_eb_level_kernels_per_step(camr_eb_level* lev);
 camr_status camr_eb_level_stream(camr_eb_level* lev, void** stream);
 camr_status camr_eb_level_get_error(camr_eb_level* lev, camr_error_info* info);

@@ -40,7 +40,7 @@ typedef struct {
   int allow_negative_energy;
   int allow_small_energy;
   int add_grav_src;
-  int pad0;
+  int eb_weights_type;  /* EB flux-redistribution weights (default 2 = rho) */
   int pad1;
   double difmag;
   double small;

@@ -123,7 +123,8 @@ inline void default_params(orc_params* p) {
   p->allow_negative_energy = 0;
   p->allow_small_energy = 1;
   p->add_grav_src = 1;
-  p->pad0 = p->pad1 = 0;
+  p->eb_weights_type = 2;  // :107
+  p->pad1 = 0;
   p->difmag = 0.1;
   p->small = 1.e-8;
   p->small_dens = 1.e-7;

@@ -435,6 +435,55 @@ double est_dt_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S) {
 
 }  // namespace
 
+// One all-regular box of an EB level: construct_hydro_source's regular
+// branch in an EB build (CAMR_construct_hydro_source.cpp:81-120, :225-238):
+// q on grow(bx, numGrow() = 5) with covered cells zero, then the
+// reference's regular hydro_umdrv accumulating into dsdt.
+static long eb_regular_box(const orc_params* p, const LevelEB& L, const Box& bx,
+                    Array4<Real> const& B, Array4<Real> const& dsdt) {
+  const Box qbx = amrex::grow(bx, 5);
+  PassMap pmap;
+  init_pass_map(&pmap);
+  FArrayBox q(qbx, QVAR), qaux(qbx, NQAUX), src_q(qbx, QVAR);
+  auto qarr = q.array();
+  auto qauxar = qaux.array();
+  auto srcqarr = src_q.array();
+  Array4<const Real> sarr(B);
+  const Real small_num = p->small_num;
+  const Real eta1 = p->dual_energy_eta1;
+  const int ane = p->allow_negative_energy;
+  ParallelFor(qbx, [&](int i, int j, int k) {
+    if (!covered(L, i, j, k)) {
+      hydro_ctoprim(i, j, k, sarr, qarr, qauxar, pmap, small_num, eta1, ane);
+    } else {
+      for (int n = 0; n < QVAR; ++n) qarr(i, j, k, n) = 0.;
+    }
+  });
+  FArrayBox flux[3], area[3], vol(bx, 1);
+  Array4<Real> fa[3];
+  Array4<Real> aa[3];
+  for (int d = 0; d < 3; ++d) {
+    const Box efbx = amrex::surroundingNodes(bx, d);
+    flux[d].resize(efbx, NVAR);
+    flux[d].setVal(0.0);
+    fa[d] = flux[d].array();
+    area[d].resize(efbx, 1);
+    area[d].setVal((d == 0) ? L.dx[1] * L.dx[2] : (d == 1) ? L.dx[0] * L.dx[2] : L.dx[0] * L.dx[1]);
+    aa[d] = area[d].array();
+  }
+  vol.setVal(L.dx[0] * L.dx[1] * L.dx[2]);
+  const amrex::GpuArray<const Array4<Real>, 3> flx_arr{{fa[0], fa[1], fa[2]}};
+  const amrex::GpuArray<const Array4<const Real>, 3> a{
+      {Array4<const Real>(aa[0]), Array4<const Real>(aa[1]), Array4<const Real>(aa[2])}};
+  const amrex::GpuArray<Real, 3> dxa{{L.dx[0], L.dx[1], L.dx[2]}};
+  const Geometry geom(L.dom, L.periodic);
+  hydro_umdrv(true, bx, geom, L.bclo, L.bchi, sarr, dsdt, qarr, qauxar, srcqarr, dxa, 0.0,
+              p->ppm_type, p->plm_iorder, p->use_pslope, p->use_flattening,
+              p->transverse_reset_density, p->small, p->small_dens, p->small_pres, p->smallu,
+              p->difmag, flx_arr, a, vol.array(), &pmap);
+  return 0;
+}
+
 extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const unsigned* flag_in,
                                const double* vfrac, const double* ap0, const double* ap1,
                                const double* ap2, const double* fc0, const double* fc1,
@@ -462,15 +511,61 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
   auto B2 = B2_f.array();
   auto k1 = d1_f.array();
   auto k2 = d2_f.array();
-  std::vector<double> fbuf[3];
-  for (int d = 0; d < 3; ++d) {
-    Box fb = amrex::surroundingNodes(L.dom, d);
-    fbuf[d].assign(size_t(fb.numPts()) * NVAR, 0.0);
-  }
   const int g_lo[3] = {L.G.lo[0], L.G.lo[1], L.G.lo[2]};
   const int g_hi[3] = {L.G.hi[0], L.G.hi[1], L.G.hi[2]};
   const int* dlo = L.dom.lo.v;
   const int* dhi = L.dom.hi.v;
+  // the level's boxes (max_grid_size chop from the low end) and their kind
+  // (CAMR_construct_hydro_source.cpp:76-78, :150-153): 0 covered (skipped),
+  // 1 grow(bx,2) all regular (regular hydro), 2 cut (hydro_umdrv_eb)
+  std::vector<Box> boxes;
+  std::vector<int> kind;
+  {
+    int step[3];
+    for (int d = 0; d < 3; ++d) {
+      const int n = L.dom.hi[d] - L.dom.lo[d] + 1;
+      step[d] = lev->max_grid_size[d] > 0 ? lev->max_grid_size[d] : n;
+    }
+    for (int k = L.dom.lo[2]; k <= L.dom.hi[2]; k += step[2])
+      for (int j = L.dom.lo[1]; j <= L.dom.hi[1]; j += step[1])
+        for (int i = L.dom.lo[0]; i <= L.dom.hi[0]; i += step[0]) {
+          const Box b(IntVect(i, j, k),
+                      IntVect(std::min(i + step[0] - 1, L.dom.hi[0]),
+                              std::min(j + step[1] - 1, L.dom.hi[1]),
+                              std::min(k + step[2] - 1, L.dom.hi[2])));
+          bool all_cov = true, all_reg = true;
+          ParallelFor(b, [&](int ii, int jj, int kk) {
+            if (!covered(L, ii, jj, kk)) all_cov = false;
+          });
+          ParallelFor(amrex::grow(b, 2), [&](int ii, int jj, int kk) {
+            if (!L.flag(ii, jj, kk).isRegular()) all_reg = false;
+          });
+          boxes.push_back(b);
+          kind.push_back(all_cov ? 0 : (all_reg ? 1 : 2));
+        }
+  }
+  // construct_hydro_source of one stage: src_to_fill = 0, then each box
+  auto stage = [&](Array4<Real> const& Bv, Array4<Real> const& kout, double dt) -> long {
+    long ne = 0;
+    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { kout(i, j, k, n) = 0.0; });
+    for (size_t b = 0; b < boxes.size(); ++b) {
+      const Box& bx = boxes[b];
+      if (kind[b] == 0) continue;
+      if (kind[b] == 1) {
+        ne += eb_regular_box(p, L, bx, Bv, kout);
+        continue;
+      }
+      FArrayBox dfab(bx, NVAR), ff[3];
+      for (int d = 0; d < 3; ++d) ff[d].resize(amrex::surroundingNodes(bx, d), NVAR);
+      ne += orc_hydro_box_eb(p, bx.lo.v, bx.hi.v, dlo, dhi, L.bclo, L.bchi, L.periodic, Bv.p,
+                             g_lo, g_hi, flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, redist,
+                             p->eb_weights_type, dfab.array().p, ff[0].array().p,
+                             ff[1].array().p, ff[2].array().p, L.dx, dt);
+      auto dv = dfab.array();
+      ParallelFor(bx, NVAR, [&](int i, int j, int k, int n) { kout(i, j, k, n) = dv(i, j, k, n); });
+    }
+    return ne;
+  };
   long nerr = 0;
   double dt_level = *dt_prev;
   for (int step = 0; step < nsteps; ++step) {
@@ -497,14 +592,10 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
         for (int n = 0; n < NVAR; ++n) S(i, j, k, n) += dt * src[n];
       });
     }
-    nerr += orc_hydro_box_eb(p, dlo, dhi, dlo, dhi, L.bclo, L.bchi, L.periodic, B.p, g_lo, g_hi,
-                             flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, redist, 2, k1.p,
-                             fbuf[0].data(), fbuf[1].data(), fbuf[2].data(), L.dx, dt);
+    nerr += stage(B, k1, dt);
     ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S(i, j, k, n) += dt * k1(i, j, k, n); });
     nerr += expand_eb(p, L, S, B2);
-    nerr += orc_hydro_box_eb(p, dlo, dhi, dlo, dhi, L.bclo, L.bchi, L.periodic, B2.p, g_lo, g_hi,
-                             flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, redist, 2, k2.p,
-                             fbuf[0].data(), fbuf[1].data(), fbuf[2].data(), L.dx, dt);
+    nerr += stage(B2, k2, dt);
     ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
       S(i, j, k, n) = 0.5 * B2(i, j, k, n) + 0.5 * S_old(i, j, k, n);
     });

@@ -109,14 +109,19 @@ def test_eb_box_conserves_mass_and_energy():
 
 
 @pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
-@pytest.mark.parametrize("kind,redist", [("periodic", 1), ("periodic", 0), ("sod", 1)])
-def test_eb_level_steps_match_oracle(kind, redist):
+@pytest.mark.parametrize("kind,redist,mgs,radius", [
+    ("periodic", 1, (0, 0, 0), None), ("periodic", 0, (0, 0, 0), None),
+    ("sod", 1, (0, 0, 0), None), ("sod", 1, (8, 8, 8), 0.15), ("sod", 1, (2, 2, 2), 0.25),
+    ("periodic", 1, (8, 8, 4), None)])
+def test_eb_level_steps_match_oracle(kind, redist, mgs, radius):
     """camr_eb_level_* steps (dt on the device, graph-captured after the
-    first step) against the EB oracle's level driver: states and dts."""
+    first step) against the EB oracle's level driver: states and dts.  With
+    a box decomposition, regular boxes run the batched regular hydro and cut
+    boxes the EB hydro, covered boxes nothing."""
     _torch()
     from test_oracle_eb import eb_level_case
     n = (16, 16, 16) if kind == "periodic" else (32, 16, 16)
-    p, lev, geo, s = eb_level_case(kind, n=n)
+    p, lev, geo, s = eb_level_case(kind, n=n, radius=radius, max_grid_size=mgs)
     if not redist:
         p.fixed_dt = 1e-4
     ref = s.copy()
@@ -129,9 +134,17 @@ def test_eb_level_steps_match_oracle(kind, redist):
         geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
                                dx=(2.0 / n[0],) * 3)
     prm = native.default_params(do_mol=1, cfl=0.3, fixed_dt=p.fixed_dt)
-    L = hydro.EBLevel(geom, prm, geo, redist=redist)
+    L = hydro.EBLevel(geom, prm, geo, redist=redist, max_grid_size=mgs)
     L.set_state(s)
-    L.advance(nsteps)
+    if mgs[0]:
+        kinds = L.boxes()
+        assert kinds["cut"] > 0 and (kind == "periodic" or kinds["regular"] > 0)
+        # tuned launch shapes change no bits
+        L.advance(2)
+        L.autotune()
+        L.advance(nsteps - 2)
+    else:
+        L.advance(nsteps)
     got = L.get_state()
     dts = L.dts()
     assert L.error()[0] == 0
