@@ -98,6 +98,98 @@ __device__ __forceinline__ void ctoprim_body(int i, int j, int k, const Space& s
 // not produced.  Stored slots: 0, 2, 3, 4, QREINT, species.
 enum { SL_0 = 0, SL_2 = 1, SL_3 = 2, SL_4 = 3, SL_RE = 4, SL_FS = 5, SL_N = 8 };
 
+// hydro_plm_d (Godunov/PLM.H:170-323) of one cell in direction d from its
+// slopes (ES_N slots): the plus state on the cell's low face (qp_o) and the
+// minus state on its high face (qm_o).
+template <int d>
+__device__ __forceinline__ void plm_edge_states(const double* q, int64_t at, int64_t sn,
+                                                const double* slope, double dtdx,
+                                                const KParams& P, double* qp_o,
+                                                double* qm_o) {
+  constexpr int l0 = d;
+  constexpr int l1 = (d == 0) ? 1 : 0;
+  constexpr int l2 = (d == 2) ? 1 : 2;
+  const double cc = q[at + SQ_C * sn];
+  const double dtdx_p = dtdx;
+  const double cs = cc * cc;
+  const double rho = q[at + SQ_RHO * sn];
+  const double vel[3] = {q[at + SQ_U * sn], q[at + SQ_V * sn], q[at + SQ_W * sn]};
+  const double pr = q[at + SQ_P * sn];
+  const double rhoe = q[at + SQ_REINT * sn];
+  const double enth = ((rhoe + pr) / rho) / cs;
+  const double drho = slope[ES_RHO];
+  const double dvel[3] = {slope[ES_U], slope[ES_V], slope[ES_W]};
+  const double dp = slope[ES_P];
+  const double drhoe = slope[ES_REINT];
+  const double alpham = 0.5 * (dp / (rho * cc) - dvel[d]) * rho / cc;
+  const double alphap = 0.5 * (dp / (rho * cc) + dvel[d]) * rho / cc;
+  const double alpha0r = drho - dp / cs;
+  const double alpha0e = drhoe - dp * enth;
+  const double alpha0v = dvel[l1];
+  const double alpha0w = dvel[l2];
+  const double wv[3] = {vel[d] - cc, vel[d], vel[d] + cc};
+  {
+    const double rho_ref = rho - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * drho;
+    double vel_ref[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      vel_ref[a] = vel[a] - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * dvel[a];
+    const double p_ref = pr - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * dp;
+    const double rhoe_ref = rhoe - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * drhoe;
+    const double apright = 0.25 * dtdx_p * (wv[0] - wv[2]) * (1.0 - copysign(1.0, wv[2])) * alphap;
+    const double amright = 0.0;
+    const double azrright = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0r;
+    const double azeright = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0e;
+    const double azv1rght = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0v;
+    const double azw1rght = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0w;
+    double r0 = rho_ref + apright + amright + azrright;
+    qp_o[ES_RHO] = dmax(r0, P.small_dens);
+    qp_o[ES_U + l0] = vel_ref[l0] + (apright - amright) * cc / rho;
+    qp_o[ES_U + l1] = vel_ref[l1] + azv1rght;
+    qp_o[ES_U + l2] = vel_ref[l2] + azw1rght;
+    double p0 = p_ref + (apright + amright) * cs;
+    qp_o[ES_P] = dmax(p0, P.small_pres);
+    qp_o[ES_REINT] = rhoe_ref + (apright + amright) * enth * cs + azeright;
+  }
+  {
+    const double rho_ref = rho + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * drho;
+    double vel_ref[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      vel_ref[a] = vel[a] + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * dvel[a];
+    const double p_ref = pr + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * dp;
+    const double rhoe_ref = rhoe + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * drhoe;
+    const double apleft = 0.0;
+    const double amleft = 0.25 * dtdx_p * (wv[2] - wv[0]) * (1.0 + copysign(1.0, wv[0])) * alpham;
+    const double azrleft = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0r;
+    const double azeleft = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0e;
+    const double azv1left = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0v;
+    const double azw1left = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0w;
+    double r0 = rho_ref + apleft + amleft + azrleft;
+    qm_o[ES_RHO] = dmax(r0, P.small_dens);
+    qm_o[ES_U + l0] = vel_ref[l0] + (apleft - amleft) * cc / rho;
+    qm_o[ES_U + l1] = vel_ref[l1] + azv1left;
+    qm_o[ES_U + l2] = vel_ref[l2] + azw1left;
+    double p0 = p_ref + (apleft + amleft) * cs;
+    qm_o[ES_P] = dmax(p0, P.small_pres);
+    qm_o[ES_REINT] = rhoe_ref + (apleft + amleft) * enth * cs + azeleft;
+  }
+  const double vel_ad = vel[l0];
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) {
+    const double qn = q[at + (SQ_FS + sp) * sn];
+    {
+      const double spzero = (vel_ad > 0) ? -1.0 : vel_ad * dtdx_p;
+      const double acmprght = 0.5 * (-1.0 - spzero) * slope[ES_FS + sp];
+      qp_o[ES_FS + sp] = qn + acmprght;
+    }
+    {
+      const double spzero = vel_ad >= 0 ? vel_ad * dtdx_p : 1.0;
+      const double acmpleft = 0.5 * (1.0 - spzero) * slope[ES_FS + sp];
+      qm_o[ES_FS + sp] = qn + acmpleft;
+    }
+  }}
+
 template <int d>
 __device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space& s,
                                                const KParams& P, const double* q, double* o) {

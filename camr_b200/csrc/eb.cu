@@ -84,8 +84,10 @@ struct EBG {
 };
 
 struct EBWork {
-  Space s;  // bx grown by 5 (+1 face layer)
+  Space s;  // bx grown by 5 (MOL) or 6 (Godunov), +1 face layer
   double *q, *sl[3], *ft[3], *qf[3], *divu, *divc, *wt, *optmp, *delm, *wtinv;
+  // Godunov (CTU-PLM) only: edge states, first-pass and D|E flux records
+  double *sm[3], *sp[3], *f1[3], *f2[6];
 };
 
 __global__ void __launch_bounds__(kEB) k_eb_ctoprim(Region r, EBWork W, EBG G, DFab u, KParams P,
@@ -538,6 +540,348 @@ __global__ void __launch_bounds__(kEB) k_eb_zero_faces(Region r, DFab f) {
 }
 
 
+// ---------------------------------------------------------------------------
+// Godunov (CTU-PLM) with embedded boundaries: Godunov_umeth_eb
+// (Godunov/Godunov_3D_eb.cpp:16-565) as face-centred passes.  The reference
+// runs transdo/transdd per cell and fills both faces of the cell; here a
+// face thread evaluates the half it needs of each of its two cells (on an
+// open face both of them are uncovered, so the reference's lo/hi-face
+// guards hold and only its no_cov_face guard, which zeroes the transverse
+// terms, remains).
+
+// flatten_eb (Godunov/flatten.H:104-134) of cell (i,j,k) in direction d:
+// 1 when the +-3 stencil leaves the q box or meets a cut cell
+// (is_cut_neighborhood, EB/eb_utils.H:7-20), else flatten.
+template <int d>
+__device__ __forceinline__ double flatten_eb_dir(int i, int j, int k, const EBWork& W,
+                                                 const EBG& G, const Region& qbox) {
+  constexpr int e0 = (d == 0), e1 = (d == 1), e2 = (d == 2);
+  if (!in_region(qbox, i + 3 * e0, j + 3 * e1, k + 3 * e2) ||
+      !in_region(qbox, i - 3 * e0, j - 3 * e1, k - 3 * e2))
+    return 1.0;
+  bool cut = f_single(G.fl(i, j, k));
+  for (int n = 1; n <= 3; ++n)
+    cut = cut || f_single(G.fl(i - n * e0, j - n * e1, k - n * e2)) ||
+          f_single(G.fl(i + n * e0, j + n * e1, k + n * e2));
+  if (cut) return 1.0;
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
+  double pp[7], un[7];
+  for (int o = -3; o <= 3; ++o) {
+    pp[o + 3] = W.q[at + o * st + SQ_P * s.sn];
+    un[o + 3] = W.q[at + o * st + (SQ_U + d) * s.sn];
+  }
+  return flatten_dir(pp, un);
+}
+
+// PLM predictor of one uncovered cell in direction d (Godunov_3D_eb.cpp:
+// 95-149): flattening, plm_slope_eb (PLM_eb.H:18-58: 4th order when the
+// cells at +-1, +-2 are uncovered, 2nd order at +-1, else 0), then
+// hydro_plm_d_eb (PLM_eb.H:111-286: a face with zero area gets a zero state).
+template <int d>
+__device__ __forceinline__ void ebc_trace_cell(int i, int j, int k, const EBWork& W,
+                                               const EBG& G, const KGeom& g, const KParams& P,
+                                               double dt, const Region& qbox) {
+  if (f_covered(G.fl(i, j, k))) return;
+  constexpr int e0 = (d == 0), e1 = (d == 1), e2 = (d == 2);
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
+  double fl = 1.0;
+  if (P.use_flattening == 1) {
+    fl = dmin(fl, flatten_eb_dir<0>(i, j, k, W, G, qbox));
+    fl = dmin(fl, flatten_eb_dir<1>(i, j, k, W, G, qbox));
+    fl = dmin(fl, flatten_eb_dir<2>(i, j, k, W, G, qbox));
+  }
+  auto open = [&](int o) { return !f_covered(G.fl(i + o * e0, j + o * e1, k + o * e2)); };
+  int order = 0;
+  if (P.plm_iorder == 4 && open(-1) && open(-2) && open(1) && open(2)) {
+    order = 4;
+  } else if (P.plm_iorder > 1 && open(-1) && open(1)) {
+    order = 2;
+  }
+  double slope[ES_N];
+  const int slot_of[ES_N] = {SQ_RHO, SQ_U, SQ_V, SQ_W, SQ_P, SQ_REINT, SQ_FS, SQ_FS + 1,
+                             SQ_FS + 2};
+  for (int n = 0; n < ES_N; ++n) {
+    if (order == 0) {
+      slope[n] = 0.0;
+      continue;
+    }
+    const double* qq = W.q + slot_of[n] * s.sn;
+    slope[n] = plm_slope(qq[at - 2 * st], qq[at - st], qq[at], qq[at + st], qq[at + 2 * st], fl,
+                         order);
+  }
+  double qp_o[ES_N], qm_o[ES_N];
+  plm_edge_states<d>(W.q, at, s.sn, slope, dt / g.dx[d], P, qp_o, qm_o);
+  if (!(G.a(d, i, j, k) > 0.0))
+    for (int n = 0; n < ES_N; ++n) qp_o[n] = 0.0;
+  if (!(G.a(d, i + e0, j + e1, k + e2) > 0.0))
+    for (int n = 0; n < ES_N; ++n) qm_o[n] = 0.0;
+  store_es(W.sp[d], s, at, qp_o);
+  store_es(W.sm[d], s, at + st, qm_o);
+}
+
+__global__ void __launch_bounds__(kEB) k_ebc_trace(Region r, EBWork W, EBG G, KGeom g, KParams P,
+                                                    DtRef dtr, Region qbox) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const double dt = dtr.get();
+  switch (blockIdx.y) {
+    case 0: ebc_trace_cell<0>(i, j, k, W, G, g, P, dt, qbox); break;
+    case 1: ebc_trace_cell<1>(i, j, k, W, G, g, P, dt, qbox); break;
+    default: ebc_trace_cell<2>(i, j, k, W, G, g, P, dt, qbox); break;
+  }
+}
+
+__device__ __forceinline__ void store_fr(double* o, const Space& s, int64_t at, const double* f,
+                                         double qpres, double qun) {
+  o[at + FR_RHO * s.sn] = f[URHO];
+  o[at + FR_MX * s.sn] = f[UMX];
+  o[at + FR_MY * s.sn] = f[UMY];
+  o[at + FR_MZ * s.sn] = f[UMZ];
+  o[at + FR_E * s.sn] = f[UEDEN];
+  for (int sp = 0; sp < NSPEC; ++sp) o[at + (FR_FS + sp) * s.sn] = f[UFS + sp];
+  o[at + FR_PRES * s.sn] = qpres;
+  o[at + FR_UN * s.sn] = qun;
+}
+
+__device__ __forceinline__ void zero_fr(double* o, const Space& s, int64_t at) {
+  for (int n = 0; n < FR_N; ++n) o[at + n * s.sn] = 0.0;
+}
+
+// First-pass Riemann flux on an open E-face (Godunov_3D_eb.cpp:157-210).
+template <int E>
+__device__ __forceinline__ void ebc_flux1_face(int i, int j, int k, const EBWork& W,
+                                               const EBG& G, const KGeom& g, const KParams& P) {
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  if (!(G.a(E, i, j, k) > 0.0)) {
+    zero_fr(W.f1[E], s, at);
+    return;
+  }
+  const int64_t stE = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
+  double qm[ES_N], qp[ES_N];
+  load_es(W.sm[E], s, at, qm);
+  load_es(W.sp[E], s, at, qp);
+  const CellAux aL = load_aux(W.q, s, at - stE, P.gamma);
+  const CellAux aR = load_aux(W.q, s, at, P.gamma);
+  const int idx = (E == 0) ? i : (E == 1) ? j : k;
+  double f[NVAR], qpres, qun;
+  cmpflx<E>(qm, qp, aL, aR, idx, g.bclo[E], g.bchi[E], g.dlo[E], g.dhi[E], P, f, qpres, qun);
+  store_fr(W.f1[E], s, at, f, qpres, qun);
+}
+
+__global__ void __launch_bounds__(kEB) k_ebc_flux1(Region r0, Region r1, Region r2, EBWork W,
+                                                    EBG G, KGeom g, KParams P) {
+  int i, j, k;
+  const int64_t t = etid();
+  switch (blockIdx.y) {
+    case 0: if (region_cell(r0, t, i, j, k)) ebc_flux1_face<0>(i, j, k, W, G, g, P); break;
+    case 1: if (region_cell(r1, t, i, j, k)) ebc_flux1_face<1>(i, j, k, W, G, g, P); break;
+    default: if (region_cell(r2, t, i, j, k)) ebc_flux1_face<2>(i, j, k, W, G, g, P); break;
+  }
+}
+
+__device__ __forceinline__ TTerms zero_tterms() {
+  TTerms t;
+  t.flxrho = t.flxu = t.flxv = t.flxw = t.flxe = 0.0;
+  for (int n = 0; n < NSPEC; ++n) t.compn[n] = 0.0;
+  t.dAup = t.pav = t.dAu = 0.0;
+  return t;
+}
+
+__device__ __forceinline__ TDTerms zero_tdterms() {
+  TDTerms t;
+  t.flxrho = t.flxu = t.flxv = t.flxw = t.flxe = 0.0;
+  for (int n = 0; n < NSPEC; ++n) t.compn[n] = 0.0;
+  t.pxnew = t.pynew = 0.0;
+  return t;
+}
+
+// D|E pass on an open D-face: the D-states of both adjacent cells corrected
+// by their E-flux differences (hydro_transdo, Godunov_utils_3D.H:22-239;
+// no_cov_face: both E-faces of the cell open), then the Riemann flux
+// (Godunov_3D_eb.cpp:212-409).
+template <int D, int E>
+__device__ __forceinline__ void ebc_flux2_face(int i, int j, int k, const EBWork& W,
+                                               const EBG& G, const KGeom& g, const KParams& P,
+                                               double dt) {
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  double* o = W.f2[combo(D, E)];
+  if (!(G.a(D, i, j, k) > 0.0)) {
+    zero_fr(o, s, at);
+    return;
+  }
+  constexpr int d0 = (D == 0), d1 = (D == 1), d2 = (D == 2);
+  constexpr int e0 = (E == 0), e1 = (E == 1), e2 = (E == 2);
+  const int64_t stD = (D == 0) ? 1 : (D == 1) ? s.sy : s.sz;
+  const int64_t stE = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
+  const double cdtdx = 1.0 / 3.0 * dt / g.dx[E];
+  const double* fE = W.f1[E];
+  double qm[ES_N], qp[ES_N], qn[ES_N];
+  {
+    const int ci = i - d0, cj = j - d1, ck = k - d2;
+    const bool ncf = G.a(E, ci + e0, cj + e1, ck + e2) > 0.0 && G.a(E, ci, cj, ck) > 0.0;
+    TTerms t = zero_tterms();
+    if (ncf) {
+      double lo[FR_N], hi[FR_N];
+      load_fr(fE, s, at - stD, lo);
+      load_fr(fE, s, at - stD + stE, hi);
+      t = transdo_terms(lo, hi, cdtdx);
+    }
+    load_es(W.sm[D], s, at, qn);
+    transdo_side(t, P.gamma, qn, cdtdx, P, qm);
+  }
+  {
+    const bool ncf = G.a(E, i + e0, j + e1, k + e2) > 0.0 && G.a(E, i, j, k) > 0.0;
+    TTerms t = zero_tterms();
+    if (ncf) {
+      double lo[FR_N], hi[FR_N];
+      load_fr(fE, s, at, lo);
+      load_fr(fE, s, at + stE, hi);
+      t = transdo_terms(lo, hi, cdtdx);
+    }
+    load_es(W.sp[D], s, at, qn);
+    transdo_side(t, P.gamma, qn, cdtdx, P, qp);
+  }
+  const CellAux aL = load_aux(W.q, s, at - stD, P.gamma);
+  const CellAux aR = load_aux(W.q, s, at, P.gamma);
+  const int idx = (D == 0) ? i : (D == 1) ? j : k;
+  double f[NVAR], qpres, qun;
+  cmpflx<D>(qm, qp, aL, aR, idx, g.bclo[D], g.bchi[D], g.dlo[D], g.dhi[D], P, f, qpres, qun);
+  store_fr(o, s, at, f, qpres, qun);
+}
+
+struct Reg6E {
+  Region r[6];
+};
+
+__global__ void __launch_bounds__(kEB) k_ebc_flux2(Reg6E regs, EBWork W, EBG G, KGeom g,
+                                                    KParams P, DtRef dtr) {
+  int i, j, k;
+  const int64_t t = etid();
+  const double dt = dtr.get();
+#define CAMR_EBF2(D, E)                                                  \
+  case combo(D, E):                                                      \
+    if (region_cell(regs.r[combo(D, E)], t, i, j, k))                    \
+      ebc_flux2_face<D, E>(i, j, k, W, G, g, P, dt);                     \
+    break;
+  switch (blockIdx.y) {
+    CAMR_EBF2(0, 1)
+    CAMR_EBF2(0, 2)
+    CAMR_EBF2(1, 0)
+    CAMR_EBF2(1, 2)
+    CAMR_EBF2(2, 0)
+    CAMR_EBF2(2, 1)
+    default: break;
+  }
+#undef CAMR_EBF2
+}
+
+// Final pass on an open D-face (Godunov_3D_eb.cpp:421-563): the D-states of
+// both cells corrected by the two transverse D|E fluxes (hydro_transdd,
+// Godunov_utils_3D.H:245-482, zero sources; no_cov_face: the cell's four
+// transverse faces open), then the Riemann flux into the face arrays.
+template <int D>
+__device__ __forceinline__ void ebc_final_face(int i, int j, int k, const EBWork& W,
+                                               const EBG& G, const KGeom& g, const KParams& P,
+                                               double dt) {
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  if (!(G.a(D, i, j, k) > 0.0)) {
+    for (int n = 0; n < NVAR; ++n) W.ft[D][at + n * s.sn] = 0.;
+    W.qf[D][at] = 0.;
+    W.qf[D][at + s.sn] = 0.;
+    return;
+  }
+  constexpr int t0 = (D == 0) ? 1 : 0;
+  constexpr int t1 = (D == 2) ? 1 : 2;
+  constexpr int d0 = (D == 0), d1 = (D == 1), d2 = (D == 2);
+  constexpr int a0 = (t0 == 0), a1 = (t0 == 1), a2 = (t0 == 2);
+  constexpr int b0 = (t1 == 0), b1 = (t1 == 1), b2 = (t1 == 2);
+  const int64_t stD = (D == 0) ? 1 : (D == 1) ? s.sy : s.sz;
+  const int64_t st0 = (t0 == 0) ? 1 : (t0 == 1) ? s.sy : s.sz;
+  const int64_t st1 = (t1 == 0) ? 1 : (t1 == 1) ? s.sy : s.sz;
+  const double hdt = 0.5 * dt;
+  const double cdtdx0 = 0.5 * dt / g.dx[t0];
+  const double cdtdx1 = 0.5 * dt / g.dx[t1];
+  const double* fa = W.f2[combo(t0, t1)];
+  const double* fb = W.f2[combo(t1, t0)];
+  double sq[ES_N];
+  for (int n = 0; n < ES_N; ++n) sq[n] = 0.0;
+  double qm[ES_N], qp[ES_N], qn[ES_N];
+  auto ncf_at = [&](int ci, int cj, int ck) {
+    return G.a(t0, ci + a0, cj + a1, ck + a2) > 0.0 && G.a(t1, ci + b0, cj + b1, ck + b2) > 0.0 &&
+           G.a(t0, ci, cj, ck) > 0.0 && G.a(t1, ci, cj, ck) > 0.0;
+  };
+  auto terms_at = [&](int64_t cell) {
+    double x0[FR_N], x1[FR_N], y0[FR_N], y1[FR_N];
+    load_fr(fa, s, cell, x0);
+    load_fr(fa, s, cell + st0, x1);
+    load_fr(fb, s, cell, y0);
+    load_fr(fb, s, cell + st1, y1);
+    return transdd_terms(x0, x1, y0, y1, P.gamma, cdtdx0, cdtdx1);
+  };
+  {
+    const TDTerms t = ncf_at(i - d0, j - d1, k - d2) ? terms_at(at - stD) : zero_tdterms();
+    load_es(W.sm[D], s, at, qn);
+    transdd_side(t, qn, sq, hdt, P, qm);
+  }
+  {
+    const TDTerms t = ncf_at(i, j, k) ? terms_at(at) : zero_tdterms();
+    load_es(W.sp[D], s, at, qn);
+    transdd_side(t, qn, sq, hdt, P, qp);
+  }
+  const CellAux aL = load_aux(W.q, s, at - stD, P.gamma);
+  const CellAux aR = load_aux(W.q, s, at, P.gamma);
+  const int idx = (D == 0) ? i : (D == 1) ? j : k;
+  double f[NVAR], qpres, qun;
+  cmpflx<D>(qm, qp, aL, aR, idx, g.bclo[D], g.bchi[D], g.dlo[D], g.dhi[D], P, f, qpres, qun);
+  for (int n = 0; n < NVAR; ++n) W.ft[D][at + n * s.sn] = f[n];
+  W.qf[D][at] = qpres;
+  W.qf[D][at + s.sn] = qun;
+  W.ft[D][at + UTEMP * s.sn] = 0.0;
+}
+
+// Final faces of the flux box ra[d]: the Godunov flux on rf[d], zero on the
+// outer layer, then adjust_fluxes_eb (as the MOL face kernel).
+template <int d>
+__device__ __forceinline__ void ebc_face_or_zero(const Region& rf, int i, int j, int k,
+                                                 const EBWork& W, const EBG& G, const KGeom& g,
+                                                 const KParams& P, const DFab& u, double dt) {
+  if (in_region(rf, i, j, k)) {
+    ebc_final_face<d>(i, j, k, W, G, g, P, dt);
+  } else {
+    const int64_t at = W.s.idx(i, j, k);
+    for (int n = 0; n < NVAR; ++n) W.ft[d][at + n * W.s.sn] = 0.;
+    W.qf[d][at] = 0.;
+    W.qf[d][at + W.s.sn] = 0.;
+  }
+  eb_adjust<d>(i, j, k, W, G, g, P, u);
+}
+
+__global__ void __launch_bounds__(kEB) k_ebc_face(Region r0, Region r1, Region r2, Region a0,
+                                                   Region a1, Region a2, EBWork W, EBG G,
+                                                   KGeom g, KParams P, DFab u, DtRef dtr) {
+  int i, j, k;
+  const int64_t t = etid();
+  const double dt = dtr.get();
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(a0, t, i, j, k)) ebc_face_or_zero<0>(r0, i, j, k, W, G, g, P, u, dt);
+      break;
+    case 1:
+      if (region_cell(a1, t, i, j, k)) ebc_face_or_zero<1>(r1, i, j, k, W, G, g, P, u, dt);
+      break;
+    default:
+      if (region_cell(a2, t, i, j, k)) ebc_face_or_zero<2>(r2, i, j, k, W, G, g, P, u, dt);
+      break;
+  }
+}
+
 // One EB hydro evaluation of box bx: the launch geometry of K1-K8 and the
 // workspace they share.  The workspace may be reused across evaluations of
 // the same box: every intermediate a kernel reads is rewritten by an
@@ -550,16 +894,22 @@ struct EBPlan {
   KParams P;
   DBox db;
   int redist, wtype;
+  bool mol;
+  DtRef dt;                    // Godunov only
   Region r5, r3, r2, r1, r0, rn, rf[3], ra[3];
   int64_t ma;
+  Region rq, r4, rf1[3];       // Godunov: q box grow(bx,6), trace cells, first-pass faces
+  Reg6E rf2;                   // Godunov: D|E faces
+  int64_t mf1, mf2;
 };
 
-// The Space of bx: grown by 5, one more high layer for faces.
-inline Space eb_space(const int bx_lo[3], const int bx_hi[3]) {
+// The Space of bx: grown by ng (5 MOL, 6 Godunov: numGrow(), CAMR.H:465-472),
+// one more high layer for faces.
+inline Space eb_space(const int bx_lo[3], const int bx_hi[3], int ng) {
   Space s;
   for (int d = 0; d < 3; ++d) {
-    s.lo[d] = bx_lo[d] - 5;
-    s.n[d] = bx_hi[d] - bx_lo[d] + 1 + 11;
+    s.lo[d] = bx_lo[d] - ng;
+    s.n[d] = bx_hi[d] - bx_lo[d] + 1 + 2 * ng + 1;
   }
   s.sy = s.n[0];
   s.sz = s.sy * s.n[1];
@@ -567,9 +917,13 @@ inline Space eb_space(const int bx_lo[3], const int bx_hi[3]) {
   return s;
 }
 
-constexpr int kEBWorkComps = SQ_N + 3 * SL_N + 3 * NVAR + 3 * 2 + 1 + NVAR + 1 + 2 * NVAR + 1;
+constexpr int kEBCommonComps = SQ_N + 3 * NVAR + 3 * 2 + 1 + NVAR + 1 + 2 * NVAR + 1;
+inline int eb_work_comps(bool mol) {
+  return kEBCommonComps + (mol ? 3 * SL_N : 6 * ES_N + 9 * FR_N);
+}
+inline int eb_grow(bool mol) { return mol ? 5 : 6; }
 
-inline void eb_carve(EBWork& W, double* base) {
+inline void eb_carve(EBWork& W, double* base, bool mol) {
   double* ptr = base;
   auto take = [&](int nc) {
     double* r = ptr;
@@ -577,7 +931,13 @@ inline void eb_carve(EBWork& W, double* base) {
     return r;
   };
   W.q = take(SQ_N);
-  for (int d = 0; d < 3; ++d) W.sl[d] = take(SL_N);
+  for (int d = 0; d < 3; ++d) {
+    W.sl[d] = mol ? take(SL_N) : nullptr;
+    W.sm[d] = mol ? nullptr : take(ES_N);
+    W.sp[d] = mol ? nullptr : take(ES_N);
+    W.f1[d] = mol ? nullptr : take(FR_N);
+  }
+  for (int c = 0; c < 6; ++c) W.f2[c] = mol ? nullptr : take(FR_N);
   for (int d = 0; d < 3; ++d) W.ft[d] = take(NVAR);
   for (int d = 0; d < 3; ++d) W.qf[d] = take(2);
   W.divu = take(1);
@@ -589,8 +949,11 @@ inline void eb_carve(EBWork& W, double* base) {
 }
 
 inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], const camr_geom& geom,
-                         const camr_eb_geom& eb, const camr_hydro_params& p, int redist) {
-  E.W.s = eb_space(bx_lo, bx_hi);
+                         const camr_eb_geom& eb, const camr_hydro_params& p, int redist,
+                         DtRef dt) {
+  E.mol = p.do_mol != 0;
+  E.dt = dt;
+  E.W.s = eb_space(bx_lo, bx_hi, eb_grow(E.mol));
   E.G.flag = eb.flag;
   E.G.vfrac = eb.vfrac;
   for (int d = 0; d < 3; ++d) {
@@ -642,6 +1005,34 @@ inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], cons
     nhi[d] = nhi[d] < ghi ? nhi[d] : ghi;
   }
   E.rn = make_region(nlo, nhi);
+  // Godunov regions (Godunov_3D_eb.cpp, bx_to_fill = grow(bx,2)): q on
+  // grow(bx,6), traces on grow(bx,4), first-pass E-faces [lo-3, hi+4] x
+  // grow(bx,4), D|E faces [lo-3, hi+4] x E in grow(bx,3) x F in grow(bx,4)
+  E.rq = reg(6, -1, 0);
+  E.r4 = reg(4, -1, 0);
+  E.mf1 = E.mf2 = 0;
+  for (int d = 0; d < 3; ++d) {
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = bx_lo[a] - (a == d ? 3 : 4);
+      hi[a] = bx_hi[a] + 4;
+    }
+    E.rf1[d] = make_region(lo, hi);
+    E.mf1 = E.rf1[d].count() > E.mf1 ? E.rf1[d].count() : E.mf1;
+  }
+  for (int D = 0; D < 3; ++D)
+    for (int Ed = 0; Ed < 3; ++Ed) {
+      if (Ed == D) continue;
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; ++a) {
+        const int gr = (a == D) ? 3 : (a == Ed) ? 3 : 4;
+        lo[a] = bx_lo[a] - gr;
+        hi[a] = bx_hi[a] + gr + (a == D ? 1 : 0);
+      }
+      Region& r = E.rf2.r[combo(D, Ed)];
+      r = make_region(lo, hi);
+      E.mf2 = r.count() > E.mf2 ? r.count() : E.mf2;
+    }
 }
 
 // K1-K8 on the stream; fo[d].p may be null (no face-flux output).
@@ -650,15 +1041,31 @@ inline int eb_issue(const EBPlan& E, const DFab& U, const DFab& dsdt, const DFab
                     cudaStream_t st) {
   int nk = 0;
   const EBWork& W = E.W;
-  k_eb_ctoprim<<<eblk(E.r5.count()), kEB, 0, st>>>(E.r5, W, E.G, U, E.P, nullptr);
-  k_eb_slope<<<dim3(eblk(E.r3.count()), 3), kEB, 0, st>>>(E.r3, W, E.G, E.P);
-  nk += 2;
+  if (E.mol) {
+    k_eb_ctoprim<<<eblk(E.r5.count()), kEB, 0, st>>>(E.r5, W, E.G, U, E.P, nullptr);
+    k_eb_slope<<<dim3(eblk(E.r3.count()), 3), kEB, 0, st>>>(E.r3, W, E.G, E.P);
+    nk += 2;
+  } else {
+    k_eb_ctoprim<<<eblk(E.rq.count()), kEB, 0, st>>>(E.rq, W, E.G, U, E.P, nullptr);
+    k_ebc_trace<<<dim3(eblk(E.r4.count()), 3), kEB, 0, st>>>(E.r4, W, E.G, E.g, E.P, E.dt,
+                                                             E.rq);
+    k_ebc_flux1<<<dim3(eblk(E.mf1), 3), kEB, 0, st>>>(E.rf1[0], E.rf1[1], E.rf1[2], W, E.G,
+                                                       E.g, E.P);
+    k_ebc_flux2<<<dim3(eblk(E.mf2), 6), kEB, 0, st>>>(E.rf2, W, E.G, E.g, E.P, E.dt);
+    nk += 4;
+  }
   if (E.rn.count() > 0) {
     k_eb_divu<<<eblk(E.rn.count()), kEB, 0, st>>>(E.rn, W, E.G, E.g);
     ++nk;
   }
-  k_eb_face<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.rf[0], E.rf[1], E.rf[2], E.ra[0], E.ra[1],
-                                                  E.ra[2], W, E.G, E.g, E.P, U);
+  if (E.mol) {
+    k_eb_face<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.rf[0], E.rf[1], E.rf[2], E.ra[0], E.ra[1],
+                                                    E.ra[2], W, E.G, E.g, E.P, U);
+  } else {
+    k_ebc_face<<<dim3(eblk(E.ma), 3), kEB, 0, st>>>(E.rf[0], E.rf[1], E.rf[2], E.ra[0],
+                                                     E.ra[1], E.ra[2], W, E.G, E.g, E.P, U,
+                                                     E.dt);
+  }
   k_eb_div<<<eblk(E.r2.count()), kEB, 0, st>>>(E.r2, W, E.G, E.g, E.P, fo[0], fo[1], fo[2],
                                                E.wtype);
   nk += 2;
@@ -810,9 +1217,29 @@ __device__ __forceinline__ void clean_eb_cell(double* s, const KParams& P, bool 
   temp_eb(s, P);
 }
 
-// MOL stage 2: S = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2, then clean_state,
-// the new-source correction (+ clean_state), post_timestep's clean_state,
-// and the cell's CFL dt.
+// The end of a level step on one cell: clean_state, the new-source
+// correction (+ clean_state), post_timestep's clean_state; returns the
+// cell's CFL dt (DBL_MAX on covered cells).
+__device__ __forceinline__ double ebl_finish(double* s, const double* sold, const KParams& P,
+                                             const LGeom& L, double dt, bool cov, int i, int j,
+                                             int k, DevError* err) {
+  clean_eb_cell(s, P, cov, i, j, k, err);
+  if (P.add_grav_src) {
+    double src[NVAR];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+    src[UMZ] = 0.5 * P.const_grav * (s[URHO] - sold[URHO]);
+    src[UEDEN] = 0.5 * P.const_grav * (s[UMZ] - sold[UMZ]);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
+    clean_eb_cell(s, P, cov, i, j, k, err);
+  }
+  clean_eb_cell(s, P, cov, i, j, k, err);
+  return cov ? DBL_MAX : cell_dt(s, L, P);
+}
+
+// MOL stage 2: S = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2, then the end of
+// the step and the cell's CFL dt.
 __global__ void __launch_bounds__(kBlk) k_ebl_update2(LGeom L, KParams P, EBG G,
                                                        const double* dtp, const double* B2,
                                                        const double* S_old, const double* dsdt,
@@ -831,19 +1258,41 @@ __global__ void __launch_bounds__(kBlk) k_ebl_update2(LGeom L, KParams P, EBG G,
     for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * dsdt[at + n * L.sn];
-    clean_eb_cell(s, P, cov, i, j, k, err);
+    v = ebl_finish(s, sold, P, L, dt, cov, i, j, k, err);
+    store_cell(S, L, at, s);
+  }
+  block_min_dt(v, bits);
+}
+
+// Godunov: S = Sborder (+ dt*src_old) + dt*dSdt, then the end of the step
+// (CAMR_advance.cpp:101-121).
+__global__ void __launch_bounds__(kBlk) k_ebl_update_ctu(LGeom L, KParams P, EBG G,
+                                                          const double* dtp, const double* B,
+                                                          const double* S_old,
+                                                          const double* dsdt, double* S,
+                                                          unsigned long long* bits,
+                                                          DevError* err) {
+  int i, j, k;
+  double v = DBL_MAX;
+  if (valid_cell(L, tid(), i, j, k)) {
+    const double dt = *dtp;
+    const int64_t at = L.idx(i, j, k);
+    const bool cov = cov_at(G, i, j, k);
+    double s[NVAR], sold[NVAR];
+    load_cell(B, L, at, s);
+    load_cell(S_old, L, at, sold);
     if (P.add_grav_src) {
       double src[NVAR];
 #pragma unroll
       for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
-      src[UMZ] = 0.5 * P.const_grav * (s[URHO] - sold[URHO]);
-      src[UEDEN] = 0.5 * P.const_grav * (s[UMZ] - sold[UMZ]);
+      src[UMZ] = P.const_grav * sold[URHO];
+      src[UEDEN] = P.const_grav * sold[UMZ];
 #pragma unroll
       for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-      clean_eb_cell(s, P, cov, i, j, k, err);
     }
-    clean_eb_cell(s, P, cov, i, j, k, err);
-    if (!cov) v = cell_dt(s, L, P);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += dt * dsdt[at + n * L.sn];
+    v = ebl_finish(s, sold, P, L, dt, cov, i, j, k, err);
     store_cell(S, L, at, s);
   }
   block_min_dt(v, bits);
@@ -879,29 +1328,31 @@ extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3
                                            camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
                                            const camr_hydro_params* p, int redist, double dt,
                                            void* stream) {
-  (void)dt;
   if (!bx_lo || !bx_hi || !geom || !uin || !eb || !dsdt || !flx0 || !flx1 || !flx2 || !p)
     return CAMR_ERR_INVALID;
-  if (!p->do_mol || p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  // Godunov with EB is PLM only (Source/CAMR.cpp:186-190)
+  if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;
   if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
     return CAMR_ERR_INVALID;
+  const int ng = eb_grow(p->do_mol != 0);
   for (int d = 0; d < 3; ++d) {
     if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
-    if (uin->lo[d] > bx_lo[d] - 5 || uin->hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
-    if (eb->g_lo[d] > bx_lo[d] - 5 || eb->g_hi[d] < bx_hi[d] + 5) return CAMR_ERR_INVALID;
+    if (uin->lo[d] > bx_lo[d] - ng || uin->hi[d] < bx_hi[d] + ng) return CAMR_ERR_INVALID;
+    if (eb->g_lo[d] > bx_lo[d] - ng || eb->g_hi[d] < bx_hi[d] + ng) return CAMR_ERR_INVALID;
   }
   if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
       !eb->fc[1] || !eb->fc[2])
     return CAMR_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   EBPlan E;
-  eb_plan_init(E, bx_lo, bx_hi, *geom, *eb, *p, redist);
-  const size_t bytes = size_t(kEBWorkComps) * E.W.s.sn * sizeof(double);
+  eb_plan_init(E, bx_lo, bx_hi, *geom, *eb, *p, redist, DtRef{dt, nullptr});
+  const size_t bytes = size_t(eb_work_comps(E.mol)) * E.W.s.sn * sizeof(double);
   double* base = nullptr;
   if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess)
     return CAMR_ERR_NOMEM;
   cudaError_t e = cudaMemsetAsync(base, 0, bytes, st);
-  eb_carve(E.W, base);
+  eb_carve(E.W, base, E.mol);
   // zero the output faces (covered cells leave theirs untouched)
   const DFab fo[3] = {make_dfab(*flx0), make_dfab(*flx1), make_dfab(*flx2)};
   int nk = 0;
@@ -1034,6 +1485,12 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err);
   nk += 3;
   nk += eb_hydro_stage(lev, st);
+  if (!lev->hp.do_mol) {
+    k_ebl_update_ctu<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old,
+                                          lev->dsdt, lev->S, lev->bits, lev->err);
+    count_launch(nk + 1);
+    return cudaGetLastError();
+  }
   k_ebl_update1<<<gv, kBlk, 0, st>>>(L, lev->P, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
                                      lev->S);
   // stage 2's Sborder reuses B (stage 1's is dead after the update)
@@ -1074,15 +1531,21 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
                                  camr_eb_level** out) {
   if (!desc || !eb || !p || !out) return CAMR_ERR_INVALID;
   *out = nullptr;
-  if (!p->do_mol || p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  // Godunov with EB is PLM only (Source/CAMR.cpp:186-190); its predictor
+  // sources are taken as zero, so no gravity with Godunov
+  if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;
+  if (!p->do_mol && p->add_grav_src && p->const_grav != 0.0) return CAMR_ERR_UNSUPPORTED;
   if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
     return CAMR_ERR_INVALID;
   const camr_geom& g = desc->geom;
+  const int ng = eb_grow(p->do_mol != 0);
   for (int d = 0; d < 3; ++d) {
     if (g.dom_hi[d] < g.dom_lo[d]) return CAMR_ERR_INVALID;
     if (!g.is_periodic[d] && (g.bc_lo[d] == CAMR_BC_INTERIOR || g.bc_hi[d] == CAMR_BC_INTERIOR))
       return CAMR_ERR_INVALID;
-    if (eb->g_lo[d] != g.dom_lo[d] - 5 || eb->g_hi[d] != g.dom_hi[d] + 5) return CAMR_ERR_INVALID;
+    if (eb->g_lo[d] != g.dom_lo[d] - ng || eb->g_hi[d] != g.dom_hi[d] + ng)
+      return CAMR_ERR_INVALID;
     if (desc->max_grid_size[d] < 0) return CAMR_ERR_INVALID;
   }
   if (!eb->flag || !eb->vfrac || !eb->ap[0] || !eb->ap[1] || !eb->ap[2] || !eb->fc[0] ||
@@ -1105,8 +1568,8 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   for (int d = 0; d < 3; ++d) {
     L.dlo[d] = g.dom_lo[d];
     L.dhi[d] = g.dom_hi[d];
-    L.plo[d] = g.dom_lo[d] - 5;
-    L.pn[d] = g.dom_hi[d] - g.dom_lo[d] + 1 + 10;
+    L.plo[d] = g.dom_lo[d] - ng;
+    L.pn[d] = g.dom_hi[d] - g.dom_lo[d] + 1 + 2 * ng;
     L.periodic[d] = g.is_periodic[d];
     L.bclo[d] = g.bc_lo[d];
     L.bchi[d] = g.bc_hi[d];
@@ -1285,12 +1748,12 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   for (const auto& b : cut_boxes) {
     const int lo[3] = {b[0], b[1], b[2]}, hi[3] = {b[3], b[4], b[5]};
     EBPlan E;
-    eb_plan_init(E, lo, hi, g, own, *p, redist);
+    eb_plan_init(E, lo, hi, g, own, *p, redist, DtRef{0.0, lev->dt_cur});
     double* w = nullptr;
-    alloc(reinterpret_cast<void**>(&w), size_t(kEBWorkComps) * E.W.s.sn * sizeof(double));
+    alloc(reinterpret_cast<void**>(&w), size_t(eb_work_comps(E.mol)) * E.W.s.sn * sizeof(double));
     if (e != cudaSuccess) break;
     lev->plan_work.push_back(w);
-    eb_carve(E.W, w);
+    eb_carve(E.W, w, E.mol);
     lev->plans.push_back(E);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);

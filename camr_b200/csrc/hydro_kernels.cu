@@ -235,89 +235,7 @@ __device__ __forceinline__ void trace_body(int i, int j, int k, const Space& s,
       stencil(slot_of[n], sv);
       slope[n] = plm_slope(sv[0], sv[1], sv[2], sv[3], sv[4], fl, P.plm_iorder);
     }
-    constexpr int l0 = d;
-    constexpr int l1 = (d == 0) ? 1 : 0;
-    constexpr int l2 = (d == 2) ? 1 : 2;
-    const double cc = q[at + SQ_C * s.sn];
-    const double dtdx_p = dt / g.dx[d];
-    const double cs = cc * cc;
-    const double rho = q[at + SQ_RHO * s.sn];
-    const double vel[3] = {q[at + SQ_U * s.sn], q[at + SQ_V * s.sn], q[at + SQ_W * s.sn]};
-    const double pr = q[at + SQ_P * s.sn];
-    const double rhoe = q[at + SQ_REINT * s.sn];
-    const double enth = ((rhoe + pr) / rho) / cs;
-    const double drho = slope[ES_RHO];
-    const double dvel[3] = {slope[ES_U], slope[ES_V], slope[ES_W]};
-    const double dp = slope[ES_P];
-    const double drhoe = slope[ES_REINT];
-    const double alpham = 0.5 * (dp / (rho * cc) - dvel[d]) * rho / cc;
-    const double alphap = 0.5 * (dp / (rho * cc) + dvel[d]) * rho / cc;
-    const double alpha0r = drho - dp / cs;
-    const double alpha0e = drhoe - dp * enth;
-    const double alpha0v = dvel[l1];
-    const double alpha0w = dvel[l2];
-    const double wv[3] = {vel[d] - cc, vel[d], vel[d] + cc};
-    {
-      const double rho_ref = rho - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * drho;
-      double vel_ref[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-        vel_ref[a] = vel[a] - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * dvel[a];
-      const double p_ref = pr - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * dp;
-      const double rhoe_ref = rhoe - 0.5 * (1.0 + dtdx_p * dmin(wv[0], 0.0)) * drhoe;
-      const double apright = 0.25 * dtdx_p * (wv[0] - wv[2]) * (1.0 - copysign(1.0, wv[2])) * alphap;
-      const double amright = 0.0;
-      const double azrright = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0r;
-      const double azeright = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0e;
-      const double azv1rght = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0v;
-      const double azw1rght = 0.25 * dtdx_p * (wv[0] - wv[1]) * (1.0 - copysign(1.0, wv[1])) * alpha0w;
-      double r0 = rho_ref + apright + amright + azrright;
-      qp_o[ES_RHO] = dmax(r0, P.small_dens);
-      qp_o[ES_U + l0] = vel_ref[l0] + (apright - amright) * cc / rho;
-      qp_o[ES_U + l1] = vel_ref[l1] + azv1rght;
-      qp_o[ES_U + l2] = vel_ref[l2] + azw1rght;
-      double p0 = p_ref + (apright + amright) * cs;
-      qp_o[ES_P] = dmax(p0, P.small_pres);
-      qp_o[ES_REINT] = rhoe_ref + (apright + amright) * enth * cs + azeright;
-    }
-    {
-      const double rho_ref = rho + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * drho;
-      double vel_ref[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-        vel_ref[a] = vel[a] + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * dvel[a];
-      const double p_ref = pr + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * dp;
-      const double rhoe_ref = rhoe + 0.5 * (1.0 - dtdx_p * dmax(wv[2], 0.0)) * drhoe;
-      const double apleft = 0.0;
-      const double amleft = 0.25 * dtdx_p * (wv[2] - wv[0]) * (1.0 + copysign(1.0, wv[0])) * alpham;
-      const double azrleft = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0r;
-      const double azeleft = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0e;
-      const double azv1left = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0v;
-      const double azw1left = 0.25 * dtdx_p * (wv[2] - wv[1]) * (1.0 + copysign(1.0, wv[1])) * alpha0w;
-      double r0 = rho_ref + apleft + amleft + azrleft;
-      qm_o[ES_RHO] = dmax(r0, P.small_dens);
-      qm_o[ES_U + l0] = vel_ref[l0] + (apleft - amleft) * cc / rho;
-      qm_o[ES_U + l1] = vel_ref[l1] + azv1left;
-      qm_o[ES_U + l2] = vel_ref[l2] + azw1left;
-      double p0 = p_ref + (apleft + amleft) * cs;
-      qm_o[ES_P] = dmax(p0, P.small_pres);
-      qm_o[ES_REINT] = rhoe_ref + (apleft + amleft) * enth * cs + azeleft;
-    }
-    const double vel_ad = vel[l0];
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) {
-      const double qn = q[at + (SQ_FS + sp) * s.sn];
-      {
-        const double spzero = (vel_ad > 0) ? -1.0 : vel_ad * dtdx_p;
-        const double acmprght = 0.5 * (-1.0 - spzero) * slope[ES_FS + sp];
-        qp_o[ES_FS + sp] = qn + acmprght;
-      }
-      {
-        const double spzero = vel_ad >= 0 ? vel_ad * dtdx_p : 1.0;
-        const double acmpleft = 0.5 * (1.0 - spzero) * slope[ES_FS + sp];
-        qm_o[ES_FS + sp] = qn + acmpleft;
-      }
-    }
+    plm_edge_states<d>(q, at, s.sn, slope, dt / g.dx[d], P, qp_o, qm_o);
   }
   store_es(spd, s, at, qp_o);
   store_es(smd, s, at + st, qm_o);

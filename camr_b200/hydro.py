@@ -105,8 +105,9 @@ def eb_geometry_to_device(geo, device="cuda"):
 
 def hydro_umdrv_eb(bx_lo, bx_hi, geom, uin, uin_lo, ebdev, params, redist=True, dt=0.0,
                    stream=None):
-    """EB per-box hydro (MOL) on CUDA tensors: uin (NVAR, ...) over a region
-    starting at uin_lo covering grow(bx, 5); ebdev from eb_geometry_to_device.
+    """EB per-box hydro on CUDA tensors (MOL, or Godunov-PLM with do_mol = 0):
+    uin (NVAR, ...) over a region starting at uin_lo covering grow(bx, 5)
+    (MOL) or grow(bx, 6) (Godunov); ebdev from eb_geometry_to_device.
     Returns (dsdt, [flx_x, flx_y, flx_z]) as new CUDA tensors."""
     torch = _torch()
     nb = [bx_hi[d] - bx_lo[d] + 1 for d in range(3)]
@@ -220,10 +221,11 @@ class Level:
 
 
 class EBLevel:
-    """One uniform level with an embedded boundary (MOL), advanced on the GPU
-    through camr_eb_level_*.  geo: eb_geometry.sphere_geometry output over
-    grow(domain, 5) (copied into the level).  redist: 1 FluxRedist, 0
-    NoRedist."""
+    """One uniform level with an embedded boundary (MOL, or Godunov-PLM with
+    do_mol = 0), advanced on the GPU through camr_eb_level_*.  geo:
+    eb_geometry.sphere_geometry output over grow(domain, 5) for MOL,
+    grow(domain, 6) for Godunov (copied into the level).  redist: 1
+    FluxRedist, 0 NoRedist.  max_grid_size chops the domain into boxes."""
 
     def __init__(self, geom, params, geo, redist=1, max_grid_size=(0, 0, 0), use_graph=True,
                  stream=None):

@@ -343,17 +343,19 @@ camr_status camr_adjoint_stream(camr_adjoint* a, void** stream);
 camr_status camr_adjoint_get_error(camr_adjoint* a, camr_error_info* info);
 
 /* ---------------------------------------------------------------------
- * Embedded-boundary per-box hydro, MOL: hydro_umdrv_eb with do_mol = 1
- * (Source/Hydro/Hydro_umdrv_eb.cpp:14-191) with flux redistribution
- * (AMReX's FluxRedist, restated).  Geometry on a cell region G covering
- * grow(bx, 5), device pointers, i fastest:
+ * Embedded-boundary per-box hydro: hydro_umdrv_eb
+ * (Source/Hydro/Hydro_umdrv_eb.cpp:14-191), MOL (MOL_umeth_eb) or, with
+ * do_mol = 0, Godunov-PLM (Godunov_umeth_eb, ppm_type must be 0; zero
+ * predictor sources), with flux redistribution (AMReX's FluxRedist,
+ * restated).  ng = 5 for MOL, 6 for Godunov.  Geometry on a cell region G
+ * covering grow(bx, ng), device pointers, i fastest:
  *   flag   G cells: bits 0-1 type (0 regular, 1 cut, 3 covered), bit
  *          2 + (di+1) + 3 (dj+1) + 9 (dk+1) connectivity to neighbour
  *          (di,dj,dk) (the cell itself included)
  *   vfrac  G cells; ap[d] faces of G in direction d (surroundingNodes(G, d));
  *   fc[d]  2 components (transverse directions in x, y, z order) on the
  *          same faces, component planes outermost.
- * uin covers grow(bx, 5).  dsdt (bx) is overwritten (the reference's
+ * uin covers grow(bx, ng).  dsdt (bx) is overwritten (the reference's
  * redistribution writes it); flx[d] receive the face-centroid fluxes of
  * bx's faces.  redist: 1 = flux redistribution, 0 = none.
  */
@@ -373,15 +375,17 @@ camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3], const ca
                                 void* stream);
 
 /* ---------------------------------------------------------------------
- * EB level: one uniform level with an embedded boundary, MOL only
- * (CAMR_advance's do_mol branch, Source/CAMR_advance.cpp:38-164, with
- * hydro_umdrv_eb per stage and the EB build's clean_state / computeTemp /
- * estTimeStep guards for covered cells), 5 ghost cells.  desc->max_grid_size
+ * EB level: one uniform level with an embedded boundary, MOL or Godunov-PLM
+ * (CAMR_advance, Source/CAMR_advance.cpp:38-164, with hydro_umdrv_eb per
+ * stage and the EB build's clean_state / computeTemp / estTimeStep guards
+ * for covered cells), 5 ghost cells for MOL, 6 for Godunov.  desc->max_grid_size
  * chops the domain into boxes (0 = one box): as in an EB build's
  * construct_hydro_source, covered boxes are skipped, boxes whose grow(box,2)
  * is all regular run the regular hydro (one batched launch per stage for
  * all of them) and the others the EB hydro.  eb: geometry over exactly grow(domain, 5), host or
- * device memory, copied into the level.  redist: 0 NoRedist, 1 FluxRedist
+ * device memory, copied into the level (grow(domain, 6) for Godunov).
+ * Godunov requires ppm_type = 0 (Source/CAMR.cpp:186-190) and no gravity
+ * source.  redist: 0 NoRedist, 1 FluxRedist
  * (StateRedist is not provided: CAMR_ERR_INVALID).  Covered cells hold zero
  * state (initData's EB_set_covered); set_state/get_state/advance/dts as
  * for camr_level_*.

@@ -128,6 +128,12 @@ struct Box {
     for (int d = 0; d < 3; ++d) { lo[d] -= n[d]; hi[d] += n[d]; }
     return *this;
   }
+  // grow by n in direction d only
+  Box& grow(int d, int n) {
+    lo[d] -= n;
+    hi[d] += n;
+    return *this;
+  }
   Box& surroundingNodes() {
     for (int d = 0; d < 3; ++d)
       if (!nodal[d]) { hi[d] += 1; nodal[d] = 1; }

@@ -25,6 +25,7 @@
 #include "Hydro.H"
 #include "Hydro_ctoprim.H"
 #include "MOL_umeth.H"
+#include "Godunov.H"
 #include "IndexDefines.H"
 #include "oracle_abi.h"
 
@@ -48,7 +49,6 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
                                  const double* fc2, int redist, int weights_type, double* dsdt,
                                  double* flx0, double* flx1, double* flx2, const double dx_in[3],
                                  double dt) {
-  (void)dt;
   shim_assert_count() = 0;
   PassMap pmap;
   init_pass_map(&pmap);
@@ -78,11 +78,16 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
     dx[d] = dx_in[d];
     dxinv[d] = 1. / dx_in[d];
   }
-  // q, qaux on grow(bx, 5): hydro_ctoprim on the non-covered cells
-  const Box qbx = amrex::grow(bx, 5);
-  FArrayBox qf(qbx, QVAR), qauxf(qbx, NQAUX);
+  // q, qaux on grow(bx, numGrow()): 5 for MOL, 6 for Godunov with flux
+  // redistribution (CAMR.H:465-472); hydro_ctoprim on the non-covered cells
+  const bool mol = p->do_mol != 0;
+  const Box qbx = amrex::grow(bx, mol ? 5 : 6);
+  FArrayBox qf(qbx, QVAR), qauxf(qbx, NQAUX), srcqf(qbx, QVAR), zsrc(qbx, NVAR);
   auto q = qf.array();
   auto qaux = qauxf.array();
+  auto srcq = srcqf.array();
+  zsrc.setVal(0.0);
+  auto src_in = zsrc.const_array();
   ParallelFor(qbx, [=](int i, int j, int k) {
     if (!flag(i, j, k).isCovered()) {
       hydro_ctoprim(i, j, k, u, q, qaux, *pm, p->small_num, p->dual_energy_eta1,
@@ -91,6 +96,17 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
       for (int n = 0; n < QVAR; n++) q(i, j, k, n) = 0.;
     }
   });
+  if (!mol) {
+    // sources for the Godunov predictor: zero (no gravity in EB runs here)
+    ParallelFor(qbx, [=](int i, int j, int k) {
+      if (!flag(i, j, k).isCovered()) {
+        hydro_srctoprim(i, j, k, Array4<const Real>(q), Array4<const Real>(qaux), src_in, srcq,
+                        *pm);
+      } else {
+        for (int n = 0; n < QVAR; n++) srcq(i, j, k, n) = 0.;
+      }
+    });
+  }
   const Box bxg_i = amrex::grow(bx, 2);
   const Box bxg_ii = amrex::grow(bxg_i, 1);
   FArrayBox divc(bxg_i, NVAR), redistwgt(bxg_i, 1);
@@ -109,9 +125,19 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
   const int* dh = dom.hiVect();
   auto divc_arr = divc.array();
   auto wt = redistwgt.array();
-  MOL_umeth_eb(Box(divc_arr), bclo, bchi, dl, dh, Array4<const Real>(q), Array4<const Real>(qaux),
-               qec_arr[0], qec_arr[1], qec_arr[2], flag, dx, ft, p->small, p->small_dens,
-               p->small_pres, p->smallu, p->plm_iorder, pm, weights_type);
+  if (mol) {
+    MOL_umeth_eb(Box(divc_arr), bclo, bchi, dl, dh, Array4<const Real>(q),
+                 Array4<const Real>(qaux), qec_arr[0], qec_arr[1], qec_arr[2], flag, dx, ft,
+                 p->small, p->small_dens, p->small_pres, p->smallu, p->plm_iorder, pm,
+                 weights_type);
+  } else {
+    Godunov_umeth_eb(Box(divc_arr), bclo, bchi, dl, dh, Array4<const Real>(q),
+                     Array4<const Real>(qaux), Array4<const Real>(srcq), ft[0], ft[1], ft[2],
+                     qec_arr[0], qec_arr[1], qec_arr[2], ap[0], ap[1], ap[2], flag, dx, dt,
+                     p->small, p->small_dens, p->small_pres, p->smallu, p->ppm_type,
+                     p->use_pslope, p->use_flattening, p->plm_iorder, pm,
+                     p->transverse_reset_density);
+  }
   adjust_fluxes_eb(bx, Array4<const Real>(q), u, ap[0], ap[1], ap[2], vf, dx, dxinv, ft, geom,
                    bclo, bchi, p->difmag);
   double* fo[3] = {flx0, flx1, flx2};
@@ -187,7 +213,8 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
 }
 
 // ---------------------------------------------------------------------------
-// EB level step (MOL), the restated level driver's CAMR_advance + post_timestep
+// EB level step (MOL or Godunov-PLM), the restated level driver's
+// CAMR_advance + post_timestep
 // (Source/CAMR_advance.cpp:38-164, Source/CAMR.cpp:679-718) with the EB
 // build's guards: covered cells skip enforce_min_density and
 // normalize_species (Source/CAMR.cpp:877-891, :960-968), reset_internal_energy
@@ -440,8 +467,8 @@ double est_dt_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S) {
 // q on grow(bx, numGrow() = 5) with covered cells zero, then the
 // reference's regular hydro_umdrv accumulating into dsdt.
 static long eb_regular_box(const orc_params* p, const LevelEB& L, const Box& bx,
-                    Array4<Real> const& B, Array4<Real> const& dsdt) {
-  const Box qbx = amrex::grow(bx, 5);
+                    Array4<Real> const& B, Array4<Real> const& dsdt, double dt) {
+  const Box qbx = amrex::grow(bx, p->do_mol ? 5 : 6);
   PassMap pmap;
   init_pass_map(&pmap);
   FArrayBox q(qbx, QVAR), qaux(qbx, NQAUX), src_q(qbx, QVAR);
@@ -459,6 +486,19 @@ static long eb_regular_box(const orc_params* p, const LevelEB& L, const Box& bx,
       for (int n = 0; n < QVAR; ++n) qarr(i, j, k, n) = 0.;
     }
   });
+  if (!p->do_mol) {
+    FArrayBox zsrc(qbx, NVAR);
+    zsrc.setVal(0.0);
+    auto src_in = zsrc.const_array();
+    ParallelFor(qbx, [&](int i, int j, int k) {
+      if (!covered(L, i, j, k)) {
+        hydro_srctoprim(i, j, k, Array4<const Real>(qarr), Array4<const Real>(qauxar), src_in,
+                        srcqarr, pmap);
+      } else {
+        for (int n = 0; n < QVAR; ++n) srcqarr(i, j, k, n) = 0.;
+      }
+    });
+  }
   FArrayBox flux[3], area[3], vol(bx, 1);
   Array4<Real> fa[3];
   Array4<Real> aa[3];
@@ -477,7 +517,7 @@ static long eb_regular_box(const orc_params* p, const LevelEB& L, const Box& bx,
       {Array4<const Real>(aa[0]), Array4<const Real>(aa[1]), Array4<const Real>(aa[2])}};
   const amrex::GpuArray<Real, 3> dxa{{L.dx[0], L.dx[1], L.dx[2]}};
   const Geometry geom(L.dom, L.periodic);
-  hydro_umdrv(true, bx, geom, L.bclo, L.bchi, sarr, dsdt, qarr, qauxar, srcqarr, dxa, 0.0,
+  hydro_umdrv(p->do_mol != 0, bx, geom, L.bclo, L.bchi, sarr, dsdt, qarr, qauxar, srcqarr, dxa, dt,
               p->ppm_type, p->plm_iorder, p->use_pslope, p->use_flattening,
               p->transverse_reset_density, p->small, p->small_dens, p->small_pres, p->smallu,
               p->difmag, flx_arr, a, vol.array(), &pmap);
@@ -498,7 +538,10 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
     L.bchi[d] = lev->bc_hi[d];
     L.dx[d] = lev->dx[d];
   }
-  L.G = amrex::grow(L.dom, 5);
+  // ghost cells: numGrow() with flux redistribution, 5 for MOL, 6 for
+  // Godunov (CAMR.H:465-472); the geometry covers grow(domain, ng)
+  const int ng = p->do_mol ? 5 : 6;
+  L.G = amrex::grow(L.dom, ng);
   std::vector<EBCellFlag> fl(size_t(L.G.numPts()));
   for (size_t c = 0; c < fl.size(); ++c) fl[c] = EBCellFlag(flag_in[c]);
   L.flag = Array4<EBCellFlag const>(fl.data(), L.G.lo,
@@ -552,7 +595,7 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
       const Box& bx = boxes[b];
       if (kind[b] == 0) continue;
       if (kind[b] == 1) {
-        ne += eb_regular_box(p, L, bx, Bv, kout);
+        ne += eb_regular_box(p, L, bx, Bv, kout, dt);
         continue;
       }
       FArrayBox dfab(bx, NVAR), ff[3];
@@ -594,14 +637,16 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
     }
     nerr += stage(B, k1, dt);
     ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S(i, j, k, n) += dt * k1(i, j, k, n); });
-    nerr += expand_eb(p, L, S, B2);
-    nerr += stage(B2, k2, dt);
-    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
-      S(i, j, k, n) = 0.5 * B2(i, j, k, n) + 0.5 * S_old(i, j, k, n);
-    });
-    ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
-      S(i, j, k, n) += 0.5 * dt * k2(i, j, k, n);
-    });
+    if (p->do_mol) {
+      nerr += expand_eb(p, L, S, B2);
+      nerr += stage(B2, k2, dt);
+      ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
+        S(i, j, k, n) = 0.5 * B2(i, j, k, n) + 0.5 * S_old(i, j, k, n);
+      });
+      ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
+        S(i, j, k, n) += 0.5 * dt * k2(i, j, k, n);
+      });
+    }
     nerr += clean_eb(p, L, S);
     if (p->add_grav_src) {
       ParallelFor(L.dom, [&](int i, int j, int k) {

@@ -35,30 +35,30 @@ def assert_bitwise(a, b, what):
         raise AssertionError(f"{what}: {nd}/{a.size} values differ (max rel {rel:.3e})")
 
 
-def periodic_case(n=24, bx=((4, 4, 4), (19, 19, 19)), seed=3, radius=0.2):
+def periodic_case(n=24, bx=((4, 4, 4), (19, 19, 19)), seed=3, radius=0.2, ng=5):
     lo, hi = bx
     dx = 1.0 / n
-    g_lo = tuple(v - 5 for v in lo)
-    g_hi = tuple(v + 5 for v in hi)
+    g_lo = tuple(v - ng for v in lo)
+    g_hi = tuple(v + ng for v in hi)
     geo = E.sphere_geometry(g_lo, g_hi, dx, radius=radius)
     s = P.random_smooth((n, n, n), seed=seed, amp=0.1, vel=0.2)
     p = oracle.default_params(do_mol=1, cfl=0.3)
     lev = oracle.make_level((n, n, n))
     oracle.init_finalize("restate", p, lev, s)
-    full = np.pad(s, ((0, 0), (5, 5), (5, 5), (5, 5)), mode="wrap")  # over [-5, n+4]
-    sl = tuple(slice(g_lo[d] + 5, g_hi[d] + 6) for d in (2, 1, 0))
+    full = np.pad(s, ((0, 0), (ng, ng), (ng, ng), (ng, ng)), mode="wrap")  # [-ng, n+ng-1]
+    sl = tuple(slice(g_lo[d] + ng, g_hi[d] + ng + 1) for d in (2, 1, 0))
     G = np.ascontiguousarray(full[(slice(None),) + sl])
     geom = hydro.make_geom((n, n, n))
     return geo, G, g_lo, lo, hi, geom, (0, 0, 0), (n - 1,) * 3, (1, 1, 1), (0, 0, 0), (0, 0, 0), dx
 
 
-def sod_sphere_case(nx=32, ny=16):
+def sod_sphere_case(nx=32, ny=16, ng=5):
     """C4's geometry at low resolution: [0,2]x[0,1]^2, sphere r = 0.15 at
     (1, 0.5, 0.5), x outflow, y/z slip walls, Sod states (x < 0.5)."""
     dx = 1.0 / ny
     n = (nx, ny, ny)
     lo, hi = (0, 0, 0), (nx - 1, ny - 1, ny - 1)
-    g_lo, g_hi = (-5, -5, -5), (nx + 4, ny + 4, ny + 4)
+    g_lo, g_hi = (-ng,) * 3, (nx + ng - 1, ny + ng - 1, ny + ng - 1)
     geo = E.sphere_geometry(g_lo, g_hi, dx, center=(1.0, 0.5, 0.5), radius=0.15)
     s = P.sod(n, (dx, dx, dx))
     s[P.UMX] += 0.05 * s[P.URHO]  # a little flow through the obstacle
@@ -66,7 +66,7 @@ def sod_sphere_case(nx=32, ny=16):
     p = oracle.default_params(do_mol=1, cfl=0.3)
     lev = oracle.make_level(n, periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4), dx=(dx,) * 3)
     oracle.init_finalize("restate", p, lev, s)
-    G = oracle.expand_state("restate", p, lev, s, ng=5)
+    G = oracle.expand_state("restate", p, lev, s, ng=ng)
     geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
                            dx=(dx,) * 3)
     return geo, G, g_lo, lo, hi, geom, lo, hi, (0, 0, 0), (2, 4, 4), (2, 4, 4), dx
@@ -75,18 +75,22 @@ def sod_sphere_case(nx=32, ny=16):
 @pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
 @pytest.mark.parametrize("case", ["periodic_box", "sod_sphere"])
 @pytest.mark.parametrize("redist", [0, 1])
-def test_eb_box_matches_oracle(case, redist):
+@pytest.mark.parametrize("do_mol", [1, 0])
+def test_eb_box_matches_oracle(case, redist, do_mol):
+    """MOL (MOL_umeth_eb) and Godunov-PLM (Godunov_umeth_eb) per box."""
     torch = _torch()
+    ng = 5 if do_mol else 6
     geo, G, g_lo, lo, hi, geom, dlo, dhi, per, bclo, bchi, dx = (
-        periodic_case() if case == "periodic_box" else sod_sphere_case())
-    p = oracle.default_params(do_mol=1, cfl=0.3)
+        periodic_case(ng=ng) if case == "periodic_box" else sod_sphere_case(ng=ng))
+    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
+    dt = 2e-3
     ref_d, ref_f, nass = oracle.hydro_box_eb(p, lo, hi, dlo, dhi, bclo, bchi, per, G, g_lo, geo,
-                                             (dx,) * 3, 1e-3, redist=redist)
+                                             (dx,) * 3, dt, redist=redist)
     assert nass == 0
     ebdev = hydro.eb_geometry_to_device(geo)
-    prm = native.default_params(do_mol=1, cfl=0.3)
+    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
     d, f = hydro.hydro_umdrv_eb(lo, hi, geom, torch.from_numpy(G).cuda(), g_lo, ebdev, prm,
-                                redist=bool(redist))
+                                redist=bool(redist), dt=dt)
     torch.cuda.synchronize()
     assert_bitwise(d.cpu().numpy(), ref_d, "dsdt")
     for dd in range(3):
@@ -109,11 +113,13 @@ def test_eb_box_conserves_mass_and_energy():
 
 
 @pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
-@pytest.mark.parametrize("kind,redist,mgs,radius", [
-    ("periodic", 1, (0, 0, 0), None), ("periodic", 0, (0, 0, 0), None),
-    ("sod", 1, (0, 0, 0), None), ("sod", 1, (8, 8, 8), 0.15), ("sod", 1, (2, 2, 2), 0.25),
-    ("periodic", 1, (8, 8, 4), None)])
-def test_eb_level_steps_match_oracle(kind, redist, mgs, radius):
+@pytest.mark.parametrize("kind,redist,mgs,radius,do_mol", [
+    ("periodic", 1, (0, 0, 0), None, 1), ("periodic", 0, (0, 0, 0), None, 1),
+    ("sod", 1, (0, 0, 0), None, 1), ("sod", 1, (8, 8, 8), 0.15, 1),
+    ("sod", 1, (2, 2, 2), 0.25, 1), ("periodic", 1, (8, 8, 4), None, 1),
+    ("sod", 1, (0, 0, 0), None, 0), ("sod", 1, (8, 8, 8), 0.15, 0),
+    ("periodic", 1, (8, 8, 4), None, 0), ("sod", 0, (2, 2, 2), 0.25, 0)])
+def test_eb_level_steps_match_oracle(kind, redist, mgs, radius, do_mol):
     """camr_eb_level_* steps (dt on the device, graph-captured after the
     first step) against the EB oracle's level driver: states and dts.  With
     a box decomposition, regular boxes run the batched regular hydro and cut
@@ -121,7 +127,7 @@ def test_eb_level_steps_match_oracle(kind, redist, mgs, radius):
     _torch()
     from test_oracle_eb import eb_level_case
     n = (16, 16, 16) if kind == "periodic" else (32, 16, 16)
-    p, lev, geo, s = eb_level_case(kind, n=n, radius=radius, max_grid_size=mgs)
+    p, lev, geo, s = eb_level_case(kind, n=n, radius=radius, max_grid_size=mgs, do_mol=do_mol)
     if not redist:
         p.fixed_dt = 1e-4
     ref = s.copy()
@@ -133,7 +139,7 @@ def test_eb_level_steps_match_oracle(kind, redist, mgs, radius):
     else:
         geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
                                dx=(2.0 / n[0],) * 3)
-    prm = native.default_params(do_mol=1, cfl=0.3, fixed_dt=p.fixed_dt)
+    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, fixed_dt=p.fixed_dt)
     L = hydro.EBLevel(geom, prm, geo, redist=redist, max_grid_size=mgs)
     L.set_state(s)
     if mgs[0]:

@@ -87,26 +87,30 @@ def test_eb_path_without_cut_cells_matches_regular_path():
         assert rel < 1e-11, (c, rel)
 
 
-def eb_level_case(kind, n=(16, 16, 16), seed=5, radius=None, max_grid_size=(0, 0, 0)):
-    """(params, level, geometry over grow(domain,5), initial state) of the
+def eb_level_case(kind, n=(16, 16, 16), seed=5, radius=None, max_grid_size=(0, 0, 0),
+                  do_mol=1):
+    """(params, level, geometry over grow(domain, ng), initial state) of the
     EB level step: 'periodic' (random smooth flow around a sphere in a
     periodic cube) or 'sod' (Sod + sphere on [0,2]x[0,1]^2, x outflow, y/z
-    slip walls).  max_grid_size chops the domain into boxes (0: one box)."""
+    slip walls).  max_grid_size chops the domain into boxes (0: one box).
+    do_mol = 0: Godunov PLM (ng = 6 ghost cells instead of 5)."""
+    ng = 5 if do_mol else 6
+    glo = (-ng,) * 3
     if kind == "periodic":
         dx = 1.0 / n[0]
-        geo = E.sphere_geometry((-5, -5, -5), tuple(v + 4 for v in n), dx,
+        geo = E.sphere_geometry(glo, tuple(v + ng - 1 for v in n), dx,
                                 radius=radius or 0.2)
         s = P.random_smooth(n, seed=seed, amp=0.1, vel=0.2)
         lev = oracle.make_level(n, dx=(dx,) * 3, max_grid_size=max_grid_size)
     else:
         dx = 2.0 / n[0]
-        geo = E.sphere_geometry((-5, -5, -5), tuple(v + 4 for v in n), dx,
+        geo = E.sphere_geometry(glo, tuple(v + ng - 1 for v in n), dx,
                                 center=(1.0, 0.5, 0.5), radius=radius or 0.15)
         s = P.sod_sphere(n, (dx,) * 3, geo)
         lev = oracle.make_level(n, periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
                                 dx=(dx,) * 3, max_grid_size=max_grid_size)
     E.set_covered(s, geo)
-    p = oracle.default_params(do_mol=1, cfl=0.3)
+    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
     s = np.ascontiguousarray(s)
     oracle.eb_init_finalize(p, lev, s)
     return p, lev, geo, s
@@ -168,12 +172,14 @@ def test_eb_level_sod_sphere_runs_and_holds_the_wall():
 def box_kinds(geo, n, mgs):
     """Counts of covered / all-regular (grow 2) / cut boxes of the chop."""
     typ = geo["flag"] & 3
+    o = -geo["lo"][0]
     out = {"covered": 0, "regular": 0, "cut": 0}
     for k in range(0, n[2], mgs[2]):
         for j in range(0, n[1], mgs[1]):
             for i in range(0, n[0], mgs[0]):
-                b = typ[5 + k:5 + k + mgs[2], 5 + j:5 + j + mgs[1], 5 + i:5 + i + mgs[0]]
-                g = typ[3 + k:7 + k + mgs[2], 3 + j:7 + j + mgs[1], 3 + i:7 + i + mgs[0]]
+                b = typ[o + k:o + k + mgs[2], o + j:o + j + mgs[1], o + i:o + i + mgs[0]]
+                g = typ[o - 2 + k:o + 2 + k + mgs[2], o - 2 + j:o + 2 + j + mgs[1],
+                        o - 2 + i:o + 2 + i + mgs[0]]
                 if np.all(b == 3):
                     out["covered"] += 1
                 elif np.all(g == 0):
@@ -212,3 +218,71 @@ def test_eb_level_box_decomposition(mgs, radius):
     # mass change of both runs
     m0 = (vf * s[P.URHO]).sum()
     assert abs((vf * a[P.URHO]).sum() - (vf * one[P.URHO]).sum()) <= 1e-12 * m0
+
+
+def periodic_case_ng(ng, seed=3, radius=0.2):
+    n = (N, N, N)
+    dx = 1.0 / N
+    geo = E.sphere_geometry((-ng,) * 3, (N + ng - 1,) * 3, dx, radius=radius)
+    s = P.random_smooth(n, seed=seed, amp=0.1, vel=0.2)
+    p = oracle.default_params(do_mol=0, ppm_type=0, cfl=0.3)
+    lev = oracle.make_level(n)
+    oracle.init_finalize("restate", p, lev, s)
+    G = np.pad(s, ((0, 0), (ng, ng), (ng, ng), (ng, ng)), mode="wrap")
+    return p, geo, G, dx
+
+
+@needs_eb
+@pytest.mark.parametrize("redist", [0, 1])
+def test_eb_godunov_box_conserves_mass_and_energy(redist):
+    """Godunov_umeth_eb (CTU-PLM with cut cells) + the EB divergence and
+    redistribution: one evaluation on a periodic domain conserves."""
+    p, geo, G, dx = periodic_case_ng(6)
+    d, _, nass = oracle.hydro_box_eb(p, (0, 0, 0), (N - 1,) * 3, (0, 0, 0), (N - 1,) * 3,
+                                     (0, 0, 0), (0, 0, 0), (1, 1, 1), G, (-6, -6, -6), geo,
+                                     (dx,) * 3, 1e-3, redist=redist)
+    assert nass == 0 and np.isfinite(d).all()
+    vf = geo["vfrac"][6:-6, 6:-6, 6:-6]
+    for c in (P.URHO, P.UEDEN, P.UFS):
+        tot = (vf * d[c]).sum() * dx ** 3
+        ref = (vf * np.abs(d[c])).sum() * dx ** 3
+        assert abs(tot) <= 1e-13 * ref, (c, tot, ref)
+
+
+@needs_eb
+def test_eb_godunov_without_cut_cells_matches_regular_ctu():
+    p, _, G, dx = periodic_case_ng(6, seed=4)
+    geo = E.sphere_geometry((-6, -6, -6), (N + 5,) * 3, dx, center=(9.0, 9.0, 9.0), radius=0.1)
+    assert np.all((geo["flag"] & 3) == 0)
+    d, _, _ = oracle.hydro_box_eb(p, (0, 0, 0), (N - 1,) * 3, (0, 0, 0), (N - 1,) * 3,
+                                  (0, 0, 0), (0, 0, 0), (1, 1, 1), G, (-6, -6, -6), geo,
+                                  (dx,) * 3, 1e-3, redist=1)
+    r, _, _ = oracle.hydro_box("restate", p, [0, 0, 0], [N - 1] * 3, [0, 0, 0], [N - 1] * 3,
+                               [0, 0, 0], [0, 0, 0], G[:, 2:-2, 2:-2, 2:-2], [-4, -4, -4],
+                               (dx,) * 3, 1e-3)
+    for c in (0, 1, 2, 3, 4, 5, 7, 8, 9):
+        rel = np.abs(d[c] - r[c]).max() / max(np.abs(r[c]).max(), 1e-300)
+        assert rel < 1e-11, (c, rel)
+
+
+@needs_eb
+@pytest.mark.parametrize("mgs", [(0, 0, 0), (8, 8, 8)])
+def test_eb_level_godunov_sod_sphere(mgs):
+    """Godunov-PLM EB level steps (6 ghost cells): finite, covered cells
+    zero, the y/z mirror symmetry kept, and the box loop agrees with the
+    one-box run to round-off."""
+    n = (32, 16, 16)
+    p, lev, geo, s = eb_level_case("sod", n=n, max_grid_size=mgs, do_mol=0)
+    a = s.copy()
+    _, hist, nass = oracle.eb_advance(p, lev, geo, a, 6)
+    assert nass == 0 and np.isfinite(a).all() and (hist > 0).all()
+    cov = (geo["flag"][6:-6, 6:-6, 6:-6] & 3) == 3
+    assert np.all(a[:, cov] == 0.0) and np.all(a[P.URHO][~cov] > 0.0)
+    assert np.abs(a[P.URHO] - a[P.URHO][:, ::-1, :]).max() < 1e-12
+    if mgs[0]:
+        _, lev1, _, _ = eb_level_case("sod", n=n, do_mol=0)
+        one = s.copy()
+        oracle.eb_advance(p, lev1, geo, one, 6)
+        for c in (0, 1, 4, 5):
+            rel = np.abs(a[c] - one[c]).max() / np.abs(one[c]).max()
+            assert rel < 1e-10, (c, rel)
