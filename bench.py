@@ -52,6 +52,12 @@ STAGE_BYTES = {
 }
 # Whole-step algorithmic bytes per zone-update (read U^n + write U^n+1).
 STEP_BYTES_PER_ZONE = 160
+# DRAM bytes (read + write) per valid cell of one launch, from an ncu
+# capture of the same kernel on the 128^3 case of this workload (inputs
+# larger than L2; traffic grows with the cell count, so the per-cell figure
+# scales to 256^3): k_flux2 3.344 GB read + 1.037 GB written per launch
+# over 128^3 cells (profiles/ncu_k_flux2_128cube_ctu_ppm.txt).
+STAGE_TRAFFIC_PER_CELL = {"flux2": (3.344e9 + 1.037e9) / 128 ** 3}
 
 
 def measured_peaks():
@@ -272,7 +278,11 @@ def run_camr(args, world, rank, local, pg):
     roofline = {
         "kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
         "frac": achieved / hbm_peak, "peak_source": f"{peak_kind} hbm_gbs",
-        "traffic": None, "algorithmic_bytes_per_cell": STAGE_BYTES[dom][0],
+        "traffic": (STAGE_TRAFFIC_PER_CELL[dom] * zones if dom in STAGE_TRAFFIC_PER_CELL
+                    else None),
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell of a "
+                          "128^3 capture, times the cells of one launch",
+        "algorithmic_bytes_per_cell": STAGE_BYTES[dom][0],
         "avg_launch_ms": acc[dom],
         "fp64_peak_tflops_measured": fp64_peak.value,
     }
