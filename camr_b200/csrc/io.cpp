@@ -1,0 +1,305 @@
+// AMReX plotfile output and input of one level (host code).
+//
+// A plotfile is a directory holding
+//   Header            the plotfile header CAMR::writePlotFile writes
+//                     (Source/Utils/CAMR_io.cpp:408-565): type string,
+//                     variable names, dimension, time, finest level, problem
+//                     box, refinement ratios, domain boxes, level steps, cell
+//                     sizes, coordinate system, boundary width, then per level
+//                     its grid count, time, step, the physical extent of
+//                     every grid and the relative path of its cell data;
+//   Level_0/Cell_H    the MultiFab header (VisMF "version 1" layout: how,
+//                     component and ghost counts, the box list, the data file
+//                     and byte offset of every box, per-box minima and maxima);
+//   Level_0/Cell_D_00000
+//                     every box as one FAB: an ASCII line naming the real
+//                     format (IEEE double, little-endian byte order), the
+//                     box and the component count, then the component planes
+//                     of the box, i fastest (the Array4 layout).
+// Covered cells of an EB level are written as zero (EB_set_covered before
+// VisMF::Write, CAMR_io.cpp:556-558): the caller passes the state as it
+// holds it, and covered cells already hold zero.
+#include <sys/stat.h>
+
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <limits>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "camr_b200.h"
+
+namespace {
+
+thread_local std::string g_io_error;
+
+camr_status io_fail(const std::string& why) {
+  g_io_error = why;
+  return CAMR_ERR_INVALID;
+}
+
+bool make_dir(const std::string& d) {
+  if (mkdir(d.c_str(), 0755) == 0) return true;
+  return errno == EEXIST;
+}
+
+std::string box_text(const int lo[3], const int hi[3]) {
+  std::ostringstream o;
+  o << "((" << lo[0] << ',' << lo[1] << ',' << lo[2] << ") (" << hi[0] << ',' << hi[1] << ','
+    << hi[2] << ") (0,0,0))";
+  return o.str();
+}
+
+// Default names of the state components (Source/Utils/CAMR_setup.cpp:159-198).
+const char* const kStateNames[CAMR_NVAR] = {"density", "xmom",  "ymom", "zmom",  "rho_E",
+                                            "rho_e",   "Temp",  "rho_F", "rho_A", "rho_P"};
+
+// The FAB real-format line of little-endian IEEE doubles.
+const char* const kFabFormat = "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (8 7 6 5 4 3 2 1)))";
+
+bool host_little_endian() {
+  const uint16_t one = 1;
+  unsigned char b;
+  std::memcpy(&b, &one, 1);
+  return b == 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* camr_io_last_error(void) { return g_io_error.c_str(); }
+
+camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                double time, int level_step, int nbox, const int* boxes,
+                                const double* state, int ncomp, const int* comps,
+                                const char* const* names) {
+  g_io_error.clear();
+  if (!dir || !geom || !prob_hi || nbox <= 0 || !boxes || !state || ncomp <= 0)
+    return io_fail("invalid arguments");
+  if (!host_little_endian()) return io_fail("big-endian hosts are not supported");
+  int n[3];
+  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
+  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
+  std::vector<int> cmap(ncomp);
+  std::vector<std::string> vnames(ncomp);
+  for (int c = 0; c < ncomp; ++c) {
+    cmap[c] = comps ? comps[c] : c;
+    if (cmap[c] < 0 || cmap[c] >= CAMR_NVAR) return io_fail("component out of range");
+    vnames[c] = (names && names[c]) ? names[c] : kStateNames[cmap[c]];
+  }
+  for (int b = 0; b < nbox; ++b)
+    for (int d = 0; d < 3; ++d) {
+      const int lo = boxes[6 * b + d], hi = boxes[6 * b + 3 + d];
+      if (lo < geom->dom_lo[d] || hi > geom->dom_hi[d] || hi < lo)
+        return io_fail("box outside the domain");
+    }
+  const std::string root(dir);
+  const std::string lev = root + "/Level_0";
+  if (!make_dir(root) || !make_dir(lev)) return io_fail("cannot create " + lev);
+
+  // Level_0/Cell_D_00000 and the per-box offsets, minima and maxima.
+  std::vector<int64_t> offs(nbox);
+  std::vector<double> mins(size_t(nbox) * ncomp), maxs(size_t(nbox) * ncomp);
+  {
+    std::FILE* f = std::fopen((lev + "/Cell_D_00000").c_str(), "wb");
+    if (!f) return io_fail("cannot write " + lev + "/Cell_D_00000");
+    std::vector<double> buf;
+    int64_t pos = 0;
+    for (int b = 0; b < nbox; ++b) {
+      const int* lo = boxes + 6 * b;
+      const int* hi = boxes + 6 * b + 3;
+      const int bn[3] = {hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1};
+      const int64_t bc = int64_t(bn[0]) * bn[1] * bn[2];
+      offs[b] = pos;
+      std::ostringstream h;
+      h << kFabFormat << box_text(lo, hi) << ' ' << ncomp << '\n';
+      const std::string hs = h.str();
+      std::fwrite(hs.data(), 1, hs.size(), f);
+      pos += int64_t(hs.size());
+      buf.resize(size_t(bc));
+      for (int c = 0; c < ncomp; ++c) {
+        const double* src = state + int64_t(cmap[c]) * ncell;
+        double mn = std::numeric_limits<double>::max();
+        double mx = std::numeric_limits<double>::lowest();
+        int64_t t = 0;
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j) {
+            const double* row = src + (int64_t(k - geom->dom_lo[2]) * n[1] +
+                                       (j - geom->dom_lo[1])) * n[0] - geom->dom_lo[0];
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+              const double v = row[i];
+              buf[size_t(t++)] = v;
+              mn = v < mn ? v : mn;
+              mx = v > mx ? v : mx;
+            }
+          }
+        mins[size_t(b) * ncomp + c] = mn;
+        maxs[size_t(b) * ncomp + c] = mx;
+        std::fwrite(buf.data(), sizeof(double), size_t(bc), f);
+        pos += bc * int64_t(sizeof(double));
+      }
+    }
+    if (std::fclose(f) != 0) return io_fail("write failed: " + lev + "/Cell_D_00000");
+  }
+  // Level_0/Cell_H
+  {
+    std::ofstream h(lev + "/Cell_H");
+    if (!h) return io_fail("cannot write " + lev + "/Cell_H");
+    h << 1 << '\n' << 1 << '\n' << ncomp << '\n' << 0 << '\n';
+    h << '(' << nbox << " 0\n";
+    for (int b = 0; b < nbox; ++b) h << box_text(boxes + 6 * b, boxes + 6 * b + 3) << '\n';
+    h << ")\n" << nbox << '\n';
+    for (int b = 0; b < nbox; ++b) h << "FabOnDisk: Cell_D_00000 " << offs[b] << '\n';
+    h << '\n' << nbox << ',' << ncomp << '\n';
+    h << std::setprecision(17);
+    for (int b = 0; b < nbox; ++b) {
+      for (int c = 0; c < ncomp; ++c) h << mins[size_t(b) * ncomp + c] << ',';
+      h << '\n';
+    }
+    h << '\n' << nbox << ',' << ncomp << '\n';
+    for (int b = 0; b < nbox; ++b) {
+      for (int c = 0; c < ncomp; ++c) h << maxs[size_t(b) * ncomp + c] << ',';
+      h << '\n';
+    }
+    if (!h) return io_fail("write failed: " + lev + "/Cell_H");
+  }
+  // Header
+  {
+    std::ofstream h(root + "/Header");
+    if (!h) return io_fail("cannot write " + root + "/Header");
+    h << std::setprecision(17);
+    h << "HyperCLaw-V1.1\n" << ncomp << '\n';
+    for (const auto& v : vnames) h << v << '\n';
+    h << 3 << '\n' << time << '\n' << 0 << '\n';
+    for (int d = 0; d < 3; ++d) h << geom->prob_lo[d] << ' ';
+    h << '\n';
+    for (int d = 0; d < 3; ++d) h << prob_hi[d] << ' ';
+    h << '\n' << '\n';
+    h << box_text(geom->dom_lo, geom->dom_hi) << ' ' << '\n';
+    h << level_step << ' ' << '\n';
+    for (int d = 0; d < 3; ++d) h << geom->dx[d] << ' ';
+    h << '\n' << 0 << '\n' << "0\n";
+    h << 0 << ' ' << nbox << ' ' << time << '\n' << level_step << '\n';
+    for (int b = 0; b < nbox; ++b)
+      for (int d = 0; d < 3; ++d) {
+        const double lo = geom->prob_lo[d] + boxes[6 * b + d] * geom->dx[d];
+        const double hi = geom->prob_lo[d] + (boxes[6 * b + 3 + d] + 1) * geom->dx[d];
+        h << lo << ' ' << hi << '\n';
+      }
+    h << "Level_0/Cell\n";
+    if (!h) return io_fail("write failed: " + root + "/Header");
+  }
+  return CAMR_OK;
+}
+
+camr_status camr_read_plotfile(const char* dir, const camr_geom* geom, int ncomp,
+                               double* state, double* time, int* level_step) {
+  g_io_error.clear();
+  if (!dir || !geom || ncomp <= 0 || !state) return io_fail("invalid arguments");
+  const std::string root(dir);
+  int n[3];
+  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
+  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
+  {
+    std::ifstream h(root + "/Header");
+    if (!h) return io_fail("cannot read " + root + "/Header");
+    std::string type;
+    int nv = 0;
+    h >> type >> nv;
+    if (type != "HyperCLaw-V1.1" || nv != ncomp) return io_fail("unexpected plotfile header");
+    std::string name;
+    for (int c = 0; c < nv; ++c) h >> name;
+    int dim = 0, finest = 0;
+    double t = 0.0;
+    h >> dim >> t >> finest;
+    if (dim != 3 || finest != 0) return io_fail("only single-level 3-D plotfiles are read");
+    if (time) *time = t;
+    double v;
+    for (int d = 0; d < 6; ++d) h >> v;  // problem box
+    std::string dom;
+    h >> dom >> dom >> dom;               // "((lo) (hi) (type))" as three tokens
+    int step = 0;
+    h >> step;
+    if (level_step) *level_step = step;
+  }
+  std::ifstream ch(root + "/Level_0/Cell_H");
+  if (!ch) return io_fail("cannot read Level_0/Cell_H");
+  int version = 0, how = 0, nc = 0, ngrow = 0;
+  ch >> version >> how >> nc >> ngrow;
+  if (nc != ncomp || ngrow != 0) return io_fail("unexpected Cell_H");
+  char paren;
+  int nbox = 0, zero = 0;
+  ch >> paren >> nbox >> zero;
+  std::vector<int> bx(size_t(nbox) * 6);
+  for (int b = 0; b < nbox; ++b) {
+    std::string tok;
+    ch >> tok;  // "((lo0,lo1,lo2)"
+    int lo[3], hi[3], ty[3];
+    if (std::sscanf(tok.c_str(), "((%d,%d,%d)", &lo[0], &lo[1], &lo[2]) != 3)
+      return io_fail("bad box in Cell_H");
+    ch >> tok;
+    if (std::sscanf(tok.c_str(), "(%d,%d,%d)", &hi[0], &hi[1], &hi[2]) != 3)
+      return io_fail("bad box in Cell_H");
+    ch >> tok;
+    if (std::sscanf(tok.c_str(), "(%d,%d,%d))", &ty[0], &ty[1], &ty[2]) != 3)
+      return io_fail("bad box in Cell_H");
+    for (int d = 0; d < 3; ++d) {
+      bx[6 * b + d] = lo[d];
+      bx[6 * b + 3 + d] = hi[d];
+      if (lo[d] < geom->dom_lo[d] || hi[d] > geom->dom_hi[d]) return io_fail("box outside domain");
+    }
+  }
+  ch >> paren;
+  int nfab = 0;
+  ch >> nfab;
+  if (nfab != nbox) return io_fail("unexpected FabOnDisk count");
+  std::vector<std::string> files(nbox);
+  std::vector<int64_t> offs(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    std::string tag;
+    ch >> tag >> files[b] >> offs[b];
+    if (tag != "FabOnDisk:") return io_fail("bad FabOnDisk line");
+  }
+  std::vector<double> buf;
+  for (int b = 0; b < nbox; ++b) {
+    std::FILE* f = std::fopen((root + "/Level_0/" + files[b]).c_str(), "rb");
+    if (!f) return io_fail("cannot read " + files[b]);
+    if (std::fseek(f, long(offs[b]), SEEK_SET) != 0) {
+      std::fclose(f);
+      return io_fail("seek failed");
+    }
+    char line[512];
+    if (!std::fgets(line, sizeof line, f) || std::strncmp(line, kFabFormat, std::strlen(kFabFormat))) {
+      std::fclose(f);
+      return io_fail("unexpected FAB header");
+    }
+    const int* lo = &bx[6 * b];
+    const int* hi = &bx[6 * b + 3];
+    const int64_t bc = int64_t(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    buf.resize(size_t(bc));
+    for (int c = 0; c < ncomp; ++c) {
+      if (std::fread(buf.data(), sizeof(double), size_t(bc), f) != size_t(bc)) {
+        std::fclose(f);
+        return io_fail("short FAB data");
+      }
+      double* dst = state + int64_t(c) * ncell;
+      int64_t t = 0;
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j) {
+          double* row = dst + (int64_t(k - geom->dom_lo[2]) * n[1] + (j - geom->dom_lo[1])) * n[0] -
+                        geom->dom_lo[0];
+          for (int i = lo[0]; i <= hi[0]; ++i) row[i] = buf[size_t(t++)];
+        }
+    }
+    std::fclose(f);
+  }
+  return CAMR_OK;
+}
+
+}  // extern "C"

@@ -489,3 +489,54 @@ class AmrHierarchy:
 
     def sync(self):
         _torch().cuda.synchronize()
+
+
+def level_boxes(n, max_grid_size, dom_lo=(0, 0, 0)):
+    """The domain chopped by max_grid_size from the low end (0 = one box),
+    as a list of (lo, hi) tuples in i-fastest order."""
+    step = [max_grid_size[d] if max_grid_size[d] > 0 else n[d] for d in range(3)]
+    out = []
+    for k in range(dom_lo[2], dom_lo[2] + n[2], step[2]):
+        for j in range(dom_lo[1], dom_lo[1] + n[1], step[1]):
+            for i in range(dom_lo[0], dom_lo[0] + n[0], step[0]):
+                lo = (i, j, k)
+                hi = tuple(min(lo[d] + step[d] - 1, dom_lo[d] + n[d] - 1) for d in range(3))
+                out.append((lo, hi))
+    return out
+
+
+def write_plotfile(path, state, geom, prob_hi, time=0.0, level_step=0,
+                   max_grid_size=(32, 32, 32), comps=None, names=None):
+    """Write one level's state (numpy (NVAR, nz, ny, nx), valid cells) as an
+    AMReX plotfile directory (camr_write_plotfile)."""
+    n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+    a = np.ascontiguousarray(state, dtype=np.float64)
+    assert a.shape == (NVAR, n[2], n[1], n[0])
+    boxes = level_boxes(n, max_grid_size, tuple(geom.dom_lo))
+    flat = np.array([list(lo) + list(hi) for lo, hi in boxes], dtype=np.int32).ravel()
+    comps = list(range(NVAR)) if comps is None else list(comps)
+    carr = np.array(comps, dtype=np.int32)
+    nm = None
+    if names is not None:
+        nm = (C.c_char_p * len(names))(*[x.encode() for x in names])
+    ph = (C.c_double * 3)(*prob_hi)
+    st = lib().camr_write_plotfile(str(path).encode(), C.byref(geom), C.byref(ph), float(time),
+                                   int(level_step), len(boxes), flat.ctypes.data, a.ctypes.data,
+                                   len(comps), carr.ctypes.data, nm)
+    if st != 0:
+        raise native.CamrError(st, "camr_write_plotfile " +
+                               lib().camr_io_last_error().decode())
+
+
+def read_plotfile(path, geom, ncomp=NVAR):
+    """Read a single-level plotfile written by write_plotfile: returns
+    (state planes (ncomp, nz, ny, nx), time, level_step)."""
+    n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+    out = np.zeros((ncomp, n[2], n[1], n[0]))
+    t = C.c_double()
+    stp = C.c_int()
+    st = lib().camr_read_plotfile(str(path).encode(), C.byref(geom), int(ncomp),
+                                  out.ctypes.data, C.byref(t), C.byref(stp))
+    if st != 0:
+        raise native.CamrError(st, "camr_read_plotfile " + lib().camr_io_last_error().decode())
+    return out, t.value, stp.value

@@ -145,6 +145,12 @@ SIGNATURES = {
     "camr_eb_level_kernels_per_step": (C.c_int64, [C.c_void_p]),
     "camr_eb_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_eb_level_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
+    "camr_write_plotfile": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.POINTER(C.c_double * 3),
+                                      C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_int, C.c_void_p, C.c_void_p]),
+    "camr_read_plotfile": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.c_int, C.c_void_p,
+                                     C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "camr_io_last_error": (C.c_char_p, []),
     "camr_adjoint_create": (C.c_int, [C.POINTER(Geom), C.POINTER(HydroParams), C.c_int,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_adjoint_destroy": (C.c_int, [C.c_void_p]),

@@ -416,6 +416,28 @@ camr_status camr_eb_level_stream(camr_eb_level* lev, void** stream);
 camr_status camr_eb_level_get_error(camr_eb_level* lev, camr_error_info* info);
 
 /* ---------------------------------------------------------------------
+ * Plotfile output / input of one level (host memory), in AMReX's plotfile
+ * layout as CAMR::writePlotFile writes it (Source/Utils/CAMR_io.cpp:408-565):
+ * dir/Header, dir/Level_0/Cell_H (VisMF header), dir/Level_0/Cell_D_00000
+ * (one FAB per box, little-endian IEEE doubles).  state: NVAR comps on the
+ * domain's valid cells, shape (NVAR, nz, ny, nx), i fastest.  boxes: nbox
+ * boxes as lo0,lo1,lo2,hi0,hi1,hi2 (the level's grids).  comps (may be
+ * NULL = 0..ncomp-1) selects the state components written and names (may
+ * be NULL) their plot names (default: the reference's state names,
+ * Source/Utils/CAMR_setup.cpp:159-198).  geom supplies the domain, dx and
+ * prob_lo.  camr_read_plotfile reads the ncomp written components back into
+ * the first ncomp planes of state (single-level plotfiles).
+ */
+camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                double time, int level_step, int nbox, const int* boxes,
+                                const double* state, int ncomp, const int* comps,
+                                const char* const* names);
+camr_status camr_read_plotfile(const char* dir, const camr_geom* geom, int ncomp,
+                               double* state, double* time, int* level_step);
+/* Why the last plotfile call on this thread failed ("" if it did not). */
+const char* camr_io_last_error(void);
+
+/* ---------------------------------------------------------------------
  * Allocation-free per-box hydro.  No counterpart in the reference: it is
  * camr_hydro_umdrv for callers that may not allocate device memory while
  * they run (code inside an arena or pool that owns all device memory,

@@ -1,0 +1,146 @@
+"""Plotfile output (camr_write_plotfile, AMReX plotfile layout as
+CAMR::writePlotFile writes it, Source/Utils/CAMR_io.cpp:408-565) and input.
+
+* write -> read returns the state bit for bit, for several box chops;
+* an independent parse of the files (this test's own reader of the AMReX
+  layout: Header fields, the VisMF Cell_H box list / offsets / min / max,
+  the FAB headers and the raw little-endian data) finds the same values;
+* a level's state after GPU steps round-trips too (GPU).
+"""
+import re
+
+import numpy as np
+import pytest
+
+from camr_b200 import hydro, native
+from camr_b200 import problems as P
+
+NAMES = ["density", "xmom", "ymom", "zmom", "rho_E", "rho_e", "Temp", "rho_F", "rho_A",
+         "rho_P"]
+
+
+def independent_read(path):
+    """Parse a single-level plotfile without the library."""
+    hdr = (path / "Header").read_text().split("\n")
+    assert hdr[0] == "HyperCLaw-V1.1"
+    nv = int(hdr[1])
+    names = hdr[2:2 + nv]
+    i = 2 + nv
+    assert int(hdr[i]) == 3
+    time = float(hdr[i + 1])
+    assert int(hdr[i + 2]) == 0
+    prob_lo = [float(x) for x in hdr[i + 3].split()]
+    prob_hi = [float(x) for x in hdr[i + 4].split()]
+    assert hdr[i + 5].strip() == ""
+    dom = [int(x) for x in re.findall(r"-?\d+", hdr[i + 6])]
+    step = int(hdr[i + 7].split()[0])
+    dx = [float(x) for x in hdr[i + 8].split()]
+    assert hdr[i + 9].strip() == "0" and hdr[i + 10].strip() == "0"
+    lev, ngrid, t2 = hdr[i + 11].split()
+    assert int(lev) == 0 and float(t2) == time
+    ngrid = int(ngrid)
+    assert int(hdr[i + 12]) == step
+    ext = [[float(v) for v in hdr[i + 13 + g].split()] for g in range(3 * ngrid)]
+    assert hdr[i + 13 + 3 * ngrid] == "Level_0/Cell"
+    cell_h = (path / "Level_0" / "Cell_H").read_text().split("\n")
+    assert cell_h[0] == "1" and cell_h[1] == "1" and int(cell_h[2]) == nv and cell_h[3] == "0"
+    nb = int(cell_h[4].strip("(").split()[0])
+    assert nb == ngrid
+    boxes = [[int(x) for x in re.findall(r"-?\d+", cell_h[5 + b])] for b in range(nb)]
+    assert cell_h[5 + nb] == ")" and int(cell_h[6 + nb]) == nb
+    fabs = [cell_h[7 + nb + b].split() for b in range(nb)]
+    data = (path / "Level_0" / "Cell_D_00000").read_bytes()
+    n = [dom[3 + d] - dom[d] + 1 for d in range(3)]
+    out = np.zeros((nv, n[2], n[1], n[0]))
+    mins = [[float(v) for v in cell_h[9 + 2 * nb + b].rstrip(",").split(",")] for b in range(nb)]
+    for b, (tag, fname, off) in enumerate(fabs):
+        assert tag == "FabOnDisk:" and fname == "Cell_D_00000"
+        off = int(off)
+        end = data.index(b"\n", off)
+        line = data[off:end].decode()
+        assert line.startswith("FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (8 7 6 5 4 3 2 1)))")
+        lo, hi = boxes[b][:3], boxes[b][3:6]
+        assert line.endswith(f" {nv}")
+        bn = [hi[d] - lo[d] + 1 for d in range(3)]
+        cnt = bn[0] * bn[1] * bn[2]
+        vals = np.frombuffer(data, dtype="<f8", count=cnt * nv, offset=end + 1)
+        vals = vals.reshape(nv, bn[2], bn[1], bn[0])
+        out[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = vals
+        for c in range(nv):
+            assert mins[b][c] == vals[c].min()
+        # the extents in Header are the physical bounds of the box
+        for d in range(3):
+            elo, ehi = ext[3 * b + d]
+            assert abs(elo - (prob_lo[d] + lo[d] * dx[d])) < 1e-12
+            assert abs(ehi - (prob_lo[d] + (hi[d] + 1) * dx[d])) < 1e-12
+    return {"names": names, "time": time, "step": step, "dom": dom, "dx": dx,
+            "prob_hi": prob_hi, "state": out, "nboxes": nb}
+
+
+@pytest.mark.parametrize("mgs", [(0, 0, 0), (8, 8, 8), (16, 8, 4)])
+def test_plotfile_round_trip(tmp_path, native_lib, mgs):
+    n = (24, 16, 16)
+    dx = (1.0 / 24, 1.0 / 16, 1.0 / 16)
+    s = P.random_smooth(n, seed=11)
+    s[P.UTEMP] = np.linspace(300, 400, s[0].size).reshape(s[0].shape)
+    geom = hydro.make_geom(n, dx=dx)
+    path = tmp_path / "plt00007"
+    hydro.write_plotfile(path, s, geom, (1.0, 1.0, 1.0), time=0.125, level_step=7,
+                         max_grid_size=mgs)
+    back, t, step = hydro.read_plotfile(path, geom)
+    assert t == 0.125 and step == 7
+    assert np.array_equal(back, s)
+    ind = independent_read(path)
+    assert ind["names"] == NAMES and ind["step"] == 7 and ind["time"] == 0.125
+    assert ind["dom"][:6] == [0, 0, 0, 23, 15, 15]
+    assert np.array_equal(ind["state"], s)
+    assert ind["nboxes"] == len(hydro.level_boxes(n, mgs))
+
+
+def test_plotfile_component_subset(tmp_path, native_lib):
+    n = (8, 8, 8)
+    s = P.random_smooth(n, seed=2)
+    geom = hydro.make_geom(n)
+    path = tmp_path / "plt_sub"
+    hydro.write_plotfile(path, s, geom, (1.0, 1.0, 1.0), comps=[0, 6], names=["rho", "T"])
+    ind = independent_read(path)
+    assert ind["names"] == ["rho", "T"]
+    assert np.array_equal(ind["state"][0], s[0]) and np.array_equal(ind["state"][1], s[6])
+    back, _, _ = hydro.read_plotfile(path, geom, ncomp=2)
+    assert np.array_equal(back[1], s[6])
+
+
+def test_plotfile_rejects_bad_input(tmp_path, native_lib):
+    geom = hydro.make_geom((8, 8, 8))
+    with pytest.raises(native.CamrError):
+        hydro.write_plotfile(tmp_path / "x", np.zeros((10, 8, 8, 8)), geom, (1, 1, 1),
+                             comps=[12])
+    with pytest.raises(native.CamrError):
+        hydro.read_plotfile(tmp_path / "missing", geom)
+
+
+@pytest.mark.gpu
+def test_level_state_plotfile_restart(tmp_path):
+    """A level's state written after GPU steps, read back and set into a new
+    level, continues exactly as the original (restart from a plotfile that
+    holds every state component)."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    n = (32, 32, 32)
+    s0 = P.blobs(n, tuple(1.0 / v for v in n), nblobs=3, seed=5)
+    geom = hydro.make_geom(n)
+    prm = native.default_params(ppm_type=1, cfl=0.7, fixed_dt=1e-3)
+    a = hydro.Level(geom, prm)
+    a.set_state(s0)
+    a.init_finalize()
+    a.advance(3)
+    mid = a.get_state()
+    hydro.write_plotfile(tmp_path / "chk", mid, geom, (1, 1, 1), time=3e-3, level_step=3)
+    back, t, step = hydro.read_plotfile(tmp_path / "chk", geom)
+    assert np.array_equal(back, mid) and step == 3
+    a.advance(2)
+    b = hydro.Level(geom, prm)
+    b.set_state(back)
+    b.advance(2)
+    assert np.array_equal(a.get_state(), b.get_state())
