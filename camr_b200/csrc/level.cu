@@ -55,10 +55,18 @@ struct camr_level {
   int steps_taken;
   bool graph_ready;
   cudaGraphExec_t graph;
-  double* staging;     // packed (NVAR x ncell) device buffer for state I/O
+  double* staging;     // packed (NVAR x ncell) device buffer for state input
+  double* staging_out; // packed device buffer for state output
   double* fixed_dev;   // device copy of one fixed dt
   bool own_stream;     // the library created `stream` (caller passed NULL)
   int64_t kernels_per_step;  // launches inside one captured step
+  // Host transfers run on their own streams so that the next state upload
+  // and the last state download overlap the level's kernels: the upload of
+  // step k+1 waits only until the unpack of step k has read `staging`, the
+  // download of step k only for its own pack, and the next pack into
+  // `staging_out` for the previous download.
+  cudaStream_t up = nullptr, down = nullptr;
+  cudaEvent_t in_free = nullptr, in_ready = nullptr, out_ready = nullptr, out_free = nullptr;
 };
 
 namespace {
@@ -246,6 +254,11 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   alloc(reinterpret_cast<void**>(&S.nstep), sizeof(int));
   alloc(reinterpret_cast<void**>(&S.err), sizeof(DevError));
   alloc(reinterpret_cast<void**>(&lev->staging), size_t(lev->ncell) * NVAR * sizeof(double));
+  alloc(reinterpret_cast<void**>(&lev->staging_out), size_t(lev->ncell) * NVAR * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&lev->up, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&lev->down, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&lev->in_free, &lev->in_ready, &lev->out_ready, &lev->out_free})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   alloc(reinterpret_cast<void**>(&lev->fixed_dev), sizeof(double));
   if (e != cudaSuccess) {
     camr_level_destroy(lev);
@@ -266,10 +279,18 @@ camr_status camr_level_destroy(camr_level* lev) {
   if (!lev) return CAMR_ERR_INVALID;
   LevelState& S = lev->st;
   if (lev->graph_ready) cudaGraphExecDestroy(lev->graph);
-  void* ptrs[] = {S.S, S.S_old, S.B, S.B2, S.flx[0], S.flx[1], S.flx[2], S.work, S.dt_cur,
-                  S.dt_hist, S.dtmin_bits, S.nstep, S.err, lev->staging, lev->fixed_dev};
+  if (lev->up) cudaStreamSynchronize(lev->up);
+  if (lev->down) cudaStreamSynchronize(lev->down);
+  void* ptrs[] = {S.S,        S.S_old,  S.B,        S.B2,         S.flx[0],
+                  S.flx[1],   S.flx[2], S.work,     S.dt_cur,     S.dt_hist,
+                  S.dtmin_bits, S.nstep, S.err,     lev->staging, lev->staging_out,
+                  lev->fixed_dev};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (cudaEvent_t ev : {lev->in_free, lev->in_ready, lev->out_ready, lev->out_free})
+    if (ev) cudaEventDestroy(ev);
+  if (lev->up) cudaStreamDestroy(lev->up);
+  if (lev->down) cudaStreamDestroy(lev->down);
   if (lev->own_stream) cudaStreamDestroy(lev->stream);
   delete lev;
   return CAMR_OK;
@@ -278,26 +299,65 @@ camr_status camr_level_destroy(camr_level* lev) {
 camr_status camr_level_set_state(camr_level* lev, const double* state, int host) {
   if (!lev || !state) return CAMR_ERR_INVALID;
   const size_t bytes = size_t(lev->ncell) * NVAR * sizeof(double);
-  cudaError_t e = cudaMemcpyAsync(lev->staging, state, bytes,
-                                  host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
-                                  lev->stream);
-  if (e != cudaSuccess) return CAMR_ERR_CUDA;
+  cudaError_t e;
+  if (host) {
+    // upload on the copy stream once the previous unpack has read staging
+    e = cudaStreamWaitEvent(lev->up, lev->in_free, 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(lev->staging, state, bytes, cudaMemcpyHostToDevice, lev->up);
+    if (e == cudaSuccess) e = cudaEventRecord(lev->in_ready, lev->up);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(lev->stream, lev->in_ready, 0);
+  } else {
+    e = cudaMemcpyAsync(lev->staging, state, bytes, cudaMemcpyDeviceToDevice, lev->stream);
+  }
+  if (e != cudaSuccess) return cuda_status(e);
   k_pack<<<grid_of(lev->ncell), kBlk, 0, lev->stream>>>(lev->L, lev->st.S, lev->staging, 0);
   count_launch();
+  e = cudaEventRecord(lev->in_free, lev->stream);
   lev->steps_taken = 0;
+  if (e != cudaSuccess) return cuda_status(e);
+  return cuda_status(cudaGetLastError());
+}
+
+// Pack the state and start its copy to `state`; host copies run on the
+// download stream and complete by the next camr_level_sync (or any call
+// that synchronises the level).
+static camr_status get_state_issue(camr_level* lev, double* state, int host) {
+  cudaError_t e = cudaStreamWaitEvent(lev->stream, lev->out_free, 0);
+  if (e != cudaSuccess) return cuda_status(e);
+  k_pack<<<grid_of(lev->ncell), kBlk, 0, lev->stream>>>(lev->L, lev->st.S, lev->staging_out, 1);
+  count_launch();
+  const size_t bytes = size_t(lev->ncell) * NVAR * sizeof(double);
+  if (host) {
+    e = cudaEventRecord(lev->out_ready, lev->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(lev->down, lev->out_ready, 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(state, lev->staging_out, bytes, cudaMemcpyDeviceToHost, lev->down);
+    if (e == cudaSuccess) e = cudaEventRecord(lev->out_free, lev->down);
+  } else {
+    e = cudaMemcpyAsync(state, lev->staging_out, bytes, cudaMemcpyDeviceToDevice, lev->stream);
+  }
+  if (e != cudaSuccess) return cuda_status(e);
   return cuda_status(cudaGetLastError());
 }
 
 camr_status camr_level_get_state(camr_level* lev, double* state, int host) {
   if (!lev || !state) return CAMR_ERR_INVALID;
-  k_pack<<<grid_of(lev->ncell), kBlk, 0, lev->stream>>>(lev->L, lev->st.S, lev->staging, 1);
-  count_launch();
-  const size_t bytes = size_t(lev->ncell) * NVAR * sizeof(double);
-  cudaError_t e = cudaMemcpyAsync(state, lev->staging, bytes,
-                                  host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
-                                  lev->stream);
-  if (e != cudaSuccess) return CAMR_ERR_CUDA;
-  if (host) e = cudaStreamSynchronize(lev->stream);
+  camr_status cs = get_state_issue(lev, state, host);
+  if (cs != CAMR_OK) return cs;
+  return cuda_status(cudaStreamSynchronize(host ? lev->down : lev->stream));
+}
+
+camr_status camr_level_get_state_async(camr_level* lev, double* state, int host) {
+  if (!lev || !state) return CAMR_ERR_INVALID;
+  return get_state_issue(lev, state, host);
+}
+
+camr_status camr_level_sync(camr_level* lev) {
+  if (!lev) return CAMR_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(lev->up);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->down);
   return cuda_status(e);
 }
 

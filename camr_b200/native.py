@@ -94,6 +94,8 @@ SIGNATURES = {
                                           C.POINTER(C.c_char_p), C.c_int,
                                           C.POINTER(C.c_int)]),
     "camr_level_kernels_per_step": (C.c_int64, [C.c_void_p]),
+    "camr_level_get_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "camr_level_sync": (C.c_int, [C.c_void_p]),
     "camr_measure_fp64_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
     "camr_hydro_umdrv_noalloc": (C.c_int, [C.POINTER(C.c_int * 3), C.POINTER(C.c_int * 3),
                                            C.POINTER(Geom), C.POINTER(Fab), C.POINTER(Fab),

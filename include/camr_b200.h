@@ -218,6 +218,13 @@ camr_status camr_level_destroy(camr_level* lev);
  * the pointer is host memory (pinned for async); otherwise device memory. */
 camr_status camr_level_set_state(camr_level* lev, const double* state, int host);
 camr_status camr_level_get_state(camr_level* lev, double* state, int host);
+/* Host transfers run on copy streams of their own: set_state(host) returns
+ * once the upload is queued (the host buffer must stay unchanged until the
+ * next camr_level_sync), and camr_level_get_state_async queues the download
+ * without waiting for it.  Both overlap the level's kernels of neighbouring
+ * steps.  camr_level_sync waits for all of the level's work and copies. */
+camr_status camr_level_get_state_async(camr_level* lev, double* state, int host);
+camr_status camr_level_sync(camr_level* lev);
 
 /* CAMR::initData's epilogue: enforce_consistent_e then computeTemp. */
 camr_status camr_level_init_finalize(camr_level* lev);
