@@ -49,6 +49,7 @@ struct KParams {
   int ppm_type, plm_iorder, use_pslope, use_flattening, transverse_reset_density;
   int dual_energy_update_E_from_e, allow_negative_energy, allow_small_energy;
   int add_grav_src;
+  int riemann_solver;  // 0 riemannus (the reference), 1 HLLC
   double difmag, small, small_dens, small_temp, small_pres, smallu, small_num;
   double dual_energy_eta1, dual_energy_eta2, const_grav, gamma;
 };
@@ -64,6 +65,7 @@ inline KParams make_kparams(const camr_hydro_params& p) {
   k.allow_negative_energy = p.allow_negative_energy;
   k.allow_small_energy = p.allow_small_energy;
   k.add_grav_src = p.add_grav_src;
+  k.riemann_solver = p.riemann_solver;
   k.difmag = p.difmag;
   k.small = p.small;
   k.small_dens = p.small_dens;

@@ -115,6 +115,73 @@ __device__ __forceinline__ ROut riemannus(double rl_in, double ul, double vl, do
   return o;
 }
 
+// HLLC approximate Riemann solver (riemann_solver = 1; not in the
+// reference, which has only riemannus).  Toro, "Riemann Solvers and
+// Numerical Methods for Fluid Dynamics", 3rd ed., sec. 10.4-10.6: Davis
+// wave-speed estimates S_L = min(u_L - c_L, u_R - c_R), S_R = max(u_L + c_L,
+// u_R + c_R); contact speed S* from the two star-momentum balances; the flux
+// of the region containing x/t = 0 (F_L, F_L + S_L (U*_L - U_L),
+// F_R + S_R (U*_R - U_R), F_R).  rho e travels like a passive density.
+// Returned interface values: the normal velocity and pressure of that region
+// (S*, p* = p_L + rho_L (S_L - u_L)(S* - u_L) in the star regions).
+__device__ __forceinline__ ROut hllc(double rl_in, double ul, double vl, double v2l,
+                                     double pl_in, double rel, double rr_in, double ur,
+                                     double vr, double v2r, double pr_in, double rer,
+                                     double gamcl, double gamcr, double smallc,
+                                     double small_dens, double small_pres) {
+  ROut o;
+  const double rl = dmax(rl_in, small_dens);
+  const double pl = dmax(pl_in, small_pres);
+  const double rr = dmax(rr_in, small_dens);
+  const double pr = dmax(pr_in, small_pres);
+  const double cl = dmax(smallc, sqrt(fabs(gamcl * pl / rl)));
+  const double cr = dmax(smallc, sqrt(fabs(gamcr * pr / rr)));
+  const double sl = dmin(ul - cl, ur - cr);
+  const double sr = dmax(ul + cl, ur + cr);
+  const double el = rel + 0.5 * rl * (ul * ul + vl * vl + v2l * v2l);
+  const double er = rer + 0.5 * rr * (ur * ur + vr * vr + v2r * v2r);
+  const double dl = rl * (sl - ul);
+  const double dr = rr * (sr - ur);
+  const double sstar = ((pr - pl) + (ul * dl - ur * dr)) / (dl - dr);
+  const double pstar = pl + dl * (sstar - ul);
+  // the side whose states enter the flux
+  const bool left = sstar >= 0.0;
+  const double rk = left ? rl : rr, uk = left ? ul : ur, vk = left ? vl : vr;
+  const double v2k = left ? v2l : v2r, pk = left ? pl : pr, ek = left ? el : er;
+  const double rek = left ? rel : rer, sk = left ? sl : sr;
+  double f_rho = rk * uk;
+  double f_un = rk * uk * uk + pk;
+  double f_ut1 = rk * uk * vk;
+  double f_ut2 = rk * uk * v2k;
+  double f_eden = uk * (ek + pk);
+  double f_eint = uk * rek;
+  double q_un = uk, q_pres = pk;
+  const bool star = left ? (sl < 0.0) : (sr > 0.0);
+  if (star) {
+    const double fac = rk * (sk - uk) / (sk - sstar);
+    const double fac_e = rek * (sk - uk) / (sk - sstar);
+    const double estar = fac * (ek / rk + (sstar - uk) * (sstar + pk / (rk * (sk - uk))));
+    f_rho = f_rho + sk * (fac - rk);
+    f_un = f_un + sk * (fac * sstar - rk * uk);
+    f_ut1 = f_ut1 + sk * (fac * vk - rk * vk);
+    f_ut2 = f_ut2 + sk * (fac * v2k - rk * v2k);
+    f_eden = f_eden + sk * (estar - ek);
+    f_eint = f_eint + sk * (fac_e - rek);
+    q_un = sstar;
+    q_pres = pstar;
+  }
+  o.ustar = q_un;
+  o.f_rho = f_rho;
+  o.f_un = f_un;
+  o.f_ut1 = f_ut1;
+  o.f_ut2 = f_ut2;
+  o.f_eden = f_eden;
+  o.f_eint = f_eint;
+  o.q_un = q_un;
+  o.q_pres = dmax(q_pres, small_pres);
+  return o;
+}
+
 // Full conserved flux of one face plus the interface pressure and normal
 // velocity.  Source/Hydro/Hydro_cmpflx.H:153-311.  ql/qr are modified in
 // place at a physical-boundary face exactly as the reference modifies its
@@ -172,9 +239,13 @@ __device__ __forceinline__ void cmpflx(double* ql, double* qr, const CellAux& aL
       v2r = v2l;
     }
   }
-  const ROut o = riemannus(ql[ES_RHO], ul, vl, v2l, ql[ES_P], ql[ES_REINT], qr[ES_RHO], ur,
-                           vr, v2r, qr[ES_P], qr[ES_REINT], cav, gamcl, gamcr, P.small, smallc,
-                           P.small_dens, P.small_pres, P.smallu);
+  const ROut o =
+      (P.riemann_solver == 1)
+          ? hllc(ql[ES_RHO], ul, vl, v2l, ql[ES_P], ql[ES_REINT], qr[ES_RHO], ur, vr, v2r,
+                 qr[ES_P], qr[ES_REINT], gamcl, gamcr, smallc, P.small_dens, P.small_pres)
+          : riemannus(ql[ES_RHO], ul, vl, v2l, ql[ES_P], ql[ES_REINT], qr[ES_RHO], ur, vr, v2r,
+                      qr[ES_P], qr[ES_REINT], cav, gamcl, gamcr, P.small, smallc, P.small_dens,
+                      P.small_pres, P.smallu);
   constexpr int fu = UMX + dir;
   constexpr int fv = (dir == 0) ? UMY : UMX;
   constexpr int fv2 = (dir == 2) ? UMY : UMZ;

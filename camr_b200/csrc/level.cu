@@ -75,7 +75,7 @@ camr_status cuda_status(cudaError_t e) { return camr::cuda_status_of(e); }
 
 camr_status check_params(const camr_hydro_params* p) {
   if (!p) return CAMR_ERR_INVALID;
-  if (p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver < 0 || p->riemann_solver > 1) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
   if (p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   if (p->cfl <= 0.0 || p->cfl > 1.0) return CAMR_ERR_INVALID;  // CAMR.cpp:172-174

@@ -68,7 +68,7 @@ extern "C" camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx
   if (!bx_lo || !bx_hi || !geom || !uin || !dsdt || !flx0 || !flx1 || !flx2 || !p ||
       !uin->ptr || !dsdt->ptr || !flx0->ptr || !flx1->ptr || !flx2->ptr)
     return CAMR_ERR_INVALID;
-  if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver < 0 || p->riemann_solver > 1 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
   for (int d = 0; d < 3; ++d) {
     if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;

@@ -58,7 +58,9 @@ typedef struct {
   int allow_negative_energy;
   int allow_small_energy;
   int add_grav_src;
-  int riemann_solver;   /* 0 = the reference's two-shock solver (riemannus) */
+  int riemann_solver;   /* 0 = the reference's two-shock solver (riemannus),
+                           1 = HLLC (no counterpart in the reference; not
+                           with embedded boundaries or the adjoint) */
   int eb_weights_type;  /* EB flux-redistribution weights (Hydro_utils_eb_K.H:
                            560-575): 0 one, 1 rho*(e + ke), 2 rho, 3 vfrac */
   double difmag;

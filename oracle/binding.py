@@ -111,7 +111,7 @@ class Params(C.Structure):
         "do_mol", "ppm_type", "plm_iorder", "use_pslope", "use_flattening",
         "transverse_reset_density", "dual_energy_update_E_from_e",
         "allow_negative_energy", "allow_small_energy", "add_grav_src",
-        "eb_weights_type", "pad1")] + [(n, C.c_double) for n in (
+        "eb_weights_type", "riemann_solver")] + [(n, C.c_double) for n in (
         "difmag", "small", "small_dens", "small_temp", "small_pres",
         "dual_energy_eta1", "dual_energy_eta2", "const_grav", "cfl",
         "init_shrink", "change_max", "fixed_dt", "initial_dt", "max_dt",

@@ -202,6 +202,71 @@ RiemannOut riemannus(double rl_in, double ul, double vl, double v2l, double pl_i
   return o;
 }
 
+// HLLC (riemann_solver = 1), an option the reference does not have: Toro,
+// "Riemann Solvers and Numerical Methods for Fluid Dynamics", 3rd ed.,
+// sec. 10.4-10.6, with Davis wave speeds; rho e is carried like a passive
+// density.  Interface values: the normal velocity and pressure of the
+// region holding x/t = 0.  The operation order is the one the device
+// kernels use, so both round alike.
+RiemannOut hllc(double rl_in, double ul, double vl, double v2l, double pl_in, double rel,
+                double rr_in, double ur, double vr, double v2r, double pr_in, double rer,
+                double gamcl, double gamcr, double smallc, double small_dens,
+                double small_pres) {
+  RiemannOut o;
+  const double rl = dmax(rl_in, small_dens);
+  const double pl = dmax(pl_in, small_pres);
+  const double rr = dmax(rr_in, small_dens);
+  const double pr = dmax(pr_in, small_pres);
+  const double cl = dmax(smallc, std::sqrt(std::fabs(gamcl * pl / rl)));
+  const double cr = dmax(smallc, std::sqrt(std::fabs(gamcr * pr / rr)));
+  const double sl = dmin(ul - cl, ur - cr);
+  const double sr = dmax(ul + cl, ur + cr);
+  const double el = rel + 0.5 * rl * (ul * ul + vl * vl + v2l * v2l);
+  const double er = rer + 0.5 * rr * (ur * ur + vr * vr + v2r * v2r);
+  const double dl = rl * (sl - ul);
+  const double dr = rr * (sr - ur);
+  const double sstar = ((pr - pl) + (ul * dl - ur * dr)) / (dl - dr);
+  const double pstar = pl + dl * (sstar - ul);
+  const bool left = sstar >= 0.0;
+  const double rk = left ? rl : rr, uk = left ? ul : ur, vk = left ? vl : vr;
+  const double v2k = left ? v2l : v2r, pk = left ? pl : pr, ek = left ? el : er;
+  const double rek = left ? rel : rer, sk = left ? sl : sr;
+  double f_rho = rk * uk;
+  double f_un = rk * uk * uk + pk;
+  double f_ut1 = rk * uk * vk;
+  double f_ut2 = rk * uk * v2k;
+  double f_eden = uk * (ek + pk);
+  double f_eint = uk * rek;
+  double q_un = uk, q_pres = pk;
+  const bool star = left ? (sl < 0.0) : (sr > 0.0);
+  if (star) {
+    const double fac = rk * (sk - uk) / (sk - sstar);
+    const double fac_e = rek * (sk - uk) / (sk - sstar);
+    const double estar = fac * (ek / rk + (sstar - uk) * (sstar + pk / (rk * (sk - uk))));
+    f_rho = f_rho + sk * (fac - rk);
+    f_un = f_un + sk * (fac * sstar - rk * uk);
+    f_ut1 = f_ut1 + sk * (fac * vk - rk * vk);
+    f_ut2 = f_ut2 + sk * (fac * v2k - rk * v2k);
+    f_eden = f_eden + sk * (estar - ek);
+    f_eint = f_eint + sk * (fac_e - rek);
+    q_un = sstar;
+    q_pres = pstar;
+  }
+  o.ustar = q_un;
+  o.f_rho = f_rho;
+  o.f_un = f_un;
+  o.f_ut1 = f_ut1;
+  o.f_ut2 = f_ut2;
+  o.f_eden = f_eden;
+  o.f_eint = f_eint;
+  o.q_un = q_un;
+  o.q_ut1 = (q_un > 0.0) ? vl : (q_un < 0.0) ? vr : 0.5 * (vl + vr);
+  o.q_ut2 = (q_un > 0.0) ? v2l : (q_un < 0.0) ? v2r : 0.5 * (v2l + v2r);
+  o.q_pres = dmax(q_pres, small_pres);
+  o.q_game = 0.5 * (gamcl + gamcr);
+  return o;
+}
+
 // Component maps of one direction (Hydro_cmpflx.H:181-223).
 struct DirMap {
   int iu, iv, iv2;  // primitive velocity slots (normal, transverse 1, 2)
@@ -266,10 +331,13 @@ void cmpflx(double* ql, double* qr, const double* qaL, const double* qaR,
       v2r = v2l;
     }
   }
-  const RiemannOut o = riemannus(ql[QRHO], ul, vl, v2l, ql[QPRES], ql[QREINT],
-                                 qr[QRHO], ur, vr, v2r, qr[QPRES], qr[QREINT],
-                                 cav, gamcl, gamcr, p.small, smallc, p.small_dens,
-                                 p.small_pres, p.smallu);
+  const RiemannOut o =
+      (p.riemann_solver == 1)
+          ? hllc(ql[QRHO], ul, vl, v2l, ql[QPRES], ql[QREINT], qr[QRHO], ur, vr, v2r,
+                 qr[QPRES], qr[QREINT], gamcl, gamcr, smallc, p.small_dens, p.small_pres)
+          : riemannus(ql[QRHO], ul, vl, v2l, ql[QPRES], ql[QREINT], qr[QRHO], ur, vr, v2r,
+                      qr[QPRES], qr[QREINT], cav, gamcl, gamcr, p.small, smallc, p.small_dens,
+                      p.small_pres, p.smallu);
   flx[URHO] = o.f_rho;
   flx[m.fu] = o.f_un;
   flx[m.fv] = o.f_ut1;

@@ -41,7 +41,8 @@ typedef struct {
   int allow_small_energy;
   int add_grav_src;
   int eb_weights_type;  /* EB flux-redistribution weights (default 2 = rho) */
-  int pad1;
+  int riemann_solver;   /* 0 riemannus (the reference); 1 HLLC (restatement
+                           only: the reference has no such option) */
   double difmag;
   double small;
   double small_dens;

@@ -124,7 +124,7 @@ inline void default_params(orc_params* p) {
   p->allow_small_energy = 1;
   p->add_grav_src = 1;
   p->eb_weights_type = 2;  // :107
-  p->pad1 = 0;
+  p->riemann_solver = 0;
   p->difmag = 0.1;
   p->small = 1.e-8;
   p->small_dens = 1.e-7;
