@@ -7,9 +7,22 @@
 
 namespace camr {
 
+// Loads of arrays that a kernel only reads go through the read-only data
+// path when CAMR_LDG is 1 (the default).
+#ifndef CAMR_LDG
+#define CAMR_LDG 1
+#endif
+__device__ __forceinline__ double ld_ro(const double* p) {
+#if CAMR_LDG
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+
 __device__ __forceinline__ void load_es(const double* a, const Space& s, int64_t at, double* r) {
 #pragma unroll
-  for (int n = 0; n < ES_N; ++n) r[n] = a[at + n * s.sn];
+  for (int n = 0; n < ES_N; ++n) r[n] = ld_ro(a + at + n * s.sn);
 }
 __device__ __forceinline__ void store_es(double* a, const Space& s, int64_t at, const double* r) {
 #pragma unroll
@@ -17,13 +30,13 @@ __device__ __forceinline__ void store_es(double* a, const Space& s, int64_t at, 
 }
 __device__ __forceinline__ void load_fr(const double* a, const Space& s, int64_t at, double* r) {
 #pragma unroll
-  for (int n = 0; n < FR_N; ++n) r[n] = a[at + n * s.sn];
+  for (int n = 0; n < FR_N; ++n) r[n] = ld_ro(a + at + n * s.sn);
 }
 __device__ __forceinline__ CellAux load_aux(const double* q, const Space& s, int64_t at,
                                             double gamma) {
   CellAux a;
-  a.c = q[at + SQ_C * s.sn];
-  a.csml = q[at + SQ_CSML * s.sn];
+  a.c = ld_ro(q + at + SQ_C * s.sn);
+  a.csml = ld_ro(q + at + SQ_CSML * s.sn);
   a.gamc = gamma;  // qaux QGAMC = EOS::REY2Gam = gamma (Hydro_ctoprim.H:83,96)
   return a;
 }
