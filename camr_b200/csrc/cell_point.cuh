@@ -122,13 +122,14 @@ __device__ __forceinline__ void plm_edge_states(const double* q, int64_t at, int
   constexpr int l0 = d;
   constexpr int l1 = (d == 0) ? 1 : 0;
   constexpr int l2 = (d == 2) ? 1 : 2;
-  const double cc = q[at + SQ_C * sn];
+  const double cc = ld_ro(q + at + SQ_C * sn);
   const double dtdx_p = dtdx;
   const double cs = cc * cc;
-  const double rho = q[at + SQ_RHO * sn];
-  const double vel[3] = {q[at + SQ_U * sn], q[at + SQ_V * sn], q[at + SQ_W * sn]};
-  const double pr = q[at + SQ_P * sn];
-  const double rhoe = q[at + SQ_REINT * sn];
+  const double rho = ld_ro(q + at + SQ_RHO * sn);
+  const double vel[3] = {ld_ro(q + at + SQ_U * sn), ld_ro(q + at + SQ_V * sn),
+                         ld_ro(q + at + SQ_W * sn)};
+  const double pr = ld_ro(q + at + SQ_P * sn);
+  const double rhoe = ld_ro(q + at + SQ_REINT * sn);
   const double enth = ((rhoe + pr) / rho) / cs;
   const double drho = slope[ES_RHO];
   const double dvel[3] = {slope[ES_U], slope[ES_V], slope[ES_W]};
@@ -190,7 +191,7 @@ __device__ __forceinline__ void plm_edge_states(const double* q, int64_t at, int
   const double vel_ad = vel[l0];
 #pragma unroll
   for (int sp = 0; sp < NSPEC; ++sp) {
-    const double qn = q[at + (SQ_FS + sp) * sn];
+    const double qn = ld_ro(q + at + (SQ_FS + sp) * sn);
     {
       const double spzero = (vel_ad > 0) ? -1.0 : vel_ad * dtdx_p;
       const double acmprght = 0.5 * (-1.0 - spzero) * slope[ES_FS + sp];
@@ -214,7 +215,7 @@ __device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space&
     return;
   }
   const double plm_theta = 2.0;
-  auto Q = [&](int off, int slot) { return q[at + off * st + slot * s.sn]; };
+  auto Q = [&](int off, int slot) { return ld_ro(q + at + off * st + slot * s.sn); };
   constexpr int un = SQ_U + d;
   constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
   constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
@@ -257,8 +258,8 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
   const int64_t at = s.idx(i, j, k);
   const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
   const int64_t atL = at - st;
-  auto Q = [&](int64_t c, int slot) { return q[c + slot * s.sn]; };
-  auto S = [&](int64_t c, int slot) { return sl[c + slot * s.sn]; };
+  auto Q = [&](int64_t c, int slot) { return ld_ro(q + c + slot * s.sn); };
+  auto S = [&](int64_t c, int slot) { return ld_ro(sl + c + slot * s.sn); };
   constexpr int un = SQ_U + d;
   constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
   constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
