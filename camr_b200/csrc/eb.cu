@@ -1443,26 +1443,33 @@ camr_fab level_fab(const LGeom& L, double* p) {
 // in an EB build): src_to_fill = 0; per box: covered boxes nothing, boxes
 // whose grow(bx,2) is all regular the regular hydro (batched), the others
 // hydro_umdrv_eb.  Sborder is lev->B.
-int eb_hydro_stage(camr_eb_level* lev, cudaStream_t st) {
-  int nk = 0;
-  cudaMemsetAsync(lev->dsdt, 0, size_t(lev->L.sn) * NVAR * sizeof(double), st);
+cudaError_t eb_hydro_stage(camr_eb_level* lev, cudaStream_t st, int* nk) {
+  cudaError_t e = cudaMemsetAsync(lev->dsdt, 0, size_t(lev->L.sn) * NVAR * sizeof(double), st);
   const int nside = int(lev->side.size());
-  if (nside) {
-    cudaEventRecord(lev->ev_fork, st);
-    for (cudaStream_t s2 : lev->side) cudaStreamWaitEvent(s2, lev->ev_fork, 0);
+  if (nside && e == cudaSuccess) {
+    e = cudaEventRecord(lev->ev_fork, st);
+    for (cudaStream_t s2 : lev->side)
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, lev->ev_fork, 0);
   }
+  if (e != cudaSuccess) return e;
   const DFab none[3] = {level_dfab(lev->L, nullptr), level_dfab(lev->L, nullptr),
                         level_dfab(lev->L, nullptr)};
   const DFab U = level_dfab(lev->L, lev->B);
   const DFab ds = level_dfab(lev->L, lev->dsdt);
   for (size_t b = 0; b < lev->plans.size(); ++b)
-    nk += eb_issue(lev->plans[b], U, ds, none, nside ? lev->side[b % nside] : st);
-  if (lev->regular) camr_batch_run(lev->regular, 0.0, lev->dt_cur, CAMR_BATCH_PERSISTENT, st);
+    *nk += eb_issue(lev->plans[b], U, ds, none, nside ? lev->side[b % nside] : st);
+  camr_status cs = CAMR_OK;
+  if (lev->regular) cs = camr_batch_run(lev->regular, 0.0, lev->dt_cur, CAMR_BATCH_PERSISTENT, st);
+  // the side streams join back whatever happened above, so that a capture
+  // in progress ends with every branch joined
   for (int i = 0; i < nside; ++i) {
-    cudaEventRecord(lev->ev_join[i], lev->side[i]);
-    cudaStreamWaitEvent(st, lev->ev_join[i], 0);
+    const cudaError_t e1 = cudaEventRecord(lev->ev_join[i], lev->side[i]);
+    const cudaError_t e2 = cudaStreamWaitEvent(st, lev->ev_join[i], 0);
+    if (e == cudaSuccess) e = (e1 != cudaSuccess) ? e1 : e2;
   }
-  return nk;
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess && cs != CAMR_OK) e = cudaErrorLaunchFailure;
+  return e;
 }
 
 cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_dev) {
@@ -1484,7 +1491,8 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   k_ebl_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->S_old, lev->err);
   k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err);
   nk += 3;
-  nk += eb_hydro_stage(lev, st);
+  cudaError_t e = eb_hydro_stage(lev, st, &nk);
+  if (e != cudaSuccess) return e;
   if (!lev->hp.do_mol) {
     k_ebl_update_ctu<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old,
                                           lev->dsdt, lev->S, lev->bits, lev->err);
@@ -1496,7 +1504,8 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   // stage 2's Sborder reuses B (stage 1's is dead after the update)
   k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B, lev->err);
   nk += 2;
-  nk += eb_hydro_stage(lev, st);
+  e = eb_hydro_stage(lev, st, &nk);
+  if (e != cudaSuccess) return e;
   k_ebl_update2<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
                                      lev->S, lev->bits, lev->err);
   nk += 1;
