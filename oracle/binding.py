@@ -32,8 +32,10 @@ def load_eb():
 
 def hydro_box_eb(p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, periodic, uin, g_lo, geo, dx, dt,
                  redist=1, weights_type=2):
-    """Per-box EB hydro (MOL).  uin: (NVAR, ...) over G = [g_lo, g_lo + shape - 1];
-    geo: eb_geometry.sphere_geometry output over the same G.  Returns
+    """Per-box EB hydro (MOL, or Godunov with p.do_mol = 0).  uin: (NVAR, ...)
+    over G = [g_lo, g_lo + shape - 1]; geo: eb_geometry.sphere_geometry
+    output over the same G.  redist: 0 none, 1 flux, 2 state redistribution.
+    Returns
     (dsdt on bx, [flx_x, flx_y, flx_z] on bx faces, nassert)."""
     lib = load_eb()
     nb = [bx_hi[d] - bx_lo[d] + 1 for d in range(3)]
@@ -51,11 +53,13 @@ def hydro_box_eb(p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, periodic, uin, g_l
     flag = np.ascontiguousarray(geo["flag"], dtype=np.uint32)
     vf = np.ascontiguousarray(geo["vfrac"], dtype=np.float64)
     P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    cent = np.ascontiguousarray(geo["cent"], dtype=np.float64)
     n = lib.orc_hydro_box_eb(C.byref(p), I3(*bx_lo), I3(*bx_hi), I3(*dom_lo), I3(*dom_hi),
                              I3(*bclo), I3(*bchi), I3(*periodic), P(uin), I3(*g_lo), I3(*g_hi),
                              P(flag), P(vf), P(arr[0]), P(arr[1]), P(arr[2]), P(fcs[0]),
-                             P(fcs[1]), P(fcs[2]), int(redist), int(weights_type), P(dsdt),
-                             P(flx[0]), P(flx[1]), P(flx[2]), _D3(*dx), C.c_double(dt))
+                             P(fcs[1]), P(fcs[2]), P(cent), int(redist), int(weights_type),
+                             P(dsdt), P(flx[0]), P(flx[1]), P(flx[2]), _D3(*dx),
+                             C.c_double(dt))
     return dsdt, flx, n
 
 
@@ -75,8 +79,9 @@ def eb_advance(p, lev, geo, state, nsteps, first_step=True, dt_prev=0.0, redist=
     P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
     dtp = C.c_double(dt_prev)
     hist = np.zeros(max(nsteps, 1))
+    cent = np.ascontiguousarray(geo["cent"], dtype=np.float64)
     n = lib.orc_eb_advance(C.byref(p), C.byref(lev), P(flag), P(vf), P(arr[0]), P(arr[1]),
-                           P(arr[2]), P(fcs[0]), P(fcs[1]), P(fcs[2]), P(state), int(nsteps),
+                           P(arr[2]), P(fcs[0]), P(fcs[1]), P(fcs[2]), P(cent), P(state), int(nsteps),
                            int(bool(first_step)), C.byref(dtp), P(hist), int(redist))
     return dtp.value, hist[:nsteps], n
 

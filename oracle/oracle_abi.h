@@ -137,7 +137,10 @@ long orc_amr_run(const orc_params* p, const orc_level* lev0, int nbox, const int
  * (redist = 1, restated) or none (redist = 0).  uin, flag, vfrac cover G =
  * [g_lo, g_hi] (at least grow(bx, 5)); ap[d] and fc[d] (2 comps) cover
  * surroundingNodes(G, d).  flag: bits 0-1 type (0 regular, 1 cut, 3
- * covered), bit 2 + (di+1) + 3(dj+1) + 9(dk+1) connectivity.  dsdt (bx) is
+ * covered), bit 2 + (di+1) + 3(dj+1) + 9(dk+1) connectivity; cent (3 comps,
+ * may be NULL = cell centres) the cell-centroid offsets.  redist: 0 none,
+ * 1 flux redistribution, 2 state redistribution (one more ghost layer:
+ * G at least grow(bx, 6) for MOL, 7 for Godunov).  dsdt (bx) is
  * overwritten; flx[d] receive the face-centroid fluxes of bx's faces. */
 long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const int bx_hi[3],
                       const int dom_lo[3], const int dom_hi[3], const int bclo[3],
@@ -145,8 +148,8 @@ long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const int bx_hi[3
                       const int g_lo[3], const int g_hi[3], const unsigned* flag,
                       const double* vfrac, const double* ap0, const double* ap1,
                       const double* ap2, const double* fc0, const double* fc1, const double* fc2,
-                      int redist, int weights_type, double* dsdt, double* flx0, double* flx1,
-                      double* flx2, const double dx[3], double dt);
+                      const double* cent, int redist, int weights_type, double* dsdt,
+                      double* flx0, double* flx1, double* flx2, const double dx[3], double dt);
 
 /* EB level steps, MOL (oracle/_ref/libcamr_ref_eb.so only): the level
  * driver's step with the EB build's guards, the whole domain as one EB box.
@@ -154,8 +157,9 @@ long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const int bx_hi[3
  * cells, updated in place (covered cells zero). */
 long orc_eb_advance(const orc_params* p, const orc_level* lev, const unsigned* flag,
                     const double* vfrac, const double* ap0, const double* ap1, const double* ap2,
-                    const double* fc0, const double* fc1, const double* fc2, double* state,
-                    int nsteps, int first_step, double* dt_prev, double* dt_hist, int redist);
+                    const double* fc0, const double* fc1, const double* fc2, const double* cent,
+                    double* state, int nsteps, int first_step, double* dt_prev, double* dt_hist,
+                    int redist);
 
 /* initData's epilogue with the EB guards (rho > 0 only), valid cells. */
 void orc_eb_init_finalize(const orc_params* p, const orc_level* lev, double* state);

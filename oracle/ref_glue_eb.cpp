@@ -38,6 +38,254 @@ Array4<Real> view(double* p, const int lo[3], const int hi[3], int nc) {
                       nc);
 }
 
+// ---------------------------------------------------------------------------
+// State redistribution (redistribution_type = StateRedist), restated from
+// the published method (Berger & Giuliani, "A state redistribution
+// algorithm for finite volume schemes on cut cell meshes", J. Comput. Phys.
+// 434 (2021) 110205); AMReX's own implementation is not available here, so
+// the neighbourhood rule below is this restatement's own:
+//   * a cut cell with volume fraction below 1/2 merges with connected,
+//     uncovered neighbours of its 3x3x3 block inside the domain (grown in
+//     periodic directions), taken in decreasing order of
+//     (m . o) / |o| with m = (ap_x(i+1) - ap_x(i), ...) the direction into the
+//     fluid and o the neighbour offset (ties in raster order), until the
+//     merged volume fraction reaches 1/2 or the neighbourhood holds 8 cells;
+//     every other cell's neighbourhood is itself;
+//   * N_j: the number of neighbourhoods that hold cell j;
+//   * Vhat_i = sum_{j in M_i} vf_j / N_j, xhat_i the matching weighted
+//     centroid (cell-width units, x_j = index + cell centroid offset),
+//     Qhat_i = sum_{j in M_i} (vf_j / N_j) U*_j / Vhat_i with U* = U + dt divc;
+//   * for neighbourhoods of more than one cell, a least-squares gradient of
+//     Qhat over the connected neighbours' (xhat, Qhat), limited
+//     Barth-Jespersen style so that no member's value leaves the range of
+//     those Qhat;
+//   * U_new_j = (1/N_j) sum_{i: j in M_i} (Qhat_i + g_i . (x_j - xhat_i)),
+//     gathered in raster order of i; dSdt = (U_new - U) / dt (0 on covered
+//     cells).
+// It conserves sum vf U exactly in exact arithmetic.
+constexpr int kSrdMax = 8;
+
+struct SrdNbhd {
+  int n;
+  int off[kSrdMax];  // offsets as (di+1) + 3(dj+1) + 9(dk+1); off[0] = 13 (the cell)
+};
+
+inline void srd_off(int o, int& di, int& dj, int& dk) {
+  di = o % 3 - 1;
+  dj = (o / 3) % 3 - 1;
+  dk = o / 9 - 1;
+}
+
+bool srd_inside(const Box& dom, const int* periodic, int i, int j, int k) {
+  const int c[3] = {i, j, k};
+  for (int d = 0; d < 3; ++d)
+    if (!periodic[d] && (c[d] < dom.lo[d] || c[d] > dom.hi[d])) return false;
+  return true;
+}
+
+SrdNbhd srd_nbhd(const Box& dom, const int* periodic, Array4<EBCellFlag const> const& flag,
+                 Array4<const Real> const& vf, const Array4<const Real>* ap, int i, int j,
+                 int k) {
+  SrdNbhd r;
+  r.n = 1;
+  r.off[0] = 13;
+  const EBCellFlag f = flag(i, j, k);
+  if (!f.isSingleValued() || !(vf(i, j, k) < 0.5)) return r;
+  const double m0 = ap[0](i + 1, j, k) - ap[0](i, j, k);
+  const double m1 = ap[1](i, j + 1, k) - ap[1](i, j, k);
+  const double m2 = ap[2](i, j, k + 1) - ap[2](i, j, k);
+  int cand[26];
+  double score[26];
+  int nc = 0;
+  for (int kk = -1; kk <= 1; ++kk)
+    for (int jj = -1; jj <= 1; ++jj)
+      for (int ii = -1; ii <= 1; ++ii) {
+        if (ii == 0 && jj == 0 && kk == 0) continue;
+        if (!f.isConnected(ii, jj, kk)) continue;
+        if (flag(i + ii, j + jj, k + kk).isCovered()) continue;
+        if (!srd_inside(dom, periodic, i + ii, j + jj, k + kk)) continue;
+        const double len = std::sqrt(double(ii * ii + jj * jj + kk * kk));
+        const double sc = (m0 * ii + m1 * jj + m2 * kk) / len;
+        // insertion keeps the order: higher score first, raster order on ties
+        int at = nc;
+        while (at > 0 && score[at - 1] < sc) {
+          score[at] = score[at - 1];
+          cand[at] = cand[at - 1];
+          --at;
+        }
+        score[at] = sc;
+        cand[at] = (ii + 1) + 3 * (jj + 1) + 9 * (kk + 1);
+        ++nc;
+      }
+  double vol = vf(i, j, k);
+  for (int c = 0; c < nc && vol < 0.5 && r.n < kSrdMax; ++c) {
+    int di, dj, dk;
+    srd_off(cand[c], di, dj, dk);
+    r.off[r.n++] = cand[c];
+    vol += vf(i + di, j + dj, k + dk);
+  }
+  return r;
+}
+
+void state_redistribute(const Box& bx, const Box& dom, const int* periodic,
+                        Array4<EBCellFlag const> const& flag, Array4<const Real> const& vf,
+                        const Array4<const Real>* ap, Array4<const Real> const& cent,
+                        Array4<const Real> const& u, Array4<const Real> const& divc, double dt,
+                        Array4<Real> const& out) {
+  const Box b4 = amrex::grow(bx, 4), b3 = amrex::grow(bx, 3), b2 = amrex::grow(bx, 2),
+            b1 = amrex::grow(bx, 1);
+  // neighbourhoods on grow(bx,4)
+  const IntVect n4(b4.hi[0] - b4.lo[0] + 1, b4.hi[1] - b4.lo[1] + 1, b4.hi[2] - b4.lo[2] + 1);
+  std::vector<SrdNbhd> nb(size_t(n4[0]) * n4[1] * n4[2]);
+  auto NB = [&](int i, int j, int k) -> SrdNbhd& {
+    return nb[size_t((i - b4.lo[0]) + n4[0] * ((j - b4.lo[1]) + n4[1] * (k - b4.lo[2])))];
+  };
+  ParallelFor(b4, [&](int i, int j, int k) {
+    SrdNbhd& r = NB(i, j, k);
+    if (flag(i, j, k).isCovered() || !srd_inside(dom, periodic, i, j, k)) {
+      r.n = 0;
+      return;
+    }
+    r = srd_nbhd(dom, periodic, flag, vf, ap, i, j, k);
+  });
+  auto holds = [&](int i, int j, int k, int di, int dj, int dk) {
+    // does the neighbourhood of (i,j,k) hold its neighbour at (di,dj,dk)?
+    const SrdNbhd& r = NB(i, j, k);
+    const int o = (di + 1) + 3 * (dj + 1) + 9 * (dk + 1);
+    for (int c = 0; c < r.n; ++c)
+      if (r.off[c] == o) return true;
+    return false;
+  };
+  // N on grow(bx,3)
+  FArrayBox Nf(b3, 1), vh(b2, 1), xh(b2, 3), qh(b2, NVAR), gr(b1, 3 * NVAR);
+  Nf.setVal(0.0);
+  auto N = Nf.array();
+  ParallelFor(b3, [&](int i, int j, int k) {
+    if (flag(i, j, k).isCovered() || !srd_inside(dom, periodic, i, j, k)) return;
+    double cnt = 0.0;
+    for (int kk = -1; kk <= 1; ++kk)
+      for (int jj = -1; jj <= 1; ++jj)
+        for (int ii = -1; ii <= 1; ++ii)
+          if (holds(i - ii, j - jj, k - kk, ii, jj, kk)) cnt += 1.0;
+    N(i, j, k) = cnt;
+  });
+  auto VH = vh.array();
+  auto XH = xh.array();
+  auto QH = qh.array();
+  ParallelFor(b2, [&](int i, int j, int k) {
+    const SrdNbhd& r = NB(i, j, k);
+    if (r.n == 0) return;
+    double v = 0.0, x0 = 0.0, x1 = 0.0, x2 = 0.0;
+    double q[NVAR];
+    for (int n = 0; n < NVAR; ++n) q[n] = 0.0;
+    for (int c = 0; c < r.n; ++c) {
+      int di, dj, dk;
+      srd_off(r.off[c], di, dj, dk);
+      const int a = i + di, b = j + dj, cc = k + dk;
+      const double w = vf(a, b, cc) / N(a, b, cc);
+      v += w;
+      x0 += w * (a + cent(a, b, cc, 0));
+      x1 += w * (b + cent(a, b, cc, 1));
+      x2 += w * (cc + cent(a, b, cc, 2));
+      for (int n = 0; n < NVAR; ++n) q[n] += w * (u(a, b, cc, n) + dt * divc(a, b, cc, n));
+    }
+    VH(i, j, k) = v;
+    XH(i, j, k, 0) = x0 / v;
+    XH(i, j, k, 1) = x1 / v;
+    XH(i, j, k, 2) = x2 / v;
+    for (int n = 0; n < NVAR; ++n) QH(i, j, k, n) = q[n] / v;
+  });
+  auto GR = gr.array();
+  ParallelFor(b1, [&](int i, int j, int k) {
+    const SrdNbhd& r = NB(i, j, k);
+    if (r.n < 2) return;
+    const EBCellFlag f = flag(i, j, k);
+    double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0;
+    for (int kk = -1; kk <= 1; ++kk)
+      for (int jj = -1; jj <= 1; ++jj)
+        for (int ii = -1; ii <= 1; ++ii) {
+          if ((ii == 0 && jj == 0 && kk == 0) || !f.isConnected(ii, jj, kk)) continue;
+          if (NB(i + ii, j + jj, k + kk).n == 0) continue;
+          const double d0 = XH(i + ii, j + jj, k + kk, 0) - XH(i, j, k, 0);
+          const double d1 = XH(i + ii, j + jj, k + kk, 1) - XH(i, j, k, 1);
+          const double d2 = XH(i + ii, j + jj, k + kk, 2) - XH(i, j, k, 2);
+          a00 += d0 * d0; a01 += d0 * d1; a02 += d0 * d2;
+          a11 += d1 * d1; a12 += d1 * d2; a22 += d2 * d2;
+        }
+    const double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22,
+                 c02 = a01 * a12 - a02 * a11;
+    const double det = a00 * c00 + a01 * c01 + a02 * c02;
+    for (int n = 0; n < NVAR; ++n) {
+      double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+      if (std::fabs(det) > 1e-10) {
+        double b0 = 0, b1v = 0, b2v = 0;
+        double qmin = QH(i, j, k, n), qmax = QH(i, j, k, n);
+        for (int kk = -1; kk <= 1; ++kk)
+          for (int jj = -1; jj <= 1; ++jj)
+            for (int ii = -1; ii <= 1; ++ii) {
+              if ((ii == 0 && jj == 0 && kk == 0) || !f.isConnected(ii, jj, kk)) continue;
+              if (NB(i + ii, j + jj, k + kk).n == 0) continue;
+              const double d0 = XH(i + ii, j + jj, k + kk, 0) - XH(i, j, k, 0);
+              const double d1 = XH(i + ii, j + jj, k + kk, 1) - XH(i, j, k, 1);
+              const double d2 = XH(i + ii, j + jj, k + kk, 2) - XH(i, j, k, 2);
+              const double dq = QH(i + ii, j + jj, k + kk, n) - QH(i, j, k, n);
+              b0 += d0 * dq; b1v += d1 * dq; b2v += d2 * dq;
+              qmin = std::min(qmin, QH(i + ii, j + jj, k + kk, n));
+              qmax = std::max(qmax, QH(i + ii, j + jj, k + kk, n));
+            }
+        const double c11 = a00 * a22 - a02 * a02, c12 = a01 * a02 - a00 * a12,
+                     c22 = a00 * a11 - a01 * a01;
+        g0 = (c00 * b0 + c01 * b1v + c02 * b2v) / det;
+        g1 = (c01 * b0 + c11 * b1v + c12 * b2v) / det;
+        g2 = (c02 * b0 + c12 * b1v + c22 * b2v) / det;
+        double alpha = 1.0;
+        for (int c = 0; c < r.n; ++c) {
+          int di, dj, dk;
+          srd_off(r.off[c], di, dj, dk);
+          const int a = i + di, b = j + dj, cc = k + dk;
+          const double v = g0 * (a + cent(a, b, cc, 0) - XH(i, j, k, 0)) +
+                           g1 * (b + cent(a, b, cc, 1) - XH(i, j, k, 1)) +
+                           g2 * (cc + cent(a, b, cc, 2) - XH(i, j, k, 2));
+          if (v > 0.0) alpha = std::min(alpha, (qmax - QH(i, j, k, n)) / v);
+          else if (v < 0.0) alpha = std::min(alpha, (qmin - QH(i, j, k, n)) / v);
+        }
+        g0 *= alpha;
+        g1 *= alpha;
+        g2 *= alpha;
+      }
+      GR(i, j, k, 3 * n) = g0;
+      GR(i, j, k, 3 * n + 1) = g1;
+      GR(i, j, k, 3 * n + 2) = g2;
+    }
+  });
+  ParallelFor(bx, [&](int i, int j, int k) {
+    if (flag(i, j, k).isCovered()) {
+      for (int n = 0; n < NVAR; ++n) out(i, j, k, n) = 0.0;
+      return;
+    }
+    double acc[NVAR];
+    for (int n = 0; n < NVAR; ++n) acc[n] = 0.0;
+    for (int kk = -1; kk <= 1; ++kk)
+      for (int jj = -1; jj <= 1; ++jj)
+        for (int ii = -1; ii <= 1; ++ii) {
+          const int a = i + ii, b = j + jj, cc = k + kk;
+          if (!holds(a, b, cc, -ii, -jj, -kk)) continue;
+          if (NB(a, b, cc).n < 2) {
+            for (int n = 0; n < NVAR; ++n) acc[n] += QH(a, b, cc, n);
+          } else {
+            const double x0 = i + cent(i, j, k, 0) - XH(a, b, cc, 0);
+            const double x1 = j + cent(i, j, k, 1) - XH(a, b, cc, 1);
+            const double x2 = k + cent(i, j, k, 2) - XH(a, b, cc, 2);
+            for (int n = 0; n < NVAR; ++n)
+              acc[n] += QH(a, b, cc, n) + (GR(a, b, cc, 3 * n) * x0 +
+                                           GR(a, b, cc, 3 * n + 1) * x1 +
+                                           GR(a, b, cc, 3 * n + 2) * x2);
+          }
+        }
+    for (int n = 0; n < NVAR; ++n) out(i, j, k, n) = (acc[n] / N(i, j, k) - u(i, j, k, n)) / dt;
+  });
+}
+
 }  // namespace
 
 extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const int bx_hi[3],
@@ -46,9 +294,9 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
                                  const int g_lo[3], const int g_hi[3], const unsigned* flag_in,
                                  const double* vfrac_in, const double* ap0, const double* ap1,
                                  const double* ap2, const double* fc0, const double* fc1,
-                                 const double* fc2, int redist, int weights_type, double* dsdt,
-                                 double* flx0, double* flx1, double* flx2, const double dx_in[3],
-                                 double dt) {
+                                 const double* fc2, const double* cent_in, int redist,
+                                 int weights_type, double* dsdt, double* flx0, double* flx1,
+                                 double* flx2, const double dx_in[3], double dt) {
   shim_assert_count() = 0;
   PassMap pmap;
   init_pass_map(&pmap);
@@ -81,7 +329,10 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
   // q, qaux on grow(bx, numGrow()): 5 for MOL, 6 for Godunov with flux
   // redistribution (CAMR.H:465-472); hydro_ctoprim on the non-covered cells
   const bool mol = p->do_mol != 0;
-  const Box qbx = amrex::grow(bx, mol ? 5 : 6);
+  // state redistribution needs one more layer of everything
+  // (CAMR.H:465-479, CAMR_construct_hydro_source.cpp:146-152)
+  const int e_srd = (redist == 2) ? 1 : 0;
+  const Box qbx = amrex::grow(bx, (mol ? 5 : 6) + e_srd);
   FArrayBox qf(qbx, QVAR), qauxf(qbx, NQAUX), srcqf(qbx, QVAR), zsrc(qbx, NVAR);
   auto q = qf.array();
   auto qaux = qauxf.array();
@@ -107,7 +358,7 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
       }
     });
   }
-  const Box bxg_i = amrex::grow(bx, 2);
+  const Box bxg_i = amrex::grow(bx, 2 + e_srd);
   const Box bxg_ii = amrex::grow(bxg_i, 1);
   FArrayBox divc(bxg_i, NVAR), redistwgt(bxg_i, 1);
   divc.setVal(0.0);
@@ -153,6 +404,19 @@ extern "C" long orc_hydro_box_eb(const orc_params* p, const int bx_lo[3], const 
                   dxinv, ft, fo_arr, p->small, p->small_dens, p->small_pres, p->smallu,
                   weights_type);
   auto out = view(dsdt, bx_lo, bx_hi, NVAR);
+  if (redist == 2) {
+    Array4<const Real> cent;
+    std::vector<double> zc;
+    if (cent_in) {
+      cent = Array4<const Real>(view(const_cast<double*>(cent_in), g_lo, g_hi, 3));
+    } else {
+      zc.assign(size_t(G.numPts()) * 3, 0.0);
+      cent = Array4<const Real>(view(zc.data(), g_lo, g_hi, 3));
+    }
+    state_redistribute(bx, dom, periodic, flag, vf, ap, cent, u, Array4<const Real>(divc_arr),
+                       dt, out);
+    return shim_assert_count();
+  }
   if (!redist) {
     ParallelFor(bx, NVAR, [=](int i, int j, int k, int n) {
       out(i, j, k, n) = flag(i, j, k).isCovered() ? 0.0 : divc_arr(i, j, k, n);
@@ -527,8 +791,8 @@ static long eb_regular_box(const orc_params* p, const LevelEB& L, const Box& bx,
 extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const unsigned* flag_in,
                                const double* vfrac, const double* ap0, const double* ap1,
                                const double* ap2, const double* fc0, const double* fc1,
-                               const double* fc2, double* state, int nsteps, int first_step,
-                               double* dt_prev, double* dt_hist, int redist) {
+                               const double* fc2, const double* cent, double* state, int nsteps,
+                               int first_step, double* dt_prev, double* dt_hist, int redist) {
   LevelEB L;
   for (int d = 0; d < 3; ++d) {
     L.dom.lo[d] = lev->dom_lo[d];
@@ -540,7 +804,7 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
   }
   // ghost cells: numGrow() with flux redistribution, 5 for MOL, 6 for
   // Godunov (CAMR.H:465-472); the geometry covers grow(domain, ng)
-  const int ng = p->do_mol ? 5 : 6;
+  const int ng = (p->do_mol ? 5 : 6) + (redist == 2 ? 1 : 0);
   L.G = amrex::grow(L.dom, ng);
   std::vector<EBCellFlag> fl(size_t(L.G.numPts()));
   for (size_t c = 0; c < fl.size(); ++c) fl[c] = EBCellFlag(flag_in[c]);
@@ -580,7 +844,7 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
           ParallelFor(b, [&](int ii, int jj, int kk) {
             if (!covered(L, ii, jj, kk)) all_cov = false;
           });
-          ParallelFor(amrex::grow(b, 2), [&](int ii, int jj, int kk) {
+          ParallelFor(amrex::grow(b, redist == 2 ? 3 : 2), [&](int ii, int jj, int kk) {
             if (!L.flag(ii, jj, kk).isRegular()) all_reg = false;
           });
           boxes.push_back(b);
@@ -601,7 +865,8 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
       FArrayBox dfab(bx, NVAR), ff[3];
       for (int d = 0; d < 3; ++d) ff[d].resize(amrex::surroundingNodes(bx, d), NVAR);
       ne += orc_hydro_box_eb(p, bx.lo.v, bx.hi.v, dlo, dhi, L.bclo, L.bchi, L.periodic, Bv.p,
-                             g_lo, g_hi, flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, redist,
+                             g_lo, g_hi, flag_in, vfrac, ap0, ap1, ap2, fc0, fc1, fc2, cent,
+                             redist,
                              p->eb_weights_type, dfab.array().p, ff[0].array().p,
                              ff[1].array().p, ff[2].array().p, L.dx, dt);
       auto dv = dfab.array();
