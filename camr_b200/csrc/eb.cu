@@ -64,6 +64,7 @@ struct EBG {
   const double* vfrac;
   const double* ap[3];
   const double* fc[3];
+  const double* cent;  // 3 comps of cell-centroid offsets, or null (cell centres)
   int lo[3], n[3];
   __device__ __forceinline__ int64_t c(int i, int j, int k) const {
     return (i - lo[0]) + int64_t(n[0]) * ((j - lo[1]) + int64_t(n[1]) * (k - lo[2]));
@@ -77,6 +78,9 @@ struct EBG {
   }
   __device__ __forceinline__ unsigned fl(int i, int j, int k) const { return flag[c(i, j, k)]; }
   __device__ __forceinline__ double vf(int i, int j, int k) const { return vfrac[c(i, j, k)]; }
+  __device__ __forceinline__ double ce(int d, int i, int j, int k) const {
+    return cent ? cent[c(i, j, k) + d * int64_t(n[0]) * n[1] * n[2]] : 0.0;
+  }
   __device__ __forceinline__ double a(int d, int i, int j, int k) const { return ap[d][f(d, i, j, k)]; }
   __device__ __forceinline__ double fcv(int d, int comp, int i, int j, int k) const {
     return fc[d][f(d, i, j, k) + comp * fn(d)];
@@ -88,6 +92,11 @@ struct EBWork {
   double *q, *sl[3], *ft[3], *qf[3], *divu, *divc, *wt, *optmp, *delm, *wtinv;
   // Godunov (CTU-PLM) only: edge states, first-pass and D|E flux records
   double *sm[3], *sp[3], *f1[3], *f2[6];
+  // state redistribution only: packed neighbourhood (count in bits 0-3,
+  // offsets of 5 bits each from bit 4), overlap count N, neighbourhood
+  // volume, centroid (3), averaged state (NVAR) and limited gradient (3 NVAR)
+  unsigned long long* nb;
+  double *nov, *vhat, *xhat, *qhat, *grad;
 };
 
 __global__ void __launch_bounds__(kEB) k_eb_ctoprim(Region r, EBWork W, EBG G, DFab u, KParams P,
@@ -882,6 +891,250 @@ __global__ void __launch_bounds__(kEB) k_ebc_face(Region r0, Region r1, Region r
   }
 }
 
+// ---------------------------------------------------------------------------
+// State redistribution (redist = 2), restated from Berger & Giuliani's
+// published method (J. Comput. Phys. 434 (2021) 110205), AMReX's own
+// StateRedist being unavailable; the neighbourhood rule is this library's:
+// a cut cell with volume fraction under 1/2 merges with connected,
+// uncovered neighbours inside the domain, in decreasing order of
+// (m . o) / |o| (m = (ap_x(i+1) - ap_x(i), ...) points into the fluid, o is
+// the neighbour offset, ties in raster order) until the merged volume
+// fraction reaches 1/2 or 8 cells.  Then per neighbourhood the overlap-
+// weighted average of U* = U + dt dSdt_pre and its centroid, a limited
+// least-squares gradient, and per cell the average over the neighbourhoods
+// that hold it.  Conservative; every sum runs in a fixed order, so the
+// result is deterministic.
+constexpr int kSrdMax = 8;
+
+__device__ __forceinline__ int nb_count(unsigned long long w) { return int(w & 15ull); }
+__device__ __forceinline__ int nb_off(unsigned long long w, int c) {
+  return int((w >> (4 + 5 * c)) & 31ull);
+}
+__device__ __forceinline__ bool nb_holds(unsigned long long w, int o) {
+  const int n = nb_count(w);
+  for (int c = 0; c < n; ++c)
+    if (nb_off(w, c) == o) return true;
+  return false;
+}
+__device__ __forceinline__ void off3(int o, int& di, int& dj, int& dk) {
+  di = o % 3 - 1;
+  dj = (o / 3) % 3 - 1;
+  dk = o / 9 - 1;
+}
+
+// Neighbourhoods of the cells of grow(bx,4).
+__global__ void __launch_bounds__(kEB) k_srd_nbhd(Region r, EBWork W, EBG G, DBox din) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const int64_t at = W.s.idx(i, j, k);
+  const unsigned w = G.fl(i, j, k);
+  if (f_covered(w) || !din.has(i, j, k)) {
+    W.nb[at] = 0ull;
+    return;
+  }
+  unsigned long long out = 1ull | (13ull << 4);
+  if (f_single(w) && G.vf(i, j, k) < 0.5) {
+    const double m0 = G.a(0, i + 1, j, k) - G.a(0, i, j, k);
+    const double m1 = G.a(1, i, j + 1, k) - G.a(1, i, j, k);
+    const double m2 = G.a(2, i, j, k + 1) - G.a(2, i, j, k);
+    int cand[26];
+    double score[26];
+    int nc = 0;
+    for (int kk = -1; kk <= 1; ++kk)
+      for (int jj = -1; jj <= 1; ++jj)
+        for (int ii = -1; ii <= 1; ++ii) {
+          if (ii == 0 && jj == 0 && kk == 0) continue;
+          if (!f_conn(w, ii, jj, kk)) continue;
+          if (f_covered(G.fl(i + ii, j + jj, k + kk))) continue;
+          if (!din.has(i + ii, j + jj, k + kk)) continue;
+          const double len = sqrt(double(ii * ii + jj * jj + kk * kk));
+          const double sc = (m0 * ii + m1 * jj + m2 * kk) / len;
+          int pos = nc;
+          while (pos > 0 && score[pos - 1] < sc) {
+            score[pos] = score[pos - 1];
+            cand[pos] = cand[pos - 1];
+            --pos;
+          }
+          score[pos] = sc;
+          cand[pos] = (ii + 1) + 3 * (jj + 1) + 9 * (kk + 1);
+          ++nc;
+        }
+    double vol = G.vf(i, j, k);
+    int n = 1;
+    for (int c = 0; c < nc && vol < 0.5 && n < kSrdMax; ++c) {
+      int di, dj, dk;
+      off3(cand[c], di, dj, dk);
+      out |= (unsigned long long)(cand[c]) << (4 + 5 * n);
+      ++n;
+      vol += G.vf(i + di, j + dj, k + dk);
+    }
+    out = (out & ~15ull) | (unsigned long long)(n);
+  }
+  W.nb[at] = out;
+}
+
+// Overlap counts N on grow(bx,3).
+__global__ void __launch_bounds__(kEB) k_srd_count(Region r, EBWork W, EBG G, DBox din) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  if (f_covered(G.fl(i, j, k)) || !din.has(i, j, k)) {
+    W.nov[at] = 0.0;
+    return;
+  }
+  double cnt = 0.0;
+  for (int kk = -1; kk <= 1; ++kk)
+    for (int jj = -1; jj <= 1; ++jj)
+      for (int ii = -1; ii <= 1; ++ii)
+        if (nb_holds(W.nb[s.idx(i - ii, j - jj, k - kk)], (ii + 1) + 3 * (jj + 1) + 9 * (kk + 1)))
+          cnt += 1.0;
+  W.nov[at] = cnt;
+}
+
+// Neighbourhood volume, centroid and averaged state on grow(bx,2).
+__global__ void __launch_bounds__(kEB) k_srd_qhat(Region r, EBWork W, EBG G, DFab u, DtRef dtr) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  const unsigned long long nw = W.nb[at];
+  const int nn = nb_count(nw);
+  if (nn == 0) return;
+  const double dt = dtr.get();
+  double v = 0.0, x0 = 0.0, x1 = 0.0, x2 = 0.0;
+  double q[NVAR];
+  for (int n = 0; n < NVAR; ++n) q[n] = 0.0;
+  for (int c = 0; c < nn; ++c) {
+    int di, dj, dk;
+    off3(nb_off(nw, c), di, dj, dk);
+    const int a = i + di, b = j + dj, cc = k + dk;
+    const int64_t am = s.idx(a, b, cc);
+    const double w = G.vf(a, b, cc) / W.nov[am];
+    v += w;
+    x0 += w * (a + G.ce(0, a, b, cc));
+    x1 += w * (b + G.ce(1, a, b, cc));
+    x2 += w * (cc + G.ce(2, a, b, cc));
+    for (int n = 0; n < NVAR; ++n) q[n] += w * (u(a, b, cc, n) + dt * W.divc[am + n * s.sn]);
+  }
+  W.vhat[at] = v;
+  W.xhat[at] = x0 / v;
+  W.xhat[at + s.sn] = x1 / v;
+  W.xhat[at + 2 * s.sn] = x2 / v;
+  for (int n = 0; n < NVAR; ++n) W.qhat[at + n * s.sn] = q[n] / v;
+}
+
+// Limited least-squares gradients of merged neighbourhoods on grow(bx,1).
+__global__ void __launch_bounds__(kEB) k_srd_grad(Region r, EBWork W, EBG G) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  const Space& s = W.s;
+  const int64_t at = s.idx(i, j, k);
+  const unsigned long long nw = W.nb[at];
+  const int nn = nb_count(nw);
+  if (nn < 2) return;
+  const unsigned f = G.fl(i, j, k);
+  const double* XH = W.xhat;
+  const double xi0 = XH[at], xi1 = XH[at + s.sn], xi2 = XH[at + 2 * s.sn];
+  double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0;
+  for (int kk = -1; kk <= 1; ++kk)
+    for (int jj = -1; jj <= 1; ++jj)
+      for (int ii = -1; ii <= 1; ++ii) {
+        if ((ii == 0 && jj == 0 && kk == 0) || !f_conn(f, ii, jj, kk)) continue;
+        const int64_t ak = s.idx(i + ii, j + jj, k + kk);
+        if (nb_count(W.nb[ak]) == 0) continue;
+        const double d0 = XH[ak] - xi0;
+        const double d1 = XH[ak + s.sn] - xi1;
+        const double d2 = XH[ak + 2 * s.sn] - xi2;
+        a00 += d0 * d0; a01 += d0 * d1; a02 += d0 * d2;
+        a11 += d1 * d1; a12 += d1 * d2; a22 += d2 * d2;
+      }
+  const double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22,
+               c02 = a01 * a12 - a02 * a11;
+  const double det = a00 * c00 + a01 * c01 + a02 * c02;
+  const double c11 = a00 * a22 - a02 * a02, c12 = a01 * a02 - a00 * a12,
+               c22 = a00 * a11 - a01 * a01;
+  for (int n = 0; n < NVAR; ++n) {
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    if (fabs(det) > 1e-10) {
+      const double* QH = W.qhat + n * s.sn;
+      const double qi = QH[at];
+      double b0 = 0, b1 = 0, b2 = 0;
+      double qmin = qi, qmax = qi;
+      for (int kk = -1; kk <= 1; ++kk)
+        for (int jj = -1; jj <= 1; ++jj)
+          for (int ii = -1; ii <= 1; ++ii) {
+            if ((ii == 0 && jj == 0 && kk == 0) || !f_conn(f, ii, jj, kk)) continue;
+            const int64_t ak = s.idx(i + ii, j + jj, k + kk);
+            if (nb_count(W.nb[ak]) == 0) continue;
+            const double d0 = XH[ak] - xi0;
+            const double d1 = XH[ak + s.sn] - xi1;
+            const double d2 = XH[ak + 2 * s.sn] - xi2;
+            const double dq = QH[ak] - qi;
+            b0 += d0 * dq; b1 += d1 * dq; b2 += d2 * dq;
+            qmin = dmin(qmin, QH[ak]);
+            qmax = dmax(qmax, QH[ak]);
+          }
+      g0 = (c00 * b0 + c01 * b1 + c02 * b2) / det;
+      g1 = (c01 * b0 + c11 * b1 + c12 * b2) / det;
+      g2 = (c02 * b0 + c12 * b1 + c22 * b2) / det;
+      double alpha = 1.0;
+      for (int c = 0; c < nn; ++c) {
+        int di, dj, dk;
+        off3(nb_off(nw, c), di, dj, dk);
+        const int a = i + di, b = j + dj, cc = k + dk;
+        const double v = g0 * (a + G.ce(0, a, b, cc) - xi0) + g1 * (b + G.ce(1, a, b, cc) - xi1) +
+                         g2 * (cc + G.ce(2, a, b, cc) - xi2);
+        if (v > 0.0) alpha = dmin(alpha, (qmax - qi) / v);
+        else if (v < 0.0) alpha = dmin(alpha, (qmin - qi) / v);
+      }
+      g0 *= alpha;
+      g1 *= alpha;
+      g2 *= alpha;
+    }
+    W.grad[at + (3 * n) * s.sn] = g0;
+    W.grad[at + (3 * n + 1) * s.sn] = g1;
+    W.grad[at + (3 * n + 2) * s.sn] = g2;
+  }
+}
+
+// The redistributed state of each cell of bx, gathered from the
+// neighbourhoods that hold it (raster order), as a rate.
+__global__ void __launch_bounds__(kEB) k_srd_final(Region r, EBWork W, EBG G, DFab u,
+                                                    DtRef dtr, DFab dsdt) {
+  int i, j, k;
+  if (!region_cell(r, etid(), i, j, k)) return;
+  if (f_covered(G.fl(i, j, k))) {
+    for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = 0.0;
+    return;
+  }
+  const Space& s = W.s;
+  const double dt = dtr.get();
+  double acc[NVAR];
+  for (int n = 0; n < NVAR; ++n) acc[n] = 0.0;
+  const double cx = i + G.ce(0, i, j, k), cy = j + G.ce(1, i, j, k), cz = k + G.ce(2, i, j, k);
+  for (int kk = -1; kk <= 1; ++kk)
+    for (int jj = -1; jj <= 1; ++jj)
+      for (int ii = -1; ii <= 1; ++ii) {
+        const int64_t aa = s.idx(i + ii, j + jj, k + kk);
+        const unsigned long long nw = W.nb[aa];
+        if (!nb_holds(nw, (1 - ii) + 3 * (1 - jj) + 9 * (1 - kk))) continue;
+        if (nb_count(nw) < 2) {
+          for (int n = 0; n < NVAR; ++n) acc[n] += W.qhat[aa + n * s.sn];
+        } else {
+          const double x0 = cx - W.xhat[aa];
+          const double x1 = cy - W.xhat[aa + s.sn];
+          const double x2 = cz - W.xhat[aa + 2 * s.sn];
+          for (int n = 0; n < NVAR; ++n)
+            acc[n] += W.qhat[aa + n * s.sn] + (W.grad[aa + (3 * n) * s.sn] * x0 +
+                                               W.grad[aa + (3 * n + 1) * s.sn] * x1 +
+                                               W.grad[aa + (3 * n + 2) * s.sn] * x2);
+        }
+      }
+  const double nov = W.nov[s.idx(i, j, k)];
+  for (int n = 0; n < NVAR; ++n) dsdt(i, j, k, n) = (acc[n] / nov - u(i, j, k, n)) / dt;
+}
+
 // One EB hydro evaluation of box bx: the launch geometry of K1-K8 and the
 // workspace they share.  The workspace may be reused across evaluations of
 // the same box: every intermediate a kernel reads is rewritten by an
@@ -896,9 +1149,11 @@ struct EBPlan {
   int redist, wtype;
   bool mol;
   DtRef dt;                    // Godunov only
-  Region r5, r3, r2, r1, r0, rn, rf[3], ra[3];
+  Region rc, rsl, rd, rn, rf[3], ra[3];  // ctoprim, MOL slopes, divergence, div u nodes, faces
+  Region r4, r3, r2, r1, r0;              // grow(bx, 4..0): redistribution
+  DBox din;                                // inside the domain (non-periodic directions)
   int64_t ma;
-  Region rq, r4, rf1[3];       // Godunov: q box grow(bx,6), trace cells, first-pass faces
+  Region rq, rt, rf1[3];       // Godunov: q box, trace cells, first-pass faces
   Reg6E rf2;                   // Godunov: D|E faces
   int64_t mf1, mf2;
 };
@@ -918,12 +1173,15 @@ inline Space eb_space(const int bx_lo[3], const int bx_hi[3], int ng) {
 }
 
 constexpr int kEBCommonComps = SQ_N + 3 * NVAR + 3 * 2 + 1 + NVAR + 1 + 2 * NVAR + 1;
-inline int eb_work_comps(bool mol) {
-  return kEBCommonComps + (mol ? 3 * SL_N : 6 * ES_N + 9 * FR_N);
+constexpr int kEBSrdComps = 1 + 1 + 1 + 3 + NVAR + 3 * NVAR;
+inline int eb_work_comps(bool mol, bool srd) {
+  return kEBCommonComps + (mol ? 3 * SL_N : 6 * ES_N + 9 * FR_N) + (srd ? kEBSrdComps : 0);
 }
-inline int eb_grow(bool mol) { return mol ? 5 : 6; }
+// ghost cells: numGrow() (CAMR.H:465-479): 5 MOL / 6 Godunov with flux
+// redistribution, one more with state redistribution
+inline int eb_grow(bool mol, bool srd = false) { return (mol ? 5 : 6) + (srd ? 1 : 0); }
 
-inline void eb_carve(EBWork& W, double* base, bool mol) {
+inline void eb_carve(EBWork& W, double* base, bool mol, bool srd = false) {
   double* ptr = base;
   auto take = [&](int nc) {
     double* r = ptr;
@@ -946,6 +1204,12 @@ inline void eb_carve(EBWork& W, double* base, bool mol) {
   W.optmp = take(NVAR);
   W.delm = take(NVAR);
   W.wtinv = take(1);
+  W.nb = srd ? reinterpret_cast<unsigned long long*>(take(1)) : nullptr;
+  W.nov = srd ? take(1) : nullptr;
+  W.vhat = srd ? take(1) : nullptr;
+  W.xhat = srd ? take(3) : nullptr;
+  W.qhat = srd ? take(NVAR) : nullptr;
+  W.grad = srd ? take(3 * NVAR) : nullptr;
 }
 
 inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], const camr_geom& geom,
@@ -953,9 +1217,11 @@ inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], cons
                          DtRef dt) {
   E.mol = p.do_mol != 0;
   E.dt = dt;
-  E.W.s = eb_space(bx_lo, bx_hi, eb_grow(E.mol));
+  const int e = (redist == 2) ? 1 : 0;  // state redistribution: one more layer
+  E.W.s = eb_space(bx_lo, bx_hi, eb_grow(E.mol, e != 0));
   E.G.flag = eb.flag;
   E.G.vfrac = eb.vfrac;
+  E.G.cent = eb.cent;
   for (int d = 0; d < 3; ++d) {
     E.G.ap[d] = eb.ap[d];
     E.G.fc[d] = eb.fc[d];
@@ -970,6 +1236,8 @@ inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], cons
     E.g.dx[d] = geom.dx[d];
     E.db.lo[d] = geom.is_periodic[d] ? geom.dom_lo[d] - 2 : geom.dom_lo[d];
     E.db.hi[d] = geom.is_periodic[d] ? geom.dom_hi[d] + 2 : geom.dom_hi[d];
+    E.din.lo[d] = geom.is_periodic[d] ? -(1 << 29) : geom.dom_lo[d];
+    E.din.hi[d] = geom.is_periodic[d] ? (1 << 29) : geom.dom_hi[d];
   }
   E.P = make_kparams(p);
   E.redist = redist;
@@ -983,22 +1251,27 @@ inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], cons
     }
     return make_region(lo, hi);
   };
-  E.r5 = reg(5, -1, 0);
+  // the divergence runs on grow(bx, 2+e) (bxg_i, CAMR_construct_hydro_source.cpp:146-152);
+  // everything feeding it grows with it
+  E.rc = reg(5 + e, -1, 0);
+  E.rsl = reg(3 + e, -1, 0);
+  E.rd = reg(2 + e, -1, 0);
+  E.r4 = reg(4, -1, 0);
   E.r3 = reg(3, -1, 0);
   E.r2 = reg(2, -1, 0);
   E.r1 = reg(1, -1, 0);
   E.r0 = reg(0, -1, 0);
   E.ma = 0;
   for (int d = 0; d < 3; ++d) {
-    E.rf[d] = reg(2, d, 1);  // faces of grow(bx,2), transverse +1
-    E.ra[d] = reg(3, d, 0);  // faces of grow(bx,3)
+    E.rf[d] = reg(2 + e, d, 1);  // faces of grow(bx,2+e), transverse +1
+    E.ra[d] = reg(3 + e, d, 0);  // faces of grow(bx,3+e)
     E.ma = E.ra[d].count() > E.ma ? E.ra[d].count() : E.ma;
   }
-  // nodes of grow(bx,4) inside the domain grown by 16 in periodic directions
+  // nodes of grow(bx,4+e) inside the domain grown by 16 in periodic directions
   int nlo[3], nhi[3];
   for (int d = 0; d < 3; ++d) {
-    nlo[d] = bx_lo[d] - 4;
-    nhi[d] = bx_hi[d] + 5;
+    nlo[d] = bx_lo[d] - 4 - e;
+    nhi[d] = bx_hi[d] + 5 + e;
     const int glo = geom.is_periodic[d] ? geom.dom_lo[d] - 16 : geom.dom_lo[d];
     const int ghi = geom.is_periodic[d] ? geom.dom_hi[d] + 1 + 16 : geom.dom_hi[d] + 1;
     nlo[d] = nlo[d] > glo ? nlo[d] : glo;
@@ -1008,14 +1281,14 @@ inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], cons
   // Godunov regions (Godunov_3D_eb.cpp, bx_to_fill = grow(bx,2)): q on
   // grow(bx,6), traces on grow(bx,4), first-pass E-faces [lo-3, hi+4] x
   // grow(bx,4), D|E faces [lo-3, hi+4] x E in grow(bx,3) x F in grow(bx,4)
-  E.rq = reg(6, -1, 0);
-  E.r4 = reg(4, -1, 0);
+  E.rq = reg(6 + e, -1, 0);
+  E.rt = reg(4 + e, -1, 0);
   E.mf1 = E.mf2 = 0;
   for (int d = 0; d < 3; ++d) {
     int lo[3], hi[3];
     for (int a = 0; a < 3; ++a) {
-      lo[a] = bx_lo[a] - (a == d ? 3 : 4);
-      hi[a] = bx_hi[a] + 4;
+      lo[a] = bx_lo[a] - (a == d ? 3 : 4) - e;
+      hi[a] = bx_hi[a] + 4 + e;
     }
     E.rf1[d] = make_region(lo, hi);
     E.mf1 = E.rf1[d].count() > E.mf1 ? E.rf1[d].count() : E.mf1;
@@ -1025,7 +1298,7 @@ inline void eb_plan_init(EBPlan& E, const int bx_lo[3], const int bx_hi[3], cons
       if (Ed == D) continue;
       int lo[3], hi[3];
       for (int a = 0; a < 3; ++a) {
-        const int gr = (a == D) ? 3 : (a == Ed) ? 3 : 4;
+        const int gr = ((a == D) ? 3 : (a == Ed) ? 3 : 4) + e;
         lo[a] = bx_lo[a] - gr;
         hi[a] = bx_hi[a] + gr + (a == D ? 1 : 0);
       }
@@ -1042,12 +1315,12 @@ inline int eb_issue(const EBPlan& E, const DFab& U, const DFab& dsdt, const DFab
   int nk = 0;
   const EBWork& W = E.W;
   if (E.mol) {
-    k_eb_ctoprim<<<eblk(E.r5.count()), kEB, 0, st>>>(E.r5, W, E.G, U, E.P, nullptr);
-    k_eb_slope<<<dim3(eblk(E.r3.count()), 3), kEB, 0, st>>>(E.r3, W, E.G, E.P);
+    k_eb_ctoprim<<<eblk(E.rc.count()), kEB, 0, st>>>(E.rc, W, E.G, U, E.P, nullptr);
+    k_eb_slope<<<dim3(eblk(E.rsl.count()), 3), kEB, 0, st>>>(E.rsl, W, E.G, E.P);
     nk += 2;
   } else {
     k_eb_ctoprim<<<eblk(E.rq.count()), kEB, 0, st>>>(E.rq, W, E.G, U, E.P, nullptr);
-    k_ebc_trace<<<dim3(eblk(E.r4.count()), 3), kEB, 0, st>>>(E.r4, W, E.G, E.g, E.P, E.dt,
+    k_ebc_trace<<<dim3(eblk(E.rt.count()), 3), kEB, 0, st>>>(E.rt, W, E.G, E.g, E.P, E.dt,
                                                              E.rq);
     k_ebc_flux1<<<dim3(eblk(E.mf1), 3), kEB, 0, st>>>(E.rf1[0], E.rf1[1], E.rf1[2], W, E.G,
                                                        E.g, E.P);
@@ -1066,9 +1339,17 @@ inline int eb_issue(const EBPlan& E, const DFab& U, const DFab& dsdt, const DFab
                                                      E.ra[1], E.ra[2], W, E.G, E.g, E.P, U,
                                                      E.dt);
   }
-  k_eb_div<<<eblk(E.r2.count()), kEB, 0, st>>>(E.r2, W, E.G, E.g, E.P, fo[0], fo[1], fo[2],
+  k_eb_div<<<eblk(E.rd.count()), kEB, 0, st>>>(E.rd, W, E.G, E.g, E.P, fo[0], fo[1], fo[2],
                                                E.wtype);
   nk += 2;
+  if (E.redist == 2) {
+    k_srd_nbhd<<<eblk(E.r4.count()), kEB, 0, st>>>(E.r4, W, E.G, E.din);
+    k_srd_count<<<eblk(E.r3.count()), kEB, 0, st>>>(E.r3, W, E.G, E.din);
+    k_srd_qhat<<<eblk(E.r2.count()), kEB, 0, st>>>(E.r2, W, E.G, U, E.dt);
+    k_srd_grad<<<eblk(E.r1.count()), kEB, 0, st>>>(E.r1, W, E.G);
+    k_srd_final<<<eblk(E.r0.count()), kEB, 0, st>>>(E.r0, W, E.G, U, E.dt, dsdt);
+    return nk + 5;
+  }
   if (E.redist) {
     k_eb_redist1<<<eblk(E.r1.count()), kEB, 0, st>>>(E.r1, W, E.G, E.db);
     ++nk;
@@ -1333,9 +1614,9 @@ extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3
   if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   // Godunov with EB is PLM only (Source/CAMR.cpp:186-190)
   if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;
-  if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
+  if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 2)
     return CAMR_ERR_INVALID;
-  const int ng = eb_grow(p->do_mol != 0);
+  const int ng = eb_grow(p->do_mol != 0, redist == 2);
   for (int d = 0; d < 3; ++d) {
     if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
     if (uin->lo[d] > bx_lo[d] - ng || uin->hi[d] < bx_hi[d] + ng) return CAMR_ERR_INVALID;
@@ -1347,12 +1628,12 @@ extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   EBPlan E;
   eb_plan_init(E, bx_lo, bx_hi, *geom, *eb, *p, redist, DtRef{dt, nullptr});
-  const size_t bytes = size_t(eb_work_comps(E.mol)) * E.W.s.sn * sizeof(double);
+  const size_t bytes = size_t(eb_work_comps(E.mol, redist == 2)) * E.W.s.sn * sizeof(double);
   double* base = nullptr;
   if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess)
     return CAMR_ERR_NOMEM;
   cudaError_t e = cudaMemsetAsync(base, 0, bytes, st);
-  eb_carve(E.W, base, E.mol);
+  eb_carve(E.W, base, E.mol, redist == 2);
   // zero the output faces (covered cells leave theirs untouched)
   const DFab fo[3] = {make_dfab(*flx0), make_dfab(*flx1), make_dfab(*flx2)};
   int nk = 0;
@@ -1393,6 +1674,7 @@ struct camr_eb_level {
   DevError* err = nullptr;
   unsigned* flag = nullptr;
   double *vfrac = nullptr, *ap[3] = {nullptr, nullptr, nullptr}, *fc[3] = {nullptr, nullptr, nullptr};
+  double* cent = nullptr;
   EBG G;                          // the level's geometry view (flags for the guards)
   std::vector<EBPlan> plans;      // cut boxes: EB hydro, one workspace each
   std::vector<double*> plan_work;
@@ -1545,10 +1827,10 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   // sources are taken as zero, so no gravity with Godunov
   if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;
   if (!p->do_mol && p->add_grav_src && p->const_grav != 0.0) return CAMR_ERR_UNSUPPORTED;
-  if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 1)
+  if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 2)
     return CAMR_ERR_INVALID;
   const camr_geom& g = desc->geom;
-  const int ng = eb_grow(p->do_mol != 0);
+  const int ng = eb_grow(p->do_mol != 0, redist == 2);
   for (int d = 0; d < 3; ++d) {
     if (g.dom_hi[d] < g.dom_lo[d]) return CAMR_ERR_INVALID;
     if (!g.is_periodic[d] && (g.bc_lo[d] == CAMR_BC_INTERIOR || g.bc_hi[d] == CAMR_BC_INTERIOR))
@@ -1619,6 +1901,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   alloc(reinterpret_cast<void**>(&lev->err), sizeof(DevError));
   alloc(reinterpret_cast<void**>(&lev->flag), size_t(gc) * sizeof(unsigned));
   alloc(reinterpret_cast<void**>(&lev->vfrac), size_t(gc) * sizeof(double));
+  if (eb->cent) alloc(reinterpret_cast<void**>(&lev->cent), size_t(3 * gc) * sizeof(double));
   for (int d = 0; d < 3; ++d) {
     alloc(reinterpret_cast<void**>(&lev->ap[d]), size_t(gf[d]) * sizeof(double));
     alloc(reinterpret_cast<void**>(&lev->fc[d]), size_t(2 * gf[d]) * sizeof(double));
@@ -1629,6 +1912,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   };
   copy(lev->flag, eb->flag, size_t(gc) * sizeof(unsigned));
   copy(lev->vfrac, eb->vfrac, size_t(gc) * sizeof(double));
+  if (eb->cent) copy(lev->cent, eb->cent, size_t(3 * gc) * sizeof(double));
   for (int d = 0; d < 3; ++d) {
     copy(lev->ap[d], eb->ap[d], size_t(gf[d]) * sizeof(double));
     copy(lev->fc[d], eb->fc[d], size_t(2 * gf[d]) * sizeof(double));
@@ -1647,12 +1931,14 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   for (int d = 0; d < 3; ++d) {
     own.ap[d] = lev->ap[d];
     own.fc[d] = lev->fc[d];
+    own.cent = lev->cent;
     lev->G.lo[d] = eb->g_lo[d];
     lev->G.n[d] = gn[d];
     lev->G.ap[d] = lev->ap[d];
     lev->G.fc[d] = lev->fc[d];
   }
   lev->G.flag = lev->flag;
+  lev->G.cent = lev->cent;
   lev->G.vfrac = lev->vfrac;
   // classify the boxes (CAMR_construct_hydro_source.cpp:76-78, :150-153)
   auto typ = [&](int i, int j, int k) {
@@ -1676,9 +1962,11 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
       continue;
     }
     bool all_reg = true;
-    for (int k = b[2] - 2; k <= b[5] + 2 && all_reg; ++k)
-      for (int j = b[1] - 2; j <= b[4] + 2 && all_reg; ++j)
-        for (int i = b[0] - 2; i <= b[3] + 2; ++i)
+    // grow(box, 2), or 3 with state redistribution (CAMR_construct_hydro_source.cpp:146-153)
+    const int gb = (redist == 2) ? 3 : 2;
+    for (int k = b[2] - gb; k <= b[5] + gb && all_reg; ++k)
+      for (int j = b[1] - gb; j <= b[4] + gb && all_reg; ++j)
+        for (int i = b[0] - gb; i <= b[3] + gb; ++i)
           if (typ(i, j, k) != 0u) {
             all_reg = false;
             break;
@@ -1759,10 +2047,11 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
     EBPlan E;
     eb_plan_init(E, lo, hi, g, own, *p, redist, DtRef{0.0, lev->dt_cur});
     double* w = nullptr;
-    alloc(reinterpret_cast<void**>(&w), size_t(eb_work_comps(E.mol)) * E.W.s.sn * sizeof(double));
+    alloc(reinterpret_cast<void**>(&w),
+          size_t(eb_work_comps(E.mol, redist == 2)) * E.W.s.sn * sizeof(double));
     if (e != cudaSuccess) break;
     lev->plan_work.push_back(w);
-    eb_carve(E.W, w, E.mol);
+    eb_carve(E.W, w, E.mol, redist == 2);
     lev->plans.push_back(E);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
@@ -1781,7 +2070,8 @@ camr_status camr_eb_level_destroy(camr_eb_level* lev) {
   void* ptrs[] = {lev->S,       lev->S_old,   lev->B,      lev->dsdt,       lev->staging,
                   lev->fixed_dev, lev->dt_cur, lev->dt_hist, lev->bits,     lev->nstep,
                   lev->err,     lev->flag,    lev->vfrac,  lev->ap[0],      lev->ap[1],
-                  lev->ap[2],   lev->fc[0],   lev->fc[1],  lev->fc[2],      lev->regular_flx};
+                  lev->ap[2],   lev->fc[0],   lev->fc[1],  lev->fc[2],      lev->regular_flx,
+                  lev->cent};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (double* w : lev->plan_work)

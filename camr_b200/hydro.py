@@ -90,10 +90,12 @@ def eb_geometry_to_device(geo, device="cuda"):
     t = {"flag": torch.from_numpy(geo["flag"].astype(np.int32)).to(device),
          "vfrac": torch.from_numpy(geo["vfrac"]).to(device),
          "ap": [torch.from_numpy(a).to(device) for a in geo["ap"]],
-         "fc": [torch.from_numpy(a).contiguous().to(device) for a in geo["fc"]]}
+         "fc": [torch.from_numpy(a).contiguous().to(device) for a in geo["fc"]],
+         "cent": torch.from_numpy(np.ascontiguousarray(geo["cent"])).to(device)}
     g = native.EBGeom()
     g.flag = t["flag"].data_ptr()
     g.vfrac = t["vfrac"].data_ptr()
+    g.cent = t["cent"].data_ptr()
     for d in range(3):
         g.ap[d] = t["ap"][d].data_ptr()
         g.fc[d] = t["fc"][d].data_ptr()
@@ -103,7 +105,7 @@ def eb_geometry_to_device(geo, device="cuda"):
     return t
 
 
-def hydro_umdrv_eb(bx_lo, bx_hi, geom, uin, uin_lo, ebdev, params, redist=True, dt=0.0,
+def hydro_umdrv_eb(bx_lo, bx_hi, geom, uin, uin_lo, ebdev, params, redist=1, dt=0.0,
                    stream=None):
     """EB per-box hydro on CUDA tensors (MOL, or Godunov-PLM with do_mol = 0):
     uin (NVAR, ...) over a region starting at uin_lo covering grow(bx, 5)
@@ -125,7 +127,7 @@ def hydro_umdrv_eb(bx_lo, bx_hi, geom, uin, uin_lo, ebdev, params, redist=True, 
     check(lib().camr_hydro_umdrv_eb(C.byref(lo3), C.byref(hi3), C.byref(geom), C.byref(fu),
                                     C.byref(ebdev["struct"]), C.byref(fd), C.byref(ff[0]),
                                     C.byref(ff[1]), C.byref(ff[2]), C.byref(params),
-                                    int(bool(redist)), float(dt), C.c_void_p(_stream_ptr(stream))),
+                                    int(redist), float(dt), C.c_void_p(_stream_ptr(stream))),
           "camr_hydro_umdrv_eb")
     return dsdt, flx
 
@@ -224,8 +226,9 @@ class EBLevel:
     """One uniform level with an embedded boundary (MOL, or Godunov-PLM with
     do_mol = 0), advanced on the GPU through camr_eb_level_*.  geo:
     eb_geometry.sphere_geometry output over grow(domain, 5) for MOL,
-    grow(domain, 6) for Godunov (copied into the level).  redist: 1
-    FluxRedist, 0 NoRedist.  max_grid_size chops the domain into boxes."""
+    grow(domain, 6) for Godunov, one more layer with state redistribution
+    (copied into the level).  redist: 1 FluxRedist, 0 NoRedist, 2 StateRedist.
+    max_grid_size chops the domain into boxes."""
 
     def __init__(self, geom, params, geo, redist=1, max_grid_size=(0, 0, 0), use_graph=True,
                  stream=None):
@@ -241,10 +244,12 @@ class EBLevel:
         host = {"flag": np.ascontiguousarray(geo["flag"], dtype=np.uint32),
                 "vfrac": np.ascontiguousarray(geo["vfrac"], dtype=np.float64),
                 "ap": [np.ascontiguousarray(a, dtype=np.float64) for a in geo["ap"]],
-                "fc": [np.ascontiguousarray(a, dtype=np.float64) for a in geo["fc"]]}
+                "fc": [np.ascontiguousarray(a, dtype=np.float64) for a in geo["fc"]],
+                "cent": np.ascontiguousarray(geo["cent"], dtype=np.float64)}
         g = native.EBGeom()
         g.flag = host["flag"].ctypes.data
         g.vfrac = host["vfrac"].ctypes.data
+        g.cent = host["cent"].ctypes.data
         for d in range(3):
             g.ap[d] = host["ap"][d].ctypes.data
             g.fc[d] = host["fc"][d].ctypes.data

@@ -54,7 +54,8 @@ class BoxTask(C.Structure):
 
 class EBGeom(C.Structure):
     _fields_ = [("flag", C.c_void_p), ("vfrac", C.c_void_p), ("ap", C.c_void_p * 3),
-                ("fc", C.c_void_p * 3), ("g_lo", C.c_int * 3), ("g_hi", C.c_int * 3)]
+                ("fc", C.c_void_p * 3), ("g_lo", C.c_int * 3), ("g_hi", C.c_int * 3),
+                ("cent", C.c_void_p)]
 
 
 class LevelDesc(C.Structure):

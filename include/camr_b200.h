@@ -366,7 +366,9 @@ camr_status camr_adjoint_get_error(camr_adjoint* a, camr_error_info* info);
  *          same faces, component planes outermost.
  * uin covers grow(bx, ng).  dsdt (bx) is overwritten (the reference's
  * redistribution writes it); flx[d] receive the face-centroid fluxes of
- * bx's faces.  redist: 1 = flux redistribution, 0 = none.
+ * bx's faces.  redist: 1 = flux redistribution, 0 = none, 2 = state
+ * redistribution (Berger & Giuliani's method, restated: AMReX's own is not
+ * the reference's code; ng grows by one).
  */
 typedef struct {
   const unsigned* flag;
@@ -375,6 +377,8 @@ typedef struct {
   const double* fc[3];
   int g_lo[3];
   int g_hi[3];
+  const double* cent;  /* cell-centroid offsets, 3 comps on G (may be NULL:
+                          cell centres); read by state redistribution */
 } camr_eb_geom;
 
 camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3], const camr_geom* geom,
@@ -390,12 +394,13 @@ camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3], const ca
  * for covered cells), 5 ghost cells for MOL, 6 for Godunov.  desc->max_grid_size
  * chops the domain into boxes (0 = one box): as in an EB build's
  * construct_hydro_source, covered boxes are skipped, boxes whose grow(box,2)
- * is all regular run the regular hydro (one batched launch per stage for
- * all of them) and the others the EB hydro.  eb: geometry over exactly grow(domain, 5), host or
- * device memory, copied into the level (grow(domain, 6) for Godunov).
- * Godunov requires ppm_type = 0 (Source/CAMR.cpp:186-190) and no gravity
- * source.  redist: 0 NoRedist, 1 FluxRedist
- * (StateRedist is not provided: CAMR_ERR_INVALID).  Covered cells hold zero
+ * (grow(box,3) with state redistribution) is all regular run the regular
+ * hydro (one batched launch per stage for all of them) and the others the
+ * EB hydro.  eb: geometry over exactly grow(domain, ng), host or device
+ * memory, copied into the level; ng = 5 for MOL, 6 for Godunov, one more
+ * with state redistribution.  Godunov requires ppm_type = 0
+ * (Source/CAMR.cpp:186-190) and no gravity source.  redist: 0 NoRedist,
+ * 1 FluxRedist, 2 StateRedist (restated method).  Covered cells hold zero
  * state (initData's EB_set_covered); set_state/get_state/advance/dts as
  * for camr_level_*.
  */

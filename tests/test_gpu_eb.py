@@ -178,3 +178,68 @@ def test_eb_level_init_finalize_matches_oracle():
     L.init_finalize()
     assert_bitwise(L.get_state(), ref, "state")
     L.close()
+
+
+@pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
+@pytest.mark.parametrize("case", ["periodic_box", "sod_sphere"])
+@pytest.mark.parametrize("do_mol", [1, 0])
+def test_eb_box_state_redistribution_matches_oracle(case, do_mol):
+    """State redistribution (redist = 2) per box, bit for bit."""
+    torch = _torch()
+    ng = (5 if do_mol else 6) + 1
+    geo, G, g_lo, lo, hi, geom, dlo, dhi, per, bclo, bchi, dx = (
+        periodic_case(ng=ng) if case == "periodic_box" else sod_sphere_case(ng=ng))
+    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
+    dt = 2e-3
+    ref_d, ref_f, nass = oracle.hydro_box_eb(p, lo, hi, dlo, dhi, bclo, bchi, per, G, g_lo, geo,
+                                             (dx,) * 3, dt, redist=2)
+    assert nass == 0
+    ebdev = hydro.eb_geometry_to_device(geo)
+    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
+    d, f = hydro.hydro_umdrv_eb(lo, hi, geom, torch.from_numpy(G).cuda(), g_lo, ebdev, prm,
+                                redist=2, dt=dt)
+    torch.cuda.synchronize()
+    assert_bitwise(d.cpu().numpy(), ref_d, "dsdt")
+    for dd in range(3):
+        assert_bitwise(f[dd].cpu().numpy(), ref_f[dd], f"flux {dd}")
+
+
+@pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
+@pytest.mark.parametrize("kind,mgs,do_mol", [("sod", (8, 8, 8), 1), ("sod", (8, 8, 8), 0),
+                                             ("periodic", (0, 0, 0), 1)])
+def test_eb_level_state_redistribution_matches_oracle(kind, mgs, do_mol):
+    """EB level steps with state redistribution against the oracle."""
+    _torch()
+    n = (16, 16, 16) if kind == "periodic" else (32, 16, 16)
+    ng = (5 if do_mol else 6) + 1
+    if kind == "periodic":
+        dx = 1.0 / n[0]
+        geo = E.sphere_geometry((-ng,) * 3, tuple(v + ng - 1 for v in n), dx, radius=0.2)
+        s = P.random_smooth(n, seed=5, amp=0.1, vel=0.2)
+        lev = oracle.make_level(n, dx=(dx,) * 3, max_grid_size=mgs)
+        geom = hydro.make_geom(n, dx=(dx,) * 3)
+    else:
+        dx = 2.0 / n[0]
+        geo = E.sphere_geometry((-ng,) * 3, tuple(v + ng - 1 for v in n), dx,
+                                center=(1.0, 0.5, 0.5), radius=0.15)
+        s = P.sod_sphere(n, (dx,) * 3, geo)
+        lev = oracle.make_level(n, periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
+                                dx=(dx,) * 3, max_grid_size=mgs)
+        geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
+                               dx=(dx,) * 3)
+    s = np.ascontiguousarray(E.set_covered(s, geo))
+    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
+    oracle.eb_init_finalize(p, lev, s)
+    ref = s.copy()
+    nsteps = 5
+    _, ref_dts, nass = oracle.eb_advance(p, lev, geo, ref, nsteps, redist=2)
+    assert nass == 0
+    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
+    L = hydro.EBLevel(geom, prm, geo, redist=2, max_grid_size=mgs)
+    L.set_state(s)
+    L.advance(nsteps)
+    got = L.get_state()
+    assert L.error()[0] == 0
+    assert_bitwise(L.dts(), ref_dts, "dt")
+    assert_bitwise(got, ref, "state")
+    L.close()
