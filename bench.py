@@ -613,33 +613,36 @@ def eb_comparison(args, n=(256, 128, 128), nsteps=None, warmup=3, cpu_n=(64, 32,
     out["regular_level_same_domain"] = {"ms_per_step": msr,
                                         "zone_updates_per_s": zones / (msr * 1e-3)}
     out["eb_over_regular_time"] = ms / msr
-    # Godunov-PLM (CTU) with the same geometry, 32^3 boxes (6 ghost cells)
+    # with the same geometry and 32^3 boxes: Godunov-PLM (CTU, 6 ghost
+    # cells) and MOL with state redistribution (6 ghost cells)
     geo6 = eb_geometry.sphere_geometry((-6, -6, -6), (n[0] + 5, n[1] + 5, n[2] + 5), dx,
                                        center=(1.0, 0.5, 0.5), radius=0.15)
-    prm_ctu = native.default_params(do_mol=0, ppm_type=0, cfl=0.3)
-    L = hydro.EBLevel(geom, prm_ctu, geo6, redist=1, max_grid_size=(32, 32, 32))
-    st = L.torch_stream()
-    L.set_state(s0)
-    L.init_finalize()
-    L.advance(1)
-    L.autotune()
-    L.advance(warmup)
-    torch.cuda.synchronize()
-    e0.record(st)
-    L.advance(nsteps)
-    e1.record(st)
-    torch.cuda.synchronize()
-    msc = e0.elapsed_time(e1) / nsteps
-    fin = L.get_state()
-    out["eb_level_godunov_plm"] = {"ms_per_step": msc, "zone_updates_per_s": zones / (msc * 1e-3),
-                                   "steps": nsteps, "max_grid_size": [32, 32, 32],
-                                   "kernels_per_step_graph": L.kernels_per_step(),
-                                   "boxes": L.boxes(), "device_error": list(L.error()),
-                                   "t_final": float(L.dts().sum()),
-                                   "finite": bool(np.isfinite(fin).all())}
-    L.close()
-    del L
-    torch.cuda.empty_cache()
+    for key, kw, redist in (("eb_level_godunov_plm", dict(do_mol=0, ppm_type=0), 1),
+                            ("eb_level_state_redist", dict(do_mol=1, ppm_type=0), 2)):
+        L = hydro.EBLevel(geom, native.default_params(cfl=0.3, **kw), geo6, redist=redist,
+                          max_grid_size=(32, 32, 32))
+        st = L.torch_stream()
+        L.set_state(s0)
+        L.init_finalize()
+        L.advance(1)
+        L.autotune()
+        L.advance(warmup)
+        torch.cuda.synchronize()
+        e0.record(st)
+        L.advance(nsteps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        msc = e0.elapsed_time(e1) / nsteps
+        fin = L.get_state()
+        out[key] = {"ms_per_step": msc, "zone_updates_per_s": zones / (msc * 1e-3),
+                    "steps": nsteps, "max_grid_size": [32, 32, 32], "redist": redist,
+                    "kernels_per_step_graph": L.kernels_per_step(),
+                    "boxes": L.boxes(), "device_error": list(L.error()),
+                    "t_final": float(L.dts().sum()),
+                    "finite": bool(np.isfinite(fin).all())}
+        L.close()
+        del L
+        torch.cuda.empty_cache()
     R.close()
     del R
     torch.cuda.empty_cache()
