@@ -353,6 +353,22 @@ camr_status camr_batch_tuning(camr_batch* b, int* chunk, unsigned* grid, int n) 
   return CAMR_OK;
 }
 
+camr_status camr_batch_set_tuning(camr_batch* b, const int* chunk, const unsigned* grid, int n) {
+  if (!b || !chunk || !grid || n < BS_COUNT) return CAMR_ERR_INVALID;
+  int ix[BS_COUNT];
+  for (int s = 0; s < BS_COUNT; ++s) {
+    ix[s] = -1;
+    for (int ci = 0; ci < kNChunk; ++ci)
+      if (kChunks[ci] == chunk[s]) ix[s] = ci;
+    if (ix[s] < 0) return CAMR_ERR_INVALID;
+  }
+  for (int s = 0; s < BS_COUNT; ++s) {
+    b->chunk_ix[s] = ix[s];
+    b->grid[s] = grid[s];
+  }
+  return CAMR_OK;
+}
+
 camr_status camr_hydro_umdrv_batched(int nbox, const camr_box_task* tasks,
                                      const camr_geom* geom, const camr_hydro_params* p,
                                      double dt, void* stream) {

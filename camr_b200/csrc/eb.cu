@@ -2030,12 +2030,17 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
     }
   }
   // cut boxes: one EB plan and workspace each, spread over side streams
+  // at the device's greatest priority: a cut box's chain of small launches
+  // is the critical path of a hydro stage, so its blocks go first whenever
+  // the regular boxes' blocks retire
   const int nside = int(std::min<size_t>(cut_boxes.size(), 8));
+  int prio_least = 0, prio_greatest = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
   if (e == cudaSuccess && nside > 0) e = cudaEventCreateWithFlags(&lev->ev_fork, cudaEventDisableTiming);
   for (int i = 0; i < nside && e == cudaSuccess; ++i) {
     cudaStream_t s2;
     cudaEvent_t ej;
-    e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, prio_greatest);
     if (e != cudaSuccess) break;
     lev->side.push_back(s2);
     e = cudaEventCreateWithFlags(&ej, cudaEventDisableTiming);
@@ -2183,9 +2188,64 @@ camr_status camr_eb_level_autotune(camr_eb_level* lev) {
                                   lev->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
   if (e != cudaSuccess) return cuda_status_of(e);
-  const camr_status cs = camr_batch_autotune(lev->regular, dt, lev->stream);
+  constexpr int NS = BS_COUNT;
+  int chunk[3][NS];
+  unsigned grid[3][NS];
+  // candidate 2: the untuned shapes
+  camr_status cs = camr_batch_tuning(lev->regular, chunk[2], grid[2], NS);
+  if (cs == CAMR_OK) cs = camr_batch_autotune(lev->regular, dt, lev->stream);
+  if (cs == CAMR_OK) cs = camr_batch_tuning(lev->regular, chunk[0], grid[0], NS);
+  if (cs != CAMR_OK) return cs;
+  // candidate 0: each stage timed alone; candidate 1: the same cells per
+  // block with one block per work unit, which leaves SMs free for the cut
+  // boxes' launches on the side streams as blocks retire
+  for (int s = 0; s < NS; ++s) {
+    chunk[1][s] = chunk[0][s];
+    grid[1][s] = 0;
+  }
+  // a whole hydro stage (dSdt zeroed, then regular and cut boxes) only reads
+  // Sborder, so it can be repeated; it is timed as a captured graph, the
+  // form the level's steps take: one untimed launch, the best of three
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_c = 0;
+  for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+    camr_batch_set_tuning(lev->regular, chunk[c], grid[c], NS);
+    int nk = 0;
+    cudaGraph_t gr = nullptr;
+    cudaGraphExec_t gx = nullptr;
+    e = cudaStreamBeginCapture(lev->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) break;
+    const int64_t before = launches_now();
+    const cudaError_t e1c = eb_hydro_stage(lev, lev->stream, &nk);
+    launches_sub(launches_now() - before);
+    e = cudaStreamEndCapture(lev->stream, &gr);
+    if (e == cudaSuccess) e = e1c;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gx, gr, 0);
+    if (gr) cudaGraphDestroy(gr);
+    if (e == cudaSuccess) e = cudaGraphLaunch(gx, lev->stream);
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+      cudaEventRecord(e0, lev->stream);
+      e = cudaGraphLaunch(gx, lev->stream);
+      cudaEventRecord(e1, lev->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (e == cudaSuccess && ms < best) {
+        best = ms;
+        best_c = c;
+      }
+    }
+    if (gx) cudaGraphExecDestroy(gx);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  camr_batch_set_tuning(lev->regular, chunk[best_c], grid[best_c], NS);
+  if (e != cudaSuccess) return cuda_status_of(e);
   // a captured step holds the old launch shapes
-  if (cs == CAMR_OK && lev->graph_ready) {
+  if (lev->graph_ready) {
     cudaGraphExecDestroy(lev->graph);
     lev->graph_ready = false;
   }

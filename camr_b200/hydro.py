@@ -382,6 +382,14 @@ class Batch:
                  "mol_flux", "consup"]
         return {n: (int(c) * 128, int(g)) for n, c, g in zip(names, ch, gr)}
 
+    def set_tuning(self, tuning):
+        """Set the launch shapes, as tuning() returns them."""
+        names = ["ctoprim", "flatten_divu", "trace", "flux1", "flux2", "flux3", "mol_slope",
+                 "mol_flux", "consup"]
+        ch = (C.c_int * 9)(*[tuning[n][0] // 128 for n in names])
+        gr = (C.c_uint * 9)(*[tuning[n][1] for n in names])
+        check(lib().camr_batch_set_tuning(self._h, ch, gr, 9), "camr_batch_set_tuning")
+
     def close(self):
         if self._h:
             lib().camr_batch_destroy(self._h)

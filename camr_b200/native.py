@@ -111,6 +111,8 @@ SIGNATURES = {
     "camr_batch_autotune": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
     "camr_batch_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint),
                                     C.c_int]),
+    "camr_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint),
+                                        C.c_int]),
     "camr_hydro_umdrv_batched": (C.c_int, [C.c_int, C.POINTER(BoxTask), C.POINTER(Geom),
                                            C.POINTER(HydroParams), C.c_double, C.c_void_p]),
     "camr_amr_create": (C.c_int, [C.POINTER(LevelDesc), C.c_int, C.c_void_p,

@@ -183,6 +183,10 @@ camr_status camr_batch_run(camr_batch* b, double dt, const double* dt_dev,
 camr_status camr_batch_autotune(camr_batch* b, double dt, void* stream);
 /* The chosen cells-per-block factor and grid of each stage (n >= 9). */
 camr_status camr_batch_tuning(camr_batch* b, int* chunk, unsigned* grid, int n);
+/* Set every stage's cells-per-block factor (1, 2 or 4: 128/256/512 cells) and
+ * grid (0 = one block per work unit, else a persistent grid of that many
+ * blocks), in camr_batch_tuning's order (n >= 9). */
+camr_status camr_batch_set_tuning(camr_batch* b, const int* chunk, const unsigned* grid, int n);
 /* One-shot convenience: create, run persistent, destroy (synchronises). */
 camr_status camr_hydro_umdrv_batched(int nbox, const camr_box_task* tasks,
                                      const camr_geom* geom,
@@ -418,9 +422,12 @@ camr_status camr_eb_level_init_finalize(camr_eb_level* lev);
 camr_status camr_eb_level_advance(camr_eb_level* lev, int nsteps, const double* fixed_dts);
 /* The dt of every step taken since creation (at most n), and their count. */
 camr_status camr_eb_level_dts(camr_eb_level* lev, double* dts, int n, int* nsteps);
-/* Time the regular boxes' batched stages on the level's current Sborder and
- * keep the fastest launch shapes (camr_batch_autotune); call after a step.
- * Synchronises. */
+/* Tune the launch shapes of the regular boxes' batched stages on the
+ * level's current Sborder; call after a step.  Each stage is first timed
+ * alone (camr_batch_autotune); then whole hydro stages, regular and cut boxes
+ * running together as one captured graph, are timed with that choice, with
+ * the same choice on non-persistent grids, and with the untuned shapes, and
+ * the fastest is kept.  Synchronises. */
 camr_status camr_eb_level_autotune(camr_eb_level* lev);
 /* How the level's boxes were classified: all-regular grow(box,2) (regular
  * hydro), cut (EB hydro), covered (skipped). */
