@@ -312,7 +312,7 @@ __device__ __forceinline__ FluxPtrs fine_fluxes(const FineDev& F, const FinePool
 
 // CTU fine update: S = Sborder (+ dt*src_old) + dt*dSdt, then the step's
 // clean_states and post_timestep's (the finest level cleans its own).
-__global__ void __launch_bounds__(kBlk) kf_update_ctu(FineDev F, FinePools fpool, KParams P,
+__global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) kf_update_ctu(FineDev F, FinePools fpool, KParams P,
                                                        const double* dtp, const double* B,
                                                        const double* S_old, double* S,
                                                        unsigned long long* bits, DevError* err) {
@@ -324,7 +324,13 @@ __global__ void __launch_bounds__(kBlk) kf_update_ctu(FineDev F, FinePools fpool
     const int64_t o = F.off[b];
     double s[NVAR], sold[NVAR], hs[NVAR];
     load_cell(B + o, L, at, s);
-    load_cell(S_old + o, L, at, sold);
+    // the gravity terms read only the old density and z momentum
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) sold[n] = 0.0;
+    if (P.add_grav_src) {
+      sold[URHO] = S_old[o + at + URHO * L.sn];
+      sold[UMZ] = S_old[o + at + UMZ * L.sn];
+    }
     if (P.add_grav_src) {
       double src[NVAR];
 #pragma unroll
@@ -370,7 +376,7 @@ __global__ void __launch_bounds__(kBlk) kf_update_mol1(FineDev F, FinePools fpoo
   store_cell(S + o, L, at, s);
 }
 
-__global__ void __launch_bounds__(kBlk) kf_update_mol2(FineDev F, FinePools fpool, KParams P,
+__global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) kf_update_mol2(FineDev F, FinePools fpool, KParams P,
                                                         const double* dtp, const double* B2,
                                                         const double* S_old, double* S,
                                                         unsigned long long* bits, DevError* err) {

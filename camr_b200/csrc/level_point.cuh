@@ -15,6 +15,12 @@ namespace camr {
 namespace {
 
 constexpr int kBlk = 256;
+// resident 256-thread blocks per SM asked of the end-of-step update kernels:
+// with 3 (at most 85 registers) the 256^3 CTU update took 1.98 ms against
+// 2.68 ms with 4 (64 registers, spills) and 3.20 ms uncapped (76 registers)
+#ifndef CAMR_MINB_UPDATE
+#define CAMR_MINB_UPDATE 3
+#endif
 inline unsigned grid_of(int64_t n) { return unsigned((n + kBlk - 1) / kBlk); }
 __device__ __forceinline__ int64_t tid() { return int64_t(blockIdx.x) * blockDim.x + threadIdx.x; }
 
@@ -414,7 +420,7 @@ struct FluxPtrs {
 };
 
 // CTU: S_new = Sborder (+ dt*src_old) + dt*dSdt, then finish_step.
-__global__ void __launch_bounds__(kBlk) k_update_ctu(LGeom L, Space sp, KParams P,
+__global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) k_update_ctu(LGeom L, Space sp, KParams P,
                                                       const double* dtp, const double* B,
                                                       const double* S_old, FluxPtrs fp,
                                                       double* S, unsigned long long* bits,
@@ -426,7 +432,14 @@ __global__ void __launch_bounds__(kBlk) k_update_ctu(LGeom L, Space sp, KParams 
     const int64_t at = L.idx(i, j, k);
     double s[NVAR], sold[NVAR], hs[NVAR];
     load_cell(B, L, at, s);
-    load_cell(S_old, L, at, sold);
+    // the old-time source and its correction in finish_step read only the
+    // old density and z momentum
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) sold[n] = 0.0;
+    if (P.add_grav_src) {
+      sold[URHO] = S_old[at + URHO * L.sn];
+      sold[UMZ] = S_old[at + UMZ * L.sn];
+    }
     if (P.add_grav_src) {
       double src[NVAR];
 #pragma unroll
@@ -473,7 +486,7 @@ __global__ void __launch_bounds__(kBlk) k_update_mol1(LGeom L, Space sp, KParams
 
 // MOL stage 2: S_new = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2 (LinComb then
 // Saxpy, CAMR_advance.cpp:134-135), then finish_step.
-__global__ void __launch_bounds__(kBlk) k_update_mol2(LGeom L, Space sp, KParams P,
+__global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) k_update_mol2(LGeom L, Space sp, KParams P,
                                                        const double* dtp, const double* B2,
                                                        const double* S_old, FluxPtrs fp,
                                                        double* S, unsigned long long* bits,
