@@ -187,11 +187,15 @@ __device__ __forceinline__ ROut hllc(double rl_in, double ul, double vl, double 
 // place at a physical-boundary face exactly as the reference modifies its
 // state arrays (:239-282).  f[UTEMP] is left at 0 (flux arrays start from
 // setVal(0), CAMR_construct_hydro_source.cpp:88).
+//
+// cmpflx_core does all but the species: the boundary edits, the Riemann
+// solve and every non-species flux component; species_flux then upwinds the
+// species edge states by the sign of ustar, one branch for all species.
 template <int dir>
-__device__ __forceinline__ void cmpflx(double* ql, double* qr, const CellAux& aL,
-                                       const CellAux& aR, int idx, int bclo, int bchi,
-                                       int domlo, int domhi, const KParams& P, double* f,
-                                       double& q_pres, double& q_un) {
+__device__ __forceinline__ ROut cmpflx_core(double* ql, double* qr, const CellAux& aL,
+                                            const CellAux& aR, int idx, int bclo, int bchi,
+                                            int domlo, int domhi, const KParams& P,
+                                            double* f) {
   constexpr int iu = ES_U + dir;
   constexpr int iv = (dir == 0) ? ES_V : ES_U;
   constexpr int iv2 = (dir == 2) ? ES_V : ES_W;
@@ -256,17 +260,35 @@ __device__ __forceinline__ void cmpflx(double* ql, double* qr, const CellAux& aL
   f[UEDEN] = o.f_eden;
   f[UEINT] = o.f_eint;
   f[UTEMP] = 0.0;
+  return o;
+}
+
+// Species fluxes of cmpflx (Hydro_cmpflx.H:289-301): the left (ustar > 0),
+// right (ustar < 0) or mean (ustar exactly 0, or NaN) species edge states
+// times the mass flux.
+__device__ __forceinline__ void species_flux(const ROut& o, double* f, const double* ql,
+                                             const double* qr) {
   const double flxrho = f[URHO];
+  if (o.ustar > 0.0) {
 #pragma unroll
-  for (int s = 0; s < NSPEC; ++s) {
-    if (o.ustar > 0.0) {
-      f[UFS + s] = flxrho * ql[ES_FS + s];
-    } else if (o.ustar < 0.0) {
-      f[UFS + s] = flxrho * qr[ES_FS + s];
-    } else {
-      f[UFS + s] = flxrho * 0.50 * (ql[ES_FS + s] + qr[ES_FS + s]);
-    }
+    for (int n = 0; n < NSPEC; ++n) f[UFS + n] = flxrho * ql[ES_FS + n];
+  } else if (o.ustar < 0.0) {
+#pragma unroll
+    for (int n = 0; n < NSPEC; ++n) f[UFS + n] = flxrho * qr[ES_FS + n];
+  } else {
+#pragma unroll
+    for (int n = 0; n < NSPEC; ++n)
+      f[UFS + n] = flxrho * 0.50 * (ql[ES_FS + n] + qr[ES_FS + n]);
   }
+}
+
+template <int dir>
+__device__ __forceinline__ void cmpflx(double* ql, double* qr, const CellAux& aL,
+                                       const CellAux& aR, int idx, int bclo, int bchi,
+                                       int domlo, int domhi, const KParams& P, double* f,
+                                       double& q_pres, double& q_un) {
+  const ROut o = cmpflx_core<dir>(ql, qr, aL, aR, idx, bclo, bchi, domlo, domhi, P, f);
+  species_flux(o, f, ql, qr);
   q_pres = o.q_pres;
   q_un = o.q_un;
 }
