@@ -25,6 +25,7 @@ BCSETS = {
     "periodic": dict(periodic=(1, 1, 1), bc_lo=(0, 0, 0), bc_hi=(0, 0, 0)),
     "walls": dict(periodic=(0, 1, 0), bc_lo=(2, 0, 4), bc_hi=(2, 0, 5)),
     "sym": dict(periodic=(0, 0, 0), bc_lo=(3, 5, 2), bc_hi=(4, 2, 3)),
+    "inflow": dict(periodic=(0, 1, 0), bc_lo=(1, 0, 4), bc_hi=(2, 0, 1)),
 }
 
 
@@ -97,6 +98,51 @@ def test_hydro_umdrv_box(cfg, bcs, oracle_kind, native_lib):
     assert_bitwise(dsdt.cpu().numpy(), dsdt_o, "dsdt")
 
 
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_hydro_umdrv_subbox(cfg, oracle_kind, native_lib):
+    """Per-box hydro on a 13x10x9 box inside a 24x20x18 domain whose index
+    space starts at (-3, 2, 0): the box touches only the z-low wall, so the
+    other faces read ghost cells that are interior cells of the level."""
+    torch = _torch()
+    from camr_b200 import hydro, native
+    n = (24, 20, 18)
+    dlo = (-3, 2, 0)
+    bcs = dict(periodic=(0, 1, 0), bc_lo=(1, 0, 4), bc_hi=(2, 0, 5))
+    lev = oracle.make_level(n, lo=dlo, **bcs)
+    p_or = oracle.default_params(**CONFIGS[cfg])
+    s = P.random_smooth(n, seed=23)
+    oracle.init_finalize(oracle_kind, p_or, lev, s)
+    border = oracle.expand_state(oracle_kind, p_or, lev, s)
+    uin_lo = [dlo[d] - 4 for d in range(3)]
+    dt = 0.5 * oracle.est_dt(oracle_kind, p_or, lev, s)
+    lo = [2, 5, 0]
+    hi = [14, 14, 8]
+    nb = [hi[d] - lo[d] + 1 for d in range(3)]
+    dsdt_o, flx_o, nass = oracle.hydro_box(oracle_kind, p_or, lo, hi, list(dlo),
+                                           [dlo[d] + n[d] - 1 for d in range(3)],
+                                           list(lev.bc_lo), list(lev.bc_hi), border, uin_lo,
+                                           list(lev.dx), dt)
+    assert nass == 0
+
+    geom = hydro.make_geom(n, dom_lo=dlo, is_periodic=bcs["periodic"], bc_lo=bcs["bc_lo"],
+                           bc_hi=bcs["bc_hi"], dx=tuple(lev.dx))
+    prm = native.default_params(**CONFIGS[cfg])
+    dev = torch.device("cuda:0")
+    uin = torch.from_numpy(border).to(dev)
+    dsdt = torch.zeros((10, nb[2], nb[1], nb[0]), dtype=torch.float64, device=dev)
+    flx = []
+    for d in range(3):
+        sh = list(nb)
+        sh[d] += 1
+        flx.append(torch.full((10, sh[2], sh[1], sh[0]), float("nan"), dtype=torch.float64,
+                              device=dev))
+    hydro.hydro_umdrv(lo, hi, geom, uin, uin_lo, dsdt, flx, prm, dt)
+    torch.cuda.synchronize()
+    for d in range(3):
+        assert_bitwise(flx[d].cpu().numpy(), flx_o[d], f"flux {d}")
+    assert_bitwise(dsdt.cpu().numpy(), dsdt_o, "dsdt")
+
+
 def _level_run(kind, cfg, n, bcs, state0, nsteps, use_graph=True, max_grid=(0, 0, 0)):
     from camr_b200 import hydro, native
     p_or = oracle.default_params(**cfg)
@@ -157,6 +203,22 @@ def test_level_mol_walls(oracle_kind, native_lib):
     bcs = dict(periodic=(0, 1, 0), bc_lo=(3, 0, 4), bc_hi=(5, 0, 2))
     s_or, hist, s_gpu, dt_last, err = _level_run(oracle_kind, dict(do_mol=1, cfl=0.3), n, bcs,
                                                  s0, 6)
+    assert err[0] == 0, err
+    assert dt_last == hist[-1]
+    assert_bitwise(s_gpu, s_or, "state")
+
+
+@pytest.mark.parametrize("cfg", ["ctu_ppm", "mol_plm"])
+def test_level_inflow(cfg, oracle_kind, native_lib):
+    """Level steps with an inflow face (ghosts copy the boundary cell, as the
+    Sod problem's bcnormal does), outflow opposite, a slip and a no-slip
+    wall in z, and 4^3-ish boxes of max_grid_size 8."""
+    _torch()
+    n = (20, 12, 16)
+    s0 = P.random_smooth(n, seed=5)
+    bcs = dict(periodic=(0, 1, 0), bc_lo=(1, 0, 4), bc_hi=(2, 0, 5))
+    s_or, hist, s_gpu, dt_last, err = _level_run(oracle_kind, CONFIGS[cfg], n, bcs, s0, 6,
+                                                 max_grid=(8, 8, 8))
     assert err[0] == 0, err
     assert dt_last == hist[-1]
     assert_bitwise(s_gpu, s_or, "state")
