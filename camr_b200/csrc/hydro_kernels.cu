@@ -726,14 +726,35 @@ __device__ __forceinline__ void batched_cell(const BoxCtx& c, int sub, int i, in
   }
 }
 
+// Stages (bit STAGE of the mask) whose blocks first copy their box context
+// into shared memory: the compiler may then reload box-uniform values from
+// there instead of holding them in registers or spilling them.  Measured
+// per stage: ctoprim, flux1, flux2 and the MOL fluxes gain (two-level MOL
+// step 90.3 -> 88.0 ms); flatten/divu, slopes and consup lose, and flux3
+// spills more.
+#ifndef CAMR_BOX_SMEM_MASK
+#define CAMR_BOX_SMEM_MASK ((1 << BS_CTOPRIM) | (1 << BS_FLUX1) | (1 << BS_FLUX2) | (1 << BS_MOLFLUX))
+#endif
+static_assert(sizeof(BoxCtx) % 8 == 0, "box context copied as 8-byte words");
+
 template <int STAGE, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
     kb_stage(const BoxCtx* __restrict__ boxes, const BatchItem* __restrict__ items, int nitems,
              int64_t nblocks, int chunk, KParams P, DtRef dt, DevError* err) {
+  constexpr bool kSmem = (CAMR_BOX_SMEM_MASK >> STAGE) & 1;
+  __shared__ BoxCtx sbox[1];
   for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
     const int it = find_item(items, nitems, b);
     const BatchItem item = items[it];
-    const BoxCtx& c = boxes[item.box];
+    if constexpr (kSmem) {
+      __syncthreads();
+      const unsigned long long* src =
+          reinterpret_cast<const unsigned long long*>(boxes + item.box);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(sbox);
+      for (int w = threadIdx.x; w < int(sizeof(BoxCtx) / 8); w += kBlock) dst[w] = src[w];
+      __syncthreads();
+    }
+    const BoxCtx& c = kSmem ? sbox[0] : boxes[item.box];
     const int64_t base = (b - item.block0) * int64_t(kBlock) * chunk;
     for (int q = 0; q < chunk; ++q) {
       int i, j, k;
@@ -901,27 +922,67 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
 }
 
 
+// Resident blocks per SM asked of each batched stage.  A batched kernel
+// reads its box's pointers, strides and geometry from the box table in
+// global memory instead of the parameter space, and without a bound the
+// compiler keeps them all in registers (MOL fluxes 142 registers against 90
+// for the per-box kernel), which halves the resident warps.  With these
+// bounds (a few spills of box-uniform values, served by L1) the two-level MOL
+// step went from 98.7 to 90.2 ms and the batched CTU-PPM hydro of 350 boxes
+// from 28.0 to 26.7 ms.
+#ifndef CAMR_BMINB_CTOPRIM
+#define CAMR_BMINB_CTOPRIM 8
+#endif
+#ifndef CAMR_BMINB_FLATDIVU
+#define CAMR_BMINB_FLATDIVU 5
+#endif
+#ifndef CAMR_BMINB_TRACE
+#define CAMR_BMINB_TRACE CAMR_MINB_TRACE
+#endif
+#ifndef CAMR_BMINB_FLUX1
+#define CAMR_BMINB_FLUX1 5
+#endif
+#ifndef CAMR_BMINB_FLUX2
+#define CAMR_BMINB_FLUX2 4
+#endif
+#ifndef CAMR_BMINB_FLUX3
+#define CAMR_BMINB_FLUX3 CAMR_MINB_FLUX3
+#endif
+#ifndef CAMR_BMINB_MOLSLOPE
+#define CAMR_BMINB_MOLSLOPE 8
+#endif
+#ifndef CAMR_BMINB_MOLFLUX
+#define CAMR_BMINB_MOLFLUX 5
+#endif
+#ifndef CAMR_BMINB_CONSUP
+#define CAMR_BMINB_CONSUP 8
+#endif
+
 int batched_min_blocks(int stage) {
   switch (stage) {
-    case BS_TRACE: return CAMR_MINB_TRACE;
-    case BS_FLUX1: return CAMR_MINB_FLUX1;
-    case BS_FLUX2: return CAMR_MINB_FLUX2;
-    case BS_FLUX3: return CAMR_MINB_FLUX3;
-    default: return 1;
+    case BS_CTOPRIM: return CAMR_BMINB_CTOPRIM;
+    case BS_FLATDIVU: return CAMR_BMINB_FLATDIVU;
+    case BS_TRACE: return CAMR_BMINB_TRACE;
+    case BS_FLUX1: return CAMR_BMINB_FLUX1;
+    case BS_FLUX2: return CAMR_BMINB_FLUX2;
+    case BS_FLUX3: return CAMR_BMINB_FLUX3;
+    case BS_MOLSLOPE: return CAMR_BMINB_MOLSLOPE;
+    case BS_MOLFLUX: return CAMR_BMINB_MOLFLUX;
+    default: return CAMR_BMINB_CONSUP;
   }
 }
 
 const void* batched_kernel(int stage) {
   switch (stage) {
-    case BS_CTOPRIM: return reinterpret_cast<const void*>(&kb_stage<BS_CTOPRIM, 1>);
-    case BS_FLATDIVU: return reinterpret_cast<const void*>(&kb_stage<BS_FLATDIVU, 1>);
-    case BS_TRACE: return reinterpret_cast<const void*>(&kb_stage<BS_TRACE, CAMR_MINB_TRACE>);
-    case BS_FLUX1: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX1, CAMR_MINB_FLUX1>);
-    case BS_FLUX2: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX2, CAMR_MINB_FLUX2>);
-    case BS_FLUX3: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX3, CAMR_MINB_FLUX3>);
-    case BS_MOLSLOPE: return reinterpret_cast<const void*>(&kb_stage<BS_MOLSLOPE, 1>);
-    case BS_MOLFLUX: return reinterpret_cast<const void*>(&kb_stage<BS_MOLFLUX, 1>);
-    default: return reinterpret_cast<const void*>(&kb_stage<BS_CONSUP, 1>);
+    case BS_CTOPRIM: return reinterpret_cast<const void*>(&kb_stage<BS_CTOPRIM, CAMR_BMINB_CTOPRIM>);
+    case BS_FLATDIVU: return reinterpret_cast<const void*>(&kb_stage<BS_FLATDIVU, CAMR_BMINB_FLATDIVU>);
+    case BS_TRACE: return reinterpret_cast<const void*>(&kb_stage<BS_TRACE, CAMR_BMINB_TRACE>);
+    case BS_FLUX1: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX1, CAMR_BMINB_FLUX1>);
+    case BS_FLUX2: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX2, CAMR_BMINB_FLUX2>);
+    case BS_FLUX3: return reinterpret_cast<const void*>(&kb_stage<BS_FLUX3, CAMR_BMINB_FLUX3>);
+    case BS_MOLSLOPE: return reinterpret_cast<const void*>(&kb_stage<BS_MOLSLOPE, CAMR_BMINB_MOLSLOPE>);
+    case BS_MOLFLUX: return reinterpret_cast<const void*>(&kb_stage<BS_MOLFLUX, CAMR_BMINB_MOLFLUX>);
+    default: return reinterpret_cast<const void*>(&kb_stage<BS_CONSUP, CAMR_BMINB_CONSUP>);
   }
 }
 
@@ -935,15 +996,15 @@ cudaError_t launch_batched_stage(int stage, const BoxCtx* boxes, const BatchItem
   case S:                                                                                 \
     kb_stage<S, M><<<grid, kBlock, 0, st>>>(boxes, items, nitems, nblocks, chunk, P, dt, err); \
     break;
-    CAMR_LB(BS_CTOPRIM, 1)
-    CAMR_LB(BS_FLATDIVU, 1)
-    CAMR_LB(BS_TRACE, CAMR_MINB_TRACE)
-    CAMR_LB(BS_FLUX1, CAMR_MINB_FLUX1)
-    CAMR_LB(BS_FLUX2, CAMR_MINB_FLUX2)
-    CAMR_LB(BS_FLUX3, CAMR_MINB_FLUX3)
-    CAMR_LB(BS_MOLSLOPE, 1)
-    CAMR_LB(BS_MOLFLUX, 1)
-    CAMR_LB(BS_CONSUP, 1)
+    CAMR_LB(BS_CTOPRIM, CAMR_BMINB_CTOPRIM)
+    CAMR_LB(BS_FLATDIVU, CAMR_BMINB_FLATDIVU)
+    CAMR_LB(BS_TRACE, CAMR_BMINB_TRACE)
+    CAMR_LB(BS_FLUX1, CAMR_BMINB_FLUX1)
+    CAMR_LB(BS_FLUX2, CAMR_BMINB_FLUX2)
+    CAMR_LB(BS_FLUX3, CAMR_BMINB_FLUX3)
+    CAMR_LB(BS_MOLSLOPE, CAMR_BMINB_MOLSLOPE)
+    CAMR_LB(BS_MOLFLUX, CAMR_BMINB_MOLFLUX)
+    CAMR_LB(BS_CONSUP, CAMR_BMINB_CONSUP)
 #undef CAMR_LB
     default: return cudaErrorInvalidValue;
   }
