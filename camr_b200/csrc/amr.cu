@@ -212,7 +212,11 @@ __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap 
 // children: per-direction MC-limited slopes, one factor alpha keeping the
 // children inside the neighbours' min/max, child = u + ox*sx + oy*sy + oz*sz
 // with o = -+1/4.  Then computeTemp on each child.
-__global__ void __launch_bounds__(kBlk) kf_interp(FineDev F, KParams P, CoarseMap CM,
+// resident 256-thread blocks per SM asked of the coarse-to-fine interpolation
+#ifndef CAMR_MINB_INTERP
+#define CAMR_MINB_INTERP 3
+#endif
+__global__ void __launch_bounds__(kBlk, CAMR_MINB_INTERP) kf_interp(FineDev F, KParams P, CoarseMap CM,
                                                    LGeom Lc, const double* c_old,
                                                    const double* c_new, const CoarseT* ctp,
                                                    const int64_t* ib0, double* B) {
