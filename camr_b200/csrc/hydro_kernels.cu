@@ -9,16 +9,24 @@ constexpr int kBlock = 128;
 
 // Minimum resident blocks per SM of the heavy kernels (register budget):
 // 4 for trace and flux3 (128 registers per thread) gave the shortest 256^3
-// CTU-PPM step on B200 among 1/2/4; flux1 and flux2 keep their natural
-// register count.
+// CTU-PPM step on B200 among 1/2/4; 6 for flux1 and flatten/divu (80
+// registers, a few spills: 2.30 -> 2.04 and 1.36 -> 1.30 ms at 256^3);
+// flux2 and the MOL fluxes keep their natural register count (the MOL
+// fluxes measured no faster at 6).
 #ifndef CAMR_MINB_TRACE
 #define CAMR_MINB_TRACE 4
 #endif
 #ifndef CAMR_MINB_FLUX1
-#define CAMR_MINB_FLUX1 1
+#define CAMR_MINB_FLUX1 6
 #endif
 #ifndef CAMR_MINB_FLUX2
 #define CAMR_MINB_FLUX2 1
+#endif
+#ifndef CAMR_MINB_FLATDIVU
+#define CAMR_MINB_FLATDIVU 6
+#endif
+#ifndef CAMR_MINB_MOLFLUX
+#define CAMR_MINB_MOLFLUX 1
 #endif
 #ifndef CAMR_MINB_FLUX3
 #define CAMR_MINB_FLUX3 4
@@ -137,7 +145,7 @@ __device__ __forceinline__ void flatten_divu_body(int i, int j, int k, const Spa
   divu[at] = ux + vy + wz;
 }
 
-__global__ void __launch_bounds__(kBlock) k_flatten_divu(Region r, Space s, KGeom g,
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_FLATDIVU) k_flatten_divu(Region r, Space s, KGeom g,
                                                           KParams P, bool do_flat,
                                                           const double* q, double* flat,
                                                           double* divu) {
@@ -570,7 +578,7 @@ __device__ __forceinline__ void mol_flux_body(int i, int j, int k, const Space& 
   face_adjust_and_store<d>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfd);
 }
 
-__global__ void __launch_bounds__(kBlock) k_mol_flux(Region r0, Region r1, Region r2, Space s,
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLFLUX) k_mol_flux(Region r0, Region r1, Region r2, Space s,
                                                       KGeom g, KParams P, const double* q,
                                                       Ptr3 slope, const double* divu,
                                                       DFab uin, DFab fx, DFab fy, DFab fz,
