@@ -220,7 +220,11 @@ __device__ void adj_slope_body(int i, int j, int k, const Space& s, const KParam
   atomic_add_cell(Lq, at + st, s.sn, bp, NQ);
 }
 
-__global__ void __launch_bounds__(kBlk) k_adj_slope(Region r0, Region r1, Region r2, Space s,
+// 128-thread blocks bounded to 3 per SM (168 registers, a few spills): at
+// 156 registers a thread, 256-thread blocks left one block (8 warps) per SM.
+constexpr int kSlopeBlk = 128;
+
+__global__ void __launch_bounds__(kSlopeBlk, 3) k_adj_slope(Region r0, Region r1, Region r2, Space s,
                                                      KParams P, const double* q, APtr3 Lsl,
                                                      double* Lq) {
   int i, j, k;
@@ -577,7 +581,8 @@ cudaError_t hydro_adj(camr_adjoint* a, const double* Bp, const Work& w, double* 
       rf[0], rf[1], rf[2], a->G, a->P, Bp, w.q, sl,
                                                  w.divu, qf, a->Ldsdt, a->Lq, Lsl, a->Ldivu,
                                                  LBp);
-  k_adj_slope<<<dim3(nblk(ms), 3), kBlk, 0, st>>>(rs[0], rs[1], rs[2], s, a->P, w.q, Lsl, a->Lq);
+  k_adj_slope<<<dim3(unsigned((ms + kSlopeBlk - 1) / kSlopeBlk), 3), kSlopeBlk, 0, st>>>(
+      rs[0], rs[1], rs[2], s, a->P, w.q, Lsl, a->Lq);
   int lo[3], hi[3];
   for (int d = 0; d < 3; ++d) {
     lo[d] = L.dlo[d];
