@@ -80,6 +80,29 @@ def test_batched_equals_per_box_and_oracle(cfg, oracle_kind, native_lib):
                 assert ((a == r) | (np.isnan(a) & np.isnan(r))).all(), (mode, lo, d)
         b.close()
 
+    # every launch shape: cells per block 128/256/512, one block per work
+    # unit or a 7-block persistent grid that strides over many work items
+    # (each block re-reads its box context on every item it takes)
+    names = ["ctoprim", "flatten_divu", "trace", "flux1", "flux2", "flux3", "mol_slope",
+             "mol_flux", "consup"]
+    for cells in (128, 256, 512):
+        for grid in (0, 7):
+            items = []
+            for lo, hi in BOXES:
+                uin, ulo, dsdt, flx = box_inputs(lo, hi)
+                items.append((list(lo), list(hi), uin, ulo, dsdt, flx))
+            b = hydro.Batch(items, geom, prm)
+            b.set_tuning({nm: (cells, grid) for nm in names})
+            assert b.tuning() == {nm: (cells, grid) for nm in names}
+            b.run(dt, hydro.Batch.PERSISTENT)
+            torch.cuda.synchronize()
+            for (lo, hi), (_, _, _, _, dsdt, flx), (d_ref, f_ref) in zip(BOXES, items, per_box):
+                assert torch.equal(dsdt, d_ref), (cells, grid, lo)
+                for d in range(3):
+                    a, r = flx[d].cpu().numpy(), f_ref[d].cpu().numpy()
+                    assert ((a == r) | (np.isnan(a) & np.isnan(r))).all(), (cells, grid, lo, d)
+            b.close()
+
     # and the per-box results equal the oracle's hydro on each box
     for (lo, hi), (dsdt, flx) in zip(BOXES, per_box):
         d_o, f_o, nass = oracle.hydro_box(oracle_kind, p_or, list(lo), list(hi), [0, 0, 0],
