@@ -40,18 +40,15 @@ __device__ __forceinline__ ROut riemannus(double rl_in, double ul, double vl, do
   double ustar = ((wl * ul + wr * ur) + (pl - pr)) / (wl + wr);
   bool mask = fabs(ustar) < smallu * 0.5 * (fabs(ul) + fabs(ur));
   ustar = mask ? 0.0 : ustar;
-  double ro, uo, po, reo, gamco;
-  if (ustar > 0.) {
-    ro = rl; uo = ul; po = pl; reo = rel; gamco = gamcl;
-  } else if (ustar < 0) {
-    ro = rr; uo = ur; po = pr; reo = rer; gamco = gamcr;
-  } else {
-    ro = 0.5 * (rl + rr);
-    uo = 0.5 * (ul + ur);
-    po = 0.5 * (pl + pr);
-    reo = 0.5 * (rel + rer);
-    gamco = 0.5 * (gamcl + gamcr);
-  }
+  // upwind state (left, right, or the mean when ustar is exactly 0),
+  // picked by selects rather than branches: the same values, fewer
+  // divergent branches
+  const bool up = ustar > 0., dn = ustar < 0;
+  double ro = up ? rl : dn ? rr : 0.5 * (rl + rr);
+  const double uo = up ? ul : dn ? ur : 0.5 * (ul + ur);
+  const double po = up ? pl : dn ? pr : 0.5 * (pl + pr);
+  const double reo = up ? rel : dn ? rer : 0.5 * (rel + rer);
+  const double gamco = up ? gamcl : dn ? gamcr : 0.5 * (gamcl + gamcr);
   ro = dmax(ro, small_dens);
   const double roinv = 1.0 / ro;
   double co = sqrt(fabs(gamco * po * roinv));
@@ -190,7 +187,7 @@ __device__ __forceinline__ ROut hllc(double rl_in, double ul, double vl, double 
 //
 // cmpflx_core does all but the species: the boundary edits, the Riemann
 // solve and every non-species flux component; species_flux then upwinds the
-// species edge states by the sign of ustar, one branch for all species.
+// species edge states by the sign of ustar.
 template <int dir>
 __device__ __forceinline__ ROut cmpflx_core(double* ql, double* qr, const CellAux& aL,
                                             const CellAux& aR, int idx, int bclo, int bchi,
@@ -265,20 +262,15 @@ __device__ __forceinline__ ROut cmpflx_core(double* ql, double* qr, const CellAu
 
 // Species fluxes of cmpflx (Hydro_cmpflx.H:289-301): the left (ustar > 0),
 // right (ustar < 0) or mean (ustar exactly 0, or NaN) species edge states
-// times the mass flux.
+// times the mass flux, picked by selects.
 __device__ __forceinline__ void species_flux(const ROut& o, double* f, const double* ql,
                                              const double* qr) {
   const double flxrho = f[URHO];
-  if (o.ustar > 0.0) {
+  const bool up = o.ustar > 0.0, dn = o.ustar < 0.0;
 #pragma unroll
-    for (int n = 0; n < NSPEC; ++n) f[UFS + n] = flxrho * ql[ES_FS + n];
-  } else if (o.ustar < 0.0) {
-#pragma unroll
-    for (int n = 0; n < NSPEC; ++n) f[UFS + n] = flxrho * qr[ES_FS + n];
-  } else {
-#pragma unroll
-    for (int n = 0; n < NSPEC; ++n)
-      f[UFS + n] = flxrho * 0.50 * (ql[ES_FS + n] + qr[ES_FS + n]);
+  for (int n = 0; n < NSPEC; ++n) {
+    const double a = ql[ES_FS + n], b = qr[ES_FS + n];
+    f[UFS + n] = up ? flxrho * a : dn ? flxrho * b : flxrho * 0.50 * (a + b);
   }
 }
 
