@@ -3,7 +3,7 @@
 The oracle is the reference's own per-box hydro compiled on the CPU
 (oracle/_ref) when present, else the repo's restatement (pinned to it by
 tests/test_oracle.py and the golden fixtures).  The bar is exact equality of
-every double; the north-star tolerance (relative L1 <= 1e-12 per conserved
+every double; the parity tolerance (relative L1 <= 1e-12 per conserved
 variable) is asserted as well so that a failure reports its size.
 """
 import numpy as np
