@@ -154,6 +154,23 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def max_over_ranks(x, pg, device="cuda"):
+    """The largest of every rank's x (every rank gets it); x itself on one
+    process.  The timing of a multi-GPU run is the slowest rank's."""
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, zones_per_rank, steps, ms):
+    """Zone-updates/s of the whole job: every rank advances its own replica
+    of zones_per_rank cells `steps` times in `ms` (the slowest rank's)."""
+    return world * zones_per_rank * steps / (ms * 1e-3)
+
+
 def c1_state(n):
     from camr_b200 import problems as P
     dx = tuple(1.0 / v for v in n)
@@ -255,12 +272,9 @@ def run_camr(args, world, rank, local, pg):
     ms = e0.elapsed_time(e1)
     launches = lib.camr_launch_count() - launches0
     err = L.error()
-    if pg is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, pg)
     ms_step = ms / args.steps
-    value = world * zones * args.steps / (ms * 1e-3)
+    value = whole_job_rate(world, zones, args.steps, ms)
 
     # Per-stage device times, live (uncaptured profiled steps).
     names = (C.c_char_p * 40)()
@@ -327,12 +341,9 @@ def run_camr(args, world, rank, local, pg):
     e2e_serial_ms = e2e_run(False, host)
     e2e_initial_ms = e2e_run(True, host0)
     e2e_ms = e2e_run(True, host)
-    if pg is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, pg)
     state_bytes = host.numel() * 8
-    e2e = {"value": world * zones / (e2e_ms * 1e-3), "unit": UNIT,
+    e2e = {"value": whole_job_rate(world, zones, 1, e2e_ms), "unit": UNIT,
            "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
            "ms_per_step": e2e_ms, "steps": e2e_steps,
            "ms_per_step_without_overlap": e2e_serial_ms,
