@@ -65,3 +65,16 @@ def test_invalid_arguments_rejected_without_gpu(native_lib):
     p = native.default_params(riemann_solver=7)
     st = native_lib.camr_level_create(C.byref(desc), C.byref(p), None, C.byref(out))
     assert native.STATUS[st] == "CAMR_ERR_UNSUPPORTED"
+
+
+def test_batch_tuning_arguments_rejected_without_gpu(native_lib):
+    """The launch-shape setters check their arguments before touching a plan."""
+    from camr_b200 import native
+    ch = (C.c_int * 9)(*([1] * 9))
+    gr = (C.c_uint * 9)(*([0] * 9))
+    st = native_lib.camr_batch_set_tuning(None, ch, gr, 9)
+    assert native.STATUS[st] == "CAMR_ERR_INVALID"
+    st = native_lib.camr_batch_tuning(None, ch, gr, 9)
+    assert native.STATUS[st] == "CAMR_ERR_INVALID"
+    st = native_lib.camr_eb_level_autotune(None)
+    assert native.STATUS[st] == "CAMR_ERR_INVALID"
