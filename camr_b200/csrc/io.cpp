@@ -1,4 +1,5 @@
-// AMReX plotfile output and input of one level (host code).
+// AMReX plotfile output (one level, or the two levels of the AMR driver)
+// and input of one level (host code).
 //
 // A plotfile is a directory holding
 //   Header            the plotfile header CAMR::writePlotFile writes
@@ -69,41 +70,21 @@ bool host_little_endian() {
   return b == 1;
 }
 
-}  // namespace
+// One level's grids as the Header describes them.
+struct LevelOut {
+  int dom_lo[3], dom_hi[3];
+  double dx[3];
+  int level_step;
+  int nbox;
+  const int* boxes;  // nbox x (lo0,lo1,lo2,hi0,hi1,hi2)
+};
 
-extern "C" {
-
-const char* camr_io_last_error(void) { return g_io_error.c_str(); }
-
-camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const double prob_hi[3],
-                                double time, int level_step, int nbox, const int* boxes,
-                                const double* state, int ncomp, const int* comps,
-                                const char* const* names) {
-  g_io_error.clear();
-  if (!dir || !geom || !prob_hi || nbox <= 0 || !boxes || !state || ncomp <= 0)
-    return io_fail("invalid arguments");
-  if (!host_little_endian()) return io_fail("big-endian hosts are not supported");
-  int n[3];
-  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
-  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
-  std::vector<int> cmap(ncomp);
-  std::vector<std::string> vnames(ncomp);
-  for (int c = 0; c < ncomp; ++c) {
-    cmap[c] = comps ? comps[c] : c;
-    if (cmap[c] < 0 || cmap[c] >= CAMR_NVAR) return io_fail("component out of range");
-    vnames[c] = (names && names[c]) ? names[c] : kStateNames[cmap[c]];
-  }
-  for (int b = 0; b < nbox; ++b)
-    for (int d = 0; d < 3; ++d) {
-      const int lo = boxes[6 * b + d], hi = boxes[6 * b + 3 + d];
-      if (lo < geom->dom_lo[d] || hi > geom->dom_hi[d] || hi < lo)
-        return io_fail("box outside the domain");
-    }
-  const std::string root(dir);
-  const std::string lev = root + "/Level_0";
-  if (!make_dir(root) || !make_dir(lev)) return io_fail("cannot create " + lev);
-
-  // Level_0/Cell_D_00000 and the per-box offsets, minima and maxima.
+// Level_L/Cell_D_00000 and Level_L/Cell_H of one level.  row(b, c, j, k)
+// returns p with p[i] = component c of cell (i, j, k) of box b.
+template <class Row>
+camr_status write_level_files(const std::string& lev, int nbox, const int* boxes, int ncomp,
+                              Row row) {
+  if (!make_dir(lev)) return io_fail("cannot create " + lev);
   std::vector<int64_t> offs(nbox);
   std::vector<double> mins(size_t(nbox) * ncomp), maxs(size_t(nbox) * ncomp);
   {
@@ -124,16 +105,14 @@ camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const do
       pos += int64_t(hs.size());
       buf.resize(size_t(bc));
       for (int c = 0; c < ncomp; ++c) {
-        const double* src = state + int64_t(cmap[c]) * ncell;
         double mn = std::numeric_limits<double>::max();
         double mx = std::numeric_limits<double>::lowest();
         int64_t t = 0;
         for (int k = lo[2]; k <= hi[2]; ++k)
           for (int j = lo[1]; j <= hi[1]; ++j) {
-            const double* row = src + (int64_t(k - geom->dom_lo[2]) * n[1] +
-                                       (j - geom->dom_lo[1])) * n[0] - geom->dom_lo[0];
+            const double* r = row(b, c, j, k);
             for (int i = lo[0]; i <= hi[0]; ++i) {
-              const double v = row[i];
+              const double v = r[i];
               buf[size_t(t++)] = v;
               mn = v < mn ? v : mn;
               mx = v > mx ? v : mx;
@@ -147,55 +126,194 @@ camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const do
     }
     if (std::fclose(f) != 0) return io_fail("write failed: " + lev + "/Cell_D_00000");
   }
-  // Level_0/Cell_H
-  {
-    std::ofstream h(lev + "/Cell_H");
-    if (!h) return io_fail("cannot write " + lev + "/Cell_H");
-    h << 1 << '\n' << 1 << '\n' << ncomp << '\n' << 0 << '\n';
-    h << '(' << nbox << " 0\n";
-    for (int b = 0; b < nbox; ++b) h << box_text(boxes + 6 * b, boxes + 6 * b + 3) << '\n';
-    h << ")\n" << nbox << '\n';
-    for (int b = 0; b < nbox; ++b) h << "FabOnDisk: Cell_D_00000 " << offs[b] << '\n';
-    h << '\n' << nbox << ',' << ncomp << '\n';
-    h << std::setprecision(17);
-    for (int b = 0; b < nbox; ++b) {
-      for (int c = 0; c < ncomp; ++c) h << mins[size_t(b) * ncomp + c] << ',';
-      h << '\n';
-    }
-    h << '\n' << nbox << ',' << ncomp << '\n';
-    for (int b = 0; b < nbox; ++b) {
-      for (int c = 0; c < ncomp; ++c) h << maxs[size_t(b) * ncomp + c] << ',';
-      h << '\n';
-    }
-    if (!h) return io_fail("write failed: " + lev + "/Cell_H");
-  }
-  // Header
-  {
-    std::ofstream h(root + "/Header");
-    if (!h) return io_fail("cannot write " + root + "/Header");
-    h << std::setprecision(17);
-    h << "HyperCLaw-V1.1\n" << ncomp << '\n';
-    for (const auto& v : vnames) h << v << '\n';
-    h << 3 << '\n' << time << '\n' << 0 << '\n';
-    for (int d = 0; d < 3; ++d) h << geom->prob_lo[d] << ' ';
+  std::ofstream h(lev + "/Cell_H");
+  if (!h) return io_fail("cannot write " + lev + "/Cell_H");
+  h << 1 << '\n' << 1 << '\n' << ncomp << '\n' << 0 << '\n';
+  h << '(' << nbox << " 0\n";
+  for (int b = 0; b < nbox; ++b) h << box_text(boxes + 6 * b, boxes + 6 * b + 3) << '\n';
+  h << ")\n" << nbox << '\n';
+  for (int b = 0; b < nbox; ++b) h << "FabOnDisk: Cell_D_00000 " << offs[b] << '\n';
+  h << '\n' << nbox << ',' << ncomp << '\n';
+  h << std::setprecision(17);
+  for (int b = 0; b < nbox; ++b) {
+    for (int c = 0; c < ncomp; ++c) h << mins[size_t(b) * ncomp + c] << ',';
     h << '\n';
-    for (int d = 0; d < 3; ++d) h << prob_hi[d] << ' ';
-    h << '\n' << '\n';
-    h << box_text(geom->dom_lo, geom->dom_hi) << ' ' << '\n';
-    h << level_step << ' ' << '\n';
-    for (int d = 0; d < 3; ++d) h << geom->dx[d] << ' ';
-    h << '\n' << 0 << '\n' << "0\n";
-    h << 0 << ' ' << nbox << ' ' << time << '\n' << level_step << '\n';
-    for (int b = 0; b < nbox; ++b)
+  }
+  h << '\n' << nbox << ',' << ncomp << '\n';
+  for (int b = 0; b < nbox; ++b) {
+    for (int c = 0; c < ncomp; ++c) h << maxs[size_t(b) * ncomp + c] << ',';
+    h << '\n';
+  }
+  if (!h) return io_fail("write failed: " + lev + "/Cell_H");
+  return CAMR_OK;
+}
+
+// The plotfile Header over nlev levels (refinement ratio 2 between them).
+camr_status write_header(const std::string& root, const std::vector<std::string>& vnames,
+                         const double prob_lo[3], const double prob_hi[3], double time,
+                         const std::vector<LevelOut>& levels) {
+  std::ofstream h(root + "/Header");
+  if (!h) return io_fail("cannot write " + root + "/Header");
+  const int nlev = int(levels.size());
+  h << std::setprecision(17);
+  h << "HyperCLaw-V1.1\n" << vnames.size() << '\n';
+  for (const auto& v : vnames) h << v << '\n';
+  h << 3 << '\n' << time << '\n' << nlev - 1 << '\n';
+  for (int d = 0; d < 3; ++d) h << prob_lo[d] << ' ';
+  h << '\n';
+  for (int d = 0; d < 3; ++d) h << prob_hi[d] << ' ';
+  h << '\n';
+  for (int l = 0; l + 1 < nlev; ++l) h << 2 << ' ';
+  h << '\n';
+  for (const auto& L : levels) h << box_text(L.dom_lo, L.dom_hi) << ' ';
+  h << '\n';
+  for (const auto& L : levels) h << L.level_step << ' ';
+  h << '\n';
+  for (const auto& L : levels) {
+    for (int d = 0; d < 3; ++d) h << L.dx[d] << ' ';
+    h << '\n';
+  }
+  h << 0 << '\n' << "0\n";
+  for (int l = 0; l < nlev; ++l) {
+    const LevelOut& L = levels[size_t(l)];
+    h << l << ' ' << L.nbox << ' ' << time << '\n' << L.level_step << '\n';
+    for (int b = 0; b < L.nbox; ++b)
       for (int d = 0; d < 3; ++d) {
-        const double lo = geom->prob_lo[d] + boxes[6 * b + d] * geom->dx[d];
-        const double hi = geom->prob_lo[d] + (boxes[6 * b + 3 + d] + 1) * geom->dx[d];
+        const double lo = prob_lo[d] + L.boxes[6 * b + d] * L.dx[d];
+        const double hi = prob_lo[d] + (L.boxes[6 * b + 3 + d] + 1) * L.dx[d];
         h << lo << ' ' << hi << '\n';
       }
-    h << "Level_0/Cell\n";
-    if (!h) return io_fail("write failed: " + root + "/Header");
+    h << "Level_" << l << "/Cell\n";
+  }
+  if (!h) return io_fail("write failed: " + root + "/Header");
+  return CAMR_OK;
+}
+
+camr_status check_names(int ncomp, const int* comps, const char* const* names,
+                        std::vector<int>& cmap, std::vector<std::string>& vnames) {
+  cmap.resize(size_t(ncomp));
+  vnames.resize(size_t(ncomp));
+  for (int c = 0; c < ncomp; ++c) {
+    cmap[size_t(c)] = comps ? comps[c] : c;
+    if (cmap[size_t(c)] < 0 || cmap[size_t(c)] >= CAMR_NVAR) return io_fail("component out of range");
+    vnames[size_t(c)] = (names && names[c]) ? names[c] : kStateNames[cmap[size_t(c)]];
   }
   return CAMR_OK;
+}
+
+bool boxes_inside(int nbox, const int* boxes, const int dlo[3], const int dhi[3]) {
+  for (int b = 0; b < nbox; ++b)
+    for (int d = 0; d < 3; ++d) {
+      const int lo = boxes[6 * b + d], hi = boxes[6 * b + 3 + d];
+      if (lo < dlo[d] || hi > dhi[d] || hi < lo) return false;
+    }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* camr_io_last_error(void) { return g_io_error.c_str(); }
+
+camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                double time, int level_step, int nbox, const int* boxes,
+                                const double* state, int ncomp, const int* comps,
+                                const char* const* names) {
+  g_io_error.clear();
+  if (!dir || !geom || !prob_hi || nbox <= 0 || !boxes || !state || ncomp <= 0)
+    return io_fail("invalid arguments");
+  if (!host_little_endian()) return io_fail("big-endian hosts are not supported");
+  std::vector<int> cmap;
+  std::vector<std::string> vnames;
+  camr_status cs = check_names(ncomp, comps, names, cmap, vnames);
+  if (cs != CAMR_OK) return cs;
+  if (!boxes_inside(nbox, boxes, geom->dom_lo, geom->dom_hi)) return io_fail("box outside the domain");
+  int n[3];
+  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
+  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
+  const std::string root(dir);
+  if (!make_dir(root)) return io_fail("cannot create " + root);
+  cs = write_level_files(root + "/Level_0", nbox, boxes, ncomp, [&](int, int c, int j, int k) {
+    return state + int64_t(cmap[size_t(c)]) * ncell +
+           (int64_t(k - geom->dom_lo[2]) * n[1] + (j - geom->dom_lo[1])) * n[0] - geom->dom_lo[0];
+  });
+  if (cs != CAMR_OK) return cs;
+  LevelOut L0;
+  for (int d = 0; d < 3; ++d) {
+    L0.dom_lo[d] = geom->dom_lo[d];
+    L0.dom_hi[d] = geom->dom_hi[d];
+    L0.dx[d] = geom->dx[d];
+  }
+  L0.level_step = level_step;
+  L0.nbox = nbox;
+  L0.boxes = boxes;
+  return write_header(root, vnames, geom->prob_lo, prob_hi, time, {L0});
+}
+
+camr_status camr_write_plotfile_amr(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                    double time, const int level_step[2], int nbox0,
+                                    const int* boxes0, const double* state0, int nbox1,
+                                    const int* boxes1, const double* state1, int ncomp,
+                                    const int* comps, const char* const* names) {
+  g_io_error.clear();
+  if (!dir || !geom || !prob_hi || !level_step || nbox0 <= 0 || !boxes0 || !state0 ||
+      nbox1 < 0 || (nbox1 > 0 && (!boxes1 || !state1)) || ncomp <= 0)
+    return io_fail("invalid arguments");
+  if (!host_little_endian()) return io_fail("big-endian hosts are not supported");
+  std::vector<int> cmap;
+  std::vector<std::string> vnames;
+  camr_status cs = check_names(ncomp, comps, names, cmap, vnames);
+  if (cs != CAMR_OK) return cs;
+  LevelOut L0, L1;
+  for (int d = 0; d < 3; ++d) {
+    L0.dom_lo[d] = geom->dom_lo[d];
+    L0.dom_hi[d] = geom->dom_hi[d];
+    L0.dx[d] = geom->dx[d];
+    L1.dom_lo[d] = 2 * geom->dom_lo[d];
+    L1.dom_hi[d] = 2 * geom->dom_hi[d] + 1;
+    L1.dx[d] = geom->dx[d] / 2;
+  }
+  L0.level_step = level_step[0];
+  L0.nbox = nbox0;
+  L0.boxes = boxes0;
+  L1.level_step = level_step[1];
+  L1.nbox = nbox1;
+  L1.boxes = boxes1;
+  if (!boxes_inside(nbox0, boxes0, L0.dom_lo, L0.dom_hi) ||
+      !boxes_inside(nbox1, boxes1, L1.dom_lo, L1.dom_hi))
+    return io_fail("box outside the domain");
+  int n[3];
+  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
+  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
+  const std::string root(dir);
+  if (!make_dir(root)) return io_fail("cannot create " + root);
+  cs = write_level_files(root + "/Level_0", nbox0, boxes0, ncomp, [&](int, int c, int j, int k) {
+    return state0 + int64_t(cmap[size_t(c)]) * ncell +
+           (int64_t(k - geom->dom_lo[2]) * n[1] + (j - geom->dom_lo[1])) * n[0] - geom->dom_lo[0];
+  });
+  if (cs != CAMR_OK) return cs;
+  // the fine boxes' states back to back, each (NVAR, nz, ny, nx) over its box
+  std::vector<int64_t> base(size_t(nbox1) + 1, 0);
+  for (int b = 0; b < nbox1; ++b) {
+    const int* lo = boxes1 + 6 * b;
+    const int* hi = boxes1 + 6 * b + 3;
+    base[size_t(b) + 1] = base[size_t(b)] + int64_t(CAMR_NVAR) * (hi[0] - lo[0] + 1) *
+                                                (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+  }
+  if (nbox1 > 0) {
+    cs = write_level_files(root + "/Level_1", nbox1, boxes1, ncomp, [&](int b, int c, int j, int k) {
+      const int* lo = boxes1 + 6 * b;
+      const int* hi = boxes1 + 6 * b + 3;
+      const int64_t bx = hi[0] - lo[0] + 1, by = hi[1] - lo[1] + 1, bz = hi[2] - lo[2] + 1;
+      return state1 + base[size_t(b)] + int64_t(cmap[size_t(c)]) * bx * by * bz +
+             (int64_t(k - lo[2]) * by + (j - lo[1])) * bx - lo[0];
+    });
+    if (cs != CAMR_OK) return cs;
+  }
+  std::vector<LevelOut> levels{L0};
+  if (nbox1 > 0) levels.push_back(L1);
+  return write_header(root, vnames, geom->prob_lo, prob_hi, time, levels);
 }
 
 camr_status camr_read_plotfile(const char* dir, const camr_geom* geom, int ncomp,

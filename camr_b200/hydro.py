@@ -541,6 +541,38 @@ def write_plotfile(path, state, geom, prob_hi, time=0.0, level_step=0,
                                lib().camr_io_last_error().decode())
 
 
+def write_plotfile_amr(path, S0, S1, geom, prob_hi, fine_boxes, time=0.0, level_steps=(0, 0),
+                       max_grid_size=(32, 32, 32), comps=None, names=None):
+    """Write the two levels of an AMR run as one plotfile
+    (camr_write_plotfile_amr): S0 the base level (NVAR, nz, ny, nx); S1 the
+    fine boxes' states back to back (each (NVAR, nz, ny, nx) over its box, as
+    AmrHierarchy.get_state returns them); fine_boxes [(lo, hi), ...] on the fine
+    index space."""
+    n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+    a = np.ascontiguousarray(S0, dtype=np.float64)
+    assert a.shape == (NVAR, n[2], n[1], n[0])
+    f = np.ascontiguousarray(S1, dtype=np.float64).ravel()
+    ncell1 = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in fine_boxes)
+    assert f.size == NVAR * ncell1
+    boxes0 = level_boxes(n, max_grid_size, tuple(geom.dom_lo))
+    b0 = np.array([list(lo) + list(hi) for lo, hi in boxes0], dtype=np.int32).ravel()
+    b1 = np.array([list(lo) + list(hi) for lo, hi in fine_boxes], dtype=np.int32).ravel()
+    comps = list(range(NVAR)) if comps is None else list(comps)
+    carr = np.array(comps, dtype=np.int32)
+    nm = None
+    if names is not None:
+        nm = (C.c_char_p * len(names))(*[x.encode() for x in names])
+    ph = (C.c_double * 3)(*prob_hi)
+    steps = (C.c_int * 2)(*level_steps)
+    st = lib().camr_write_plotfile_amr(str(path).encode(), C.byref(geom), C.byref(ph), float(time),
+                                       steps, len(boxes0), b0.ctypes.data, a.ctypes.data,
+                                       len(fine_boxes), b1.ctypes.data if len(fine_boxes) else None,
+                                       f.ctypes.data, len(comps), carr.ctypes.data, nm)
+    if st != 0:
+        raise native.CamrError(st, "camr_write_plotfile_amr " +
+                               lib().camr_io_last_error().decode())
+
+
 def read_plotfile(path, geom, ncomp=NVAR):
     """Read a single-level plotfile written by write_plotfile: returns
     (state planes (ncomp, nz, ny, nx), time, level_step)."""

@@ -155,6 +155,10 @@ SIGNATURES = {
                                       C.c_int, C.c_void_p, C.c_void_p]),
     "camr_read_plotfile": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.c_int, C.c_void_p,
                                      C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "camr_write_plotfile_amr": (C.c_int, [C.c_char_p, C.POINTER(Geom),
+                                          C.POINTER(C.c_double * 3), C.c_double, C.c_void_p,
+                                          C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "camr_io_last_error": (C.c_char_p, []),
     "camr_adjoint_create": (C.c_int, [C.POINTER(Geom), C.POINTER(HydroParams), C.c_int,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),

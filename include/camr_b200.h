@@ -455,6 +455,19 @@ camr_status camr_write_plotfile(const char* dir, const camr_geom* geom, const do
                                 const char* const* names);
 camr_status camr_read_plotfile(const char* dir, const camr_geom* geom, int ncomp,
                                double* state, double* time, int* level_step);
+/* The two levels of the AMR driver (camr_amr_*, refinement ratio 2) as one
+ * plotfile, as CAMR::writePlotFile writes a two-level hierarchy: level 0 as
+ * above (geom, boxes0, state0); level 1 on the fine index space (domain
+ * 2*dom_lo .. 2*dom_hi+1, cell size dx/2), nbox1 boxes (lo0,lo1,lo2,
+ * hi0,hi1,hi2) whose states lie back to back in state1, each
+ * (NVAR, nz, ny, nx) over its own box (the layout of camr_amr_get_state).
+ * level_step[2]: the step counts of the two levels.  nbox1 = 0 writes a
+ * single-level plotfile. */
+camr_status camr_write_plotfile_amr(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                    double time, const int level_step[2], int nbox0,
+                                    const int* boxes0, const double* state0, int nbox1,
+                                    const int* boxes1, const double* state1, int ncomp,
+                                    const int* comps, const char* const* names);
 /* Why the last plotfile call on this thread failed ("" if it did not). */
 const char* camr_io_last_error(void);
 

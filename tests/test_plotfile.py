@@ -119,6 +119,87 @@ def test_plotfile_rejects_bad_input(tmp_path, native_lib):
         hydro.read_plotfile(tmp_path / "missing", geom)
 
 
+def read_level(path, lev, nv):
+    """Boxes and per-box arrays of Level_<lev> (VisMF header + FAB data)."""
+    cell_h = (path / f"Level_{lev}" / "Cell_H").read_text().split("\n")
+    assert cell_h[0] == "1" and cell_h[1] == "1" and int(cell_h[2]) == nv and cell_h[3] == "0"
+    nb = int(cell_h[4].strip("(").split()[0])
+    boxes = [[int(x) for x in re.findall(r"-?\d+", cell_h[5 + b])] for b in range(nb)]
+    fabs = [cell_h[7 + nb + b].split() for b in range(nb)]
+    data = (path / f"Level_{lev}" / "Cell_D_00000").read_bytes()
+    out = []
+    for b, (tag, fname, off) in enumerate(fabs):
+        assert tag == "FabOnDisk:" and fname == "Cell_D_00000"
+        end = data.index(b"\n", int(off))
+        assert data[int(off):end].decode().startswith("FAB ((8, (64 11 52 0 1 12 0 1023))")
+        lo, hi = boxes[b][:3], boxes[b][3:6]
+        bn = [hi[d] - lo[d] + 1 for d in range(3)]
+        vals = np.frombuffer(data, dtype="<f8", count=nv * bn[0] * bn[1] * bn[2], offset=end + 1)
+        out.append((lo, hi, vals.reshape(nv, bn[2], bn[1], bn[0])))
+    return out
+
+
+def test_two_level_plotfile(tmp_path, native_lib):
+    """The AMR driver's two levels as one plotfile: the Header's finest
+    level, refinement ratio, per-level domains, steps, cell sizes and grid
+    extents, and both levels' data, parsed without the library."""
+    n = (16, 16, 8)
+    dx = (1.0 / 16, 1.0 / 16, 0.5 / 8)
+    geom = hydro.make_geom(n, dx=dx, prob_hi=(1.0, 1.0, 0.5))
+    s0 = P.random_smooth(n, seed=3)
+    fine = [((4, 4, 2), (11, 19, 9)), ((20, 0, 0), (27, 7, 15))]
+    rng = np.random.default_rng(9)
+    parts = []
+    for lo, hi in fine:
+        bn = [hi[d] - lo[d] + 1 for d in range(3)]
+        parts.append(rng.standard_normal((10, bn[2], bn[1], bn[0])))
+    s1 = np.concatenate([p.ravel() for p in parts])
+    path = tmp_path / "plt_amr"
+    hydro.write_plotfile_amr(path, s0, s1, geom, (1.0, 1.0, 0.5), fine, time=0.25,
+                             level_steps=(5, 10), max_grid_size=(8, 8, 8))
+    hdr = (path / "Header").read_text().split("\n")
+    assert hdr[0] == "HyperCLaw-V1.1" and int(hdr[1]) == 10 and hdr[2:12] == NAMES
+    i = 12
+    assert int(hdr[i]) == 3 and float(hdr[i + 1]) == 0.25 and int(hdr[i + 2]) == 1
+    assert [float(x) for x in hdr[i + 4].split()] == [1.0, 1.0, 0.5]
+    assert hdr[i + 5].split() == ["2"]
+    doms = [[int(x) for x in m] for m in
+            [re.findall(r"-?\d+", b) for b in re.findall(r"\(\([^)]*\) \([^)]*\) \([^)]*\)\)",
+                                                        hdr[i + 6])]]
+    assert doms[0][:6] == [0, 0, 0, 15, 15, 7] and doms[1][:6] == [0, 0, 0, 31, 31, 15]
+    assert hdr[i + 7].split() == ["5", "10"]
+    assert [float(x) for x in hdr[i + 8].split()] == list(dx)
+    assert [float(x) for x in hdr[i + 9].split()] == [v / 2 for v in dx]
+    assert hdr[i + 10] == "0" and hdr[i + 11] == "0"
+    j = i + 12
+    nb0 = len(hydro.level_boxes(n, (8, 8, 8)))
+    assert hdr[j].split() == ["0", str(nb0), "0.25"] and hdr[j + 1] == "5"
+    assert hdr[j + 2 + 3 * nb0] == "Level_0/Cell"
+    j = j + 3 + 3 * nb0
+    assert hdr[j].split() == ["1", "2", "0.25"] and hdr[j + 1] == "10"
+    for b, (lo, hi) in enumerate(fine):
+        for d in range(3):
+            elo, ehi = (float(v) for v in hdr[j + 2 + 3 * b + d].split())
+            assert abs(elo - lo[d] * dx[d] / 2) < 1e-15 and abs(ehi - (hi[d] + 1) * dx[d] / 2) < 1e-15
+    assert hdr[j + 2 + 3 * len(fine)] == "Level_1/Cell"
+    back0 = np.zeros_like(s0)
+    for lo, hi, v in read_level(path, 0, 10):
+        back0[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = v
+    assert np.array_equal(back0, s0)
+    lev1 = read_level(path, 1, 10)
+    assert [(tuple(lo), tuple(hi)) for lo, hi, _ in lev1] == fine
+    for (_, _, v), p in zip(lev1, parts):
+        assert np.array_equal(v, p)
+
+
+def test_two_level_plotfile_rejects_fine_box_outside(tmp_path, native_lib):
+    geom = hydro.make_geom((8, 8, 8))
+    with pytest.raises(native.CamrError):
+        hydro.write_plotfile_amr(tmp_path / "bad", np.zeros((10, 8, 8, 8)),
+                                 np.zeros(10 * 8 ** 3), geom, (1, 1, 1),
+                                 [((10, 10, 10), (17, 17, 17))])
+
+
 @pytest.mark.gpu
 def test_level_state_plotfile_restart(tmp_path):
     """A level's state written after GPU steps, read back and set into a new
@@ -144,3 +225,32 @@ def test_level_state_plotfile_restart(tmp_path):
     b.set_state(back)
     b.advance(2)
     assert np.array_equal(a.get_state(), b.get_state())
+
+
+@pytest.mark.gpu
+def test_amr_hierarchy_two_level_plotfile(tmp_path):
+    """Both levels of a GPU AMR run, written after a few coarse steps, parse
+    back to exactly the states the hierarchy holds."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    n0 = (16, 16, 16)
+    boxes = [((8, 8, 8), (23, 15, 15)), ((0, 16, 16), (7, 31, 23))]
+    S0, S1 = P.amr_initial(n0, boxes, nblobs=3, r_min=0.1, r_max=0.2)
+    geom = hydro.make_geom(n0)
+    h = hydro.AmrHierarchy(geom, native.default_params(ppm_type=1, cfl=0.5), boxes)
+    h.set_state(S0, S1)
+    h.init_finalize()
+    h.advance(2)
+    c0, c1 = h.get_state()
+    t0, t1 = h.clock()[:2]
+    h.close()
+    hydro.write_plotfile_amr(tmp_path / "plt_amr_gpu", c0, c1, geom, (1, 1, 1), boxes,
+                             time=t0, level_steps=(2, 4))
+    back0 = np.zeros_like(c0)
+    for lo, hi, v in read_level(tmp_path / "plt_amr_gpu", 0, 10):
+        back0[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = v
+    assert np.array_equal(back0, c0)
+    lev1 = read_level(tmp_path / "plt_amr_gpu", 1, 10)
+    assert np.array_equal(np.concatenate([v.ravel() for _, _, v in lev1]), np.asarray(c1).ravel())
+    assert t0 > 0 and abs(t0 - t1) <= 1e-12 * t0
