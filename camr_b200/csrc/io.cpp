@@ -25,6 +25,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
@@ -201,6 +202,132 @@ camr_status check_names(int ncomp, const int* comps, const char* const* names,
   return CAMR_OK;
 }
 
+bool boxes_inside(int nbox, const int* boxes, const int dlo[3], const int dhi[3]);
+
+// Header fields the readers check: variable count, dimension, time, finest
+// level and the level steps.
+camr_status read_header(const std::string& root, int ncomp, int* finest, double* time,
+                        int steps[2]) {
+  std::ifstream h(root + "/Header");
+  if (!h) return io_fail("cannot read " + root + "/Header");
+  std::string line;
+  std::vector<std::string> lines;
+  while (std::getline(h, line)) lines.push_back(line);
+  if (lines.size() < 3 || lines[0] != "HyperCLaw-V1.1") return io_fail("unexpected plotfile header");
+  const int nv = std::atoi(lines[1].c_str());
+  if (nv != ncomp || lines.size() < size_t(nv) + 10) return io_fail("unexpected plotfile header");
+  size_t i = 2 + size_t(nv);
+  const int dim = std::atoi(lines[i].c_str());
+  const double t = std::atof(lines[i + 1].c_str());
+  *finest = std::atoi(lines[i + 2].c_str());
+  if (dim != 3 || *finest < 0 || *finest > 1) return io_fail("only 3-D plotfiles of one or two levels are read");
+  if (time) *time = t;
+  std::istringstream st(lines[i + 7]);  // level steps
+  for (int l = 0; l <= *finest; ++l) st >> steps[l];
+  return CAMR_OK;
+}
+
+// A level's VisMF header: boxes (6 ints each), data files and offsets.
+camr_status read_cell_h(const std::string& lev, int ncomp, std::vector<int>& bx,
+                        std::vector<std::string>& files, std::vector<int64_t>& offs) {
+  std::ifstream ch(lev + "/Cell_H");
+  if (!ch) return io_fail("cannot read " + lev + "/Cell_H");
+  int version = 0, how = 0, nc = 0, ngrow = 0;
+  ch >> version >> how >> nc >> ngrow;
+  if (nc != ncomp || ngrow != 0) return io_fail("unexpected Cell_H");
+  char paren;
+  int nbox = 0, zero = 0;
+  ch >> paren >> nbox >> zero;
+  if (nbox < 0) return io_fail("bad box count in Cell_H");
+  bx.assign(size_t(nbox) * 6, 0);
+  for (int b = 0; b < nbox; ++b) {
+    std::string tok;
+    int lo[3], hi[3], ty[3];
+    ch >> tok;  // "((lo0,lo1,lo2)"
+    if (std::sscanf(tok.c_str(), "((%d,%d,%d)", &lo[0], &lo[1], &lo[2]) != 3)
+      return io_fail("bad box in Cell_H");
+    ch >> tok;
+    if (std::sscanf(tok.c_str(), "(%d,%d,%d)", &hi[0], &hi[1], &hi[2]) != 3)
+      return io_fail("bad box in Cell_H");
+    ch >> tok;
+    if (std::sscanf(tok.c_str(), "(%d,%d,%d))", &ty[0], &ty[1], &ty[2]) != 3)
+      return io_fail("bad box in Cell_H");
+    for (int d = 0; d < 3; ++d) {
+      bx[size_t(6 * b + d)] = lo[d];
+      bx[size_t(6 * b + 3 + d)] = hi[d];
+    }
+  }
+  ch >> paren;
+  int nfab = 0;
+  ch >> nfab;
+  if (nfab != nbox) return io_fail("unexpected FabOnDisk count");
+  files.assign(size_t(nbox), "");
+  offs.assign(size_t(nbox), 0);
+  for (int b = 0; b < nbox; ++b) {
+    std::string tag;
+    ch >> tag >> files[size_t(b)] >> offs[size_t(b)];
+    if (tag != "FabOnDisk:") return io_fail("bad FabOnDisk line");
+  }
+  return CAMR_OK;
+}
+
+// One FAB of box [lo, hi] into row(c, j, k)[i].
+template <class Row>
+camr_status read_fab(const std::string& file, int64_t off, const int lo[3], const int hi[3],
+                     int ncomp, Row row) {
+  std::FILE* f = std::fopen(file.c_str(), "rb");
+  if (!f) return io_fail("cannot read " + file);
+  if (std::fseek(f, long(off), SEEK_SET) != 0) {
+    std::fclose(f);
+    return io_fail("seek failed");
+  }
+  char line[512];
+  if (!std::fgets(line, sizeof line, f) || std::strncmp(line, kFabFormat, std::strlen(kFabFormat))) {
+    std::fclose(f);
+    return io_fail("unexpected FAB header");
+  }
+  const int64_t bc = int64_t(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+  std::vector<double> buf(static_cast<size_t>(bc));
+  for (int c = 0; c < ncomp; ++c) {
+    if (std::fread(buf.data(), sizeof(double), size_t(bc), f) != size_t(bc)) {
+      std::fclose(f);
+      return io_fail("short FAB data");
+    }
+    int64_t t = 0;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j) {
+        double* r = row(c, j, k);
+        for (int i = lo[0]; i <= hi[0]; ++i) r[i] = buf[size_t(t++)];
+      }
+  }
+  std::fclose(f);
+  return CAMR_OK;
+}
+
+// Level 0 into the domain-shaped state (first ncomp planes).
+camr_status read_level0(const std::string& root, const camr_geom* geom, int ncomp, double* state) {
+  int n[3];
+  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
+  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
+  std::vector<int> bx;
+  std::vector<std::string> files;
+  std::vector<int64_t> offs;
+  camr_status cs = read_cell_h(root + "/Level_0", ncomp, bx, files, offs);
+  if (cs != CAMR_OK) return cs;
+  const int nbox = int(files.size());
+  if (!boxes_inside(nbox, bx.data(), geom->dom_lo, geom->dom_hi)) return io_fail("box outside domain");
+  for (int b = 0; b < nbox; ++b) {
+    cs = read_fab(root + "/Level_0/" + files[size_t(b)], offs[size_t(b)], &bx[size_t(6 * b)],
+                  &bx[size_t(6 * b + 3)], ncomp, [&](int c, int j, int k) {
+                    return state + int64_t(c) * ncell +
+                           (int64_t(k - geom->dom_lo[2]) * n[1] + (j - geom->dom_lo[1])) * n[0] -
+                           geom->dom_lo[0];
+                  });
+    if (cs != CAMR_OK) return cs;
+  }
+  return CAMR_OK;
+}
+
 bool boxes_inside(int nbox, const int* boxes, const int dlo[3], const int dhi[3]) {
   for (int b = 0; b < nbox; ++b)
     for (int d = 0; d < 3; ++d) {
@@ -321,101 +448,55 @@ camr_status camr_read_plotfile(const char* dir, const camr_geom* geom, int ncomp
   g_io_error.clear();
   if (!dir || !geom || ncomp <= 0 || !state) return io_fail("invalid arguments");
   const std::string root(dir);
-  int n[3];
-  for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
-  const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
-  {
-    std::ifstream h(root + "/Header");
-    if (!h) return io_fail("cannot read " + root + "/Header");
-    std::string type;
-    int nv = 0;
-    h >> type >> nv;
-    if (type != "HyperCLaw-V1.1" || nv != ncomp) return io_fail("unexpected plotfile header");
-    std::string name;
-    for (int c = 0; c < nv; ++c) h >> name;
-    int dim = 0, finest = 0;
-    double t = 0.0;
-    h >> dim >> t >> finest;
-    if (dim != 3 || finest != 0) return io_fail("only single-level 3-D plotfiles are read");
-    if (time) *time = t;
-    double v;
-    for (int d = 0; d < 6; ++d) h >> v;  // problem box
-    std::string dom;
-    h >> dom >> dom >> dom;               // "((lo) (hi) (type))" as three tokens
-    int step = 0;
-    h >> step;
-    if (level_step) *level_step = step;
+  int finest = 0;
+  int steps[2] = {0, 0};
+  camr_status cs = read_header(root, ncomp, &finest, time, steps);
+  if (cs != CAMR_OK) return cs;
+  if (finest != 0) return io_fail("only single-level 3-D plotfiles are read");
+  if (level_step) *level_step = steps[0];
+  return read_level0(root, geom, ncomp, state);
+}
+
+camr_status camr_read_plotfile_amr(const char* dir, const camr_geom* geom, int ncomp,
+                                   double* state0, int nbox1, const int* boxes1,
+                                   double* state1, double* time, int level_step[2]) {
+  g_io_error.clear();
+  if (!dir || !geom || ncomp <= 0 || !state0 || nbox1 < 0 || (nbox1 > 0 && (!boxes1 || !state1)))
+    return io_fail("invalid arguments");
+  const std::string root(dir);
+  int finest = 0;
+  int steps[2] = {0, 0};
+  camr_status cs = read_header(root, ncomp, &finest, time, steps);
+  if (cs != CAMR_OK) return cs;
+  if (finest != (nbox1 > 0 ? 1 : 0)) return io_fail("level count differs from the hierarchy's");
+  if (level_step) {
+    level_step[0] = steps[0];
+    level_step[1] = steps[1];
   }
-  std::ifstream ch(root + "/Level_0/Cell_H");
-  if (!ch) return io_fail("cannot read Level_0/Cell_H");
-  int version = 0, how = 0, nc = 0, ngrow = 0;
-  ch >> version >> how >> nc >> ngrow;
-  if (nc != ncomp || ngrow != 0) return io_fail("unexpected Cell_H");
-  char paren;
-  int nbox = 0, zero = 0;
-  ch >> paren >> nbox >> zero;
-  std::vector<int> bx(size_t(nbox) * 6);
-  for (int b = 0; b < nbox; ++b) {
-    std::string tok;
-    ch >> tok;  // "((lo0,lo1,lo2)"
-    int lo[3], hi[3], ty[3];
-    if (std::sscanf(tok.c_str(), "((%d,%d,%d)", &lo[0], &lo[1], &lo[2]) != 3)
-      return io_fail("bad box in Cell_H");
-    ch >> tok;
-    if (std::sscanf(tok.c_str(), "(%d,%d,%d)", &hi[0], &hi[1], &hi[2]) != 3)
-      return io_fail("bad box in Cell_H");
-    ch >> tok;
-    if (std::sscanf(tok.c_str(), "(%d,%d,%d))", &ty[0], &ty[1], &ty[2]) != 3)
-      return io_fail("bad box in Cell_H");
-    for (int d = 0; d < 3; ++d) {
-      bx[6 * b + d] = lo[d];
-      bx[6 * b + 3 + d] = hi[d];
-      if (lo[d] < geom->dom_lo[d] || hi[d] > geom->dom_hi[d]) return io_fail("box outside domain");
-    }
-  }
-  ch >> paren;
-  int nfab = 0;
-  ch >> nfab;
-  if (nfab != nbox) return io_fail("unexpected FabOnDisk count");
-  std::vector<std::string> files(nbox);
-  std::vector<int64_t> offs(nbox);
-  for (int b = 0; b < nbox; ++b) {
-    std::string tag;
-    ch >> tag >> files[b] >> offs[b];
-    if (tag != "FabOnDisk:") return io_fail("bad FabOnDisk line");
-  }
-  std::vector<double> buf;
-  for (int b = 0; b < nbox; ++b) {
-    std::FILE* f = std::fopen((root + "/Level_0/" + files[b]).c_str(), "rb");
-    if (!f) return io_fail("cannot read " + files[b]);
-    if (std::fseek(f, long(offs[b]), SEEK_SET) != 0) {
-      std::fclose(f);
-      return io_fail("seek failed");
-    }
-    char line[512];
-    if (!std::fgets(line, sizeof line, f) || std::strncmp(line, kFabFormat, std::strlen(kFabFormat))) {
-      std::fclose(f);
-      return io_fail("unexpected FAB header");
-    }
-    const int* lo = &bx[6 * b];
-    const int* hi = &bx[6 * b + 3];
-    const int64_t bc = int64_t(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
-    buf.resize(size_t(bc));
-    for (int c = 0; c < ncomp; ++c) {
-      if (std::fread(buf.data(), sizeof(double), size_t(bc), f) != size_t(bc)) {
-        std::fclose(f);
-        return io_fail("short FAB data");
-      }
-      double* dst = state + int64_t(c) * ncell;
-      int64_t t = 0;
-      for (int k = lo[2]; k <= hi[2]; ++k)
-        for (int j = lo[1]; j <= hi[1]; ++j) {
-          double* row = dst + (int64_t(k - geom->dom_lo[2]) * n[1] + (j - geom->dom_lo[1])) * n[0] -
-                        geom->dom_lo[0];
-          for (int i = lo[0]; i <= hi[0]; ++i) row[i] = buf[size_t(t++)];
-        }
-    }
-    std::fclose(f);
+  cs = read_level0(root, geom, ncomp, state0);
+  if (cs != CAMR_OK || nbox1 == 0) return cs;
+  // level 1: the same boxes, in the same order, as the hierarchy's
+  std::vector<int> bx;
+  std::vector<std::string> files;
+  std::vector<int64_t> offs;
+  cs = read_cell_h(root + "/Level_1", ncomp, bx, files, offs);
+  if (cs != CAMR_OK) return cs;
+  if (int(files.size()) != nbox1) return io_fail("fine box count differs from the hierarchy's");
+  for (int k = 0; k < 6 * nbox1; ++k)
+    if (bx[size_t(k)] != boxes1[k]) return io_fail("fine boxes differ from the hierarchy's");
+  int64_t base = 0;
+  for (int b = 0; b < nbox1; ++b) {
+    const int* lo = boxes1 + 6 * b;
+    const int* hi = boxes1 + 6 * b + 3;
+    const int64_t bxn = hi[0] - lo[0] + 1, byn = hi[1] - lo[1] + 1, bzn = hi[2] - lo[2] + 1;
+    double* dst = state1 + base;
+    cs = read_fab(root + "/Level_1/" + files[size_t(b)], offs[size_t(b)], lo, hi, ncomp,
+                  [&](int c, int j, int k) {
+                    return dst + int64_t(c) * bxn * byn * bzn + (int64_t(k - lo[2]) * byn +
+                                                                  (j - lo[1])) * bxn - lo[0];
+                  });
+    if (cs != CAMR_OK) return cs;
+    base += int64_t(CAMR_NVAR) * bxn * byn * bzn;
   }
   return CAMR_OK;
 }

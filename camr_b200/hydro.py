@@ -573,6 +573,28 @@ def write_plotfile_amr(path, S0, S1, geom, prob_hi, fine_boxes, time=0.0, level_
                                lib().camr_io_last_error().decode())
 
 
+def read_plotfile_amr(path, geom, fine_boxes, ncomp=NVAR):
+    """Read a plotfile of write_plotfile_amr back for the hierarchy with
+    these fine boxes: returns (S0 (ncomp, nz, ny, nx), S1 flat in the
+    AmrHierarchy.set_state layout, time, (step0, step1))."""
+    n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+    s0 = np.zeros((ncomp, n[2], n[1], n[0]))
+    ncell1 = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in fine_boxes)
+    s1 = np.zeros(NVAR * ncell1)
+    b1 = np.array([list(lo) + list(hi) for lo, hi in fine_boxes], dtype=np.int32).ravel()
+    t = C.c_double()
+    steps = (C.c_int * 2)()
+    st = lib().camr_read_plotfile_amr(str(path).encode(), C.byref(geom), int(ncomp),
+                                      s0.ctypes.data, len(fine_boxes),
+                                      b1.ctypes.data if len(fine_boxes) else None,
+                                      s1.ctypes.data if len(fine_boxes) else None, C.byref(t),
+                                      steps)
+    if st != 0:
+        raise native.CamrError(st, "camr_read_plotfile_amr " +
+                               lib().camr_io_last_error().decode())
+    return s0, s1, t.value, (steps[0], steps[1])
+
+
 def read_plotfile(path, geom, ncomp=NVAR):
     """Read a single-level plotfile written by write_plotfile: returns
     (state planes (ncomp, nz, ny, nx), time, level_step)."""

@@ -159,6 +159,9 @@ SIGNATURES = {
                                           C.POINTER(C.c_double * 3), C.c_double, C.c_void_p,
                                           C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                           C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "camr_read_plotfile_amr": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.c_int, C.c_void_p,
+                                         C.c_int, C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_double), C.c_void_p]),
     "camr_io_last_error": (C.c_char_p, []),
     "camr_adjoint_create": (C.c_int, [C.POINTER(Geom), C.POINTER(HydroParams), C.c_int,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),

@@ -468,6 +468,13 @@ camr_status camr_write_plotfile_amr(const char* dir, const camr_geom* geom, cons
                                     const int* boxes0, const double* state0, int nbox1,
                                     const int* boxes1, const double* state1, int ncomp,
                                     const int* comps, const char* const* names);
+/* Reads a plotfile of camr_write_plotfile_amr back: level 0 into state0
+ * (first ncomp planes), level 1 into state1 laid out as for the writer; the
+ * file's fine boxes must be boxes1 in the same order (a restart of the same
+ * hierarchy).  level_step (may be NULL) receives both levels' steps. */
+camr_status camr_read_plotfile_amr(const char* dir, const camr_geom* geom, int ncomp,
+                                   double* state0, int nbox1, const int* boxes1,
+                                   double* state1, double* time, int level_step[2]);
 /* Why the last plotfile call on this thread failed ("" if it did not). */
 const char* camr_io_last_error(void);
 

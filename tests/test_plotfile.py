@@ -192,6 +192,32 @@ def test_two_level_plotfile(tmp_path, native_lib):
         assert np.array_equal(v, p)
 
 
+def test_two_level_plotfile_round_trip(tmp_path, native_lib):
+    """write_plotfile_amr -> read_plotfile_amr returns both levels bit for
+    bit; a hierarchy with other fine boxes is refused."""
+    n = (8, 8, 8)
+    geom = hydro.make_geom(n)
+    s0 = P.random_smooth(n, seed=4)
+    fine = [((0, 0, 0), (7, 5, 3)), ((10, 8, 6), (15, 15, 15))]
+    rng = np.random.default_rng(5)
+    cells = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in fine)
+    s1 = rng.standard_normal(10 * cells)
+    path = tmp_path / "plt_rt"
+    hydro.write_plotfile_amr(path, s0, s1, geom, (1, 1, 1), fine, time=0.5, level_steps=(3, 6),
+                             max_grid_size=(4, 4, 4))
+    b0, b1, t, steps = hydro.read_plotfile_amr(path, geom, fine)
+    assert np.array_equal(b0, s0) and np.array_equal(b1, s1)
+    assert t == 0.5 and steps == (3, 6)
+    with pytest.raises(native.CamrError):
+        hydro.read_plotfile_amr(path, geom, [((0, 0, 0), (7, 5, 3))])
+    with pytest.raises(native.CamrError):
+        hydro.read_plotfile(path, geom)  # two levels: not a single-level plotfile
+    # a single-level plotfile reads back through the two-level reader too
+    hydro.write_plotfile(tmp_path / "plt_one", s0, geom, (1, 1, 1), time=0.25, level_step=2)
+    c0, _, t1, st1 = hydro.read_plotfile_amr(tmp_path / "plt_one", geom, [])
+    assert np.array_equal(c0, s0) and t1 == 0.25 and st1[0] == 2
+
+
 def test_two_level_plotfile_rejects_fine_box_outside(tmp_path, native_lib):
     geom = hydro.make_geom((8, 8, 8))
     with pytest.raises(native.CamrError):
