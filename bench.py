@@ -171,6 +171,19 @@ def whole_job_rate(world, zones_per_rank, steps, ms):
     return world * zones_per_rank * steps / (ms * 1e-3)
 
 
+def c1_config(n, world):
+    """The `config` of the C1 line (both arms report the same one)."""
+    state_gb = 10 * n[0] * n[1] * n[2] * 8 / 1e9
+    return {"workload": f"c1: {n[0]}^3 periodic CTU-PPM, CFL 0.7, 16 blobs",
+            "domain": list(n), "method": "CTU Godunov, PPM, two-shock Riemann",
+            "cfl": CFL,
+            "boxes": f"{(n[0] // 64) * (n[1] // 64) * (n[2] // 64)} x 64^3 "
+                     "(advanced as one padded domain)",
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 (state {state_gb:.2g} GB, intermediates "
+                  f"~{state_gb * 18.7:.2g} GB)"}
+
+
 def c1_state(n):
     from camr_b200 import problems as P
     dx = tuple(1.0 / v for v in n)
@@ -204,15 +217,14 @@ def run_reference(args, world, rank):
         return
     n = (128, 128, 128)
     rate, secs, kind, nth = cpu_reference_rate(n, args.steps, warmup=args.warmup)
-    sample = (f"{n[0]}^3 sample of the workload (same blob statistics), {args.steps} steps, "
-              f"tiles 1024x16x16, {nth} threads")
+    sample = (f"{n[0]}^3 sample of the workload (the same blob field at half the "
+              f"resolution), {args.steps} steps, tiles 1024x16x16, {nth} threads")
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
-        "data": "synthetic (seeded blobs)",
-        "config": {"workload": "c1 CTU-PPM periodic blobs, CFL 0.7", "domain": list(n),
-                   "method": "CTU-PPM", "cfl": CFL},
+        "data": "synthetic (seeded overpressure blobs, numpy PCG64 seed 1)",
+        "config": c1_config((args.n, args.n, args.n), world),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nth,
                          "kind": "reference" if kind == "ref" else "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -377,11 +389,7 @@ def run_camr(args, world, rank, local, pg):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded overpressure blobs, numpy PCG64 seed 1)",
-            "config": {"workload": "c1: 256^3 periodic CTU-PPM, CFL 0.7, 16 blobs",
-                       "domain": list(n), "method": "CTU Godunov, PPM, two-shock Riemann",
-                       "cfl": CFL, "boxes": "64 x 64^3 (advanced as one padded domain)",
-                       "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (state 1.3 GB, intermediates ~25 GB)"},
+            "config": c1_config(n, world),
             "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "stages_ms": acc, "device_error": list(err),
