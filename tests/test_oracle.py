@@ -67,6 +67,32 @@ def test_restatement_equals_reference_box(cfg, bcs):
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_restatement_equals_reference_subbox(cfg):
+    """A box inside a larger domain whose index space starts at (-3, 2, 0),
+    touching only the z-low wall."""
+    n = (20, 16, 12)
+    dlo = (-3, 2, 0)
+    lev = oracle.make_level(n, lo=dlo, periodic=(0, 1, 0), bc_lo=(1, 0, 4), bc_hi=(2, 0, 5))
+    p = oracle.default_params(**CONFIGS[cfg])
+    s = P.random_smooth(n, seed=8)
+    oracle.init_finalize("ref", p, lev, s)
+    border = oracle.expand_state("ref", p, lev, s)
+    assert same_bits(border, oracle.expand_state("restate", p, lev, s)) == 0
+    dt = 0.5 * oracle.est_dt("ref", p, lev, s)
+    lo, hi = [2, 5, 0], [11, 12, 6]
+    dhi = [dlo[d] + n[d] - 1 for d in range(3)]
+    args = (p, lo, hi, list(dlo), dhi, list(lev.bc_lo), list(lev.bc_hi), border,
+            [dlo[d] - 4 for d in range(3)], list(lev.dx), dt)
+    a = oracle.hydro_box("restate", *args)
+    b = oracle.hydro_box("ref", *args)
+    assert a[2] == 0 and b[2] == 0
+    assert same_bits(a[0], b[0]) == 0
+    for d in range(3):
+        assert same_bits(a[1][d], b[1][d]) == 0
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built (reference sources absent)")
 @pytest.mark.parametrize("cfg", ["ctu_ppm", "mol_plm"])
 def test_restatement_equals_reference_run(cfg):
     n = (16, 12, 10)
