@@ -224,7 +224,10 @@ def run_reference(args, world, rank):
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
         "data": "synthetic (seeded overpressure blobs, numpy PCG64 seed 1)",
-        "config": c1_config((args.n, args.n, args.n), world),
+        "config": dict(c1_config(n, world),
+                       workload=f"c1 sample: {n[0]}^3 periodic CTU-PPM, CFL 0.7, 16 blobs "
+                                f"(the {args.n}^3 workload's blob field at {n[0]}^3; "
+                                "zone-updates/s does not depend on the domain size)"),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nth,
                          "kind": "reference" if kind == "ref" else "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -180,5 +180,8 @@ void launches_sub(int64_t n);  // take back launches counted during a capture
 // camr_last_error_string.
 camr_status cuda_status_of(cudaError_t e);
 const char* last_error_text();
+// The parameter checks of the per-box hydro and the level drivers
+// (Source/CAMR.cpp:160-190): CAMR_OK, or the status to return.
+camr_status check_hydro_params(const camr_hydro_params* p);
 
 }  // namespace camr

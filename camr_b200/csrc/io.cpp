@@ -447,6 +447,8 @@ camr_status camr_read_plotfile(const char* dir, const camr_geom* geom, int ncomp
                                double* state, double* time, int* level_step) {
   g_io_error.clear();
   if (!dir || !geom || ncomp <= 0 || !state) return io_fail("invalid arguments");
+  // the state holds NVAR planes: more components would write past its end
+  if (ncomp > CAMR_NVAR) return io_fail("ncomp exceeds NVAR");
   const std::string root(dir);
   int finest = 0;
   int steps[2] = {0, 0};
@@ -463,6 +465,9 @@ camr_status camr_read_plotfile_amr(const char* dir, const camr_geom* geom, int n
   g_io_error.clear();
   if (!dir || !geom || ncomp <= 0 || !state0 || nbox1 < 0 || (nbox1 > 0 && (!boxes1 || !state1)))
     return io_fail("invalid arguments");
+  // level-1 boxes lie NVAR planes apart in state1: more components would
+  // write into the next box and past the end of the array
+  if (ncomp > CAMR_NVAR) return io_fail("ncomp exceeds NVAR");
   const std::string root(dir);
   int finest = 0;
   int steps[2] = {0, 0};

@@ -58,6 +58,8 @@ struct camr_level {
   double* staging;     // packed (NVAR x ncell) device buffer for state input
   double* staging_out; // packed device buffer for state output
   double* fixed_dev;   // device copy of one fixed dt
+  double* src_h = nullptr;  // sources_for_hydro (CTU with gravity), padded NVAR
+  bool ctu_grav = false;
   bool own_stream;     // the library created `stream` (caller passed NULL)
   int64_t kernels_per_step;  // launches inside one captured step
   // Host transfers run on their own streams so that the next state upload
@@ -73,7 +75,13 @@ namespace {
 
 camr_status cuda_status(cudaError_t e) { return camr::cuda_status_of(e); }
 
-camr_status check_params(const camr_hydro_params* p) {
+camr_status check_params(const camr_hydro_params* p) { return camr::check_hydro_params(p); }
+
+}  // namespace
+
+namespace camr {
+
+camr_status check_hydro_params(const camr_hydro_params* p) {
   if (!p) return CAMR_ERR_INVALID;
   if (p->riemann_solver < 0 || p->riemann_solver > 1) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
@@ -83,7 +91,7 @@ camr_status check_params(const camr_hydro_params* p) {
   return CAMR_OK;
 }
 
-}  // namespace
+}  // namespace camr
 
 extern "C" {
 
@@ -183,9 +191,6 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   if (!desc || !out) return CAMR_ERR_INVALID;
   camr_status cs = check_params(p);
   if (cs != CAMR_OK) return cs;
-  // Sources for the CTU transverse terms come from const_grav; only the
-  // zero-gravity case (every source +0) is implemented on the device.
-  if (p->add_grav_src && p->const_grav != 0.0 && !p->do_mol) return CAMR_ERR_UNSUPPORTED;
   camr_level* lev = new (std::nothrow) camr_level();
   if (!lev) return CAMR_ERR_NOMEM;
   lev->hp = *p;
@@ -232,8 +237,12 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   lev->hist_cap = 1 << 16;
   LevelState& S = lev->st;
   const bool mol = p->do_mol != 0;
+  // A CTU step with gravity feeds the old-time source into the hydro
+  // (hydro_srctoprim); with const_grav = 0 every source term is +0, which
+  // the kernels reproduce without a source array.
+  lev->ctu_grav = !mol && p->add_grav_src && p->const_grav != 0.0;
   const size_t state_bytes = size_t(sp.sn) * NVAR * sizeof(double);
-  const size_t work_bytes = work_doubles(sp, mol, false) * sizeof(double);
+  const size_t work_bytes = work_doubles(sp, mol, lev->ctu_grav) * sizeof(double);
   cudaError_t e = cudaSuccess;
   // Zero-fill on the level's own stream: a non-blocking stream does not
   // order against the legacy default stream, so a plain cudaMemset could
@@ -248,6 +257,7 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   if (mol) alloc(reinterpret_cast<void**>(&S.B2), state_bytes);
   for (int d = 0; d < 3; ++d) alloc(reinterpret_cast<void**>(&S.flx[d]), state_bytes);
   alloc(reinterpret_cast<void**>(&S.work), work_bytes);
+  if (lev->ctu_grav) alloc(reinterpret_cast<void**>(&lev->src_h), state_bytes);
   alloc(reinterpret_cast<void**>(&S.dt_cur), sizeof(double));
   alloc(reinterpret_cast<void**>(&S.dt_hist), sizeof(double) * lev->hist_cap);
   alloc(reinterpret_cast<void**>(&S.dtmin_bits), sizeof(unsigned long long));
@@ -270,7 +280,7 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
     return cuda_status(e);
   }
   S.w.s = sp;
-  work_carve(S.w, S.work, mol, false);
+  work_carve(S.w, S.work, mol, lev->ctu_grav);
   *out = lev;
   return CAMR_OK;
 }
@@ -284,7 +294,7 @@ camr_status camr_level_destroy(camr_level* lev) {
   void* ptrs[] = {S.S,        S.S_old,  S.B,        S.B2,         S.flx[0],
                   S.flx[1],   S.flx[2], S.work,     S.dt_cur,     S.dt_hist,
                   S.dtmin_bits, S.nstep, S.err,     lev->staging, lev->staging_out,
-                  lev->fixed_dev};
+                  lev->fixed_dev, lev->src_h};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t ev : {lev->in_free, lev->in_ready, lev->out_ready, lev->out_free})
@@ -431,6 +441,13 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   const Space& sp = S.w.s;
   H.uin = sdfab(S.B);
   H.src = H.uin;
+  if (lev->ctu_grav) {
+    mark("src_hydro");
+    k_src_hydro<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S_old, lev->src_h);
+    count_launch();
+    H.has_src = true;
+    H.src = sdfab(lev->src_h);
+  }
   cudaError_t e = launch_hydro_fluxes(H, S.w, st);
   if (e != cudaSuccess) return e;
   if (!H.mol) {

@@ -299,6 +299,46 @@ __global__ void __launch_bounds__(kBlk) k_expand(LGeom L, KParams P, const doubl
   store_cell(B, L, L.idx(i, j, k), s);
 }
 
+// sources_for_hydro of a CTU step with gravity (Source/Hydro/
+// CAMR_construct_hydro_source.cpp:28-34): zero, plus 1.0 x the old-time
+// gravity source (Source/GravitySrc.cpp:36-70, from the cleaned S_old) on
+// valid cells, copied to the ghost cells inside the periodic extension of
+// the domain (FillBoundary); ghost cells beyond a physical boundary keep 0.
+__global__ void __launch_bounds__(kBlk) k_src_hydro(LGeom L, KParams P, const double* S_old,
+                                                     double* out) {
+  int i, j, k;
+  if (!padded_cell(L, tid(), i, j, k)) return;
+  const int c[3] = {i, j, k};
+  int img[3];
+  bool physical = false;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    img[d] = c[d];
+    if (c[d] < L.dlo[d] || c[d] > L.dhi[d]) {
+      if (L.periodic[d]) {
+        const int len = L.dhi[d] - L.dlo[d] + 1;
+        img[d] = L.dlo[d] + (((c[d] - L.dlo[d]) % len) + len) % len;
+      } else {
+        physical = true;
+      }
+    }
+  }
+  const int64_t at = L.idx(i, j, k);
+  double src[NVAR];
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+  if (!physical) {
+    const int64_t im = L.idx(img[0], img[1], img[2]);
+    src[UMZ] = P.const_grav * S_old[im + URHO * L.sn];
+    src[UEDEN] = P.const_grav * S_old[im + UMZ * L.sn];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) out[at + n * L.sn] = 0.0 + 1.0 * src[n];
+  } else {
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) out[at + n * L.sn] = 0.0;
+  }
+}
+
 // Block-wide min of positive doubles into *bits (order-preserving as u64).
 __device__ __forceinline__ void block_min_dt(double v, unsigned long long* bits) {
   unsigned long long b = __double_as_longlong(v);

@@ -9,9 +9,9 @@
 // permitted or would fight another allocator.
 //
 // Limits: the scratch holds CAMR_NOALLOC_SCRATCH_BYTES (64 MiB), enough for
-// a cubic CTU box of up to 28^3 cells or a MOL box of up to 49^3 (without
-// sources); larger boxes are rejected with CAMR_ERR_INVALID (use
-// camr_hydro_umdrv for them).
+// a cubic CTU box of up to 28^3 cells or a MOL box of up to 49^3 without a
+// source fab (with one, CTU boxes up to 27^3); larger boxes are rejected
+// with CAMR_ERR_INVALID (use camr_hydro_umdrv for them).
 // The array lives in every GPU that loads this library until the process
 // exits.  All calls share the one array: calls that overlap on the GPU (two
 // streams, two host threads) race on it and must be serialised by the caller.
@@ -36,21 +36,36 @@ std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
 thread_local char g_msg[200] = "";
 
-// One-time set-up on the current device: the scratch's device address.
-cudaError_t scratch_address(void** out) {
+// The scratch's device address on the current device.  Outside stream
+// capture it is looked up again on every call (a cheap table lookup once
+// the module is loaded), so a device reset, which reloads the module at a
+// new address, never leaves a stale pointer behind.  While `st` is being
+// captured the address cached by the last uncaptured call on this device
+// is used: the first call on a device must come before any capture.
+cudaError_t scratch_address(cudaStream_t st, void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_addr[dev] = p;
+  } else if (!g_addr[dev]) {
+    return cudaErrorStreamCaptureUnsupported;
   }
   *out = g_addr[dev];
   return cudaSuccess;
+}
+
+camr_status reject(camr_status s, const char* why) {
+  std::snprintf(g_msg, sizeof(g_msg), "%s", why);
+  return s;
 }
 
 }  // namespace
@@ -67,17 +82,21 @@ extern "C" camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx
   g_msg[0] = '\0';
   if (!bx_lo || !bx_hi || !geom || !uin || !dsdt || !flx0 || !flx1 || !flx2 || !p ||
       !uin->ptr || !dsdt->ptr || !flx0->ptr || !flx1->ptr || !flx2->ptr)
-    return CAMR_ERR_INVALID;
-  if (p->riemann_solver < 0 || p->riemann_solver > 1 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
-  if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
+    return reject(CAMR_ERR_INVALID, "a required pointer is NULL");
+  // the same parameter checks as camr_hydro_umdrv
+  const camr_status cs = check_hydro_params(p);
+  if (cs != CAMR_OK) return reject(cs, "parameters rejected (as camr_hydro_umdrv rejects them)");
   for (int d = 0; d < 3; ++d) {
-    if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
-    if (uin->lo[d] > bx_lo[d] - NGROW || uin->hi[d] < bx_hi[d] + NGROW) return CAMR_ERR_INVALID;
+    if (bx_hi[d] < bx_lo[d]) return reject(CAMR_ERR_INVALID, "empty box");
+    if (uin->lo[d] > bx_lo[d] - NGROW || uin->hi[d] < bx_hi[d] + NGROW)
+      return reject(CAMR_ERR_INVALID, "uin does not cover grow(bx, 4)");
     if (src && src->ptr && (src->lo[d] > bx_lo[d] - NGROW || src->hi[d] < bx_hi[d] + NGROW))
-      return CAMR_ERR_INVALID;
-    if (dsdt->lo[d] > bx_lo[d] || dsdt->hi[d] < bx_hi[d]) return CAMR_ERR_INVALID;
+      return reject(CAMR_ERR_INVALID, "src does not cover grow(bx, 4)");
+    if (dsdt->lo[d] > bx_lo[d] || dsdt->hi[d] < bx_hi[d])
+      return reject(CAMR_ERR_INVALID, "dsdt does not cover bx");
   }
-  if (uin->ncomp < NVAR || dsdt->ncomp < NVAR) return CAMR_ERR_INVALID;
+  if (uin->ncomp < NVAR || dsdt->ncomp < NVAR)
+    return reject(CAMR_ERR_INVALID, "uin and dsdt need NVAR components");
 
   const bool mol = p->do_mol != 0;
   const bool has_src = src && src->ptr;
@@ -91,7 +110,8 @@ extern "C" camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx
     return CAMR_ERR_INVALID;
   }
   void* base = nullptr;
-  if (scratch_address(&base) != cudaSuccess) return CAMR_ERR_CUDA;
+  const cudaError_t ea = scratch_address(static_cast<cudaStream_t>(stream), &base);
+  if (ea != cudaSuccess) return cuda_status_of(ea);
   // Every scratch slot a call reads is written earlier in the same call
   // (each pass reads only the regions the previous passes produced), so no
   // clearing is needed between calls.
@@ -118,6 +138,5 @@ extern "C" camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx
   Lh.dsdt = make_dfab(*dsdt);
   Lh.dt = DtRef{dt, nullptr};
   Lh.err = nullptr;
-  const cudaError_t e = launch_hydro(Lh, w, static_cast<cudaStream_t>(stream));
-  return e == cudaSuccess ? CAMR_OK : CAMR_ERR_CUDA;
+  return cuda_status_of(launch_hydro(Lh, w, static_cast<cudaStream_t>(stream)));
 }

@@ -486,9 +486,11 @@ const char* camr_io_last_error(void);
  * cudaMalloc/cudaMallocAsync would fight another allocator).  Same
  * arguments and results as camr_hydro_umdrv; the scratch is a fixed
  * CAMR_NOALLOC_SCRATCH_BYTES array in device memory, which every GPU that
- * loads the library keeps until the process exits.  Boxes whose scratch
- * does not fit are rejected with CAMR_ERR_INVALID (camr_noalloc_last_error
- * says why).  The first call on a device looks up the array's device
+ * loads the library keeps until the process exits.  It holds a CTU box of
+ * up to 28^3 cells or a MOL box of up to 49^3 without a source fab (CTU up
+ * to 27^3 with one).  Boxes whose scratch does not fit are rejected with
+ * CAMR_ERR_INVALID, and parameters exactly as camr_hydro_umdrv rejects them
+ * (camr_noalloc_last_error says why).  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress); make that first call before any stream
  * capture.  All calls share the one array: calls that overlap on the GPU
  * race on it and must be serialised by the caller.  Calls no cudaMalloc,

@@ -101,13 +101,19 @@ def lib_path(kind):
     raise ValueError(kind)
 
 
-def build(ref=None):
-    """Build the restatement, and the reference library when its sources exist."""
+def build(ref=None, ref_src=None):
+    """Build the restatement, and the reference library from the reference
+    checkout's Source/ directory: `ref_src`, else $CAMR_REF_SRC.  ref=None
+    builds the reference library when such a directory is given and exists;
+    ref=True without one is an error."""
     subprocess.run(["make", "-C", HERE, "all"], check=True)
-    src = os.environ.get("CAMR_REF_SRC", "/root/reference/Source")
+    src = ref_src or os.environ.get("CAMR_REF_SRC")
     if ref is None:
-        ref = os.path.isdir(src)
+        ref = bool(src) and os.path.isdir(src)
     if ref:
+        if not src:
+            raise RuntimeError("building the reference library needs its Source/ directory: "
+                               "pass ref_src= or set CAMR_REF_SRC")
         subprocess.run(["make", "-C", HERE, "ref", f"REF_SRC={src}"], check=True)
 
 

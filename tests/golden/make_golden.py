@@ -1,7 +1,8 @@
 """Generate the golden fixtures from the reference's own hydro kernels.
 
-Run where the reference sources exist (it builds oracle/_ref):
-    python tests/golden/make_golden.py
+Run where the reference sources exist (it builds oracle/_ref from the
+reference checkout's Source/ directory named by CAMR_REF_SRC):
+    CAMR_REF_SRC=<reference checkout>/Source python tests/golden/make_golden.py
 Each fixture stores its exact inputs (small arrays) and the SHA-256 of the
 exact bytes the reference produced, plus summary sums for diagnostics.
 The reference's repository holds no tests, golden data or fixtures of its

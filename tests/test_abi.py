@@ -78,3 +78,32 @@ def test_batch_tuning_arguments_rejected_without_gpu(native_lib):
     assert native.STATUS[st] == "CAMR_ERR_INVALID"
     st = native_lib.camr_eb_level_autotune(None)
     assert native.STATUS[st] == "CAMR_ERR_INVALID"
+
+
+def test_per_box_entry_points_reject_the_same_parameters(native_lib):
+    """camr_hydro_umdrv and camr_hydro_umdrv_noalloc validate parameters the
+    same way, before any CUDA call (the fab pointers are never read)."""
+    from camr_b200 import native
+    lo = (C.c_int * 3)(0, 0, 0)
+    hi = (C.c_int * 3)(7, 7, 7)
+    geom = native.Geom()
+    fabs = []
+    for _ in range(5):
+        f = native.Fab()
+        f.ptr = 0x1000  # never dereferenced: the checks fail first
+        f.lo = (C.c_int * 3)(-4, -4, -4)
+        f.hi = (C.c_int * 3)(11, 11, 11)
+        f.ncomp = 10
+        fabs.append(f)
+    uin, dsdt, fx, fy, fz = fabs
+    bad = [dict(cfl=1.5), dict(cfl=0.0), dict(do_mol=1, cfl=0.5), dict(riemann_solver=7),
+           dict(do_mol=0, ppm_type=3)]
+    for cfg in bad:
+        p = native.default_params(**cfg)
+        got = []
+        for fn in (native_lib.camr_hydro_umdrv, native_lib.camr_hydro_umdrv_noalloc):
+            got.append(fn(C.byref(lo), C.byref(hi), C.byref(geom), C.byref(uin), None,
+                          C.byref(dsdt), C.byref(fx), C.byref(fy), C.byref(fz), C.byref(p),
+                          1e-3, None))
+        assert got[0] == got[1] != 0, (cfg, got)
+        assert native_lib.camr_noalloc_last_error() != b""

@@ -22,7 +22,11 @@ def test_reference_arm_line(tmp_path):
     import bench
     assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
     assert line["higher_is_better"] is True and line["steps"] == 1
-    assert line["config"] == bench.c1_config((256, 256, 256), 1)
+    # the C1 config's keys, with the workload naming the sample that ran
+    full = bench.c1_config((256, 256, 256), 1)
+    assert set(line["config"]) == set(full)
+    assert line["config"]["workload"].startswith("c1 sample: 128^3")
+    assert line["config"]["domain"] == [128, 128, 128]
     assert line["value"] > 0 and line["cpu_baseline"]["value"] == line["value"]
     assert line["cpu_baseline"]["kind"] in ("reference", "port")
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"],

@@ -119,6 +119,23 @@ def test_plotfile_rejects_bad_input(tmp_path, native_lib):
         hydro.read_plotfile(tmp_path / "missing", geom)
 
 
+def test_plotfile_readers_reject_more_components_than_nvar(tmp_path, native_lib):
+    """A plotfile may repeat components (11 here); the readers fill NVAR-plane
+    states, so they refuse ncomp > NVAR instead of writing past them."""
+    n = (8, 8, 8)
+    geom = hydro.make_geom(n)
+    s = P.random_smooth(n, seed=3)
+    comps = list(range(10)) + [0]
+    path = tmp_path / "plt_11"
+    hydro.write_plotfile(path, s, geom, (1, 1, 1), comps=comps,
+                         names=NAMES + ["density_again"])
+    assert independent_read(path)["names"][-1] == "density_again"
+    for read in (lambda: hydro.read_plotfile(path, geom, ncomp=11),
+                 lambda: hydro.read_plotfile_amr(path, geom, [((0, 0, 0), (3, 3, 3))], ncomp=11)):
+        with pytest.raises(native.CamrError, match="ncomp exceeds NVAR"):
+            read()
+
+
 def read_level(path, lev, nv):
     """Boxes and per-box arrays of Level_<lev> (VisMF header + FAB data)."""
     cell_h = (path / f"Level_{lev}" / "Cell_H").read_text().split("\n")

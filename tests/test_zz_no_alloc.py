@@ -104,3 +104,26 @@ def test_noalloc_rejects_boxes_beyond_the_scratch(native_lib):
                flx, prm, 1e-3)
     assert native.STATUS[st] == "CAMR_ERR_INVALID"
     assert b"static scratch" in native_lib.camr_noalloc_last_error()
+
+
+def test_noalloc_rejects_a_source_box_beyond_the_scratch(native_lib):
+    """A 28^3 CTU box fits without a source fab but not with one."""
+    torch = _torch()
+    from camr_b200 import hydro, native
+    n = (28, 28, 28)
+    geom = hydro.make_geom(n)
+    prm = native.default_params(do_mol=0, ppm_type=1)
+    uin = torch.ones((10, n[2] + 8, n[1] + 8, n[0] + 8), dtype=torch.float64, device="cuda:0")
+    src = torch.zeros_like(uin)
+    dsdt, flx = _fresh(torch, n, np.zeros((10, n[2], n[1], n[0])))
+    lo, hi = [0, 0, 0], [27, 27, 27]
+    fu = hydro.fab_of(uin, [-4, -4, -4])
+    fs = hydro.fab_of(src, [-4, -4, -4])
+    fd = hydro.fab_of(dsdt, lo)
+    ff = [hydro.fab_of(f, lo) for f in flx]
+    st = native_lib.camr_hydro_umdrv_noalloc(
+        C.byref((C.c_int * 3)(*lo)), C.byref((C.c_int * 3)(*hi)), C.byref(geom), C.byref(fu),
+        C.byref(fs), C.byref(fd), C.byref(ff[0]), C.byref(ff[1]), C.byref(ff[2]),
+        C.byref(prm), 1e-3, None)
+    assert native.STATUS[st] == "CAMR_ERR_INVALID"
+    assert b"static scratch" in native_lib.camr_noalloc_last_error()
