@@ -887,7 +887,7 @@ extern "C" {
 camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* boxes,
                             const camr_hydro_params* p, void* stream, camr_amr** out) {
   if (!base || !p || !out || nbox < 1 || !boxes) return CAMR_ERR_INVALID;
-  if (p->riemann_solver < 0 || p->riemann_solver > 1 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver < 0 || p->riemann_solver > 1) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
   if (p->cfl <= 0.0 || p->cfl > 1.0) return CAMR_ERR_INVALID;
   if (p->do_mol && p->cfl > 0.3 && p->fixed_dt <= 0.0) return CAMR_ERR_INVALID;

@@ -152,7 +152,7 @@ camr_status batch_create_impl(int nbox, const camr_box_task* tasks, const camr_g
                               camr_batch** out, const unsigned* ebflag = nullptr,
                               const int* eblo = nullptr, const int* ebn = nullptr) {
   if (nbox <= 0 || !tasks || !geom || !p || !out) return CAMR_ERR_INVALID;
-  if (p->riemann_solver < 0 || p->riemann_solver > 1 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver < 0 || p->riemann_solver > 1) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   camr_batch* b = new (std::nothrow) camr_batch();

@@ -622,6 +622,17 @@ __device__ __forceinline__ void ebc_trace_cell(int i, int j, int k, const EBWork
     slope[n] = plm_slope(qq[at - 2 * st], qq[at - st], qq[at], qq[at + st], qq[at + 2 * st], fl,
                          order);
   }
+  if (P.use_pslope && order > 0) {
+    // plm_pslope_eb (PLM_eb.H:63-104) with the zero predictor sources of an
+    // EB Godunov step
+    double pv[5], rv[5], su[5];
+    for (int o = 0; o < 5; ++o) {
+      pv[o] = W.q[at + (o - 2) * st + SQ_P * s.sn];
+      rv[o] = W.q[at + (o - 2) * st + SQ_RHO * s.sn];
+      su[o] = 0.0;
+    }
+    slope[ES_P] = plm_pslope(pv, rv, su, g.dx[d], fl, order);
+  }
   double qp_o[ES_N], qm_o[ES_N];
   plm_edge_states<d>(W.q, at, s.sn, slope, dt / g.dx[d], P, qp_o, qm_o);
   if (!(G.a(d, i, j, k) > 0.0))
@@ -1611,7 +1622,7 @@ extern "C" camr_status camr_hydro_umdrv_eb(const int bx_lo[3], const int bx_hi[3
                                            void* stream) {
   if (!bx_lo || !bx_hi || !geom || !uin || !eb || !dsdt || !flx0 || !flx1 || !flx2 || !p)
     return CAMR_ERR_INVALID;
-  if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
   // Godunov with EB is PLM only (Source/CAMR.cpp:186-190)
   if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;
   if (p->eb_weights_type < 0 || p->eb_weights_type > 3 || redist < 0 || redist > 2)
@@ -1822,7 +1833,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
                                  camr_eb_level** out) {
   if (!desc || !eb || !p || !out) return CAMR_ERR_INVALID;
   *out = nullptr;
-  if (p->riemann_solver != 0 || p->use_pslope) return CAMR_ERR_UNSUPPORTED;
+  if (p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
   // Godunov with EB is PLM only (Source/CAMR.cpp:186-190); its predictor
   // sources are taken as zero, so no gravity with Godunov
   if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;

@@ -163,7 +163,8 @@ template <int d>
 __device__ __forceinline__ void trace_body(int i, int j, int k, const Space& s,
                                            const KGeom& g, const KParams& P,
                                            const DtRef& dtr, const double* q,
-                                           const double* flat, double* smd, double* spd) {
+                                           const double* flat, double* smd, double* spd,
+                                           const double* srcq = nullptr) {
   const int64_t at = s.idx(i, j, k);
   const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
   const double dt = dtr.get();
@@ -243,6 +244,17 @@ __device__ __forceinline__ void trace_body(int i, int j, int k, const Space& s,
       stencil(slot_of[n], sv);
       slope[n] = plm_slope(sv[0], sv[1], sv[2], sv[3], sv[4], fl, P.plm_iorder);
     }
+    if (P.use_pslope) {
+      // Godunov_3D.cpp:120-146: the pressure slope of plm_pslope, with
+      // the primitive sources (zero when the box has none)
+      double pv[5], rv[5], su[5];
+      stencil(SQ_P, pv);
+      stencil(SQ_RHO, rv);
+#pragma unroll
+      for (int o = 0; o < 5; ++o)
+        su[o] = srcq ? srcq[at + (o - 2) * st + (ES_U + d) * s.sn] : 0.0;
+      slope[ES_P] = plm_pslope(pv, rv, su, g.dx[d], fl, P.plm_iorder);
+    }
     plm_edge_states<d>(q, at, s.sn, slope, dt / g.dx[d], P, qp_o, qm_o);
   }
   store_es(spd, s, at, qp_o);
@@ -253,13 +265,14 @@ __global__ void __launch_bounds__(kBlock, CAMR_MINB_TRACE) k_trace(Region r, Spa
                                                    DtRef dtr, const double* q,
                                                    const double* flat, double* sm0,
                                                    double* sm1, double* sm2, double* sp0,
-                                                   double* sp1, double* sp2) {
+                                                   double* sp1, double* sp2,
+                                                   const double* srcq) {
   int i, j, k;
   if (!region_cell(r, gtid(), i, j, k)) return;
   switch (blockIdx.y) {
-    case 0: trace_body<0>(i, j, k, s, g, P, dtr, q, flat, sm0, sp0); break;
-    case 1: trace_body<1>(i, j, k, s, g, P, dtr, q, flat, sm1, sp1); break;
-    default: trace_body<2>(i, j, k, s, g, P, dtr, q, flat, sm2, sp2); break;
+    case 0: trace_body<0>(i, j, k, s, g, P, dtr, q, flat, sm0, sp0, srcq); break;
+    case 1: trace_body<1>(i, j, k, s, g, P, dtr, q, flat, sm1, sp1, srcq); break;
+    default: trace_body<2>(i, j, k, s, g, P, dtr, q, flat, sm2, sp2, srcq); break;
   }
 }
 
@@ -675,9 +688,9 @@ __device__ __forceinline__ void batched_cell(const BoxCtx& c, int sub, int i, in
     flatten_divu_body(i, j, k, w.s, c.g, P, !c.mol, w.q, w.flat, w.divu);
   } else if constexpr (STAGE == BS_TRACE) {
     switch (sub) {
-      case 0: trace_body<0>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[0], w.sp[0]); break;
-      case 1: trace_body<1>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[1], w.sp[1]); break;
-      default: trace_body<2>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[2], w.sp[2]); break;
+      case 0: trace_body<0>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[0], w.sp[0], w.srcq); break;
+      case 1: trace_body<1>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[1], w.sp[1], w.srcq); break;
+      default: trace_body<2>(i, j, k, w.s, c.g, P, dt, w.q, w.flat, w.sm[2], w.sp[2], w.srcq); break;
     }
   } else if constexpr (STAGE == BS_FLUX1) {
     switch (sub) {
@@ -840,7 +853,8 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
   if (!L.mol) {
     mark("trace");
     k_trace<<<dim3(grid_for(r1.count()), 3), kBlock, 0, st>>>(
-        r1, s, g, L.P, L.dt, w.q, w.flat, w.sm[0], w.sm[1], w.sm[2], w.sp[0], w.sp[1], w.sp[2]);
+        r1, s, g, L.P, L.dt, w.q, w.flat, w.sm[0], w.sm[1], w.sm[2], w.sp[0], w.sp[1], w.sp[2],
+        w.srcq);
     // first pass: E-faces [lo,hi+1] x grow(bx,1) in the other directions
     Region rf[3];
     for (int E = 0; E < 3; ++E) {

@@ -480,6 +480,40 @@ __device__ __forceinline__ double plm_slope(double qm2, double qm, double qc, do
   return flat * dsgn * dmin(dlim, fabs(dtemp));
 }
 
+// plm_pslope (Source/Hydro/Godunov/PLM.H:84-165): the pressure slope with
+// the hydrostatic part rho * src_u * dx taken out of each difference and
+// added back at the end (use_pslope = 1).  p, r, su: the 5-point stencils
+// of pressure, density and the primitive source of the normal velocity.
+__device__ __forceinline__ double plm_pslope(const double* p, const double* r, const double* su,
+                                             double dx, double flat, int order) {
+  if (order == 1) return 0.;
+  double dlft, drgt, dcen, dfm = 0.0, dfp = 0.0, dlim, dsgn, dtemp;
+  const double qm2 = p[0], qm = p[1], qc = p[2], qp = p[3], qp2 = p[4];
+  if (order == 4) {
+    dlft = qm - qm2 - 0.25 * dx * (r[1] + r[0]) * (su[1] + su[0]);
+    drgt = qc - qm - 0.25 * dx * (r[1] + r[2]) * (su[1] + su[2]);
+    dcen = 0.5 * (dlft + drgt);
+    dsgn = copysign(1.0, dcen);
+    dlim = (dlft * drgt >= 0.0) ? 2.0 * dmin(fabs(dlft), fabs(drgt)) : 0.0;
+    dfm = dsgn * dmin(dlim, fabs(dcen));
+    dlft = qp - qc - 0.25 * dx * (r[3] + r[2]) * (su[3] + su[2]);
+    drgt = qp2 - qp - 0.25 * dx * (r[3] + r[4]) * (su[3] + su[4]);
+    dcen = 0.5 * (dlft + drgt);
+    dsgn = copysign(1.0, dcen);
+    dlim = (dlft * drgt >= 0.0) ? 2.0 * dmin(fabs(dlft), fabs(drgt)) : 0.0;
+    dfp = dsgn * dmin(dlim, fabs(dcen));
+  }
+  dlft = qc - qm - 0.25 * dx * (r[2] + r[1]) * (su[2] + su[1]);
+  drgt = qp - qc - 0.25 * dx * (r[2] + r[3]) * (su[2] + su[3]);
+  dcen = 0.5 * (dlft + drgt);
+  dsgn = copysign(1.0, dcen);
+  dlim = (dlft * drgt >= 0.0) ? 2.0 * dmin(fabs(dlft), fabs(drgt)) : 0.0;
+  dtemp = 4.0 / 3.0 * dcen - 1.0 / 6.0 * (dfp + dfm);
+  double dp = flat * dsgn * dmin(dlim, fabs(dtemp));
+  dp += r[2] * su[2] * dx;
+  return dp;
+}
+
 // ---------------------------------------------------------------------------
 // Transverse corrections (Source/Hydro/Godunov/Godunov_utils_3D.H).  The
 // reference's transdo/transdd each fill the plus state on a cell's low face

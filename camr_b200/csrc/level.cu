@@ -60,6 +60,7 @@ struct camr_level {
   double* fixed_dev;   // device copy of one fixed dt
   double* src_h = nullptr;  // sources_for_hydro (CTU with gravity), padded NVAR
   bool ctu_grav = false;
+  FloorList floor;          // cells below the density floor of the current pass
   bool own_stream;     // the library created `stream` (caller passed NULL)
   int64_t kernels_per_step;  // launches inside one captured step
   // Host transfers run on their own streams so that the next state upload
@@ -85,7 +86,6 @@ camr_status check_hydro_params(const camr_hydro_params* p) {
   if (!p) return CAMR_ERR_INVALID;
   if (p->riemann_solver < 0 || p->riemann_solver > 1) return CAMR_ERR_UNSUPPORTED;
   if (!p->do_mol && p->ppm_type != 0 && p->ppm_type != 1) return CAMR_ERR_INVALID;
-  if (p->use_pslope) return CAMR_ERR_UNSUPPORTED;
   if (p->cfl <= 0.0 || p->cfl > 1.0) return CAMR_ERR_INVALID;  // CAMR.cpp:172-174
   if (p->do_mol && p->cfl > 0.3 && p->fixed_dt <= 0.0) return CAMR_ERR_INVALID;  // :175-177
   return CAMR_OK;
@@ -270,6 +270,10 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   for (cudaEvent_t* ev : {&lev->in_free, &lev->in_ready, &lev->out_ready, &lev->out_free})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   alloc(reinterpret_cast<void**>(&lev->fixed_dev), sizeof(double));
+  alloc(reinterpret_cast<void**>(&lev->floor.count), sizeof(int));
+  alloc(reinterpret_cast<void**>(&lev->floor.cells), sizeof(int64_t) * kFloorCap);
+  alloc(reinterpret_cast<void**>(&lev->floor.enforced), sizeof(double) * NVAR * kFloorCap);
+  alloc(reinterpret_cast<void**>(&lev->floor.total), sizeof(unsigned long long));
   if (e != cudaSuccess) {
     camr_level_destroy(lev);
     return CAMR_ERR_NOMEM;
@@ -294,7 +298,8 @@ camr_status camr_level_destroy(camr_level* lev) {
   void* ptrs[] = {S.S,        S.S_old,  S.B,        S.B2,         S.flx[0],
                   S.flx[1],   S.flx[2], S.work,     S.dt_cur,     S.dt_hist,
                   S.dtmin_bits, S.nstep, S.err,     lev->staging, lev->staging_out,
-                  lev->fixed_dev, lev->src_h};
+                  lev->fixed_dev, lev->src_h, lev->floor.count, lev->floor.cells,
+                  lev->floor.enforced, lev->floor.total};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t ev : {lev->in_free, lev->in_ready, lev->out_ready, lev->out_free})
@@ -401,10 +406,30 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   mark("dt_next");
   k_dt_next<<<1, 1, 0, st>>>(c, first ? 1 : 0, fixed_dev, S.dtmin_bits, S.dt_cur, S.dt_hist,
                              S.nstep, lev->hist_cap);
+  // Each cleaning pass lists the cells below the density floor and a
+  // one-block fixup resets them in the reference's order (a no-op launch
+  // when the list is empty).
+  const FloorList& fl = lev->floor;
+  auto fixup = [&](int mode, FloorArgs a) {
+    switch (mode) {
+      case FLOOR_CLEAN: k_floor_fixup<FLOOR_CLEAN><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
+      case FLOOR_EXPAND: k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
+      case FLOOR_CTU: k_floor_fixup<FLOOR_CTU><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
+      default: k_floor_fixup<FLOOR_MOL2><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
+    }
+    count_launch();
+  };
+  FloorArgs fa{};
   mark("clean_copy");
-  k_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, S.S, S.S_old, S.err);
+  k_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, S.S, S.S_old, S.err, fl);
+  fa.in = S.S;
+  fa.out = S.S_old;
+  fixup(FLOOR_CLEAN, fa);
   mark("expand");
-  k_expand<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S_old, S.B, S.err);
+  k_expand<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S_old, S.B, S.err, fl);
+  fa.in = S.S_old;
+  fa.out = S.B;
+  fixup(FLOOR_EXPAND, fa);
   count_launch(3);
   HydroLaunch H;
   for (int d = 0; d < 3; ++d) {
@@ -453,22 +478,29 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   if (!H.mol) {
     mark("update");
     k_update_ctu<<<gv, kBlk, 0, st>>>(L, sp, lev->P, S.dt_cur, S.B, S.S_old, fp, S.S,
-                                      S.dtmin_bits, S.err);
+                                      S.dtmin_bits, S.err, 1, fl);
     count_launch();
+    FloorArgs fu{nullptr, S.S, S.B, S.S_old, fp, sp, S.dt_cur, S.dtmin_bits, 1};
+    fixup(FLOOR_CTU, fu);
   } else {
     mark("update_mol1");
     k_update_mol1<<<gv, kBlk, 0, st>>>(L, sp, lev->P, S.dt_cur, S.B, S.S_old, fp, S.S);
     mark("expand2");
-    k_expand<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S, S.B2, S.err);
+    k_expand<<<grid_of(npad), kBlk, 0, st>>>(L, lev->P, S.S, S.B2, S.err, fl);
     count_launch(2);
+    fa.in = S.S;
+    fa.out = S.B2;
+    fixup(FLOOR_EXPAND, fa);
     H.uin = sdfab(S.B2);
     H.src = H.uin;
     e = launch_hydro_fluxes(H, S.w, st);
     if (e != cudaSuccess) return e;
     mark("update_mol2");
     k_update_mol2<<<gv, kBlk, 0, st>>>(L, sp, lev->P, S.dt_cur, S.B2, S.S_old, fp, S.S,
-                                       S.dtmin_bits, S.err);
+                                       S.dtmin_bits, S.err, 1, fl);
     count_launch();
+    FloorArgs fu{nullptr, S.S, S.B2, S.S_old, fp, sp, S.dt_cur, S.dtmin_bits, 1};
+    fixup(FLOOR_MOL2, fu);
   }
   mark("end");
   return cudaGetLastError();
@@ -601,6 +633,17 @@ camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab) {
   fab->kstride = lev->L.sz;
   fab->nstride = lev->L.sn;
   fab->ncomp = NVAR;
+  return CAMR_OK;
+}
+
+camr_status camr_level_floor_resets(camr_level* lev, int64_t* cells) {
+  if (!lev || !cells) return CAMR_ERR_INVALID;
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, lev->floor.total, sizeof(h), cudaMemcpyDeviceToHost,
+                                  lev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  *cells = int64_t(h);
   return CAMR_OK;
 }
 

@@ -229,14 +229,38 @@ __device__ __forceinline__ bool valid_cell(const LGeom& L, int64_t t, int& i, in
   return true;
 }
 
+// Cells below the density floor met by a fused clean or update pass.  The
+// reference's enforce_min_density (Source/CAMR.cpp:941-1045) walks a box's
+// cells in raster order and resets each one in place, so a cell reset early
+// can be the neighbour a later cell copies: a parallel pass cannot
+// reproduce that.  The pass therefore appends such cells here and
+// k_floor_fixup redoes them one after another in the reference's order.
+// count == nullptr: no list; the pass then resets from the neighbours'
+// values before the reset (exact when no two flagged cells are neighbours)
+// and an update pass reports the crossing in the error word.
+constexpr int kFloorCap = 4096;
+struct FloorList {
+  int* count = nullptr;        // cells appended by the current pass (reset by the fixup)
+  int64_t* cells = nullptr;    // their padded-array indices (kFloorCap)
+  double* enforced = nullptr;  // kFloorCap x NVAR scratch of the fixup
+  unsigned long long* total = nullptr;  // cells reset since the level was created
+};
+
+__device__ __forceinline__ void floor_push(const FloorList& fl, int64_t at) {
+  const int slot = atomicAdd(fl.count, 1);
+  if (slot < kFloorCap) fl.cells[slot] = at;
+}
+
 // clean_state on valid cells: S_old = clean(S)  (CAMR_advance.cpp:83).
 __global__ void __launch_bounds__(kBlk) k_clean_copy(LGeom L, KParams P, const double* S,
-                                                      double* out, DevError* err) {
+                                                      double* out, DevError* err,
+                                                      FloorList fl = FloorList{}) {
   int i, j, k;
   if (!valid_cell(L, tid(), i, j, k)) return;
   const int64_t at = L.idx(i, j, k);
   double s[NVAR];
   load_cell(S, L, at, s);
+  if (fl.count && s[URHO] < P.small_dens) floor_push(fl, at);
   enforce_min_density(s, S, L, P, i, j, k, err);
   normalize_species(s);
   compute_temp(s, P);
@@ -250,7 +274,8 @@ __global__ void __launch_bounds__(kBlk) k_clean_copy(LGeom L, KParams P, const d
 // src (foextrap / reflect_even / reflect_odd; ext_dir copies the boundary
 // cell as Exec/Sod's bcnormal does) and only computeTemp.
 __global__ void __launch_bounds__(kBlk) k_expand(LGeom L, KParams P, const double* src,
-                                                  double* B, DevError* err) {
+                                                  double* B, DevError* err,
+                                                  FloorList fl = FloorList{}) {
   int i, j, k;
   if (!padded_cell(L, tid(), i, j, k)) return;
   const int c[3] = {i, j, k};
@@ -271,6 +296,9 @@ __global__ void __launch_bounds__(kBlk) k_expand(LGeom L, KParams P, const doubl
   double s[NVAR];
   if (!physical) {
     load_cell(src, L, L.idx(img[0], img[1], img[2]), s);
+    // the valid cell itself (not a periodic ghost image) joins the list
+    if (fl.count && s[URHO] < P.small_dens && img[0] == i && img[1] == j && img[2] == k)
+      floor_push(fl, L.idx(i, j, k));
     enforce_min_density(s, src, L, P, img[0], img[1], img[2], err);
     normalize_species(s);
   } else {
@@ -391,6 +419,12 @@ __global__ void __launch_bounds__(kBlk) k_est_dt(LGeom L, KParams P, const doubl
   block_min_dt(v, bits);
 }
 
+// Error code of a density that fails `rho >= small_dens`: 3 exactly zero
+// (amrex::Error in enforce_min_density), 5 below the floor, 2 NaN.
+__device__ __forceinline__ int floor_code(double rho, const KParams& P) {
+  return rho == 0. ? 3 : (rho < P.small_dens ? 5 : 2);
+}
+
 // The end of a level step on one valid cell, from the state right after
 // the hydro Saxpy: clean_state, the new-source correction (+ its
 // clean_state) and, with `post`, post_timestep's clean_state (a level that
@@ -399,10 +433,10 @@ __global__ void __launch_bounds__(kBlk) k_est_dt(LGeom L, KParams P, const doubl
 __device__ __forceinline__ double finish_step(double* s, const double* sold, const KParams& P,
                                               const LGeom& L, double dt, int i, int j, int k,
                                               DevError* err, bool post = true) {
-  // clean_state(S_new): enforce_min_density cannot see the other cells'
-  // post-Saxpy values inside this fused pass; a density below the floor is
-  // reported instead of reset.
-  if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
+  // clean_state(S_new).  The density floor is handled before this point
+  // (k_floor_fixup resets the cells below it); a density still below the
+  // floor here (no floor list) or NaN is reported in the error word.
+  if (!(s[URHO] >= P.small_dens)) report_error(err, floor_code(s[URHO], P), i, j, k);
   normalize_species(s);
   compute_temp(s, P);
   if (P.add_grav_src) {
@@ -413,12 +447,12 @@ __device__ __forceinline__ double finish_step(double* s, const double* sold, con
     src[UEDEN] = 0.5 * P.const_grav * (s[UMZ] - sold[UMZ]);
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-    if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
+    if (!(s[URHO] >= P.small_dens)) report_error(err, floor_code(s[URHO], P), i, j, k);
     normalize_species(s);
     compute_temp(s, P);
   }
   if (post) {
-    if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
+    if (!(s[URHO] >= P.small_dens)) report_error(err, floor_code(s[URHO], P), i, j, k);
     normalize_species(s);
     compute_temp(s, P);
   }
@@ -459,40 +493,57 @@ struct FluxPtrs {
   double* q[3];
 };
 
-// CTU: S_new = Sborder (+ dt*src_old) + dt*dSdt, then finish_step.
+// CTU: the state right after the Saxpys, S_new = Sborder (+ dt*src_old) +
+// dt*dSdt; sold receives the old density and z momentum the gravity terms
+// read (zero without gravity).
+__device__ __forceinline__ void ctu_raw(const LGeom& L, const Space& sp, const KParams& P,
+                                        double dt, const double* B, const double* S_old,
+                                        const FluxPtrs& fp, int i, int j, int k, double* s,
+                                        double* sold) {
+  const int64_t at = L.idx(i, j, k);
+  double hs[NVAR];
+  load_cell(B, L, at, s);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) sold[n] = 0.0;
+  if (P.add_grav_src) {
+    sold[URHO] = S_old[at + URHO * L.sn];
+    sold[UMZ] = S_old[at + UMZ * L.sn];
+  }
+  if (P.add_grav_src) {
+    double src[NVAR];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+    src[UMZ] = P.const_grav * sold[URHO];
+    src[UEDEN] = P.const_grav * sold[UMZ];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
+  }
+  cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] += dt * hs[n];
+}
+
+// CTU: S_new = Sborder (+ dt*src_old) + dt*dSdt, then finish_step.  With a
+// floor list, a cell below the density floor keeps its post-Saxpy state
+// and joins the list (k_floor_fixup finishes it).
 __global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) k_update_ctu(LGeom L, Space sp, KParams P,
                                                       const double* dtp, const double* B,
                                                       const double* S_old, FluxPtrs fp,
                                                       double* S, unsigned long long* bits,
-                                                      DevError* err, int post = 1) {
+                                                      DevError* err, int post = 1,
+                                                      FloorList fl = FloorList{}) {
   int i, j, k;
   double v = DBL_MAX;
   if (valid_cell(L, tid(), i, j, k)) {
     const double dt = *dtp;
     const int64_t at = L.idx(i, j, k);
-    double s[NVAR], sold[NVAR], hs[NVAR];
-    load_cell(B, L, at, s);
-    // the old-time source and its correction in finish_step read only the
-    // old density and z momentum
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) sold[n] = 0.0;
-    if (P.add_grav_src) {
-      sold[URHO] = S_old[at + URHO * L.sn];
-      sold[UMZ] = S_old[at + UMZ * L.sn];
+    double s[NVAR], sold[NVAR];
+    ctu_raw(L, sp, P, dt, B, S_old, fp, i, j, k, s, sold);
+    if (fl.count && s[URHO] < P.small_dens) {
+      floor_push(fl, at);
+    } else {
+      v = finish_step(s, sold, P, L, dt, i, j, k, err, post != 0);
     }
-    if (P.add_grav_src) {
-      double src[NVAR];
-#pragma unroll
-      for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
-      src[UMZ] = P.const_grav * sold[URHO];
-      src[UEDEN] = P.const_grav * sold[UMZ];
-#pragma unroll
-      for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-    }
-    cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += dt * hs[n];
-    v = finish_step(s, sold, P, L, dt, i, j, k, err, post != 0);
     store_cell(S, L, at, s);
   }
   if (bits) block_min_dt(v, bits);
@@ -524,30 +575,291 @@ __global__ void __launch_bounds__(kBlk) k_update_mol1(LGeom L, Space sp, KParams
   store_cell(S, L, at, s);
 }
 
-// MOL stage 2: S_new = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2 (LinComb then
-// Saxpy, CAMR_advance.cpp:134-135), then finish_step.
+// MOL stage 2 right after the LinComb and Saxpy (CAMR_advance.cpp:134-135):
+// S_new = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2; sold = S_old.
+__device__ __forceinline__ void mol2_raw(const LGeom& L, const Space& sp, double dt,
+                                         const double* B2, const double* S_old,
+                                         const FluxPtrs& fp, int i, int j, int k, double* s,
+                                         double* sold) {
+  const int64_t at = L.idx(i, j, k);
+  double b[NVAR], hs[NVAR];
+  load_cell(B2, L, at, b);
+  load_cell(S_old, L, at, sold);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
+  cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * hs[n];
+}
+
+// MOL stage 2, then finish_step (floor list as k_update_ctu).
 __global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) k_update_mol2(LGeom L, Space sp, KParams P,
                                                        const double* dtp, const double* B2,
                                                        const double* S_old, FluxPtrs fp,
                                                        double* S, unsigned long long* bits,
-                                                       DevError* err, int post = 1) {
+                                                       DevError* err, int post = 1,
+                                                       FloorList fl = FloorList{}) {
   int i, j, k;
   double v = DBL_MAX;
   if (valid_cell(L, tid(), i, j, k)) {
     const double dt = *dtp;
     const int64_t at = L.idx(i, j, k);
-    double s[NVAR], sold[NVAR], b[NVAR], hs[NVAR];
-    load_cell(B2, L, at, b);
-    load_cell(S_old, L, at, sold);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
-    cell_dsdt(L, sp, i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * hs[n];
-    v = finish_step(s, sold, P, L, dt, i, j, k, err, post != 0);
+    double s[NVAR], sold[NVAR];
+    mol2_raw(L, sp, dt, B2, S_old, fp, i, j, k, s, sold);
+    if (fl.count && s[URHO] < P.small_dens) {
+      floor_push(fl, at);
+    } else {
+      v = finish_step(s, sold, P, L, dt, i, j, k, err, post != 0);
+    }
     store_cell(S, L, at, s);
   }
   if (bits) block_min_dt(v, bits);
+}
+
+// What k_floor_fixup finishes: the pass whose list it reads.
+enum { FLOOR_CLEAN = 0, FLOOR_EXPAND = 1, FLOOR_CTU = 2, FLOOR_MOL2 = 3 };
+
+struct FloorArgs {
+  const double* in;   // CLEAN / EXPAND: the array being cleaned
+  double* out;        // CLEAN: S_old; EXPAND: Sborder; CTU / MOL2: S_new
+  const double* B;    // CTU: Sborder; MOL2: Sborder2
+  const double* S_old;
+  FluxPtrs fp;
+  Space sp;
+  const double* dtp;
+  unsigned long long* bits;  // CFL minimum (CTU / MOL2; may be null)
+  int post;
+};
+
+// Sort key of a listed cell: its level box, then its padded index (raster
+// order inside the box).
+__device__ __forceinline__ int64_t floor_key(const LGeom& L, int64_t at, int i, int j, int k) {
+  const int nb0 = (L.dhi[0] - L.dlo[0] + L.boxsz[0]) / L.boxsz[0];
+  const int nb1 = (L.dhi[1] - L.dlo[1] + L.boxsz[1]) / L.boxsz[1];
+  const int64_t box = (i - L.dlo[0]) / L.boxsz[0] +
+                      int64_t(nb0) * ((j - L.dlo[1]) / L.boxsz[1] +
+                                      int64_t(nb1) * ((k - L.dlo[2]) / L.boxsz[2]));
+  return (box << 40) | at;
+}
+
+__device__ __forceinline__ int floor_find(const int64_t* key, int n, int64_t want) {
+  int lo = 0, hi = n - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    if (key[mid] == want) return mid;
+    if (key[mid] < want) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ void decode_cell(const LGeom& L, int64_t at, int& i, int& j, int& k) {
+  k = int(at / L.sz);
+  const int64_t r = at - int64_t(k) * L.sz;
+  j = int(r / L.sy);
+  i = int(r - int64_t(j) * L.sy);
+  i += L.plo[0];
+  j += L.plo[1];
+  k += L.plo[2];
+}
+
+// The state of a cell as enforce_min_density finds it before any reset:
+// the array being cleaned, or (updates) the post-Saxpy state, which the
+// update pass stored for listed cells and which is recomputed for others.
+template <int MODE>
+__device__ __forceinline__ void floor_raw(const LGeom& L, const KParams& P, const FloorArgs& a,
+                                          bool listed, int64_t at, int i, int j, int k,
+                                          double* s) {
+  if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
+    load_cell(a.in, L, at, s);
+  } else {
+    if (listed) {
+      load_cell(a.out, L, at, s);
+    } else {
+      double sold[NVAR];
+      if constexpr (MODE == FLOOR_CTU) ctu_raw(L, a.sp, P, *a.dtp, a.B, a.S_old, a.fp, i, j, k, s, sold);
+      else mol2_raw(L, a.sp, *a.dtp, a.B, a.S_old, a.fp, i, j, k, s, sold);
+    }
+  }
+}
+
+// enforce_min_density (Source/CAMR.cpp:941-1045) on the listed cells in the
+// reference's order -- box by box, cells in raster order, each reset in
+// place so that later cells see it -- then the rest of the listed cells'
+// pass (normalize_species + computeTemp, or the end of the step with its
+// CFL dt).  One block: the list is sorted by (box, raster position); the
+// window of a cell never leaves its box, so the boxes are independent and
+// one thread walks each box's cells in order; then all threads finish the
+// cells.  The window is the level box holding the cell (the reference's GPU
+// build loops over boxes; its OpenMP build over tiles of them).  More than
+// kFloorCap listed cells: error code 5 and the cells stay as the pass left
+// them.  The count is cleared at the end, ready for the next pass.
+template <int MODE>
+__global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorList fl,
+                                                       FloorArgs a, DevError* err) {
+  constexpr int64_t kAtMask = (int64_t(1) << 40) - 1;
+  __shared__ int64_t key[kFloorCap];
+  const int n = *fl.count;
+  if (n == 0) return;
+  if (n > kFloorCap) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int i, j, k;
+      decode_cell(L, fl.cells[0], i, j, k);
+      report_error(err, 5, i, j, k);
+      *fl.count = 0;
+    }
+    return;
+  }
+  int N = 1;
+  while (N < n) N <<= 1;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    if (t < n) {
+      const int64_t at = fl.cells[t];
+      int i, j, k;
+      decode_cell(L, at, i, j, k);
+      key[t] = floor_key(L, at, i, j, k);
+    } else {
+      key[t] = INT64_MAX;
+    }
+  }
+  __syncthreads();
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < N; t += blockDim.x) {
+        const int u = t ^ stride;
+        if (u > t) {
+          const bool up = (t & size) == 0;
+          const int64_t x = key[t], y = key[u];
+          if ((x > y) == up) {
+            key[t] = y;
+            key[u] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  double* enf = fl.enforced;
+  for (int t0 = threadIdx.x; t0 < n; t0 += blockDim.x) {
+    const int64_t box = key[t0] >> 40;
+    if (t0 > 0 && (key[t0 - 1] >> 40) == box) continue;  // not the first cell of its box
+    for (int m = t0; m < n && (key[m] >> 40) == box; ++m) {
+      const int64_t at = key[m] & kAtMask;
+      int i, j, k;
+      decode_cell(L, at, i, j, k);
+      double s[NVAR];
+      floor_raw<MODE>(L, P, a, true, at, i, j, k, s);
+      if (s[URHO] == 0.) {
+        report_error(err, 3, i, j, k);  // amrex::Error in the reference
+      } else {
+        int blo[3], bhi[3];
+        const int c[3] = {i, j, k};
+        for (int d = 0; d < 3; ++d) {
+          const int b = (c[d] - L.dlo[d]) / L.boxsz[d];
+          blo[d] = L.dlo[d] + b * L.boxsz[d];
+          bhi[d] = min(blo[d] + L.boxsz[d] - 1, L.dhi[d]);
+        }
+        double max_dens = s[URHO];
+        int64_t pick = at;
+        int pick_m = -1;
+        for (int kk = -1; kk <= 1; kk++)
+          for (int jj = -1; jj <= 1; jj++)
+            for (int ii = -1; ii <= 1; ii++) {
+              if (i + ii >= blo[0] && j + jj >= blo[1] && k + kk >= blo[2] && i + ii <= bhi[0] &&
+                  j + jj <= bhi[1] && k + kk <= bhi[2]) {
+                const int64_t nat = L.idx(i + ii, j + jj, k + kk);
+                const int mm = floor_find(key, n, (box << 40) | nat);
+                double r;
+                if (mm >= 0 && mm < m) {
+                  r = enf[int64_t(mm) * NVAR + URHO];  // reset earlier in this walk
+                } else if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
+                  r = a.in[nat];
+                } else {
+                  // an update pass stored the post-Saxpy state of listed
+                  // cells; for the others the stored density is the
+                  // post-Saxpy one too (the cleans and the gravity source
+                  // leave the density alone)
+                  r = a.out[nat];
+                }
+                if (r > max_dens) {
+                  pick = nat;
+                  pick_m = mm;
+                  max_dens = r;
+                }
+              }
+            }
+        if (max_dens < P.small_dens) {
+          double massfrac[NSPEC];
+          for (int sp = 0; sp < NSPEC; ++sp) massfrac[sp] = s[UFS + sp] / s[URHO];
+          const double small_e = eos_rty2e(P.gamma, P.small_temp, massfrac);
+          s[URHO] = P.small_dens;
+          s[UTEMP] = P.small_temp;
+          s[UMX] = 0.;
+          s[UMY] = 0.;
+          s[UMZ] = 0.;
+          s[UEINT] = P.small_dens * small_e;
+          s[UEDEN] = s[UEINT];
+        } else if (pick_m >= 0) {
+          // a cell reset earlier (a listed cell not yet reached lies below
+          // the floor, so it never is the densest at or above it)
+          for (int q = 0; q < NVAR; ++q) s[q] = enf[int64_t(pick_m) * NVAR + q];
+        } else {
+          int pi, pj, pk;
+          decode_cell(L, pick, pi, pj, pk);
+          floor_raw<MODE>(L, P, a, false, pick, pi, pj, pk, s);
+        }
+      }
+      for (int q = 0; q < NVAR; ++q) enf[int64_t(m) * NVAR + q] = s[q];
+    }
+  }
+  __syncthreads();
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    const int64_t at = key[m] & kAtMask;
+    int i, j, k;
+    decode_cell(L, at, i, j, k);
+    double s[NVAR];
+    for (int q = 0; q < NVAR; ++q) s[q] = enf[int64_t(m) * NVAR + q];
+    if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
+      normalize_species(s);
+      compute_temp(s, P);
+      if constexpr (MODE == FLOOR_CLEAN) {
+        store_cell(a.out, L, at, s);
+      } else {
+        // the cell and every ghost cell that is its periodic image
+        // (FillBoundary after normalize_species)
+        int lo[3], hi[3], len[3];
+        const int c[3] = {i, j, k};
+        for (int d = 0; d < 3; ++d) {
+          len[d] = L.dhi[d] - L.dlo[d] + 1;
+          lo[d] = hi[d] = 0;
+          if (L.periodic[d]) {
+            while (c[d] + (lo[d] - 1) * len[d] >= L.plo[d]) --lo[d];
+            while (c[d] + (hi[d] + 1) * len[d] <= L.plo[d] + L.pn[d] - 1) ++hi[d];
+          }
+        }
+        for (int mz = lo[2]; mz <= hi[2]; ++mz)
+          for (int my = lo[1]; my <= hi[1]; ++my)
+            for (int mx = lo[0]; mx <= hi[0]; ++mx)
+              store_cell(a.out, L, L.idx(i + mx * len[0], j + my * len[1], k + mz * len[2]), s);
+      }
+    } else {
+      double sold[NVAR];
+      for (int q = 0; q < NVAR; ++q) sold[q] = 0.0;
+      if (P.add_grav_src) {
+        sold[URHO] = a.S_old[at + URHO * L.sn];
+        sold[UMZ] = a.S_old[at + UMZ * L.sn];
+      }
+      const double v = finish_step(s, sold, P, L, *a.dtp, i, j, k, err, a.post != 0);
+      store_cell(a.out, L, at, s);
+      if (a.bits) atomicMin(a.bits, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (fl.total) atomicAdd(fl.total, (unsigned long long)n);
+    *fl.count = 0;
+  }
 }
 
 struct DtCtl {

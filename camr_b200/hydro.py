@@ -218,6 +218,12 @@ class Level:
         lib().camr_level_get_error(self._h, C.byref(info))
         return (info.code, info.i, info.j, info.k)
 
+    def floor_resets(self):
+        """Cells enforce_min_density has reset since the level was created."""
+        v = C.c_int64()
+        check(lib().camr_level_floor_resets(self._h, C.byref(v)), "floor_resets")
+        return v.value
+
     def sync(self):
         _torch().cuda.synchronize()
 

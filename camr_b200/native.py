@@ -88,6 +88,7 @@ SIGNATURES = {
     "camr_level_est_dt": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "camr_level_state_fab": (C.c_int, [C.c_void_p, C.POINTER(Fab)]),
     "camr_level_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
+    "camr_level_floor_resets": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "camr_launch_count": (C.c_int64, []),
     "camr_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_last_error_string": (C.c_char_p, []),

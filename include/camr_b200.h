@@ -110,7 +110,9 @@ typedef struct {
 typedef struct {
   int code;      /* 0 none, 1 non-positive density/energy seen by ctoprim, 2 NaN,
                     3 density exactly zero in enforce_min_density, 4 index
-                    out of range */
+                    out of range, 5 density below small_dens left unreset
+                    (more cells below the floor in one pass than the reset
+                    list holds, or a driver without the list) */
   int i, j, k;   /* cell of the first failure */
 } camr_error_info;
 
@@ -264,6 +266,14 @@ camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab);
 
 /* Read and clear the device error word (synchronises the level's stream). */
 camr_status camr_level_get_error(camr_level* lev, camr_error_info* info);
+
+/* Cells reset by enforce_min_density (Source/CAMR.cpp:941-1045) since the
+ * level was created, counted over every clean_state of every step
+ * (synchronises the level's stream).  Each cleaning pass of a step lists
+ * the cells below small_dens and resets them in the reference's order: box
+ * by box, in raster order, each reset visible to the cells after it.  At
+ * most 4096 cells per pass; more set error code 5. */
+camr_status camr_level_floor_resets(camr_level* lev, int64_t* cells);
 
 /* ---------------------------------------------------------------------
  * Two-level AMR hierarchy (refinement ratio 2, subcycled): a base level

@@ -208,15 +208,16 @@ def test_c4_sod_sphere_64x32x32_150_steps(do_mol):
            nsteps, {"oracle": "ref (EB kernels) + restated redistribution", "boxes": kinds})
 
 
-@pytest.mark.parametrize("ppm_type", [0, 1])
-def test_hydro_umdrv_with_nonzero_sources(ppm_type, oracle_kind, native_lib):
+@pytest.mark.parametrize("ppm_type,pslope", [(0, 0), (1, 0), (0, 1)])
+def test_hydro_umdrv_with_nonzero_sources(ppm_type, pslope, oracle_kind, native_lib):
     """The per-box CTU hydro with a non-zero source fab: hydro_srctoprim
-    (Hydro_ctoprim.H:106-157) feeds the primitive sources into the predictor
-    and the transverse (transdd) corrections."""
+    (Hydro_ctoprim.H:106-157) feeds the primitive sources into the
+    transverse (transdd) corrections and, with use_pslope = 1, into the
+    pressure slope of plm_pslope (PLM.H:84-165)."""
     torch = _torch()
     n = (20, 16, 12)
     bcs = dict(periodic=(0, 1, 0), bc_lo=(2, 0, 4), bc_hi=(2, 0, 3))
-    cfg = dict(do_mol=0, ppm_type=ppm_type)
+    cfg = dict(do_mol=0, ppm_type=ppm_type, use_pslope=pslope)
     p_or = oracle.default_params(**cfg)
     lev = oracle.make_level(n, **bcs)
     s = P.random_smooth(n, seed=31)
@@ -248,15 +249,15 @@ def test_hydro_umdrv_with_nonzero_sources(ppm_type, oracle_kind, native_lib):
     d0, _, _ = oracle.hydro_box(oracle_kind, p_or, lo, hi, lo, hi, list(lev.bc_lo),
                                 list(lev.bc_hi), border, [-4, -4, -4], list(lev.dx), dt)
     assert not np.array_equal(d0, dsdt_o)
-    report(f"hydro_umdrv CTU ppm_type={ppm_type} with sources: dsdt", dsdt.cpu().numpy(), dsdt_o,
-           1, {"oracle": oracle_kind})
+    what = f"hydro_umdrv CTU ppm_type={ppm_type} use_pslope={pslope} with sources"
+    report(f"{what}: dsdt", dsdt.cpu().numpy(), dsdt_o, 1, {"oracle": oracle_kind})
     for d in range(3):
-        report(f"hydro_umdrv CTU ppm_type={ppm_type} with sources: flux {d}",
+        report(f"{what}: flux {d}",
                flx[d].cpu().numpy(), flx_o[d], 1, {"oracle": oracle_kind})
 
 
-@pytest.mark.parametrize("ppm_type", [0, 1])
-def test_level_ctu_with_gravity(ppm_type, oracle_kind, native_lib):
+@pytest.mark.parametrize("ppm_type,pslope", [(0, 0), (1, 0), (0, 1)])
+def test_level_ctu_with_gravity(ppm_type, pslope, oracle_kind, native_lib):
     """CTU level steps with const_grav != 0: the old-time gravity source
     enters the hydro through sources_for_hydro -> hydro_srctoprim
     (CAMR_construct_hydro_source.cpp:28-34, 120-134), the old and new
@@ -265,10 +266,118 @@ def test_level_ctu_with_gravity(ppm_type, oracle_kind, native_lib):
     n = (16, 16, 24)
     bcs = dict(periodic=(1, 1, 0), bc_lo=(0, 0, 4), bc_hi=(0, 0, 4))
     s0 = P.random_smooth(n, seed=17)
-    cfg = dict(do_mol=0, ppm_type=ppm_type, cfl=0.6, const_grav=-2.0)
+    cfg = dict(do_mol=0, ppm_type=ppm_type, cfl=0.6, const_grav=-2.0, use_pslope=pslope)
     got, ref = level_parity(oracle_kind, cfg, n, bcs, s0, 12)
     # gravity changed the flow (else the case would not test the sources)
     flat, _ = level_parity(oracle_kind, dict(cfg, const_grav=0.0), n, bcs, s0, 12)
     assert not np.array_equal(flat, ref)
-    report(f"level CTU ppm_type={ppm_type} const_grav=-2", got, ref, 12,
+    report(f"level CTU ppm_type={ppm_type} use_pslope={pslope} const_grav=-2", got, ref, 12,
            {"oracle": oracle_kind})
+
+
+def evacuating_flow(n, seed=4, speed=3.0):
+    """A smooth random density with the outward flow u = speed (x - 1/2):
+    the centre empties, so cells fall below a raised density floor."""
+    s = P.random_smooth((n, n, n), seed=seed, amp=0.2, vel=0.0)
+    x = (np.arange(n) + 0.5) / n - 0.5
+    vel = (speed * x[None, None, :], speed * x[None, :, None], speed * x[:, None, None])
+    rho = s[P.URHO]
+    for d in range(3):
+        s[P.UMX + d] = rho * vel[d]
+    s[P.UEDEN] = s[P.UEINT] + 0.5 * rho * sum(v * v for v in vel)
+    return s
+
+
+@pytest.mark.parametrize("cfg", [dict(do_mol=0, ppm_type=1, cfl=0.5), dict(do_mol=1, cfl=0.3)],
+                         ids=["ctu_ppm", "mol_plm"])
+def test_density_floor_resets_match_oracle(cfg, oracle_kind, native_lib):
+    """enforce_min_density (Source/CAMR.cpp:941-1045) after the update and in
+    the MOL stage-2 ghost fill: cells below small_dens take the state of the
+    densest neighbour in their box or the small state, in the reference's
+    sequential order, bit for bit, with the error word clear."""
+    _torch()
+    n = 24
+    s0 = evacuating_flow(n)
+    cfg = dict(cfg, small_dens=0.45)
+    mgs = (8, 8, 8)
+    p = oracle.default_params(**cfg)
+    lev = oracle.make_level((n, n, n), max_grid_size=mgs)
+    ref = s0.copy()
+    oracle.init_finalize(oracle_kind, p, lev, ref)
+    _, hist, nass = oracle.advance(oracle_kind, p, lev, ref, 14)
+    assert nass == 0
+    # the floor acts: without it the run ends elsewhere
+    free = s0.copy()
+    oracle.init_finalize(oracle_kind, oracle.default_params(**dict(cfg, small_dens=1e-7)), lev,
+                         free)
+    oracle.advance(oracle_kind, oracle.default_params(**dict(cfg, small_dens=1e-7)), lev, free, 14)
+    assert not np.array_equal(free, ref)
+    L = hydro.Level(hydro.make_geom((n, n, n)), native.default_params(**cfg), max_grid_size=mgs,
+                    use_graph=True)
+    L.set_state(s0)
+    L.init_finalize()
+    L.advance(14)
+    got = L.get_state()
+    resets = L.floor_resets()
+    err = L.error()
+    dt_last = L.last_dt()
+    L.close()
+    assert err[0] == 0, err
+    assert resets > 0
+    assert dt_last == hist[-1]
+    assert ref[P.URHO].min() >= cfg["small_dens"]
+    report(f"density floor {'MOL' if cfg['do_mol'] else 'CTU'}", got, ref, 14,
+           {"oracle": oracle_kind, "cells_reset": resets})
+
+
+@pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
+def test_eb_level_godunov_pslope():
+    """use_pslope = 1 on an EB Godunov-PLM level: plm_pslope_eb (PLM_eb.H:
+    63-104) in the cut boxes, plm_pslope in the regular ones."""
+    _torch()
+    from test_oracle_eb import eb_level_case
+    n = (32, 16, 16)
+    mgs = (8, 8, 8)
+    p, lev, geo, s = eb_level_case("sod", n=n, max_grid_size=mgs, do_mol=0)
+    p.use_pslope = 1
+    ref = s.copy()
+    _, ref_dts, nass = oracle.eb_advance(p, lev, geo, ref, 8, redist=1)
+    assert nass == 0
+    geom = hydro.make_geom(n, is_periodic=(0, 0, 0), bc_lo=(2, 4, 4), bc_hi=(2, 4, 4),
+                           dx=(2.0 / n[0],) * 3)
+    prm = native.default_params(do_mol=0, ppm_type=0, cfl=0.3, use_pslope=1)
+    L = hydro.EBLevel(geom, prm, geo, redist=1, max_grid_size=mgs)
+    L.set_state(s)
+    L.advance(8)
+    got = L.get_state()
+    dts = L.dts()
+    assert L.error()[0] == 0
+    L.close()
+    assert np.array_equal(np.asarray(dts), ref_dts)
+    report("eb level Godunov-PLM use_pslope=1", got, ref, 8, {"oracle": "ref EB kernels"})
+
+
+def test_amr_ctu_plm_pslope(oracle_kind, native_lib):
+    """use_pslope = 1 in the two-level driver (CTU-PLM, zero sources)."""
+    _torch()
+    n0 = (16, 16, 16)
+    boxes = [((8, 8, 8), (15, 15, 23)), ((16, 8, 8), (23, 15, 15))]
+    S0, S1 = P.amr_initial(n0, boxes, nblobs=4, r_min=0.1, r_max=0.2)
+    cfg = dict(do_mol=0, ppm_type=0, cfl=0.5, use_pslope=1)
+    p = oracle.default_params(**cfg)
+    lev = oracle.make_level(n0)
+    bx = np.array([list(lo) + list(hi) for lo, hi in boxes], dtype=np.int32)
+    o0, o1 = S0.copy(), S1.copy()
+    clock = np.zeros(4)
+    oracle.amr_run(oracle_kind, p, lev, bx, o0, o1, 0, do_init=True, clock=clock)
+    _, nerr = oracle.amr_run(oracle_kind, p, lev, bx, o0, o1, 3, first_step=True, clock=clock)
+    assert nerr == 0
+    h = hydro.AmrHierarchy(hydro.make_geom(n0), native.default_params(**cfg), boxes)
+    h.set_state(S0, S1)
+    h.init_finalize()
+    h.advance(3)
+    g0, g1 = h.get_state()
+    assert h.error()[0] == 0
+    h.close()
+    report("amr CTU-PLM use_pslope=1: level 0", g0, o0, 3, {"oracle": oracle_kind})
+    report("amr CTU-PLM use_pslope=1: level 1", g1, o1, 3, {"oracle": oracle_kind})
