@@ -183,5 +183,8 @@ const char* last_error_text();
 // The parameter checks of the per-box hydro and the level drivers
 // (Source/CAMR.cpp:160-190): CAMR_OK, or the status to return.
 camr_status check_hydro_params(const camr_hydro_params* p);
+// The library-wide device error word (camr_get_error) on the current
+// device; looked up outside stream capture, cached for use inside it.
+cudaError_t library_error_word(cudaStream_t st, DevError** out);
 
 }  // namespace camr

@@ -172,7 +172,10 @@ camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3], const camr_
   Lh.flx[2] = make_dfab(*flx2);
   Lh.dsdt = make_dfab(*dsdt);
   Lh.dt = DtRef{dt, nullptr};
-  Lh.err = nullptr;
+  // ctoprim's checks (Hydro_ctoprim.H:56,68) report into the library's
+  // error word (camr_get_error) where the reference asserts
+  cudaError_t ee = library_error_word(st, &Lh.err);
+  if (ee != cudaSuccess) return cuda_status(ee);
   Work w;
   w.s = make_space(bx_lo, bx_hi);
   const size_t bytes = work_doubles(w.s, Lh.mol, Lh.has_src) * sizeof(double);

@@ -83,6 +83,49 @@ def hydro_umdrv(bx_lo, bx_hi, geom, uin, uin_lo, dsdt, flx, params, dt, src=None
     check(st, "camr_hydro_umdrv")
 
 
+def box_fabs(boxes, tensors, ng):
+    """camr_box_fab array for boxes [(lo, hi)] and their (NVAR, nz, ny, nx)
+    CUDA tensors, each covering its box grown by ng."""
+    arr = (native.BoxFab * len(boxes))()
+    for b, ((lo, hi), t) in enumerate(zip(boxes, tensors)):
+        for d in range(3):
+            arr[b].lo[d] = lo[d]
+            arr[b].hi[d] = hi[d]
+        arr[b].fab = fab_of(t, [lo[d] - ng for d in range(3)])
+    return arr
+
+
+def fill_ghosts(geom, boxes, tensors, ng, stream=None):
+    """FillPatch on one level (camr_fill_ghosts): ng ghost layers of every
+    box's tensor from the boxes' valid cells and the physical BCs."""
+    arr = box_fabs(boxes, tensors, ng)
+    check(lib().camr_fill_ghosts(C.byref(geom), len(boxes), arr, int(ng),
+                                 C.c_void_p(_stream_ptr(stream))), "camr_fill_ghosts")
+
+
+def clean_state(geom, boxes, tensors, ng, params, stream=None):
+    """clean_state of the boxes with ng ghost layers (camr_clean_state)."""
+    arr = box_fabs(boxes, tensors, ng)
+    check(lib().camr_clean_state(C.byref(geom), len(boxes), arr, int(ng), C.byref(params),
+                                 C.c_void_p(_stream_ptr(stream))), "camr_clean_state")
+
+
+def est_dt(geom, boxes, tensors, ng, params, stream=None):
+    """estTimeStep's hydro dt over the boxes' valid cells (camr_est_dt)."""
+    arr = box_fabs(boxes, tensors, ng)
+    v = C.c_double()
+    check(lib().camr_est_dt(C.byref(geom), len(boxes), arr, C.byref(params), C.byref(v),
+                            C.c_void_p(_stream_ptr(stream))), "camr_est_dt")
+    return v.value
+
+
+def get_error(stream=None):
+    """Read and clear the library's device error word: (code, i, j, k)."""
+    info = native.ErrorInfo()
+    lib().camr_get_error(C.c_void_p(_stream_ptr(stream)), C.byref(info))
+    return (info.code, info.i, info.j, info.k)
+
+
 def eb_geometry_to_device(geo, device="cuda"):
     """eb_geometry.sphere_geometry output -> dict of CUDA tensors (kept
     alive by the caller) and the camr_eb_geom struct pointing at them."""

@@ -58,6 +58,10 @@ class EBGeom(C.Structure):
                 ("cent", C.c_void_p)]
 
 
+class BoxFab(C.Structure):
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("fab", Fab)]
+
+
 class LevelDesc(C.Structure):
     _fields_ = [("geom", Geom), ("max_grid_size", C.c_int * 3), ("use_graph", C.c_int)]
 
@@ -89,6 +93,13 @@ SIGNATURES = {
     "camr_level_state_fab": (C.c_int, [C.c_void_p, C.POINTER(Fab)]),
     "camr_level_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
     "camr_level_floor_resets": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "camr_fill_ghosts": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab), C.c_int,
+                                   C.c_void_p]),
+    "camr_clean_state": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab), C.c_int,
+                                   C.POINTER(HydroParams), C.c_void_p]),
+    "camr_est_dt": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab),
+                              C.POINTER(HydroParams), C.POINTER(C.c_double), C.c_void_p]),
+    "camr_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
     "camr_launch_count": (C.c_int64, []),
     "camr_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_last_error_string": (C.c_char_p, []),

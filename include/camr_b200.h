@@ -145,6 +145,50 @@ camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3],
                              void* stream);
 
 /* ---------------------------------------------------------------------
+ * Fab-level pieces of the level step for callers that keep their own box
+ * loop (a CAMR build whose AMReX level driver stays and calls into this
+ * library for parts of the step).  A level's data is a list of boxes, each
+ * with a device fab (NVAR comps) covering the box grown by ng.  The boxes
+ * must not overlap; they need not cover the domain (ghost cells whose
+ * source no box holds are left alone, as at a coarse-fine boundary).
+ * Stream-ordered; temporaries from cudaMallocAsync.
+ */
+typedef struct {
+  int lo[3];
+  int hi[3];
+  camr_fab fab;
+} camr_box_fab;
+
+/* The single-level FillPatch of expand_state (Source/CAMR.cpp:1243-1250):
+ * ng ghost layers of every fab from the valid cells of the boxes (interior
+ * and periodic neighbours), past a physical boundary from the BC map of
+ * Source/Utils/CAMR_setup.cpp:19-21 (foextrap and ext_dir copy the boundary
+ * cell -- Exec/Sod's bcnormal -- reflect_even / reflect_odd mirror it). */
+camr_status camr_fill_ghosts(const camr_geom* geom, int nbox, const camr_box_fab* boxes, int ng,
+                             void* stream);
+/* clean_state (Source/CAMR.cpp:1253-1262) of the boxes with ng ghost
+ * layers: enforce_min_density on the valid cells (box by box in raster
+ * order, each reset seen by the cells after it, as the reference's loop;
+ * at most 4096 cells below the floor per call, else error code 5),
+ * normalize_species on the valid cells, its FillBoundary of the interior
+ * and periodic ghost cells, then computeTemp on every cell of the grown
+ * boxes.  Errors go to the library's error word (camr_get_error). */
+camr_status camr_clean_state(const camr_geom* geom, int nbox, const camr_box_fab* boxes, int ng,
+                             const camr_hydro_params* p, void* stream);
+/* estTimeStep's hydro limit (Source/CAMR.cpp:490-563 with
+ * Source/Utils/Timestep.H:18-61): cfl * the minimum over the valid cells of
+ * dx_d / (c + |u_d|), capped by max_dt; fixed_dt when that is set.
+ * Synchronises the stream. */
+camr_status camr_est_dt(const camr_geom* geom, int nbox, const camr_box_fab* boxes,
+                        const camr_hydro_params* p, double* dt, void* stream);
+/* Read and clear the library's device error word on the current device
+ * after the work queued on `stream` (synchronises it).  camr_hydro_umdrv and
+ * camr_clean_state report into it where the reference would abort
+ * (Source/Hydro/Hydro_ctoprim.H:56,68; Source/CAMR.cpp:997).  Returns
+ * CAMR_ERR_NUMERIC when a failure was recorded. */
+camr_status camr_get_error(void* stream, camr_error_info* info);
+
+/* ---------------------------------------------------------------------
  * Batched per-box hydro over the boxes of one level (uneven sizes allowed):
  * the work-list form of the reference's MFIter box loop
  * (Source/Hydro/CAMR_construct_hydro_source.cpp:71-254).  Each task is one
