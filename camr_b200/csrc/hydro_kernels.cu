@@ -444,13 +444,13 @@ __device__ __forceinline__ void adjust_flux(double* f, const double* uL, const d
   for (int n = 0; n < NVAR; ++n) f[n] *= area;
 }
 
-template <int F>
+template <int F, bool MET = false>
 __device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, double qun,
                                                       int i, int j, int k,
                                                       const Space& s, const KGeom& g,
                                                       const KParams& P, const DFab& uin,
                                                       const double* divu, DFab flx,
-                                                      double* qf) {
+                                                      double* qf, const Metrics* M = nullptr) {
   constexpr int e0 = (F == 0), e1 = (F == 1), e2 = (F == 2);
   constexpr int t1 = (F == 0) ? 1 : 0;
   constexpr int t2 = (F == 2) ? 1 : 2;
@@ -468,8 +468,10 @@ __device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, d
     uL[n] = uin(i - e0, j - e1, k - e2, n);
     uR[n] = uin(i, j, k, n);
   }
-  const double area = (F == 0) ? g.dx[1] * g.dx[2] : (F == 1) ? g.dx[0] * g.dx[2]
-                                                              : g.dx[0] * g.dx[1];
+  double area = (F == 0) ? g.dx[1] * g.dx[2] : (F == 1) ? g.dx[0] * g.dx[2]
+                                                        : g.dx[0] * g.dx[1];
+  // hydro_ext_flx (Hydro_utils_K.H:224-234) with the caller's face areas
+  if constexpr (MET) area = M->a[F](i, j, k, 0);
   const int idx = (F == 0) ? i : (F == 1) ? j : k;
   adjust_flux<F>(f, uL, uR, dv, idx, g.dx[F], g, P, area);
 #pragma unroll
@@ -481,14 +483,14 @@ __device__ __forceinline__ void face_adjust_and_store(double* f, double qpres, d
 // ---------------------------------------------------------------------------
 // K6: final fluxes on the F-faces of bx (Godunov_3D.cpp:388-452):
 // hydro_transdd halves of the two cells, Riemann, then adjust_fluxes.
-template <int F>
+template <int F, bool MET = false>
 __device__ __forceinline__ void flux3_body(int i, int j, int k, const Space& s, const KGeom& g,
                                            const KParams& P, const DtRef& dtr,
                                            const double* q, const double* srcq, bool has_src,
                                            const double* smF, const double* spF,
                                            const double* fa, const double* fb,
                                            const double* divu, const DFab& uin, DFab flx,
-                                           double* qfF) {
+                                           double* qfF, const Metrics* M = nullptr) {
   constexpr int t0 = (F == 0) ? 1 : 0;
   constexpr int t1 = (F == 2) ? 1 : 2;
   const int64_t stF = (F == 0) ? 1 : (F == 1) ? s.sy : s.sz;
@@ -530,32 +532,33 @@ __device__ __forceinline__ void flux3_body(int i, int j, int k, const Space& s, 
   const int idx = (F == 0) ? i : (F == 1) ? j : k;
   double f[NVAR], qpres, qun;
   cmpflx<F>(qm, qp, aL, aR, idx, g.bclo[F], g.bchi[F], g.dlo[F], g.dhi[F], P, f, qpres, qun);
-  face_adjust_and_store<F>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfF);
+  face_adjust_and_store<F, MET>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfF, M);
 }
 
+template <bool MET>
 __global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX3) k_flux3(Region r0, Region r1, Region r2, Space s,
                                                    KGeom g, KParams P, DtRef dtr,
                                                    const double* q, const double* srcq,
                                                    bool has_src, Ptr3 sm, Ptr3 sp, Ptr6 f2,
                                                    const double* divu, DFab uin, DFab fx,
-                                                   DFab fy, DFab fz, Ptr3 qf) {
+                                                   DFab fy, DFab fz, Ptr3 qf, Metrics M) {
   int i, j, k;
   const int64_t t = gtid();
   switch (blockIdx.y) {
     case 0:
       if (region_cell(r0, t, i, j, k))
-        flux3_body<0>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[0], sp.p[0],
-                      f2.p[combo(1, 2)], f2.p[combo(2, 1)], divu, uin, fx, qf.p[0]);
+        flux3_body<0, MET>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[0], sp.p[0],
+                           f2.p[combo(1, 2)], f2.p[combo(2, 1)], divu, uin, fx, qf.p[0], &M);
       break;
     case 1:
       if (region_cell(r1, t, i, j, k))
-        flux3_body<1>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[1], sp.p[1],
-                      f2.p[combo(0, 2)], f2.p[combo(2, 0)], divu, uin, fy, qf.p[1]);
+        flux3_body<1, MET>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[1], sp.p[1],
+                           f2.p[combo(0, 2)], f2.p[combo(2, 0)], divu, uin, fy, qf.p[1], &M);
       break;
     default:
       if (region_cell(r2, t, i, j, k))
-        flux3_body<2>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[2], sp.p[2],
-                      f2.p[combo(0, 1)], f2.p[combo(1, 0)], divu, uin, fz, qf.p[2]);
+        flux3_body<2, MET>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[2], sp.p[2],
+                           f2.p[combo(0, 1)], f2.p[combo(1, 0)], divu, uin, fz, qf.p[2], &M);
       break;
   }
 }
@@ -580,57 +583,71 @@ __global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Regi
 }
 
 // MOL face pass: edge states + Riemann (mol_edges_cmpflx), then adjust_fluxes.
-template <int d>
+template <int d, bool MET = false>
 __device__ __forceinline__ void mol_flux_body(int i, int j, int k, const Space& s,
                                               const KGeom& g, const KParams& P,
                                               const double* q, const double* sl,
                                               const double* divu, const DFab& uin, DFab flx,
-                                              double* qfd) {
+                                              double* qfd, const Metrics* M = nullptr) {
   double f[NVAR], qpres, qun;
   mol_edges_cmpflx<d>(i, j, k, s, g, P, q, sl, f, qpres, qun);
-  face_adjust_and_store<d>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfd);
+  face_adjust_and_store<d, MET>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfd, M);
 }
 
+template <bool MET>
 __global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLFLUX) k_mol_flux(Region r0, Region r1, Region r2, Space s,
                                                       KGeom g, KParams P, const double* q,
                                                       Ptr3 slope, const double* divu,
                                                       DFab uin, DFab fx, DFab fy, DFab fz,
-                                                      Ptr3 qf) {
+                                                      Ptr3 qf, Metrics M) {
   int i, j, k;
   const int64_t t = gtid();
   switch (blockIdx.y) {
     case 0:
       if (region_cell(r0, t, i, j, k))
-        mol_flux_body<0>(i, j, k, s, g, P, q, slope.p[0], divu, uin, fx, qf.p[0]);
+        mol_flux_body<0, MET>(i, j, k, s, g, P, q, slope.p[0], divu, uin, fx, qf.p[0], &M);
       break;
     case 1:
       if (region_cell(r1, t, i, j, k))
-        mol_flux_body<1>(i, j, k, s, g, P, q, slope.p[1], divu, uin, fy, qf.p[1]);
+        mol_flux_body<1, MET>(i, j, k, s, g, P, q, slope.p[1], divu, uin, fy, qf.p[1], &M);
       break;
     default:
       if (region_cell(r2, t, i, j, k))
-        mol_flux_body<2>(i, j, k, s, g, P, q, slope.p[2], divu, uin, fz, qf.p[2]);
+        mol_flux_body<2, MET>(i, j, k, s, g, P, q, slope.p[2], divu, uin, fz, qf.p[2], &M);
       break;
   }
 }
 
 // ---------------------------------------------------------------------------
 // K7: hydro_consup (Hydro_utils_K.H:239-257) with pdivu (:175-202).
+template <bool MET = false>
 __device__ __forceinline__ void consup_body(int i, int j, int k, const Space& s, const KGeom& g,
                                             const DFab& fx, const DFab& fy, const DFab& fz,
-                                            const Ptr3& qf, const DFab& dsdt) {
+                                            const Ptr3& qf, const DFab& dsdt,
+                                            const Metrics* M = nullptr) {
   const int64_t at = s.idx(i, j, k);
-  const double a0 = g.dx[1] * g.dx[2], a1 = g.dx[0] * g.dx[2], a2 = g.dx[0] * g.dx[1];
-  const double vol = g.dx[0] * g.dx[1] * g.dx[2];
+  // face areas low/high in each direction and the cell volume
+  double a0 = g.dx[1] * g.dx[2], a1 = g.dx[0] * g.dx[2], a2 = g.dx[0] * g.dx[1];
+  double a0h = a0, a1h = a1, a2h = a2;
+  double vol = g.dx[0] * g.dx[1] * g.dx[2];
+  if constexpr (MET) {
+    a0 = M->a[0](i, j, k, 0);
+    a0h = M->a[0](i + 1, j, k, 0);
+    a1 = M->a[1](i, j, k, 0);
+    a1h = M->a[1](i, j + 1, k, 0);
+    a2 = M->a[2](i, j, k, 0);
+    a2h = M->a[2](i, j, k + 1, 0);
+    vol = M->vol(i, j, k, 0);
+  }
   const double* q1 = qf.p[0];
   const double* q2 = qf.p[1];
   const double* q3 = qf.p[2];
   const int64_t sn = s.sn;
   const double pdivu =
       0.5 *
-      ((q1[at + 1] + q1[at]) * (q1[at + 1 + sn] * a0 - q1[at + sn] * a0) +
-       (q2[at + s.sy] + q2[at]) * (q2[at + s.sy + sn] * a1 - q2[at + sn] * a1) +
-       (q3[at + s.sz] + q3[at]) * (q3[at + s.sz + sn] * a2 - q3[at + sn] * a2)) /
+      ((q1[at + 1] + q1[at]) * (q1[at + 1 + sn] * a0h - q1[at + sn] * a0) +
+       (q2[at + s.sy] + q2[at]) * (q2[at + s.sy + sn] * a1h - q2[at + sn] * a1) +
+       (q3[at + s.sz] + q3[at]) * (q3[at + s.sz + sn] * a2h - q3[at + sn] * a2)) /
       vol;
   const double volinv = 1.0 / vol;
 #pragma unroll
@@ -642,11 +659,44 @@ __device__ __forceinline__ void consup_body(int i, int j, int k, const Space& s,
   dsdt(i, j, k, UEINT) -= pdivu;
 }
 
+template <bool MET>
 __global__ void __launch_bounds__(kBlock) k_consup(Region r, Space s, KGeom g, DFab fx,
-                                                    DFab fy, DFab fz, Ptr3 qf, DFab dsdt) {
+                                                    DFab fy, DFab fz, Ptr3 qf, DFab dsdt,
+                                                    Metrics M) {
   int i, j, k;
   if (!region_cell(r, gtid(), i, j, k)) return;
-  consup_body(i, j, k, s, g, fx, fy, fz, qf, dsdt);
+  consup_body<MET>(i, j, k, s, g, fx, fy, fz, qf, dsdt, &M);
+}
+
+// The caller's primitive state and qaux (QVAR / NQAUX comps, the reference's
+// layout, Source/Utils/IndexDefines.H:54-77) and primitive sources into the
+// hydro's own q record and edge-state-layout srcq, on grow(bx,4).
+// QGAME / QTEMP / QGAMC / QDPDR / QDPDE are not read: the gamma-law EOS
+// makes QGAMC = eos_gamma, which the kernels use directly.
+__global__ void __launch_bounds__(kBlock) k_import_q(Region r, Space s, DFab qin, DFab qaux,
+                                                      DFab srcqin, bool has_srcq, double* q,
+                                                      double* srcq) {
+  int i, j, k;
+  if (!region_cell(r, gtid(), i, j, k)) return;
+  const int64_t at = s.idx(i, j, k);
+  q[at + SQ_RHO * s.sn] = qin(i, j, k, QRHO);
+  q[at + SQ_U * s.sn] = qin(i, j, k, QU);
+  q[at + SQ_V * s.sn] = qin(i, j, k, QV);
+  q[at + SQ_W * s.sn] = qin(i, j, k, QW);
+  q[at + SQ_P * s.sn] = qin(i, j, k, QPRES);
+  q[at + SQ_REINT * s.sn] = qin(i, j, k, QREINT);
+  for (int sp = 0; sp < NSPEC; ++sp) q[at + (SQ_FS + sp) * s.sn] = qin(i, j, k, QFS + sp);
+  q[at + SQ_C * s.sn] = qaux(i, j, k, QC);
+  q[at + SQ_CSML * s.sn] = qaux(i, j, k, QCSML);
+  if (has_srcq) {
+    srcq[at + ES_RHO * s.sn] = srcqin(i, j, k, QRHO);
+    srcq[at + ES_U * s.sn] = srcqin(i, j, k, QU);
+    srcq[at + ES_V * s.sn] = srcqin(i, j, k, QV);
+    srcq[at + ES_W * s.sn] = srcqin(i, j, k, QW);
+    srcq[at + ES_P * s.sn] = srcqin(i, j, k, QPRES);
+    srcq[at + ES_REINT * s.sn] = srcqin(i, j, k, QREINT);
+    for (int sp = 0; sp < NSPEC; ++sp) srcq[at + (ES_FS + sp) * s.sn] = srcqin(i, j, k, QFS + sp);
+  }
 }
 
 
@@ -843,8 +893,13 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
     if (L.timer) L.timer->mark(st, what);
   };
   mark("ctoprim");
-  k_ctoprim<<<grid_for(r4.count()), kBlock, 0, st>>>(r4, s, L.uin, L.src, L.has_src, L.P, w.q,
-                                                     w.srcq, L.err);
+  if (L.ext_q) {
+    k_import_q<<<grid_for(r4.count()), kBlock, 0, st>>>(r4, s, L.qin, L.qauxin, L.srcqin,
+                                                         L.ext_srcq, w.q, w.srcq);
+  } else {
+    k_ctoprim<<<grid_for(r4.count()), kBlock, 0, st>>>(r4, s, L.uin, L.src, L.has_src, L.P, w.q,
+                                                       w.srcq, L.err);
+  }
   mark("flatten_divu");
   k_flatten_divu<<<grid_for(r1.count()), kBlock, 0, st>>>(r1, s, g, L.P, !L.mol, w.q, w.flat,
                                                           w.divu);
@@ -910,9 +965,14 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       m = (rb[F].count() > m) ? rb[F].count() : m;
     }
     mark("flux3");
-    k_flux3<<<dim3(grid_for(m), 3), kBlock, 0, st>>>(rb[0], rb[1], rb[2], s, g, L.P, L.dt, w.q,
-                                                    w.srcq, L.has_src, sm, sp, f2, w.divu,
-                                                    L.uin, L.flx[0], L.flx[1], L.flx[2], qf);
+    if (L.M.on)
+      k_flux3<true><<<dim3(grid_for(m), 3), kBlock, 0, st>>>(
+          rb[0], rb[1], rb[2], s, g, L.P, L.dt, w.q, w.srcq, L.has_src, sm, sp, f2, w.divu, L.uin,
+          L.flx[0], L.flx[1], L.flx[2], qf, L.M);
+    else
+      k_flux3<false><<<dim3(grid_for(m), 3), kBlock, 0, st>>>(
+          rb[0], rb[1], rb[2], s, g, L.P, L.dt, w.q, w.srcq, L.has_src, sm, sp, f2, w.divu, L.uin,
+          L.flx[0], L.flx[1], L.flx[2], qf, L.M);
     count_launch(4);
   } else {
     Region rs[3], rb[3];
@@ -935,9 +995,14 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
     mark("mol_slope");
     k_mol_slope<<<dim3(grid_for(ms), 3), kBlock, 0, st>>>(rs[0], rs[1], rs[2], s, L.P, w.q, sl);
     mark("mol_flux");
-    k_mol_flux<<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(rb[0], rb[1], rb[2], s, g, L.P, w.q,
-                                                        sl, w.divu, L.uin, L.flx[0], L.flx[1],
-                                                        L.flx[2], qf);
+    if (L.M.on)
+      k_mol_flux<true><<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(
+          rb[0], rb[1], rb[2], s, g, L.P, w.q, sl, w.divu, L.uin, L.flx[0], L.flx[1], L.flx[2], qf,
+          L.M);
+    else
+      k_mol_flux<false><<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(
+          rb[0], rb[1], rb[2], s, g, L.P, w.q, sl, w.divu, L.uin, L.flx[0], L.flx[1], L.flx[2], qf,
+          L.M);
     count_launch(2);
   }
   return cudaGetLastError();
@@ -1114,8 +1179,12 @@ cudaError_t launch_hydro(const HydroLaunch& L, const Work& w, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   const Region rb = make_region(L.g.lo, L.g.hi);
   Ptr3 qf{{w.qf[0], w.qf[1], w.qf[2]}};
-  k_consup<<<grid_for(rb.count()), kBlock, 0, st>>>(rb, w.s, L.g, L.flx[0], L.flx[1], L.flx[2],
-                                                    qf, L.dsdt);
+  if (L.M.on)
+    k_consup<true><<<grid_for(rb.count()), kBlock, 0, st>>>(rb, w.s, L.g, L.flx[0], L.flx[1],
+                                                            L.flx[2], qf, L.dsdt, L.M);
+  else
+    k_consup<false><<<grid_for(rb.count()), kBlock, 0, st>>>(rb, w.s, L.g, L.flx[0], L.flx[1],
+                                                             L.flx[2], qf, L.dsdt, L.M);
   count_launch(1);
   return cudaGetLastError();
 }

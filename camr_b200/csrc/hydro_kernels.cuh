@@ -64,6 +64,15 @@ struct StageTimer {
   }
 };
 
+// Caller-supplied metric arrays of the reference's hydro_umdrv (Source/
+// Hydro/Hydro.H:11-35): face areas a[d] on surroundingNodes(bx,d) and cell
+// volumes on bx.  on = 0: Cartesian metrics from dx (the default).
+struct Metrics {
+  DFab a[3];
+  DFab vol;
+  int on = 0;
+};
+
 struct HydroLaunch {
   KGeom g;
   KParams P;
@@ -76,6 +85,13 @@ struct HydroLaunch {
   DtRef dt;
   DevError* err;
   StageTimer* timer = nullptr;
+  // Caller-supplied primitive state (QVAR comps), qaux (NQAUX) and
+  // primitive sources (QVAR) on grow(bx,4), in the reference's layout,
+  // used instead of ctoprim / srctoprim (ext_q; srcq only with ext_srcq).
+  bool ext_q = false;
+  bool ext_srcq = false;
+  DFab qin, qauxin, srcqin;
+  Metrics M;
 };
 
 // ---- batched (work-list) launches over many boxes of one level ----

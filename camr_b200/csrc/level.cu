@@ -133,24 +133,52 @@ const char* camr_version(void) { return "camr_b200 0.1 (sm_100a, FP64)"; }
 
 int64_t camr_launch_count(void) { return g_launches.load(); }
 
-camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3], const camr_geom* geom,
-                             const camr_fab* uin, const camr_fab* src, camr_fab* dsdt,
-                             camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
-                             const camr_hydro_params* p, double dt, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// The per-box hydro behind camr_hydro_umdrv and camr_hydro_umdrv_full: q
+// (with qaux and the primitive sources src_q) either from ctoprim /
+// srctoprim of uin and src, or the caller's; area/vol either Cartesian from
+// dx or the caller's.
+camr_status umdrv_common(const int bx_lo[3], const int bx_hi[3], const camr_geom* geom,
+                         const camr_fab* uin, const camr_fab* src, const camr_fab* q,
+                         const camr_fab* qaux, const camr_fab* src_q, camr_fab* dsdt,
+                         camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                         const camr_fab* const* area, const camr_fab* vol,
+                         const camr_hydro_params* p, double dt, void* stream) {
   if (!bx_lo || !bx_hi || !geom || !uin || !dsdt || !flx0 || !flx1 || !flx2 || !uin->ptr ||
       !dsdt->ptr || !flx0->ptr || !flx1->ptr || !flx2->ptr)
     return CAMR_ERR_INVALID;
   camr_status cs = check_params(p);
   if (cs != CAMR_OK) return cs;
-  for (int d = 0; d < 3; ++d) {
+  auto covers = [&](const camr_fab* f, int grow, int hi_extra_dir) {
+    for (int d = 0; d < 3; ++d) {
+      const int hx = (d == hi_extra_dir) ? 1 : 0;
+      if (f->lo[d] > bx_lo[d] - grow || f->hi[d] < bx_hi[d] + grow + hx) return false;
+    }
+    return true;
+  };
+  for (int d = 0; d < 3; ++d)
     if (bx_hi[d] < bx_lo[d]) return CAMR_ERR_INVALID;
-    // uin must cover grow(bx, 4)
-    if (uin->lo[d] > bx_lo[d] - NGROW || uin->hi[d] < bx_hi[d] + NGROW) return CAMR_ERR_INVALID;
-    if (src && src->ptr && (src->lo[d] > bx_lo[d] - NGROW || src->hi[d] < bx_hi[d] + NGROW))
-      return CAMR_ERR_INVALID;
-    if (dsdt->lo[d] > bx_lo[d] || dsdt->hi[d] < bx_hi[d]) return CAMR_ERR_INVALID;
-  }
+  // uin must cover grow(bx, 4)
+  if (!covers(uin, NGROW, -1) || !covers(dsdt, 0, -1)) return CAMR_ERR_INVALID;
+  if (src && src->ptr && !covers(src, NGROW, -1)) return CAMR_ERR_INVALID;
   if (uin->ncomp < NVAR || dsdt->ncomp < NVAR) return CAMR_ERR_INVALID;
+  const bool ext_q = q != nullptr;
+  if (ext_q) {
+    if (!q->ptr || !qaux || !qaux->ptr || q->ncomp < QVAR || qaux->ncomp < NQAUX ||
+        !covers(q, NGROW, -1) || !covers(qaux, NGROW, -1))
+      return CAMR_ERR_INVALID;
+    if (src_q && (!src_q->ptr || src_q->ncomp < QVAR || !covers(src_q, NGROW, -1)))
+      return CAMR_ERR_INVALID;
+  }
+  const bool met = area != nullptr;
+  if (met) {
+    for (int d = 0; d < 3; ++d)
+      if (!area[d] || !area[d]->ptr || !covers(area[d], 0, d)) return CAMR_ERR_INVALID;
+    if (!vol || !vol->ptr || !covers(vol, 0, -1)) return CAMR_ERR_INVALID;
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   HydroLaunch Lh;
   for (int d = 0; d < 3; ++d) {
@@ -166,6 +194,19 @@ camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3], const camr_
   Lh.uin = make_dfab(*uin);
   Lh.has_src = src && src->ptr;
   Lh.src = Lh.has_src ? make_dfab(*src) : Lh.uin;
+  if (ext_q) {
+    Lh.ext_q = true;
+    Lh.qin = make_dfab(*q);
+    Lh.qauxin = make_dfab(*qaux);
+    Lh.ext_srcq = src_q != nullptr;
+    Lh.srcqin = Lh.ext_srcq ? make_dfab(*src_q) : Lh.qin;
+    Lh.has_src = Lh.ext_srcq;  // the srcq array holds the caller's sources
+  }
+  if (met) {
+    for (int d = 0; d < 3; ++d) Lh.M.a[d] = make_dfab(*area[d]);
+    Lh.M.vol = make_dfab(*vol);
+    Lh.M.on = 1;
+  }
   Lh.mol = p->do_mol != 0;
   Lh.flx[0] = make_dfab(*flx0);
   Lh.flx[1] = make_dfab(*flx1);
@@ -187,6 +228,32 @@ camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3], const camr_
   cudaError_t e2 = cudaFreeAsync(base, st);
   if (e != cudaSuccess) return cuda_status(e);
   return cuda_status(e2);
+}
+
+}  // namespace
+
+extern "C" {
+
+camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3], const camr_geom* geom,
+                             const camr_fab* uin, const camr_fab* src, camr_fab* dsdt,
+                             camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                             const camr_hydro_params* p, double dt, void* stream) {
+  return umdrv_common(bx_lo, bx_hi, geom, uin, src, nullptr, nullptr, nullptr, dsdt, flx0, flx1,
+                      flx2, nullptr, nullptr, p, dt, stream);
+}
+
+camr_status camr_hydro_umdrv_full(const int bx_lo[3], const int bx_hi[3], const camr_geom* geom,
+                                  const camr_fab* uin, const camr_fab* q, const camr_fab* qaux,
+                                  const camr_fab* src_q, camr_fab* dsdt, camr_fab* flx0,
+                                  camr_fab* flx1, camr_fab* flx2, const camr_fab* area0,
+                                  const camr_fab* area1, const camr_fab* area2,
+                                  const camr_fab* vol, const camr_hydro_params* p, double dt,
+                                  void* stream) {
+  if (!q || !qaux) return CAMR_ERR_INVALID;
+  const bool met = area0 || area1 || area2 || vol;
+  const camr_fab* area[3] = {area0, area1, area2};
+  return umdrv_common(bx_lo, bx_hi, geom, uin, nullptr, q, qaux, src_q, dsdt, flx0, flx1, flx2,
+                      met ? area : nullptr, vol, p, dt, stream);
 }
 
 camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_params* p,

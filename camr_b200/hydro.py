@@ -83,6 +83,32 @@ def hydro_umdrv(bx_lo, bx_hi, geom, uin, uin_lo, dsdt, flx, params, dt, src=None
     check(st, "camr_hydro_umdrv")
 
 
+def hydro_umdrv_full(bx_lo, bx_hi, geom, uin, uin_lo, q, qaux, dsdt, flx, params, dt,
+                     src_q=None, area=None, vol=None, stream=None):
+    """The per-box hydro with the reference's full argument list
+    (camr_hydro_umdrv_full): q (QVAR) and qaux (5) tensors on grow(bx,4)
+    starting at uin_lo, optional src_q (QVAR) likewise, optional face areas
+    area[d] (1 comp on the d-faces of bx) and volumes vol (1 comp on bx)."""
+    lo = (C.c_int * 3)(*bx_lo)
+    hi = (C.c_int * 3)(*bx_hi)
+    fu, fq, fa = fab_of(uin, uin_lo), fab_of(q, uin_lo), fab_of(qaux, uin_lo)
+    fs = fab_of(src_q, uin_lo) if src_q is not None else None
+    fd = fab_of(dsdt, bx_lo)
+    ff = [fab_of(f, bx_lo) for f in flx]
+    fm = [fab_of(a, bx_lo) for a in area] if area is not None else [None] * 3
+    fv = fab_of(vol, bx_lo) if vol is not None else None
+
+    def ref(f):
+        return C.byref(f) if f is not None else None
+
+    st = lib().camr_hydro_umdrv_full(C.byref(lo), C.byref(hi), C.byref(geom), C.byref(fu),
+                                     C.byref(fq), C.byref(fa), ref(fs), C.byref(fd),
+                                     C.byref(ff[0]), C.byref(ff[1]), C.byref(ff[2]), ref(fm[0]),
+                                     ref(fm[1]), ref(fm[2]), ref(fv), C.byref(params), float(dt),
+                                     C.c_void_p(_stream_ptr(stream)))
+    check(st, "camr_hydro_umdrv_full")
+
+
 def box_fabs(boxes, tensors, ng):
     """camr_box_fab array for boxes [(lo, hi)] and their (NVAR, nz, ny, nx)
     CUDA tensors, each covering its box grown by ng."""

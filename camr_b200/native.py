@@ -81,6 +81,13 @@ SIGNATURES = {
                                    C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
                                    C.POINTER(Fab), C.POINTER(HydroParams), C.c_double,
                                    C.c_void_p]),
+    "camr_hydro_umdrv_full": (C.c_int, [C.POINTER(C.c_int * 3), C.POINTER(C.c_int * 3),
+                                        C.POINTER(Geom), C.POINTER(Fab), C.POINTER(Fab),
+                                        C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
+                                        C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
+                                        C.POINTER(Fab), C.POINTER(Fab), C.POINTER(Fab),
+                                        C.POINTER(Fab), C.POINTER(HydroParams), C.c_double,
+                                        C.c_void_p]),
     "camr_level_create": (C.c_int, [C.POINTER(LevelDesc), C.POINTER(HydroParams), C.c_void_p,
                                     C.POINTER(C.c_void_p)]),
     "camr_level_destroy": (C.c_int, [C.c_void_p]),

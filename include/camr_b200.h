@@ -40,7 +40,7 @@ enum {
   CAMR_BC_SYMMETRY = 3, CAMR_BC_SLIPWALL = 4, CAMR_BC_NOSLIPWALL = 5
 };
 
-enum { CAMR_NVAR = 10, CAMR_QVAR = 11, CAMR_NGDNV = 6 };
+enum { CAMR_NVAR = 10, CAMR_QVAR = 11, CAMR_NQAUX = 5, CAMR_NGDNV = 6 };
 
 /* The CAMR.* ParmParse parameters the hydro advance reads, by their
  * reference names (Source/Params/_cpp_parameters), plus eos_gamma (the
@@ -143,6 +143,28 @@ camr_status camr_hydro_umdrv(const int bx_lo[3], const int bx_hi[3],
                              camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
                              const camr_hydro_params* p, double dt,
                              void* stream);
+
+/* The per-box hydro with the reference's full argument list
+ * (Source/Hydro/Hydro.H:11-35): the caller supplies q (QVAR comps, the
+ * reference's primitive layout Source/Utils/IndexDefines.H:54-59) and qaux
+ * (NQAUX = 5 comps, :72-77) on grow(bx,4), as construct_hydro_source's
+ * ctoprim computes them (Source/Hydro/CAMR_construct_hydro_source.cpp:
+ * 108-120); src_q (QVAR comps on grow(bx,4), CTU only; NULL = zero) as
+ * srctoprim computes them; and optionally the metric arrays: face areas
+ * area[d] (1 comp on surroundingNodes(bx,d)) and cell volumes vol (1 comp
+ * on bx) -- all four or none (none: Cartesian from geom->dx).  The
+ * gamma-law EOS supplies QGAMC, QDPDR, QDPDE, QGAME and QTEMP, which are not
+ * read.  uin (grow(bx,4)) is still read by the artificial viscosity.  dsdt
+ * accumulated, flx overwritten, as camr_hydro_umdrv. */
+camr_status camr_hydro_umdrv_full(const int bx_lo[3], const int bx_hi[3],
+                                  const camr_geom* geom, const camr_fab* uin,
+                                  const camr_fab* q, const camr_fab* qaux,
+                                  const camr_fab* src_q, camr_fab* dsdt,
+                                  camr_fab* flx0, camr_fab* flx1, camr_fab* flx2,
+                                  const camr_fab* area0, const camr_fab* area1,
+                                  const camr_fab* area2, const camr_fab* vol,
+                                  const camr_hydro_params* p, double dt,
+                                  void* stream);
 
 /* ---------------------------------------------------------------------
  * Fab-level pieces of the level step for callers that keep their own box

@@ -224,6 +224,62 @@ def hydro_box(kind, p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, uin, uin_lo, dx
     return dsdt, flx, nass
 
 
+def ref_ctoprim(p, lo, hi, uin, uin_lo, src=None):
+    """The reference's hydro_ctoprim / hydro_srctoprim over [lo, hi] of uin
+    (oracle/_ref only): (q (QVAR, ...), qaux (5, ...), src_q (QVAR, ...))."""
+    lib = load("ref")
+    lib.orc_ref_ctoprim.restype = C.c_long
+    n = [hi[d] - lo[d] + 1 for d in range(3)]
+    uin = np.ascontiguousarray(uin, dtype=np.float64)
+    uin_hi = [uin_lo[d] + uin.shape[3 - d] - 1 for d in range(3)]
+    q = np.zeros((QVAR, n[2], n[1], n[0]))
+    qaux = np.zeros((5, n[2], n[1], n[0]))
+    srcq = np.zeros((QVAR, n[2], n[1], n[0]))
+    srcp = None
+    if src is not None:
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        srcp = src.ctypes.data
+    vp = C.c_void_p
+    nass = lib.orc_ref_ctoprim(C.byref(p), _I3(*lo), _I3(*hi), vp(uin.ctypes.data), _I3(*uin_lo),
+                               _I3(*uin_hi), vp(srcp), vp(q.ctypes.data), vp(qaux.ctypes.data),
+                               vp(srcq.ctypes.data))
+    assert nass == 0
+    return q, qaux, srcq
+
+
+def ref_hydro_box_full(p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, uin, uin_lo, q, qaux, srcq,
+                       area, vol, dx, dt):
+    """The reference's hydro_umdrv with caller q/qaux/src_q and metrics
+    (oracle/_ref only); returns (dsdt, [flx_x, flx_y, flx_z], nassert)."""
+    lib = load("ref")
+    lib.orc_ref_hydro_box_full.restype = C.c_long
+    nb = [bx_hi[d] - bx_lo[d] + 1 for d in range(3)]
+    uin = np.ascontiguousarray(uin, dtype=np.float64)
+    uin_hi = [uin_lo[d] + uin.shape[3 - d] - 1 for d in range(3)]
+    dsdt = np.zeros((NVAR, nb[2], nb[1], nb[0]))
+    flx = []
+    for d in range(3):
+        s = list(nb)
+        s[d] += 1
+        flx.append(np.zeros((NVAR, s[2], s[1], s[0])))
+    keep = []
+
+    def ptr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return C.c_void_p(a.ctypes.data)
+
+    areas = list(area) if area is not None else [None, None, None]
+    nass = lib.orc_ref_hydro_box_full(
+        C.byref(p), _I3(*bx_lo), _I3(*bx_hi), _I3(*dom_lo), _I3(*dom_hi), _I3(*bclo), _I3(*bchi),
+        ptr(uin), _I3(*uin_lo), _I3(*uin_hi), ptr(q), ptr(qaux), ptr(srcq), ptr(areas[0]),
+        ptr(areas[1]), ptr(areas[2]), ptr(vol), ptr(dsdt), ptr(flx[0]), ptr(flx[1]), ptr(flx[2]),
+        _D3(*dx), C.c_double(dt))
+    return dsdt, flx, nass
+
+
 def init_finalize(kind, p, lev, state):
     load(kind).orc_init_finalize(C.byref(p), C.byref(lev), state)
 

@@ -90,6 +90,25 @@ long orc_hydro_box(const orc_params* p, const int bx_lo[3], const int bx_hi[3],
                    const int dsdt_lo[3], const int dsdt_hi[3], double* flx0,
                    double* flx1, double* flx2, const double dx[3], double dt);
 
+/* oracle/_ref only: the reference's hydro_ctoprim + hydro_srctoprim over
+ * [lo, hi] of uin (src NULL = zero sources): q (QVAR), qaux (NQAUX) and
+ * src_q (QVAR) on that region. */
+long orc_ref_ctoprim(const orc_params* p, const int lo[3], const int hi[3], const double* uin,
+                     const int uin_lo[3], const int uin_hi[3], const double* src, double* q,
+                     double* qaux, double* srcq);
+
+/* oracle/_ref only: the reference's hydro_umdrv with caller q, qaux (and
+ * src_q, NULL = zero) on grow(bx,4) and caller face areas / volumes (NULL
+ * = Cartesian from dx); flx overwritten, dsdt (on bx) accumulated. */
+long orc_ref_hydro_box_full(const orc_params* p, const int bx_lo[3], const int bx_hi[3],
+                            const int dom_lo[3], const int dom_hi[3], const int bclo[3],
+                            const int bchi[3], const double* uin, const int uin_lo[3],
+                            const int uin_hi[3], const double* q, const double* qaux,
+                            const double* srcq, const double* area0, const double* area1,
+                            const double* area2, const double* vol, double* dsdt,
+                            double* flx0, double* flx1, double* flx2, const double dx[3],
+                            double dt);
+
 /* Fill every ParmParse default of the reference (Source/Params/_cpp_parameters). */
 void orc_default_params(orc_params* p);
 

@@ -210,3 +210,37 @@ def test_conservation_periodic_oracle(cfg):
     for comp in range(5):
         scale = np.abs(a[comp]).sum()
         assert abs(s[comp].sum() - a[comp].sum()) <= 1e-12 * scale
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("cfg", ["ctu_ppm", "ctu_plm", "mol_plm"])
+def test_reference_full_interface_equals_per_box_call(cfg):
+    """The reference's hydro_umdrv driven with caller q/qaux/src_q from its own
+    ctoprim/srctoprim and Cartesian area/volume arrays gives the same bits as
+    the per-box glue that computes them (the pin of the full-interface
+    oracle used by the GPU test of camr_hydro_umdrv_full)."""
+    n = (10, 9, 8)
+    lev = oracle.make_level(n, **BCSETS["walls"])
+    p = oracle.default_params(**CONFIGS[cfg])
+    s = P.random_smooth(n, seed=4)
+    oracle.init_finalize("ref", p, lev, s)
+    border = oracle.expand_state("ref", p, lev, s)
+    rng = np.random.default_rng(2)
+    src = rng.standard_normal(border.shape) * 0.2
+    dt = 0.5 * oracle.est_dt("ref", p, lev, s)
+    lo, hi = [0, 0, 0], [n[0] - 1, n[1] - 1, n[2] - 1]
+    glo, ghi = [-4, -4, -4], [n[0] + 3, n[1] + 3, n[2] + 3]
+    q, qaux, srcq = oracle.ref_ctoprim(p, glo, ghi, border, glo, src=src)
+    dx = list(lev.dx)
+    area = [np.full((n[2] + (d == 2), n[1] + (d == 1), n[0] + (d == 0)),
+                    (dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1])[d]) for d in range(3)]
+    vol = np.full((n[2], n[1], n[0]), dx[0] * dx[1] * dx[2])
+    d1, f1, nass = oracle.ref_hydro_box_full(p, lo, hi, lo, hi, list(lev.bc_lo), list(lev.bc_hi),
+                                             border, glo, q, qaux, srcq, area, vol, dx, dt)
+    assert nass == 0
+    d0, f0, nass = oracle.hydro_box("ref", p, lo, hi, lo, hi, list(lev.bc_lo), list(lev.bc_hi),
+                                    border, glo, dx, dt, src=src)
+    assert nass == 0
+    assert same_bits(d1, d0) == 0
+    for d in range(3):
+        assert same_bits(f1[d], f0[d]) == 0
