@@ -50,8 +50,23 @@ STAGE_BYTES = {
     "flux3": (1288, "read states, 6 x 10 records, divu, U; write 3 x 10 fluxes + 3 x 2"),
     "update": (528, "read Sborder, U_old, 3 x 10 fluxes, 3 x 2; write U"),
 }
-# Whole-step algorithmic bytes per zone-update (read U^n + write U^n+1).
+# Whole-step algorithmic bytes per zone-update: CTU reads U^n and writes
+# U^n+1 (160 B); SSP-RK2 reads U^n, writes U*, reads U* and U^n, writes
+# U^n+1 (400 B).  FP64, NVAR = 10; ghosts and temporaries excluded.
 STEP_BYTES_PER_ZONE = 160
+MOL_BYTES_PER_ZONE = 400
+# Algorithmic flops per zone-update (+, -, *, / and sqrt, one each), counted
+# on the reference's own per-box hydro with a counting amrex::Real on one
+# 64^3 box of the configuration's data (oracle/count_flops.py; recounted by
+# tests/test_flops.py).  CTU-PPM: 3239 adds, 3362 muls, 345 divisions, 65
+# square roots; SSP-RK2 MOL-PLM: two hydro evaluations per step.
+FLOPS_PER_ZONE_UPDATE = {"ctu_ppm": 7011.0, "mol_plm": 2770.3}
+# Divisions and square roots per zone-update among those flops: on the GPU
+# each expands into a reciprocal or root estimate and Newton steps, and with
+# -fmad=false (bit-exact parity with the reference's unfused CPU arithmetic)
+# no add or multiply fuses into an FMA, so the FP64 pipe's ceiling for this
+# code is half the DFMA peak in flop/s.
+DIVSQRT_PER_ZONE_UPDATE = {"ctu_ppm": 410.3, "mol_plm": 296.8}
 # DRAM bytes (read + write) per valid cell of one launch, from an ncu
 # capture of the same kernel on the 128^3 case of this workload (inputs
 # larger than L2; traffic grows with the cell count, so the per-cell figure
@@ -184,6 +199,64 @@ def c1_config(n, world):
                   f"~{state_gb * 18.7:.2g} GB)"}
 
 
+def c1_rooflines(zones, acc, dom, ms_step, hbm_peak, peak_kind, fp64_peak):
+    """The roofline objects of the C1 line.  `roofline` is the dominant
+    kernel against HBM on the workload's algorithmic bytes (160 B per
+    zone-update: read U^n, write U^n+1) with the FP64 side beside it (the
+    reference's counted flops per zone-update); the kernel's own
+    intermediate-array bytes are kept apart under `kernel_intermediates`.
+    `step_roofline` is the same for the whole step."""
+    t_dom = acc[dom] * 1e-3
+    achieved = STEP_BYTES_PER_ZONE * zones / t_dom / 1e9
+    flops = FLOPS_PER_ZONE_UPDATE["ctu_ppm"]
+    inter = STAGE_BYTES[dom][0] * zones / t_dom / 1e9
+    roofline = {
+        "kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+        "frac": achieved / hbm_peak, "peak_source": f"{peak_kind} hbm_gbs",
+        "algorithmic_bytes_per_zone_update": STEP_BYTES_PER_ZONE,
+        "units_per_launch": zones,
+        "avg_launch_ms": acc[dom],
+        "traffic": (STAGE_TRAFFIC_PER_CELL[dom] * zones if dom in STAGE_TRAFFIC_PER_CELL
+                    else None),
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell of a "
+                          "128^3 capture, times the cells of one launch",
+        "kernel_intermediates": {
+            "bytes_per_cell": STAGE_BYTES[dom][0], "what": STAGE_BYTES[dom][1],
+            "achieved_gbs": inter, "frac": inter / hbm_peak},
+        "fp64_whole_step": fp64_roofline("ctu_ppm", zones / (ms_step * 1e-3), fp64_peak),
+    }
+    step_achieved = STEP_BYTES_PER_ZONE * zones / (ms_step * 1e-3) / 1e9
+    step_roofline = {"bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved": step_achieved,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": step_achieved / hbm_peak,
+                     "fp64": fp64_roofline("ctu_ppm", zones / (ms_step * 1e-3), fp64_peak)}
+    return roofline, step_roofline
+
+
+def level_hbm(method, zone_rate):
+    """Achieved algorithmic HBM bandwidth of a level step: 400 B per
+    zone-update for SSP-RK2 (MOL), 160 B for CTU."""
+    peak, kind = measured_peaks()
+    b = MOL_BYTES_PER_ZONE if method.startswith("mol") else STEP_BYTES_PER_ZONE
+    gbs = b * zone_rate / 1e9
+    return {"bytes_per_zone_update": b, "achieved_gbs": gbs, "peak_gbs": peak,
+            "frac": gbs / peak, "peak_source": f"{kind} hbm_gbs"}
+
+
+def fp64_roofline(method, zone_rate, fp64_peak):
+    """Counted flops per zone-update x zone-updates/s against the measured
+    DFMA peak (an FMA counts 2 flops there; this code issues no FMAs, so
+    frac_of_unfused_peak, against half that peak, is its pipe's ceiling)."""
+    f = FLOPS_PER_ZONE_UPDATE[method]
+    tf = f * zone_rate / 1e12
+    return {"flops_per_zone_update": f, "divisions_and_sqrts_per_zone_update":
+            DIVSQRT_PER_ZONE_UPDATE[method], "achieved_tflops": tf,
+            "peak_tflops": fp64_peak, "peak_source": "measured DFMA (camr_measure_fp64_peak)",
+            "frac": tf / fp64_peak if fp64_peak else None,
+            "frac_of_unfused_peak": 2 * tf / fp64_peak if fp64_peak else None,
+            "flop_source": "reference hydro with a counting amrex::Real, one 64^3 box "
+                           "(oracle/count_flops.py)"}
+
+
 def c1_state(n):
     from camr_b200 import problems as P
     dx = tuple(1.0 / v for v in n)
@@ -267,6 +340,7 @@ def run_camr(args, world, rank, local, pg):
 
     fp64_peak = C.c_double()
     lib.camr_measure_fp64_peak(C.byref(fp64_peak), C.c_void_p(L.stream_ptr))
+    args.fp64_peak = fp64_peak.value
 
     sampler = ClockSampler(local)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -305,22 +379,8 @@ def run_camr(args, world, rank, local, pg):
             acc[k] = acc.get(k, 0.0) + times[i] / nprof
     hbm_peak, peak_kind = measured_peaks()
     dom = max((k for k in acc if k in STAGE_BYTES), key=lambda k: acc[k])
-    dom_bytes = STAGE_BYTES[dom][0] * zones
-    achieved = dom_bytes / (acc[dom] * 1e-3) / 1e9
-    roofline = {
-        "kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-        "frac": achieved / hbm_peak, "peak_source": f"{peak_kind} hbm_gbs",
-        "traffic": (STAGE_TRAFFIC_PER_CELL[dom] * zones if dom in STAGE_TRAFFIC_PER_CELL
-                    else None),
-        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell of a "
-                          "128^3 capture, times the cells of one launch",
-        "algorithmic_bytes_per_cell": STAGE_BYTES[dom][0],
-        "avg_launch_ms": acc[dom],
-        "fp64_peak_tflops_measured": fp64_peak.value,
-    }
-    step_achieved = STEP_BYTES_PER_ZONE * zones / (ms_step * 1e-3) / 1e9
-    step_roofline = {"bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved": step_achieved,
-                     "peak": hbm_peak, "unit": "GB/s", "frac": step_achieved / hbm_peak}
+    roofline, step_roofline = c1_rooflines(zones, acc, dom, ms_step, hbm_peak, peak_kind,
+                                           fp64_peak.value)
 
     # End to end through the C ABI with host buffers: every step uploads a
     # state from pinned host memory, advances it one step (a step after a
@@ -383,7 +443,7 @@ def run_camr(args, world, rank, local, pg):
         L.close()
         batched = batched_comparison(args)
         amr = amr_comparison(args)
-        adj = adjoint_comparison(args)
+        adj = adjoint_comparison(args, fd_cells=args.fd_cells)
         ebc = eb_comparison(args)
 
     if rank == 0:
@@ -545,7 +605,11 @@ def amr_comparison(args, steps=None, per_box_steps=2, warmup=3):
             if prof:
                 profile_range(args, False)
             ms = e0.elapsed_time(e1) / k
-            res[mname] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms * 1e-3)}
+            rate = zones / (ms * 1e-3)
+            res[mname] = {"ms_per_step": ms, "zone_updates_per_s": rate,
+                          "hbm": level_hbm(name, rate), "fp64": fp64_roofline(
+                              "mol_plm" if name == "mol_plm" else "ctu_ppm", rate,
+                              args.fp64_peak)}
         res["kernels_per_step_graph"] = h.kernels_per_step()
         res["device_error"] = list(h.error())
         if compare:
@@ -748,11 +812,23 @@ def adjoint_comparison(args, n=128, nsteps=200, every=20, fd_cells=0):
            "timing": "CUDA events on the adjoint's stream",
            "device_error": list(A.error())}
     if fd_cells:
+        # Central differences (eps = 1e-6 rho at fixed p, u) of J at seeded
+        # cells inside the sphere, with the forward dt sequence frozen.  The
+        # one-sided differences D+ and D- are kept too: where the +-eps runs
+        # straddle a limiter or Riemann branch (a kink of J), D+ and D- part
+        # and the central difference is the mean of two one-sided slopes,
+        # while the adjoint takes the slope of the branch the forward took.
         rng = np.random.default_rng(64)
         inside = np.argwhere(r < 0.2)
         cells = [tuple(int(v) for v in inside[t])
                  for t in rng.choice(len(inside), fd_cells, replace=False)]
-        errs = []
+
+        def J(state):
+            o = A.forward(torch.from_numpy(state).cuda(), nsteps, fixed_dts=dts)
+            return float((o[0] * mask).sum()) * dV
+
+        j0 = J(s)
+        samples = []
         for (k, j, i) in cells:
             eps = 1e-6 * s[0, k, j, i]
             res = []
@@ -760,16 +836,34 @@ def adjoint_comparison(args, n=128, nsteps=200, every=20, fd_cells=0):
                 st = s.copy()
                 st[0, k, j, i] += sg * eps
                 st[7, k, j, i] += sg * eps
-                o = A.forward(torch.from_numpy(st).cuda(), nsteps, fixed_dts=dts)
-                res.append(float((o[0] * mask).sum()) * dV)
+                res.append(J(st))
             fd = (res[0] - res[1]) / (2 * eps)
+            dp = (res[0] - j0) / eps
+            dm = (j0 - res[1]) / eps
             ad = float(grad[k, j, i])
-            errs.append(abs(fd - ad) / max(abs(fd), abs(ad)))
-        errs = np.array(errs)
-        out["fd_check"] = {"cells": fd_cells, "eps_rel": 1e-6,
-                           "median_rel_err": float(np.median(errs)),
-                           "max_rel_err": float(errs.max()),
-                           "frac_within_1e-6": float(np.mean(errs <= 1e-6))}
+            scale = max(abs(fd), abs(ad), 1e-300)
+            kink = abs(dp - dm) / max(abs(dp), abs(dm), 1e-300)
+            samples.append({"cell": [i, j, k], "adjoint": ad, "central": fd, "d_plus": dp,
+                            "d_minus": dm, "rel_err": abs(fd - ad) / scale,
+                            "one_sided_split": kink,
+                            "rel_err_nearest_one_sided": min(abs(dp - ad), abs(dm - ad)) / scale})
+        errs = np.array([x["rel_err"] for x in samples])
+        # a sample straddles a kink when its one-sided slopes part by far
+        # more than the O(eps) curvature of a smooth J allows
+        kinked = [x for x in samples if x["one_sided_split"] > 1e-4]
+        smooth = [x for x in samples if x["one_sided_split"] <= 1e-4]
+        out["fd_check"] = {
+            "cells": fd_cells, "seed": 64, "eps_rel": 1e-6, "steps": nsteps,
+            "median_rel_err": float(np.median(errs)), "max_rel_err": float(errs.max()),
+            "frac_within_1e-6": float(np.mean(errs <= 1e-6)),
+            "kinked_samples": len(kinked), "kink_criterion": "|D+ - D-| / max|D+-| > 1e-4",
+            "smooth_samples": len(smooth),
+            "smooth_median_rel_err": (float(np.median([x["rel_err"] for x in smooth]))
+                                      if smooth else None),
+            "smooth_max_rel_err": (float(max(x["rel_err"] for x in smooth)) if smooth else None),
+            "kinked_max_rel_err_vs_nearest_one_sided": (
+                float(max(x["rel_err_nearest_one_sided"] for x in kinked)) if kinked else None),
+            "samples": samples}
     A.close()
     torch.cuda.empty_cache()
     return out
@@ -872,11 +966,16 @@ def main():
             print(json.dumps({"workload": "c4-eb", **eb_comparison(args)}))
         return
     if args.workload == "c2-amr":
+        import ctypes as C
+
         import torch
         from camr_b200 import build, native
         if not os.path.exists(native.LIB_PATH):
             build.build()
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        peak = C.c_double()
+        native.lib().camr_measure_fp64_peak(C.byref(peak), None)
+        args.fp64_peak = peak.value
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({"workload": "c2-amr", **amr_comparison(args)}))
         return

@@ -138,16 +138,20 @@ def random_smooth(n, seed=0, amp=0.2, vel=0.3, gamma=1.4):
 
 
 def amr_box_list(nbox=350, fine_n=512, sizes=(16, 24, 32, 48, 64), seed=7, nblobs=16,
-                 blob_seed=1, align=8, max_tries=200000):
+                 blob_seed=1, align=8, near_tries=400, far_tries=4000):
     """Synthetic fine-level box list of the two-level configuration.
 
-    Boxes with per-dimension sizes drawn uniformly from `sizes` are placed
-    without overlap on the fine index space (fine_n^3, refinement ratio 2 of
-    the base level), each centred near one of the overpressure blobs of the
-    base data (where the flow has its gradients), at `align`-aligned
-    corners.  Returns a list of (lo, hi) integer triples.  The reference
-    builds its boxes with AMReX's clusterer, which is not available here;
-    this list stands in for it with the same box-size statistics.
+    Each box's per-dimension sizes are drawn uniformly from `sizes`; the box
+    is then placed without overlap on the fine index space (fine_n^3,
+    refinement ratio 2 of the base level) at an `align`-aligned corner:
+    first near one of the overpressure blobs of the base data (where the
+    flow has its gradients), and if no free place turns up there, anywhere
+    in the domain.  A drawn size is kept, never redrawn, so the list has the
+    size distribution the configuration states (expected volume per box
+    mean(sizes)^3, 350 x 36.8^3 = 17.4M cells).  Returns a list of (lo, hi)
+    integer triples.  The reference builds its boxes with AMReX's clusterer,
+    which is not available here; this list stands in for it with the same
+    box-size statistics.
     """
     rng = np.random.default_rng(seed)
     brng = np.random.default_rng(blob_seed)
@@ -158,20 +162,30 @@ def amr_box_list(nbox=350, fine_n=512, sizes=(16, 24, 32, 48, 64), seed=7, nblob
         centres.append(c * fine_n)
     occ = np.zeros((fine_n // align,) * 3, dtype=bool)
     boxes = []
-    tries = 0
-    while len(boxes) < nbox and tries < max_tries:
-        tries += 1
-        sz = rng.choice(sizes, size=3)
-        c = centres[rng.integers(len(centres))] + rng.normal(0.0, fine_n * 0.08, size=3)
-        lo = np.floor((c - sz / 2) / align).astype(int) * align
+
+    def place(lo, sz):
         lo = np.clip(lo, 0, fine_n - sz)
         lo = (lo // align) * align
         a = lo // align
         b = (lo + sz + align - 1) // align
         if occ[a[0]:b[0], a[1]:b[1], a[2]:b[2]].any():
-            continue
+            return False
         occ[a[0]:b[0], a[1]:b[1], a[2]:b[2]] = True
         boxes.append((tuple(int(v) for v in lo), tuple(int(v) for v in lo + sz - 1)))
+        return True
+
+    for _ in range(nbox):
+        sz = rng.choice(sizes, size=3)
+        done = False
+        for _t in range(near_tries):
+            c = centres[rng.integers(len(centres))] + rng.normal(0.0, fine_n * 0.08, size=3)
+            if place(np.floor((c - sz / 2) / align).astype(int) * align, sz):
+                done = True
+                break
+        if not done:
+            for _t in range(far_tries):
+                if place(rng.integers(0, fine_n - sz + 1, size=3), sz):
+                    break
     return boxes
 
 

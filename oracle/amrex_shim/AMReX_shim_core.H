@@ -44,9 +44,17 @@
   } while (0)
 #define AMREX_ALWAYS_ASSERT_WITH_MESSAGE(x, m) AMREX_ALWAYS_ASSERT(x)
 
+#ifdef CAMR_FLOP_COUNT
+#include "camr_counted_real.H"
+#endif
+
 namespace amrex {
 
+#ifdef CAMR_FLOP_COUNT
+using Real = camr_flops::CountedReal;
+#else
 using Real = double;
+#endif
 
 // Assertion failures in the reference kernels are counted, not fatal, so that
 // the oracle never aborts the test process; the count is read by the glue.
@@ -73,10 +81,18 @@ template <class T>
 inline const T& min(const T& a, const T& b) { return std::min(a, b); }
 template <class T>
 inline const T& max(const T& a, const T& b) { return std::max(a, b); }
+#ifdef CAMR_FLOP_COUNT
+inline Real min(Real a, Real b) { return std::min(a, b); }
+inline Real max(Real a, Real b) { return std::max(a, b); }
+#endif
 
 namespace Math {
 inline double copysign(double a, double b) { return std::copysign(a, b); }
 inline double abs(double a) { return std::fabs(a); }
+#ifdef CAMR_FLOP_COUNT
+inline Real copysign(Real a, Real b) { return camr_flops::copysign(a, b); }
+inline Real abs(Real a) { return camr_flops::abs(a); }
+#endif
 }  // namespace Math
 
 template <class T, int N>
@@ -246,7 +262,7 @@ class FArrayBox {
   FArrayBox(const Box& b, int nc, Arena* = nullptr) { resize(b, nc); }
   void resize(const Box& b, int nc, Arena* = nullptr) {
     bx_ = b; nc_ = nc;
-    data_.assign(size_t(b.numPts()) * nc, std::numeric_limits<double>::quiet_NaN());
+    data_.assign(size_t(b.numPts()) * nc, Real(std::numeric_limits<double>::quiet_NaN()));
   }
   Array4<Real> array() {
     return Array4<Real>(data_.data(), bx_.lo,
@@ -262,7 +278,7 @@ class FArrayBox {
  private:
   Box bx_;
   int nc_ = 0;
-  std::vector<double> data_;
+  std::vector<Real> data_;
 };
 
 class Geometry {

@@ -224,6 +224,29 @@ def hydro_box(kind, p, bx_lo, bx_hi, dom_lo, dom_hi, bclo, bchi, uin, uin_lo, dx
     return dsdt, flx, nass
 
 
+def lib_path_flops():
+    return os.path.join(HERE, "_ref", "libcamr_ref_flops.so")
+
+
+def count_flops(p, n, bclo, bchi, uin, dx, dt):
+    """Operations of the reference's per-box hydro (ctoprim, srctoprim,
+    hydro_umdrv) on the box [0, n-1] with uin (NVAR, n2+8, n1+8, n0+8) on
+    grow(box, 4): dict of adds, muls, divs, sqrts, cmps, other (abs /
+    copysign) and flops = adds + muls + divs + sqrts."""
+    lib = C.CDLL(lib_path_flops())
+    lib.orc_count_flops.restype = C.c_long
+    uin = np.ascontiguousarray(uin, dtype=np.float64)
+    assert uin.shape == (NVAR, n[2] + 8, n[1] + 8, n[0] + 8)
+    c = (C.c_longlong * 6)()
+    nass = lib.orc_count_flops(C.byref(p), _I3(*n), _I3(*bclo), _I3(*bchi),
+                               C.c_void_p(uin.ctypes.data), _D3(*dx), C.c_double(dt), c)
+    assert nass == 0
+    names = ["adds", "muls", "divs", "sqrts", "cmps", "other"]
+    out = {k: int(v) for k, v in zip(names, c)}
+    out["flops"] = out["adds"] + out["muls"] + out["divs"] + out["sqrts"]
+    return out
+
+
 def ref_ctoprim(p, lo, hi, uin, uin_lo, src=None):
     """The reference's hydro_ctoprim / hydro_srctoprim over [lo, hi] of uin
     (oracle/_ref only): (q (QVAR, ...), qaux (5, ...), src_q (QVAR, ...))."""

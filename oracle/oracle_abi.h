@@ -109,6 +109,13 @@ long orc_ref_hydro_box_full(const orc_params* p, const int bx_lo[3], const int b
                             double* flx0, double* flx1, double* flx2, const double dx[3],
                             double dt);
 
+/* oracle/_ref/libcamr_ref_flops.so only: the reference's per-box hydro on
+ * the box [0, n-1] (uin: NVAR comps on grow(bx,4), zero sources, Cartesian
+ * metrics) with counted operations: counts = adds, multiplies, divides,
+ * square roots, comparisons, abs/copysign. */
+long orc_count_flops(const orc_params* p, const int n[3], const int bclo[3], const int bchi[3],
+                     const double* uin, const double dx[3], double dt, long long counts[6]);
+
 /* Fill every ParmParse default of the reference (Source/Params/_cpp_parameters). */
 void orc_default_params(orc_params* p);
 
