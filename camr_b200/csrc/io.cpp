@@ -84,13 +84,14 @@ struct LevelOut {
 // returns p with p[i] = component c of cell (i, j, k) of box b.
 template <class Row>
 camr_status write_level_files(const std::string& lev, int nbox, const int* boxes, int ncomp,
-                              Row row) {
+                              Row row, const std::string& mf = "Cell") {
   if (!make_dir(lev)) return io_fail("cannot create " + lev);
+  const std::string dname = mf + "_D_00000";
   std::vector<int64_t> offs(nbox);
   std::vector<double> mins(size_t(nbox) * ncomp), maxs(size_t(nbox) * ncomp);
   {
-    std::FILE* f = std::fopen((lev + "/Cell_D_00000").c_str(), "wb");
-    if (!f) return io_fail("cannot write " + lev + "/Cell_D_00000");
+    std::FILE* f = std::fopen((lev + "/" + dname).c_str(), "wb");
+    if (!f) return io_fail("cannot write " + lev + "/" + dname);
     std::vector<double> buf;
     int64_t pos = 0;
     for (int b = 0; b < nbox; ++b) {
@@ -125,15 +126,15 @@ camr_status write_level_files(const std::string& lev, int nbox, const int* boxes
         pos += bc * int64_t(sizeof(double));
       }
     }
-    if (std::fclose(f) != 0) return io_fail("write failed: " + lev + "/Cell_D_00000");
+    if (std::fclose(f) != 0) return io_fail("write failed: " + lev + "/" + dname);
   }
-  std::ofstream h(lev + "/Cell_H");
-  if (!h) return io_fail("cannot write " + lev + "/Cell_H");
+  std::ofstream h(lev + "/" + mf + "_H");
+  if (!h) return io_fail("cannot write " + lev + "/" + mf + "_H");
   h << 1 << '\n' << 1 << '\n' << ncomp << '\n' << 0 << '\n';
   h << '(' << nbox << " 0\n";
   for (int b = 0; b < nbox; ++b) h << box_text(boxes + 6 * b, boxes + 6 * b + 3) << '\n';
   h << ")\n" << nbox << '\n';
-  for (int b = 0; b < nbox; ++b) h << "FabOnDisk: Cell_D_00000 " << offs[b] << '\n';
+  for (int b = 0; b < nbox; ++b) h << "FabOnDisk: " << dname << ' ' << offs[b] << '\n';
   h << '\n' << nbox << ',' << ncomp << '\n';
   h << std::setprecision(17);
   for (int b = 0; b < nbox; ++b) {
@@ -145,7 +146,7 @@ camr_status write_level_files(const std::string& lev, int nbox, const int* boxes
     for (int c = 0; c < ncomp; ++c) h << maxs[size_t(b) * ncomp + c] << ',';
     h << '\n';
   }
-  if (!h) return io_fail("write failed: " + lev + "/Cell_H");
+  if (!h) return io_fail("write failed: " + lev + "/" + mf + "_H");
   return CAMR_OK;
 }
 
@@ -229,9 +230,10 @@ camr_status read_header(const std::string& root, int ncomp, int* finest, double*
 
 // A level's VisMF header: boxes (6 ints each), data files and offsets.
 camr_status read_cell_h(const std::string& lev, int ncomp, std::vector<int>& bx,
-                        std::vector<std::string>& files, std::vector<int64_t>& offs) {
-  std::ifstream ch(lev + "/Cell_H");
-  if (!ch) return io_fail("cannot read " + lev + "/Cell_H");
+                        std::vector<std::string>& files, std::vector<int64_t>& offs,
+                        const std::string& mf = "Cell") {
+  std::ifstream ch(lev + "/" + mf + "_H");
+  if (!ch) return io_fail("cannot read " + lev + "/" + mf + "_H");
   int version = 0, how = 0, nc = 0, ngrow = 0;
   ch >> version >> how >> nc >> ngrow;
   if (nc != ncomp || ngrow != 0) return io_fail("unexpected Cell_H");
@@ -502,6 +504,234 @@ camr_status camr_read_plotfile_amr(const char* dir, const camr_geom* geom, int n
                   });
     if (cs != CAMR_OK) return cs;
     base += int64_t(CAMR_NVAR) * bxn * byn * bzn;
+  }
+  return CAMR_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Checkpoints: CAMR::checkPoint (Source/Utils/CAMR_io.cpp:45-60) is
+// AmrLevel::checkPoint for each level inside Amr::checkPoint, plus the
+// CPUtime file; restart (:23-43) reads them back.  The directory holds
+//   Header          Amr's header: "CheckPointVersion_1.0", the dimension,
+//                   the cumulative time, max and finest level, each level's
+//                   Geometry, the refinement ratios, dt_level, dt_min,
+//                   n_cycle, level_steps and level_count; then per level
+//                   (AmrLevel::checkPoint) the level, its Geometry, the
+//                   refinement ratio to the next level, the BoxArray, the
+//                   number of state types (1) and the StateData record: the
+//                   domain, the BoxArray, the old and new time intervals,
+//                   the MultiFab count (1: no old data is dumped) and the
+//                   relative name of the new data, Level_L/SD_0_New_MF;
+//   Level_L/SD_0_New_MF_H, _D_00000   that MultiFab (VisMF, as plotfiles);
+//   CPUtime         the elapsed CPU time, 15 digits.
+// The text layout restates AMReX's stream formats (Geometry: coordinate
+// system, offset and cell size; the real box; the index domain; the
+// periodicity); AMReX itself is not present to read them, so this layout is
+// not pinned by AMReX's own reader.  The library's reader reads back what
+// the writer writes.
+namespace {
+
+const char* const kCheckpointVersion = "CheckPointVersion_1.0";
+const char* const kStateMF = "SD_0_New_MF";
+
+std::string geometry_text(const int dlo[3], const int dhi[3], const double dx[3],
+                          const double plo[3], const double phi[3], const int periodic[3]) {
+  std::ostringstream o;
+  o << std::setprecision(17);
+  o << "(0 (" << plo[0] << ',' << plo[1] << ',' << plo[2] << ")(" << dx[0] << ',' << dx[1] << ','
+    << dx[2] << ") 1)";
+  o << "(RealBox " << plo[0] << ' ' << phi[0] << ' ' << plo[1] << ' ' << phi[1] << ' ' << plo[2]
+    << ' ' << phi[2] << " )";
+  o << box_text(dlo, dhi) << " P(" << periodic[0] << ',' << periodic[1] << ',' << periodic[2]
+    << ')';
+  return o.str();
+}
+
+void boxarray_text(std::ostream& h, int nbox, const int* boxes) {
+  h << '(' << nbox << " 0\n";
+  for (int b = 0; b < nbox; ++b) h << box_text(boxes + 6 * b, boxes + 6 * b + 3) << '\n';
+  h << ")\n";
+}
+
+// The state of level 0 (domain-shaped) or level 1 (boxes back to back) as
+// the row function write_level_files takes.
+struct LevelData {
+  const camr_geom* geom;
+  int nbox;
+  const int* boxes;
+  double* state;  // level 0: (NVAR, nz, ny, nx) of the domain; level 1: per box
+  bool domain_shaped;
+  std::vector<int64_t> base;
+  void init() {
+    base.assign(size_t(nbox) + 1, 0);
+    for (int b = 0; b < nbox; ++b) {
+      const int* lo = boxes + 6 * b;
+      const int* hi = boxes + 6 * b + 3;
+      base[size_t(b) + 1] = base[size_t(b)] + int64_t(CAMR_NVAR) * (hi[0] - lo[0] + 1) *
+                                                  (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    }
+  }
+  double* row(int b, int c, int j, int k) const {
+    if (domain_shaped) {
+      int n[3];
+      for (int d = 0; d < 3; ++d) n[d] = geom->dom_hi[d] - geom->dom_lo[d] + 1;
+      const int64_t ncell = int64_t(n[0]) * n[1] * n[2];
+      return state + int64_t(c) * ncell +
+             (int64_t(k - geom->dom_lo[2]) * n[1] + (j - geom->dom_lo[1])) * n[0] -
+             geom->dom_lo[0];
+    }
+    const int* lo = boxes + 6 * b;
+    const int* hi = boxes + 6 * b + 3;
+    const int64_t bx = hi[0] - lo[0] + 1, by = hi[1] - lo[1] + 1, bz = hi[2] - lo[2] + 1;
+    return state + base[size_t(b)] + int64_t(c) * bx * by * bz +
+           (int64_t(k - lo[2]) * by + (j - lo[1])) * bx - lo[0];
+  }
+};
+
+std::vector<std::string> read_lines(const std::string& path) {
+  std::vector<std::string> lines;
+  std::ifstream f(path);
+  std::string line;
+  while (std::getline(f, line)) lines.push_back(line);
+  return lines;
+}
+
+}  // namespace
+
+extern "C" {
+
+camr_status camr_write_checkpoint(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                  const double time[2], const double dt[2],
+                                  const int level_step[2], int nbox0, const int* boxes0,
+                                  const double* state0, int nbox1, const int* boxes1,
+                                  const double* state1, double cpu_time) {
+  g_io_error.clear();
+  if (!dir || !geom || !prob_hi || !time || !dt || !level_step || nbox0 <= 0 || !boxes0 ||
+      !state0 || nbox1 < 0 || (nbox1 > 0 && (!boxes1 || !state1)))
+    return io_fail("invalid arguments");
+  if (!host_little_endian()) return io_fail("big-endian hosts are not supported");
+  const int nlev = nbox1 > 0 ? 2 : 1;
+  int dlo[2][3], dhi[2][3];
+  double dxl[2][3];
+  for (int d = 0; d < 3; ++d) {
+    dlo[0][d] = geom->dom_lo[d];
+    dhi[0][d] = geom->dom_hi[d];
+    dxl[0][d] = geom->dx[d];
+    dlo[1][d] = 2 * geom->dom_lo[d];
+    dhi[1][d] = 2 * geom->dom_hi[d] + 1;
+    dxl[1][d] = geom->dx[d] / 2;
+  }
+  if (!boxes_inside(nbox0, boxes0, dlo[0], dhi[0]) ||
+      (nlev == 2 && !boxes_inside(nbox1, boxes1, dlo[1], dhi[1])))
+    return io_fail("box outside the domain");
+  const std::string root(dir);
+  if (!make_dir(root)) return io_fail("cannot create " + root);
+  const int nb[2] = {nbox0, nbox1};
+  const int* bl[2] = {boxes0, boxes1};
+  const double* sl[2] = {state0, state1};
+  for (int l = 0; l < nlev; ++l) {
+    LevelData D{geom, nb[l], bl[l], const_cast<double*>(sl[l]), l == 0, {}};
+    D.init();
+    camr_status cs = write_level_files(
+        root + "/Level_" + std::to_string(l), nb[l], bl[l], CAMR_NVAR,
+        [&](int b, int c, int j, int k) { return D.row(b, c, j, k); }, kStateMF);
+    if (cs != CAMR_OK) return cs;
+  }
+  std::ofstream h(root + "/Header");
+  if (!h) return io_fail("cannot write " + root + "/Header");
+  h << std::setprecision(17);
+  h << kCheckpointVersion << '\n' << 3 << '\n' << time[0] << '\n' << nlev - 1 << '\n'
+    << nlev - 1 << '\n';
+  std::string gtext[2];
+  for (int l = 0; l < nlev; ++l) {
+    gtext[l] = geometry_text(dlo[l], dhi[l], dxl[l], geom->prob_lo, prob_hi, geom->is_periodic);
+    h << gtext[l] << ' ';
+  }
+  h << '\n';
+  for (int l = 0; l + 1 < nlev; ++l) h << "(2,2,2) ";
+  h << '\n';
+  for (int l = 0; l < nlev; ++l) h << dt[l] << ' ';  // dt_level
+  h << '\n';
+  for (int l = 0; l < nlev; ++l) h << dt[l] << ' ';  // dt_min
+  h << '\n';
+  for (int l = 0; l < nlev; ++l) h << (l == 0 ? 1 : 2) << ' ';  // n_cycle
+  h << '\n';
+  for (int l = 0; l < nlev; ++l) h << level_step[l] << ' ';
+  h << '\n';
+  for (int l = 0; l < nlev; ++l) h << 0 << ' ';  // level_count (steps since regrid)
+  h << '\n';
+  for (int l = 0; l < nlev; ++l) {
+    h << l << '\n' << gtext[l] << '\n' << (l + 1 < nlev ? "(2,2,2)" : "(1,1,1)") << '\n';
+    boxarray_text(h, nb[l], bl[l]);
+    h << 1 << '\n';
+    // StateData::checkPoint
+    h << box_text(dlo[l], dhi[l]) << '\n';
+    boxarray_text(h, nb[l], bl[l]);
+    h << time[l] - dt[l] << '\n' << time[l] - dt[l] << '\n' << time[l] << '\n' << time[l] << '\n';
+    h << 1 << '\n' << "Level_" << l << '/' << kStateMF << '\n';
+  }
+  if (!h) return io_fail("write failed: " + root + "/Header");
+  std::ofstream cpu(root + "/CPUtime");
+  cpu << std::setprecision(15) << cpu_time;
+  if (!cpu) return io_fail("write failed: " + root + "/CPUtime");
+  return CAMR_OK;
+}
+
+camr_status camr_read_checkpoint(const char* dir, const camr_geom* geom, double time[2],
+                                 double dt[2], int level_step[2], double* state0, int nbox1,
+                                 const int* boxes1, double* state1) {
+  g_io_error.clear();
+  if (!dir || !geom || !time || !dt || !level_step || !state0 || nbox1 < 0 ||
+      (nbox1 > 0 && (!boxes1 || !state1)))
+    return io_fail("invalid arguments");
+  const std::string root(dir);
+  const std::vector<std::string> L = read_lines(root + "/Header");
+  if (L.size() < 12 || L[0] != kCheckpointVersion || std::atoi(L[1].c_str()) != 3)
+    return io_fail("not a 3-D checkpoint of this layout");
+  const int finest = std::atoi(L[4].c_str());
+  if (finest != (nbox1 > 0 ? 1 : 0)) return io_fail("level count differs from the hierarchy's");
+  const int nlev = finest + 1;
+  // lines: 5 geometries, 6 ratios, 7 dt_level, 8 dt_min, 9 n_cycle, 10 level_steps
+  {
+    std::istringstream a(L[7]), b(L[10]);
+    for (int l = 0; l < nlev; ++l) a >> dt[l];
+    for (int l = 0; l < nlev; ++l) b >> level_step[l];
+  }
+  // per level: the StateData record's new time (the line after the old
+  // interval) -- find each "Level_L/SD_0_New_MF" line and read back 2 lines
+  for (int l = 0; l < nlev; ++l) {
+    const std::string tag = "Level_" + std::to_string(l) + "/" + kStateMF;
+    size_t at = 0;
+    while (at < L.size() && L[at] != tag) ++at;
+    if (at == L.size() || at < 3) return io_fail("no state record for level " + std::to_string(l));
+    time[l] = std::atof(L[at - 2].c_str());
+  }
+  for (int l = 0; l < nlev; ++l) {
+    std::vector<int> bx;
+    std::vector<std::string> files;
+    std::vector<int64_t> offs;
+    const std::string lev = root + "/Level_" + std::to_string(l);
+    camr_status cs = read_cell_h(lev, CAMR_NVAR, bx, files, offs, kStateMF);
+    if (cs != CAMR_OK) return cs;
+    const int nbox = int(files.size());
+    if (l == 0) {
+      if (!boxes_inside(nbox, bx.data(), geom->dom_lo, geom->dom_hi))
+        return io_fail("box outside domain");
+    } else {
+      if (nbox != nbox1) return io_fail("fine box count differs from the hierarchy's");
+      for (int k = 0; k < 6 * nbox1; ++k)
+        if (bx[size_t(k)] != boxes1[k]) return io_fail("fine boxes differ from the hierarchy's");
+    }
+    LevelData D{geom, nbox, l == 0 ? bx.data() : boxes1, l == 0 ? state0 : state1, l == 0, {}};
+    D.init();
+    for (int b = 0; b < nbox; ++b) {
+      cs = read_fab(lev + "/" + files[size_t(b)], offs[size_t(b)], &bx[size_t(6 * b)],
+                    &bx[size_t(6 * b + 3)], CAMR_NVAR,
+                    [&](int c, int j, int k) { return D.row(b, c, j, k); });
+      if (cs != CAMR_OK) return cs;
+    }
   }
   return CAMR_OK;
 }

@@ -61,6 +61,7 @@ struct camr_level {
   double* src_h = nullptr;  // sources_for_hydro (CTU with gravity), padded NVAR
   bool ctu_grav = false;
   FloorList floor;          // cells below the density floor of the current pass
+  bool restart_est = false; // next step: CFL estimate from the state, then computeNewDt
   bool own_stream;     // the library created `stream` (caller passed NULL)
   int64_t kernels_per_step;  // launches inside one captured step
   // Host transfers run on their own streams so that the next state upload
@@ -454,7 +455,7 @@ camr_status camr_level_init_finalize(camr_level* lev) {
 }
 
 static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_dev,
-                              StageTimer* tm = nullptr) {
+                              StageTimer* tm = nullptr, bool est = false) {
   LevelState& S = lev->st;
   const LGeom& L = lev->L;
   cudaStream_t st = lev->stream;
@@ -465,7 +466,7 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   auto mark = [&](const char* what) {
     if (tm) tm->mark(st, what);
   };
-  if (first) {
+  if (first || est) {
     mark("est_dt");
     k_reset_bits<<<1, 1, 0, st>>>(S.dtmin_bits);
     k_est_dt<<<gv, kBlk, 0, st>>>(L, lev->P, S.S, S.dtmin_bits);
@@ -591,7 +592,12 @@ camr_status camr_level_advance(camr_level* lev, int nsteps, const double* fixed_
       fixed_dev = lev->fixed_dev;
     }
     cudaError_t e;
-    if (!first && !fixed_dts && lev->desc.use_graph) {
+    if (lev->restart_est) {
+      // the first step after a restart: estTimeStep on the restored state,
+      // then computeNewDt against the checkpoint's dt (uncaptured)
+      lev->restart_est = false;
+      e = issue_step(lev, false, fixed_dev, nullptr, true);
+    } else if (!first && !fixed_dts && lev->desc.use_graph) {
       if (!lev->graph_ready) {
         cudaGraph_t g;
         e = cudaStreamBeginCapture(lev->stream, cudaStreamCaptureModeThreadLocal);
@@ -703,6 +709,18 @@ camr_status camr_level_state_fab(camr_level* lev, camr_fab* fab) {
   fab->kstride = lev->L.sz;
   fab->nstride = lev->L.sn;
   fab->ncomp = NVAR;
+  return CAMR_OK;
+}
+
+camr_status camr_level_restart(camr_level* lev, double dt_prev, int steps_done) {
+  if (!lev || !(dt_prev > 0.0) || steps_done < 1) return CAMR_ERR_INVALID;
+  cudaError_t e = cudaMemcpyAsync(lev->st.dt_cur, &dt_prev, sizeof(double),
+                                  cudaMemcpyHostToDevice, lev->stream);
+  // the pageable source must outlive the copy
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  lev->steps_taken = steps_done;
+  lev->restart_est = true;
   return CAMR_OK;
 }
 

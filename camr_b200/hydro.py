@@ -287,6 +287,11 @@ class Level:
         lib().camr_level_get_error(self._h, C.byref(info))
         return (info.code, info.i, info.j, info.k)
 
+    def restart(self, dt_prev, steps_done):
+        """Continue from a checkpoint's state (set_state first): the next dt
+        follows computeNewDt against dt_prev."""
+        check(lib().camr_level_restart(self._h, float(dt_prev), int(steps_done)), "restart")
+
     def floor_resets(self):
         """Cells enforce_min_density has reset since the level was created."""
         v = C.c_int64()
@@ -646,6 +651,57 @@ def write_plotfile_amr(path, S0, S1, geom, prob_hi, fine_boxes, time=0.0, level_
     if st != 0:
         raise native.CamrError(st, "camr_write_plotfile_amr " +
                                lib().camr_io_last_error().decode())
+
+
+def write_checkpoint(path, geom, prob_hi, S0, time, dt, level_step, S1=None, fine_boxes=(),
+                     max_grid_size=(32, 32, 32), cpu_time=0.0):
+    """Checkpoint of one level (S0) or of the two-level hierarchy (S0, S1,
+    fine_boxes) in CAMR::checkPoint's layout (camr_write_checkpoint).  time,
+    dt, level_step: per level (a number for one level)."""
+    n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+    a = np.ascontiguousarray(S0, dtype=np.float64)
+    assert a.shape == (NVAR, n[2], n[1], n[0])
+    boxes0 = level_boxes(n, max_grid_size, tuple(geom.dom_lo))
+    b0 = np.array([list(lo) + list(hi) for lo, hi in boxes0], dtype=np.int32).ravel()
+    two = len(fine_boxes) > 0
+    f = np.ascontiguousarray(S1, dtype=np.float64).ravel() if two else None
+    b1 = (np.array([list(lo) + list(hi) for lo, hi in fine_boxes], dtype=np.int32).ravel()
+          if two else None)
+    per = (lambda v: tuple(v) if np.ndim(v) else (v, 0))  # noqa: E731
+    t = (C.c_double * 2)(*per(time))
+    d = (C.c_double * 2)(*per(dt))
+    stp = (C.c_int * 2)(*[int(x) for x in per(level_step)])
+    ph = (C.c_double * 3)(*prob_hi)
+    st = lib().camr_write_checkpoint(str(path).encode(), C.byref(geom), C.byref(ph), C.byref(t),
+                                     C.byref(d), C.byref(stp), len(boxes0), b0.ctypes.data,
+                                     a.ctypes.data, len(fine_boxes),
+                                     b1.ctypes.data if two else None,
+                                     f.ctypes.data if two else None, float(cpu_time))
+    if st != 0:
+        raise native.CamrError(st, "camr_write_checkpoint " + lib().camr_io_last_error().decode())
+
+
+def read_checkpoint(path, geom, fine_boxes=()):
+    """Read a checkpoint of write_checkpoint back: (S0, S1 or None, times,
+    dts, level steps), the per-level values as tuples."""
+    n = tuple(geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3))
+    s0 = np.zeros((NVAR, n[2], n[1], n[0]))
+    ncell1 = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in fine_boxes)
+    two = len(fine_boxes) > 0
+    s1 = np.zeros(NVAR * ncell1) if two else None
+    b1 = (np.array([list(lo) + list(hi) for lo, hi in fine_boxes], dtype=np.int32).ravel()
+          if two else None)
+    t = (C.c_double * 2)()
+    d = (C.c_double * 2)()
+    stp = (C.c_int * 2)()
+    st = lib().camr_read_checkpoint(str(path).encode(), C.byref(geom), C.byref(t), C.byref(d),
+                                    C.byref(stp), s0.ctypes.data, len(fine_boxes),
+                                    b1.ctypes.data if two else None,
+                                    s1.ctypes.data if two else None)
+    if st != 0:
+        raise native.CamrError(st, "camr_read_checkpoint " + lib().camr_io_last_error().decode())
+    nl = 2 if two else 1
+    return s0, s1, tuple(t)[:nl], tuple(d)[:nl], tuple(stp)[:nl]
 
 
 def read_plotfile_amr(path, geom, fine_boxes, ncomp=NVAR):

@@ -107,6 +107,15 @@ SIGNATURES = {
     "camr_est_dt": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab),
                               C.POINTER(HydroParams), C.POINTER(C.c_double), C.c_void_p]),
     "camr_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),
+    "camr_level_restart": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    "camr_write_checkpoint": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.POINTER(C.c_double * 3),
+                                        C.POINTER(C.c_double * 2), C.POINTER(C.c_double * 2),
+                                        C.POINTER(C.c_int * 2), C.c_int, C.c_void_p,
+                                        C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_double]),
+    "camr_read_checkpoint": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.POINTER(C.c_double * 2),
+                                       C.POINTER(C.c_double * 2), C.POINTER(C.c_int * 2),
+                                       C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "camr_launch_count": (C.c_int64, []),
     "camr_level_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "camr_last_error_string": (C.c_char_p, []),

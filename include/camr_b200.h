@@ -303,6 +303,14 @@ camr_status camr_level_sync(camr_level* lev);
 /* CAMR::initData's epilogue: enforce_consistent_e then computeTemp. */
 camr_status camr_level_init_finalize(camr_level* lev);
 
+/* Restart (Amr::restart / CAMR::restart, Source/Utils/CAMR_io.cpp:23-43)
+ * after camr_level_set_state with a checkpoint's state: dt_prev is the
+ * checkpoint's dt_level and steps_done its level step count.  The next
+ * step estimates the CFL dt from the restored state and applies
+ * computeNewDt against dt_prev (change_max), as a run that never stopped
+ * would, instead of computeInitialDt. */
+camr_status camr_level_restart(camr_level* lev, double dt_prev, int steps_done);
+
 /* Advance nsteps coarse steps.  The dt of each step is computed on the
  * device (first step: computeInitialDt; later: computeNewDt) unless
  * fixed_dts is non-NULL (host array of nsteps dts).  Stream-ordered; no
@@ -551,6 +559,27 @@ camr_status camr_write_plotfile_amr(const char* dir, const camr_geom* geom, cons
 camr_status camr_read_plotfile_amr(const char* dir, const camr_geom* geom, int ncomp,
                                    double* state0, int nbox1, const int* boxes1,
                                    double* state1, double* time, int level_step[2]);
+/* Checkpoint of one level or of the two-level hierarchy, in the layout of
+ * CAMR::checkPoint (Source/Utils/CAMR_io.cpp:45-60), i.e. AMReX's
+ * Amr::checkPoint with AmrLevel / StateData records: dir/Header (times,
+ * dt_level, n_cycle, level steps, per-level geometry, BoxArray and state
+ * record), Level_L/SD_0_New_MF_H and _D_00000 (VisMF, NVAR comps, the new
+ * state), and dir/CPUtime.  time[l], dt[l], level_step[l]: each level's
+ * time, last dt and step count.  Level 0: nbox0 boxes (lo0,lo1,lo2,hi0,
+ * hi1,hi2) with state0 over the domain (NVAR, nz, ny, nx); level 1 (nbox1 =
+ * 0: none) as for camr_write_plotfile_amr.  AMReX is not present here, so
+ * its own restart reader has not read these files. */
+camr_status camr_write_checkpoint(const char* dir, const camr_geom* geom, const double prob_hi[3],
+                                  const double time[2], const double dt[2],
+                                  const int level_step[2], int nbox0, const int* boxes0,
+                                  const double* state0, int nbox1, const int* boxes1,
+                                  const double* state1, double cpu_time);
+/* Reads a checkpoint of camr_write_checkpoint back: times, dts, steps and
+ * the states (level 1 for the same fine boxes in the same order). */
+camr_status camr_read_checkpoint(const char* dir, const camr_geom* geom, double time[2],
+                                 double dt[2], int level_step[2], double* state0, int nbox1,
+                                 const int* boxes1, double* state1);
+
 /* Why the last plotfile call on this thread failed ("" if it did not). */
 const char* camr_io_last_error(void);
 

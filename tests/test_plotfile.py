@@ -297,3 +297,101 @@ def test_amr_hierarchy_two_level_plotfile(tmp_path):
     lev1 = read_level(tmp_path / "plt_amr_gpu", 1, 10)
     assert np.array_equal(np.concatenate([v.ravel() for _, _, v in lev1]), np.asarray(c1).ravel())
     assert t0 > 0 and abs(t0 - t1) <= 1e-12 * t0
+
+
+def parse_checkpoint_header(path):
+    """This test's own reading of the checkpoint Header layout."""
+    L = (path / "Header").read_text().split("\n")
+    assert L[0] == "CheckPointVersion_1.0" and int(L[1]) == 3
+    out = {"time": float(L[2]), "max_level": int(L[3]), "finest": int(L[4]),
+           "dt_level": [float(x) for x in L[7].split()],
+           "n_cycle": [int(x) for x in L[9].split()],
+           "level_steps": [int(x) for x in L[10].split()]}
+    out["state_files"] = [x for x in L if x.startswith("Level_") and x.endswith("SD_0_New_MF")]
+    return out
+
+
+@pytest.mark.parametrize("levels", [1, 2])
+def test_checkpoint_round_trip(tmp_path, native_lib, levels):
+    """camr_write_checkpoint -> camr_read_checkpoint returns states, times,
+    dts and level steps bit for bit; the Header and the VisMF data parse
+    independently; CPUtime holds the CPU time."""
+    n = (16, 8, 8)
+    geom = hydro.make_geom(n)
+    s0 = P.random_smooth(n, seed=8)
+    fine = [((0, 0, 0), (7, 5, 3)), ((16, 8, 6), (23, 15, 15))] if levels == 2 else []
+    rng = np.random.default_rng(1)
+    cells = sum((h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1) for l, h in fine)
+    s1 = rng.standard_normal(10 * cells) if fine else None
+    t = (0.25, 0.25) if levels == 2 else 0.25
+    dt = (1e-3, 5e-4) if levels == 2 else 1e-3
+    steps = (7, 14) if levels == 2 else 7
+    path = tmp_path / "chk00007"
+    hydro.write_checkpoint(path, geom, (1, 0.5, 0.5), s0, t, dt, steps, S1=s1, fine_boxes=fine,
+                           max_grid_size=(8, 8, 8), cpu_time=12.5)
+    b0, b1, tt, dd, ss = hydro.read_checkpoint(path, geom, fine)
+    assert np.array_equal(b0, s0)
+    if fine:
+        assert np.array_equal(b1, s1)
+    assert tt == (t if levels == 2 else (t,)) and dd == (dt if levels == 2 else (dt,))
+    assert ss == (steps if levels == 2 else (steps,))
+    h = parse_checkpoint_header(path)
+    assert h["finest"] == levels - 1 and h["n_cycle"] == [1, 2][:levels]
+    assert h["state_files"] == [f"Level_{l}/SD_0_New_MF" for l in range(levels)]
+    assert float((path / "CPUtime").read_text()) == 12.5
+    got = np.zeros_like(s0)
+    for lo, hi, v in read_level_mf(path, 0, "SD_0_New_MF"):
+        got[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = v
+    assert np.array_equal(got, s0)
+    with pytest.raises(native.CamrError):
+        hydro.read_checkpoint(path, geom, [] if fine else [((0, 0, 0), (1, 1, 1))])
+
+
+def read_level_mf(path, lev, mf):
+    cell_h = (path / f"Level_{lev}" / f"{mf}_H").read_text().split("\n")
+    nb = int(cell_h[4].strip("(").split()[0])
+    boxes = [[int(x) for x in re.findall(r"-?\d+", cell_h[5 + b])] for b in range(nb)]
+    fabs = [cell_h[7 + nb + b].split() for b in range(nb)]
+    out = []
+    for b, (tag, fname, off) in enumerate(fabs):
+        assert tag == "FabOnDisk:" and fname == f"{mf}_D_00000"
+        data = (path / f"Level_{lev}" / fname).read_bytes()
+        end = data.index(b"\n", int(off))
+        lo, hi = boxes[b][:3], boxes[b][3:6]
+        bn = [hi[d] - lo[d] + 1 for d in range(3)]
+        vals = np.frombuffer(data, dtype="<f8", count=10 * bn[0] * bn[1] * bn[2], offset=end + 1)
+        out.append((lo, hi, vals.reshape(10, bn[2], bn[1], bn[0])))
+    return out
+
+
+@pytest.mark.gpu
+def test_level_checkpoint_restart_continues_exactly(tmp_path):
+    """Checkpoint after 4 steps (device dts), restart into a new level with
+    camr_level_restart: the next steps (computeNewDt against the checkpoint's
+    dt) give the same states and dts as the run that never stopped."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    n = (24, 24, 24)
+    s0 = P.blobs(n, tuple(1.0 / v for v in n), nblobs=3, seed=5, r_min=0.1, r_max=0.2)
+    geom = hydro.make_geom(n)
+    prm = native.default_params(ppm_type=1, cfl=0.7)
+    a = hydro.Level(geom, prm)
+    a.set_state(s0)
+    a.init_finalize()
+    a.advance(4)
+    mid = a.get_state()
+    dt4 = a.last_dt()
+    hydro.write_checkpoint(tmp_path / "chk4", geom, (1, 1, 1), mid, 0.0, dt4, 4)
+    a.advance(3)
+    want = a.get_state()
+    want_dt = a.last_dt()
+    a.close()
+    back, _, _, dd, ss = hydro.read_checkpoint(tmp_path / "chk4", geom)
+    b = hydro.Level(geom, prm)
+    b.set_state(back)
+    b.restart(dd[0], ss[0])
+    b.advance(3)
+    assert b.last_dt() == want_dt
+    assert np.array_equal(b.get_state(), want)
+    b.close()
