@@ -287,6 +287,18 @@ __global__ void __launch_bounds__(kFB) k_fab_ghost_temp(FabSet S, KParams P) {
   for (int n = 0; n < NVAR; ++n) b.f(i, j, k, n) = s[n];
 }
 
+// computeTemp in place on every ghost cell of the fabs (within ng).
+__global__ void __launch_bounds__(kFB) k_fab_ghost_temp_in_place(FabSet S, KParams P) {
+  const FabBox& b = S.box[blockIdx.y];
+  int i, j, k;
+  if (!fab_region_cell(b, int64_t(blockIdx.x) * kFB + threadIdx.x, i, j, k)) return;
+  if (in_box(b, i, j, k)) return;
+  double s[NVAR];
+  for (int n = 0; n < NVAR; ++n) s[n] = b.f(i, j, k, n);
+  compute_temp(s, P);
+  for (int n = 0; n < NVAR; ++n) b.f(i, j, k, n) = s[n];
+}
+
 // computeTemp on the valid cells (after every ghost cell has read them).
 __global__ void __launch_bounds__(kFB) k_fab_valid_temp(FabSet S, KParams P) {
   const FabBox& b = S.box[blockIdx.y];
@@ -419,9 +431,9 @@ camr_status camr_fill_ghosts(const camr_geom* geom, int nbox, const camr_box_fab
   return cuda_status_of(e);
 }
 
-camr_status camr_clean_state(const camr_geom* geom, int nbox, const camr_box_fab* boxes, int ng,
-                             const camr_hydro_params* p, void* stream) {
-  if (!p) return CAMR_ERR_INVALID;
+camr_status camr_clean_state_parts(const camr_geom* geom, int nbox, const camr_box_fab* boxes,
+                                   int ng, const camr_hydro_params* p, int parts, void* stream) {
+  if (!p || parts <= 0 || parts > 15) return CAMR_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   DevError* err = nullptr;
   cudaError_t e = library_error_word(st, &err);
@@ -432,35 +444,56 @@ camr_status camr_clean_state(const camr_geom* geom, int nbox, const camr_box_fab
   camr_status cs = make_fabset(geom, nbox, boxes, ng, st, S, &dev, &mx);
   if (cs != CAMR_OK) return cs;
   const KParams P = make_kparams(*p);
-  // the list of cells below the density floor: count, then the cells
   void* fbuf = nullptr;
-  e = cudaMallocAsync(&fbuf, sizeof(int64_t) * (kFloorCap + 1), st);
-  if (e != cudaSuccess) {
-    cudaFreeAsync(dev, st);
-    return CAMR_ERR_NOMEM;
+  if (parts & CAMR_CLEAN_VALID) {
+    // the list of cells below the density floor: count, then the cells
+    e = cudaMallocAsync(&fbuf, sizeof(int64_t) * (kFloorCap + 1), st);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(dev, st);
+      return CAMR_ERR_NOMEM;
+    }
+    FloorList fl;
+    fl.count = static_cast<int*>(fbuf);
+    fl.cells = static_cast<int64_t*>(fbuf) + 1;
+    e = cudaMemsetAsync(fl.count, 0, sizeof(int), st);
+    int64_t mv = 0;
+    for (int b = 0; b < nbox; ++b) {
+      const int64_t c = int64_t(boxes[b].hi[0] - boxes[b].lo[0] + 1) *
+                        (boxes[b].hi[1] - boxes[b].lo[1] + 1) *
+                        (boxes[b].hi[2] - boxes[b].lo[2] + 1);
+      mv = c > mv ? c : mv;
+    }
+    if (e == cudaSuccess) {
+      k_fab_floor_list<<<fab_grid(S, mv), kFB, 0, st>>>(S, P, fl);
+      k_fab_floor_walk<<<1, 1024, 0, st>>>(S, P, fl, err);
+      k_fab_normalize<<<fab_grid(S, mx), kFB, 0, st>>>(S);
+      count_launch(3);
+    }
   }
-  FloorList fl;
-  fl.count = static_cast<int*>(fbuf);
-  fl.cells = static_cast<int64_t*>(fbuf) + 1;
-  e = cudaMemsetAsync(fl.count, 0, sizeof(int), st);
-  int64_t mv = 0;
-  for (int b = 0; b < nbox; ++b) {
-    const int64_t c = int64_t(boxes[b].hi[0] - boxes[b].lo[0] + 1) *
-                      (boxes[b].hi[1] - boxes[b].lo[1] + 1) * (boxes[b].hi[2] - boxes[b].lo[2] + 1);
-    mv = c > mv ? c : mv;
-  }
-  if (e == cudaSuccess) {
-    k_fab_floor_list<<<fab_grid(S, mv), kFB, 0, st>>>(S, P, fl);
-    k_fab_floor_walk<<<1, 1024, 0, st>>>(S, P, fl, err);
-    k_fab_normalize<<<fab_grid(S, mx), kFB, 0, st>>>(S);
+  if (e == cudaSuccess && ng > 0 && (parts & CAMR_CLEAN_GHOSTS_FROM_OWNERS)) {
     k_fab_ghost_temp<<<fab_grid(S, mx), kFB, 0, st>>>(S, P);
-    k_fab_valid_temp<<<fab_grid(S, mx), kFB, 0, st>>>(S, P);
-    count_launch(5);
-    e = cudaGetLastError();
+    count_launch();
   }
-  cudaFreeAsync(fbuf, st);
+  if (e == cudaSuccess && ng > 0 && (parts & CAMR_CLEAN_GHOSTS_TEMP)) {
+    k_fab_ghost_temp_in_place<<<fab_grid(S, mx), kFB, 0, st>>>(S, P);
+    count_launch();
+  }
+  if (e == cudaSuccess && (parts & CAMR_CLEAN_VALID_TEMP)) {
+    k_fab_valid_temp<<<fab_grid(S, mx), kFB, 0, st>>>(S, P);
+    count_launch();
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (fbuf) cudaFreeAsync(fbuf, st);
   cudaFreeAsync(dev, st);
   return cuda_status_of(e);
+}
+
+camr_status camr_clean_state(const camr_geom* geom, int nbox, const camr_box_fab* boxes, int ng,
+                             const camr_hydro_params* p, void* stream) {
+  return camr_clean_state_parts(geom, nbox, boxes, ng, p,
+                                CAMR_CLEAN_VALID | CAMR_CLEAN_GHOSTS_FROM_OWNERS |
+                                    CAMR_CLEAN_VALID_TEMP,
+                                stream);
 }
 
 camr_status camr_est_dt(const camr_geom* geom, int nbox, const camr_box_fab* boxes,

@@ -11,6 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("CAMR_B200_LIB") or os.path.join(HERE, "_lib", "libcamr_b200.so")
 
 NVAR = 10
+# camr_clean_state_parts parts (include/camr_b200.h)
+CLEAN_VALID, CLEAN_GHOSTS_FROM_OWNERS, CLEAN_GHOSTS_TEMP, CLEAN_VALID_TEMP = 1, 2, 4, 8
 STATUS = {0: "CAMR_OK", 1: "CAMR_ERR_INVALID", 2: "CAMR_ERR_UNSUPPORTED", 3: "CAMR_ERR_CUDA",
           4: "CAMR_ERR_NUMERIC", 5: "CAMR_ERR_NOMEM", 6: "CAMR_ERR_TIMEOUT"}
 
@@ -104,6 +106,8 @@ SIGNATURES = {
                                    C.c_void_p]),
     "camr_clean_state": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab), C.c_int,
                                    C.POINTER(HydroParams), C.c_void_p]),
+    "camr_clean_state_parts": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab), C.c_int,
+                                         C.POINTER(HydroParams), C.c_int, C.c_void_p]),
     "camr_est_dt": (C.c_int, [C.POINTER(Geom), C.c_int, C.POINTER(BoxFab),
                               C.POINTER(HydroParams), C.POINTER(C.c_double), C.c_void_p]),
     "camr_get_error": (C.c_int, [C.c_void_p, C.POINTER(ErrorInfo)]),

@@ -197,6 +197,26 @@ camr_status camr_fill_ghosts(const camr_geom* geom, int nbox, const camr_box_fab
  * boxes.  Errors go to the library's error word (camr_get_error). */
 camr_status camr_clean_state(const camr_geom* geom, int nbox, const camr_box_fab* boxes, int ng,
                              const camr_hydro_params* p, void* stream);
+/* The parts of camr_clean_state, for a caller whose boxes are spread over
+ * processes and who exchanges ghost cells between them itself: clean_state
+ * = CAMR_CLEAN_VALID (enforce_min_density + normalize_species on the valid
+ * cells), then normalize_species' FillBoundary of the interior and periodic
+ * ghost cells from the owners' normalized valid cells, then computeTemp on
+ * every cell.  CAMR_CLEAN_GHOSTS_FROM_OWNERS does that FillBoundary for
+ * ghosts whose owner is in the list and computeTemp on all ghost cells;
+ * a distributed caller instead fills the interior ghosts itself after
+ * CAMR_CLEAN_VALID and then asks for CAMR_CLEAN_GHOSTS_TEMP (computeTemp on
+ * every ghost cell in place).  CAMR_CLEAN_VALID_TEMP: computeTemp on the
+ * valid cells, which must come after every ghost fill has read them.
+ * camr_clean_state = VALID | GHOSTS_FROM_OWNERS | VALID_TEMP. */
+enum {
+  CAMR_CLEAN_VALID = 1,
+  CAMR_CLEAN_GHOSTS_FROM_OWNERS = 2,
+  CAMR_CLEAN_GHOSTS_TEMP = 4,
+  CAMR_CLEAN_VALID_TEMP = 8
+};
+camr_status camr_clean_state_parts(const camr_geom* geom, int nbox, const camr_box_fab* boxes,
+                                   int ng, const camr_hydro_params* p, int parts, void* stream);
 /* estTimeStep's hydro limit (Source/CAMR.cpp:490-563 with
  * Source/Utils/Timestep.H:18-61): cfl * the minimum over the valid cells of
  * dx_d / (c + |u_d|), capped by max_dt; fixed_dt when that is set.
