@@ -31,6 +31,11 @@ constexpr int kBlock = 128;
 #ifndef CAMR_MINB_FLUX3
 #define CAMR_MINB_FLUX3 4
 #endif
+// 1: the level and per-box CTU paths run the second and final flux passes
+// as one kernel with the second-pass records in shared memory (k_flux23)
+#ifndef CAMR_FLUX23
+#define CAMR_FLUX23 1
+#endif
 
 inline unsigned grid_for(int64_t n) { return unsigned((n + kBlock - 1) / kBlock); }
 
@@ -345,10 +350,10 @@ struct Reg6 {
 // K5: second pass "D|E": D-face states corrected by E fluxes (hydro_transdo,
 // Godunov_3D.cpp:218-380), then the Riemann flux.  blockIdx.y = combo(D,E).
 template <int D, int E>
-__device__ __forceinline__ void flux2_body(int i, int j, int k, const Space& s, const KGeom& g,
-                                           const KParams& P, const DtRef& dtr, const double* q,
-                                           const double* smD, const double* spD,
-                                           const double* fE, double* o) {
+__device__ __forceinline__ void flux2_record(int i, int j, int k, const Space& s, const KGeom& g,
+                                             const KParams& P, const DtRef& dtr, const double* q,
+                                             const double* smD, const double* spD,
+                                             const double* fE, double* rec) {
   const int64_t stD = (D == 0) ? 1 : (D == 1) ? s.sy : s.sz;
   const int64_t stE = (E == 0) ? 1 : (E == 1) ? s.sy : s.sz;
   const int64_t at = s.idx(i, j, k);
@@ -379,15 +384,27 @@ __device__ __forceinline__ void flux2_body(int i, int j, int k, const Space& s, 
   const int idx = (D == 0) ? i : (D == 1) ? j : k;
   double f[NVAR], qpres, qun;
   cmpflx<D>(qm, qp, aL, aR, idx, g.bclo[D], g.bchi[D], g.dlo[D], g.dhi[D], P, f, qpres, qun);
-  o[at + FR_RHO * s.sn] = f[URHO];
-  o[at + FR_MX * s.sn] = f[UMX];
-  o[at + FR_MY * s.sn] = f[UMY];
-  o[at + FR_MZ * s.sn] = f[UMZ];
-  o[at + FR_E * s.sn] = f[UEDEN];
+  rec[FR_RHO] = f[URHO];
+  rec[FR_MX] = f[UMX];
+  rec[FR_MY] = f[UMY];
+  rec[FR_MZ] = f[UMZ];
+  rec[FR_E] = f[UEDEN];
 #pragma unroll
-  for (int spc = 0; spc < NSPEC; ++spc) o[at + (FR_FS + spc) * s.sn] = f[UFS + spc];
-  o[at + FR_PRES * s.sn] = qpres;
-  o[at + FR_UN * s.sn] = qun;
+  for (int spc = 0; spc < NSPEC; ++spc) rec[FR_FS + spc] = f[UFS + spc];
+  rec[FR_PRES] = qpres;
+  rec[FR_UN] = qun;
+}
+
+template <int D, int E>
+__device__ __forceinline__ void flux2_body(int i, int j, int k, const Space& s, const KGeom& g,
+                                           const KParams& P, const DtRef& dtr, const double* q,
+                                           const double* smD, const double* spD,
+                                           const double* fE, double* o) {
+  double rec[FR_N];
+  flux2_record<D, E>(i, j, k, s, g, P, dtr, q, smD, spD, fE, rec);
+  const int64_t at = s.idx(i, j, k);
+#pragma unroll
+  for (int n = 0; n < FR_N; ++n) o[at + n * s.sn] = rec[n];
 }
 
 __global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX2) k_flux2(Reg6 regs, Space s, KGeom g, KParams P,
@@ -559,6 +576,163 @@ __global__ void __launch_bounds__(kBlock, CAMR_MINB_FLUX3) k_flux3(Region r0, Re
       if (region_cell(r2, t, i, j, k))
         flux3_body<2, MET>(i, j, k, s, g, P, dtr, q, srcq, has_src, sm.p[2], sp.p[2],
                            f2.p[combo(0, 1)], f2.p[combo(1, 0)], divu, uin, fz, qf.p[2], &M);
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5 + K6 fused (the level and per-box paths).  For the final fluxes on the
+// F-faces, a block owns a column of kF23T0 x kF23T1 F-faces (transverse
+// directions t0 < t1) and marches along F.  For each cell layer c it
+// computes, into shared memory, the second-pass records that the final
+// fluxes read -- (t0|t1) on the layer's t0-faces and (t1|t0) on its t1-faces
+// (flux2_record: hydro_transdo halves + Riemann, Godunov_3D.cpp:218-380) --
+// then the final fluxes of the F-faces between layers c-1 and c (flux3:
+// hydro_transdd halves + Riemann + adjust_fluxes, :388-452).  Two layers of
+// records stay in shared memory; none goes to HBM.  A record on the edge of
+// a column is computed by both columns that read it (1/16 more records);
+// the F range is cut into segments that start one layer early.
+constexpr int kF23T0 = 16, kF23T1 = 16;
+constexpr int kF23Threads = kF23T0 * kF23T1;
+constexpr int kF23NA = (kF23T0 + 1) * kF23T1;  // (t0|t1) records of a layer
+constexpr int kF23NB = kF23T0 * (kF23T1 + 1);  // (t1|t0) records of a layer
+constexpr int kF23Smem = 2 * (kF23NA + kF23NB) * FR_N * int(sizeof(double));
+
+template <int F>
+__device__ __forceinline__ void flux23_column(const Space& s, const KGeom& g, const KParams& P,
+                                              const DtRef& dtr, const double* q,
+                                              const double* srcq, bool has_src, const Ptr3& sm,
+                                              const Ptr3& sp, const Ptr3& f1,
+                                              const double* divu, const DFab& uin,
+                                              const DFab& flx, double* qfF, int seg_len,
+                                              double* sh) {
+  constexpr int t0 = (F == 0) ? 1 : 0;
+  constexpr int t1 = (F == 2) ? 1 : 2;
+  const int nt0 = g.hi[t0] - g.lo[t0] + 1;
+  const int nt1 = g.hi[t1] - g.lo[t1] + 1;
+  const int ncol0 = (nt0 + kF23T0 - 1) / kF23T0;
+  const int ncol1 = (nt1 + kF23T1 - 1) / kF23T1;
+  if (int(blockIdx.x) >= ncol0 * ncol1) return;
+  const int p0base = g.lo[t0] + int(blockIdx.x % ncol0) * kF23T0;
+  const int p1base = g.lo[t1] + int(blockIdx.x / ncol0) * kF23T1;
+  const int f_begin = g.lo[F] + int(blockIdx.y) * seg_len;
+  if (f_begin > g.hi[F] + 1) return;
+  const int f_end = min(f_begin + seg_len - 1, g.hi[F] + 1);
+  const double* smT0 = sm.p[t0];
+  const double* spT0 = sp.p[t0];
+  const double* smT1 = sm.p[t1];
+  const double* spT1 = sp.p[t1];
+  const double* f1T0 = f1.p[t0];
+  const double* f1T1 = f1.p[t1];
+  for (int c = f_begin - 1; c <= f_end; ++c) {
+    const int L = (c - f_begin + 1) & 1;
+    double* A = sh + L * (kF23NA + kF23NB) * FR_N;
+    double* B = A + kF23NA * FR_N;
+    for (int r = threadIdx.x; r < kF23NA + kF23NB; r += kF23Threads) {
+      int idx[3];
+      idx[F] = c;
+      double rec[FR_N];
+      if (r < kF23NA) {
+        idx[t0] = p0base + r % (kF23T0 + 1);
+        idx[t1] = p1base + r / (kF23T0 + 1);
+        if (idx[t0] > g.hi[t0] + 1 || idx[t1] > g.hi[t1]) continue;
+        flux2_record<t0, t1>(idx[0], idx[1], idx[2], s, g, P, dtr, q, smT0, spT0, f1T1, rec);
+#pragma unroll
+        for (int n = 0; n < FR_N; ++n) A[n * kF23NA + r] = rec[n];
+      } else {
+        const int rb = r - kF23NA;
+        idx[t0] = p0base + rb % kF23T0;
+        idx[t1] = p1base + rb / kF23T0;
+        if (idx[t0] > g.hi[t0] || idx[t1] > g.hi[t1] + 1) continue;
+        flux2_record<t1, t0>(idx[0], idx[1], idx[2], s, g, P, dtr, q, smT1, spT1, f1T0, rec);
+#pragma unroll
+        for (int n = 0; n < FR_N; ++n) B[n * kF23NB + rb] = rec[n];
+      }
+    }
+    __syncthreads();
+    if (c >= f_begin) {
+      const int a0 = threadIdx.x % kF23T0, a1 = threadIdx.x / kF23T0;
+      int idx[3];
+      idx[F] = c;
+      idx[t0] = p0base + a0;
+      idx[t1] = p1base + a1;
+      if (idx[t0] <= g.hi[t0] && idx[t1] <= g.hi[t1]) {
+        const double* Am = sh + ((L ^ 1) * (kF23NA + kF23NB)) * FR_N;  // layer c - 1
+        const double* Bm = Am + kF23NA * FR_N;
+        const double* Ap = A;
+        const double* Bp = B;
+        const int ia = a1 * (kF23T0 + 1) + a0;  // t0-face low of the cell column
+        const int ib = a1 * kF23T0 + a0;        // t1-face low
+        const int i = idx[0], j = idx[1], k = idx[2];
+        const int64_t stF = (F == 0) ? 1 : (F == 1) ? s.sy : s.sz;
+        const int64_t at = s.idx(i, j, k);
+        const double dt = dtr.get();
+        const double hdt = 0.5 * dt;
+        const double cdtdx0 = 0.5 * dt / g.dx[t0];
+        const double cdtdx1 = 0.5 * dt / g.dx[t1];
+        double qm[ES_N], qp[ES_N], qn[ES_N], sq[ES_N];
+#pragma unroll
+        for (int n = 0; n < ES_N; ++n) sq[n] = 0.0;
+        {
+          double a0r[FR_N], a1r[FR_N], b0r[FR_N], b1r[FR_N];
+#pragma unroll
+          for (int n = 0; n < FR_N; ++n) {
+            a0r[n] = Am[n * kF23NA + ia];
+            a1r[n] = Am[n * kF23NA + ia + 1];
+            b0r[n] = Bm[n * kF23NB + ib];
+            b1r[n] = Bm[n * kF23NB + ib + kF23T0];
+          }
+          const TDTerms t = transdd_terms(a0r, a1r, b0r, b1r, P.gamma, cdtdx0, cdtdx1);
+          if (has_src) load_es(srcq, s, at - stF, sq);
+          load_es(sm.p[F], s, at, qn);
+          transdd_side(t, qn, sq, hdt, P, qm);
+        }
+        {
+          double a0r[FR_N], a1r[FR_N], b0r[FR_N], b1r[FR_N];
+#pragma unroll
+          for (int n = 0; n < FR_N; ++n) {
+            a0r[n] = Ap[n * kF23NA + ia];
+            a1r[n] = Ap[n * kF23NA + ia + 1];
+            b0r[n] = Bp[n * kF23NB + ib];
+            b1r[n] = Bp[n * kF23NB + ib + kF23T0];
+          }
+          const TDTerms t = transdd_terms(a0r, a1r, b0r, b1r, P.gamma, cdtdx0, cdtdx1);
+          if (has_src) load_es(srcq, s, at, sq);
+          load_es(sp.p[F], s, at, qn);
+          transdd_side(t, qn, sq, hdt, P, qp);
+        }
+        const CellAux aL = load_aux(q, s, at - stF, P.gamma);
+        const CellAux aR = load_aux(q, s, at, P.gamma);
+        const int fidx = (F == 0) ? i : (F == 1) ? j : k;
+        double f[NVAR], qpres, qun;
+        cmpflx<F>(qm, qp, aL, aR, fidx, g.bclo[F], g.bchi[F], g.dlo[F], g.dhi[F], P, f, qpres,
+                  qun);
+        face_adjust_and_store<F>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfF);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kF23Threads, 2) k_flux23(Space s, KGeom g, KParams P, DtRef dtr,
+                                                          const double* q, const double* srcq,
+                                                          bool has_src, Ptr3 sm, Ptr3 sp,
+                                                          Ptr3 f1, const double* divu, DFab uin,
+                                                          DFab fx, DFab fy, DFab fz, Ptr3 qf,
+                                                          int seg_len) {
+  extern __shared__ double sh[];
+  switch (blockIdx.z) {
+    case 0:
+      flux23_column<0>(s, g, P, dtr, q, srcq, has_src, sm, sp, f1, divu, uin, fx, qf.p[0],
+                       seg_len, sh);
+      break;
+    case 1:
+      flux23_column<1>(s, g, P, dtr, q, srcq, has_src, sm, sp, f1, divu, uin, fy, qf.p[1],
+                       seg_len, sh);
+      break;
+    default:
+      flux23_column<2>(s, g, P, dtr, q, srcq, has_src, sm, sp, f1, divu, uin, fz, qf.p[2],
+                       seg_len, sh);
       break;
   }
 }
@@ -927,6 +1101,36 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
                                                     w.sm[0], w.sm[1], w.sm[2], w.sp[0],
                                                     w.sp[1], w.sp[2], w.f1[0], w.f1[1],
                                                     w.f1[2]);
+    if (CAMR_FLUX23 && !L.M.on) {
+      // second and final passes fused: the records of the second pass live
+      // in shared memory only (k_flux23); caller metric arrays take the
+      // two-kernel path below
+      static bool attr_set = false;
+      if (!attr_set) {
+        cudaError_t ea = cudaFuncSetAttribute(k_flux23, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              kF23Smem);
+        if (ea != cudaSuccess) return ea;
+        attr_set = true;
+      }
+      int ncols = 0, nfaces = 0;
+      for (int F = 0; F < 3; ++F) {
+        const int t0 = (F == 0) ? 1 : 0, t1 = (F == 2) ? 1 : 2;
+        const int c0 = (g.hi[t0] - g.lo[t0] + kF23T0) / kF23T0;
+        const int c1 = (g.hi[t1] - g.lo[t1] + kF23T1) / kF23T1;
+        ncols = std::max(ncols, c0 * c1);
+        nfaces = std::max(nfaces, g.hi[F] - g.lo[F] + 2);
+      }
+      // segments of about 64 face layers (each recomputes one layer)
+      const int nseg = std::max(1, (nfaces + 32) / 64);
+      const int seg_len = (nfaces + nseg - 1) / nseg;
+      Ptr3 sm{{w.sm[0], w.sm[1], w.sm[2]}}, sp{{w.sp[0], w.sp[1], w.sp[2]}},
+          f1{{w.f1[0], w.f1[1], w.f1[2]}};
+      mark("flux23");
+      k_flux23<<<dim3(unsigned(ncols), unsigned(nseg), 3), kF23Threads, kF23Smem, st>>>(
+          s, g, L.P, L.dt, w.q, w.srcq, L.has_src, sm, sp, f1, w.divu, L.uin, L.flx[0],
+          L.flx[1], L.flx[2], qf, seg_len);
+      count_launch(3);
+    } else {
     // second pass "D|E": D-faces [lo,hi+1], F in grow 1, E in bx
     Reg6 r6;
     m = 0;
@@ -974,6 +1178,7 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
           rb[0], rb[1], rb[2], s, g, L.P, L.dt, w.q, w.srcq, L.has_src, sm, sp, f2, w.divu, L.uin,
           L.flx[0], L.flx[1], L.flx[2], qf, L.M);
     count_launch(4);
+    }
   } else {
     Region rs[3], rb[3];
     int64_t ms = 0, mb = 0;
