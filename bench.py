@@ -48,6 +48,10 @@ STAGE_BYTES = {
     "flux1": (688, "read 6 edge states x 9 + c,csml, write 3 flux records x 10"),
     "flux2": (1168, "read 6 x 9 states + 3 x 10 records, write 6 x 10 records"),
     "flux3": (1288, "read states, 6 x 10 records, divu, U; write 3 x 10 fluxes + 3 x 2"),
+    # the second and final passes fused (k_flux23): the 6 x 10 second-pass
+    # records stay in shared memory
+    "flux23": (1496, "read 6 x 9 edge states, 3 x 10 first-pass records, divu, U; "
+                     "write 3 x 10 fluxes + 3 x 2"),
     "update": (528, "read Sborder, U_old, 3 x 10 fluxes, 3 x 2; write U"),
 }
 # Whole-step algorithmic bytes per zone-update: CTU reads U^n and writes

@@ -500,6 +500,7 @@ cudaError_t fwd_step_tape(camr_adjoint* a, const double* dtp, unsigned long long
   H.dsdt = sdfab(nullptr);
   H.uin = sdfab(t.B);
   H.src = H.uin;
+  H.keep_slopes = true;  // the backward pass reads the forward slopes
   cudaError_t e = launch_hydro_fluxes(H, t.w1, st);
   if (e != cudaSuccess) return e;
   FluxPtrs fp1, fp2;

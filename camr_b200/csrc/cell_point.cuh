@@ -205,13 +205,12 @@ __device__ __forceinline__ void plm_edge_states(const double* q, int64_t at, int
   }}
 
 template <int d>
-__device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space& s,
-                                               const KParams& P, const double* q, double* o) {
-  const int64_t at = s.idx(i, j, k);
+__device__ __forceinline__ void mol_slope_compute(int64_t at, const Space& s, const KParams& P,
+                                                  const double* q, double* o) {
   const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
   if (P.plm_iorder == 1) {
 #pragma unroll
-    for (int n = 0; n < SL_N; ++n) o[at + n * s.sn] = 0.;
+    for (int n = 0; n < SL_N; ++n) o[n] = 0.;
     return;
   }
   const double plm_theta = 2.0;
@@ -222,28 +221,38 @@ __device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space&
   const double c = Q(0, SQ_C);
   double dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
   double drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
-  o[at + SL_0 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  o[SL_0] = mol_limiter(dlft, drgt, plm_theta);
   const double cs2 = c * c;
   dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
   drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
-  o[at + SL_2 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  o[SL_2] = mol_limiter(dlft, drgt, plm_theta);
   dlft = Q(0, t1) - Q(-1, t1);
   drgt = Q(1, t1) - Q(0, t1);
-  o[at + SL_3 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  o[SL_3] = mol_limiter(dlft, drgt, plm_theta);
   dlft = Q(0, t2) - Q(-1, t2);
   drgt = Q(1, t2) - Q(0, t2);
-  o[at + SL_4 * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  o[SL_4] = mol_limiter(dlft, drgt, plm_theta);
   const double enth = (Q(0, SQ_REINT) + Q(0, SQ_P)) / dmax(Q(0, SQ_RHO), P.small_dens);
   dlft = (Q(0, SQ_REINT) - Q(-1, SQ_REINT)) - enth * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
   drgt = (Q(1, SQ_REINT) - Q(0, SQ_REINT)) - enth * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
-  o[at + SL_RE * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+  o[SL_RE] = mol_limiter(dlft, drgt, plm_theta);
 #pragma unroll
   for (int sp = 0; sp < NSPEC; ++sp) {
     const int n = SQ_FS + sp;
     dlft = Q(0, SQ_RHO) * Q(0, n) - Q(-1, SQ_RHO) * Q(-1, n) - Q(0, n) * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
     drgt = Q(1, SQ_RHO) * Q(1, n) - Q(0, SQ_RHO) * Q(0, n) - Q(0, n) * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
-    o[at + (SL_FS + sp) * s.sn] = mol_limiter(dlft, drgt, plm_theta);
+    o[SL_FS + sp] = mol_limiter(dlft, drgt, plm_theta);
   }
+}
+
+template <int d>
+__device__ __forceinline__ void mol_slope_body(int i, int j, int k, const Space& s,
+                                               const KParams& P, const double* q, double* o) {
+  const int64_t at = s.idx(i, j, k);
+  double sl[SL_N];
+  mol_slope_compute<d>(at, s, P, q, sl);
+#pragma unroll
+  for (int n = 0; n < SL_N; ++n) o[at + n * s.sn] = sl[n];
 }
 
 // MOL face of direction d at (i,j,k) (between the cells at -e_d and 0): the
@@ -324,6 +333,114 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
   const CellAux aR = load_aux(q, s, at, P.gamma);
   const int idx = (d == 0) ? i : (d == 1) ? j : k;
   cmpflx<d>(ql, qr, aL, aR, idx, g.bclo[d], g.bchi[d], g.dlo[d], g.dhi[d], P, f, qpres, qun);
+}
+
+// The MOL edge states of one cell in direction d, from the cell's slopes
+// (the halves of mol_riemann_{x,y,z} that read this cell, MOL_riemann_K.H:
+// 12-167 and the y/z versions): qr, the state on the cell's low face (the
+// right state of that face), complete; and the pieces of the state on its
+// high face (the left state of the next face), whose species fall back to
+// the next cell's when their sum is below small_dens (the quirk of
+// MOL_riemann_K.H:82-86), so the face completes them.
+struct MolLeft {
+  double p, un, ut1, ut2, reint;
+  double spec[NSPEC];
+  double sum;
+  double c, csml;
+};
+
+template <int d>
+__device__ __forceinline__ void mol_cell_states(int64_t at, const Space& s, const KParams& P,
+                                                const double* q, const double* sl, double* qr,
+                                                MolLeft& l) {
+  auto Q = [&](int slot) { return ld_ro(q + at + slot * s.sn); };
+  constexpr int un = SQ_U + d;
+  constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
+  constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
+  const double cspeed = Q(SQ_C);
+  const double enth = (Q(SQ_REINT) + Q(SQ_P)) / dmax(Q(SQ_RHO), P.small_dens);
+  const double d0 = sl[SL_0], d2 = sl[SL_2];
+  {
+    // left state of the next face (this cell as atL)
+    const double pl = Q(SQ_P) + 0.5 * (d0 + d2) * cspeed;
+    l.p = dmax(pl, P.small_pres);
+    l.un = Q(un) + 0.5 * ((d2 - d0) / Q(SQ_RHO));
+    l.ut1 = Q(t1) + 0.5 * sl[SL_3];
+    l.ut2 = Q(t2) + 0.5 * sl[SL_4];
+    double sum = 0.;
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) {
+      const double specden =
+          Q(SQ_RHO) * Q(SQ_FS + sp) + 0.5 * (sl[SL_FS + sp] + Q(SQ_FS + sp) * (d0 + d2) / cspeed);
+      sum += specden;
+      l.spec[sp] = specden;
+    }
+    l.sum = sum;
+    l.reint = Q(SQ_REINT) + 0.5 * (sl[SL_RE] + enth * (d0 + d2) / cspeed);
+  }
+  {
+    // right state of this cell's low face (this cell as at)
+    const double pr = Q(SQ_P) - 0.5 * (d0 + d2) * cspeed;
+    qr[ES_P] = dmax(pr, P.small_pres);
+    qr[ES_U + d] = Q(un) - 0.5 * ((d2 - d0) / Q(SQ_RHO));
+    qr[ES_U + (t1 - SQ_U)] = Q(t1) - 0.5 * sl[SL_3];
+    qr[ES_U + (t2 - SQ_U)] = Q(t2) - 0.5 * sl[SL_4];
+    double sum = 0.;
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) {
+      const double specden =
+          Q(SQ_RHO) * Q(SQ_FS + sp) - 0.5 * (sl[SL_FS + sp] + Q(SQ_FS + sp) * (d0 + d2) / cspeed);
+      sum += specden;
+      qr[ES_FS + sp] = specden;
+    }
+    if (sum < P.small_dens) {
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = Q(SQ_FS + sp);
+    } else {
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = qr[ES_FS + sp] / sum;
+    }
+    qr[ES_RHO] = dmax(sum, P.small_dens);
+    qr[ES_REINT] = Q(SQ_REINT) - 0.5 * (sl[SL_RE] + enth * (d0 + d2) / cspeed);
+  }
+  l.c = cspeed;
+  l.csml = Q(SQ_CSML);
+}
+
+// The Riemann flux of the d-face at (i,j,k) from the left pieces of cell
+// (i,j,k) - e_d and the right state of cell (i,j,k) (hydro_cmpflx).
+template <int d>
+__device__ __forceinline__ void mol_face_from_states(int i, int j, int k, const Space& s,
+                                                     const KGeom& g, const KParams& P,
+                                                     const double* q, const MolLeft& l,
+                                                     const double* qr, const CellAux& aR,
+                                                     double* f, double& qpres, double& qun) {
+  const int64_t at = s.idx(i, j, k);
+  constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
+  constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
+  double ql[ES_N];
+  ql[ES_P] = l.p;
+  ql[ES_U + d] = l.un;
+  ql[ES_U + (t1 - SQ_U)] = l.ut1;
+  ql[ES_U + (t2 - SQ_U)] = l.ut2;
+  if (l.sum < P.small_dens) {
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = ld_ro(q + at + (SQ_FS + sp) * s.sn);
+  } else {
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = l.spec[sp] / l.sum;
+  }
+  ql[ES_RHO] = dmax(l.sum, P.small_dens);
+  ql[ES_REINT] = l.reint;
+  CellAux aL;
+  aL.c = l.c;
+  aL.csml = l.csml;
+  aL.gamc = P.gamma;
+  double qrr[ES_N];
+#pragma unroll
+  for (int n = 0; n < ES_N; ++n) qrr[n] = qr[n];
+  const int idx = (d == 0) ? i : (d == 1) ? j : k;
+  cmpflx<d>(ql, qrr, aL, aR, idx, g.bclo[d], g.bchi[d], g.dlo[d], g.dhi[d], P, f, qpres, qun);
 }
 
 }  // namespace camr

@@ -31,6 +31,11 @@ constexpr int kBlock = 128;
 #ifndef CAMR_MINB_FLUX3
 #define CAMR_MINB_FLUX3 4
 #endif
+// 1: the level and per-box MOL paths run slopes and faces as one pass per
+// direction (k_mol_fx / fy / fz)
+#ifndef CAMR_MOLFUSE
+#define CAMR_MOLFUSE 1
+#endif
 // 1: the level and per-box CTU paths run the second and final flux passes
 // as one kernel with the second-pass records in shared memory (k_flux23)
 #ifndef CAMR_FLUX23
@@ -596,7 +601,7 @@ constexpr int kF23T0 = 16, kF23T1 = 16;
 constexpr int kF23Threads = kF23T0 * kF23T1;
 constexpr int kF23NA = (kF23T0 + 1) * kF23T1;  // (t0|t1) records of a layer
 constexpr int kF23NB = kF23T0 * (kF23T1 + 1);  // (t1|t0) records of a layer
-constexpr int kF23Smem = 2 * (kF23NA + kF23NB) * FR_N * int(sizeof(double));
+constexpr int kF23SmemCol = 2 * (kF23NA + kF23NB) * FR_N * int(sizeof(double));
 
 template <int F>
 __device__ __forceinline__ void flux23_column(const Space& s, const KGeom& g, const KParams& P,
@@ -714,6 +719,113 @@ __device__ __forceinline__ void flux23_column(const Space& s, const KGeom& g, co
   }
 }
 
+// The x-faces (F = 0) with the same records, marching along z instead, so
+// that consecutive threads stay consecutive in x: a block owns kF23T0
+// x-faces x kF23T1 cells in y; per z-plane it computes the (1|2) records on
+// the plane's y-faces and the (2|1) records on the z-faces above the plane
+// (those below come from the previous plane), then the plane's x-faces.
+constexpr int kF23XA = (kF23T0 + 1) * (kF23T1 + 1);  // (1|2) records of a plane
+constexpr int kF23XB = (kF23T0 + 1) * kF23T1;        // (2|1) records of a z-face layer
+constexpr int kF23SmemX = (kF23XA + 2 * kF23XB) * FR_N * int(sizeof(double));
+constexpr int kF23Smem = (kF23SmemCol > kF23SmemX) ? kF23SmemCol : kF23SmemX;
+
+__device__ __forceinline__ void flux23_x(const Space& s, const KGeom& g, const KParams& P,
+                                         const DtRef& dtr, const double* q, const double* srcq,
+                                         bool has_src, const Ptr3& sm, const Ptr3& sp,
+                                         const Ptr3& f1, const double* divu, const DFab& uin,
+                                         const DFab& flx, double* qf0, int seg_len, double* sh) {
+  const int nfx = g.hi[0] - g.lo[0] + 2;  // x-faces
+  const int ncx = (nfx + kF23T0 - 1) / kF23T0;
+  const int ncy = (g.hi[1] - g.lo[1] + kF23T1) / kF23T1;
+  if (int(blockIdx.x) >= ncx * ncy) return;
+  const int i0 = g.lo[0] + int(blockIdx.x % ncx) * kF23T0;  // first x-face of the tile
+  const int j0 = g.lo[1] + int(blockIdx.x / ncx) * kF23T1;
+  const int k_begin = g.lo[2] + int(blockIdx.y) * seg_len;
+  if (k_begin > g.hi[2]) return;
+  const int k_end = min(k_begin + seg_len - 1, g.hi[2]);
+  double* A = sh;                      // (1|2) on y-faces of the plane
+  double* Bl[2] = {A + kF23XA * FR_N, A + kF23XA * FR_N + kF23XB * FR_N};
+  // (2|1) records on the z-faces at k (layer (k - k_begin) & 1) and k + 1
+  auto fill_b = [&](int kz, double* Bz) {
+    for (int r = threadIdx.x; r < kF23XB; r += kF23Threads) {
+      const int ci = i0 - 1 + r % (kF23T0 + 1);
+      const int cj = j0 + r / (kF23T0 + 1);
+      if (ci > g.hi[0] + 1 || cj > g.hi[1]) continue;
+      double rec[FR_N];
+      flux2_record<2, 1>(ci, cj, kz, s, g, P, dtr, q, sm.p[2], sp.p[2], f1.p[1], rec);
+#pragma unroll
+      for (int n = 0; n < FR_N; ++n) Bz[n * kF23XB + r] = rec[n];
+    }
+  };
+  fill_b(k_begin, Bl[0]);
+  for (int k = k_begin; k <= k_end; ++k) {
+    const int L = (k - k_begin) & 1;
+    double* Blo = Bl[L];
+    double* Bhi = Bl[L ^ 1];
+    for (int r = threadIdx.x; r < kF23XA + kF23XB; r += kF23Threads) {
+      double rec[FR_N];
+      if (r < kF23XA) {
+        const int ci = i0 - 1 + r % (kF23T0 + 1);
+        const int fj = j0 + r / (kF23T0 + 1);
+        if (ci > g.hi[0] + 1 || fj > g.hi[1] + 1) continue;
+        flux2_record<1, 2>(ci, fj, k, s, g, P, dtr, q, sm.p[1], sp.p[1], f1.p[2], rec);
+#pragma unroll
+        for (int n = 0; n < FR_N; ++n) A[n * kF23XA + r] = rec[n];
+      } else {
+        const int rb = r - kF23XA;
+        const int ci = i0 - 1 + rb % (kF23T0 + 1);
+        const int cj = j0 + rb / (kF23T0 + 1);
+        if (ci > g.hi[0] + 1 || cj > g.hi[1]) continue;
+        flux2_record<2, 1>(ci, cj, k + 1, s, g, P, dtr, q, sm.p[2], sp.p[2], f1.p[1], rec);
+#pragma unroll
+        for (int n = 0; n < FR_N; ++n) Bhi[n * kF23XB + rb] = rec[n];
+      }
+    }
+    __syncthreads();
+    const int a0 = threadIdx.x % kF23T0, a1 = threadIdx.x / kF23T0;
+    const int i = i0 + a0, j = j0 + a1;
+    if (i <= g.hi[0] + 1 && j <= g.hi[1]) {
+      // records of the cells i-1 (tile x-cell a0) and i (a0 + 1)
+      const int64_t at = s.idx(i, j, k);
+      const double dt = dtr.get();
+      const double hdt = 0.5 * dt;
+      const double cdtdx0 = 0.5 * dt / g.dx[1];
+      const double cdtdx1 = 0.5 * dt / g.dx[2];
+      double qm[ES_N], qp[ES_N], qn[ES_N], sq[ES_N];
+#pragma unroll
+      for (int n = 0; n < ES_N; ++n) sq[n] = 0.0;
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int xi = a0 + side;
+        double a0r[FR_N], a1r[FR_N], b0r[FR_N], b1r[FR_N];
+#pragma unroll
+        for (int n = 0; n < FR_N; ++n) {
+          a0r[n] = A[n * kF23XA + a1 * (kF23T0 + 1) + xi];
+          a1r[n] = A[n * kF23XA + (a1 + 1) * (kF23T0 + 1) + xi];
+          b0r[n] = Blo[n * kF23XB + a1 * (kF23T0 + 1) + xi];
+          b1r[n] = Bhi[n * kF23XB + a1 * (kF23T0 + 1) + xi];
+        }
+        const TDTerms t = transdd_terms(a0r, a1r, b0r, b1r, P.gamma, cdtdx0, cdtdx1);
+        if (side == 0) {
+          if (has_src) load_es(srcq, s, at - 1, sq);
+          load_es(sm.p[0], s, at, qn);
+          transdd_side(t, qn, sq, hdt, P, qm);
+        } else {
+          if (has_src) load_es(srcq, s, at, sq);
+          load_es(sp.p[0], s, at, qn);
+          transdd_side(t, qn, sq, hdt, P, qp);
+        }
+      }
+      const CellAux aL = load_aux(q, s, at - 1, P.gamma);
+      const CellAux aR = load_aux(q, s, at, P.gamma);
+      double f[NVAR], qpres, qun;
+      cmpflx<0>(qm, qp, aL, aR, i, g.bclo[0], g.bchi[0], g.dlo[0], g.dhi[0], P, f, qpres, qun);
+      face_adjust_and_store<0>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qf0);
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(kF23Threads, 2) k_flux23(Space s, KGeom g, KParams P, DtRef dtr,
                                                           const double* q, const double* srcq,
                                                           bool has_src, Ptr3 sm, Ptr3 sp,
@@ -723,8 +835,7 @@ __global__ void __launch_bounds__(kF23Threads, 2) k_flux23(Space s, KGeom g, KPa
   extern __shared__ double sh[];
   switch (blockIdx.z) {
     case 0:
-      flux23_column<0>(s, g, P, dtr, q, srcq, has_src, sm, sp, f1, divu, uin, fx, qf.p[0],
-                       seg_len, sh);
+      flux23_x(s, g, P, dtr, q, srcq, has_src, sm, sp, f1, divu, uin, fx, qf.p[0], seg_len, sh);
       break;
     case 1:
       flux23_column<1>(s, g, P, dtr, q, srcq, has_src, sm, sp, f1, divu, uin, fy, qf.p[1],
@@ -790,6 +901,97 @@ __global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLFLUX) k_mol_flux(Region r
         mol_flux_body<2, MET>(i, j, k, s, g, P, q, slope.p[2], divu, uin, fz, qf.p[2], &M);
       break;
   }
+}
+
+// ---------------------------------------------------------------------------
+// MOL slopes and face pass fused (the level and per-box paths): a cell's
+// slopes (mol_slope_compute) become its two edge states at once
+// (mol_cell_states) and the face between two cells takes the left pieces of
+// one and the right state of the other (mol_face_from_states); the slopes
+// never go to HBM.  x-faces: a block covers kMolRow consecutive cells of an
+// x-row and passes the left pieces to the next thread through shared
+// memory.  y- and z-faces: each thread walks a column of cells along the
+// face direction and carries the previous cell's left pieces in registers
+// (segments of about 64 cells, each starting one cell early).
+constexpr int kMolRow = 128;
+
+__global__ void __launch_bounds__(kMolRow) k_mol_fx(Space s, KGeom g, KParams P, const double* q,
+                                                    const double* divu, DFab uin, DFab fx,
+                                                    double* qf0) {
+  __shared__ MolLeft left[kMolRow];
+  constexpr int per = kMolRow - 1;
+  const int i = g.lo[0] + int(blockIdx.x) * per - 1 + int(threadIdx.x);
+  const int j = g.lo[1] + int(blockIdx.y);
+  const int k = g.lo[2] + int(blockIdx.z);
+  const bool have = i <= g.hi[0] + 1;
+  double qr[ES_N];
+  MolLeft l;
+  if (have) {
+    const int64_t at = s.idx(i, j, k);
+    double sl[SL_N];
+    mol_slope_compute<0>(at, s, P, q, sl);
+    mol_cell_states<0>(at, s, P, q, sl, qr, l);
+    left[threadIdx.x] = l;
+  }
+  __syncthreads();
+  if (have && threadIdx.x > 0) {
+    CellAux aR;
+    aR.c = l.c;
+    aR.csml = l.csml;
+    aR.gamc = P.gamma;
+    double f[NVAR], qpres, qun;
+    mol_face_from_states<0>(i, j, k, s, g, P, q, left[threadIdx.x - 1], qr, aR, f, qpres, qun);
+    face_adjust_and_store<0>(f, qpres, qun, i, j, k, s, g, P, uin, divu, fx, qf0);
+  }
+}
+
+template <int d>
+__device__ __forceinline__ void mol_column(const Space& s, const KGeom& g, const KParams& P,
+                                           const double* q, const double* divu,
+                                           const DFab& uin, const DFab& flx, double* qfd,
+                                           int seg) {
+  constexpr int T = (d == 1) ? 2 : 1;  // the transverse direction besides x
+  const int i = g.lo[0] + int(blockIdx.x) * kMolRow + int(threadIdx.x);
+  if (i > g.hi[0]) return;
+  const int t = g.lo[T] + int(blockIdx.y);
+  const int f_begin = g.lo[d] + int(blockIdx.z) * seg;
+  if (f_begin > g.hi[d] + 1) return;
+  const int f_end = min(f_begin + seg - 1, g.hi[d] + 1);
+  MolLeft prev;
+  for (int c = f_begin - 1; c <= f_end; ++c) {
+    int idx[3];
+    idx[0] = i;
+    idx[T] = t;
+    idx[d] = c;
+    const int64_t at = s.idx(idx[0], idx[1], idx[2]);
+    double sl[SL_N], qr[ES_N];
+    MolLeft l;
+    mol_slope_compute<d>(at, s, P, q, sl);
+    mol_cell_states<d>(at, s, P, q, sl, qr, l);
+    if (c >= f_begin) {
+      CellAux aR;
+      aR.c = l.c;
+      aR.csml = l.csml;
+      aR.gamc = P.gamma;
+      double f[NVAR], qpres, qun;
+      mol_face_from_states<d>(idx[0], idx[1], idx[2], s, g, P, q, prev, qr, aR, f, qpres, qun);
+      face_adjust_and_store<d>(f, qpres, qun, idx[0], idx[1], idx[2], s, g, P, uin, divu, flx,
+                               qfd);
+    }
+    prev = l;
+  }
+}
+
+__global__ void __launch_bounds__(kMolRow) k_mol_fy(Space s, KGeom g, KParams P, const double* q,
+                                                    const double* divu, DFab uin, DFab fy,
+                                                    double* qf1, int seg) {
+  mol_column<1>(s, g, P, q, divu, uin, fy, qf1, seg);
+}
+
+__global__ void __launch_bounds__(kMolRow) k_mol_fz(Space s, KGeom g, KParams P, const double* q,
+                                                    const double* divu, DFab uin, DFab fz,
+                                                    double* qf2, int seg) {
+  mol_column<2>(s, g, P, q, divu, uin, fz, qf2, seg);
 }
 
 // ---------------------------------------------------------------------------
@@ -1113,13 +1315,17 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
         attr_set = true;
       }
       int ncols = 0, nfaces = 0;
-      for (int F = 0; F < 3; ++F) {
-        const int t0 = (F == 0) ? 1 : 0, t1 = (F == 2) ? 1 : 2;
+      for (int F = 1; F < 3; ++F) {
+        const int t0 = 0, t1 = (F == 2) ? 1 : 2;
         const int c0 = (g.hi[t0] - g.lo[t0] + kF23T0) / kF23T0;
         const int c1 = (g.hi[t1] - g.lo[t1] + kF23T1) / kF23T1;
         ncols = std::max(ncols, c0 * c1);
         nfaces = std::max(nfaces, g.hi[F] - g.lo[F] + 2);
       }
+      // the x-faces march along z over cell planes
+      ncols = std::max(ncols, ((g.hi[0] - g.lo[0] + 2 + kF23T0 - 1) / kF23T0) *
+                                  ((g.hi[1] - g.lo[1] + kF23T1) / kF23T1));
+      nfaces = std::max(nfaces, g.hi[2] - g.lo[2] + 1);
       // segments of about 64 face layers (each recomputes one layer)
       const int nseg = std::max(1, (nfaces + 32) / 64);
       const int seg_len = (nfaces + nseg - 1) / nseg;
@@ -1195,6 +1401,23 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       rb[d] = make_region(flo, fhi);
       ms = (rs[d].count() > ms) ? rs[d].count() : ms;
       mb = (rb[d].count() > mb) ? rb[d].count() : mb;
+    }
+    if (CAMR_MOLFUSE && !L.M.on && !L.keep_slopes) {
+      // slopes, edge states and faces fused (k_mol_fx / fy / fz)
+      const int nb[3] = {g.hi[0] - g.lo[0] + 1, g.hi[1] - g.lo[1] + 1, g.hi[2] - g.lo[2] + 1};
+      mark("mol_faces");
+      k_mol_fx<<<dim3(unsigned((nb[0] + 1 + kMolRow - 2) / (kMolRow - 1)), unsigned(nb[1]),
+                      unsigned(nb[2])),
+                 kMolRow, 0, st>>>(s, g, L.P, w.q, w.divu, L.uin, L.flx[0], qf.p[0]);
+      const int segy = std::max(1, (nb[1] + 1 + 32) / 64), segz = std::max(1, (nb[2] + 1 + 32) / 64);
+      const int leny = (nb[1] + 1 + segy - 1) / segy, lenz = (nb[2] + 1 + segz - 1) / segz;
+      const unsigned gx = unsigned((nb[0] + kMolRow - 1) / kMolRow);
+      k_mol_fy<<<dim3(gx, unsigned(nb[2]), unsigned(segy)), kMolRow, 0, st>>>(
+          s, g, L.P, w.q, w.divu, L.uin, L.flx[1], qf.p[1], leny);
+      k_mol_fz<<<dim3(gx, unsigned(nb[1]), unsigned(segz)), kMolRow, 0, st>>>(
+          s, g, L.P, w.q, w.divu, L.uin, L.flx[2], qf.p[2], lenz);
+      count_launch(3);
+      return cudaGetLastError();
     }
     Ptr3 sl{{w.slope[0], w.slope[1], w.slope[2]}};
     mark("mol_slope");

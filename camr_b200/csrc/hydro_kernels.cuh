@@ -92,6 +92,9 @@ struct HydroLaunch {
   bool ext_srcq = false;
   DFab qin, qauxin, srcqin;
   Metrics M;
+  // MOL: keep the slopes in Work::slope (the adjoint's tape reads them);
+  // otherwise slopes and faces run fused and the slope arrays stay unused
+  bool keep_slopes = false;
 };
 
 // ---- batched (work-list) launches over many boxes of one level ----
