@@ -570,8 +570,8 @@ def amr_comparison(args, steps=None, per_box_steps=2, warmup=3):
     from camr_b200 import hydro, native, problems
     if steps is None:
         steps = args.amr_steps
-    n0 = (256, 256, 256)
-    fine_n = 512
+    n0 = (args.amr_n0,) * 3
+    fine_n = 2 * args.amr_n0
     boxes = problems.amr_box_list(nbox=args.nbox, fine_n=fine_n)
     S0, S1 = problems.amr_initial(n0, boxes, vel=None)
     geom = hydro.make_geom(n0)
@@ -947,6 +947,8 @@ def main():
                     help="finite-difference cells of the c3-adjoint workload")
     ap.add_argument("--nbox", type=int, default=350)
     ap.add_argument("--amr-steps", type=int, default=4, help="timed coarse steps of c2-amr")
+    ap.add_argument("--amr-n0", type=int, default=256,
+                    help="base level size of c2-amr (fine index space twice that)")
     ap.add_argument("--eb-steps", type=int, default=150, help="timed steps of c4-eb")
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed region (C1 steps; c2-amr MOL batched steps; "

@@ -32,14 +32,21 @@ constexpr int kBlock = 128;
 #define CAMR_MINB_FLUX3 4
 #endif
 // 1: the level and per-box MOL paths run slopes and faces as one pass per
-// direction (k_mol_fx / fy / fz)
+// direction (k_mol_fx / fy / fz).  Measured on B200 (256^3 MOL-PLM level):
+// 22.5 ms for the fused faces against 6.5 + 13.6 ms for slopes + faces, so
+// the default keeps the two kernels: the column walks of the y- and z-faces
+// give each thread a long serial chain and fewer threads to hide it.
 #ifndef CAMR_MOLFUSE
-#define CAMR_MOLFUSE 1
+#define CAMR_MOLFUSE 0
 #endif
 // 1: the level and per-box CTU paths run the second and final flux passes
-// as one kernel with the second-pass records in shared memory (k_flux23)
+// as one kernel with the second-pass records in shared memory (k_flux23).
+// Measured on B200 (256^3 CTU-PPM): 22.2 ms against 9.7 + 6.1 ms for the
+// two kernels (two blocks of 8 warps per SM, a barrier per layer and a
+// third, one-warp round of record work per layer), so the default keeps
+// the two kernels and their records in HBM.
 #ifndef CAMR_FLUX23
-#define CAMR_FLUX23 1
+#define CAMR_FLUX23 0
 #endif
 
 inline unsigned grid_for(int64_t n) { return unsigned((n + kBlock - 1) / kBlock); }
