@@ -575,7 +575,11 @@ def amr_comparison(args, steps=None, per_box_steps=2, warmup=3):
     boxes = problems.amr_box_list(nbox=args.nbox, fine_n=fine_n)
     S0, S1 = problems.amr_initial(n0, boxes, vel=None)
     geom = hydro.make_geom(n0)
-    out = {"base": list(n0), "boxes": len(boxes)}
+    out = {"base": list(n0), "boxes": len(boxes),
+           "parity": "hydro: the reference's kernels bit for bit; the coarse-fine coupling "
+                     "(FillPatch interpolation, flux register, average down) equals the "
+                     "restated AMReX algorithms of the oracle bit for bit; AMReX itself is "
+                     "absent, so that coupling is unpinned against AMReX"}
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     methods = (("mol_plm", dict(do_mol=1, ppm_type=0, cfl=0.3), True),
@@ -663,7 +667,10 @@ def eb_comparison(args, n=(256, 128, 128), nsteps=None, warmup=3, cpu_n=(64, 32,
     out = {"domain": list(n), "cells": zones, "cut_cells": int((typ == 1).sum()),
            "covered_cells": int((typ == 3).sum()), "boxes_32": boxes,
            "geometry_build_s": geo_s, "method": "MOL-PLM RK2, two-shock Riemann, FluxRedist",
-           "cfl": 0.3, "steps": nsteps}
+           "cfl": 0.3, "steps": nsteps,
+           "parity": "EB hydro: the reference's EB kernels bit for bit; flux and state "
+                     "redistribution and the sphere geometry are restated (AMReX absent: "
+                     "unpinned against AMReX)"}
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     # 32^3 boxes (the configuration): regular boxes through the batched
