@@ -680,6 +680,7 @@ struct camr_amr {
   double *staging0 = nullptr, *staging1 = nullptr;
   int fine_mode = CAMR_BATCH_PERSISTENT;
   int steps_taken = 0;
+  bool restart_est = false;  // next step: CFL estimate of the restored state, then computeNewDt
   bool graph_ready = false;
   cudaGraphExec_t graph;
   int64_t kernels_per_step = 0;
@@ -727,7 +728,7 @@ namespace {
 
 inline unsigned blocks_of(int64_t n) { return unsigned((n + kBlk - 1) / kBlk); }
 
-cudaError_t amr_issue_step(camr_amr* a, bool first) {
+cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   cudaStream_t st = a->stream;
   const LGeom& Lc = a->Lc;
   const FineDev F = a->fine();
@@ -746,7 +747,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first) {
   const double* dt1 = &a->clock->dt1;
   DtCtl c{a->hp.cfl, a->hp.max_dt, a->hp.fixed_dt, a->hp.initial_dt, a->hp.init_shrink,
           a->hp.change_max};
-  if (first) {
+  if (first || est) {
     k_reset_bits2<<<1, 1, 0, st>>>(a->bits0, a->bits1);
     k_est_dt<<<gv0, kBlk, 0, st>>>(Lc, P, a->S0, a->bits0);
     kf_est_dt<<<gf_valid, kBlk, 0, st>>>(F, P, a->S1, a->bits1);
@@ -1182,6 +1183,7 @@ camr_status camr_amr_set_state(camr_amr* a, const double* S0, const double* S1, 
   count_launch(2);
   e = cudaMemsetAsync(a->clock, 0, sizeof(AmrClock), a->stream);
   a->steps_taken = 0;
+  a->restart_est = false;
   if (e != cudaSuccess) return CAMR_ERR_CUDA;
   return cuda_status_of(cudaGetLastError());
 }
@@ -1216,7 +1218,10 @@ camr_status camr_amr_advance(camr_amr* a, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     const bool first = a->steps_taken == 0;
     cudaError_t e;
-    if (!first && a->desc.use_graph && a->fine_mode == CAMR_BATCH_PERSISTENT) {
+    if (a->restart_est) {
+      a->restart_est = false;
+      e = amr_issue_step(a, false, true);
+    } else if (!first && a->desc.use_graph && a->fine_mode == CAMR_BATCH_PERSISTENT) {
       if (!a->graph_ready) {
         cudaGraph_t gr;
         e = cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal);
@@ -1241,6 +1246,25 @@ camr_status camr_amr_advance(camr_amr* a, int nsteps) {
     if (e != cudaSuccess) return cuda_status_of(e);
     a->steps_taken++;
   }
+  return CAMR_OK;
+}
+
+camr_status camr_amr_restart(camr_amr* a, const double clock[4], int steps_done) {
+  if (!a || !clock || steps_done < 1 || !(clock[2] > 0.0) || !(clock[3] > 0.0))
+    return CAMR_ERR_INVALID;
+  AmrClock h;
+  cudaError_t e = cudaMemcpyAsync(&h, a->clock, sizeof(h), cudaMemcpyDeviceToHost, a->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  h.tc_new = clock[0];
+  h.tf_new = clock[1];
+  h.dt0 = clock[2];
+  h.dt1 = clock[3];
+  e = cudaMemcpyAsync(a->clock, &h, sizeof(h), cudaMemcpyHostToDevice, a->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  a->steps_taken = steps_done;
+  a->restart_est = true;
   return CAMR_OK;
 }
 

@@ -563,6 +563,12 @@ class AmrHierarchy:
         check(lib().camr_amr_clock(self._h, c), "camr_amr_clock")
         return list(c)
 
+    def restart(self, clock, steps_done):
+        """Continue from a checkpoint's states (set_state first): clock =
+        (t0, t1, dt0, dt1) as clock() returns it."""
+        c = (C.c_double * 4)(*clock)
+        check(lib().camr_amr_restart(self._h, C.byref(c), int(steps_done)), "amr restart")
+
     def autotune(self):
         check(lib().camr_amr_autotune(self._h), "camr_amr_autotune")
 

@@ -412,6 +412,13 @@ camr_status camr_amr_advance(camr_amr* a, int nsteps);
  * dt of level 1 (synchronises). */
 camr_status camr_amr_clock(camr_amr* a, double clock[4]);
 
+/* Restart after camr_amr_set_state with a checkpoint's states: clock as
+ * camr_amr_clock returns it (times and last dts of both levels) and the
+ * coarse steps done.  The next coarse step estimates the CFL dt of both
+ * levels from the restored states and applies computeNewDt against the
+ * checkpoint's dts, as an uninterrupted run would (synchronises). */
+camr_status camr_amr_restart(camr_amr* a, const double clock[4], int steps_done);
+
 /* Autotune the fine level's batched hydro on its current state (after at
  * least one step); synchronises. */
 camr_status camr_amr_autotune(camr_amr* a);

@@ -395,3 +395,42 @@ def test_level_checkpoint_restart_continues_exactly(tmp_path):
     assert b.last_dt() == want_dt
     assert np.array_equal(b.get_state(), want)
     b.close()
+
+
+@pytest.mark.gpu
+def test_amr_checkpoint_restart_continues_exactly(tmp_path):
+    """Two-level checkpoint after 3 coarse steps, restart into a new
+    hierarchy with camr_amr_restart: the next coarse steps (CFL estimates
+    of the restored states, computeNewDt against the checkpoint's dts) give
+    the same states and clock as the run that never stopped."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    n0 = (16, 16, 16)
+    boxes = [((8, 8, 8), (23, 15, 15)), ((0, 16, 16), (7, 31, 23))]
+    S0, S1 = P.amr_initial(n0, boxes, nblobs=3, r_min=0.1, r_max=0.2)
+    geom = hydro.make_geom(n0)
+    prm = native.default_params(ppm_type=1, cfl=0.5)
+    a = hydro.AmrHierarchy(geom, prm, boxes)
+    a.set_state(S0, S1)
+    a.init_finalize()
+    a.advance(3)
+    c0, c1 = a.get_state()
+    t0, t1, d0, d1 = a.clock()
+    hydro.write_checkpoint(tmp_path / "chk3", geom, (1, 1, 1), c0, (t0, t1), (d0, d1), (3, 6),
+                           S1=c1, fine_boxes=boxes)
+    a.advance(2)
+    want0, want1 = a.get_state()
+    want_clock = a.clock()
+    a.close()
+    b0, b1, tt, dd, ss = hydro.read_checkpoint(tmp_path / "chk3", geom, boxes)
+    assert tt == (t0, t1) and dd == (d0, d1) and ss == (3, 6)
+    b = hydro.AmrHierarchy(geom, prm, boxes)
+    b.set_state(b0, b1)
+    b.restart((tt[0], tt[1], dd[0], dd[1]), ss[0])
+    b.advance(2)
+    got0, got1 = b.get_state()
+    assert b.clock() == want_clock
+    assert np.array_equal(got0, want0)
+    assert np.array_equal(np.asarray(got1).ravel(), np.asarray(want1).ravel())
+    b.close()
