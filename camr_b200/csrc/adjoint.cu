@@ -632,7 +632,7 @@ cudaError_t adj_step(camr_adjoint* a, const double* dtp, const StepTape& t) {
 // free device memory.
 bool alloc_tapes(camr_adjoint* a) {
   if (a->tapes_ok) return true;
-  const size_t wb = work_doubles(a->G.sp, true, false) * sizeof(double);
+  const size_t wb = work_doubles(a->G.sp, true, false, false) * sizeof(double);
   const size_t per = 6 * a->sbytes + 2 * wb;
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
@@ -655,8 +655,8 @@ bool alloc_tapes(camr_adjoint* a) {
     t.B2 = take(a->sbytes);
     t.Spre = take(a->sbytes);
     t.w1.s = t.w2.s = a->G.sp;
-    work_carve(t.w1, take(wb), true, false);
-    work_carve(t.w2, take(wb), true, false);
+    work_carve(t.w1, take(wb), true, false, false);
+    work_carve(t.w2, take(wb), true, false, false);
     a->tapes.push_back(t);
   }
   a->tapes_ok = true;
@@ -729,7 +729,7 @@ camr_status camr_adjoint_create(const camr_geom* geom, const camr_hydro_params* 
                       &a->flx[2], &a->Lam, &a->LB, &a->LB2, &a->LSold, &a->LStar, &a->Ldsdt,
                       &a->Spre})
     alloc(pp, a->sbytes);
-  const size_t wb = work_doubles(a->G.sp, true, false) * sizeof(double);
+  const size_t wb = work_doubles(a->G.sp, true, false, false) * sizeof(double);
   alloc(&a->work1, wb);
   alloc(&a->work2, wb);
   alloc(&a->Lq, size_t(L.sn) * (NQ + 3 * NS + 1) * sizeof(double));
@@ -748,8 +748,8 @@ camr_status camr_adjoint_create(const camr_geom* geom, const camr_hydro_params* 
   a->Lsl = a->Lq + size_t(L.sn) * NQ;
   a->Ldivu = a->Lsl + size_t(L.sn) * 3 * NS;
   a->w1.s = a->w2.s = a->G.sp;
-  work_carve(a->w1, a->work1, true, false);
-  work_carve(a->w2, a->work2, true, false);
+  work_carve(a->w1, a->work1, true, false, false);
+  work_carve(a->w2, a->work2, true, false, false);
   *out = a;
   return CAMR_OK;
 }

@@ -39,6 +39,28 @@ constexpr int kBlock = 128;
 #ifndef CAMR_MOLFUSE
 #define CAMR_MOLFUSE 0
 #endif
+// 1: the MOL right-hand side runs as a cell pass and a face pass
+// (k_mol_states + k_mol_face): each (cell, dir) turns its slopes into its
+// two edge states at once, so the face pass reads two 9-slot records
+// instead of both cells' primitive states and slopes.  0 (the default):
+// slopes into HBM (k_mol_slope), then edge states + Riemann per face
+// (k_mol_flux).  Measured on B200 (256^3 MOL-PLM level, ms per step):
+// states 13.3 + faces 7.0 against slopes 6.5 + faces 13.6, so the edge-state
+// arithmetic costs the same wherever it runs; batched two-level MOL step
+// 129.7 ms (112.0 with 5 / 4 blocks per SM for the two batched stages)
+// against 111.7, EB level 11.6 against 9.7 ms.  Bit-exact either way (the
+// whole GPU suite passed with it on).  A workspace carved without the
+// edge-state arrays (the adjoint's slope tape, the allocation-free entry
+// point) always takes the slope path.
+#ifndef CAMR_MOLSPLIT
+#define CAMR_MOLSPLIT 0
+#endif
+#ifndef CAMR_MINB_MOLSTATES
+#define CAMR_MINB_MOLSTATES 1
+#endif
+#ifndef CAMR_MINB_MOLFACE
+#define CAMR_MINB_MOLFACE 1
+#endif
 // 1: the level and per-box CTU paths run the second and final flux passes
 // as one kernel with the second-pass records in shared memory (k_flux23).
 // Measured on B200 (256^3 CTU-PPM): 22.2 ms against 9.7 + 6.1 ms for the
@@ -911,6 +933,114 @@ __global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLFLUX) k_mol_flux(Region r
 }
 
 // ---------------------------------------------------------------------------
+// MOL as a cell pass and a face pass.  The cell pass stores, per direction
+// d, the right state of the cell's low d-face (ES_* slots, complete) in
+// rst[d] and the pieces of the left state of its high d-face (ML_* slots:
+// the species stay unnormalised with their sum, because when the sum is
+// below small_dens the reference takes the species of the cell on the
+// other side, MOL_riemann_K.H:82-86) in lpc[d].  The face pass completes
+// the left state, runs hydro_cmpflx and adjust_fluxes.  The operations and
+// their order are those of mol_edges_cmpflx (mol_slope_compute,
+// mol_cell_states, mol_face_from_states).
+enum { ML_P = 0, ML_UN, ML_UT1, ML_UT2, ML_REINT, ML_FS, ML_SUM = ML_FS + NSPEC, ML_N };
+static_assert(int(ML_N) <= int(ES_N), "left pieces fit an edge-state array");
+
+template <int d>
+__device__ __forceinline__ void mol_states_body(int i, int j, int k, const Space& s,
+                                                const KParams& P, const double* q, double* lpc,
+                                                double* rst) {
+  const int64_t at = s.idx(i, j, k);
+  const int64_t sn = s.sn;
+  double sl[SL_N], qr[ES_N];
+  MolLeft l;
+  mol_slope_compute<d>(at, s, P, q, sl);
+  mol_cell_states<d>(at, s, P, q, sl, qr, l);
+  store_es(rst, s, at, qr);
+  lpc[at + ML_P * sn] = l.p;
+  lpc[at + ML_UN * sn] = l.un;
+  lpc[at + ML_UT1 * sn] = l.ut1;
+  lpc[at + ML_UT2 * sn] = l.ut2;
+  lpc[at + ML_REINT * sn] = l.reint;
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) lpc[at + (ML_FS + sp) * sn] = l.spec[sp];
+  lpc[at + ML_SUM * sn] = l.sum;
+}
+
+template <int d, bool MET = false>
+__device__ __forceinline__ void mol_face_body(int i, int j, int k, const Space& s,
+                                              const KGeom& g, const KParams& P,
+                                              const double* q, const double* lpc,
+                                              const double* rst, const double* divu,
+                                              const DFab& uin, DFab flx, double* qfd,
+                                              const Metrics* M = nullptr) {
+  const int64_t st = (d == 0) ? 1 : (d == 1) ? s.sy : s.sz;
+  const int64_t at = s.idx(i, j, k);
+  const int64_t atL = at - st;
+  const int64_t sn = s.sn;
+  MolLeft l;
+  l.p = ld_ro(lpc + atL + ML_P * sn);
+  l.un = ld_ro(lpc + atL + ML_UN * sn);
+  l.ut1 = ld_ro(lpc + atL + ML_UT1 * sn);
+  l.ut2 = ld_ro(lpc + atL + ML_UT2 * sn);
+  l.reint = ld_ro(lpc + atL + ML_REINT * sn);
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) l.spec[sp] = ld_ro(lpc + atL + (ML_FS + sp) * sn);
+  l.sum = ld_ro(lpc + atL + ML_SUM * sn);
+  l.c = ld_ro(q + atL + SQ_C * sn);
+  l.csml = ld_ro(q + atL + SQ_CSML * sn);
+  double qr[ES_N];
+  load_es(rst, s, at, qr);
+  const CellAux aR = load_aux(q, s, at, P.gamma);
+  double f[NVAR], qpres, qun;
+  mol_face_from_states<d>(i, j, k, s, g, P, q, l, qr, aR, f, qpres, qun);
+  face_adjust_and_store<d, MET>(f, qpres, qun, i, j, k, s, g, P, uin, divu, flx, qfd, M);
+}
+
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLSTATES) k_mol_states(Region r0, Region r1, Region r2,
+                                                                    Space s, KParams P,
+                                                                    const double* q, Ptr3 lpc,
+                                                                    Ptr3 rst) {
+  int i, j, k;
+  const int64_t t = gtid();
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(r0, t, i, j, k)) mol_states_body<0>(i, j, k, s, P, q, lpc.p[0], rst.p[0]);
+      break;
+    case 1:
+      if (region_cell(r1, t, i, j, k)) mol_states_body<1>(i, j, k, s, P, q, lpc.p[1], rst.p[1]);
+      break;
+    default:
+      if (region_cell(r2, t, i, j, k)) mol_states_body<2>(i, j, k, s, P, q, lpc.p[2], rst.p[2]);
+      break;
+  }
+}
+
+template <bool MET>
+__global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLFACE) k_mol_face(Region r0, Region r1, Region r2,
+                                                                Space s, KGeom g, KParams P,
+                                                                const double* q, Ptr3 lpc,
+                                                                Ptr3 rst, const double* divu,
+                                                                DFab uin, DFab fx, DFab fy,
+                                                                DFab fz, Ptr3 qf, Metrics M) {
+  int i, j, k;
+  const int64_t t = gtid();
+  switch (blockIdx.y) {
+    case 0:
+      if (region_cell(r0, t, i, j, k))
+        mol_face_body<0, MET>(i, j, k, s, g, P, q, lpc.p[0], rst.p[0], divu, uin, fx, qf.p[0], &M);
+      break;
+    case 1:
+      if (region_cell(r1, t, i, j, k))
+        mol_face_body<1, MET>(i, j, k, s, g, P, q, lpc.p[1], rst.p[1], divu, uin, fy, qf.p[1], &M);
+      break;
+    default:
+      if (region_cell(r2, t, i, j, k))
+        mol_face_body<2, MET>(i, j, k, s, g, P, q, lpc.p[2], rst.p[2], divu, uin, fz, qf.p[2], &M);
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // MOL slopes and face pass fused (the level and per-box paths): a cell's
 // slopes (mol_slope_compute) become its two edge states at once
 // (mol_cell_states) and the face between two cells takes the left pieces of
@@ -1163,17 +1293,34 @@ __device__ __forceinline__ void batched_cell(const BoxCtx& c, int sub, int i, in
         break;
     }
   } else if constexpr (STAGE == BS_MOLSLOPE) {
+    // the cell pass: slopes, or (split layout) the two edge states
+#if CAMR_MOLSPLIT
+    switch (sub) {
+      case 0: mol_states_body<0>(i, j, k, w.s, P, w.q, w.sm[0], w.sp[0]); break;
+      case 1: mol_states_body<1>(i, j, k, w.s, P, w.q, w.sm[1], w.sp[1]); break;
+      default: mol_states_body<2>(i, j, k, w.s, P, w.q, w.sm[2], w.sp[2]); break;
+    }
+#else
     switch (sub) {
       case 0: mol_slope_body<0>(i, j, k, w.s, P, w.q, w.slope[0]); break;
       case 1: mol_slope_body<1>(i, j, k, w.s, P, w.q, w.slope[1]); break;
       default: mol_slope_body<2>(i, j, k, w.s, P, w.q, w.slope[2]); break;
     }
+#endif
   } else if constexpr (STAGE == BS_MOLFLUX) {
+#if CAMR_MOLSPLIT
+    switch (sub) {
+      case 0: mol_face_body<0>(i, j, k, w.s, c.g, P, w.q, w.sm[0], w.sp[0], w.divu, c.uin, c.flx[0], w.qf[0]); break;
+      case 1: mol_face_body<1>(i, j, k, w.s, c.g, P, w.q, w.sm[1], w.sp[1], w.divu, c.uin, c.flx[1], w.qf[1]); break;
+      default: mol_face_body<2>(i, j, k, w.s, c.g, P, w.q, w.sm[2], w.sp[2], w.divu, c.uin, c.flx[2], w.qf[2]); break;
+    }
+#else
     switch (sub) {
       case 0: mol_flux_body<0>(i, j, k, w.s, c.g, P, w.q, w.slope[0], w.divu, c.uin, c.flx[0], w.qf[0]); break;
       case 1: mol_flux_body<1>(i, j, k, w.s, c.g, P, w.q, w.slope[1], w.divu, c.uin, c.flx[1], w.qf[1]); break;
       default: mol_flux_body<2>(i, j, k, w.s, c.g, P, w.q, w.slope[2], w.divu, c.uin, c.flx[2], w.qf[2]); break;
     }
+#endif
   } else {
     Ptr3 qf{{w.qf[0], w.qf[1], w.qf[2]}};
     consup_body(i, j, k, w.s, c.g, c.flx[0], c.flx[1], c.flx[2], qf, c.dsdt);
@@ -1220,11 +1367,13 @@ __global__ void __launch_bounds__(kBlock, MINB)
 }
 }  // namespace
 
-size_t work_doubles(const Space& s, bool mol, bool has_src) {
+size_t work_doubles(const Space& s, bool mol, bool has_src, bool mol_split) {
   size_t c = SQ_N + 1 /*divu*/;
   if (has_src) c += ES_N;
   if (!mol) {
     c += 1 /*flat*/ + 6 * ES_N + 3 * FR_N + 6 * FR_N;
+  } else if (mol_split && CAMR_MOLSPLIT) {
+    c += 6 * ES_N;  // left pieces and right states per direction
   } else {
     c += 3 * SL_N;
   }
@@ -1232,7 +1381,7 @@ size_t work_doubles(const Space& s, bool mol, bool has_src) {
   return c * size_t(s.sn);
 }
 
-void work_carve(Work& w, double* base, bool mol, bool has_src) {
+void work_carve(Work& w, double* base, bool mol, bool has_src, bool mol_split) {
   double* p = base;
   const int64_t sn = w.s.sn;
   auto take = [&](int ncomp) {
@@ -1254,6 +1403,11 @@ void work_carve(Work& w, double* base, bool mol, bool has_src) {
       w.f1[d] = take(FR_N);
     }
     for (int c = 0; c < 6; ++c) w.f2[c] = take(FR_N);
+  } else if (mol_split && CAMR_MOLSPLIT) {
+    for (int d = 0; d < 3; ++d) {
+      w.sm[d] = take(ES_N);  // ML_* left pieces of the cell's high face
+      w.sp[d] = take(ES_N);  // right state of the cell's low face
+    }
   } else {
     for (int d = 0; d < 3; ++d) w.slope[d] = take(SL_N);
   }
@@ -1424,6 +1578,25 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       k_mol_fz<<<dim3(gx, unsigned(nb[1]), unsigned(segz)), kMolRow, 0, st>>>(
           s, g, L.P, w.q, w.divu, L.uin, L.flx[2], qf.p[2], lenz);
       count_launch(3);
+      return cudaGetLastError();
+    }
+    if (!w.slope[0]) {
+      if (L.keep_slopes) return cudaErrorInvalidValue;  // a tape needs the slope layout
+      Ptr3 lpc{{w.sm[0], w.sm[1], w.sm[2]}};
+      Ptr3 rst{{w.sp[0], w.sp[1], w.sp[2]}};
+      mark("mol_states");
+      k_mol_states<<<dim3(grid_for(ms), 3), kBlock, 0, st>>>(rs[0], rs[1], rs[2], s, L.P, w.q,
+                                                             lpc, rst);
+      mark("mol_face");
+      if (L.M.on)
+        k_mol_face<true><<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(
+            rb[0], rb[1], rb[2], s, g, L.P, w.q, lpc, rst, w.divu, L.uin, L.flx[0], L.flx[1],
+            L.flx[2], qf, L.M);
+      else
+        k_mol_face<false><<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(
+            rb[0], rb[1], rb[2], s, g, L.P, w.q, lpc, rst, w.divu, L.uin, L.flx[0], L.flx[1],
+            L.flx[2], qf, L.M);
+      count_launch(2);
       return cudaGetLastError();
     }
     Ptr3 sl{{w.slope[0], w.slope[1], w.slope[2]}};

@@ -38,7 +38,8 @@ struct Work {
   double* f1[3];    // FR_N comps each
   double* f2[6];    // FR_N comps each, index combo(D,E)
   double* qf[3];    // 2 comps each: interface pressure, normal velocity
-  double* slope[3]; // MOL: 8 comps each
+  double* slope[3]; // MOL slope layout: 8 comps each (split layout: sm/sp hold
+                    // the ML_* left pieces / right edge states instead)
 };
 
 // Combination index of the second-pass "D|E" fluxes.
@@ -46,8 +47,11 @@ __host__ __device__ constexpr int combo(int D, int E) {
   return D * 2 + ((E > D) ? E - 1 : E);
 }
 
-size_t work_doubles(const Space& s, bool mol, bool has_src);
-void work_carve(Work& w, double* base, bool mol, bool has_src);
+// mol_split = false: the MOL slope layout (slope[d]) instead of the edge
+// states of the split cell/face passes (sm[d], sp[d]) -- smaller, and what
+// a slope tape needs.
+size_t work_doubles(const Space& s, bool mol, bool has_src, bool mol_split = true);
+void work_carve(Work& w, double* base, bool mol, bool has_src, bool mol_split = true);
 
 // Optional per-stage event marks (profiling): mark() records the next event
 // on the launch stream before a stage is issued.

@@ -102,7 +102,7 @@ extern "C" camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx
   const bool has_src = src && src->ptr;
   Work w;
   w.s = make_space(bx_lo, bx_hi);
-  const size_t need = work_doubles(w.s, mol, has_src) * sizeof(double);
+  const size_t need = work_doubles(w.s, mol, has_src, false) * sizeof(double);
   if (need > kScratchBytes) {
     std::snprintf(g_msg, sizeof(g_msg),
                   "box needs %zu bytes of scratch; the static scratch holds %zu bytes",
@@ -115,7 +115,7 @@ extern "C" camr_status camr_hydro_umdrv_noalloc(const int bx_lo[3], const int bx
   // Every scratch slot a call reads is written earlier in the same call
   // (each pass reads only the regions the previous passes produced), so no
   // clearing is needed between calls.
-  work_carve(w, static_cast<double*>(base), mol, has_src);
+  work_carve(w, static_cast<double*>(base), mol, has_src, false);
 
   HydroLaunch Lh;
   for (int d = 0; d < 3; ++d) {
