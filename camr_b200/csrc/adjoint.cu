@@ -716,6 +716,7 @@ camr_status camr_adjoint_create(const camr_geom* geom, const camr_hydro_params* 
   L.sy = a->G.sp.sy;
   L.sz = a->G.sp.sz;
   L.sn = a->G.sp.sn;
+  lgeom_finish(L);
   a->ncell = int64_t(L.dhi[0] - L.dlo[0] + 1) * (L.dhi[1] - L.dlo[1] + 1) *
              (L.dhi[2] - L.dlo[2] + 1);
   a->sbytes = size_t(L.sn) * NVAR * sizeof(double);

@@ -956,6 +956,7 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
   Lc.sy = sp0.sy;
   Lc.sz = sp0.sz;
   Lc.sn = sp0.sn;
+  lgeom_finish(Lc);
   a->ncell0 = ncell0;
   const bool mol = p->do_mol != 0;
   cudaError_t e = cudaSuccess;
@@ -1007,6 +1008,7 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
     L.sy = sp.sy;
     L.sz = sp.sz;
     L.sn = sp.sn;
+    lgeom_finish(L);
     off[b] = total;
     total += (int64_t(sp.sn) * NVAR + 31) / 32 * 32;
     poff[b] = ptotal;

@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include "camr_b200.h"
+#include "fastdiv.h"
 
 namespace camr {
 
@@ -131,19 +132,26 @@ inline DFab make_dfab(const camr_fab& f) {
   return d;
 }
 
-// A rectangular index region launched as a flat 1-D grid, i fastest.
+// A rectangular index region launched as a flat 1-D grid, i fastest.  Build
+// it with make_region (a default-constructed one is empty).
 struct Region {
-  int lo[3], n[3];
+  int lo[3] = {0, 0, 0}, n[3] = {0, 0, 0};
+  Decode3 dc = {0, 0, 0, {0u, 0}, {0u, 0}};
   int64_t count() const { return int64_t(n[0]) * n[1] * n[2]; }
 };
 
 __device__ __forceinline__ bool region_cell(const Region& r, int64_t t, int& i, int& j, int& k) {
   if (t >= int64_t(r.n[0]) * r.n[1] * r.n[2]) return false;
-  const int64_t nxy = int64_t(r.n[0]) * r.n[1];
-  k = int(t / nxy);
-  const int64_t rem = t - int64_t(k) * nxy;
-  j = int(rem / r.n[0]);
-  i = int(rem - int64_t(j) * r.n[0]);
+  if (r.dc.fast) {
+    decode3(r.dc, t, i, j, k);
+  } else {
+    // a region not built by make_region, or of 2^31 cells or more
+    const int64_t nxy = int64_t(r.n[0]) * r.n[1];
+    k = int(t / nxy);
+    const int64_t rem = t - int64_t(k) * nxy;
+    j = int(rem / r.n[0]);
+    i = int(rem - int64_t(j) * r.n[0]);
+  }
   i += r.lo[0];
   j += r.lo[1];
   k += r.lo[2];
@@ -156,6 +164,7 @@ inline Region make_region(const int lo[3], const int hi[3]) {
     r.lo[d] = lo[d];
     r.n[d] = hi[d] - lo[d] + 1;
   }
+  if (r.count() > 0) r.dc = make_decode3(r.n[0], r.n[1], r.n[2]);
   return r;
 }
 

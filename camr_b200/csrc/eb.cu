@@ -1405,13 +1405,15 @@ __global__ void __launch_bounds__(kBlk) k_ebl_est_dt(LGeom L, KParams P, EBG G, 
 
 __global__ void __launch_bounds__(kBlk) k_ebl_clean_copy(LGeom L, KParams P, EBG G,
                                                           const double* S, double* out,
-                                                          DevError* err) {
+                                                          DevError* err, FloorList fl) {
   int i, j, k;
   if (!valid_cell(L, tid(), i, j, k)) return;
   const int64_t at = L.idx(i, j, k);
   double s[NVAR];
   load_cell(S, L, at, s);
   if (!cov_at(G, i, j, k)) {
+    // below the floor: listed, k_floor_fixup redoes it in the reference's order
+    if (s[URHO] < P.small_dens) floor_push(fl, at);
     enforce_min_density(s, S, L, P, i, j, k, err);
     normalize_species(s);
   }
@@ -1422,7 +1424,7 @@ __global__ void __launch_bounds__(kBlk) k_ebl_clean_copy(LGeom L, KParams P, EBG
 // expand_state with the EB guards (fill rules as k_expand's).
 __global__ void __launch_bounds__(kBlk) k_ebl_expand(LGeom L, KParams P, EBG G,
                                                       const double* src, double* B,
-                                                      DevError* err) {
+                                                      DevError* err, FloorList fl) {
   int i, j, k;
   if (!padded_cell(L, tid(), i, j, k)) return;
   const int c[3] = {i, j, k};
@@ -1444,6 +1446,9 @@ __global__ void __launch_bounds__(kBlk) k_ebl_expand(LGeom L, KParams P, EBG G,
   if (!physical) {
     load_cell(src, L, L.idx(img[0], img[1], img[2]), s);
     if (!cov_at(G, img[0], img[1], img[2])) {
+      // the valid cell itself (not a periodic ghost image) joins the list
+      if (s[URHO] < P.small_dens && img[0] == i && img[1] == j && img[2] == k)
+        floor_push(fl, L.idx(i, j, k));
       enforce_min_density(s, src, L, P, img[0], img[1], img[2], err);
       normalize_species(s);
     }
@@ -1497,9 +1502,9 @@ __global__ void __launch_bounds__(kBlk) k_ebl_update1(LGeom L, KParams P, const 
   store_cell(S, L, at, s);
 }
 
-// clean_state of one cell inside the fused end of step: a density under
-// the floor is reported (enforce_min_density cannot see its neighbours'
-// new values here).
+// clean_state of one cell inside the fused end of step.  The update
+// kernels hand a cell below the density floor to k_floor_fixup before this
+// point; one still below it here (or NaN) is reported.
 __device__ __forceinline__ void clean_eb_cell(double* s, const KParams& P, bool cov, int i, int j,
                                               int k, DevError* err) {
   if (!cov) {
@@ -1536,7 +1541,7 @@ __global__ void __launch_bounds__(kBlk) k_ebl_update2(LGeom L, KParams P, EBG G,
                                                        const double* dtp, const double* B2,
                                                        const double* S_old, const double* dsdt,
                                                        double* S, unsigned long long* bits,
-                                                       DevError* err) {
+                                                       DevError* err, FloorList fl) {
   int i, j, k;
   double v = DBL_MAX;
   if (valid_cell(L, tid(), i, j, k)) {
@@ -1550,7 +1555,9 @@ __global__ void __launch_bounds__(kBlk) k_ebl_update2(LGeom L, KParams P, EBG G,
     for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * dsdt[at + n * L.sn];
-    v = ebl_finish(s, sold, P, L, dt, cov, i, j, k, err);
+    // below the floor: the post-Saxpy state stays for k_floor_fixup
+    if (!cov && s[URHO] < P.small_dens) floor_push(fl, at);
+    else v = ebl_finish(s, sold, P, L, dt, cov, i, j, k, err);
     store_cell(S, L, at, s);
   }
   block_min_dt(v, bits);
@@ -1563,7 +1570,7 @@ __global__ void __launch_bounds__(kBlk) k_ebl_update_ctu(LGeom L, KParams P, EBG
                                                           const double* S_old,
                                                           const double* dsdt, double* S,
                                                           unsigned long long* bits,
-                                                          DevError* err) {
+                                                          DevError* err, FloorList fl) {
   int i, j, k;
   double v = DBL_MAX;
   if (valid_cell(L, tid(), i, j, k)) {
@@ -1584,7 +1591,8 @@ __global__ void __launch_bounds__(kBlk) k_ebl_update_ctu(LGeom L, KParams P, EBG
     }
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) s[n] += dt * dsdt[at + n * L.sn];
-    v = ebl_finish(s, sold, P, L, dt, cov, i, j, k, err);
+    if (!cov && s[URHO] < P.small_dens) floor_push(fl, at);
+    else v = ebl_finish(s, sold, P, L, dt, cov, i, j, k, err);
     store_cell(S, L, at, s);
   }
   block_min_dt(v, bits);
@@ -1683,6 +1691,7 @@ struct camr_eb_level {
   unsigned long long* bits = nullptr;
   int* nstep = nullptr;
   DevError* err = nullptr;
+  FloorList floor;                // cells below the density floor of the current pass
   unsigned* flag = nullptr;
   double *vfrac = nullptr, *ap[3] = {nullptr, nullptr, nullptr}, *fc[3] = {nullptr, nullptr, nullptr};
   double* cent = nullptr;
@@ -1781,27 +1790,51 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   }
   k_dt_next<<<1, 1, 0, st>>>(c, first ? 1 : 0, fixed_dev, lev->bits, lev->dt_cur, lev->dt_hist,
                              lev->nstep, lev->hist_cap);
-  k_ebl_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->S_old, lev->err);
-  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err);
-  nk += 3;
+  // Each cleaning pass lists the non-covered cells below the density floor
+  // and a one-block fixup resets them in the reference's order (a no-op
+  // launch when the list is empty).
+  const FloorList& fl = lev->floor;
+  FloorArgs fa{};
+  fa.in = lev->S;
+  fa.out = lev->S_old;
+  k_ebl_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->S_old, lev->err, fl);
+  k_floor_fixup<FLOOR_CLEAN><<<1, 1024, 0, st>>>(L, lev->P, fl, fa, lev->err);
+  fa.in = lev->S_old;
+  fa.out = lev->B;
+  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err, fl);
+  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(L, lev->P, fl, fa, lev->err);
+  nk += 5;
   cudaError_t e = eb_hydro_stage(lev, st, &nk);
   if (e != cudaSuccess) return e;
+  FloorArgs fu{};
+  fu.out = lev->S;
+  fu.B = lev->B;
+  fu.S_old = lev->S_old;
+  fu.dtp = lev->dt_cur;
+  fu.bits = lev->bits;
+  fu.post = 1;
+  fu.dsdt = lev->dsdt;
   if (!lev->hp.do_mol) {
     k_ebl_update_ctu<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old,
-                                          lev->dsdt, lev->S, lev->bits, lev->err);
-    count_launch(nk + 1);
+                                          lev->dsdt, lev->S, lev->bits, lev->err, fl);
+    k_floor_fixup<FLOOR_DSDT_CTU><<<1, 1024, 0, st>>>(L, lev->P, fl, fu, lev->err);
+    count_launch(nk + 2);
     return cudaGetLastError();
   }
   k_ebl_update1<<<gv, kBlk, 0, st>>>(L, lev->P, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
                                      lev->S);
   // stage 2's Sborder reuses B (stage 1's is dead after the update)
-  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B, lev->err);
-  nk += 2;
+  fa.in = lev->S;
+  fa.out = lev->B;
+  k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B, lev->err, fl);
+  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(L, lev->P, fl, fa, lev->err);
+  nk += 3;
   e = eb_hydro_stage(lev, st, &nk);
   if (e != cudaSuccess) return e;
   k_ebl_update2<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
-                                     lev->S, lev->bits, lev->err);
-  nk += 1;
+                                     lev->S, lev->bits, lev->err, fl);
+  k_floor_fixup<FLOOR_DSDT_MOL2><<<1, 1024, 0, st>>>(L, lev->P, fl, fu, lev->err);
+  nk += 2;
   count_launch(nk);
   return cudaGetLastError();
 }
@@ -1882,6 +1915,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   L.sy = L.pn[0];
   L.sz = L.sy * L.pn[1];
   L.sn = L.sz * L.pn[2];
+  lgeom_finish(L);
   lev->ncell = int64_t(g.dom_hi[0] - g.dom_lo[0] + 1) * (g.dom_hi[1] - g.dom_lo[1] + 1) *
                (g.dom_hi[2] - g.dom_lo[2] + 1);
   lev->npad = L.sn;
@@ -1910,6 +1944,10 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   alloc(reinterpret_cast<void**>(&lev->bits), sizeof(unsigned long long));
   alloc(reinterpret_cast<void**>(&lev->nstep), sizeof(int));
   alloc(reinterpret_cast<void**>(&lev->err), sizeof(DevError));
+  alloc(reinterpret_cast<void**>(&lev->floor.count), sizeof(int));
+  alloc(reinterpret_cast<void**>(&lev->floor.cells), sizeof(int64_t) * kFloorCap);
+  alloc(reinterpret_cast<void**>(&lev->floor.enforced), sizeof(double) * NVAR * kFloorCap);
+  alloc(reinterpret_cast<void**>(&lev->floor.total), sizeof(unsigned long long));
   alloc(reinterpret_cast<void**>(&lev->flag), size_t(gc) * sizeof(unsigned));
   alloc(reinterpret_cast<void**>(&lev->vfrac), size_t(gc) * sizeof(double));
   if (eb->cent) alloc(reinterpret_cast<void**>(&lev->cent), size_t(3 * gc) * sizeof(double));
@@ -2087,7 +2125,8 @@ camr_status camr_eb_level_destroy(camr_eb_level* lev) {
                   lev->fixed_dev, lev->dt_cur, lev->dt_hist, lev->bits,     lev->nstep,
                   lev->err,     lev->flag,    lev->vfrac,  lev->ap[0],      lev->ap[1],
                   lev->ap[2],   lev->fc[0],   lev->fc[1],  lev->fc[2],      lev->regular_flx,
-                  lev->cent};
+                  lev->cent,    lev->floor.count, lev->floor.cells, lev->floor.enforced,
+                  lev->floor.total};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (double* w : lev->plan_work)
@@ -2278,6 +2317,17 @@ int64_t camr_eb_level_kernels_per_step(camr_eb_level* lev) {
 camr_status camr_eb_level_stream(camr_eb_level* lev, void** stream) {
   if (!lev || !stream) return CAMR_ERR_INVALID;
   *stream = lev->stream;
+  return CAMR_OK;
+}
+
+camr_status camr_eb_level_floor_resets(camr_eb_level* lev, int64_t* cells) {
+  if (!lev || !cells) return CAMR_ERR_INVALID;
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, lev->floor.total, sizeof(h), cudaMemcpyDeviceToHost,
+                                  lev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lev->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  *cells = int64_t(h);
   return CAMR_OK;
 }
 

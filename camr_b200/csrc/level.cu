@@ -303,6 +303,7 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   L.sy = sp.sy;
   L.sz = sp.sz;
   L.sn = sp.sn;
+  lgeom_finish(L);
   lev->ncell = int64_t(L.dhi[0] - L.dlo[0] + 1) * (L.dhi[1] - L.dlo[1] + 1) *
                (L.dhi[2] - L.dlo[2] + 1);
   lev->hist_cap = 1 << 16;

@@ -34,10 +34,20 @@ struct LGeom {
   int bclo[3], bchi[3];
   int boxsz[3];             // enforce_min_density window (box size)
   double dx[3];
+  // flat-index decoding of valid / padded cells (lgeom_finish; without it
+  // the kernels divide in 64 bits)
+  Decode3 vdc = {0, 0, 0, {0u, 0}, {0u, 0}};
+  Decode3 pdc = {0, 0, 0, {0u, 0}, {0u, 0}};
   __host__ __device__ int64_t idx(int i, int j, int k) const {
     return (i - plo[0]) + (j - plo[1]) * sy + (k - plo[2]) * sz;
   }
 };
+
+// Call once the domain and padded extents are set.
+inline void lgeom_finish(LGeom& L) {
+  L.vdc = make_decode3(L.dhi[0] - L.dlo[0] + 1, L.dhi[1] - L.dlo[1] + 1, L.dhi[2] - L.dlo[2] + 1);
+  L.pdc = make_decode3(L.pn[0], L.pn[1], L.pn[2]);
+}
 
 struct LevelState {
   double* S;       // state (valid cells meaningful)
@@ -203,11 +213,15 @@ __device__ void enforce_min_density(double* s, const double* src, const LGeom& L
 __device__ __forceinline__ bool padded_cell(const LGeom& L, int64_t t, int& i, int& j, int& k) {
   const int64_t n = int64_t(L.pn[0]) * L.pn[1] * L.pn[2];
   if (t >= n) return false;
-  const int64_t nxy = int64_t(L.pn[0]) * L.pn[1];
-  k = int(t / nxy);
-  const int64_t r = t - int64_t(k) * nxy;
-  j = int(r / L.pn[0]);
-  i = int(r - int64_t(j) * L.pn[0]);
+  if (L.pdc.fast) {
+    decode3(L.pdc, t, i, j, k);
+  } else {
+    const int64_t nxy = int64_t(L.pn[0]) * L.pn[1];
+    k = int(t / nxy);
+    const int64_t r = t - int64_t(k) * nxy;
+    j = int(r / L.pn[0]);
+    i = int(r - int64_t(j) * L.pn[0]);
+  }
   i += L.plo[0];
   j += L.plo[1];
   k += L.plo[2];
@@ -218,11 +232,15 @@ __device__ __forceinline__ bool valid_cell(const LGeom& L, int64_t t, int& i, in
   const int n0 = L.dhi[0] - L.dlo[0] + 1, n1 = L.dhi[1] - L.dlo[1] + 1,
             n2 = L.dhi[2] - L.dlo[2] + 1;
   if (t >= int64_t(n0) * n1 * n2) return false;
-  const int64_t nxy = int64_t(n0) * n1;
-  k = int(t / nxy);
-  const int64_t r = t - int64_t(k) * nxy;
-  j = int(r / n0);
-  i = int(r - int64_t(j) * n0);
+  if (L.vdc.fast) {
+    decode3(L.vdc, t, i, j, k);
+  } else {
+    const int64_t nxy = int64_t(n0) * n1;
+    k = int(t / nxy);
+    const int64_t r = t - int64_t(k) * nxy;
+    j = int(r / n0);
+    i = int(r - int64_t(j) * n0);
+  }
   i += L.dlo[0];
   j += L.dlo[1];
   k += L.dlo[2];
@@ -616,8 +634,12 @@ __global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) k_update_mol2(LGeom L,
   if (bits) block_min_dt(v, bits);
 }
 
-// What k_floor_fixup finishes: the pass whose list it reads.
-enum { FLOOR_CLEAN = 0, FLOOR_EXPAND = 1, FLOOR_CTU = 2, FLOOR_MOL2 = 3 };
+// What k_floor_fixup finishes: the pass whose list it reads.  The DSDT
+// modes are the updates of a level whose hydro right-hand side is an array
+// (the EB level): CTU S_new = Sborder (+ dt*src_old) + dt*dsdt, MOL stage 2
+// S_new = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*dsdt.
+enum { FLOOR_CLEAN = 0, FLOOR_EXPAND = 1, FLOOR_CTU = 2, FLOOR_MOL2 = 3, FLOOR_DSDT_CTU = 4,
+       FLOOR_DSDT_MOL2 = 5 };
 
 struct FloorArgs {
   const double* in;   // CLEAN / EXPAND: the array being cleaned
@@ -629,7 +651,38 @@ struct FloorArgs {
   const double* dtp;
   unsigned long long* bits;  // CFL minimum (CTU / MOL2; may be null)
   int post;
+  const double* dsdt = nullptr;  // DSDT modes: the hydro right-hand side
 };
+
+// The DSDT modes' post-Saxpy state of a cell (the operations of the EB
+// level's update kernels).
+template <int MODE>
+__device__ __forceinline__ void dsdt_raw(const LGeom& L, const KParams& P, const FloorArgs& a,
+                                         int64_t at, double* s) {
+  const double dt = *a.dtp;
+  if constexpr (MODE == FLOOR_DSDT_CTU) {
+    load_cell(a.B, L, at, s);
+    if (P.add_grav_src) {
+      double src[NVAR];
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+      src[UMZ] = P.const_grav * a.S_old[at + URHO * L.sn];
+      src[UEDEN] = P.const_grav * a.S_old[at + UMZ * L.sn];
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
+    }
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += dt * a.dsdt[at + n * L.sn];
+  } else {
+    double b[NVAR], sold[NVAR];
+    load_cell(a.B, L, at, b);
+    load_cell(a.S_old, L, at, sold);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * b[n] + 0.5 * sold[n];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * a.dsdt[at + n * L.sn];
+  }
+}
 
 // Sort key of a listed cell: its level box, then its padded index (raster
 // order inside the box).
@@ -675,6 +728,8 @@ __device__ __forceinline__ void floor_raw(const LGeom& L, const KParams& P, cons
   } else {
     if (listed) {
       load_cell(a.out, L, at, s);
+    } else if constexpr (MODE == FLOOR_DSDT_CTU || MODE == FLOOR_DSDT_MOL2) {
+      dsdt_raw<MODE>(L, P, a, at, s);
     } else {
       double sold[NVAR];
       if constexpr (MODE == FLOOR_CTU) ctu_raw(L, a.sp, P, *a.dtp, a.B, a.S_old, a.fp, i, j, k, s, sold);

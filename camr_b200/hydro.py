@@ -409,6 +409,12 @@ class EBLevel:
               "camr_eb_level_boxes")
         return {"regular": r.value, "cut": c.value, "covered": v.value}
 
+    def floor_resets(self):
+        """Cells enforce_min_density has reset since the level was created."""
+        v = C.c_int64()
+        check(lib().camr_eb_level_floor_resets(self._h, C.byref(v)), "floor_resets")
+        return v.value
+
     def error(self):
         info = native.ErrorInfo()
         lib().camr_eb_level_get_error(self._h, C.byref(info))

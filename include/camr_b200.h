@@ -546,6 +546,11 @@ camr_status camr_eb_level_boxes(camr_eb_level* lev, int* regular, int* cut, int*
 int64_t camr_eb_level_kernels_per_step(camr_eb_level* lev);
 camr_status camr_eb_level_stream(camr_eb_level* lev, void** stream);
 camr_status camr_eb_level_get_error(camr_eb_level* lev, camr_error_info* info);
+/* Cells enforce_min_density has reset since the level was created
+ * (synchronises).  As camr_level_floor_resets, with the EB build's guard:
+ * covered cells are never reset, but they are neighbours like any other
+ * cell (Source/CAMR.cpp:960-1043). */
+camr_status camr_eb_level_floor_resets(camr_eb_level* lev, int64_t* cells);
 
 /* ---------------------------------------------------------------------
  * Plotfile output / input of one level (host memory), in AMReX's plotfile

@@ -629,8 +629,18 @@ long enforce_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S, co
   return nerr;
 }
 
-long clean_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S) {
-  long nerr = enforce_eb(p, L, S, L.dom);
+// The level's boxes are enforce_min_density's windows (its MFIter loop over
+// the boxes, Source/CAMR.cpp:960-1043, without tiling as on the GPU).
+long enforce_boxes(const orc_params* p, const LevelEB& L, Array4<Real> const& S,
+                   const std::vector<Box>& boxes) {
+  long nerr = 0;
+  for (const Box& b : boxes) nerr += enforce_eb(p, L, S, b);
+  return nerr;
+}
+
+long clean_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& S,
+              const std::vector<Box>& boxes) {
+  long nerr = enforce_boxes(p, L, S, boxes);
   ParallelFor(L.dom, [&](int i, int j, int k) {
     if (!covered(L, i, j, k)) normalize_eb(S, i, j, k);
   });
@@ -650,11 +660,11 @@ int bc_kind_of(int n, int d, int phys) {
 
 // expand_state: FillPatch(src) into B over G + clean_state(B).
 long expand_eb(const orc_params* p, const LevelEB& L, Array4<Real> const& src,
-               Array4<Real> const& B) {
+               Array4<Real> const& B, const std::vector<Box>& boxes) {
   ParallelFor(L.dom, [&](int i, int j, int k) {
     for (int n = 0; n < NVAR; ++n) B(i, j, k, n) = src(i, j, k, n);
   });
-  long nerr = enforce_eb(p, L, B, L.dom);
+  long nerr = enforce_boxes(p, L, B, boxes);
   ParallelFor(L.dom, [&](int i, int j, int k) {
     if (!covered(L, i, j, k)) normalize_eb(B, i, j, k);
   });
@@ -888,8 +898,8 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
       dt = std::min(std::numeric_limits<double>::max(), 1 * dt_min) / 1;
     }
     ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S_old(i, j, k, n) = S(i, j, k, n); });
-    nerr += clean_eb(p, L, S_old);
-    nerr += expand_eb(p, L, S_old, B);
+    nerr += clean_eb(p, L, S_old, boxes);
+    nerr += expand_eb(p, L, S_old, B, boxes);
     ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S(i, j, k, n) = B(i, j, k, n); });
     if (p->add_grav_src) {
       ParallelFor(L.dom, [&](int i, int j, int k) {
@@ -903,7 +913,7 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
     nerr += stage(B, k1, dt);
     ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) { S(i, j, k, n) += dt * k1(i, j, k, n); });
     if (p->do_mol) {
-      nerr += expand_eb(p, L, S, B2);
+      nerr += expand_eb(p, L, S, B2, boxes);
       nerr += stage(B2, k2, dt);
       ParallelFor(L.dom, NVAR, [&](int i, int j, int k, int n) {
         S(i, j, k, n) = 0.5 * B2(i, j, k, n) + 0.5 * S_old(i, j, k, n);
@@ -912,7 +922,7 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
         S(i, j, k, n) += 0.5 * dt * k2(i, j, k, n);
       });
     }
-    nerr += clean_eb(p, L, S);
+    nerr += clean_eb(p, L, S, boxes);
     if (p->add_grav_src) {
       ParallelFor(L.dom, [&](int i, int j, int k) {
         Real src[NVAR];
@@ -921,9 +931,9 @@ extern "C" long orc_eb_advance(const orc_params* p, const orc_level* lev, const 
         src[UEDEN] = 0.5 * p->const_grav * (S(i, j, k, UMZ) - S_old(i, j, k, UMZ));
         for (int n = 0; n < NVAR; ++n) S(i, j, k, n) += dt * src[n];
       });
-      nerr += clean_eb(p, L, S);
+      nerr += clean_eb(p, L, S, boxes);
     }
-    nerr += clean_eb(p, L, S);
+    nerr += clean_eb(p, L, S, boxes);
     dt_level = dt;
     if (dt_hist) dt_hist[step] = dt;
   }

@@ -243,3 +243,47 @@ def test_eb_level_state_redistribution_matches_oracle(kind, mgs, do_mol):
     assert_bitwise(L.dts(), ref_dts, "dt")
     assert_bitwise(got, ref, "state")
     L.close()
+
+
+@pytest.mark.skipif(not HAVE_EB, reason="EB oracle library not built")
+@pytest.mark.parametrize("do_mol", [1, 0], ids=["mol", "godunov_plm"])
+def test_eb_level_density_floor_matches_oracle(do_mol):
+    """enforce_min_density on an EB level (Source/CAMR.cpp:941-1045 with the
+    EB guard :960-968): an outward flow around a sphere empties cells below
+    a raised small_dens; the level's boxes are the windows, covered cells
+    are skipped but are neighbours.  States and dts bit for bit against the
+    oracle, cells reset, error word clear."""
+    _torch()
+    from test_gpu_configs import evacuating_flow
+    n = 24
+    ng = 5 if do_mol else 6
+    dx = 1.0 / n
+    geo = E.sphere_geometry((-ng,) * 3, (n + ng - 1,) * 3, dx, center=(0.3, 0.55, 0.5),
+                            radius=0.12)
+    s = np.ascontiguousarray(E.set_covered(evacuating_flow(n), geo))
+    mgs = (8, 8, 8)
+    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, small_dens=0.45)
+    lev = oracle.make_level((n, n, n), dx=(dx,) * 3, max_grid_size=mgs)
+    oracle.eb_init_finalize(p, lev, s)
+    ref = s.copy()
+    nsteps = 14
+    _, ref_dts, nass = oracle.eb_advance(p, lev, geo, ref, nsteps, redist=1)
+    assert nass == 0
+    free = s.copy()
+    p_free = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3)
+    oracle.eb_advance(p_free, lev, geo, free, nsteps, redist=1)
+    assert not np.array_equal(free, ref)  # the floor acts
+    geom = hydro.make_geom((n, n, n), dx=(dx,) * 3)
+    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, small_dens=0.45)
+    L = hydro.EBLevel(geom, prm, geo, redist=1, max_grid_size=mgs)
+    L.set_state(s)
+    L.advance(nsteps)
+    got = L.get_state()
+    dts = L.dts()
+    resets = L.floor_resets()
+    err = L.error()
+    L.close()
+    assert err[0] == 0, err
+    assert resets > 0
+    assert_bitwise(dts, ref_dts, "dt")
+    assert_bitwise(got, ref, "state")
