@@ -144,13 +144,15 @@ __global__ void __launch_bounds__(kBlk) kf_init_finalize(FineDev F, KParams P, d
 // S_old = clean_state(S) on the fine valid cells (the density floor's
 // neighbour window is the box).
 __global__ void __launch_bounds__(kBlk) kf_clean_copy(FineDev F, KParams P, const double* S,
-                                                       double* out, DevError* err) {
+                                                       double* out, DevError* err,
+                                                       FloorList fl) {
   FINE_VALID_PROLOGUE
   if (!ok) return;
   const double* Sb = S + F.off[b];
   const int64_t at = L.idx(i, j, k);
   double s[NVAR];
   load_cell(Sb, L, at, s);
+  if (s[URHO] < P.small_dens) floor_push(fl, (int64_t(b) << 40) | at);
   enforce_min_density(s, Sb, L, P, i, j, k, err);
   normalize_species(s);
   compute_temp(s, P);
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(kBlk) kf_est_dt(FineDev F, KParams P, const do
 // kf_interp.
 __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap CM,
                                                  const double* src, double* B, int3 fdlo,
-                                                 int3 fdn, DevError* err) {
+                                                 int3 fdn, DevError* err, FloorList fl) {
   const int b = box_of_block(F.gb0, F.nbox, blockIdx.x);
   const LGeom& L = F.L[b];
   const int64_t t = (int64_t(blockIdx.x) - F.gb0[b]) * kBlk + threadIdx.x;
@@ -188,6 +190,7 @@ __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap 
   if (valid) {
     const double* sb = src + F.off[b];
     load_cell(sb, L, L.idx(i, j, k), s);
+    if (s[URHO] < P.small_dens) floor_push(fl, (int64_t(b) << 40) | L.idx(i, j, k));
     enforce_min_density(s, sb, L, P, i, j, k, err);
   } else {
     const int wi = wrapi(i, fdlo.x, fdn.x), wj = wrapi(j, fdlo.y, fdn.y),
@@ -314,42 +317,80 @@ __device__ __forceinline__ FluxPtrs fine_fluxes(const FineDev& F, const FinePool
   return r;
 }
 
-// CTU fine update: S = Sborder (+ dt*src_old) + dt*dSdt, then the step's
-// clean_states and post_timestep's (the finest level cleans its own).
+// The fine updates' post-Saxpy states of cell (i,j,k) of box b (the fixup
+// recomputes them for neighbours of cells below the density floor).  CTU:
+// S = Sborder (+ dt*src_old) + dt*dSdt; sold holds the old density and z
+// momentum the gravity terms read (zero otherwise).
+__device__ __forceinline__ void fine_ctu_raw(const FineDev& F, const FinePools& fpool,
+                                             const KParams& P, double dt, const double* B,
+                                             const double* S_old, int b, const LGeom& L, int i,
+                                             int j, int k, double* s, double* sold) {
+  const int64_t at = L.idx(i, j, k);
+  const int64_t o = F.off[b];
+  double hs[NVAR];
+  load_cell(B + o, L, at, s);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) sold[n] = 0.0;
+  if (P.add_grav_src) {
+    sold[URHO] = S_old[o + at + URHO * L.sn];
+    sold[UMZ] = S_old[o + at + UMZ * L.sn];
+  }
+  if (P.add_grav_src) {
+    double src[NVAR];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
+    src[UMZ] = P.const_grav * sold[URHO];
+    src[UEDEN] = P.const_grav * sold[UMZ];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
+  }
+  const FluxPtrs fp = fine_fluxes(F, fpool, b);
+  cell_dsdt(L, space_of(L), i, j, k, fp.f, fp.q, hs);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] += dt * hs[n];
+}
+
+// MOL stage 2: S = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*k2; sold = S_old.
+__device__ __forceinline__ void fine_mol2_raw(const FineDev& F, const FinePools& fpool,
+                                              double dt, const double* B2, const double* S_old,
+                                              int b, const LGeom& L, int i, int j, int k,
+                                              double* s, double* sold) {
+  const int64_t at = L.idx(i, j, k);
+  const int64_t o = F.off[b];
+  double bb[NVAR], hs[NVAR];
+  load_cell(B2 + o, L, at, bb);
+  load_cell(S_old + o, L, at, sold);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * bb[n] + 0.5 * sold[n];
+  const FluxPtrs fp = fine_fluxes(F, fpool, b);
+  cell_dsdt(L, space_of(L), i, j, k, fp.f, fp.q, hs);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * hs[n];
+}
+
+// Fine-level density-floor list entry: box << 40 | index in the box's arrays.
+__device__ __forceinline__ void fine_floor_push(const FloorList& fl, int b, int64_t at) {
+  floor_push(fl, (int64_t(b) << 40) | at);
+}
+
+// CTU fine update, then the step's clean_states and post_timestep's (the
+// finest level cleans its own).  A cell below the density floor keeps its
+// post-Saxpy state and joins the list (kf_floor_fixup finishes it).
 __global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) kf_update_ctu(FineDev F, FinePools fpool, KParams P,
                                                        const double* dtp, const double* B,
                                                        const double* S_old, double* S,
-                                                       unsigned long long* bits, DevError* err) {
+                                                       unsigned long long* bits, DevError* err,
+                                                       FloorList fl) {
   FINE_VALID_PROLOGUE
   double v = DBL_MAX;
   if (ok) {
     const double dt = *dtp;
     const int64_t at = L.idx(i, j, k);
-    const int64_t o = F.off[b];
-    double s[NVAR], sold[NVAR], hs[NVAR];
-    load_cell(B + o, L, at, s);
-    // the gravity terms read only the old density and z momentum
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) sold[n] = 0.0;
-    if (P.add_grav_src) {
-      sold[URHO] = S_old[o + at + URHO * L.sn];
-      sold[UMZ] = S_old[o + at + UMZ * L.sn];
-    }
-    if (P.add_grav_src) {
-      double src[NVAR];
-#pragma unroll
-      for (int n = 0; n < NVAR; ++n) src[n] = 0.0;
-      src[UMZ] = P.const_grav * sold[URHO];
-      src[UEDEN] = P.const_grav * sold[UMZ];
-#pragma unroll
-      for (int n = 0; n < NVAR; ++n) s[n] += dt * src[n];
-    }
-    const FluxPtrs fp = fine_fluxes(F, fpool, b);
-    cell_dsdt(L, space_of(L), i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += dt * hs[n];
-    v = finish_step(s, sold, P, L, dt, i, j, k, err, true);
-    store_cell(S + o, L, at, s);
+    double s[NVAR], sold[NVAR];
+    fine_ctu_raw(F, fpool, P, dt, B, S_old, b, L, i, j, k, s, sold);
+    if (s[URHO] < P.small_dens) fine_floor_push(fl, b, at);
+    else v = finish_step(s, sold, P, L, dt, i, j, k, err, true);
+    store_cell(S + F.off[b], L, at, s);
   }
   if (bits) block_min_dt(v, bits);
 }
@@ -383,26 +424,156 @@ __global__ void __launch_bounds__(kBlk) kf_update_mol1(FineDev F, FinePools fpoo
 __global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) kf_update_mol2(FineDev F, FinePools fpool, KParams P,
                                                         const double* dtp, const double* B2,
                                                         const double* S_old, double* S,
-                                                        unsigned long long* bits, DevError* err) {
+                                                        unsigned long long* bits, DevError* err,
+                                                        FloorList fl) {
   FINE_VALID_PROLOGUE
   double v = DBL_MAX;
   if (ok) {
     const double dt = *dtp;
     const int64_t at = L.idx(i, j, k);
-    const int64_t o = F.off[b];
-    double s[NVAR], sold[NVAR], bb[NVAR], hs[NVAR];
-    load_cell(B2 + o, L, at, bb);
-    load_cell(S_old + o, L, at, sold);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] = 0.5 * bb[n] + 0.5 * sold[n];
-    const FluxPtrs fp = fine_fluxes(F, fpool, b);
-    cell_dsdt(L, space_of(L), i, j, k, fp.f, fp.q, hs);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) s[n] += 0.5 * dt * hs[n];
-    v = finish_step(s, sold, P, L, dt, i, j, k, err, true);
-    store_cell(S + o, L, at, s);
+    double s[NVAR], sold[NVAR];
+    fine_mol2_raw(F, fpool, dt, B2, S_old, b, L, i, j, k, s, sold);
+    if (s[URHO] < P.small_dens) fine_floor_push(fl, b, at);
+    else v = finish_step(s, sold, P, L, dt, i, j, k, err, true);
+    store_cell(S + F.off[b], L, at, s);
   }
   if (bits) block_min_dt(v, bits);
+}
+
+// The passes of the fine level whose cells below the density floor
+// kf_floor_fixup finishes.
+enum { FFLOOR_CLEAN = 0, FFLOOR_FILL = 1, FFLOOR_CTU = 2, FFLOOR_MOL2 = 3 };
+
+struct FineFloorArgs {
+  const double* in;      // CLEAN / FILL: the pool being cleaned
+  double* out;           // CLEAN: S_old; FILL: Sborder; CTU / MOL2: S
+  const double* B;       // CTU / MOL2: the stage's Sborder
+  const double* S_old;
+  FinePools fp;
+  const double* dtp;
+  unsigned long long* bits;  // CFL minimum of the updates (may be null)
+  int3 fdlo, fdn;        // the fine domain (FILL: periodic images)
+};
+
+// The fine level's view of floor_walk: each fine box is its own window.
+template <int MODE>
+struct FineFloorPolicy {
+  const FineDev& F;
+  const KParams& P;
+  const FineFloorArgs& a;
+  __device__ void decode(int64_t box, int64_t at, int& i, int& j, int& k) const {
+    decode_cell(F.L[box], at, i, j, k);
+  }
+  __device__ void window(int64_t box, int, int, int, int* blo, int* bhi) const {
+    const LGeom& L = F.L[box];
+    for (int d = 0; d < 3; ++d) {
+      blo[d] = L.dlo[d];
+      bhi[d] = L.dhi[d];
+    }
+  }
+  __device__ int64_t idx(int64_t box, int i, int j, int k) const { return F.L[box].idx(i, j, k); }
+  __device__ double dens(int64_t box, int64_t at) const {
+    // as in the single-level fixup: the updates' stored densities are the
+    // post-Saxpy ones for every cell
+    if constexpr (MODE == FFLOOR_CLEAN || MODE == FFLOOR_FILL) return a.in[F.off[box] + at];
+    else return a.out[F.off[box] + at];
+  }
+  __device__ void raw(bool listed, int64_t box, int64_t at, int i, int j, int k,
+                      double* s) const {
+    const LGeom& L = F.L[box];
+    const int b = int(box);
+    if constexpr (MODE == FFLOOR_CLEAN || MODE == FFLOOR_FILL) {
+      load_cell(a.in + F.off[b], L, at, s);
+    } else if (listed) {
+      load_cell(a.out + F.off[b], L, at, s);
+    } else {
+      double sold[NVAR];
+      if constexpr (MODE == FFLOOR_CTU)
+        fine_ctu_raw(F, a.fp, P, *a.dtp, a.B, a.S_old, b, L, i, j, k, s, sold);
+      else
+        fine_mol2_raw(F, a.fp, *a.dtp, a.B, a.S_old, b, L, i, j, k, s, sold);
+    }
+  }
+};
+
+// enforce_min_density on the fine cells a pass listed (floor_walk, each box
+// its own window as in the reference's MFIter loop), then the rest of the
+// pass for them: CLEAN normalize_species + computeTemp; FILL the same, into
+// the cell and into every ghost cell of any fine box that is its image
+// (FillBoundary); CTU / MOL2 the end of the step and its CFL dt.  One
+// block; more than kFloorCap cells: error code 5.
+template <int MODE>
+__global__ void __launch_bounds__(1024) kf_floor_fixup(FineDev F, KParams P, FloorList fl,
+                                                        FineFloorArgs a, DevError* err) {
+  __shared__ int64_t key[kFloorCap];
+  const int n = *fl.count;
+  if (n == 0) return;
+  if (n > kFloorCap) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int64_t c = fl.cells[0];
+      int i, j, k;
+      decode_cell(F.L[c >> 40], c & kFloorAtMask, i, j, k);
+      report_error(err, 5, i, j, k);
+      *fl.count = 0;
+    }
+    return;
+  }
+  for (int t = threadIdx.x; t < n; t += blockDim.x) key[t] = fl.cells[t];
+  floor_sort(key, n);
+  double* enf = fl.enforced;
+  floor_walk(FineFloorPolicy<MODE>{F, P, a}, P, key, n, enf, err);
+  __syncthreads();
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    const int b = int(key[m] >> 40);
+    const int64_t at = key[m] & kFloorAtMask;
+    const LGeom& L = F.L[b];
+    int i, j, k;
+    decode_cell(L, at, i, j, k);
+    double s[NVAR];
+    for (int q = 0; q < NVAR; ++q) s[q] = enf[int64_t(m) * NVAR + q];
+    if constexpr (MODE == FFLOOR_CLEAN || MODE == FFLOOR_FILL) {
+      normalize_species(s);
+      compute_temp(s, P);
+      store_cell(a.out + F.off[b], L, at, s);
+      if constexpr (MODE == FFLOOR_FILL) {
+        const int len[3] = {a.fdn.x, a.fdn.y, a.fdn.z};
+        const int c[3] = {i, j, k};
+        for (int ob = 0; ob < F.nbox; ++ob) {
+          const LGeom& Lo = F.L[ob];
+          for (int mz = -1; mz <= 1; ++mz)
+            for (int my = -1; my <= 1; ++my)
+              for (int mx = -1; mx <= 1; ++mx) {
+                const int m3[3] = {mx, my, mz};
+                int g[3];
+                bool in_pad = true, in_valid = true;
+                for (int d = 0; d < 3; ++d) {
+                  g[d] = c[d] + m3[d] * len[d];
+                  in_pad = in_pad && g[d] >= Lo.plo[d] && g[d] <= Lo.plo[d] + Lo.pn[d] - 1;
+                  in_valid = in_valid && g[d] >= Lo.dlo[d] && g[d] <= Lo.dhi[d];
+                }
+                if (in_pad && !in_valid)
+                  store_cell(a.out + F.off[ob], Lo, Lo.idx(g[0], g[1], g[2]), s);
+              }
+        }
+      }
+    } else {
+      double sold[NVAR];
+      for (int q = 0; q < NVAR; ++q) sold[q] = 0.0;
+      if (P.add_grav_src) {
+        sold[URHO] = a.S_old[F.off[b] + at + URHO * L.sn];
+        sold[UMZ] = a.S_old[F.off[b] + at + UMZ * L.sn];
+      }
+      const double v = finish_step(s, sold, P, L, *a.dtp, i, j, k, err, true);
+      store_cell(a.out + F.off[b], L, at, s);
+      if (a.bits) atomicMin(a.bits, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (fl.total) atomicAdd(fl.total, (unsigned long long)n);
+    *fl.count = 0;
+  }
 }
 
 // Packed (per box (NVAR, nz, ny, nx), boxes back to back) <-> fine pools.
@@ -506,34 +677,47 @@ __device__ __forceinline__ double avg_down_cell(const FineDev& F, const double* 
   return volfrac * c;
 }
 
-// post_timestep of level 0: S += (CrseAdd + FineAdd sums) (reflux), the
-// covered cells replaced by the average of the fine cells (avgDown), then
-// clean_state; the cell's CFL dt for the next step.  As in the fused
-// single-level update, a density under the floor is reported in the error
-// word instead of reset from the neighbours.
-__global__ void __launch_bounds__(kBlk) k_coarse_post(LGeom Lc, KParams P, CoarseMap CM,
-                                                       FluxRegDev R, FineDev F,
-                                                       const double* S1, double* S0,
-                                                       unsigned long long* bits, DevError* err) {
+// post_timestep on level 0 (Source/CAMR.cpp:679-718), part 1: reflux (the
+// flux-register sums) and avgDown (covered cells replaced by the average of
+// the fine cells), left raw in S0; cells below the density floor join the
+// list (k_floor_fixup<FLOOR_INPLACE> resets them in the reference's order).
+__global__ void __launch_bounds__(kBlk) k_coarse_raw(LGeom Lc, KParams P, CoarseMap CM,
+                                                      FluxRegDev R, FineDev F,
+                                                      const double* S1, double* S0,
+                                                      FloorList fl) {
+  int i, j, k;
+  if (!valid_cell(Lc, tid(), i, j, k)) return;
+  const int64_t at = Lc.idx(i, j, k);
+  const int c = CM.cell(i, j, k);
+  const int bi = CM.bmap[c];
+  const int ob = CM.cmap[c];
+  double s[NVAR];
+  load_cell(S0, Lc, at, s);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) {
+    const double corr =
+        (bi >= 0) ? R.d[bi + int64_t(n) * R.nbnd] + R.cfp[bi + int64_t(n) * R.nbnd] : 0.0 + 0.0;
+    s[n] = s[n] + corr;
+  }
+  if (ob >= 0) {
+    for (int n = 0; n < NVAR; ++n) s[n] = avg_down_cell(F, S1, ob, i, j, k, n);
+  }
+  if (s[URHO] < P.small_dens) floor_push(fl, at);
+  store_cell(S0, Lc, at, s);
+}
+
+// Part 2: the rest of clean_state (normalize_species, computeTemp) on every
+// cell and the cell's CFL dt for the next step.
+__global__ void __launch_bounds__(kBlk) k_coarse_finish(LGeom Lc, KParams P, double* S0,
+                                                         unsigned long long* bits,
+                                                         DevError* err) {
   int i, j, k;
   double v = DBL_MAX;
   if (valid_cell(Lc, tid(), i, j, k)) {
     const int64_t at = Lc.idx(i, j, k);
-    const int c = CM.cell(i, j, k);
-    const int bi = CM.bmap[c];
-    const int ob = CM.cmap[c];
     double s[NVAR];
     load_cell(S0, Lc, at, s);
-#pragma unroll
-    for (int n = 0; n < NVAR; ++n) {
-      const double corr =
-          (bi >= 0) ? R.d[bi + int64_t(n) * R.nbnd] + R.cfp[bi + int64_t(n) * R.nbnd] : 0.0 + 0.0;
-      s[n] = s[n] + corr;
-    }
-    if (ob >= 0) {
-      for (int n = 0; n < NVAR; ++n) s[n] = avg_down_cell(F, S1, ob, i, j, k, n);
-    }
-    if (!(s[URHO] >= P.small_dens)) report_error(err, s[URHO] == 0. ? 3 : 5, i, j, k);
+    if (!(s[URHO] >= P.small_dens)) report_error(err, floor_code(s[URHO], P), i, j, k);
     normalize_species(s);
     compute_temp(s, P);
     store_cell(S0, Lc, at, s);
@@ -677,6 +861,7 @@ struct camr_amr {
   int hist_cap = 1 << 14;
   unsigned long long *bits0 = nullptr, *bits1 = nullptr;
   DevError* err = nullptr;
+  FloorList floor;  // cells below the density floor of the current pass (both levels)
   double *staging0 = nullptr, *staging1 = nullptr;
   int fine_mode = CAMR_BATCH_PERSISTENT;
   int steps_taken = 0;
@@ -762,8 +947,20 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   if (e != cudaSuccess) return e;
 
   // ---- level 0: CAMR_advance with CrseAdd, no post_timestep yet ----
-  k_clean_copy<<<gv0, kBlk, 0, st>>>(Lc, P, a->S0, a->S0_old, a->err);
-  k_expand<<<blocks_of(npad0), kBlk, 0, st>>>(Lc, P, a->S0_old, a->B0, a->err);
+  // Each cleaning pass lists the cells below the density floor and a
+  // one-block fixup resets them in the reference's order (a no-op launch
+  // when the list is empty).
+  const FloorList& fl = a->floor;
+  FloorArgs fa{};
+  fa.in = a->S0;
+  fa.out = a->S0_old;
+  k_clean_copy<<<gv0, kBlk, 0, st>>>(Lc, P, a->S0, a->S0_old, a->err, fl);
+  k_floor_fixup<FLOOR_CLEAN><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+  fa.in = a->S0_old;
+  fa.out = a->B0;
+  k_expand<<<blocks_of(npad0), kBlk, 0, st>>>(Lc, P, a->S0_old, a->B0, a->err, fl);
+  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+  count_launch(2);
   count_launch(2);
   HydroLaunch H;
   for (int d = 0; d < 3; ++d) {
@@ -807,11 +1004,18 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   count_launch();
   if (!mol) {
     k_update_ctu<<<gv0, kBlk, 0, st>>>(Lc, sp0, P, dt0, a->B0, a->S0_old, fp0, a->S0, nullptr,
-                                       a->err, 0);
+                                       a->err, 0, fl);
+    FloorArgs fu{nullptr, a->S0, a->B0, a->S0_old, fp0, sp0, dt0, nullptr, 0};
+    k_floor_fixup<FLOOR_CTU><<<1, 1024, 0, st>>>(Lc, P, fl, fu, a->err);
+    count_launch();
     count_launch();
   } else {
     k_update_mol1<<<gv0, kBlk, 0, st>>>(Lc, sp0, P, dt0, a->B0, a->S0_old, fp0, a->S0);
-    k_expand<<<blocks_of(npad0), kBlk, 0, st>>>(Lc, P, a->S0, a->B0_2, a->err);
+    fa.in = a->S0;
+    fa.out = a->B0_2;
+    k_expand<<<blocks_of(npad0), kBlk, 0, st>>>(Lc, P, a->S0, a->B0_2, a->err, fl);
+    k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+    count_launch();
     count_launch(2);
     H.uin = sdfab(a->B0_2);
     H.src = H.uin;
@@ -819,7 +1023,10 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     if (e != cudaSuccess) return e;
     k_crse_add<<<gb, kBlk, 0, st>>>(R, Lc, a->flx0[0], a->flx0[1], a->flx0[2], dt0, fac, vol0);
     k_update_mol2<<<gv0, kBlk, 0, st>>>(Lc, sp0, P, dt0, a->B0_2, a->S0_old, fp0, a->S0,
-                                        nullptr, a->err, 0);
+                                        nullptr, a->err, 0, fl);
+    FloorArgs fu{nullptr, a->S0, a->B0_2, a->S0_old, fp0, sp0, dt0, nullptr, 0};
+    k_floor_fixup<FLOOR_MOL2><<<1, 1024, 0, st>>>(Lc, P, fl, fu, a->err);
+    count_launch();
     count_launch(2);
   }
 
@@ -831,8 +1038,20 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   for (int sc = 0; sc < RR; ++sc) {
     unsigned long long* fbits = (sc == RR - 1) ? a->bits1 : nullptr;
     k_fine_clock<<<1, 1, 0, st>>>(a->clock);
-    kf_clean_copy<<<gf_valid, kBlk, 0, st>>>(F, P, a->S1, a->S1_old, a->err);
-    kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1_old, a->B1, fdlo, fdn, a->err);
+    FineFloorArgs ff{};
+    ff.fp = FP;
+    ff.dtp = dt1;
+    ff.fdlo = fdlo;
+    ff.fdn = fdn;
+    ff.in = a->S1;
+    ff.out = a->S1_old;
+    kf_clean_copy<<<gf_valid, kBlk, 0, st>>>(F, P, a->S1, a->S1_old, a->err, fl);
+    kf_floor_fixup<FFLOOR_CLEAN><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+    ff.in = a->S1_old;
+    ff.out = a->B1;
+    kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1_old, a->B1, fdlo, fdn, a->err, fl);
+    kf_floor_fixup<FFLOOR_FILL><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+    count_launch(2);
     kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[0],
                                           a->d_ib0, a->B1);
     count_launch(4);
@@ -842,12 +1061,23 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     count_launch();
     if (!mol) {
       kf_update_ctu<<<gf_valid, kBlk, 0, st>>>(F, FP, P, dt1, a->B1, a->S1_old, a->S1, fbits,
-                                               a->err);
+                                               a->err, fl);
+      ff.in = nullptr;
+      ff.out = a->S1;
+      ff.B = a->B1;
+      ff.S_old = a->S1_old;
+      ff.bits = fbits;
+      kf_floor_fixup<FFLOOR_CTU><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+      count_launch();
       count_launch();
     } else {
       kf_update_mol1<<<gf_valid, kBlk, 0, st>>>(F, FP, P, dt1, a->B1, a->S1_old, a->S1);
       // Sborder of the second stage reuses B1 (the first one is consumed)
-      kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1, a->B1, fdlo, fdn, a->err);
+      ff.in = a->S1;
+      ff.out = a->B1;
+      kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1, a->B1, fdlo, fdn, a->err, fl);
+      kf_floor_fixup<FFLOOR_FILL><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+      count_launch();
       kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[1],
                                             a->d_ib0, a->B1);
       count_launch(3);
@@ -855,14 +1085,25 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
       if (cs != CAMR_OK) return cudaErrorLaunchFailure;
       k_fine_add<<<gb, kBlk, 0, st>>>(R, F, FP, dt1, fac, volf8);
       kf_update_mol2<<<gf_valid, kBlk, 0, st>>>(F, FP, P, dt1, a->B1, a->S1_old, a->S1, fbits,
-                                                a->err);
+                                                a->err, fl);
+      ff.in = nullptr;
+      ff.out = a->S1;
+      ff.B = a->B1;
+      ff.S_old = a->S1_old;
+      ff.bits = fbits;
+      kf_floor_fixup<FFLOOR_MOL2><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+      count_launch();
       count_launch(2);
     }
   }
 
   // ---- level 0 post_timestep: reflux, avgDown, clean_state ----
-  k_coarse_post<<<gv0, kBlk, 0, st>>>(Lc, P, CM, R, F, a->S1, a->S0, a->bits0, a->err);
-  count_launch();
+  k_coarse_raw<<<gv0, kBlk, 0, st>>>(Lc, P, CM, R, F, a->S1, a->S0, fl);
+  fa.in = a->S0;
+  fa.out = a->S0;
+  k_floor_fixup<FLOOR_INPLACE><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+  k_coarse_finish<<<gv0, kBlk, 0, st>>>(Lc, P, a->S0, a->bits0, a->err);
+  count_launch(3);
   return cudaGetLastError();
 }
 
@@ -874,7 +1115,8 @@ void amr_free(camr_amr* a) {
                   a->d_L, a->d_off, a->d_vb0, a->d_gb0, a->d_ib0, a->d_poff, a->d_qf, a->d_cmap,
                   a->d_bmap, a->d_bcell, a->d_mask, a->d_cstart, a->d_contrib, a->d_reg,
                   a->d_cfp, a->clock, a->hist, a->bits0, a->bits1, a->err, a->staging0,
-                  a->staging1};
+                  a->staging1, a->floor.count, a->floor.cells, a->floor.enforced,
+                  a->floor.total};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (a->own_stream) cudaStreamDestroy(a->stream);
@@ -1032,6 +1274,10 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
   alloc(reinterpret_cast<void**>(&a->bits0), sizeof(unsigned long long));
   alloc(reinterpret_cast<void**>(&a->bits1), sizeof(unsigned long long));
   alloc(reinterpret_cast<void**>(&a->err), sizeof(DevError));
+  alloc(reinterpret_cast<void**>(&a->floor.count), sizeof(int));
+  alloc(reinterpret_cast<void**>(&a->floor.cells), sizeof(int64_t) * kFloorCap);
+  alloc(reinterpret_cast<void**>(&a->floor.enforced), sizeof(double) * NVAR * kFloorCap);
+  alloc(reinterpret_cast<void**>(&a->floor.total), sizeof(unsigned long long));
   if (e != cudaSuccess) {
     amr_free(a);
     return CAMR_ERR_NOMEM;
@@ -1267,6 +1513,17 @@ camr_status camr_amr_restart(camr_amr* a, const double clock[4], int steps_done)
   if (e != cudaSuccess) return cuda_status_of(e);
   a->steps_taken = steps_done;
   a->restart_est = true;
+  return CAMR_OK;
+}
+
+camr_status camr_amr_floor_resets(camr_amr* a, int64_t* cells) {
+  if (!a || !cells) return CAMR_ERR_INVALID;
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, a->floor.total, sizeof(h), cudaMemcpyDeviceToHost,
+                                  a->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
+  if (e != cudaSuccess) return cuda_status_of(e);
+  *cells = int64_t(h);
   return CAMR_OK;
 }
 

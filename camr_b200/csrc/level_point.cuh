@@ -638,8 +638,10 @@ __global__ void __launch_bounds__(kBlk, CAMR_MINB_UPDATE) k_update_mol2(LGeom L,
 // modes are the updates of a level whose hydro right-hand side is an array
 // (the EB level): CTU S_new = Sborder (+ dt*src_old) + dt*dsdt, MOL stage 2
 // S_new = 0.5*Sborder2 + 0.5*S_old + 0.5*dt*dsdt.
+// INPLACE: a pass that left the raw state in the array (in == out) for a
+// later kernel to finish.
 enum { FLOOR_CLEAN = 0, FLOOR_EXPAND = 1, FLOOR_CTU = 2, FLOOR_MOL2 = 3, FLOOR_DSDT_CTU = 4,
-       FLOOR_DSDT_MOL2 = 5 };
+       FLOOR_DSDT_MOL2 = 5, FLOOR_INPLACE = 6 };
 
 struct FloorArgs {
   const double* in;   // CLEAN / EXPAND: the array being cleaned
@@ -723,7 +725,7 @@ template <int MODE>
 __device__ __forceinline__ void floor_raw(const LGeom& L, const KParams& P, const FloorArgs& a,
                                           bool listed, int64_t at, int i, int j, int k,
                                           double* s) {
-  if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
+  if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND || MODE == FLOOR_INPLACE) {
     load_cell(a.in, L, at, s);
   } else {
     if (listed) {
@@ -738,46 +740,14 @@ __device__ __forceinline__ void floor_raw(const LGeom& L, const KParams& P, cons
   }
 }
 
-// enforce_min_density (Source/CAMR.cpp:941-1045) on the listed cells in the
-// reference's order -- box by box, cells in raster order, each reset in
-// place so that later cells see it -- then the rest of the listed cells'
-// pass (normalize_species + computeTemp, or the end of the step with its
-// CFL dt).  One block: the list is sorted by (box, raster position); the
-// window of a cell never leaves its box, so the boxes are independent and
-// one thread walks each box's cells in order; then all threads finish the
-// cells.  The window is the level box holding the cell (the reference's GPU
-// build loops over boxes; its OpenMP build over tiles of them).  More than
-// kFloorCap listed cells: error code 5 and the cells stay as the pass left
-// them.  The count is cleared at the end, ready for the next pass.
-template <int MODE>
-__global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorList fl,
-                                                       FloorArgs a, DevError* err) {
-  constexpr int64_t kAtMask = (int64_t(1) << 40) - 1;
-  __shared__ int64_t key[kFloorCap];
-  const int n = *fl.count;
-  if (n == 0) return;
-  if (n > kFloorCap) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int i, j, k;
-      decode_cell(L, fl.cells[0], i, j, k);
-      report_error(err, 5, i, j, k);
-      *fl.count = 0;
-    }
-    return;
-  }
+// Sort n listed keys (box << 40 | array index) in shared memory, ascending:
+// bitonic over the next power of two, padded with INT64_MAX.  All threads
+// of the block call it.
+__device__ __forceinline__ void floor_sort(int64_t* key, int n) {
   int N = 1;
   while (N < n) N <<= 1;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    if (t < n) {
-      const int64_t at = fl.cells[t];
-      int i, j, k;
-      decode_cell(L, at, i, j, k);
-      key[t] = floor_key(L, at, i, j, k);
-    } else {
-      key[t] = INT64_MAX;
-    }
-  }
+  for (int t = threadIdx.x; t < N; t += blockDim.x)
+    if (t >= n) key[t] = INT64_MAX;
   __syncthreads();
   for (int size = 2; size <= N; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
@@ -795,26 +765,37 @@ __global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorL
       __syncthreads();
     }
   }
-  double* enf = fl.enforced;
+}
+
+constexpr int64_t kFloorAtMask = (int64_t(1) << 40) - 1;
+
+// enforce_min_density (Source/CAMR.cpp:941-1045) on the sorted listed
+// cells in the reference's order -- box by box, cells in raster order, each
+// reset kept in `enf` so that later cells of the box see it; one thread per
+// box (a cell's window never leaves its box, so boxes are independent).
+// The policy gives the pass's view of the level:
+//   decode(box, at, i, j, k)         cell of an array index
+//   window(box, i, j, k, blo, bhi)   enforce_min_density's window (the box)
+//   idx(box, i, j, k)                array index of a cell
+//   dens(box, at)                    density as the pass left it
+//   raw(listed, box, at, i, j, k, s) the state enforce_min_density sees
+template <class Pol>
+__device__ __forceinline__ void floor_walk(const Pol& pol, const KParams& P, const int64_t* key,
+                                           int n, double* enf, DevError* err) {
   for (int t0 = threadIdx.x; t0 < n; t0 += blockDim.x) {
     const int64_t box = key[t0] >> 40;
     if (t0 > 0 && (key[t0 - 1] >> 40) == box) continue;  // not the first cell of its box
     for (int m = t0; m < n && (key[m] >> 40) == box; ++m) {
-      const int64_t at = key[m] & kAtMask;
+      const int64_t at = key[m] & kFloorAtMask;
       int i, j, k;
-      decode_cell(L, at, i, j, k);
+      pol.decode(box, at, i, j, k);
       double s[NVAR];
-      floor_raw<MODE>(L, P, a, true, at, i, j, k, s);
+      pol.raw(true, box, at, i, j, k, s);
       if (s[URHO] == 0.) {
         report_error(err, 3, i, j, k);  // amrex::Error in the reference
       } else {
         int blo[3], bhi[3];
-        const int c[3] = {i, j, k};
-        for (int d = 0; d < 3; ++d) {
-          const int b = (c[d] - L.dlo[d]) / L.boxsz[d];
-          blo[d] = L.dlo[d] + b * L.boxsz[d];
-          bhi[d] = min(blo[d] + L.boxsz[d] - 1, L.dhi[d]);
-        }
+        pol.window(box, i, j, k, blo, bhi);
         double max_dens = s[URHO];
         int64_t pick = at;
         int pick_m = -1;
@@ -823,20 +804,11 @@ __global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorL
             for (int ii = -1; ii <= 1; ii++) {
               if (i + ii >= blo[0] && j + jj >= blo[1] && k + kk >= blo[2] && i + ii <= bhi[0] &&
                   j + jj <= bhi[1] && k + kk <= bhi[2]) {
-                const int64_t nat = L.idx(i + ii, j + jj, k + kk);
+                const int64_t nat = pol.idx(box, i + ii, j + jj, k + kk);
                 const int mm = floor_find(key, n, (box << 40) | nat);
-                double r;
-                if (mm >= 0 && mm < m) {
-                  r = enf[int64_t(mm) * NVAR + URHO];  // reset earlier in this walk
-                } else if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
-                  r = a.in[nat];
-                } else {
-                  // an update pass stored the post-Saxpy state of listed
-                  // cells; for the others the stored density is the
-                  // post-Saxpy one too (the cleans and the gravity source
-                  // leave the density alone)
-                  r = a.out[nat];
-                }
+                // a cell reset earlier in this walk, else the pass's value
+                const double r =
+                    (mm >= 0 && mm < m) ? enf[int64_t(mm) * NVAR + URHO] : pol.dens(box, nat);
                 if (r > max_dens) {
                   pick = nat;
                   pick_m = mm;
@@ -861,21 +833,91 @@ __global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorL
           for (int q = 0; q < NVAR; ++q) s[q] = enf[int64_t(pick_m) * NVAR + q];
         } else {
           int pi, pj, pk;
-          decode_cell(L, pick, pi, pj, pk);
-          floor_raw<MODE>(L, P, a, false, pick, pi, pj, pk, s);
+          pol.decode(box, pick, pi, pj, pk);
+          pol.raw(false, box, pick, pi, pj, pk, s);
         }
       }
       for (int q = 0; q < NVAR; ++q) enf[int64_t(m) * NVAR + q] = s[q];
     }
   }
+}
+
+// The single-level view of floor_walk: boxes of boxsz cells tile the domain.
+template <int MODE>
+struct LevelFloorPolicy {
+  const LGeom& L;
+  const KParams& P;
+  const FloorArgs& a;
+  __device__ void decode(int64_t, int64_t at, int& i, int& j, int& k) const {
+    decode_cell(L, at, i, j, k);
+  }
+  __device__ void window(int64_t, int i, int j, int k, int* blo, int* bhi) const {
+    const int c[3] = {i, j, k};
+    for (int d = 0; d < 3; ++d) {
+      const int b = (c[d] - L.dlo[d]) / L.boxsz[d];
+      blo[d] = L.dlo[d] + b * L.boxsz[d];
+      bhi[d] = min(blo[d] + L.boxsz[d] - 1, L.dhi[d]);
+    }
+  }
+  __device__ int64_t idx(int64_t, int i, int j, int k) const { return L.idx(i, j, k); }
+  __device__ double dens(int64_t, int64_t at) const {
+    // the cleans read the array being cleaned; an update pass stored the
+    // post-Saxpy state of listed cells, and for the others the stored
+    // density is the post-Saxpy one too (the cleans and the gravity source
+    // leave the density alone)
+    if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND || MODE == FLOOR_INPLACE)
+      return a.in[at];
+    else
+      return a.out[at];
+  }
+  __device__ void raw(bool listed, int64_t, int64_t at, int i, int j, int k, double* s) const {
+    floor_raw<MODE>(L, P, a, listed, at, i, j, k, s);
+  }
+};
+
+// enforce_min_density on a pass's listed cells (floor_walk), then the rest
+// of the listed cells' pass: normalize_species + computeTemp (CLEAN,
+// EXPAND), nothing (INPLACE: a later kernel finishes every cell), or the
+// end of the step with its CFL dt (updates).  One block.  The window is the
+// level box holding the cell (the reference's GPU build loops over boxes;
+// its OpenMP build over tiles of them).  More than kFloorCap listed cells:
+// error code 5 and the cells stay as the pass left them.  The count is
+// cleared at the end, ready for the next pass.
+template <int MODE>
+__global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorList fl,
+                                                       FloorArgs a, DevError* err) {
+  __shared__ int64_t key[kFloorCap];
+  const int n = *fl.count;
+  if (n == 0) return;
+  if (n > kFloorCap) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int i, j, k;
+      decode_cell(L, fl.cells[0], i, j, k);
+      report_error(err, 5, i, j, k);
+      *fl.count = 0;
+    }
+    return;
+  }
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int64_t at = fl.cells[t];
+    int i, j, k;
+    decode_cell(L, at, i, j, k);
+    key[t] = floor_key(L, at, i, j, k);
+  }
+  floor_sort(key, n);
+  double* enf = fl.enforced;
+  floor_walk(LevelFloorPolicy<MODE>{L, P, a}, P, key, n, enf, err);
   __syncthreads();
   for (int m = threadIdx.x; m < n; m += blockDim.x) {
-    const int64_t at = key[m] & kAtMask;
+    const int64_t at = key[m] & kFloorAtMask;
     int i, j, k;
     decode_cell(L, at, i, j, k);
     double s[NVAR];
     for (int q = 0; q < NVAR; ++q) s[q] = enf[int64_t(m) * NVAR + q];
-    if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
+    if constexpr (MODE == FLOOR_INPLACE) {
+      store_cell(a.out, L, at, s);
+    } else if constexpr (MODE == FLOOR_CLEAN || MODE == FLOOR_EXPAND) {
       normalize_species(s);
       compute_temp(s, P);
       if constexpr (MODE == FLOOR_CLEAN) {

@@ -575,6 +575,12 @@ class AmrHierarchy:
         c = (C.c_double * 4)(*clock)
         check(lib().camr_amr_restart(self._h, C.byref(c), int(steps_done)), "amr restart")
 
+    def floor_resets(self):
+        """Cells enforce_min_density has reset on either level so far."""
+        v = C.c_int64()
+        check(lib().camr_amr_floor_resets(self._h, C.byref(v)), "floor_resets")
+        return v.value
+
     def autotune(self):
         check(lib().camr_amr_autotune(self._h), "camr_amr_autotune")
 

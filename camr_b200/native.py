@@ -114,6 +114,7 @@ SIGNATURES = {
     "camr_level_restart": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "camr_amr_restart": (C.c_int, [C.c_void_p, C.POINTER(C.c_double * 4), C.c_int]),
     "camr_eb_level_floor_resets": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "camr_amr_floor_resets": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "camr_write_checkpoint": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.POINTER(C.c_double * 3),
                                         C.POINTER(C.c_double * 2), C.POINTER(C.c_double * 2),
                                         C.POINTER(C.c_int * 2), C.c_int, C.c_void_p,

@@ -112,7 +112,7 @@ typedef struct {
                     3 density exactly zero in enforce_min_density, 4 index
                     out of range, 5 density below small_dens left unreset
                     (more cells below the floor in one pass than the reset
-                    list holds, or a driver without the list) */
+                    list holds: 4096) */
   int i, j, k;   /* cell of the first failure */
 } camr_error_info;
 
@@ -418,6 +418,14 @@ camr_status camr_amr_clock(camr_amr* a, double clock[4]);
  * levels from the restored states and applies computeNewDt against the
  * checkpoint's dts, as an uninterrupted run would (synchronises). */
 camr_status camr_amr_restart(camr_amr* a, const double clock[4], int steps_done);
+
+/* Cells enforce_min_density has reset on either level since the hierarchy
+ * was created (synchronises).  Every cleaning pass of both levels lists the
+ * cells below small_dens and resets them in the reference's order, each
+ * box of a level its own window (the fine boxes, the base level's
+ * max_grid_size boxes); post_timestep's clean of level 0 follows reflux and
+ * avgDown.  At most 4096 cells per pass; more set error code 5. */
+camr_status camr_amr_floor_resets(camr_amr* a, int64_t* cells);
 
 /* Autotune the fine level's batched hydro on its current state (after at
  * least one step); synchronises. */

@@ -119,3 +119,63 @@ def test_amr_gpu_larger_matches_oracle_and_conserves(oracle_kind):
     assert_bitwise(g1, o1, "level 1")
     for comp in (P.URHO, P.UMX, P.UMY, P.UMZ, P.UEDEN):
         assert abs(start[comp].sum() - g0[comp].sum()) <= 1e-13 * np.abs(start[comp]).sum()
+
+
+def inject(S0, boxes):
+    """Fine box states equal to their coarse parents' (ratio 2), back to
+    back in the camr_amr_set_state layout."""
+    parts = []
+    for lo, hi in boxes:
+        sl = tuple(slice(lo[d] // 2, hi[d] // 2 + 1) for d in (2, 1, 0))
+        c = S0[(slice(None),) + sl]
+        parts.append(np.ascontiguousarray(c.repeat(2, 1).repeat(2, 2).repeat(2, 3)).ravel())
+    return np.concatenate(parts)
+
+
+@pytest.mark.parametrize("method", ["mol_plm", "ctu_ppm"])
+def test_amr_density_floor_matches_oracle(method, oracle_kind):
+    """enforce_min_density on both levels of the two-level step (every
+    clean_state of CAMR_advance and post_timestep, Source/CAMR.cpp:941-1045):
+    an outward flow empties the centre below a raised small_dens; each box
+    is its own window (the base level's 8^3 boxes, each fine box), cells
+    reset in the reference's order.  States and clock bit for bit against
+    the oracle's two-level driver, cells reset, error word clear."""
+    _torch()
+    from test_gpu_configs import evacuating_flow
+    n0 = (16, 16, 16)
+    boxes = [((8, 8, 8), (23, 23, 23)), ((24, 0, 0), (31, 7, 15))]
+    S0 = evacuating_flow(16)
+    S1 = inject(S0, boxes)
+    cfg = dict(METHODS[method], small_dens=0.45)
+    mgs = (8, 8, 8)
+    nsteps = 8
+    p = oracle.default_params(**cfg)
+    lev = oracle.make_level(n0, max_grid_size=mgs)
+    bx = box_array(boxes)
+    o0, o1 = S0.copy(), S1.copy()
+    clock = np.zeros(4)
+    oracle.amr_run(oracle_kind, p, lev, bx, o0, o1, 0, do_init=True, clock=clock)
+    _, nerr = oracle.amr_run(oracle_kind, p, lev, bx, o0, o1, nsteps, first_step=True,
+                             clock=clock)
+    assert nerr == 0
+    f0, f1 = S0.copy(), S1.copy()
+    pf = oracle.default_params(**METHODS[method])
+    cf = np.zeros(4)
+    oracle.amr_run(oracle_kind, pf, lev, bx, f0, f1, 0, do_init=True, clock=cf)
+    oracle.amr_run(oracle_kind, pf, lev, bx, f0, f1, nsteps, first_step=True, clock=cf)
+    assert not (np.array_equal(f0, o0) and np.array_equal(f1, o1))  # the floor acts
+    h = hydro.AmrHierarchy(hydro.make_geom(n0), native.default_params(**cfg), boxes,
+                           max_grid_size=mgs)
+    h.set_state(S0, S1)
+    h.init_finalize()
+    h.advance(nsteps)
+    g0, g1 = h.get_state()
+    gclock = h.clock()
+    resets = h.floor_resets()
+    err = h.error()
+    h.close()
+    assert err[0] == 0, err
+    assert resets > 0
+    assert_bitwise(gclock, clock, "clock (times, dts)")
+    assert_bitwise(g0, o0, "level 0")
+    assert_bitwise(g1, o1, "level 1")

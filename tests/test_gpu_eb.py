@@ -249,8 +249,8 @@ def test_eb_level_state_redistribution_matches_oracle(kind, mgs, do_mol):
 @pytest.mark.parametrize("do_mol", [1, 0], ids=["mol", "godunov_plm"])
 def test_eb_level_density_floor_matches_oracle(do_mol):
     """enforce_min_density on an EB level (Source/CAMR.cpp:941-1045 with the
-    EB guard :960-968): an outward flow around a sphere empties cells below
-    a raised small_dens; the level's boxes are the windows, covered cells
+    EB guard :960-968): an outward flow from a sphere at the centre empties
+    cells below a raised small_dens; the level's boxes are the windows, covered cells
     are skipped but are neighbours.  States and dts bit for bit against the
     oracle, cells reset, error word clear."""
     _torch()
@@ -258,11 +258,10 @@ def test_eb_level_density_floor_matches_oracle(do_mol):
     n = 24
     ng = 5 if do_mol else 6
     dx = 1.0 / n
-    geo = E.sphere_geometry((-ng,) * 3, (n + ng - 1,) * 3, dx, center=(0.3, 0.55, 0.5),
-                            radius=0.12)
-    s = np.ascontiguousarray(E.set_covered(evacuating_flow(n), geo))
+    geo = E.sphere_geometry((-ng,) * 3, (n + ng - 1,) * 3, dx, radius=0.1)
+    s = np.ascontiguousarray(E.set_covered(evacuating_flow(n, speed=1.5), geo))
     mgs = (8, 8, 8)
-    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, small_dens=0.45)
+    p = oracle.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, small_dens=0.7)
     lev = oracle.make_level((n, n, n), dx=(dx,) * 3, max_grid_size=mgs)
     oracle.eb_init_finalize(p, lev, s)
     ref = s.copy()
@@ -274,7 +273,7 @@ def test_eb_level_density_floor_matches_oracle(do_mol):
     oracle.eb_advance(p_free, lev, geo, free, nsteps, redist=1)
     assert not np.array_equal(free, ref)  # the floor acts
     geom = hydro.make_geom((n, n, n), dx=(dx,) * 3)
-    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, small_dens=0.45)
+    prm = native.default_params(do_mol=do_mol, ppm_type=0, cfl=0.3, small_dens=0.7)
     L = hydro.EBLevel(geom, prm, geo, redist=1, max_grid_size=mgs)
     L.set_state(s)
     L.advance(nsteps)
