@@ -505,7 +505,7 @@ struct FineFloorPolicy {
 template <int MODE>
 __global__ void __launch_bounds__(1024) kf_floor_fixup(FineDev F, KParams P, FloorList fl,
                                                         FineFloorArgs a, DevError* err) {
-  __shared__ int64_t key[kFloorCap];
+  extern __shared__ int64_t key[];
   const int n = *fl.count;
   if (n == 0) return;
   if (n > kFloorCap) {
@@ -574,6 +574,21 @@ __global__ void __launch_bounds__(1024) kf_floor_fixup(FineDev F, KParams P, Flo
     if (fl.total) atomicAdd(fl.total, (unsigned long long)n);
     *fl.count = 0;
   }
+}
+
+// Allow the fine fixups their dynamic shared memory (and this translation
+// unit's single-level ones).
+cudaError_t kf_floor_prepare() {
+  const void* f[] = {reinterpret_cast<const void*>(&kf_floor_fixup<FFLOOR_CLEAN>),
+                     reinterpret_cast<const void*>(&kf_floor_fixup<FFLOOR_FILL>),
+                     reinterpret_cast<const void*>(&kf_floor_fixup<FFLOOR_CTU>),
+                     reinterpret_cast<const void*>(&kf_floor_fixup<FFLOOR_MOL2>)};
+  for (const void* k : f) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFloorSmem));
+    if (e != cudaSuccess) return e;
+  }
+  return floor_prepare();
 }
 
 // Packed (per box (NVAR, nz, ny, nx), boxes back to back) <-> fine pools.
@@ -955,11 +970,11 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   fa.in = a->S0;
   fa.out = a->S0_old;
   k_clean_copy<<<gv0, kBlk, 0, st>>>(Lc, P, a->S0, a->S0_old, a->err, fl);
-  k_floor_fixup<FLOOR_CLEAN><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+  k_floor_fixup<FLOOR_CLEAN><<<1, 1024, kFloorSmem, st>>>(Lc, P, fl, fa, a->err);
   fa.in = a->S0_old;
   fa.out = a->B0;
   k_expand<<<blocks_of(npad0), kBlk, 0, st>>>(Lc, P, a->S0_old, a->B0, a->err, fl);
-  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, kFloorSmem, st>>>(Lc, P, fl, fa, a->err);
   count_launch(2);
   count_launch(2);
   HydroLaunch H;
@@ -1006,7 +1021,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     k_update_ctu<<<gv0, kBlk, 0, st>>>(Lc, sp0, P, dt0, a->B0, a->S0_old, fp0, a->S0, nullptr,
                                        a->err, 0, fl);
     FloorArgs fu{nullptr, a->S0, a->B0, a->S0_old, fp0, sp0, dt0, nullptr, 0};
-    k_floor_fixup<FLOOR_CTU><<<1, 1024, 0, st>>>(Lc, P, fl, fu, a->err);
+    k_floor_fixup<FLOOR_CTU><<<1, 1024, kFloorSmem, st>>>(Lc, P, fl, fu, a->err);
     count_launch();
     count_launch();
   } else {
@@ -1014,7 +1029,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     fa.in = a->S0;
     fa.out = a->B0_2;
     k_expand<<<blocks_of(npad0), kBlk, 0, st>>>(Lc, P, a->S0, a->B0_2, a->err, fl);
-    k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+    k_floor_fixup<FLOOR_EXPAND><<<1, 1024, kFloorSmem, st>>>(Lc, P, fl, fa, a->err);
     count_launch();
     count_launch(2);
     H.uin = sdfab(a->B0_2);
@@ -1025,7 +1040,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     k_update_mol2<<<gv0, kBlk, 0, st>>>(Lc, sp0, P, dt0, a->B0_2, a->S0_old, fp0, a->S0,
                                         nullptr, a->err, 0, fl);
     FloorArgs fu{nullptr, a->S0, a->B0_2, a->S0_old, fp0, sp0, dt0, nullptr, 0};
-    k_floor_fixup<FLOOR_MOL2><<<1, 1024, 0, st>>>(Lc, P, fl, fu, a->err);
+    k_floor_fixup<FLOOR_MOL2><<<1, 1024, kFloorSmem, st>>>(Lc, P, fl, fu, a->err);
     count_launch();
     count_launch(2);
   }
@@ -1046,11 +1061,11 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     ff.in = a->S1;
     ff.out = a->S1_old;
     kf_clean_copy<<<gf_valid, kBlk, 0, st>>>(F, P, a->S1, a->S1_old, a->err, fl);
-    kf_floor_fixup<FFLOOR_CLEAN><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+    kf_floor_fixup<FFLOOR_CLEAN><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
     ff.in = a->S1_old;
     ff.out = a->B1;
     kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1_old, a->B1, fdlo, fdn, a->err, fl);
-    kf_floor_fixup<FFLOOR_FILL><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+    kf_floor_fixup<FFLOOR_FILL><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
     count_launch(2);
     kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[0],
                                           a->d_ib0, a->B1);
@@ -1067,7 +1082,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
       ff.B = a->B1;
       ff.S_old = a->S1_old;
       ff.bits = fbits;
-      kf_floor_fixup<FFLOOR_CTU><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+      kf_floor_fixup<FFLOOR_CTU><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
       count_launch();
       count_launch();
     } else {
@@ -1076,7 +1091,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
       ff.in = a->S1;
       ff.out = a->B1;
       kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1, a->B1, fdlo, fdn, a->err, fl);
-      kf_floor_fixup<FFLOOR_FILL><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+      kf_floor_fixup<FFLOOR_FILL><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
       count_launch();
       kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[1],
                                             a->d_ib0, a->B1);
@@ -1091,7 +1106,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
       ff.B = a->B1;
       ff.S_old = a->S1_old;
       ff.bits = fbits;
-      kf_floor_fixup<FFLOOR_MOL2><<<1, 1024, 0, st>>>(F, P, fl, ff, a->err);
+      kf_floor_fixup<FFLOOR_MOL2><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
       count_launch();
       count_launch(2);
     }
@@ -1101,7 +1116,7 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   k_coarse_raw<<<gv0, kBlk, 0, st>>>(Lc, P, CM, R, F, a->S1, a->S0, fl);
   fa.in = a->S0;
   fa.out = a->S0;
-  k_floor_fixup<FLOOR_INPLACE><<<1, 1024, 0, st>>>(Lc, P, fl, fa, a->err);
+  k_floor_fixup<FLOOR_INPLACE><<<1, 1024, kFloorSmem, st>>>(Lc, P, fl, fa, a->err);
   k_coarse_finish<<<gv0, kBlk, 0, st>>>(Lc, P, a->S0, a->bits0, a->err);
   count_launch(3);
   return cudaGetLastError();
@@ -1167,6 +1182,7 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
           cmap[c] = b;
         }
   }
+  if (kf_floor_prepare() != cudaSuccess) return CAMR_ERR_CUDA;
   camr_amr* a = new (std::nothrow) camr_amr();
   if (!a) return CAMR_ERR_NOMEM;
   a->hp = *p;

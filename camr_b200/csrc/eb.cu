@@ -1798,11 +1798,11 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   fa.in = lev->S;
   fa.out = lev->S_old;
   k_ebl_clean_copy<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->S_old, lev->err, fl);
-  k_floor_fixup<FLOOR_CLEAN><<<1, 1024, 0, st>>>(L, lev->P, fl, fa, lev->err);
+  k_floor_fixup<FLOOR_CLEAN><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, fa, lev->err);
   fa.in = lev->S_old;
   fa.out = lev->B;
   k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S_old, lev->B, lev->err, fl);
-  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(L, lev->P, fl, fa, lev->err);
+  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, fa, lev->err);
   nk += 5;
   cudaError_t e = eb_hydro_stage(lev, st, &nk);
   if (e != cudaSuccess) return e;
@@ -1817,7 +1817,7 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   if (!lev->hp.do_mol) {
     k_ebl_update_ctu<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old,
                                           lev->dsdt, lev->S, lev->bits, lev->err, fl);
-    k_floor_fixup<FLOOR_DSDT_CTU><<<1, 1024, 0, st>>>(L, lev->P, fl, fu, lev->err);
+    k_floor_fixup<FLOOR_DSDT_CTU><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, fu, lev->err);
     count_launch(nk + 2);
     return cudaGetLastError();
   }
@@ -1827,13 +1827,13 @@ cudaError_t eb_issue_step(camr_eb_level* lev, bool first, const double* fixed_de
   fa.in = lev->S;
   fa.out = lev->B;
   k_ebl_expand<<<gp, kBlk, 0, st>>>(L, lev->P, G, lev->S, lev->B, lev->err, fl);
-  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(L, lev->P, fl, fa, lev->err);
+  k_floor_fixup<FLOOR_EXPAND><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, fa, lev->err);
   nk += 3;
   e = eb_hydro_stage(lev, st, &nk);
   if (e != cudaSuccess) return e;
   k_ebl_update2<<<gv, kBlk, 0, st>>>(L, lev->P, G, lev->dt_cur, lev->B, lev->S_old, lev->dsdt,
                                      lev->S, lev->bits, lev->err, fl);
-  k_floor_fixup<FLOOR_DSDT_MOL2><<<1, 1024, 0, st>>>(L, lev->P, fl, fu, lev->err);
+  k_floor_fixup<FLOOR_DSDT_MOL2><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, fu, lev->err);
   nk += 2;
   count_launch(nk);
   return cudaGetLastError();
@@ -1867,6 +1867,7 @@ camr_status camr_eb_level_create(const camr_level_desc* desc, const camr_eb_geom
   if (!desc || !eb || !p || !out) return CAMR_ERR_INVALID;
   *out = nullptr;
   if (p->riemann_solver != 0) return CAMR_ERR_UNSUPPORTED;
+  if (floor_prepare() != cudaSuccess) return CAMR_ERR_CUDA;
   // Godunov with EB is PLM only (Source/CAMR.cpp:186-190); its predictor
   // sources are taken as zero, so no gravity with Godunov
   if (!p->do_mol && p->ppm_type != 0) return CAMR_ERR_INVALID;

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kFB) k_fab_floor_list(FabSet S, KParams P, Flo
 __global__ void __launch_bounds__(1024) k_fab_floor_walk(FabSet S, KParams P, FloorList fl,
                                                           DevError* err) {
   constexpr int64_t kMask = (int64_t(1) << 40) - 1;
-  __shared__ int64_t key[kFloorCap];
+  extern __shared__ int64_t key[];
   const int n = *fl.count;
   if (n == 0) return;
   if (n > kFloorCap) {
@@ -463,9 +463,12 @@ camr_status camr_clean_state_parts(const camr_geom* geom, int nbox, const camr_b
                         (boxes[b].hi[2] - boxes[b].lo[2] + 1);
       mv = c > mv ? c : mv;
     }
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&k_fab_floor_walk),
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFloorSmem));
     if (e == cudaSuccess) {
       k_fab_floor_list<<<fab_grid(S, mv), kFB, 0, st>>>(S, P, fl);
-      k_fab_floor_walk<<<1, 1024, 0, st>>>(S, P, fl, err);
+      k_fab_floor_walk<<<1, 1024, kFloorSmem, st>>>(S, P, fl, err);
       k_fab_normalize<<<fab_grid(S, mx), kFB, 0, st>>>(S);
       count_launch(3);
     }

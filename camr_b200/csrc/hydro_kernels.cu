@@ -36,6 +36,10 @@ constexpr int kBlock = 128;
 // 22.5 ms for the fused faces against 6.5 + 13.6 ms for slopes + faces, so
 // the default keeps the two kernels: the column walks of the y- and z-faces
 // give each thread a long serial chain and fewer threads to hide it.
+// 2: only the x-faces fused (row tiles), y and z as the two kernels: the
+// fused x pass took 7.8 ms per step against about 6.6 ms for the x share of
+// the two kernels (MOL level 28.2 against 26.7 ms), so the fusion loses
+// even without the column walks.
 #ifndef CAMR_MOLFUSE
 #define CAMR_MOLFUSE 0
 #endif
@@ -880,10 +884,10 @@ __global__ void __launch_bounds__(kF23Threads, 2) k_flux23(Space s, KGeom g, KPa
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Region r2, Space s,
                                                        KParams P, const double* q,
-                                                       Ptr3 slope) {
+                                                       Ptr3 slope, int dbase) {
   int i, j, k;
   const int64_t t = gtid();
-  switch (blockIdx.y) {
+  switch (int(blockIdx.y) + dbase) {
     case 0:
       if (region_cell(r0, t, i, j, k)) mol_slope_body<0>(i, j, k, s, P, q, slope.p[0]);
       break;
@@ -913,10 +917,10 @@ __global__ void __launch_bounds__(kBlock, CAMR_MINB_MOLFLUX) k_mol_flux(Region r
                                                       KGeom g, KParams P, const double* q,
                                                       Ptr3 slope, const double* divu,
                                                       DFab uin, DFab fx, DFab fy, DFab fz,
-                                                      Ptr3 qf, Metrics M) {
+                                                      Ptr3 qf, Metrics M, int dbase) {
   int i, j, k;
   const int64_t t = gtid();
-  switch (blockIdx.y) {
+  switch (int(blockIdx.y) + dbase) {
     case 0:
       if (region_cell(r0, t, i, j, k))
         mol_flux_body<0, MET>(i, j, k, s, g, P, q, slope.p[0], divu, uin, fx, qf.p[0], &M);
@@ -1563,7 +1567,7 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       ms = (rs[d].count() > ms) ? rs[d].count() : ms;
       mb = (rb[d].count() > mb) ? rb[d].count() : mb;
     }
-    if (CAMR_MOLFUSE && !L.M.on && !L.keep_slopes) {
+    if (CAMR_MOLFUSE == 1 && !L.M.on && !L.keep_slopes) {
       // slopes, edge states and faces fused (k_mol_fx / fy / fz)
       const int nb[3] = {g.hi[0] - g.lo[0] + 1, g.hi[1] - g.lo[1] + 1, g.hi[2] - g.lo[2] + 1};
       mark("mol_faces");
@@ -1599,18 +1603,30 @@ cudaError_t launch_hydro_fluxes(const HydroLaunch& L, const Work& w, cudaStream_
       count_launch(2);
       return cudaGetLastError();
     }
+    int dbase = 0;
+    if (CAMR_MOLFUSE == 2 && !L.M.on && !L.keep_slopes) {
+      // x-faces fused by row tiles (k_mol_fx), y and z as two passes
+      const int nx = g.hi[0] - g.lo[0] + 1;
+      mark("mol_fx");
+      k_mol_fx<<<dim3(unsigned((nx + 1 + kMolRow - 2) / (kMolRow - 1)), unsigned(g.hi[1] - g.lo[1] + 1),
+                      unsigned(g.hi[2] - g.lo[2] + 1)),
+                 kMolRow, 0, st>>>(s, g, L.P, w.q, w.divu, L.uin, L.flx[0], qf.p[0]);
+      count_launch();
+      dbase = 1;
+    }
     Ptr3 sl{{w.slope[0], w.slope[1], w.slope[2]}};
     mark("mol_slope");
-    k_mol_slope<<<dim3(grid_for(ms), 3), kBlock, 0, st>>>(rs[0], rs[1], rs[2], s, L.P, w.q, sl);
+    k_mol_slope<<<dim3(grid_for(ms), 3 - dbase), kBlock, 0, st>>>(rs[0], rs[1], rs[2], s, L.P,
+                                                                   w.q, sl, dbase);
     mark("mol_flux");
     if (L.M.on)
-      k_mol_flux<true><<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(
+      k_mol_flux<true><<<dim3(grid_for(mb), 3 - dbase), kBlock, 0, st>>>(
           rb[0], rb[1], rb[2], s, g, L.P, w.q, sl, w.divu, L.uin, L.flx[0], L.flx[1], L.flx[2], qf,
-          L.M);
+          L.M, dbase);
     else
-      k_mol_flux<false><<<dim3(grid_for(mb), 3), kBlock, 0, st>>>(
+      k_mol_flux<false><<<dim3(grid_for(mb), 3 - dbase), kBlock, 0, st>>>(
           rb[0], rb[1], rb[2], s, g, L.P, w.q, sl, w.divu, L.uin, L.flx[0], L.flx[1], L.flx[2], qf,
-          L.M);
+          L.M, dbase);
     count_launch(2);
   }
   return cudaGetLastError();

@@ -262,6 +262,7 @@ camr_status camr_level_create(const camr_level_desc* desc, const camr_hydro_para
   if (!desc || !out) return CAMR_ERR_INVALID;
   camr_status cs = check_params(p);
   if (cs != CAMR_OK) return cs;
+  if (floor_prepare() != cudaSuccess) return CAMR_ERR_CUDA;
   camr_level* lev = new (std::nothrow) camr_level();
   if (!lev) return CAMR_ERR_NOMEM;
   lev->hp = *p;
@@ -484,10 +485,10 @@ static cudaError_t issue_step(camr_level* lev, bool first, const double* fixed_d
   const FloorList& fl = lev->floor;
   auto fixup = [&](int mode, FloorArgs a) {
     switch (mode) {
-      case FLOOR_CLEAN: k_floor_fixup<FLOOR_CLEAN><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
-      case FLOOR_EXPAND: k_floor_fixup<FLOOR_EXPAND><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
-      case FLOOR_CTU: k_floor_fixup<FLOOR_CTU><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
-      default: k_floor_fixup<FLOOR_MOL2><<<1, 1024, 0, st>>>(L, lev->P, fl, a, S.err); break;
+      case FLOOR_CLEAN: k_floor_fixup<FLOOR_CLEAN><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, a, S.err); break;
+      case FLOOR_EXPAND: k_floor_fixup<FLOOR_EXPAND><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, a, S.err); break;
+      case FLOOR_CTU: k_floor_fixup<FLOOR_CTU><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, a, S.err); break;
+      default: k_floor_fixup<FLOOR_MOL2><<<1, 1024, kFloorSmem, st>>>(L, lev->P, fl, a, S.err); break;
     }
     count_launch();
   };

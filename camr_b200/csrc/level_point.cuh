@@ -256,7 +256,10 @@ __device__ __forceinline__ bool valid_cell(const LGeom& L, int64_t t, int& i, in
 // count == nullptr: no list; the pass then resets from the neighbours'
 // values before the reset (exact when no two flagged cells are neighbours)
 // and an update pass reports the crossing in the error word.
-constexpr int kFloorCap = 4096;
+constexpr int kFloorCap = 16384;
+// The fixups sort the list in dynamic shared memory (above the 48 KB
+// default: floor_prepare / kf_floor_prepare raise each kernel's limit).
+constexpr size_t kFloorSmem = sizeof(int64_t) * kFloorCap;
 struct FloorList {
   int* count = nullptr;        // cells appended by the current pass (reset by the fixup)
   int64_t* cells = nullptr;    // their padded-array indices (kFloorCap)
@@ -886,7 +889,7 @@ struct LevelFloorPolicy {
 template <int MODE>
 __global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorList fl,
                                                        FloorArgs a, DevError* err) {
-  __shared__ int64_t key[kFloorCap];
+  extern __shared__ int64_t key[];
   const int n = *fl.count;
   if (n == 0) return;
   if (n > kFloorCap) {
@@ -957,6 +960,23 @@ __global__ void __launch_bounds__(1024) k_floor_fixup(LGeom L, KParams P, FloorL
     if (fl.total) atomicAdd(fl.total, (unsigned long long)n);
     *fl.count = 0;
   }
+}
+
+// Allow the fixups of this translation unit their dynamic shared memory.
+inline cudaError_t floor_prepare() {
+  const void* f[] = {reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_CLEAN>),
+                     reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_EXPAND>),
+                     reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_CTU>),
+                     reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_MOL2>),
+                     reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_DSDT_CTU>),
+                     reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_DSDT_MOL2>),
+                     reinterpret_cast<const void*>(&k_floor_fixup<FLOOR_INPLACE>)};
+  for (const void* k : f) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFloorSmem));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 struct DtCtl {

@@ -112,7 +112,7 @@ typedef struct {
                     3 density exactly zero in enforce_min_density, 4 index
                     out of range, 5 density below small_dens left unreset
                     (more cells below the floor in one pass than the reset
-                    list holds: 4096) */
+                    list holds: 16384) */
   int i, j, k;   /* cell of the first failure */
 } camr_error_info;
 
@@ -191,7 +191,7 @@ camr_status camr_fill_ghosts(const camr_geom* geom, int nbox, const camr_box_fab
 /* clean_state (Source/CAMR.cpp:1253-1262) of the boxes with ng ghost
  * layers: enforce_min_density on the valid cells (box by box in raster
  * order, each reset seen by the cells after it, as the reference's loop;
- * at most 4096 cells below the floor per call, else error code 5),
+ * at most 16384 cells below the floor per call, else error code 5),
  * normalize_species on the valid cells, its FillBoundary of the interior
  * and periodic ghost cells, then computeTemp on every cell of the grown
  * boxes.  Errors go to the library's error word (camr_get_error). */
@@ -366,7 +366,7 @@ camr_status camr_level_get_error(camr_level* lev, camr_error_info* info);
  * (synchronises the level's stream).  Each cleaning pass of a step lists
  * the cells below small_dens and resets them in the reference's order: box
  * by box, in raster order, each reset visible to the cells after it.  At
- * most 4096 cells per pass; more set error code 5. */
+ * most 16384 cells per pass; more set error code 5. */
 camr_status camr_level_floor_resets(camr_level* lev, int64_t* cells);
 
 /* ---------------------------------------------------------------------
@@ -424,7 +424,7 @@ camr_status camr_amr_restart(camr_amr* a, const double clock[4], int steps_done)
  * cells below small_dens and resets them in the reference's order, each
  * box of a level its own window (the fine boxes, the base level's
  * max_grid_size boxes); post_timestep's clean of level 0 follows reflux and
- * avgDown.  At most 4096 cells per pass; more set error code 5. */
+ * avgDown.  At most 16384 cells per pass; more set error code 5. */
 camr_status camr_amr_floor_resets(camr_amr* a, int64_t* cells);
 
 /* Autotune the fine level's batched hydro on its current state (after at

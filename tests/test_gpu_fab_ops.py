@@ -79,14 +79,21 @@ def test_fill_ghosts_and_clean_state_match_expand_state(bcs, oracle_kind, native
         assert_bitwise(t.cpu().numpy(), want, f"box {lo}-{hi}")
 
 
-def test_clean_state_valid_cells_match_oracle(oracle_kind, native_lib):
+@pytest.mark.parametrize("n,mgs,frac", [((16, 16, 16), (8, 8, 8), None),
+                                        ((32, 32, 32), (16, 16, 16), 0.3)],
+                         ids=["small", "many_below_floor"])
+def test_clean_state_valid_cells_match_oracle(n, mgs, frac, oracle_kind, native_lib):
     """clean_state of a MultiFab without ghost cells (the reference's
-    clean_state(S_old) at the start of CAMR_advance)."""
+    clean_state(S_old) at the start of CAMR_advance).  many_below_floor: the
+    floor is the density's 30th percentile, ~9800 cells below it in one
+    pass (more than 4096: the fixup's list and its shared-memory sort hold
+    16384)."""
     torch = _torch()
-    n = (16, 16, 16)
-    mgs = (8, 8, 8)
-    cfg = dict(do_mol=1, cfl=0.3, small_dens=0.9)
     s = P.random_smooth(n, seed=29)
+    small = 0.9 if frac is None else float(np.quantile(s[P.URHO], frac))
+    cfg = dict(do_mol=1, cfl=0.3, small_dens=small)
+    if frac is not None:
+        assert (s[P.URHO] < small).sum() > 4096
     lev = oracle.make_level(n, max_grid_size=mgs)
     ref = s.copy()
     oracle.clean_state(oracle_kind, oracle.default_params(**cfg), lev, ref)
