@@ -4,6 +4,7 @@
 #pragma once
 
 #include "hydro_point.cuh"
+#include "rndiv.h"
 
 namespace camr {
 
@@ -219,12 +220,43 @@ __device__ __forceinline__ void mol_slope_compute(int64_t at, const Space& s, co
   constexpr int t1 = (d == 0) ? SQ_V : SQ_U;
   constexpr int t2 = (d == 2) ? SQ_V : SQ_W;
   const double c = Q(0, SQ_C);
-  double dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
-  double drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c - 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
-  o[SL_0] = mol_limiter(dlft, drgt, plm_theta);
   const double cs2 = c * c;
-  dlft = 0.5 * (Q(0, SQ_P) - Q(-1, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
-  drgt = 0.5 * (Q(1, SQ_P) - Q(0, SQ_P)) / c + 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
+  const double dpl = Q(0, SQ_P) - Q(-1, SQ_P);
+  const double dpr = Q(1, SQ_P) - Q(0, SQ_P);
+  const double enth = (Q(0, SQ_REINT) + Q(0, SQ_P)) / dmax(Q(0, SQ_RHO), P.small_dens);
+  // the reference's quotients by c (2) and by c^2 (8); with every operand
+  // in range they come from the two reciprocals (rn_div_unchecked, the
+  // same bits as the divisions), else from the divisions
+  const double nc[2] = {0.5 * dpl, 0.5 * dpr};
+  double ns[2 + 2 * NSPEC];
+  ns[0] = enth * dpl;
+  ns[1] = enth * dpr;
+#pragma unroll
+  for (int sp = 0; sp < NSPEC; ++sp) {
+    ns[2 + 2 * sp] = Q(0, SQ_FS + sp) * dpl;
+    ns[3 + 2 * sp] = Q(0, SQ_FS + sp) * dpr;
+  }
+  bool ok = rd_in_range(c) & rd_in_range(cs2) & rd_in_range(nc[0]) & rd_in_range(nc[1]);
+#pragma unroll
+  for (int m = 0; m < 2 + 2 * NSPEC; ++m) ok = ok & rd_in_range(ns[m]);
+  double qc[2], qs[2 + 2 * NSPEC];
+  if (ok) {
+    const double ic = 1.0 / c, ics2 = 1.0 / cs2;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) qc[m] = rn_div_unchecked(nc[m], c, ic);
+#pragma unroll
+    for (int m = 0; m < 2 + 2 * NSPEC; ++m) qs[m] = rn_div_unchecked(ns[m], cs2, ics2);
+  } else {
+#pragma unroll
+    for (int m = 0; m < 2; ++m) qc[m] = nc[m] / c;
+#pragma unroll
+    for (int m = 0; m < 2 + 2 * NSPEC; ++m) qs[m] = ns[m] / cs2;
+  }
+  double dlft = qc[0] - 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
+  double drgt = qc[1] - 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
+  o[SL_0] = mol_limiter(dlft, drgt, plm_theta);
+  dlft = qc[0] + 0.5 * Q(0, SQ_RHO) * (Q(0, un) - Q(-1, un));
+  drgt = qc[1] + 0.5 * Q(0, SQ_RHO) * (Q(1, un) - Q(0, un));
   o[SL_2] = mol_limiter(dlft, drgt, plm_theta);
   dlft = Q(0, t1) - Q(-1, t1);
   drgt = Q(1, t1) - Q(0, t1);
@@ -232,15 +264,14 @@ __device__ __forceinline__ void mol_slope_compute(int64_t at, const Space& s, co
   dlft = Q(0, t2) - Q(-1, t2);
   drgt = Q(1, t2) - Q(0, t2);
   o[SL_4] = mol_limiter(dlft, drgt, plm_theta);
-  const double enth = (Q(0, SQ_REINT) + Q(0, SQ_P)) / dmax(Q(0, SQ_RHO), P.small_dens);
-  dlft = (Q(0, SQ_REINT) - Q(-1, SQ_REINT)) - enth * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
-  drgt = (Q(1, SQ_REINT) - Q(0, SQ_REINT)) - enth * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
+  dlft = (Q(0, SQ_REINT) - Q(-1, SQ_REINT)) - qs[0];
+  drgt = (Q(1, SQ_REINT) - Q(0, SQ_REINT)) - qs[1];
   o[SL_RE] = mol_limiter(dlft, drgt, plm_theta);
 #pragma unroll
   for (int sp = 0; sp < NSPEC; ++sp) {
     const int n = SQ_FS + sp;
-    dlft = Q(0, SQ_RHO) * Q(0, n) - Q(-1, SQ_RHO) * Q(-1, n) - Q(0, n) * (Q(0, SQ_P) - Q(-1, SQ_P)) / cs2;
-    drgt = Q(1, SQ_RHO) * Q(1, n) - Q(0, SQ_RHO) * Q(0, n) - Q(0, n) * (Q(1, SQ_P) - Q(0, SQ_P)) / cs2;
+    dlft = Q(0, SQ_RHO) * Q(0, n) - Q(-1, SQ_RHO) * Q(-1, n) - qs[2 + 2 * sp];
+    drgt = Q(1, SQ_RHO) * Q(1, n) - Q(0, SQ_RHO) * Q(0, n) - qs[3 + 2 * sp];
     o[SL_FS + sp] = mol_limiter(dlft, drgt, plm_theta);
   }
 }
@@ -282,11 +313,18 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
     ql[ES_U + d] = Q(atL, un) + 0.5 * ((d2 - d0) / Q(atL, SQ_RHO));
     ql[ES_U + (t1 - SQ_U)] = Q(atL, t1) + 0.5 * S(atL, SL_3);
     ql[ES_U + (t2 - SQ_U)] = Q(atL, t2) + 0.5 * S(atL, SL_4);
+    // the four quotients by cspeed, then the three by sum, each group from
+    // one reciprocal (rn_div_group: the same bits as the divisions)
+    double nq[NSPEC + 1], qq[NSPEC + 1];
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) nq[sp] = Q(atL, SQ_FS + sp) * (d0 + d2);
+    nq[NSPEC] = enth * (d0 + d2);
+    rn_div_group<NSPEC + 1>(nq, cspeed, qq);
     double sum = 0.;
 #pragma unroll
     for (int sp = 0; sp < NSPEC; ++sp) {
       const double specden = Q(atL, SQ_RHO) * Q(atL, SQ_FS + sp) +
-                             0.5 * (S(atL, SL_FS + sp) + Q(atL, SQ_FS + sp) * (d0 + d2) / cspeed);
+                             0.5 * (S(atL, SL_FS + sp) + qq[sp]);
       sum += specden;
       ql[ES_FS + sp] = specden;
     }
@@ -296,11 +334,13 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
 #pragma unroll
       for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = Q(at, SQ_FS + sp);
     } else {
+      double ys[NSPEC];
+      rn_div_group<NSPEC>(ql + ES_FS, sum, ys);
 #pragma unroll
-      for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = ql[ES_FS + sp] / sum;
+      for (int sp = 0; sp < NSPEC; ++sp) ql[ES_FS + sp] = ys[sp];
     }
     ql[ES_RHO] = dmax(sum, P.small_dens);
-    ql[ES_REINT] = Q(atL, SQ_REINT) + 0.5 * (S(atL, SL_RE) + enth * (d0 + d2) / cspeed);
+    ql[ES_REINT] = Q(atL, SQ_REINT) + 0.5 * (S(atL, SL_RE) + qq[NSPEC]);
   }
   {
     const double cspeed = Q(at, SQ_C);
@@ -311,11 +351,16 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
     qr[ES_U + d] = Q(at, un) - 0.5 * ((d2 - d0) / Q(at, SQ_RHO));
     qr[ES_U + (t1 - SQ_U)] = Q(at, t1) - 0.5 * S(at, SL_3);
     qr[ES_U + (t2 - SQ_U)] = Q(at, t2) - 0.5 * S(at, SL_4);
+    double nq[NSPEC + 1], qq[NSPEC + 1];
+#pragma unroll
+    for (int sp = 0; sp < NSPEC; ++sp) nq[sp] = Q(at, SQ_FS + sp) * (d0 + d2);
+    nq[NSPEC] = enth * (d0 + d2);
+    rn_div_group<NSPEC + 1>(nq, cspeed, qq);
     double sum = 0.;
 #pragma unroll
     for (int sp = 0; sp < NSPEC; ++sp) {
       const double specden = Q(at, SQ_RHO) * Q(at, SQ_FS + sp) -
-                             0.5 * (S(at, SL_FS + sp) + Q(at, SQ_FS + sp) * (d0 + d2) / cspeed);
+                             0.5 * (S(at, SL_FS + sp) + qq[sp]);
       sum += specden;
       qr[ES_FS + sp] = specden;
     }
@@ -323,11 +368,13 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
 #pragma unroll
       for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = Q(at, SQ_FS + sp);
     } else {
+      double ys[NSPEC];
+      rn_div_group<NSPEC>(qr + ES_FS, sum, ys);
 #pragma unroll
-      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = qr[ES_FS + sp] / sum;
+      for (int sp = 0; sp < NSPEC; ++sp) qr[ES_FS + sp] = ys[sp];
     }
     qr[ES_RHO] = dmax(sum, P.small_dens);
-    qr[ES_REINT] = Q(at, SQ_REINT) - 0.5 * (S(at, SL_RE) + enth * (d0 + d2) / cspeed);
+    qr[ES_REINT] = Q(at, SQ_REINT) - 0.5 * (S(at, SL_RE) + qq[NSPEC]);
   }
   const CellAux aL = load_aux(q, s, atL, P.gamma);
   const CellAux aR = load_aux(q, s, at, P.gamma);

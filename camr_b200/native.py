@@ -115,6 +115,7 @@ SIGNATURES = {
     "camr_amr_restart": (C.c_int, [C.c_void_p, C.POINTER(C.c_double * 4), C.c_int]),
     "camr_eb_level_floor_resets": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "camr_amr_floor_resets": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "camr_check_rn_div": (C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64), C.c_void_p]),
     "camr_write_checkpoint": (C.c_int, [C.c_char_p, C.POINTER(Geom), C.POINTER(C.c_double * 3),
                                         C.POINTER(C.c_double * 2), C.POINTER(C.c_double * 2),
                                         C.POINTER(C.c_int * 2), C.c_int, C.c_void_p,

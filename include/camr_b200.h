@@ -660,6 +660,13 @@ const char* camr_last_error_string(void);
  * chains (a roofline denominator); synchronises.  Result in TFLOP/s. */
 camr_status camr_measure_fp64_peak(double* tflops, void* stream);
 
+/* Check the kernels' shared-reciprocal quotient (a / b from RN(1/b) with
+ * fused multiply-add corrections) against the device's IEEE division on
+ * about 5 n operand pairs (random, next to rounding midpoints, integer
+ * ratios, special values); *mismatches counts the pairs whose bits differ
+ * (synchronises). */
+camr_status camr_check_rn_div(int64_t n, uint64_t seed, int64_t* mismatches, void* stream);
+
 /* Kernel launches issued by the library so far (for accounting; graph
  * replays count the kernels they contain). */
 int64_t camr_launch_count(void);
