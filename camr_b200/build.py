@@ -14,7 +14,7 @@ OUT = os.path.join(HERE, "_lib", "libcamr_b200.so")
 SOURCES = ["hydro_kernels.cu", "level.cu", "peak.cu", "noalloc.cu", "batch.cu", "amr.cu",
            "adjoint.cu", "eb.cu", "fab_ops.cu", "io.cpp"]
 HEADERS = ["camr_common.cuh", "hydro_point.cuh", "hydro_kernels.cuh", "level_point.cuh",
-           "adjoint_point.cuh", "cell_point.cuh", "fastdiv.h"]
+           "adjoint_point.cuh", "cell_point.cuh", "fastdiv.h", "rndiv.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

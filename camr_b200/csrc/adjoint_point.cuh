@@ -21,6 +21,8 @@
 
 #include <cmath>
 
+#include "rndiv.h"
+
 #ifdef __CUDACC__
 #define CAMR_HD __host__ __device__ __forceinline__
 #else
@@ -397,20 +399,28 @@ CAMR_HD void edge_fwd(const double* q, const double* s, const double* yq, double
     e.t1 = q[t1] - 0.5 * s[S3];
     e.t2 = q[t2] - 0.5 * s[S4];
   }
+  // the quotients by c (NSP + 1) and by the sum (NSP), each group from
+  // one reciprocal (rn_div_group: the same bits as the divisions)
+  double nq[NSP + 1], qq[NSP + 1];
+  for (int sp = 0; sp < NSP; ++sp) nq[sp] = q[QY + sp] * t.a;
+  nq[NSP] = t.enth * t.a;
+  rn_div_group<NSP + 1>(nq, c, qq);
   double sum = 0.;
   for (int sp = 0; sp < NSP; ++sp) {
     if (sign > 0)
-      t.sd[sp] = q[QR] * q[QY + sp] + 0.5 * (s[SY + sp] + q[QY + sp] * t.a / c);
+      t.sd[sp] = q[QR] * q[QY + sp] + 0.5 * (s[SY + sp] + qq[sp]);
     else
-      t.sd[sp] = q[QR] * q[QY + sp] - 0.5 * (s[SY + sp] + q[QY + sp] * t.a / c);
+      t.sd[sp] = q[QR] * q[QY + sp] - 0.5 * (s[SY + sp] + qq[sp]);
     sum += t.sd[sp];
   }
   t.sum = sum;
   t.fallback = sum < P.small_dens;
-  for (int sp = 0; sp < NSP; ++sp) e.y[sp] = t.fallback ? yq[sp] : t.sd[sp] / sum;
+  double ys[NSP];
+  rn_div_group<NSP>(t.sd, sum, ys);
+  for (int sp = 0; sp < NSP; ++sp) e.y[sp] = t.fallback ? yq[sp] : ys[sp];
   e.rho = hmax(sum, P.small_dens);
-  if (sign > 0) e.re = q[QRE] + 0.5 * (s[SRE] + t.enth * t.a / c);
-  else e.re = q[QRE] - 0.5 * (s[SRE] + t.enth * t.a / c);
+  if (sign > 0) e.re = q[QRE] + 0.5 * (s[SRE] + qq[NSP]);
+  else e.re = q[QRE] - 0.5 * (s[SRE] + qq[NSP]);
 }
 
 // VJP of edge_fwd: accumulates into bq, bs (this cell) and byq (the cell
@@ -675,24 +685,38 @@ CAMR_HD void slope_fwd(const double* qm, const double* q0, const double* qp, con
   constexpr int t1 = (d == 0) ? QV : QU;
   constexpr int t2 = (d == 2) ? QV : QW;
   const double c = q0[QC];
-  double dl = 0.5 * (q0[QP] - qm[QP]) / c - 0.5 * q0[QR] * (q0[un] - qm[un]);
-  double dr = 0.5 * (qp[QP] - q0[QP]) / c - 0.5 * q0[QR] * (qp[un] - q0[un]);
-  o[S0] = limiter_fwd(dl, dr, t.lt[S0]);
   t.cs2 = c * c;
-  dl = 0.5 * (q0[QP] - qm[QP]) / c + 0.5 * q0[QR] * (q0[un] - qm[un]);
-  dr = 0.5 * (qp[QP] - q0[QP]) / c + 0.5 * q0[QR] * (qp[un] - q0[un]);
+  t.rden = hmax(q0[QR], P.small_dens);
+  t.enth = (q0[QRE] + q0[QP]) / t.rden;
+  const double dpl = q0[QP] - qm[QP], dpr = qp[QP] - q0[QP];
+  // the quotients by c (2) and by c^2 (2 + 2 NSP), each group from one
+  // reciprocal (rn_div_group: the same bits as the divisions)
+  const double nc[2] = {0.5 * dpl, 0.5 * dpr};
+  double qc[2];
+  rn_div_group<2>(nc, c, qc);
+  double ns[2 + 2 * NSP], qs[2 + 2 * NSP];
+  ns[0] = t.enth * dpl;
+  ns[1] = t.enth * dpr;
+  for (int sp = 0; sp < NSP; ++sp) {
+    ns[2 + 2 * sp] = q0[QY + sp] * dpl;
+    ns[3 + 2 * sp] = q0[QY + sp] * dpr;
+  }
+  rn_div_group<2 + 2 * NSP>(ns, t.cs2, qs);
+  double dl = qc[0] - 0.5 * q0[QR] * (q0[un] - qm[un]);
+  double dr = qc[1] - 0.5 * q0[QR] * (qp[un] - q0[un]);
+  o[S0] = limiter_fwd(dl, dr, t.lt[S0]);
+  dl = qc[0] + 0.5 * q0[QR] * (q0[un] - qm[un]);
+  dr = qc[1] + 0.5 * q0[QR] * (qp[un] - q0[un]);
   o[S2] = limiter_fwd(dl, dr, t.lt[S2]);
   o[S3] = limiter_fwd(q0[t1] - qm[t1], qp[t1] - q0[t1], t.lt[S3]);
   o[S4] = limiter_fwd(q0[t2] - qm[t2], qp[t2] - q0[t2], t.lt[S4]);
-  t.rden = hmax(q0[QR], P.small_dens);
-  t.enth = (q0[QRE] + q0[QP]) / t.rden;
-  dl = (q0[QRE] - qm[QRE]) - t.enth * (q0[QP] - qm[QP]) / t.cs2;
-  dr = (qp[QRE] - q0[QRE]) - t.enth * (qp[QP] - q0[QP]) / t.cs2;
+  dl = (q0[QRE] - qm[QRE]) - qs[0];
+  dr = (qp[QRE] - q0[QRE]) - qs[1];
   o[SRE] = limiter_fwd(dl, dr, t.lt[SRE]);
   for (int sp = 0; sp < NSP; ++sp) {
     const int n = QY + sp;
-    dl = q0[QR] * q0[n] - qm[QR] * qm[n] - q0[n] * (q0[QP] - qm[QP]) / t.cs2;
-    dr = qp[QR] * qp[n] - q0[QR] * q0[n] - q0[n] * (qp[QP] - q0[QP]) / t.cs2;
+    dl = q0[QR] * q0[n] - qm[QR] * qm[n] - qs[2 + 2 * sp];
+    dr = qp[QR] * qp[n] - q0[QR] * q0[n] - qs[3 + 2 * sp];
     o[SY + sp] = limiter_fwd(dl, dr, t.lt[SY + sp]);
   }
 }
