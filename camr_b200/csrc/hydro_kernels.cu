@@ -28,6 +28,13 @@ constexpr int kBlock = 128;
 #ifndef CAMR_MINB_MOLFLUX
 #define CAMR_MINB_MOLFLUX 1
 #endif
+// Resident blocks asked of the MOL slope kernel (0: none).  Measured on
+// B200 (256^3 MOL-PLM level): 8 (64 registers) 5.64 ms per step against
+// 5.47 unbounded (72 registers); with the faces at 6 blocks (80 registers)
+// as well, 5.86 + 12.75 against 5.47 + 12.17.
+#ifndef CAMR_MINB_MOLSLOPE
+#define CAMR_MINB_MOLSLOPE 0
+#endif
 #ifndef CAMR_MINB_FLUX3
 #define CAMR_MINB_FLUX3 4
 #endif
@@ -882,7 +889,12 @@ __global__ void __launch_bounds__(kF23Threads, 2) k_flux23(Space s, KGeom g, KPa
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_mol_slope(Region r0, Region r1, Region r2, Space s,
+#if CAMR_MINB_MOLSLOPE > 0
+#define CAMR_MOLSLOPE_BOUNDS __launch_bounds__(kBlock, CAMR_MINB_MOLSLOPE)
+#else
+#define CAMR_MOLSLOPE_BOUNDS __launch_bounds__(kBlock)
+#endif
+__global__ void CAMR_MOLSLOPE_BOUNDS k_mol_slope(Region r0, Region r1, Region r2, Space s,
                                                        KParams P, const double* q,
                                                        Ptr3 slope, int dbase) {
   int i, j, k;
