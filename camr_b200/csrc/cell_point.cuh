@@ -6,13 +6,6 @@
 #include "hydro_point.cuh"
 #include "rndiv.h"
 
-// 1: the MOL edge states divide by the cell density once (enth and the
-// normal-velocity term share its reciprocal when rho >= small_dens).
-// Measured on B200 (256^3 MOL-PLM level): faces 12.61 against 12.25 ms per
-// step without it (the extra branch costs more than the division), so off.
-#ifndef CAMR_RDIV_RHO
-#define CAMR_RDIV_RHO 0
-#endif
 
 namespace camr {
 
@@ -314,26 +307,11 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
   double ql[ES_N], qr[ES_N];
   {
     const double cspeed = Q(atL, SQ_C);
-    const double rho_c = Q(atL, SQ_RHO);
+    const double enth = (Q(atL, SQ_REINT) + Q(atL, SQ_P)) / dmax(Q(atL, SQ_RHO), P.small_dens);
     const double d0 = S(atL, SL_0), d2 = S(atL, SL_2);
     double pl = Q(atL, SQ_P) + 0.5 * (d0 + d2) * cspeed;
     ql[ES_P] = dmax(pl, P.small_pres);
-    // enth and the normal-velocity term: both divide by rho when rho is
-    // at or above small_dens (dmax then returns rho), one reciprocal
-    double enth, dun;
-    {
-      const double nr[2] = {Q(atL, SQ_REINT) + Q(atL, SQ_P), d2 - d0};
-      if (CAMR_RDIV_RHO && rho_c >= P.small_dens) {
-        double qr2[2];
-        rn_div_group<2>(nr, rho_c, qr2);
-        enth = qr2[0];
-        dun = qr2[1];
-      } else {
-        enth = nr[0] / dmax(rho_c, P.small_dens);
-        dun = nr[1] / rho_c;
-      }
-    }
-    ql[ES_U + d] = Q(atL, un) + 0.5 * dun;
+    ql[ES_U + d] = Q(atL, un) + 0.5 * ((d2 - d0) / Q(atL, SQ_RHO));
     ql[ES_U + (t1 - SQ_U)] = Q(atL, t1) + 0.5 * S(atL, SL_3);
     ql[ES_U + (t2 - SQ_U)] = Q(atL, t2) + 0.5 * S(atL, SL_4);
     // the four quotients by cspeed, then the three by sum, each group from
@@ -367,26 +345,11 @@ __device__ __forceinline__ void mol_edges_cmpflx(int i, int j, int k, const Spac
   }
   {
     const double cspeed = Q(at, SQ_C);
-    const double rho_c = Q(at, SQ_RHO);
+    const double enth = (Q(at, SQ_REINT) + Q(at, SQ_P)) / dmax(Q(at, SQ_RHO), P.small_dens);
     const double d0 = S(at, SL_0), d2 = S(at, SL_2);
     double pr = Q(at, SQ_P) - 0.5 * (d0 + d2) * cspeed;
     qr[ES_P] = dmax(pr, P.small_pres);
-    // enth and the normal-velocity term: both divide by rho when rho is
-    // at or above small_dens (dmax then returns rho), one reciprocal
-    double enth, dun;
-    {
-      const double nr[2] = {Q(at, SQ_REINT) + Q(at, SQ_P), d2 - d0};
-      if (CAMR_RDIV_RHO && rho_c >= P.small_dens) {
-        double qr2[2];
-        rn_div_group<2>(nr, rho_c, qr2);
-        enth = qr2[0];
-        dun = qr2[1];
-      } else {
-        enth = nr[0] / dmax(rho_c, P.small_dens);
-        dun = nr[1] / rho_c;
-      }
-    }
-    qr[ES_U + d] = Q(at, un) - 0.5 * dun;
+    qr[ES_U + d] = Q(at, un) - 0.5 * ((d2 - d0) / Q(at, SQ_RHO));
     qr[ES_U + (t1 - SQ_U)] = Q(at, t1) - 0.5 * S(at, SL_3);
     qr[ES_U + (t2 - SQ_U)] = Q(at, t2) - 0.5 * S(at, SL_4);
     double nq[NSPEC + 1], qq[NSPEC + 1];

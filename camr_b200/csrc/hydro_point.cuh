@@ -7,27 +7,6 @@
 #pragma once
 
 #include "camr_common.cuh"
-#include "rndiv.h"
-
-// 1: riemannus forms its two quotients by wl + wr from one reciprocal
-// (rn_div_group).  Measured on B200 (256^3 levels): 0.1 ms slower per step
-// for both CTU-PPM and MOL-PLM, so off.
-#ifndef CAMR_RDIV_RIEMANN
-#define CAMR_RDIV_RIEMANN 0
-#endif
-// 1: the transverse updates (transdo / transdd) form the velocity and
-// kinetic-energy quotients by the new density from one reciprocal.
-// Measured on B200 (256^3 CTU-PPM): flux2 9.22-9.29 against 9.01-9.15 ms
-// per step without it, so off.
-#ifndef CAMR_RDIV_TRANS
-#define CAMR_RDIV_TRANS 0
-#endif
-// 1: the PPM characteristic projection forms its two quotients by the
-// reference sound speed squared from one reciprocal.  Measured: trace 5.17
-// against 5.07-5.11 ms per 256^3 step, so off.
-#ifndef CAMR_RDIV_PPM
-#define CAMR_RDIV_PPM 0
-#endif
 
 namespace camr {
 
@@ -56,20 +35,9 @@ __device__ __forceinline__ ROut riemannus(double rl_in, double ul, double vl, do
   const double pr = dmax(pr_in, small_pres);
   const double wl = dmax(wsmall, sqrt(fabs(gamcl * pl * rl)));
   const double wr = dmax(wsmall, sqrt(fabs(gamcr * pr * rr)));
-#if CAMR_RDIV_RIEMANN
-  // both quotients by wl + wr from one reciprocal (rn_div_group: the same
-  // bits as the divisions)
-  const double nw[2] = {(wr * pl + wl * pr) + wl * wr * (ul - ur), (wl * ul + wr * ur) + (pl - pr)};
-  double qw[2];
-  rn_div_group<2>(nw, wl + wr, qw);
-  double pstar = qw[0];
-  pstar = dmax(pstar, small_pres);
-  double ustar = qw[1];
-#else
   double pstar = ((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr);
   pstar = dmax(pstar, small_pres);
   double ustar = ((wl * ul + wr * ur) + (pl - pr)) / (wl + wr);
-#endif
   bool mask = fabs(ustar) < smallu * 0.5 * (fabs(ul) + fabs(ur));
   ustar = mask ? 0.0 : ustar;
   // upwind state (left, right, or the mean when ustar is exactly 0),
@@ -440,16 +408,7 @@ __device__ __forceinline__ void ppm_project(const Traced4& I, int wref, double g
   const double cc_ref = sqrt(gam_ref * p_ref / rho_ref);
   const double csq_ref = cc_ref * cc_ref;
   const double cc_ref_inv = 1.0 / cc_ref;
-  const double dptot0 = p_ref - I.p[1];
-  const double ncs[2] = {(p_ref + rhoe_g_ref) * rho_ref_inv, dptot0};
-  double qcs[2];
-#if CAMR_RDIV_PPM
-  rn_div_group<2>(ncs, csq_ref, qcs);  // both quotients by csq_ref
-#else
-  qcs[0] = ncs[0] / csq_ref;
-  qcs[1] = ncs[1] / csq_ref;
-#endif
-  const double h_g_ref = qcs[0];
+  const double h_g_ref = (p_ref + rhoe_g_ref) * rho_ref_inv / csq_ref;
   const double dum = un_ref - I.un[0];
   const double dptotm = p_ref - I.p[0];
   const double drho = rho_ref - I.rho[1];
@@ -459,7 +418,7 @@ __device__ __forceinline__ void ppm_project(const Traced4& I, int wref, double g
   const double dptotp = p_ref - I.p[2];
   double alpham = 0.5 * (dptotm * rho_ref_inv * cc_ref_inv - dum) * rho_ref * cc_ref_inv;
   double alphap = 0.5 * (dptotp * rho_ref_inv * cc_ref_inv + dup) * rho_ref * cc_ref_inv;
-  double alpha0r = drho - qcs[1];
+  double alpha0r = drho - dptot / csq_ref;
   double alpha0e_g = drhoe_g - dptot * h_g_ref;
   if (plus_state) {
     if (un - cc > 0.) alpham = 0.;
@@ -622,22 +581,10 @@ __device__ __forceinline__ void transdo_side(const TTerms& t, double c, const do
     reset_state = true;
   }
   out[ES_RHO] = rrnewr;
-#if CAMR_RDIV_TRANS
-  // the velocity and kinetic-energy quotients by rrnewr from one reciprocal
-  const double nv[4] = {runewr, rvnewr, rwnewr,
-                        0.5 * (runewr * runewr + rvnewr * rvnewr + rwnewr * rwnewr)};
-  double qv[4];
-  rn_div_group<4>(nv, rrnewr, qv);
-  out[ES_U] = qv[0];
-  out[ES_V] = qv[1];
-  out[ES_W] = qv[2];
-  const double rhoekinr = qv[3];
-#else
   out[ES_U] = runewr / rrnewr;
   out[ES_V] = rvnewr / rrnewr;
   out[ES_W] = rwnewr / rrnewr;
   const double rhoekinr = 0.5 * (runewr * runewr + rvnewr * rvnewr + rwnewr * rwnewr) / rrnewr;
-#endif
   out[ES_REINT] = renewr - rhoekinr;
   if (!reset_state) {
     const double pnewr = qn[ES_P] - cdtdx * (t.dAup + t.pav * t.dAu * (c - 1.0));
@@ -718,21 +665,10 @@ __device__ __forceinline__ void transdd_side(const TDTerms& t, const double* qn,
     reset_state = true;
   }
   out[ES_RHO] = rrnewr + hdt * srcq[ES_RHO];
-#if CAMR_RDIV_TRANS
-  const double nv[4] = {runewr, rvnewr, rwnewr,
-                        0.5 * (runewr * runewr + rvnewr * rvnewr + rwnewr * rwnewr)};
-  double qv[4];
-  rn_div_group<4>(nv, rrnewr, qv);
-  out[ES_U] = qv[0] + hdt * srcq[ES_U];
-  out[ES_V] = qv[1] + hdt * srcq[ES_V];
-  out[ES_W] = qv[2] + hdt * srcq[ES_W];
-  const double rhoekinr = qv[3];
-#else
   out[ES_U] = runewr / rrnewr + hdt * srcq[ES_U];
   out[ES_V] = rvnewr / rrnewr + hdt * srcq[ES_V];
   out[ES_W] = rwnewr / rrnewr + hdt * srcq[ES_W];
   const double rhoekinr = 0.5 * (runewr * runewr + rvnewr * rvnewr + rwnewr * rwnewr) / rrnewr;
-#endif
   out[ES_REINT] = renewr - rhoekinr + hdt * srcq[ES_REINT];
   double pout;
   if (!reset_state) {

@@ -138,13 +138,6 @@ __device__ __forceinline__ void compute_temp(double* s, const KParams& P) {
 }
 
 // normalize_species (Source/CAMR.cpp:884-905).
-// 1: normalize_species forms its three quotients by the sum from one
-// reciprocal.  Measured on B200 (256^3): the update kernels 2.10-2.11 ->
-// 2.14 ms (CTU), 2.19 -> 2.22 ms (MOL stage 2), so off.
-#ifndef CAMR_RDIV_NORM
-#define CAMR_RDIV_NORM 0
-#endif
-
 __device__ __forceinline__ void normalize_species(double* s) {
   double sum = 0.;
 #pragma unroll
@@ -154,16 +147,8 @@ __device__ __forceinline__ void normalize_species(double* s) {
   }
   if (s[URHO] > 0.) {
     sum /= s[URHO];
-#if CAMR_RDIV_NORM
-    // the three quotients by sum from one reciprocal (rn_div_group)
-    double y[NSPEC];
-    rn_div_group<NSPEC>(s + UFS, sum, y);
-#pragma unroll
-    for (int sp = 0; sp < NSPEC; ++sp) s[UFS + sp] = y[sp];
-#else
 #pragma unroll
     for (int sp = 0; sp < NSPEC; ++sp) s[UFS + sp] /= sum;
-#endif
   }
 }
 
