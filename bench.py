@@ -404,14 +404,18 @@ def run_camr(args, world, rank, local, pg):
     # in a run of that length
     e2e_steps = max(2, args.steps)
 
-    def e2e_run(overlap, src):
+    def e2e_run(overlap, src, up=True, step=True, down=True):
         torch.cuda.synchronize()
         e0.record(st)
         for _ in range(e2e_steps):
-            native.check(lib.camr_level_set_state(L._h, C.c_void_p(src.data_ptr()), 1), "set")
-            L.advance(1)
-            get = lib.camr_level_get_state_async if overlap else lib.camr_level_get_state
-            native.check(get(L._h, C.c_void_p(out.data_ptr()), 1), "get")
+            if up:
+                native.check(lib.camr_level_set_state(L._h, C.c_void_p(src.data_ptr()), 1),
+                             "set")
+            if step:
+                L.advance(1)
+            if down:
+                get = lib.camr_level_get_state_async if overlap else lib.camr_level_get_state
+                native.check(get(L._h, C.c_void_p(out.data_ptr()), 1), "get")
         native.check(lib.camr_level_sync(L._h), "sync")
         e1.record(st)
         torch.cuda.synchronize()
@@ -419,6 +423,12 @@ def run_camr(args, world, rank, local, pg):
 
     e2e_serial_ms = e2e_run(False, host)
     e2e_initial_ms = e2e_run(True, host0)
+    # the copy pipeline without the step (upload + unpack, pack + download,
+    # both directions at once), and each direction alone: the PCIe floor the
+    # end-to-end step sits on
+    copies_ms = e2e_run(True, host, step=False)
+    up_ms = e2e_run(True, host, step=False, down=False)
+    down_ms = e2e_run(True, host, up=False, step=False)
     e2e_ms = e2e_run(True, host)
     e2e_ms = max_over_ranks(e2e_ms, pg)
     state_bytes = host.numel() * 8
@@ -427,6 +437,10 @@ def run_camr(args, world, rank, local, pg):
            "ms_per_step": e2e_ms, "steps": e2e_steps,
            "ms_per_step_without_overlap": e2e_serial_ms,
            "ms_per_step_from_initial_state": e2e_initial_ms,
+           "ms_per_step_copies_only": copies_ms,
+           "ms_per_step_upload_only": up_ms, "ms_per_step_download_only": down_ms,
+           "pcie_gbs_upload_only": state_bytes / up_ms / 1e6,
+           "pcie_gbs_download_only": state_bytes / down_ms / 1e6,
            "input": "the state after the warm-up steps, uploaded every step",
            "timing": "CUDA events on the level's stream around the loop; the level's copy "
                      "streams are synchronised before the closing event"}
