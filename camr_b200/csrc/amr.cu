@@ -76,10 +76,23 @@ struct CoarseMap {
     for (int d = 0; d < 3; ++d) w[d] = ((((c[d] - dlo[d]) % n[d]) + n[d]) % n[d]);
     return w[0] + n[0] * (w[1] + n[1] * w[2]);
   }
+  // cell() of a cell inside the domain, without the periodic wrap
+  __device__ __forceinline__ int cell_in(int i, int j, int k) const {
+    return (i - dlo[0]) + n[0] * ((j - dlo[1]) + n[1] * (k - dlo[2]));
+  }
 };
 
 __device__ __forceinline__ int floordiv2(int v) { return (v >= 0) ? v / RR : -((-v + RR - 1) / RR); }
 __device__ __forceinline__ int wrapi(int v, int lo, int n) { return lo + (((v - lo) % n) + n) % n; }
+// wrapi without the divisions when v is less than one period outside
+// [lo, lo + n), as the coarse neighbours of a fine box's ghost shell are.
+__device__ __forceinline__ int wrap_near(int v, int lo, int n) {
+  int w = v - lo;
+  if (w < 0) w += n;
+  else if (w >= n) w -= n;
+  if (unsigned(w) >= unsigned(n)) w = ((w % n) + n) % n;
+  return lo + w;
+}
 
 __device__ __forceinline__ int box_of_block(const int64_t* b0, int nbox, int64_t blk) {
   int lo = 0, hi = nbox - 1;
@@ -193,9 +206,11 @@ __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap 
     if (s[URHO] < P.small_dens) floor_push(fl, (int64_t(b) << 40) | L.idx(i, j, k));
     enforce_min_density(s, sb, L, P, i, j, k, err);
   } else {
-    const int wi = wrapi(i, fdlo.x, fdn.x), wj = wrapi(j, fdlo.y, fdn.y),
-              wk = wrapi(k, fdlo.z, fdn.z);
-    const int ob = CM.cmap[CM.cell(floordiv2(wi), floordiv2(wj), floordiv2(wk))];
+    // a ghost cell lies at most NGROW cells outside its box, so within one
+    // period of the fine domain; its image's coarse parent is a domain cell
+    const int wi = wrap_near(i, fdlo.x, fdn.x), wj = wrap_near(j, fdlo.y, fdn.y),
+              wk = wrap_near(k, fdlo.z, fdn.z);
+    const int ob = CM.cmap[CM.cell_in(floordiv2(wi), floordiv2(wj), floordiv2(wk))];
     if (ob < 0) return;
     const LGeom& Lo = F.L[ob];
     const double* so = src + F.off[ob];
@@ -216,6 +231,12 @@ __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap 
 // children inside the neighbours' min/max, child = u + ox*sx + oy*sy + oz*sz
 // with o = -+1/4.  Then computeTemp on each child.
 // resident 256-thread blocks per SM asked of the coarse-to-fine interpolation
+// 1: the coarse-to-fine interpolation runs over a list of (coarse cell,
+// component) pairs (kf_interp_list); 0: one thread per coarse cell of each
+// box's grown shell walks the components (kf_interp).
+#ifndef CAMR_INTERP_LIST
+#define CAMR_INTERP_LIST 1
+#endif
 #ifndef CAMR_MINB_INTERP
 #define CAMR_MINB_INTERP 3
 #endif
@@ -296,6 +317,103 @@ __global__ void __launch_bounds__(kBlk, CAMR_MINB_INTERP) kf_interp(FineDev F, K
 #pragma unroll 1
   for (int q = 0; q < 8; ++q) {
     const int64_t at = at0 + (q & 1) * cstep[0] + ((q >> 1) & 1) * cstep[1] + (q >> 2) * cstep[2];
+    double s[NVAR];
+    load_cell(Bb, L, at, s);
+    compute_temp(s, P);
+    store_cell(Bb, L, at, s);
+  }
+}
+
+// The same interpolation spread over (coarse cell, component) pairs: the
+// coarse ghost cells to fill are listed once when the hierarchy is built
+// (box, coarse i, j, k, in kf_interp's order), a block takes kInterpItems
+// of them and one thread per (cell, component) gathers that component's 27
+// neighbours and writes its 8 children; after a barrier one thread per
+// child runs computeTemp.  Each value is computed by the arithmetic of
+// kf_interp, so the two give the same bits; this form has ten independent
+// gathers per cell in flight instead of one component after another.
+constexpr int kInterpItems = kBlk / NVAR;
+static_assert(kInterpItems * RR * RR * RR <= kBlk, "one thread per child");
+__global__ void __launch_bounds__(kBlk) kf_interp_list(FineDev F, KParams P, LGeom Lc,
+                                                        const double* c_old, const double* c_new,
+                                                        const CoarseT* ctp, const int4* items,
+                                                        int64_t nitems, double* B) {
+  const int slot = int(threadIdx.x) % kInterpItems;
+  const int n = int(threadIdx.x) / kInterpItems;
+  const int64_t first = int64_t(blockIdx.x) * kInterpItems;
+  const int64_t it = first + slot;
+  if (n < NVAR && it < nitems) {
+    const int4 c = items[it];
+    const int b = c.x, ci = c.y, cj = c.z, ck = c.w;
+    const LGeom& L = F.L[b];
+    const CoarseT ct = *ctp;
+    // the neighbours' periodic images (the indices coarse_at reads)
+    int w[3][3];
+    const int cc[3] = {ci, cj, ck};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int o = 0; o < 3; ++o) w[d][o] = wrap_near(cc[d] + o - 1, Lc.dlo[d], Lc.dhi[d] - Lc.dlo[d] + 1);
+    double v[27];
+#pragma unroll
+    for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+        for (int di = 0; di < 3; ++di) {
+          const int64_t at = Lc.idx(w[0][di], w[1][dj], w[2][dk]) + n * Lc.sn;
+          double x;
+          if (ct.mode == 0) x = c_new[at];
+          else if (ct.mode == 1) x = c_old[at];
+          else x = ct.alpha * c_old[at] + ct.beta * c_new[at];
+          v[dk * 9 + dj * 3 + di] = x;
+        }
+    const double uc = v[13];
+    const double up[3] = {v[14], v[16], v[22]};
+    const double um[3] = {v[12], v[10], v[4]};
+    double sl[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double dc = 0.5 * (up[d] - um[d]);
+      const double df = 2.0 * (up[d] - uc);
+      const double db = 2.0 * (uc - um[d]);
+      double sv = (df * db >= 0.0) ? dmin(fabs(df), fabs(db)) : 0.0;
+      sv = copysign(1.0, dc) * dmin(sv, fabs(dc));
+      sl[d] = sv;
+    }
+    double alpha = 1.0;
+    if (sl[0] != 0.0 || sl[1] != 0.0 || sl[2] != 0.0) {
+      const double dumax = fabs(sl[0]) * 0.25 + fabs(sl[1]) * 0.25 + fabs(sl[2]) * 0.25;
+      double umax = uc, umin = uc;
+#pragma unroll
+      for (int q = 0; q < 27; ++q) {
+        umax = dmax(umax, v[q]);
+        umin = dmin(umin, v[q]);
+      }
+      if (dumax * alpha > (umax - uc)) alpha = (umax - uc) / dumax;
+      if (dumax * alpha > (uc - umin)) alpha = (uc - umin) / dumax;
+    }
+    const double sa[3] = {sl[0] * alpha, sl[1] * alpha, sl[2] * alpha};
+    double* Bn = B + F.off[b] + L.idx(RR * ci, RR * cj, RR * ck) + int64_t(n) * L.sn;
+#pragma unroll
+    for (int kc = 0; kc < RR; ++kc)
+#pragma unroll
+      for (int jc = 0; jc < RR; ++jc)
+#pragma unroll
+        for (int ic = 0; ic < RR; ++ic) {
+          const double ox = ic ? 0.25 : -0.25, oy = jc ? 0.25 : -0.25, oz = kc ? 0.25 : -0.25;
+          Bn[ic + jc * L.sy + kc * L.sz] = uc + ox * sa[0] + oy * sa[1] + oz * sa[2];
+        }
+  }
+  __syncthreads();
+  // computeTemp on the children, one thread each
+  const int q = int(threadIdx.x) % (RR * RR * RR);
+  const int64_t cit = first + int(threadIdx.x) / (RR * RR * RR);
+  if (int(threadIdx.x) < kInterpItems * RR * RR * RR && cit < nitems) {
+    const int4 c = items[cit];
+    const LGeom& L = F.L[c.x];
+    double* Bb = B + F.off[c.x];
+    const int64_t at = L.idx(RR * c.y + (q & 1), RR * c.z + ((q >> 1) & 1), RR * c.w + (q >> 2));
     double s[NVAR];
     load_cell(Bb, L, at, s);
     compute_temp(s, P);
@@ -703,7 +821,7 @@ __global__ void __launch_bounds__(kBlk) k_coarse_raw(LGeom Lc, KParams P, Coarse
   int i, j, k;
   if (!valid_cell(Lc, tid(), i, j, k)) return;
   const int64_t at = Lc.idx(i, j, k);
-  const int c = CM.cell(i, j, k);
+  const int c = CM.cell_in(i, j, k);
   const int bi = CM.bmap[c];
   const int ob = CM.cmap[c];
   double s[NVAR];
@@ -746,7 +864,7 @@ __global__ void __launch_bounds__(kBlk) k_init_avgdown(LGeom Lc, CoarseMap CM, F
                                                         const double* S1, double* S0) {
   int i, j, k;
   if (!valid_cell(Lc, tid(), i, j, k)) return;
-  const int ob = CM.cmap[CM.cell(i, j, k)];
+  const int ob = CM.cmap[CM.cell_in(i, j, k)];
   if (ob < 0) return;
   const int64_t at = Lc.idx(i, j, k);
   for (int n = 0; n < NVAR; ++n) S0[at + n * Lc.sn] = avg_down_cell(F, S1, ob, i, j, k, n);
@@ -861,6 +979,8 @@ struct camr_amr {
   LGeom* d_L = nullptr;
   int64_t *d_off = nullptr, *d_vb0 = nullptr, *d_gb0 = nullptr, *d_poff = nullptr,
           *d_ib0 = nullptr;
+  int4* d_icell = nullptr;  // coarse ghost cells that kf_interp_list fills
+  int64_t n_icell = 0;
   double** d_qf = nullptr;
   camr_batch* plan = nullptr;
   int fdlo[3], fdn[3];
@@ -943,6 +1063,8 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
   const unsigned gf_valid = unsigned(a->h_vb0[a->nbox]);
   const unsigned gf_grown = unsigned(a->h_gb0[a->nbox]);
   const unsigned gf_interp = unsigned(a->h_ib0[a->nbox]);
+  const unsigned gf_ilist =
+      unsigned(std::max<int64_t>(1, (a->n_icell + kInterpItems - 1) / kInterpItems));
   const double* dt0 = &a->clock->dt0;
   const double* dt1 = &a->clock->dt1;
   DtCtl c{a->hp.cfl, a->hp.max_dt, a->hp.fixed_dt, a->hp.initial_dt, a->hp.init_shrink,
@@ -1067,8 +1189,13 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
     kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1_old, a->B1, fdlo, fdn, a->err, fl);
     kf_floor_fixup<FFLOOR_FILL><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
     count_launch(2);
+#if CAMR_INTERP_LIST
+    kf_interp_list<<<gf_ilist, kBlk, 0, st>>>(F, P, Lc, a->S0_old, a->S0, &a->clock->ct[0],
+                                              a->d_icell, a->n_icell, a->B1);
+#else
     kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[0],
                                           a->d_ib0, a->B1);
+#endif
     count_launch(4);
     camr_status cs = camr_batch_run(a->plan, 0.0, dt1, a->fine_mode, st);
     if (cs != CAMR_OK) return cudaErrorLaunchFailure;
@@ -1093,8 +1220,13 @@ cudaError_t amr_issue_step(camr_amr* a, bool first, bool est = false) {
       kf_fill<<<gf_grown, kBlk, 0, st>>>(F, P, CM, a->S1, a->B1, fdlo, fdn, a->err, fl);
       kf_floor_fixup<FFLOOR_FILL><<<1, 1024, kFloorSmem, st>>>(F, P, fl, ff, a->err);
       count_launch();
+#if CAMR_INTERP_LIST
+      kf_interp_list<<<gf_ilist, kBlk, 0, st>>>(F, P, Lc, a->S0_old, a->S0, &a->clock->ct[1],
+                                                a->d_icell, a->n_icell, a->B1);
+#else
       kf_interp<<<gf_interp, kBlk, 0, st>>>(F, P, CM, Lc, a->S0_old, a->S0, &a->clock->ct[1],
                                             a->d_ib0, a->B1);
+#endif
       count_launch(3);
       cs = camr_batch_run(a->plan, 0.0, dt1, a->fine_mode, st);
       if (cs != CAMR_OK) return cudaErrorLaunchFailure;
@@ -1131,7 +1263,7 @@ void amr_free(camr_amr* a) {
                   a->d_bmap, a->d_bcell, a->d_mask, a->d_cstart, a->d_contrib, a->d_reg,
                   a->d_cfp, a->clock, a->hist, a->bits0, a->bits1, a->err, a->staging0,
                   a->staging1, a->floor.count, a->floor.cells, a->floor.enforced,
-                  a->floor.total};
+                  a->floor.total, a->d_icell};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (a->own_stream) cudaStreamDestroy(a->stream);
@@ -1304,6 +1436,31 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
   if (e == cudaSuccess) e = upload(&a->d_vb0, a->h_vb0, st);
   if (e == cudaSuccess) e = upload(&a->d_gb0, a->h_gb0, st);
   if (e == cudaSuccess) e = upload(&a->d_ib0, a->h_ib0, st);
+  {
+    // the coarse cells of grow(coarsened box, 2) outside the coarsened box
+    // that no fine box covers, in kf_interp's order
+    std::vector<int4> icell;
+    for (int b = 0; b < nbox; ++b) {
+      const int* bx = boxes + 6 * b;
+      int clo[3], ncn[3];
+      for (int d = 0; d < 3; ++d) {
+        clo[d] = bx[d] / RR - 2;
+        ncn[d] = (bx[3 + d] - bx[d] + 1) / RR + 4;
+      }
+      for (int kk = 0; kk < ncn[2]; ++kk)
+        for (int jj = 0; jj < ncn[1]; ++jj)
+          for (int ii = 0; ii < ncn[0]; ++ii) {
+            if (ii >= 2 && ii < ncn[0] - 2 && jj >= 2 && jj < ncn[1] - 2 && kk >= 2 &&
+                kk < ncn[2] - 2)
+              continue;
+            const int ci = clo[0] + ii, cj = clo[1] + jj, ck = clo[2] + kk;
+            if (cmap[cidx(ci, cj, ck)] >= 0) continue;
+            icell.push_back(make_int4(b, ci, cj, ck));
+          }
+    }
+    a->n_icell = int64_t(icell.size());
+    if (e == cudaSuccess && !icell.empty()) e = upload(&a->d_icell, icell, st);
+  }
   // the fine hydro plan (fluxes only) over the B1 pool
   std::vector<camr_box_task> tasks(nbox);
   for (int b = 0; b < nbox; ++b) {
