@@ -20,11 +20,18 @@ using namespace camr;
 
 namespace {
 
+// 1: every stage table carries the item of each block (one int per block);
+// 0: each block binary-searches the items.
+#ifndef CAMR_BATCH_BLOCKMAP
+#define CAMR_BATCH_BLOCKMAP 1
+#endif
+
 constexpr int kChunks[] = {1, 2, 4};
 constexpr int kNChunk = 3;
 
 struct StageTable {
   BatchItem* items = nullptr;  // device
+  int* bitem = nullptr;        // device: the item of each block (null: binary search)
   int nitems = 0;
   int64_t nblocks = 0;
 };
@@ -96,6 +103,7 @@ camr_status fill_box(const camr_box_task& t, const camr_geom& geom, bool mol, bo
 
 cudaError_t build_tables(camr_batch* b, cudaStream_t st) {
   std::vector<BatchItem> items;
+  std::vector<int> bitem;
   for (int stage = 0; stage < BS_COUNT; ++stage) {
     if (!stage_used(stage, b->mol)) continue;
     for (int ci = 0; ci < kNChunk; ++ci) {
@@ -125,7 +133,21 @@ cudaError_t build_tables(camr_batch* b, cudaStream_t st) {
       e = cudaMemcpyAsync(T.items, items.data(), sizeof(BatchItem) * items.size(),
                           cudaMemcpyHostToDevice, st);
       if (e != cudaSuccess) return e;
-      e = cudaStreamSynchronize(st);  // `items` is reused for the next table
+      if (CAMR_BATCH_BLOCKMAP && block > 0 && block < (int64_t(1) << 31)) {
+        // one int per block, so that a block reads its item instead of
+        // binary-searching the items' first blocks
+        bitem.assign(size_t(block), 0);
+        for (size_t n = 0; n < items.size(); ++n) {
+          const int64_t end = (n + 1 < items.size()) ? items[n + 1].block0 : block;
+          for (int64_t q = items[n].block0; q < end; ++q) bitem[size_t(q)] = int(n);
+        }
+        e = cudaMalloc(&T.bitem, sizeof(int) * bitem.size());
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpyAsync(T.bitem, bitem.data(), sizeof(int) * bitem.size(),
+                            cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+      }
+      e = cudaStreamSynchronize(st);  // `items` and `bitem` are reused for the next table
       if (e != cudaSuccess) return e;
     }
   }
@@ -135,7 +157,8 @@ cudaError_t build_tables(camr_batch* b, cudaStream_t st) {
 cudaError_t run_stage(camr_batch* b, int stage, int ci, unsigned grid, DtRef dt,
                       cudaStream_t st) {
   const StageTable& T = b->tab[stage][ci];
-  return launch_batched_stage(stage, b->dev_boxes, T.items, T.nitems, T.nblocks, kChunks[ci],
+  return launch_batched_stage(stage, b->dev_boxes, T.items, T.nitems, T.bitem, T.nblocks,
+                              kChunks[ci],
                               grid, b->P, dt, nullptr, st);
 }
 
@@ -247,8 +270,10 @@ camr_status camr_batch_create(int nbox, const camr_box_task* tasks, const camr_g
 camr_status camr_batch_destroy(camr_batch* b) {
   if (!b) return CAMR_ERR_INVALID;
   for (int s = 0; s < BS_COUNT; ++s)
-    for (int c = 0; c < kNChunk; ++c)
+    for (int c = 0; c < kNChunk; ++c) {
       if (b->tab[s][c].items) cudaFree(b->tab[s][c].items);
+      if (b->tab[s][c].bitem) cudaFree(b->tab[s][c].bitem);
+    }
   if (b->dev_boxes) cudaFree(b->dev_boxes);
   if (b->work) cudaFree(b->work);
   delete b;

@@ -1357,11 +1357,12 @@ static_assert(sizeof(BoxCtx) % 8 == 0, "box context copied as 8-byte words");
 template <int STAGE, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
     kb_stage(const BoxCtx* __restrict__ boxes, const BatchItem* __restrict__ items, int nitems,
-             int64_t nblocks, int chunk, KParams P, DtRef dt, DevError* err) {
+             const int* __restrict__ bitem, int64_t nblocks, int chunk, KParams P, DtRef dt,
+             DevError* err) {
   constexpr bool kSmem = (CAMR_BOX_SMEM_MASK >> STAGE) & 1;
   __shared__ BoxCtx sbox[1];
   for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
-    const int it = find_item(items, nitems, b);
+    const int it = bitem ? bitem[b] : find_item(items, nitems, b);
     const BatchItem item = items[it];
     if constexpr (kSmem) {
       __syncthreads();
@@ -1710,14 +1711,16 @@ const void* batched_kernel(int stage) {
 }
 
 cudaError_t launch_batched_stage(int stage, const BoxCtx* boxes, const BatchItem* items,
-                                 int nitems, int64_t nblocks, int chunk, unsigned grid,
-                                 const KParams& P, DtRef dt, DevError* err, cudaStream_t st) {
+                                 int nitems, const int* bitem, int64_t nblocks, int chunk,
+                                 unsigned grid, const KParams& P, DtRef dt, DevError* err,
+                                 cudaStream_t st) {
   if (nblocks <= 0) return cudaSuccess;
   if (grid == 0 || grid > nblocks) grid = unsigned(nblocks);
   switch (stage) {
 #define CAMR_LB(S, M)                                                                     \
   case S:                                                                                 \
-    kb_stage<S, M><<<grid, kBlock, 0, st>>>(boxes, items, nitems, nblocks, chunk, P, dt, err); \
+    kb_stage<S, M><<<grid, kBlock, 0, st>>>(boxes, items, nitems, bitem, nblocks, chunk, P, dt, \
+                                            err);                                            \
     break;
     CAMR_LB(BS_CTOPRIM, CAMR_BMINB_CTOPRIM)
     CAMR_LB(BS_FLATDIVU, CAMR_BMINB_FLATDIVU)

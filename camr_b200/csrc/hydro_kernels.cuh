@@ -131,9 +131,12 @@ struct BatchItem {
 };
 
 int stage_regions(int stage, const KGeom& g, Region* out);
+// bitem: the item of each of the nblocks blocks (or null: each block
+// binary-searches the items' first blocks).
 cudaError_t launch_batched_stage(int stage, const BoxCtx* boxes, const BatchItem* items,
-                                 int nitems, int64_t nblocks, int chunk, unsigned grid,
-                                 const KParams& P, DtRef dt, DevError* err, cudaStream_t st);
+                                 int nitems, const int* bitem, int64_t nblocks, int chunk,
+                                 unsigned grid, const KParams& P, DtRef dt, DevError* err,
+                                 cudaStream_t st);
 const void* batched_kernel(int stage);
 int batched_min_blocks(int stage);
 constexpr int kBatchBlock = 128;
