@@ -62,6 +62,8 @@ struct FineDev {
   const int64_t* gb0;      // nbox+1: first block of each box's grown cells
   const int64_t* poff;     // per box: offset of its cells in the packed I/O array
   double* const* qf;       // nbox*3: interface p, u_n of each box's last hydro
+  const int* vbox;         // per valid-cell block: its box (null: search vb0)
+  const int* gbox;         // per grown-cell block: its box (null: search gb0)
 };
 
 // Coarse cell lookups (periodic wrap).
@@ -130,7 +132,7 @@ __device__ __forceinline__ double coarse_at(const LGeom& Lc, const double* c_old
 }
 
 #define FINE_VALID_PROLOGUE                                          \
-  const int b = box_of_block(F.vb0, F.nbox, blockIdx.x);             \
+  const int b = F.vbox ? F.vbox[blockIdx.x] : box_of_block(F.vb0, F.nbox, blockIdx.x); \
   const LGeom& L = F.L[b];                                           \
   const int64_t t = (int64_t(blockIdx.x) - F.vb0[b]) * kBlk + threadIdx.x; \
   int i, j, k;                                                       \
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kBlk) kf_est_dt(FineDev F, KParams P, const do
 __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap CM,
                                                  const double* src, double* B, int3 fdlo,
                                                  int3 fdn, DevError* err, FloorList fl) {
-  const int b = box_of_block(F.gb0, F.nbox, blockIdx.x);
+  const int b = F.gbox ? F.gbox[blockIdx.x] : box_of_block(F.gb0, F.nbox, blockIdx.x);
   const LGeom& L = F.L[b];
   const int64_t t = (int64_t(blockIdx.x) - F.gb0[b]) * kBlk + threadIdx.x;
   int i, j, k;
@@ -234,6 +236,11 @@ __global__ void __launch_bounds__(kBlk) kf_fill(FineDev F, KParams P, CoarseMap 
 // 1: the coarse-to-fine interpolation runs over a list of (coarse cell,
 // component) pairs (kf_interp_list); 0: one thread per coarse cell of each
 // box's grown shell walks the components (kf_interp).
+// 1: the fine kernels read their block's box from a per-block table; 0:
+// each block binary-searches the boxes' first blocks.
+#ifndef CAMR_FINE_BLOCKMAP
+#define CAMR_FINE_BLOCKMAP 1
+#endif
 #ifndef CAMR_INTERP_LIST
 #define CAMR_INTERP_LIST 1
 #endif
@@ -981,6 +988,7 @@ struct camr_amr {
           *d_ib0 = nullptr;
   int4* d_icell = nullptr;  // coarse ghost cells that kf_interp_list fills
   int64_t n_icell = 0;
+  int *d_vbox = nullptr, *d_gbox = nullptr;  // box of each valid / grown block
   double** d_qf = nullptr;
   camr_batch* plan = nullptr;
   int fdlo[3], fdn[3];
@@ -1014,6 +1022,8 @@ struct camr_amr {
     F.gb0 = d_gb0;
     F.poff = d_poff;
     F.qf = d_qf;
+    F.vbox = d_vbox;
+    F.gbox = d_gbox;
     return F;
   }
   FinePools pools() const {
@@ -1263,7 +1273,7 @@ void amr_free(camr_amr* a) {
                   a->d_bmap, a->d_bcell, a->d_mask, a->d_cstart, a->d_contrib, a->d_reg,
                   a->d_cfp, a->clock, a->hist, a->bits0, a->bits1, a->err, a->staging0,
                   a->staging1, a->floor.count, a->floor.cells, a->floor.enforced,
-                  a->floor.total, a->d_icell};
+                  a->floor.total, a->d_icell, a->d_vbox, a->d_gbox};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (a->own_stream) cudaStreamDestroy(a->stream);
@@ -1436,6 +1446,18 @@ camr_status camr_amr_create(const camr_level_desc* base, int nbox, const int* bo
   if (e == cudaSuccess) e = upload(&a->d_vb0, a->h_vb0, st);
   if (e == cudaSuccess) e = upload(&a->d_gb0, a->h_gb0, st);
   if (e == cudaSuccess) e = upload(&a->d_ib0, a->h_ib0, st);
+  if (CAMR_FINE_BLOCKMAP) {
+    // the box of every block of the valid-cell and grown-cell launches, so
+    // that a block reads it instead of binary-searching vb0 / gb0
+    auto block_boxes = [&](const std::vector<int64_t>& b0, int** dst) {
+      std::vector<int> m(size_t(b0[size_t(nbox)]), 0);
+      for (int b = 0; b < nbox; ++b)
+        for (int64_t q = b0[size_t(b)]; q < b0[size_t(b) + 1]; ++q) m[size_t(q)] = b;
+      if (e == cudaSuccess && !m.empty()) e = upload(dst, m, st);
+    };
+    block_boxes(a->h_vb0, &a->d_vbox);
+    block_boxes(a->h_gb0, &a->d_gbox);
+  }
   {
     // the coarse cells of grow(coarsened box, 2) outside the coarsened box
     // that no fine box covers, in kf_interp's order
