@@ -483,3 +483,317 @@ class DistributedLevel:
         # post_timestep's clean_state (Source/CAMR.cpp:679-718)
         self.clean_valid(S)
         self.S = S
+
+
+RR = 2  # refinement ratio of the two-level hierarchy
+
+
+class FluxRegister:
+    """The two-level flux register (refinement ratio 2) of a hierarchy whose
+    coarse boxes and fine boxes are both spread over the ranks: AMReX's
+    YAFluxRegister as the reference drives it -- CrseAdd and FineAdd after
+    every hydro call of the coarse and the fine level
+    (Source/Hydro/CAMR_construct_hydro_source.cpp:211-250), then Reflux in
+    post_timestep (Source/CAMR.cpp:686, 803-825).
+
+    Semantics (those of the two-level driver on one GPU and of its oracle):
+
+    * the coarse cells outside the fine region that share a face with a
+      fine-covered cell are the register's boundary cells (periodic
+      neighbours included; the domain must be periodic, as the two-level
+      driver's is);
+    * crse_add: at each boundary cell of a coarse box, for the faces in the
+      order x-, x+, y-, y+, z-, z+ whose other side is fine-covered, d -=
+      dtdx * flux on a low face and d += dtdx * flux on a high face;
+    * fine_add: for each fine box, direction and side (low, high), every
+      uncovered coarse cell just outside the box gets its 4 fine face fluxes
+      (slower transverse index outer), scaled by dtdx, subtracted on the
+      box's low side and added on its high side, into cfp;
+    * reflux: every coarse cell S = S + (d + cfp).
+
+    Across ranks the fine face values travel from each fine box's owner to
+    the owners of the coarse cells they correct, one message per pair of
+    ranks at reflux time, and each coarse owner adds them in the order the
+    single-process register does (call, fine box, direction, side, sub-face
+    per cell), so the result does not depend on the partition, bit for bit.
+
+    cboxes / fboxes: [(lo, hi)] of the coarse level's boxes (coarse index
+    space) and of the fine boxes (fine index space, lo even and hi odd in
+    each direction, disjoint); cowner / fowner: their ranks.  Fluxes are
+    tensors (NVAR, nk, nj, ni) on a box's faces in one direction (the
+    extent in that direction one larger), as camr_hydro_umdrv writes them.
+    pg: torch.distributed (None: one process).  Every rank makes the same
+    calls in the same order (crse_add and fine_add with possibly empty
+    dicts)."""
+
+    def __init__(self, geom, cboxes, cowner, fboxes, fowner, rank=0, nranks=1, device=None,
+                 pg=None):
+        import torch
+        self.torch = torch
+        self.rank, self.nranks, self.pg = rank, nranks, pg
+        self.device = device or torch.device("cpu")
+        if not all(geom.is_periodic[d] for d in range(3)):
+            raise ValueError("the flux register needs a periodic domain")
+        dlo = np.array([geom.dom_lo[d] for d in range(3)])
+        n = np.array([geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3)])
+        self.dlo, self.n = dlo, n
+        ncell = int(np.prod(n))
+        self.cboxes = [(tuple(lo), tuple(hi)) for lo, hi in cboxes]
+        self.fboxes = [(tuple(lo), tuple(hi)) for lo, hi in fboxes]
+        self.cowner = np.asarray(cowner, dtype=np.int64)
+        self.fowner = np.asarray(fowner, dtype=np.int64)
+
+        # coarse cell (flat, i fastest) -> coarse box, and -> fine box or -1
+        cbox_of = np.full(ncell, -1, dtype=np.int64)
+        for c, (lo, hi) in enumerate(self.cboxes):
+            cbox_of[self._cells(lo, hi)] = c
+        if (cbox_of < 0).any():
+            raise ValueError("the coarse boxes do not cover the domain")
+        cmap = np.full(ncell, -1, dtype=np.int64)
+        for b, (lo, hi) in enumerate(self.fboxes):
+            if any(lo[d] % RR or (hi[d] + 1) % RR or hi[d] < lo[d] for d in range(3)):
+                raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
+            cells = self._cells([lo[d] // RR for d in range(3)], [hi[d] // RR for d in range(3)])
+            if (cmap[cells] >= 0).any():
+                raise ValueError(f"fine box {b} overlaps another")
+            cmap[cells] = b
+        cov = (cmap >= 0).reshape(n[2], n[1], n[0])
+        near = np.zeros_like(cov)
+        for ax in range(3):
+            near |= np.roll(cov, 1, axis=ax) | np.roll(cov, -1, axis=ax)
+        bnd = (near & ~cov).ravel()
+        self.cmap, self.cbox_of = cmap, cbox_of
+
+        # this rank's register: its boundary cells, numbered in flat order
+        mine_bnd = bnd & (self.cowner[cbox_of] == rank)
+        reg_of = np.full(ncell, -1, dtype=np.int64)
+        reg_of[mine_bnd] = np.arange(int(mine_bnd.sum()))
+        self.nreg = int(mine_bnd.sum())
+        self.reg_of = reg_of
+        self.mine_c = [c for c in range(len(self.cboxes)) if self.cowner[c] == rank]
+        self.mine_f = [b for b in range(len(self.fboxes)) if self.fowner[b] == rank]
+
+        T = torch
+        dev = self.device
+        # CrseAdd of each coarse box of this rank: per (direction, side),
+        # the register slots and the face indices
+        self._crse = {}
+        unit = np.eye(3, dtype=np.int64)
+        for c in self.mine_c:
+            lo, hi = self.cboxes[c]
+            ijk = self._coords(lo, hi)
+            cell = self._wrap_flat(ijk)
+            sel = bnd[cell]
+            ijk = [a[sel] for a in ijk]
+            reg = reg_of[cell[sel]]
+            items = []
+            for d in range(3):
+                ext = [hi[e] - lo[e] + 1 + (e == d) for e in range(3)]
+                for side in (0, 1):
+                    nb = [ijk[e] + (unit[d][e] if side else -unit[d][e]) for e in range(3)]
+                    m = cmap[self._wrap_flat(nb)] >= 0
+                    if not m.any():
+                        continue
+                    f = [ijk[e][m] + (unit[d][e] if side else 0) - lo[e] for e in range(3)]
+                    fflat = f[0] + ext[0] * (f[1] + ext[1] * f[2])
+                    items.append((d, side, T.as_tensor(reg[m], device=dev),
+                                  T.as_tensor(fflat, device=dev)))
+            self._crse[c] = items
+
+        # FineAdd contributions of all fine boxes in the single-process
+        # order: fine box, direction, side, cell, sub-face (a2 outer)
+        parts = {k: [] for k in ("b", "d", "flat", "cell", "neg")}
+        for b, (flo, fhi) in enumerate(self.fboxes):
+            clo = [flo[e] // RR for e in range(3)]
+            chi = [fhi[e] // RR for e in range(3)]
+            for d in range(3):
+                t1 = 1 if d == 0 else 0
+                t2 = 1 if d == 2 else 2
+                ext = [fhi[e] - flo[e] + 1 + (e == d) for e in range(3)]
+                for side in (0, 1):
+                    alo, ahi = list(clo), list(chi)
+                    alo[d] = ahi[d] = chi[d] + 1 if side else clo[d] - 1
+                    fface = RR * (chi[d] + 1) if side else RR * clo[d]
+                    ijk = self._coords(alo, ahi)
+                    cell = self._wrap_flat(ijk)
+                    keep = cmap[cell] < 0
+                    ijk = [a[keep] for a in ijk]
+                    cell = cell[keep]
+                    sub = []
+                    for a2 in range(RR):
+                        for a1 in range(RR):
+                            fi = [None] * 3
+                            fi[d] = np.full(cell.shape, fface)
+                            fi[t1] = RR * ijk[t1] + a1
+                            fi[t2] = RR * ijk[t2] + a2
+                            f = [fi[e] - flo[e] for e in range(3)]
+                            sub.append(f[0] + ext[0] * (f[1] + ext[1] * f[2]))
+                    k = cell.size
+                    # per cell its sub-faces, a2 outer
+                    parts["flat"].append(np.stack(sub, axis=1).ravel())
+                    parts["cell"].append(np.repeat(cell, RR * RR))
+                    parts["b"].append(np.full(k * RR * RR, b))
+                    parts["d"].append(np.full(k * RR * RR, d))
+                    parts["neg"].append(np.full(k * RR * RR, side == 0))
+        cat = {k: (np.concatenate(v) if v else np.zeros(0, dtype=np.int64))
+               for k, v in parts.items()}
+        src_rank = self.fowner[cat["b"]] if cat["b"].size else cat["b"]
+        dst_rank = self.cowner[cbox_of[cat["cell"]]] if cat["cell"].size else cat["cell"]
+
+        # sender side: per destination rank, per (fine box, direction) of
+        # this rank, the face indices and signs, in the global order
+        self._send = {}
+        for r in range(nranks):
+            m = (src_rank == rank) & (dst_rank == r)
+            if not m.any():
+                continue
+            segs = []
+            bb, dd = cat["b"][m], cat["d"][m]
+            key = bb * 3 + dd
+            starts = np.flatnonzero(np.r_[True, key[1:] != key[:-1]])
+            ends = np.r_[starts[1:], key.size]
+            fl, ng = cat["flat"][m], cat["neg"][m]
+            for s0, s1 in zip(starts, ends):
+                segs.append((int(bb[s0]), int(dd[s0]), T.as_tensor(fl[s0:s1], device=dev),
+                             T.as_tensor(ng[s0:s1], device=dev)))
+            self._send[r] = (segs, int(m.sum()))
+
+        # receiver side: the contributions to this rank's cells in the
+        # global order, where each sender's part sits, and the rounds in
+        # which no two contributions share a register slot
+        m = dst_rank == rank
+        tgt = reg_of[cat["cell"][m]]
+        srcs = src_rank[m]
+        self._recv_pos = {int(r): T.as_tensor(np.flatnonzero(srcs == r), device=dev)
+                          for r in np.unique(srcs)}
+        self._nrecv = int(m.sum())
+        order = np.argsort(tgt, kind="stable")
+        rnd = np.empty(tgt.size, dtype=np.int64)
+        if tgt.size:
+            st = tgt[order]
+            first = np.r_[True, st[1:] != st[:-1]]
+            start_of = np.maximum.accumulate(np.where(first, np.arange(st.size), 0))
+            rnd[order] = np.arange(st.size) - start_of
+        self._rounds = []
+        for k in range(int(rnd.max()) + 1 if rnd.size else 0):
+            sel = np.flatnonzero(rnd == k)
+            self._rounds.append((T.as_tensor(sel, device=dev), T.as_tensor(tgt[sel], device=dev)))
+
+        # reflux of each coarse box of this rank: its register slots
+        self._apply = {}
+        for c in self.mine_c:
+            lo, hi = self.cboxes[c]
+            cell = self._wrap_flat(self._coords(lo, hi))
+            loc = np.flatnonzero(reg_of[cell] >= 0)
+            self._apply[c] = (T.as_tensor(loc, device=dev), T.as_tensor(reg_of[cell[loc]], device=dev))
+        self.reset()
+
+    # ---- index helpers (coarse index space, i fastest) ----
+    def _coords(self, lo, hi):
+        ax = [np.arange(lo[e], hi[e] + 1, dtype=np.int64) for e in range(3)]
+        K, J, I = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+        return [I.ravel(), J.ravel(), K.ravel()]
+
+    def _wrap_flat(self, ijk):
+        w = [(ijk[e] - self.dlo[e]) % self.n[e] for e in range(3)]
+        return w[0] + self.n[0] * (w[1] + self.n[1] * w[2])
+
+    def _cells(self, lo, hi):
+        return self._wrap_flat(self._coords(lo, hi))
+
+    # ---- the register ----
+    def reset(self):
+        """Zero the register (FluxRegister::reset at the start of each
+        coarse step) and drop the fine calls kept since the last reset."""
+        T = self.torch
+        self.d = T.zeros((NVAR, self.nreg), dtype=T.float64, device=self.device)
+        self.cfp = T.zeros((NVAR, self.nreg), dtype=T.float64, device=self.device)
+        self._fine = []
+
+    def crse_add(self, fluxes, dtdx):
+        """CrseAdd of the coarse boxes of this rank: fluxes {box: [fx, fy,
+        fz]} (face fluxes, area-weighted), scaled by dtdx."""
+        for c in sorted(fluxes):
+            if c not in self._crse:
+                raise ValueError(f"coarse box {c} is not on rank {self.rank}")
+            f = fluxes[c]
+            for d, side, reg, fflat in self._crse[c]:
+                v = dtdx * f[d].reshape(NVAR, -1)[:, fflat]
+                if side:
+                    self.d[:, reg] = self.d[:, reg] + v
+                else:
+                    self.d[:, reg] = self.d[:, reg] - v
+
+    def fine_add(self, fluxes, dtdx):
+        """FineAdd of one fine hydro call: fluxes {fine box: [fx, fy, fz]}
+        for every fine box of this rank (an empty dict on a rank with none),
+        scaled by dtdx.  The scaled values of each destination rank are kept
+        until reflux."""
+        T = self.torch
+        if sorted(fluxes) != self.mine_f:
+            raise ValueError("fine_add needs the fluxes of exactly this rank's fine boxes")
+        out = {}
+        for r, (segs, cnt) in self._send.items():
+            vals = T.empty((NVAR, cnt), dtype=T.float64, device=self.device)
+            at = 0
+            for b, d, fflat, neg in segs:
+                k = fflat.numel()
+                v = dtdx * fluxes[b][d].reshape(NVAR, -1)[:, fflat]
+                vals[:, at:at + k] = T.where(neg, -v, v)
+                at += k
+            out[r] = vals
+        self._fine.append(out)
+
+    def reflux(self, S, ng=0):
+        """Reflux: the fine values travel to the coarse owners, the register
+        adds them in the single-process order, then every valid cell of this
+        rank's coarse boxes becomes S + (d + cfp).  S: {coarse box: tensor
+        (NVAR, ...) covering the box grown by ng}, updated in place."""
+        T = self.torch
+        ncall = len(self._fine)
+        if ncall == 0:
+            self._apply_corrections(S, ng)
+            return
+        got = {}
+        if self.rank in self._send:
+            got[self.rank] = [call[self.rank] for call in self._fine]
+        if self.pg is not None and self.nranks > 1:
+            ops, bufs = [], {}
+            for r in sorted(self._send):
+                if r == self.rank:
+                    continue
+                buf = T.cat([call[r] for call in self._fine], dim=1).contiguous()
+                bufs[("s", r)] = buf
+                ops.append(self.pg.isend(buf, dst=r))
+            for r, pos in sorted(self._recv_pos.items()):
+                if r == self.rank:
+                    continue
+                buf = T.empty((NVAR, ncall * pos.numel()), dtype=T.float64, device=self.device)
+                bufs[("r", r)] = buf
+                ops.append(self.pg.irecv(buf, src=r))
+            for op in ops:
+                op.wait()
+            for r, pos in self._recv_pos.items():
+                if r != self.rank:
+                    got[r] = list(bufs[("r", r)].split(pos.numel(), dim=1))
+        for s in range(ncall):
+            allv = T.empty((NVAR, self._nrecv), dtype=T.float64, device=self.device)
+            for r, pos in self._recv_pos.items():
+                allv[:, pos] = got[r][s]
+            for sel, reg in self._rounds:
+                self.cfp[:, reg] = self.cfp[:, reg] + allv[:, sel]
+        self._apply_corrections(S, ng)
+
+    def _apply_corrections(self, S, ng):
+        T = self.torch
+        for c in sorted(S):
+            if c not in self._apply:
+                raise ValueError(f"coarse box {c} is not on rank {self.rank}")
+            lo, hi = self.cboxes[c]
+            ext = [hi[e] - lo[e] + 1 for e in range(3)]
+            loc, reg = self._apply[c]
+            corr = T.zeros((NVAR, ext[0] * ext[1] * ext[2]), dtype=T.float64, device=self.device)
+            corr[:, loc] = self.d[:, reg] + self.cfp[:, reg]
+            t = S[c]
+            v = t[:, ng:ng + ext[2], ng:ng + ext[1], ng:ng + ext[0]] if ng else t
+            v.add_(corr.reshape(NVAR, ext[2], ext[1], ext[0]))

@@ -1096,6 +1096,70 @@ extern "C" long orc_amr_run(const orc_params* p, const orc_level* lev0, int nbox
   return nerr;
 }
 
+// The two-level flux register alone, on fluxes the caller supplies: CrseAdd
+// of each coarse box's face fluxes (scale dtdx_c), then FineAdd of every
+// fine box's face fluxes for each of ncall fine hydro calls (scale dtdx_f),
+// then the reflux of post_timestep, S0 += d + cfp over the whole coarse
+// domain -- the same make_fluxreg / crse_add / fine_add and reflux loop as
+// orc_amr_run.  The domain must be periodic (as orc_amr_run's).
+// cflux: for each coarse box c, for d = 0..2, NVAR comps on faces(box c, d);
+// fflux: for each call, each fine box b, d = 0..2, NVAR comps on
+// faces(fine box b, d); every fab with i fastest and the component slowest.
+extern "C" void orc_fluxreg_reflux(const orc_level* lev0, int ncbox, const int* cboxes,
+                                   const double* cflux, double dtdx_c, int nfbox,
+                                   const int* fboxes, int ncall, const double* fflux,
+                                   double dtdx_f, double* S0) {
+  using namespace orc;
+  const orc_level& Lc = *lev0;
+  const Grid gc = make_grid(Lc);
+  Fab Sc;
+  Sc.view(S0, gc.dom.lo, gc.dom.hi, NVAR);
+  Fine fn;
+  for (int b = 0; b < nfbox; ++b) {
+    Box3 bx;
+    for (int d = 0; d < 3; ++d) {
+      bx.lo[d] = fboxes[6 * b + d];
+      bx.hi[d] = fboxes[6 * b + 3 + d];
+    }
+    fn.boxes.push_back(bx);
+  }
+  FluxReg fr = make_fluxreg(gc, Lc, fn.boxes);
+  for (auto& v : fr.d.own) v = 0.0;
+  for (auto& v : fr.cfp.own) v = 0.0;
+  size_t off = 0;
+  for (int c = 0; c < ncbox; ++c) {
+    Box3 bx;
+    for (int d = 0; d < 3; ++d) {
+      bx.lo[d] = cboxes[6 * c + d];
+      bx.hi[d] = cboxes[6 * c + 3 + d];
+    }
+    Fab f[3];
+    for (int d = 0; d < 3; ++d) {
+      const Box3 fb = faces(bx, d);
+      f[d].view(const_cast<double*>(cflux) + off, fb.lo, fb.hi, NVAR);
+      off += size_t(f[d].sn) * NVAR;
+    }
+    crse_add(fr, bx, f, dtdx_c);
+  }
+  for (int d = 0; d < 3; ++d) fn.F[d].resize(nfbox);
+  off = 0;
+  for (int call = 0; call < ncall; ++call) {
+    for (int b = 0; b < nfbox; ++b)
+      for (int d = 0; d < 3; ++d) {
+        const Box3 fb = faces(fn.boxes[b], d);
+        fn.F[d][b].view(const_cast<double*>(fflux) + off, fb.lo, fb.hi, NVAR);
+        off += size_t(fn.F[d][b].sn) * NVAR;
+      }
+    fine_add(fr, gc, fn, dtdx_f);
+  }
+  for_box(gc.dom, [&](int i, int j, int k) {
+    for (int n = 0; n < NVAR; ++n) {
+      const double dcorr = fr.d(i, j, k, n) + fr.cfp(i, j, k, n);
+      Sc(i, j, k, n) = Sc(i, j, k, n) + dcorr;
+    }
+  });
+}
+
 namespace orc {
 namespace {
 }  // namespace

@@ -1,0 +1,171 @@
+"""The two-level flux register across ranks (camr_b200/distributed.py
+FluxRegister) on CPU, against the oracle's restated YAFluxRegister
+(oracle/level_driver.cpp make_fluxreg / crse_add / fine_add and the reflux
+of post_timestep, through orc_fluxreg_reflux), bit for bit.
+
+The fine boxes are placed so that the register meets its corner cases: two
+fine boxes touching the same uncovered coarse cell from different sides
+(its contributions must be added in the single-process box order), fine
+boxes whose neighbours wrap around the periodic domain, a one-coarse-cell
+fine box, fine boxes owned by one rank correcting coarse cells owned by the
+other, and signed zeros in the state (the reflux adds +0 to every cell)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from camr_b200 import distributed as D
+from camr_b200 import hydro
+
+N = (16, 12, 8)
+MGS = (8, 6, 4)
+FBOXES = [((2, 2, 2), (9, 9, 7)),       # coarse 1..4 x 1..4 x 1..3
+          ((10, 2, 2), (15, 7, 5)),     # touches the first along x
+          ((28, 0, 12), (31, 5, 15)),   # neighbours across the periodic x, y and z edges
+          ((20, 16, 4), (21, 17, 5)),   # one coarse cell
+          ((0, 18, 0), (3, 23, 1))]     # low x and high y edges
+NCALL = 4   # two subcycles of a two-stage fine step
+DTDX_C, DTDX_F = 0.37, 0.1825
+
+
+def _inputs():
+    """Seeded coarse state, coarse face fluxes and fine face fluxes."""
+    rng = np.random.default_rng(11)
+    cboxes = hydro.level_boxes(N, MGS)
+    S = rng.standard_normal((10,) + N[::-1])
+    S[3, 0, 0, :4] = -0.0
+    S[2, 1, 2, 5:9] = 0.0
+
+    def faces(lo, hi, d):
+        shape = [hi[e] - lo[e] + 1 + (e == d) for e in range(3)]
+        f = rng.standard_normal((10,) + tuple(shape[::-1]))
+        f[:, 0, 0, 0] = 0.0
+        return f
+
+    cflux = [[faces(lo, hi, d) for d in range(3)] for lo, hi in cboxes]
+    fflux = [[[faces(lo, hi, d) for d in range(3)] for lo, hi in FBOXES]
+             for _ in range(NCALL)]
+    return cboxes, S, cflux, fflux
+
+
+def _oracle(cboxes, S, cflux, fflux):
+    import oracle
+    lev = oracle.make_level(N)
+    out = np.ascontiguousarray(S.copy())
+    cb = np.array([list(lo) + list(hi) for lo, hi in cboxes])
+    fb = np.array([list(lo) + list(hi) for lo, hi in FBOXES])
+    oracle.fluxreg_reflux("restate", lev, cb, cflux, DTDX_C, fb, fflux, DTDX_F, out)
+    return out
+
+
+def _run_rank(rank, world, cowner, fowner, pg, ng):
+    cboxes, S, cflux, fflux = _inputs()
+    geom = hydro.make_geom(N)
+    fr = D.FluxRegister(geom, cboxes, cowner, FBOXES, fowner, rank, world,
+                        torch.device("cpu"), pg)
+    fr.crse_add({c: [torch.from_numpy(a) for a in cflux[c]] for c in fr.mine_c}, DTDX_C)
+    for call in range(NCALL):
+        fr.fine_add({b: [torch.from_numpy(a) for a in fflux[call][b]] for b in fr.mine_f},
+                    DTDX_F)
+    mine = {}
+    for c in fr.mine_c:
+        lo, hi = cboxes[c]
+        part = S[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
+        t = torch.full((10,) + tuple(hi[e] - lo[e] + 1 + 2 * ng for e in (2, 1, 0)), np.nan,
+                       dtype=torch.float64)
+        t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng] = torch.from_numpy(part)
+        mine[c] = t
+    fr.reflux(mine, ng)
+    out = {}
+    for c, t in mine.items():
+        out[c] = t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng].numpy().copy()
+    return out, fr
+
+
+def _assemble(cboxes, parts):
+    full = np.full((10,) + N[::-1], np.nan)
+    for c, a in parts.items():
+        lo, hi = cboxes[c]
+        full[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1] = a
+    return full
+
+
+def _same_bits(a, b):
+    return np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+def test_flux_register_one_rank_matches_oracle(oracle_kind):
+    cboxes, S, cflux, fflux = _inputs()
+    want = _oracle(cboxes, S, cflux, fflux)
+    assert not _same_bits(want, S)        # the register changed something
+    parts, fr = _run_rank(0, 1, [0] * len(cboxes), [0] * len(FBOXES), None, 2)
+    got = _assemble(cboxes, parts)
+    assert _same_bits(got, want)
+    # a cell that two fine boxes correct (coarse (5, 4, 1): x+ of the first
+    # box, y+ of the second) takes more than one box side's 4 sub-faces per
+    # fine call
+    assert len(fr._rounds) > 4
+
+
+def test_flux_register_rejects_bad_boxes():
+    geom = hydro.make_geom(N)
+    cboxes = hydro.level_boxes(N, MGS)
+    with pytest.raises(ValueError):
+        D.FluxRegister(geom, cboxes, [0] * len(cboxes), [((1, 0, 0), (4, 3, 3))], [0])
+    with pytest.raises(ValueError):
+        D.FluxRegister(geom, cboxes, [0] * len(cboxes),
+                       [((0, 0, 0), (3, 3, 3)), ((2, 2, 2), (5, 5, 5))], [0, 0])
+    walls = hydro.make_geom(N, is_periodic=(0, 1, 1), bc_lo=(2, 0, 0), bc_hi=(2, 0, 0))
+    with pytest.raises(ValueError):
+        D.FluxRegister(walls, cboxes, [0] * len(cboxes), FBOXES, [0] * len(FBOXES))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, fowner, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cboxes = hydro.level_boxes(N, MGS)
+        cowner = D.sfc_partition(cboxes, world)
+        parts, fr = _run_rank(rank, world, cowner, fowner, dist, 1)
+        q.put((rank, parts, len(fr._send), len(fr._recv_pos)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("fowner", [[0, 1, 0, 1, 1], [1, 1, 1, 1, 1]])
+def test_flux_register_two_ranks_matches_oracle(oracle_kind, fowner):
+    world = 2
+    cboxes, S, cflux, fflux = _inputs()
+    want = _oracle(cboxes, S, cflux, fflux)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, fowner, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    parts = {}
+    for rank, pr, nsend, nrecv in res:
+        assert not set(pr) & set(parts)
+        parts.update(pr)
+        if rank == 1:
+            assert nsend == 2     # fine boxes of rank 1 correct cells of both ranks
+    got = _assemble(cboxes, parts)
+    assert _same_bits(got, want)
