@@ -62,15 +62,16 @@ def _oracle(cboxes, S, cflux, fflux):
     return out
 
 
-def _run_rank(rank, world, cowner, fowner, pg, ng):
+def _run_rank(rank, world, cowner, fowner, pg, ng, device=None):
+    device = device or torch.device("cpu")
     cboxes, S, cflux, fflux = _inputs()
     geom = hydro.make_geom(N)
-    fr = D.FluxRegister(geom, cboxes, cowner, FBOXES, fowner, rank, world,
-                        torch.device("cpu"), pg)
-    fr.crse_add({c: [torch.from_numpy(a) for a in cflux[c]] for c in fr.mine_c}, DTDX_C)
+    fr = D.FluxRegister(geom, cboxes, cowner, FBOXES, fowner, rank, world, device, pg)
+    fr.crse_add({c: [torch.from_numpy(a).to(device) for a in cflux[c]] for c in fr.mine_c},
+                DTDX_C)
     for call in range(NCALL):
-        fr.fine_add({b: [torch.from_numpy(a) for a in fflux[call][b]] for b in fr.mine_f},
-                    DTDX_F)
+        fr.fine_add({b: [torch.from_numpy(a).to(device) for a in fflux[call][b]]
+                     for b in fr.mine_f}, DTDX_F)
     mine = {}
     for c in fr.mine_c:
         lo, hi = cboxes[c]
@@ -78,11 +79,12 @@ def _run_rank(rank, world, cowner, fowner, pg, ng):
         t = torch.full((10,) + tuple(hi[e] - lo[e] + 1 + 2 * ng for e in (2, 1, 0)), np.nan,
                        dtype=torch.float64)
         t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng] = torch.from_numpy(part)
-        mine[c] = t
+        mine[c] = t.to(device)
     fr.reflux(mine, ng)
     out = {}
     for c, t in mine.items():
-        out[c] = t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng].numpy().copy()
+        out[c] = t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng,
+                   ng:t.shape[3] - ng].cpu().numpy().copy()
     return out, fr
 
 
@@ -109,6 +111,21 @@ def test_flux_register_one_rank_matches_oracle(oracle_kind):
     # box, y+ of the second) takes more than one box side's 4 sub-faces per
     # fine call
     assert len(fr._rounds) > 4
+
+
+@pytest.mark.gpu
+def test_flux_register_on_device_matches_oracle(oracle_kind):
+    """The same register with its tensors (register, plan indices, fluxes,
+    states) in device memory: the products, sums and scatters then run as
+    device kernels and must still give the oracle's bits."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    cboxes, S, cflux, fflux = _inputs()
+    want = _oracle(cboxes, S, cflux, fflux)
+    parts, fr = _run_rank(0, 1, [0] * len(cboxes), [0] * len(FBOXES), None, 1,
+                          torch.device("cuda:0"))
+    assert fr.d.is_cuda
+    assert _same_bits(_assemble(cboxes, parts), want)
 
 
 def test_flux_register_rejects_bad_boxes():
