@@ -302,6 +302,17 @@ class DistributedLevel:
         self.steps = 0
         self.mol = params.do_mol != 0
         self.grav = params.add_grav_src != 0
+        self.registers = []
+
+    def attach_flux_register(self, fr, role):
+        """After every hydro call of this level, pass its boxes' face fluxes
+        to the flux register fr: CrseAdd when this level is the register's
+        coarse level (role "coarse"), FineAdd when it is the fine level
+        (role "fine"), scaled as construct_hydro_source does
+        (Source/Hydro/CAMR_construct_hydro_source.cpp:240-252)."""
+        if role not in ("coarse", "fine"):
+            raise ValueError(role)
+        self.registers.append((fr, role))
 
     # ---- state in and out (the valid cells of this rank's boxes) ----
     def _shape(self, b, ng):
@@ -392,7 +403,7 @@ class DistributedLevel:
 
     def _hydro(self, B, src_h, dt):
         T = self.torch
-        out = {}
+        out, fluxes = {}, {}
         for b in self.mine:
             lo, hi = self.boxes[b]
             dsdt = T.zeros(self._shape(b, 0), dtype=T.float64, device=self.device)
@@ -405,6 +416,13 @@ class DistributedLevel:
             self.hydro.hydro_umdrv(list(lo), list(hi), self.geom, B[b], uin_lo, dsdt, flx,
                                    self.params, dt, src=src_h[b] if src_h else None)
             out[b] = dsdt
+            fluxes[b] = flx
+        dx = [self.geom.dx[d] for d in range(3)]
+        for fr, role in self.registers:
+            if role == "coarse":
+                fr.crse_add(fluxes, FluxRegister.crse_scale(dx, dt, self.mol))
+            else:
+                fr.fine_add(fluxes, FluxRegister.fine_scale(dx, dt, self.mol))
         return out
 
     def _grav(self, rho, mz, g):
@@ -687,6 +705,21 @@ class FluxRegister:
             loc = np.flatnonzero(reg_of[cell] >= 0)
             self._apply[c] = (T.as_tensor(loc, device=dev), T.as_tensor(reg_of[cell[loc]], device=dev))
         self.reset()
+
+    @staticmethod
+    def crse_scale(dx, dt, mol):
+        """CrseAdd's factor for one hydro call of the coarse level:
+        fac_for_reflux * dt / vol, fac_for_reflux 0.5 for MOL (each of its
+        two stages adds) and 1 for CTU (Source/Hydro/
+        CAMR_construct_hydro_source.cpp:24, 240-247)."""
+        return ((0.5 if mol else 1.0) * dt) / (dx[0] * dx[1] * dx[2])
+
+    @staticmethod
+    def fine_scale(dx_f, dt_f, mol):
+        """FineAdd's factor for one hydro call of the fine level: the fine
+        call's fac_for_reflux * dt / vol, over the ratio^3 fine cells of a
+        coarse cell (YAFluxRegister's FineAdd, ratio 2)."""
+        return ((0.5 if mol else 1.0) * dt_f) / ((dx_f[0] * dx_f[1] * dx_f[2]) * float(RR ** 3))
 
     # ---- index helpers (coarse index space, i fastest) ----
     def _coords(self, lo, hi):

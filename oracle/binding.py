@@ -169,7 +169,8 @@ def load(kind="restate"):
     lib.orc_amr_run.argtypes = [C.POINTER(Params), C.POINTER(Level), C.c_int, C.c_void_p,
                                 _DP, _DP, C.c_int, C.c_int, C.c_int, _DP, C.c_void_p]
     lib.orc_fluxreg_reflux.restype = None
-    lib.orc_fluxreg_reflux.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, _DP, C.c_double,
+    lib.orc_fluxreg_reflux.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, C.c_int, _DP,
+                                       C.c_double,
                                        C.c_int, C.c_void_p, C.c_int, _DP, C.c_double, _DP]
     _LIBS[kind] = lib
     return lib
@@ -359,14 +360,16 @@ def amr_run(kind, p, lev0, boxes, S0, S1, nsteps, do_init=False, first_step=True
 def fluxreg_reflux(kind, lev0, cboxes, cflux, dtdx_c, fboxes, fflux, dtdx_f, S0):
     """The restated two-level flux register on given fluxes, S0 refluxed in
     place (orc_fluxreg_reflux).  cboxes / fboxes: (n, 6) lo/hi of the
-    coarse and fine boxes; cflux[c][d]: NVAR x faces(coarse box c, d)
-    arrays (component slowest, i fastest); fflux[call][b][d]: the same for
-    fine box b in each fine hydro call."""
+    coarse and fine boxes; cflux[call][c][d]: NVAR x faces(coarse box c, d)
+    arrays (component slowest, i fastest) of each coarse hydro call;
+    fflux[call][b][d]: the same for fine box b in each fine hydro call."""
     cb = np.ascontiguousarray(cboxes, dtype=np.int32).reshape(-1, 6)
     fb = np.ascontiguousarray(fboxes, dtype=np.int32).reshape(-1, 6)
-    cf = np.ascontiguousarray(np.concatenate([np.ravel(a) for per in cflux for a in per]))
+    cf = np.ascontiguousarray(np.concatenate([np.ravel(a) for call in cflux for per in call
+                                              for a in per]))
     ff = (np.ascontiguousarray(np.concatenate([np.ravel(a) for call in fflux for per in call
                                                 for a in per]))
           if fflux else np.zeros(1))
-    load(kind).orc_fluxreg_reflux(C.byref(lev0), len(cb), cb.ctypes.data, cf, float(dtdx_c),
+    load(kind).orc_fluxreg_reflux(C.byref(lev0), len(cb), cb.ctypes.data, len(cflux), cf,
+                                  float(dtdx_c),
                                   len(fb), fb.ctypes.data, len(fflux), ff, float(dtdx_f), S0)

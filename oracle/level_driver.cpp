@@ -1097,16 +1097,18 @@ extern "C" long orc_amr_run(const orc_params* p, const orc_level* lev0, int nbox
 }
 
 // The two-level flux register alone, on fluxes the caller supplies: CrseAdd
-// of each coarse box's face fluxes (scale dtdx_c), then FineAdd of every
+// of each coarse box's face fluxes for each of ncrse coarse hydro calls
+// (scale dtdx_c), then FineAdd of every
 // fine box's face fluxes for each of ncall fine hydro calls (scale dtdx_f),
 // then the reflux of post_timestep, S0 += d + cfp over the whole coarse
 // domain -- the same make_fluxreg / crse_add / fine_add and reflux loop as
 // orc_amr_run.  The domain must be periodic (as orc_amr_run's).
-// cflux: for each coarse box c, for d = 0..2, NVAR comps on faces(box c, d);
+// cflux: for each coarse call, each coarse box c, d = 0..2, NVAR comps on
+// faces(box c, d);
 // fflux: for each call, each fine box b, d = 0..2, NVAR comps on
 // faces(fine box b, d); every fab with i fastest and the component slowest.
 extern "C" void orc_fluxreg_reflux(const orc_level* lev0, int ncbox, const int* cboxes,
-                                   const double* cflux, double dtdx_c, int nfbox,
+                                   int ncrse, const double* cflux, double dtdx_c, int nfbox,
                                    const int* fboxes, int ncall, const double* fflux,
                                    double dtdx_f, double* S0) {
   using namespace orc;
@@ -1127,20 +1129,21 @@ extern "C" void orc_fluxreg_reflux(const orc_level* lev0, int ncbox, const int* 
   for (auto& v : fr.d.own) v = 0.0;
   for (auto& v : fr.cfp.own) v = 0.0;
   size_t off = 0;
-  for (int c = 0; c < ncbox; ++c) {
-    Box3 bx;
-    for (int d = 0; d < 3; ++d) {
-      bx.lo[d] = cboxes[6 * c + d];
-      bx.hi[d] = cboxes[6 * c + 3 + d];
+  for (int call = 0; call < ncrse; ++call)
+    for (int c = 0; c < ncbox; ++c) {
+      Box3 bx;
+      for (int d = 0; d < 3; ++d) {
+        bx.lo[d] = cboxes[6 * c + d];
+        bx.hi[d] = cboxes[6 * c + 3 + d];
+      }
+      Fab f[3];
+      for (int d = 0; d < 3; ++d) {
+        const Box3 fb = faces(bx, d);
+        f[d].view(const_cast<double*>(cflux) + off, fb.lo, fb.hi, NVAR);
+        off += size_t(f[d].sn) * NVAR;
+      }
+      crse_add(fr, bx, f, dtdx_c);
     }
-    Fab f[3];
-    for (int d = 0; d < 3; ++d) {
-      const Box3 fb = faces(bx, d);
-      f[d].view(const_cast<double*>(cflux) + off, fb.lo, fb.hi, NVAR);
-      off += size_t(f[d].sn) * NVAR;
-    }
-    crse_add(fr, bx, f, dtdx_c);
-  }
   for (int d = 0; d < 3; ++d) fn.F[d].resize(nfbox);
   off = 0;
   for (int call = 0; call < ncall; ++call) {

@@ -58,7 +58,7 @@ def _oracle(cboxes, S, cflux, fflux):
     out = np.ascontiguousarray(S.copy())
     cb = np.array([list(lo) + list(hi) for lo, hi in cboxes])
     fb = np.array([list(lo) + list(hi) for lo, hi in FBOXES])
-    oracle.fluxreg_reflux("restate", lev, cb, cflux, DTDX_C, fb, fflux, DTDX_F, out)
+    oracle.fluxreg_reflux("restate", lev, cb, [cflux], DTDX_C, fb, fflux, DTDX_F, out)
     return out
 
 
