@@ -240,7 +240,10 @@ camr_status read_cell_h(const std::string& lev, int ncomp, std::vector<int>& bx,
   char paren;
   int nbox = 0, zero = 0;
   ch >> paren >> nbox >> zero;
-  if (nbox < 0) return io_fail("bad box count in Cell_H");
+  // a count beyond any real BoxArray (a damaged header) is refused before
+  // it sizes the box list
+  constexpr int kMaxBoxes = 1 << 22;
+  if (!ch || nbox < 0 || nbox > kMaxBoxes) return io_fail("bad box count in Cell_H");
   bx.assign(size_t(nbox) * 6, 0);
   for (int b = 0; b < nbox; ++b) {
     std::string tok;

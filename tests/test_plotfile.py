@@ -136,6 +136,22 @@ def test_plotfile_readers_reject_more_components_than_nvar(tmp_path, native_lib)
             read()
 
 
+def test_plotfile_reader_rejects_damaged_box_count(tmp_path, native_lib):
+    """A Cell_H whose box count is absurd (a damaged file) is refused with
+    an error instead of sizing the box list from it."""
+    n = (8, 8, 8)
+    geom = hydro.make_geom(n)
+    path = tmp_path / "plt_bad"
+    hydro.write_plotfile(path, P.random_smooth(n, seed=4), geom, (1, 1, 1))
+    cell_h = path / "Level_0" / "Cell_H"
+    lines = cell_h.read_text().split("\n")
+    assert lines[4].startswith("(")
+    lines[4] = "(2147483647 0"
+    cell_h.write_text("\n".join(lines))
+    with pytest.raises(native.CamrError, match="bad box count"):
+        hydro.read_plotfile(path, geom)
+
+
 def read_level(path, lev, nv):
     """Boxes and per-box arrays of Level_<lev> (VisMF header + FAB data)."""
     cell_h = (path / f"Level_{lev}" / "Cell_H").read_text().split("\n")
