@@ -830,3 +830,147 @@ class FluxRegister:
             t = S[c]
             v = t[:, ng:ng + ext[2], ng:ng + ext[1], ng:ng + ext[0]] if ng else t
             v.add_(corr.reshape(NVAR, ext[2], ext[1], ext[0]))
+
+
+class AverageDown:
+    """avgDown of a two-level hierarchy (refinement ratio 2) whose coarse
+    and fine boxes are spread over the ranks (CAMR::avgDown,
+    Source/CAMR.cpp:693, 1048-1064, amrex::average_down): every coarse cell
+    that a fine box covers becomes 1/8 of the sum of its 8 children, summed
+    from 0.0 with the x index fastest, then z.
+
+    Each fine box's owner forms the averages of its box and sends them to
+    the owners of the coarse cells, one message per pair of ranks, so the
+    result does not depend on the partition, bit for bit.  Boxes and owners
+    as for FluxRegister; every rank makes the same calls."""
+
+    def __init__(self, geom, cboxes, cowner, fboxes, fowner, rank=0, nranks=1, device=None,
+                 pg=None):
+        import torch
+        self.torch = torch
+        self.rank, self.nranks, self.pg = rank, nranks, pg
+        self.device = device or torch.device("cpu")
+        dlo = np.array([geom.dom_lo[d] for d in range(3)])
+        dhi = np.array([geom.dom_hi[d] for d in range(3)])
+        n = dhi - dlo + 1
+        self.cboxes = [(tuple(lo), tuple(hi)) for lo, hi in cboxes]
+        self.fboxes = [(tuple(lo), tuple(hi)) for lo, hi in fboxes]
+        cowner = np.asarray(cowner, dtype=np.int64)
+        fowner = np.asarray(fowner, dtype=np.int64)
+        ncell = int(np.prod(n))
+        cbox_of = np.full(ncell, -1, dtype=np.int64)
+        cloc = np.full(ncell, -1, dtype=np.int64)   # flat index inside its coarse box
+        for c, (lo, hi) in enumerate(self.cboxes):
+            ijk = _box_coords(lo, hi)
+            cell = _flat(ijk, dlo, n)
+            cbox_of[cell] = c
+            cloc[cell] = np.arange(cell.size)
+        if (cbox_of < 0).any():
+            raise ValueError("the coarse boxes do not cover the domain")
+        self.mine_f = [b for b in range(len(self.fboxes)) if fowner[b] == rank]
+        T = torch
+        dev = self.device
+
+        def kji(c, places):
+            # flat places inside coarse box c -> (k, j, i) offsets in it
+            lo, hi = self.cboxes[c]
+            nx, ny = hi[0] - lo[0] + 1, hi[1] - lo[1] + 1
+            return tuple(T.as_tensor(a, device=dev)
+                         for a in (places // (nx * ny), (places // nx) % ny, places % nx))
+
+        # per fine box: its coarse cells' (coarse box, place) and owner
+        self._send = {}   # dest rank -> [(fine box, positions in the box's averages)]
+        self._recv = {}   # src rank -> [(coarse box, place) per entry, in message order]
+        self._local = []  # (fine box, positions, coarse box, places) on this rank
+        for b, (flo, fhi) in enumerate(self.fboxes):
+            if any(flo[d] % RR or (fhi[d] + 1) % RR or fhi[d] < flo[d] for d in range(3)):
+                raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
+            clo = [flo[d] // RR for d in range(3)]
+            chi = [fhi[d] // RR for d in range(3)]
+            if any(clo[d] < dlo[d] or chi[d] > dhi[d] for d in range(3)):
+                raise ValueError(f"fine box {b} lies outside the domain")
+            cell = _flat(_box_coords(clo, chi), dlo, n)
+            cb, pl = cbox_of[cell], cloc[cell]
+            dest = cowner[cb]
+            src = int(fowner[b])
+            for r in np.unique(dest):
+                r = int(r)
+                pos = np.flatnonzero(dest == r)
+                if src == rank and r == rank:
+                    for c in np.unique(cb[pos]):
+                        m = pos[cb[pos] == c]
+                        self._local.append((b, T.as_tensor(m, device=dev), int(c),
+                                            kji(int(c), pl[m])))
+                elif src == rank:
+                    self._send.setdefault(r, []).append((b, T.as_tensor(pos, device=dev)))
+                elif r == rank:
+                    self._recv.setdefault(src, []).append((cb[pos], pl[pos]))
+        # the receiver's writes grouped by coarse box: (start, stop) of each
+        # run within the concatenated message
+        self._recv_groups = {}
+        for s, items in self._recv.items():
+            cbs = np.concatenate([x[0] for x in items])
+            pls = np.concatenate([x[1] for x in items])
+            groups = []
+            for c in np.unique(cbs):
+                m = np.flatnonzero(cbs == c)
+                groups.append((int(c), T.as_tensor(m, device=dev), kji(int(c), pls[m])))
+            self._recv_groups[s] = (groups, int(cbs.size))
+
+    def _averages(self, t, ng):
+        """(NVAR, cells of the coarsened box) from a fine box's tensor."""
+        T = self.torch
+        v = t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng] if ng else t
+        c = T.zeros((NVAR, v.shape[1] // RR, v.shape[2] // RR, v.shape[3] // RR),
+                    dtype=T.float64, device=self.device)
+        for kr in range(RR):
+            for jr in range(RR):
+                for ir in range(RR):
+                    c = c + v[:, kr::RR, jr::RR, ir::RR]
+        return ((1.0 / float(RR ** 3)) * c).reshape(NVAR, -1)
+
+    def __call__(self, S_fine, S_coarse, ng_f=0, ng_c=0):
+        """S_fine: {fine box: tensor (NVAR, ...) covering the box grown by
+        ng_f} for this rank's fine boxes; S_coarse: {coarse box: tensor
+        covering it grown by ng_c} for this rank's coarse boxes, whose
+        covered valid cells are overwritten."""
+        T = self.torch
+        if sorted(S_fine) != self.mine_f:
+            raise ValueError("average-down needs exactly this rank's fine boxes")
+        avg = {b: self._averages(S_fine[b], ng_f) for b in self.mine_f}
+
+        def put(c, at, vals):
+            t = S_coarse[c]
+            v = t[:, ng_c:t.shape[1] - ng_c, ng_c:t.shape[2] - ng_c,
+                  ng_c:t.shape[3] - ng_c] if ng_c else t
+            v[:, at[0], at[1], at[2]] = vals
+
+        for b, pos, c, places in self._local:
+            put(c, places, avg[b][:, pos])
+        if self.pg is None or self.nranks == 1:
+            return
+        ops, bufs = [], {}
+        for r, items in sorted(self._send.items()):
+            buf = T.cat([avg[b][:, pos] for b, pos in items], dim=1).contiguous()
+            bufs[("s", r)] = buf
+            ops.append(self.pg.isend(buf, dst=r))
+        for s, (groups, cnt) in sorted(self._recv_groups.items()):
+            buf = T.empty((NVAR, cnt), dtype=T.float64, device=self.device)
+            bufs[("r", s)] = buf
+            ops.append(self.pg.irecv(buf, src=s))
+        for op in ops:
+            op.wait()
+        for s, (groups, _) in sorted(self._recv_groups.items()):
+            buf = bufs[("r", s)]
+            for c, sel, places in groups:
+                put(c, places, buf[:, sel])
+
+
+def _box_coords(lo, hi):
+    ax = [np.arange(lo[e], hi[e] + 1, dtype=np.int64) for e in range(3)]
+    K, J, I = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    return [I.ravel(), J.ravel(), K.ravel()]
+
+
+def _flat(ijk, dlo, n):
+    return (ijk[0] - dlo[0]) + n[0] * ((ijk[1] - dlo[1]) + n[1] * (ijk[2] - dlo[2]))

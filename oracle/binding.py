@@ -172,6 +172,8 @@ def load(kind="restate"):
     lib.orc_fluxreg_reflux.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, C.c_int, _DP,
                                        C.c_double,
                                        C.c_int, C.c_void_p, C.c_int, _DP, C.c_double, _DP]
+    lib.orc_avg_down.restype = None
+    lib.orc_avg_down.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, _DP, _DP]
     _LIBS[kind] = lib
     return lib
 
@@ -373,3 +375,12 @@ def fluxreg_reflux(kind, lev0, cboxes, cflux, dtdx_c, fboxes, fflux, dtdx_f, S0)
     load(kind).orc_fluxreg_reflux(C.byref(lev0), len(cb), cb.ctypes.data, len(cflux), cf,
                                   float(dtdx_c),
                                   len(fb), fb.ctypes.data, len(fflux), ff, float(dtdx_f), S0)
+
+
+def avg_down(kind, lev0, fboxes, fine_states, S0):
+    """The restated avgDown (orc_avg_down): S0's covered cells from the fine
+    boxes' states (fine_states[b]: NVAR x box, component slowest), in
+    place."""
+    fb = np.ascontiguousarray(fboxes, dtype=np.int32).reshape(-1, 6)
+    s1 = np.ascontiguousarray(np.concatenate([np.ravel(a) for a in fine_states]))
+    load(kind).orc_avg_down(C.byref(lev0), len(fb), fb.ctypes.data, s1, S0)

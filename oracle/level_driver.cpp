@@ -1163,6 +1163,31 @@ extern "C" void orc_fluxreg_reflux(const orc_level* lev0, int ncbox, const int* 
   });
 }
 
+// avgDown alone (the avg_down of orc_amr_run's post_timestep): S1 holds the
+// fine boxes' valid states back to back (NVAR comps each, i fastest); the
+// coarse cells they cover in S0 become the averages of their children.
+extern "C" void orc_avg_down(const orc_level* lev0, int nfbox, const int* fboxes, double* S1,
+                             double* S0) {
+  using namespace orc;
+  const Grid gc = make_grid(*lev0);
+  Fab Sc;
+  Sc.view(S0, gc.dom.lo, gc.dom.hi, NVAR);
+  Fine fn;
+  fn.S.resize(nfbox);
+  size_t off = 0;
+  for (int b = 0; b < nfbox; ++b) {
+    Box3 bx;
+    for (int d = 0; d < 3; ++d) {
+      bx.lo[d] = fboxes[6 * b + d];
+      bx.hi[d] = fboxes[6 * b + 3 + d];
+    }
+    fn.boxes.push_back(bx);
+    fn.S[b].view(S1 + off, bx.lo, bx.hi, NVAR);
+    off += size_t(fn.S[b].sn) * NVAR;
+  }
+  avg_down(gc, fn, Sc);
+}
+
 namespace orc {
 namespace {
 }  // namespace

@@ -186,3 +186,102 @@ def test_flux_register_two_ranks_matches_oracle(oracle_kind, fowner):
             assert nsend == 2     # fine boxes of rank 1 correct cells of both ranks
     got = _assemble(cboxes, parts)
     assert _same_bits(got, want)
+
+
+# ---- average-down across ranks (distributed.AverageDown) ----
+
+def _fine_states():
+    rng = np.random.default_rng(29)
+    out = []
+    for lo, hi in FBOXES:
+        a = rng.standard_normal((10,) + tuple(hi[e] - lo[e] + 1 for e in (2, 1, 0)))
+        a[1, 0, 0, :2] = -0.0
+        out.append(a)
+    return out
+
+
+def _avg_oracle(S):
+    import oracle
+    out = np.ascontiguousarray(S.copy())
+    fb = np.array([list(lo) + list(hi) for lo, hi in FBOXES])
+    oracle.avg_down("restate", oracle.make_level(N), fb, _fine_states(), out)
+    return out
+
+
+def _avg_rank(rank, world, cowner, fowner, pg, ng, device=None):
+    device = device or torch.device("cpu")
+    cboxes, S, _, _ = _inputs()
+    fs = _fine_states()
+    ad = D.AverageDown(hydro.make_geom(N), cboxes, cowner, FBOXES, fowner, rank, world,
+                       device, pg)
+    fine = {}
+    for b in ad.mine_f:
+        t = torch.full((10,) + tuple(s + 2 * ng for s in fs[b].shape[1:]), np.nan,
+                       dtype=torch.float64)
+        t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng] = torch.from_numpy(fs[b])
+        fine[b] = t.to(device)
+    crse = {}
+    for c, (lo, hi) in enumerate(cboxes):
+        if cowner[c] != rank:
+            continue
+        t = torch.full((10,) + tuple(hi[e] - lo[e] + 1 + 2 * ng for e in (2, 1, 0)), np.nan,
+                       dtype=torch.float64)
+        t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng, ng:t.shape[3] - ng] = torch.from_numpy(
+            S[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1])
+        crse[c] = t.to(device)
+    ad(fine, crse, ng_f=ng, ng_c=ng)
+    return {c: t[:, ng:t.shape[1] - ng, ng:t.shape[2] - ng,
+                 ng:t.shape[3] - ng].cpu().numpy().copy() for c, t in crse.items()}
+
+
+def test_average_down_one_rank_matches_oracle(oracle_kind):
+    cboxes, S, _, _ = _inputs()
+    want = _avg_oracle(S)
+    assert not _same_bits(want, S)
+    got = _assemble(cboxes, _avg_rank(0, 1, [0] * len(cboxes), [0] * len(FBOXES), None, 2))
+    assert _same_bits(got, want)
+
+
+@pytest.mark.gpu
+def test_average_down_on_device_matches_oracle(oracle_kind):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    cboxes, S, _, _ = _inputs()
+    want = _avg_oracle(S)
+    got = _assemble(cboxes, _avg_rank(0, 1, [0] * len(cboxes), [0] * len(FBOXES), None, 1,
+                                      torch.device("cuda:0")))
+    assert _same_bits(got, want)
+
+
+def _avg_worker(rank, world, port, fowner, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cboxes = hydro.level_boxes(N, MGS)
+        q.put((rank, _avg_rank(rank, world, D.sfc_partition(cboxes, world), fowner, dist, 1)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("fowner", [[0, 1, 0, 1, 1], [1, 1, 1, 1, 1]])
+def test_average_down_two_ranks_matches_oracle(oracle_kind, fowner):
+    world = 2
+    cboxes, S, _, _ = _inputs()
+    want = _avg_oracle(S)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_avg_worker, args=(r, world, port, fowner, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    parts = {}
+    for _, pr in res:
+        assert not set(pr) & set(parts)
+        parts.update(pr)
+    assert _same_bits(_assemble(cboxes, parts), want)
