@@ -128,6 +128,24 @@ def test_flux_register_on_device_matches_oracle(oracle_kind):
     assert _same_bits(_assemble(cboxes, parts), want)
 
 
+def test_flux_register_comparison_sees_the_order(oracle_kind):
+    """The oracle given the fine boxes in reverse order (its additions to a
+    cell that two boxes correct then come in the other order) differs from
+    the register in some bits: the bit-for-bit comparisons above check the
+    order of the additions, not only their sum."""
+    import oracle
+    cboxes, S, cflux, fflux = _inputs()
+    rev = np.ascontiguousarray(S.copy())
+    cb = np.array([list(lo) + list(hi) for lo, hi in cboxes])
+    fb = np.array([list(lo) + list(hi) for lo, hi in FBOXES[::-1]])
+    oracle.fluxreg_reflux("restate", oracle.make_level(N), cb, [cflux], DTDX_C, fb,
+                          [call[::-1] for call in fflux], DTDX_F, rev)
+    parts, _ = _run_rank(0, 1, [0] * len(cboxes), [0] * len(FBOXES), None, 0)
+    got = _assemble(cboxes, parts)
+    assert not _same_bits(got, rev)
+    assert np.allclose(got, rev, rtol=0, atol=1e-12)
+
+
 def test_flux_register_rejects_bad_boxes():
     geom = hydro.make_geom(N)
     cboxes = hydro.level_boxes(N, MGS)
