@@ -974,3 +974,244 @@ def _box_coords(lo, hi):
 
 def _flat(ijk, dlo, n):
     return (ijk[0] - dlo[0]) + n[0] * ((ijk[1] - dlo[1]) + n[1] * (ijk[2] - dlo[2]))
+
+
+class TwoLevelFill:
+    """The ghost cells of the fine boxes of a two-level hierarchy (ratio 2,
+    periodic domain) whose coarse and fine boxes are spread over the ranks:
+    the fill of FillPatchTwoLevels as the two-level driver does it
+    (Source/CAMR.cpp:1243-1250, AMReX FillPatchTwoLevels with
+    CellConservativeLinear):
+
+    * a ghost cell that a fine box covers (through the periodic domain)
+      takes that box's valid value;
+    * every other ghost cell takes the conservative linear interpolation of
+      the coarse data at time t: per direction an MC-limited slope of the
+      coarse cell holding it, one factor alpha <= 1 for the three slopes so
+      that no child leaves the min/max of the 27 coarse neighbours, and the
+      child at -+1/4 of each slope; the coarse data at t is the new (old)
+      state within 1e-3 (t1 - t0) of t1 (t0), else alpha old + beta new
+      (StateData::getData).
+
+    The coarse owners send the coarse cells each fine box's interpolation
+    reads (combined in time), the fine owners the valid cells other fine
+    boxes' ghosts copy, one message per pair of ranks; every value is formed
+    with the same operations in the same order as on one process, so the
+    result does not depend on the partition, bit for bit.  Boxes and owners
+    as for FluxRegister; every rank makes the same calls."""
+
+    def __init__(self, geom, cboxes, cowner, fboxes, fowner, rank=0, nranks=1, device=None,
+                 pg=None, ng=NG):
+        import torch
+        self.torch = torch
+        self.rank, self.nranks, self.pg, self.ng = rank, nranks, pg, ng
+        self.device = device or torch.device("cpu")
+        if not all(geom.is_periodic[d] for d in range(3)):
+            raise ValueError("the two-level fill needs a periodic domain")
+        T = torch
+        dev = self.device
+        dlo = np.array([geom.dom_lo[d] for d in range(3)])
+        n = np.array([geom.dom_hi[d] - geom.dom_lo[d] + 1 for d in range(3)])
+        fdlo, fn = RR * dlo, RR * n
+        self.cboxes = [(tuple(lo), tuple(hi)) for lo, hi in cboxes]
+        self.fboxes = [(tuple(lo), tuple(hi)) for lo, hi in fboxes]
+        cowner = np.asarray(cowner, dtype=np.int64)
+        fowner = np.asarray(fowner, dtype=np.int64)
+        self.mine_c = [c for c in range(len(self.cboxes)) if cowner[c] == rank]
+        self.mine_f = [b for b in range(len(self.fboxes)) if fowner[b] == rank]
+        ncell = int(np.prod(n))
+        cbox_of = np.full(ncell, -1, dtype=np.int64)
+        cloc = np.full(ncell, -1, dtype=np.int64)
+        for c, (lo, hi) in enumerate(self.cboxes):
+            cell = _flat(_box_coords(lo, hi), dlo, n)
+            cbox_of[cell] = c
+            cloc[cell] = np.arange(cell.size)
+        if (cbox_of < 0).any():
+            raise ValueError("the coarse boxes do not cover the domain")
+        cmap = np.full(ncell, -1, dtype=np.int64)
+        for b, (lo, hi) in enumerate(self.fboxes):
+            if any(lo[d] % RR or (hi[d] + 1) % RR or hi[d] < lo[d] for d in range(3)):
+                raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
+            cells = _flat(_box_coords([lo[d] // RR for d in range(3)],
+                                      [hi[d] // RR for d in range(3)]), dlo, n)
+            if (cmap[cells] >= 0).any():
+                raise ValueError(f"fine box {b} overlaps another")
+            cmap[cells] = b
+
+        # per fine box: fine-fine sources and the interpolated cells
+        coarse_items = {}   # (src rank, dst rank) -> [(fine box, coarse box, places, positions)]
+        fine_items = {}     # (src rank, dst rank) -> [(dst box, src box, src idx, dst idx)]
+        self._interp = {}   # fine box of this rank -> plan of its interpolated cells
+        for b, (lo, hi) in enumerate(self.fboxes):
+            glo = [lo[d] - ng for d in range(3)]
+            ghi = [hi[d] + ng for d in range(3)]
+            gext = [ghi[d] - glo[d] + 1 for d in range(3)]
+            f = _box_coords(glo, ghi)
+            gflat = np.arange(f[0].size)
+            ghost = np.zeros(f[0].size, dtype=bool)
+            for d in range(3):
+                ghost |= (f[d] < lo[d]) | (f[d] > hi[d])
+            f = [a[ghost] for a in f]
+            gflat = gflat[ghost]
+            w = [(f[d] - fdlo[d]) % fn[d] + fdlo[d] for d in range(3)]
+            ob = cmap[_flat([w[d] // RR for d in range(3)], dlo, n)]
+            rb = int(fowner[b])
+            # fine-fine copies, grouped by source box
+            for o in np.unique(ob[ob >= 0]):
+                m = ob == o
+                olo, ohi = self.fboxes[o]
+                oext = [ohi[d] - olo[d] + 1 + 2 * ng for d in range(3)]
+                sidx = ((w[0][m] - olo[0] + ng) + oext[0] * ((w[1][m] - olo[1] + ng)
+                                                              + oext[1] * (w[2][m] - olo[2] + ng)))
+                fine_items.setdefault((int(fowner[o]), rb), []).append(
+                    (b, int(o), sidx, gflat[m]))
+            # interpolated cells: the coarse cell holding each, its 27
+            # neighbours (dk, dj, di from -1 to 1) and the child's offsets
+            m = ob < 0
+            fi = [a[m] for a in f]
+            cc = [a // RR for a in fi]
+            nbr = []
+            for dk in (-1, 0, 1):
+                for dj in (-1, 0, 1):
+                    for di in (-1, 0, 1):
+                        nbr.append(_flat([(cc[0] + di - dlo[0]) % n[0] + dlo[0],
+                                          (cc[1] + dj - dlo[1]) % n[1] + dlo[1],
+                                          (cc[2] + dk - dlo[2]) % n[2] + dlo[2]], dlo, n))
+            nbr = np.stack(nbr) if fi[0].size else np.zeros((27, 0), dtype=np.int64)
+            uniq, inv = np.unique(nbr, return_inverse=True)
+            inv = inv.reshape(nbr.shape)
+            off = [np.where(fi[d] - RR * cc[d] == 0, -0.25, 0.25) for d in range(3)]
+            if rb == rank:
+                self._interp[b] = (T.as_tensor(gflat[m], device=dev),
+                                   T.as_tensor(inv, device=dev),
+                                   [T.as_tensor(o, device=dev) for o in off], int(uniq.size))
+            ucb = cbox_of[uniq]
+            uown = cowner[ucb]
+            for c in np.unique(ucb):
+                sel = np.flatnonzero(ucb == c)
+                coarse_items.setdefault((int(uown[sel[0]]), rb), []).append(
+                    (b, int(c), cloc[uniq[sel]], sel))
+
+        def tens(a):
+            return T.as_tensor(np.asarray(a, dtype=np.int64), device=dev)
+
+        # this rank's part of the plan: what it sends to and receives from
+        # each rank (itself included), in one order on both sides
+        self._send, self._recv = {}, {}
+        for r in range(nranks):
+            ci = coarse_items.get((rank, r), [])
+            fi_ = fine_items.get((rank, r), [])
+            if ci or fi_:
+                self._send[r] = ([(c, tens(pl)) for _, c, pl, _ in ci],
+                                 [(o, tens(si)) for _, o, si, _ in fi_],
+                                 sum(len(pl) for _, _, pl, _ in ci) + sum(len(si) for _, _, si, _ in fi_))
+            ci = coarse_items.get((r, rank), [])
+            fi_ = fine_items.get((r, rank), [])
+            if ci or fi_:
+                self._recv[r] = ([(b, tens(pos)) for b, _, _, pos in ci],
+                                 [(b, tens(di)) for b, _, _, di in fi_],
+                                 sum(len(pos) for _, _, _, pos in ci) + sum(len(di) for _, _, _, di in fi_))
+
+    @staticmethod
+    def time_weights(t0, t1, t):
+        """StateData::getData's choice: (0, new), (1, old) or (2, alpha, beta)."""
+        teps = (t1 - t0) * 1.e-3
+        if t1 - teps < t < t1 + teps:
+            return (0, 0.0, 0.0)
+        if t0 - teps < t < t0 + teps:
+            return (1, 0.0, 0.0)
+        return (2, (t1 - t) / (t1 - t0), (t - t0) / (t1 - t0))
+
+    def __call__(self, fine, c_old, c_new, t0, t1, t):
+        """fine: {fine box: contiguous tensor (NVAR, ...) covering the box
+        grown by ng, valid cells set} for this rank's fine boxes, whose
+        ghost cells are filled in place; c_old / c_new: {coarse box: tensor
+        (NVAR, ...) of its valid cells} for this rank's coarse boxes at
+        times t0 / t1."""
+        T = self.torch
+        if sorted(fine) != self.mine_f:
+            raise ValueError("the fill needs exactly this rank's fine boxes")
+        mode, wa, wb = self.time_weights(t0, t1, t)
+        cache = {}
+
+        def coarse_at(c):
+            if c not in cache:
+                o = c_old[c].reshape(NVAR, -1)
+                nw = c_new[c].reshape(NVAR, -1)
+                cache[c] = nw if mode == 0 else o if mode == 1 else wa * o + wb * nw
+            return cache[c]
+
+        def pack(r):
+            citems, fitems, _ = self._send[r]
+            parts = [coarse_at(c)[:, pl] for c, pl in citems]
+            parts += [fine[o].view(NVAR, -1)[:, si] for o, si in fitems]
+            return T.cat(parts, dim=1)
+
+        got = {}
+        if self.rank in self._send:
+            got[self.rank] = pack(self.rank)
+        if self.pg is not None and self.nranks > 1:
+            ops, bufs = [], {}
+            for r in sorted(self._send):
+                if r == self.rank:
+                    continue
+                bufs[("s", r)] = pack(r).contiguous()
+                ops.append(self.pg.isend(bufs[("s", r)], dst=r))
+            for r, (_, _, cnt) in sorted(self._recv.items()):
+                if r == self.rank:
+                    continue
+                bufs[("r", r)] = T.empty((NVAR, cnt), dtype=T.float64, device=self.device)
+                ops.append(self.pg.irecv(bufs[("r", r)], src=r))
+            for op in ops:
+                op.wait()
+            for r in self._recv:
+                if r != self.rank:
+                    got[r] = bufs[("r", r)]
+        # the coarse cells each fine box reads, and the fine-fine copies
+        compact = {b: T.empty((NVAR, self._interp[b][3]), dtype=T.float64, device=self.device)
+                   for b in self.mine_f}
+        for r, (citems, fitems, _) in self._recv.items():
+            buf = got[r]
+            at = 0
+            for b, pos in citems:
+                k = pos.numel()
+                compact[b][:, pos] = buf[:, at:at + k]
+                at += k
+            for b, di in fitems:
+                k = di.numel()
+                fine[b].view(NVAR, -1)[:, di] = buf[:, at:at + k]
+                at += k
+        for b in self.mine_f:
+            gidx, inv, off, _ = self._interp[b]
+            if gidx.numel():
+                fine[b].view(NVAR, -1)[:, gidx] = self._cons_interp(compact[b], inv, off)
+
+    def _cons_interp(self, cv, inv, off):
+        """CellConservativeLinear (ratio 2, limited), the operations of the
+        single-process fill in its order; std::min / std::max are written
+        as the selects they are."""
+        T = self.torch
+        at = [cv[:, inv[q]] for q in range(27)]     # (dk, dj, di) from -1 to 1
+        uc = at[13]
+        sl = []
+        for step in (1, 3, 9):                      # x, y, z neighbours
+            up, um = at[13 + step], at[13 - step]
+            dc = 0.5 * (up - um)
+            df = 2.0 * (up - uc)
+            db = 2.0 * (uc - um)
+            adf, adb = df.abs(), db.abs()
+            sv = T.where(df * db >= 0.0, T.where(adb < adf, adb, adf), T.zeros_like(df))
+            adc = dc.abs()
+            sv = T.copysign(T.ones_like(dc), dc) * T.where(adc < sv, adc, sv)
+            sl.append(sv)
+        anyn = (sl[0] != 0.0) | (sl[1] != 0.0) | (sl[2] != 0.0)
+        dumax = sl[0].abs() * 0.25 + sl[1].abs() * 0.25 + sl[2].abs() * 0.25
+        umax, umin = uc, uc
+        for q in range(27):
+            v = at[q]
+            umax = T.where(umax < v, v, umax)
+            umin = T.where(v < umin, v, umin)
+        alpha = T.ones_like(uc)
+        alpha = T.where(anyn & (dumax * alpha > (umax - uc)), (umax - uc) / dumax, alpha)
+        alpha = T.where(anyn & (dumax * alpha > (uc - umin)), (uc - umin) / dumax, alpha)
+        return uc + off[0] * (sl[0] * alpha) + off[1] * (sl[1] * alpha) + off[2] * (sl[2] * alpha)

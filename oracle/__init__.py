@@ -16,5 +16,5 @@ from .binding import (  # noqa: F401
     hydro_box, advance, advance_fixed_dt, est_dt, init_finalize,
     expand_state, clean_state, amr_run, build, lib_path, lib_path_eb, hydro_box_eb,
     eb_advance, eb_init_finalize, ref_ctoprim, ref_hydro_box_full,
-    count_flops, lib_path_flops, fluxreg_reflux, avg_down,
+    count_flops, lib_path_flops, fluxreg_reflux, avg_down, fine_fill_ghosts,
 )

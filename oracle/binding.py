@@ -172,6 +172,9 @@ def load(kind="restate"):
     lib.orc_fluxreg_reflux.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, C.c_int, _DP,
                                        C.c_double,
                                        C.c_int, C.c_void_p, C.c_int, _DP, C.c_double, _DP]
+    lib.orc_fine_fill_ghosts.restype = None
+    lib.orc_fine_fill_ghosts.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, _DP, _DP, _DP,
+                                         C.c_double, C.c_double, C.c_double]
     lib.orc_avg_down.restype = None
     lib.orc_avg_down.argtypes = [C.POINTER(Level), C.c_int, C.c_void_p, _DP, _DP]
     _LIBS[kind] = lib
@@ -384,3 +387,21 @@ def avg_down(kind, lev0, fboxes, fine_states, S0):
     fb = np.ascontiguousarray(fboxes, dtype=np.int32).reshape(-1, 6)
     s1 = np.ascontiguousarray(np.concatenate([np.ravel(a) for a in fine_states]))
     load(kind).orc_avg_down(C.byref(lev0), len(fb), fb.ctypes.data, s1, S0)
+
+
+def fine_fill_ghosts(kind, lev0, fboxes, grown, c_old, c_new, t0, t1, t):
+    """The restated two-level ghost fill (orc_fine_fill_ghosts) of the fine
+    boxes' grown-by-4 states grown[b] (NVAR x grown box, valid cells set),
+    from the coarse states c_old / c_new at times t0 / t1, for time t.
+    Returns the filled arrays."""
+    fb = np.ascontiguousarray(fboxes, dtype=np.int32).reshape(-1, 6)
+    sizes = [a.size for a in grown]
+    flat = np.ascontiguousarray(np.concatenate([np.ravel(a) for a in grown]))
+    load(kind).orc_fine_fill_ghosts(C.byref(lev0), len(fb), fb.ctypes.data, flat,
+                                    np.ascontiguousarray(c_old), np.ascontiguousarray(c_new),
+                                    float(t0), float(t1), float(t))
+    out, at = [], 0
+    for a, k in zip(grown, sizes):
+        out.append(flat[at:at + k].reshape(a.shape))
+        at += k
+    return out

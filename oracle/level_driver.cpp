@@ -1188,6 +1188,64 @@ extern "C" void orc_avg_down(const orc_level* lev0, int nfbox, const int* fboxes
   avg_down(gc, fn, Sc);
 }
 
+// The ghost cells of FillPatchTwoLevels alone (fine_expand's fill, without
+// its cleaning passes): Bv holds each fine box grown by 4 back to back (NVAR
+// comps each, i fastest) with the valid cells set; every ghost cell that a
+// fine box covers (through the periodic domain) gets that box's valid
+// value, every other one the conservative interpolation of the coarse data
+// at time t from c_old (time t0) and c_new (time t1).
+extern "C" void orc_fine_fill_ghosts(const orc_level* lev0, int nfbox, const int* fboxes,
+                                     double* Bv, const double* c_old, const double* c_new,
+                                     double t0, double t1, double t) {
+  using namespace orc;
+  const orc_level& Lc = *lev0;
+  const Grid gc = make_grid(Lc);
+  Fab Co, Cn;
+  Co.view(const_cast<double*>(c_old), gc.dom.lo, gc.dom.hi, NVAR);
+  Cn.view(const_cast<double*>(c_new), gc.dom.lo, gc.dom.hi, NVAR);
+  Fine fn;
+  fn.L = Lc;
+  for (int d = 0; d < 3; ++d) {
+    fn.L.dom_lo[d] = Lc.dom_lo[d] * RR;
+    fn.L.dom_hi[d] = (Lc.dom_hi[d] + 1) * RR - 1;
+    fn.L.dx[d] = Lc.dx[d] / RR;
+  }
+  std::vector<Fab> B(nfbox);
+  size_t off = 0;
+  for (int b = 0; b < nfbox; ++b) {
+    Box3 bx;
+    for (int d = 0; d < 3; ++d) {
+      bx.lo[d] = fboxes[6 * b + d];
+      bx.hi[d] = fboxes[6 * b + 3 + d];
+    }
+    fn.boxes.push_back(bx);
+    const Box3 g4 = grow(bx, 4);
+    B[b].view(Bv + off, g4.lo, g4.hi, NVAR);
+    off += size_t(B[b].sn) * NVAR;
+  }
+  const FluxReg fr = make_fluxreg(gc, Lc, fn.boxes);
+  CoarseAt C{&Co, &Cn, t0, t1, t, 0, 0.0, 0.0};
+  C.init();
+  fine_fill_boundary(fn, fr, B);
+  int fdlo[3], fn_n[3];
+  for (int d = 0; d < 3; ++d) {
+    fdlo[d] = fn.L.dom_lo[d];
+    fn_n[d] = fn.L.dom_hi[d] - fn.L.dom_lo[d] + 1;
+  }
+  for (int b = 0; b < nfbox; ++b) {
+    const Box3& bx = fn.boxes[b];
+    for_box(grow(bx, 4), [&](int i, int j, int k) {
+      const bool valid = i >= bx.lo[0] && i <= bx.hi[0] && j >= bx.lo[1] && j <= bx.hi[1] &&
+                         k >= bx.lo[2] && k <= bx.hi[2];
+      if (valid) return;
+      const int wi = wrap(i, fdlo[0], fn_n[0]), wj = wrap(j, fdlo[1], fn_n[1]),
+                wk = wrap(k, fdlo[2], fn_n[2]);
+      if (fr.box_at(wi / RR, wj / RR, wk / RR) < 0)
+        for (int n = 0; n < NVAR; ++n) B[b](i, j, k, n) = cons_interp(C, gc, i, j, k, n);
+    });
+  }
+}
+
 namespace orc {
 namespace {
 }  // namespace
