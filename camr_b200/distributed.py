@@ -32,6 +32,24 @@ from . import native
 
 NVAR = native.NVAR
 NG = 4
+RR = 2  # refinement ratio of a two-level hierarchy
+
+
+def _box_coords(lo, hi):
+    """(i, j, k) of every cell of [lo, hi], i fastest, as three arrays."""
+    ax = [np.arange(lo[e], hi[e] + 1, dtype=np.int64) for e in range(3)]
+    K, J, I = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    return [I.ravel(), J.ravel(), K.ravel()]
+
+
+def _flat(ijk, dlo, n):
+    """Flat index (i fastest) of in-domain cells of a domain at dlo of size n."""
+    return (ijk[0] - dlo[0]) + n[0] * ((ijk[1] - dlo[1]) + n[1] * (ijk[2] - dlo[2]))
+
+
+def _wrap_flat(ijk, dlo, n):
+    """Flat index of the periodic images of any cells."""
+    return _flat([(ijk[e] - dlo[e]) % n[e] + dlo[e] for e in range(3)], dlo, n)
 
 
 def morton_key(lo, bits=21):
@@ -503,8 +521,6 @@ class DistributedLevel:
         self.S = S
 
 
-RR = 2  # refinement ratio of the two-level hierarchy
-
 
 class FluxRegister:
     """The two-level flux register (refinement ratio 2) of a hierarchy whose
@@ -564,14 +580,15 @@ class FluxRegister:
         # coarse cell (flat, i fastest) -> coarse box, and -> fine box or -1
         cbox_of = np.full(ncell, -1, dtype=np.int64)
         for c, (lo, hi) in enumerate(self.cboxes):
-            cbox_of[self._cells(lo, hi)] = c
+            cbox_of[_wrap_flat(_box_coords(lo, hi), dlo, n)] = c
         if (cbox_of < 0).any():
             raise ValueError("the coarse boxes do not cover the domain")
         cmap = np.full(ncell, -1, dtype=np.int64)
         for b, (lo, hi) in enumerate(self.fboxes):
             if any(lo[d] % RR or (hi[d] + 1) % RR or hi[d] < lo[d] for d in range(3)):
                 raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
-            cells = self._cells([lo[d] // RR for d in range(3)], [hi[d] // RR for d in range(3)])
+            cells = _wrap_flat(_box_coords([lo[d] // RR for d in range(3)],
+                                           [hi[d] // RR for d in range(3)]), dlo, n)
             if (cmap[cells] >= 0).any():
                 raise ValueError(f"fine box {b} overlaps another")
             cmap[cells] = b
@@ -599,8 +616,8 @@ class FluxRegister:
         unit = np.eye(3, dtype=np.int64)
         for c in self.mine_c:
             lo, hi = self.cboxes[c]
-            ijk = self._coords(lo, hi)
-            cell = self._wrap_flat(ijk)
+            ijk = _box_coords(lo, hi)
+            cell = _wrap_flat(ijk, dlo, n)
             sel = bnd[cell]
             ijk = [a[sel] for a in ijk]
             reg = reg_of[cell[sel]]
@@ -609,7 +626,7 @@ class FluxRegister:
                 ext = [hi[e] - lo[e] + 1 + (e == d) for e in range(3)]
                 for side in (0, 1):
                     nb = [ijk[e] + (unit[d][e] if side else -unit[d][e]) for e in range(3)]
-                    m = cmap[self._wrap_flat(nb)] >= 0
+                    m = cmap[_wrap_flat(nb, dlo, n)] >= 0
                     if not m.any():
                         continue
                     f = [ijk[e][m] + (unit[d][e] if side else 0) - lo[e] for e in range(3)]
@@ -632,8 +649,8 @@ class FluxRegister:
                     alo, ahi = list(clo), list(chi)
                     alo[d] = ahi[d] = chi[d] + 1 if side else clo[d] - 1
                     fface = RR * (chi[d] + 1) if side else RR * clo[d]
-                    ijk = self._coords(alo, ahi)
-                    cell = self._wrap_flat(ijk)
+                    ijk = _box_coords(alo, ahi)
+                    cell = _wrap_flat(ijk, dlo, n)
                     keep = cmap[cell] < 0
                     ijk = [a[keep] for a in ijk]
                     cell = cell[keep]
@@ -701,7 +718,7 @@ class FluxRegister:
         self._apply = {}
         for c in self.mine_c:
             lo, hi = self.cboxes[c]
-            cell = self._wrap_flat(self._coords(lo, hi))
+            cell = _wrap_flat(_box_coords(lo, hi), dlo, n)
             loc = np.flatnonzero(reg_of[cell] >= 0)
             self._apply[c] = (T.as_tensor(loc, device=dev), T.as_tensor(reg_of[cell[loc]], device=dev))
         self.reset()
@@ -720,19 +737,6 @@ class FluxRegister:
         call's fac_for_reflux * dt / vol, over the ratio^3 fine cells of a
         coarse cell (YAFluxRegister's FineAdd, ratio 2)."""
         return ((0.5 if mol else 1.0) * dt_f) / ((dx_f[0] * dx_f[1] * dx_f[2]) * float(RR ** 3))
-
-    # ---- index helpers (coarse index space, i fastest) ----
-    def _coords(self, lo, hi):
-        ax = [np.arange(lo[e], hi[e] + 1, dtype=np.int64) for e in range(3)]
-        K, J, I = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
-        return [I.ravel(), J.ravel(), K.ravel()]
-
-    def _wrap_flat(self, ijk):
-        w = [(ijk[e] - self.dlo[e]) % self.n[e] for e in range(3)]
-        return w[0] + self.n[0] * (w[1] + self.n[1] * w[2])
-
-    def _cells(self, lo, hi):
-        return self._wrap_flat(self._coords(lo, hi))
 
     # ---- the register ----
     def reset(self):
@@ -965,15 +969,6 @@ class AverageDown:
             for c, sel, places in groups:
                 put(c, places, buf[:, sel])
 
-
-def _box_coords(lo, hi):
-    ax = [np.arange(lo[e], hi[e] + 1, dtype=np.int64) for e in range(3)]
-    K, J, I = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
-    return [I.ravel(), J.ravel(), K.ravel()]
-
-
-def _flat(ijk, dlo, n):
-    return (ijk[0] - dlo[0]) + n[0] * ((ijk[1] - dlo[1]) + n[1] * (ijk[2] - dlo[2]))
 
 
 class TwoLevelFill:
