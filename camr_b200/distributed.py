@@ -1065,16 +1065,24 @@ class TwoLevelFill:
             m = ob < 0
             fi = [a[m] for a in f]
             cc = [a // RR for a in fi]
+            # every coarse cell those read lies in one index box around the
+            # coarsened ghost region; a mask over it picks the ones read
+            blo = [(lo[d] - ng) // RR - 1 for d in range(3)]
+            bext = [(hi[d] + ng) // RR + 1 - blo[d] + 1 for d in range(3)]
             nbr = []
             for dk in (-1, 0, 1):
                 for dj in (-1, 0, 1):
                     for di in (-1, 0, 1):
-                        nbr.append(_flat([(cc[0] + di - dlo[0]) % n[0] + dlo[0],
-                                          (cc[1] + dj - dlo[1]) % n[1] + dlo[1],
-                                          (cc[2] + dk - dlo[2]) % n[2] + dlo[2]], dlo, n))
+                        nbr.append((cc[0] + di - blo[0]) + bext[0] * (
+                            (cc[1] + dj - blo[1]) + bext[1] * (cc[2] + dk - blo[2])))
             nbr = np.stack(nbr) if fi[0].size else np.zeros((27, 0), dtype=np.int64)
-            uniq, inv = np.unique(nbr, return_inverse=True)
-            inv = inv.reshape(nbr.shape)
+            need = np.zeros(bext[0] * bext[1] * bext[2], dtype=bool)
+            need[nbr.ravel()] = True
+            inv = (np.cumsum(need) - 1)[nbr]
+            loc = np.flatnonzero(need)
+            bc = [loc % bext[0] + blo[0], (loc // bext[0]) % bext[1] + blo[1],
+                  loc // (bext[0] * bext[1]) + blo[2]]
+            uniq = _wrap_flat(bc, dlo, n)
             off = [np.where(fi[d] - RR * cc[d] == 0, -0.25, 0.25) for d in range(3)]
             if rb == rank:
                 self._interp[b] = (T.as_tensor(gflat[m], device=dev),
