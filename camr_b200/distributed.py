@@ -52,6 +52,42 @@ def _wrap_flat(ijk, dlo, n):
     return _flat([(ijk[e] - dlo[e]) % n[e] + dlo[e] for e in range(3)], dlo, n)
 
 
+def _hierarchy_maps(cboxes, fboxes, dlo, n):
+    """The checks and maps the two-level pieces share.  The coarse boxes
+    must lie in the domain, be disjoint and cover it; the fine boxes must be
+    aligned to the refinement ratio (lo even, hi odd), lie in the fine
+    domain and be disjoint.  Returns, over the flat coarse cells: the coarse
+    box holding each, its flat place in that box, and the fine box covering
+    it (-1 if none)."""
+    ncell = int(np.prod(n))
+    dhi = [dlo[d] + n[d] - 1 for d in range(3)]
+    cbox_of = np.full(ncell, -1, dtype=np.int64)
+    cloc = np.full(ncell, -1, dtype=np.int64)
+    for c, (lo, hi) in enumerate(cboxes):
+        if any(lo[d] < dlo[d] or hi[d] > dhi[d] or hi[d] < lo[d] for d in range(3)):
+            raise ValueError(f"coarse box {c} lies outside the domain or is empty")
+        cell = _flat(_box_coords(lo, hi), dlo, n)
+        if (cbox_of[cell] >= 0).any():
+            raise ValueError(f"coarse box {c} overlaps another")
+        cbox_of[cell] = c
+        cloc[cell] = np.arange(cell.size)
+    if (cbox_of < 0).any():
+        raise ValueError("the coarse boxes do not cover the domain")
+    cmap = np.full(ncell, -1, dtype=np.int64)
+    for b, (lo, hi) in enumerate(fboxes):
+        if any(lo[d] % RR or (hi[d] + 1) % RR or hi[d] < lo[d] for d in range(3)):
+            raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
+        clo = [lo[d] // RR for d in range(3)]
+        chi = [hi[d] // RR for d in range(3)]
+        if any(clo[d] < dlo[d] or chi[d] > dhi[d] for d in range(3)):
+            raise ValueError(f"fine box {b} lies outside the domain")
+        cells = _flat(_box_coords(clo, chi), dlo, n)
+        if (cmap[cells] >= 0).any():
+            raise ValueError(f"fine box {b} overlaps another")
+        cmap[cells] = b
+    return cbox_of, cloc, cmap
+
+
 def morton_key(lo, bits=21):
     """Interleaved bits of three non-negative integers (x lowest)."""
     key = 0
@@ -578,20 +614,7 @@ class FluxRegister:
         self.fowner = np.asarray(fowner, dtype=np.int64)
 
         # coarse cell (flat, i fastest) -> coarse box, and -> fine box or -1
-        cbox_of = np.full(ncell, -1, dtype=np.int64)
-        for c, (lo, hi) in enumerate(self.cboxes):
-            cbox_of[_wrap_flat(_box_coords(lo, hi), dlo, n)] = c
-        if (cbox_of < 0).any():
-            raise ValueError("the coarse boxes do not cover the domain")
-        cmap = np.full(ncell, -1, dtype=np.int64)
-        for b, (lo, hi) in enumerate(self.fboxes):
-            if any(lo[d] % RR or (hi[d] + 1) % RR or hi[d] < lo[d] for d in range(3)):
-                raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
-            cells = _wrap_flat(_box_coords([lo[d] // RR for d in range(3)],
-                                           [hi[d] // RR for d in range(3)]), dlo, n)
-            if (cmap[cells] >= 0).any():
-                raise ValueError(f"fine box {b} overlaps another")
-            cmap[cells] = b
+        cbox_of, _, cmap = _hierarchy_maps(self.cboxes, self.fboxes, dlo, n)
         cov = (cmap >= 0).reshape(n[2], n[1], n[0])
         near = np.zeros_like(cov)
         for ax in range(3):
@@ -861,16 +884,7 @@ class AverageDown:
         self.fboxes = [(tuple(lo), tuple(hi)) for lo, hi in fboxes]
         cowner = np.asarray(cowner, dtype=np.int64)
         fowner = np.asarray(fowner, dtype=np.int64)
-        ncell = int(np.prod(n))
-        cbox_of = np.full(ncell, -1, dtype=np.int64)
-        cloc = np.full(ncell, -1, dtype=np.int64)   # flat index inside its coarse box
-        for c, (lo, hi) in enumerate(self.cboxes):
-            ijk = _box_coords(lo, hi)
-            cell = _flat(ijk, dlo, n)
-            cbox_of[cell] = c
-            cloc[cell] = np.arange(cell.size)
-        if (cbox_of < 0).any():
-            raise ValueError("the coarse boxes do not cover the domain")
+        cbox_of, cloc, _ = _hierarchy_maps(self.cboxes, self.fboxes, dlo, n)
         self.mine_f = [b for b in range(len(self.fboxes)) if fowner[b] == rank]
         T = torch
         dev = self.device
@@ -887,12 +901,8 @@ class AverageDown:
         self._recv = {}   # src rank -> [(coarse box, place) per entry, in message order]
         self._local = []  # (fine box, positions, coarse box, places) on this rank
         for b, (flo, fhi) in enumerate(self.fboxes):
-            if any(flo[d] % RR or (fhi[d] + 1) % RR or fhi[d] < flo[d] for d in range(3)):
-                raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
             clo = [flo[d] // RR for d in range(3)]
             chi = [fhi[d] // RR for d in range(3)]
-            if any(clo[d] < dlo[d] or chi[d] > dhi[d] for d in range(3)):
-                raise ValueError(f"fine box {b} lies outside the domain")
             cell = _flat(_box_coords(clo, chi), dlo, n)
             cb, pl = cbox_of[cell], cloc[cell]
             dest = cowner[cb]
@@ -1014,24 +1024,7 @@ class TwoLevelFill:
         fowner = np.asarray(fowner, dtype=np.int64)
         self.mine_c = [c for c in range(len(self.cboxes)) if cowner[c] == rank]
         self.mine_f = [b for b in range(len(self.fboxes)) if fowner[b] == rank]
-        ncell = int(np.prod(n))
-        cbox_of = np.full(ncell, -1, dtype=np.int64)
-        cloc = np.full(ncell, -1, dtype=np.int64)
-        for c, (lo, hi) in enumerate(self.cboxes):
-            cell = _flat(_box_coords(lo, hi), dlo, n)
-            cbox_of[cell] = c
-            cloc[cell] = np.arange(cell.size)
-        if (cbox_of < 0).any():
-            raise ValueError("the coarse boxes do not cover the domain")
-        cmap = np.full(ncell, -1, dtype=np.int64)
-        for b, (lo, hi) in enumerate(self.fboxes):
-            if any(lo[d] % RR or (hi[d] + 1) % RR or hi[d] < lo[d] for d in range(3)):
-                raise ValueError(f"fine box {b} is not aligned to the refinement ratio")
-            cells = _flat(_box_coords([lo[d] // RR for d in range(3)],
-                                      [hi[d] // RR for d in range(3)]), dlo, n)
-            if (cmap[cells] >= 0).any():
-                raise ValueError(f"fine box {b} overlaps another")
-            cmap[cells] = b
+        cbox_of, cloc, cmap = _hierarchy_maps(self.cboxes, self.fboxes, dlo, n)
 
         # per fine box: fine-fine sources and the interpolated cells
         coarse_items = {}   # (src rank, dst rank) -> [(fine box, coarse box, places, positions)]

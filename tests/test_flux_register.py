@@ -157,6 +157,19 @@ def test_flux_register_rejects_bad_boxes():
     walls = hydro.make_geom(N, is_periodic=(0, 1, 1), bc_lo=(2, 0, 0), bc_hi=(2, 0, 0))
     with pytest.raises(ValueError):
         D.FluxRegister(walls, cboxes, [0] * len(cboxes), FBOXES, [0] * len(FBOXES))
+    # every two-level piece refuses boxes outside the domain, overlapping
+    # coarse boxes and coarse boxes that leave cells uncovered
+    for cls in (D.FluxRegister, D.AverageDown, D.TwoLevelFill):
+        with pytest.raises(ValueError, match="outside the domain"):
+            cls(geom, cboxes, [0] * len(cboxes), [((30, 0, 0), (33, 3, 3))], [0])
+        with pytest.raises(ValueError, match="outside the domain"):
+            cls(geom, cboxes, [0] * len(cboxes), [((-4, 0, 0), (-1, 3, 3))], [0])
+        with pytest.raises(ValueError, match="overlaps"):
+            cls(geom, cboxes + [cboxes[0]], [0] * (len(cboxes) + 1), FBOXES, [0] * len(FBOXES))
+        with pytest.raises(ValueError, match="do not cover"):
+            cls(geom, cboxes[1:], [0] * (len(cboxes) - 1), FBOXES, [0] * len(FBOXES))
+        with pytest.raises(ValueError, match="not aligned"):
+            cls(geom, cboxes, [0] * len(cboxes), [((1, 0, 0), (4, 3, 3))], [0])
 
 
 def _free_port():
