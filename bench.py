@@ -365,6 +365,17 @@ def run_camr(args, world, rank, local, pg):
     ms = e0.elapsed_time(e1)
     launches = lib.camr_launch_count() - launches0
     err = L.error()
+    # conservation over the timed steps, outside the timed region: the
+    # integrated quantities of the state they started from and of the one
+    # they left (a periodic domain: mass and total energy to round-off)
+    try:
+        from camr_b200 import metrics
+        dxs = tuple(geom.dx[d] for d in range(3))
+        conservation = dict(metrics.drift(metrics.integrated_quantities(s_start, dxs),
+                                          metrics.integrated_quantities(L.get_state(), dxs)),
+                            steps=args.steps)
+    except Exception as exc:  # a diagnostic: it never costs the benchmark line
+        conservation = {"error": f"{type(exc).__name__}: {exc}"}
     ms = max_over_ranks(ms, pg)
     ms_step = ms / args.steps
     value = whole_job_rate(world, zones, args.steps, ms)
@@ -473,6 +484,7 @@ def run_camr(args, world, rank, local, pg):
             "config": c1_config(n, world),
             "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "conservation": conservation,
             "stages_ms": acc, "device_error": list(err),
             "batched_amr_patches": batched,
             "amr_two_level": amr,
