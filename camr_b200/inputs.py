@@ -170,3 +170,16 @@ def redistribution(table):
     if w not in REDIST:
         raise ValueError(f"CAMR.redistribution_type: {w!r} is not one of {sorted(REDIST)}")
     return REDIST[w]
+
+
+READ_NAMES = (tuple("CAMR." + f for f in INT_FIELDS + REAL_FIELDS)
+              + ("eos.gamma", "CAMR.lo_bc", "CAMR.hi_bc", "CAMR.redistribution_type",
+                 "amr.n_cell", "amr.max_grid_size", "geometry.prob_lo", "geometry.prob_hi",
+                 "geometry.is_periodic"))
+
+
+def unused(table):
+    """The names of the file that none of this module's readers act on (run
+    control, tagging, plotting, reactions ...), sorted: what a CAMR run of
+    the same file would do that this library leaves to its caller."""
+    return sorted(k for k in table if k not in READ_NAMES)

@@ -105,3 +105,10 @@ def test_geometry_needs_its_sizes(native_lib):
                      "CAMR.lo_bc = Interior Interior Interior\n"
                      "CAMR.hi_bc = Interior Interior Interior")
     assert inputs.geometry(t)[1] is None
+
+
+def test_unused_names_are_listed():
+    t = inputs.parse(SOD_X + "amr.max_level = 2\nCAMR.do_react = 0\namr.plot_int = 10\n")
+    assert inputs.unused(t) == ["CAMR.do_react", "amr.max_level", "amr.plot_int",
+                                "max_step", "stop_time"]
+    assert "CAMR.cfl" not in inputs.unused(t) and "eos.gamma" not in inputs.unused(t)
