@@ -37,12 +37,23 @@ REAL_FIELDS = ("difmag", "small", "small_dens", "small_temp", "small_pres",
 REDIST = {"NoRedist": 0, "FluxRedist": 1, "StateRedist": 2}
 
 
+def _strip_comment(line):
+    """The line up to its first `#` outside double quotes."""
+    quoted = False
+    for k, ch in enumerate(line):
+        if ch == '"':
+            quoted = not quoted
+        elif ch == "#" and not quoted:
+            return line[:k]
+    return line
+
+
 def parse(text, overrides=()):
     """{name: [values]} from ParmParse text plus `name=value ...` overrides."""
     table = {}
 
     def take(line, where):
-        line = line.split("#", 1)[0].strip()
+        line = _strip_comment(line).strip()
         if not line:
             return
         if "=" not in line:

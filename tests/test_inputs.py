@@ -112,3 +112,9 @@ def test_unused_names_are_listed():
     assert inputs.unused(t) == ["CAMR.do_react", "amr.max_level", "amr.plot_int",
                                 "max_step", "stop_time"]
     assert "CAMR.cfl" not in inputs.unused(t) and "eos.gamma" not in inputs.unused(t)
+
+
+def test_quotes_keep_blanks_and_hashes():
+    t = inputs.parse('CAMR.job_name = "run #3 of 5"   # a comment\nx = a "b c" d')
+    assert t["CAMR.job_name"] == ["run #3 of 5"]
+    assert t["x"] == ["a", "b c", "d"]
