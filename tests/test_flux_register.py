@@ -316,3 +316,36 @@ def test_average_down_several_ranks_matches_oracle(oracle_kind, world, fowner):
         assert not set(pr) & set(parts)
         parts.update(pr)
     assert _same_bits(_assemble(cboxes, parts), want)
+
+
+def test_flux_register_two_coarse_calls_and_reset(oracle_kind):
+    """Two CrseAdd calls per coarse step (the MOL stages) accumulate in call
+    order as the oracle's register does; after reset() a reflux with no new
+    calls leaves the state's values as they are (it adds +0)."""
+    import oracle
+    cboxes, S, cflux, fflux = _inputs()
+    rng = np.random.default_rng(12)
+    cflux2 = [[rng.standard_normal(a.shape) for a in per] for per in cflux]
+    want = np.ascontiguousarray(S.copy())
+    cb = np.array([list(lo) + list(hi) for lo, hi in cboxes])
+    fb = np.array([list(lo) + list(hi) for lo, hi in FBOXES])
+    oracle.fluxreg_reflux("restate", oracle.make_level(N), cb, [cflux, cflux2], DTDX_C, fb,
+                          fflux, DTDX_F, want)
+    fr = D.FluxRegister(hydro.make_geom(N), cboxes, [0] * len(cboxes), FBOXES,
+                        [0] * len(FBOXES))
+    for calls in (cflux, cflux2):
+        fr.crse_add({c: [torch.from_numpy(a) for a in calls[c]] for c in fr.mine_c}, DTDX_C)
+    for call in range(NCALL):
+        fr.fine_add({b: [torch.from_numpy(a) for a in fflux[call][b]] for b in fr.mine_f},
+                    DTDX_F)
+    mine = {}
+    for c, (lo, hi) in enumerate(cboxes):
+        mine[c] = torch.from_numpy(np.ascontiguousarray(
+            S[:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]))
+    fr.reflux(mine)
+    got = _assemble(cboxes, {c: t.numpy() for c, t in mine.items()})
+    assert _same_bits(got, want)
+    fr.reset()
+    fr.reflux(mine)
+    again = _assemble(cboxes, {c: t.numpy() for c, t in mine.items()})
+    assert np.array_equal(again, want)
