@@ -361,9 +361,13 @@ class DistributedLevel:
     def attach_flux_register(self, fr, role):
         """After every hydro call of this level, pass its boxes' face fluxes
         to the flux register fr: CrseAdd when this level is the register's
-        coarse level (role "coarse"), FineAdd when it is the fine level
-        (role "fine"), scaled as construct_hydro_source does
-        (Source/Hydro/CAMR_construct_hydro_source.cpp:240-252)."""
+        coarse level (role "coarse": the register's coarse boxes are this
+        level's boxes, in their order), FineAdd when it is the fine level
+        (role "fine": the register's fine boxes are this level's boxes, in
+        their order, as for a fine level that covers its domain), scaled as
+        construct_hydro_source does
+        (Source/Hydro/CAMR_construct_hydro_source.cpp:240-252).  A register
+        given other boxes refuses the calls (ValueError)."""
         if role not in ("coarse", "fine"):
             raise ValueError(role)
         self.registers.append((fr, role))
