@@ -367,9 +367,14 @@ class DistributedLevel:
         their order, as for a fine level that covers its domain), scaled as
         construct_hydro_source does
         (Source/Hydro/CAMR_construct_hydro_source.cpp:240-252).  A register
-        given other boxes refuses the calls (ValueError)."""
+        built on other boxes is refused here (ValueError)."""
         if role not in ("coarse", "fine"):
             raise ValueError(role)
+        theirs = getattr(fr, "cboxes" if role == "coarse" else "fboxes", None)
+        if theirs is not None:
+            norm = [(tuple(lo), tuple(hi)) for lo, hi in theirs]
+            if norm != [(tuple(lo), tuple(hi)) for lo, hi in self.boxes]:
+                raise ValueError(f"the register's {role} boxes are not this level's boxes")
         self.registers.append((fr, role))
 
     # ---- state in and out (the valid cells of this rank's boxes) ----

@@ -19,7 +19,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from camr_b200 import distributed as D
-from camr_b200 import hydro
+from camr_b200 import hydro, native
 
 N = (16, 12, 8)
 MGS = (8, 6, 4)
@@ -349,3 +349,20 @@ def test_flux_register_two_coarse_calls_and_reset(oracle_kind):
     fr.reflux(mine)
     again = _assemble(cboxes, {c: t.numpy() for c, t in mine.items()})
     assert np.array_equal(again, want)
+
+
+def test_level_refuses_a_register_on_other_boxes(native_lib):
+    """attach_flux_register checks that the register's boxes of that role are
+    the level's own boxes (no device work: the level is only constructed)."""
+    geom = hydro.make_geom(N)
+    L = D.DistributedLevel(geom, native.default_params(), MGS, device=torch.device("cpu"))
+    ok = D.FluxRegister(geom, L.boxes, L.owner, FBOXES, [0] * len(FBOXES))
+    L.attach_flux_register(ok, "coarse")
+    other = hydro.level_boxes(N, (4, 6, 4))
+    bad = D.FluxRegister(geom, other, [0] * len(other), FBOXES, [0] * len(FBOXES))
+    with pytest.raises(ValueError, match="coarse boxes"):
+        L.attach_flux_register(bad, "coarse")
+    with pytest.raises(ValueError, match="fine boxes"):
+        L.attach_flux_register(ok, "fine")
+    with pytest.raises(ValueError):
+        L.attach_flux_register(ok, "middle")
