@@ -358,6 +358,17 @@ class DistributedLevel:
         self.grav = params.add_grav_src != 0
         self.registers = []
 
+    @classmethod
+    def from_inputs(cls, table, rank=0, nranks=1, pg=None, device=None):
+        """The level a CAMR inputs file describes (camr_b200.inputs: the
+        `CAMR.` parameters, the base geometry and boundary words,
+        amr.max_grid_size, which the file must give)."""
+        from . import inputs
+        geom, mgs = inputs.geometry(table)
+        if mgs is None:
+            raise ValueError("amr.max_grid_size is required for a box-distributed level")
+        return cls(geom, inputs.hydro_params(table), mgs, rank, nranks, pg, device)
+
     def attach_flux_register(self, fr, role):
         """After every hydro call of this level, pass its boxes' face fluxes
         to the flux register fr: CrseAdd when this level is the register's

@@ -118,3 +118,18 @@ def test_quotes_keep_blanks_and_hashes():
     t = inputs.parse('CAMR.job_name = "run #3 of 5"   # a comment\nx = a "b c" d')
     assert t["CAMR.job_name"] == ["run #3 of 5"]
     assert t["x"] == ["a", "b c", "d"]
+
+
+def test_distributed_level_from_inputs(native_lib):
+    """A box-distributed level built from an inputs file (constructed only:
+    no device work)."""
+    import torch
+
+    from camr_b200 import distributed as D
+    L = D.DistributedLevel.from_inputs(inputs.parse(SOD_X), device=torch.device("cpu"))
+    assert L.n == (128, 16, 16) and len(L.boxes) == 4
+    assert L.params.ppm_type == 1 and L.params.cfl == 0.6
+    assert [L.geom.bc_lo[k] for k in range(3)] == [1, 0, 0]
+    with pytest.raises(ValueError, match="max_grid_size"):
+        D.DistributedLevel.from_inputs(inputs.parse(SOD_X.replace("amr.max_grid_size", "#")),
+                                       device=torch.device("cpu"))
